@@ -1,0 +1,154 @@
+/*
+ * fnec_oracle.h -- CPU oracle for the Hallen method-of-moments hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is a plain-C restatement of the reference
+ * CPU path of dc0sk/fnec-rust (crates/nec_solver, apps/nec-cli) used as the
+ * checker for the CUDA library.  Only tests/, __graft_entry__.smoke() and the
+ * cpu_baseline / reference arm of bench.py may load it; the product library
+ * (libfnec_cuda.so) never links or calls it.
+ *
+ * Faithfulness rules: every function follows the cited reference function
+ * operation by operation, compiled with -O2 -ffp-contract=off (no FMA
+ * contraction, like rustc), against glibc libm (the libm Rust's f64::sin,
+ * cos, sqrt, ln, hypot, log10, asin and tan call on linux-gnu).  Complex
+ * arithmetic follows num-complex 0.4.6 (the version pinned in the
+ * reference's Cargo.lock): mul (ac-bd, ad+bc); div ((ac+bd)/|w|^2,
+ * (bc-ad)/|w|^2); norm = hypot; exp(0+jt) = (cos t, sin t).
+ *
+ * Parity pin: the golden values of corpus/reference-results.json (feedpoint
+ * impedances to 6 decimals, current samples, pattern samples to 4 decimals)
+ * are checked by tests/test_oracle_golden.py against this oracle.
+ */
+#ifndef FNEC_ORACLE_H
+#define FNEC_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* One wire segment; mirrors nec_solver::geometry::Segment (geometry.rs:115-134). */
+typedef struct {
+    uint32_t tag;
+    uint32_t tag_index;   /* 1-based index within the tag */
+    double start[3];
+    double end[3];
+    double mid[3];
+    double dir[3];
+    double length;
+    double radius;
+} or_seg;
+
+/* One GW card (geometry.rs:710-754 consumes these fields). */
+typedef struct {
+    uint32_t tag;
+    uint32_t segments;
+    double start[3];
+    double end[3];
+    double radius;
+} or_wire;
+
+/* One voltage-source EX card (types 0/5), in deck order. */
+typedef struct {
+    uint32_t tag;
+    uint32_t segment;
+    double v_re;
+    double v_im;
+} or_source;
+
+enum { OR_GROUND_FREE = 0, OR_GROUND_PEC = 1 };
+enum {
+    OR_OK = 0,
+    OR_ERR_SINGULAR = -1,
+    OR_ERR_ZERO_SEGMENTS = -2,
+    OR_ERR_ZERO_LENGTH = -3,
+    OR_ERR_NO_WIRES = -4,
+    OR_ERR_SEGMENT_NOT_FOUND = -5,
+    OR_ERR_CAPACITY = -6,
+    OR_ERR_DIM = -7
+};
+
+/* geometry.rs:676-754 (GW only). Returns N, or a negative error. */
+int64_t or_build_geometry(const or_wire *wires, int64_t nw, or_seg *out, int64_t cap);
+/* geometry.rs:168-185. out holds 2*cap int64 (first,last). Returns count. */
+int64_t or_wire_endpoints(const or_seg *segs, int64_t n, int64_t *out, int64_t cap);
+/* geometry.rs:200-225. */
+int64_t or_merge_collinear(const or_seg *segs, int64_t n, int64_t *out, int64_t cap);
+/* geometry.rs:274-339. Returns the number of junctions (may exceed cap:
+ * only the first cap are written). */
+int64_t or_detect_junctions(const or_seg *segs, const int64_t *ep, int64_t w, double tol,
+                            int64_t *ja, int64_t *jb, double *jsign, int64_t cap);
+/* solve_session.rs:1386-1400: merged endpoints + cross-component junctions. */
+int64_t or_cli_junctions(const or_seg *segs, int64_t n, const int64_t *merged, int64_t w,
+                         int64_t *ja, int64_t *jb, double *jsign, int64_t cap);
+/* excitation.rs:119-244.  rhs: 2n doubles (re,im); cosv: n doubles. */
+int or_hallen_rhs(const or_seg *segs, int64_t n, double freq_hz, const or_source *src,
+                  int64_t ns, double *rhs, double *cosv);
+/* excitation.rs:78-90 / :450-482 (V/dl per segment).  v: 2n doubles. */
+int or_excitation(const or_seg *segs, int64_t n, const or_source *src, int64_t ns, double *v);
+/* matrix.rs:186-218.  z: 2*n*n doubles, row-major, interleaved re/im. */
+void or_assemble_z(const or_seg *segs, int64_t n, double freq_hz, int ground, double *z);
+/* One element: matrix.rs:297-331 (elem) + image (:265-279) when ground=PEC. */
+void or_z_element(const or_seg *obs, const or_seg *src, double freq_hz, int ground,
+                  int is_self, double *out2);
+/* linear.rs:672-797 + :1321-1383.  x: 2*(n+w) doubles.  pivots (optional):
+ * n+w int32 pivot rows.  gram (optional): 2*S*(S+1) doubles, the augmented
+ * [A|b] before elimination.  naive != 0 runs the literal dense triple loop
+ * over M; naive == 0 skips structural zeros (value-identical, see .c). */
+int or_solve_hallen(const double *z, int64_t n, const double *rhs, const double *cosv,
+                    const int64_t *ep, int64_t w, const int64_t *ja, const int64_t *jb,
+                    const double *jsign, int64_t nj, double *x, int32_t *pivots,
+                    double *gram, int naive, int nthreads);
+/* linear.rs:1321-1383 on a dense S x S matrix a (2*S*S) and b (2*S).
+ * a and b are overwritten.  x: 2*S.  pivots optional. */
+int or_solve_square(double *a, double *b, int64_t s, double *x, int32_t *pivots, int nthreads);
+/* solve_session.rs:846-947 (voltage sources only): per EX card with a
+ * matching segment, (seg index, V, I, Zin).  out: 7 doubles per row
+ * (idx, v_re, v_im, i_re, i_im, z_re, z_im).  Returns row count. */
+int64_t or_feedpoints(const or_seg *segs, int64_t n, const or_source *src, int64_t ns,
+                      const double *cur, double *out, int64_t cap);
+/* farfield.rs:422-464 (PEC or free). */
+double or_integrate_power(const or_seg *segs, int64_t n, const double *cur, double freq_hz,
+                          int ground);
+/* farfield.rs:563-647.  pts: 2p (theta,phi deg).  out: 4 doubles per point
+ * (gain_total, gain_theta, gain_phi, axial_ratio).  total_out optional.
+ * uf_out optional: 4 doubles per point (F_theta re,im, F_phi re,im). */
+void or_radiation_pattern(const or_seg *segs, int64_t n, const double *cur, double freq_hz,
+                          int ground, const double *pts, int64_t p, double *out,
+                          double *total_out, double *uf_out);
+/* farfield.rs:677-699. pts: 2*max(nt,1)*max(np,1). Returns count. */
+int64_t or_rp_card_points(uint32_t n_theta, uint32_t n_phi, double theta0, double phi0,
+                          double d_theta, double d_phi, double *pts);
+
+/* A whole per-frequency solve of the CLI standard Hallen branch
+ * (solve_session.rs:1186-1437 + :1645): geometry -> rhs -> Z -> merged
+ * endpoints + junctions -> solve_hallen -> feedpoints -> pattern.  */
+typedef struct {
+    const or_wire *wires;
+    int64_t n_wires;
+    const or_source *sources;
+    int64_t n_sources;
+    int ground;
+    double freq_hz;
+    const double *points; /* 2*n_points (theta, phi) deg; may be NULL */
+    int64_t n_points;
+    /* outputs (caller-allocated) */
+    double *currents;     /* 2*N */
+    double *feed;         /* 7 * n_sources */
+    int64_t *n_feed;
+    double *pattern;      /* 4 * n_points */
+    int32_t *pivots;      /* S, optional */
+    int status;
+} or_problem;
+
+/* Solve one problem; returns its status. */
+int or_solve_problem(or_problem *p);
+/* Solve many independent problems on nthreads host threads (one problem per
+ * thread at a time), mirroring the reference's rayon per-frequency
+ * parallelism.  Each solve is single-threaded, as in the reference. */
+void or_solve_problems(or_problem *ps, int64_t count, int nthreads);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

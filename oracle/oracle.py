@@ -1,0 +1,314 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+The oracle is a C restatement of the reference CPU Hallen path
+(crates/nec_solver/src/{geometry,excitation,matrix,linear,farfield}.rs and
+apps/nec-cli/src/solve_session.rs); see fnec_oracle.c for per-function
+citations.  Only tests/, __graft_entry__.smoke() and bench.py's CPU arms
+import this module.  It is the checker, never the measured product.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "liboracle.so")
+
+SEG_DTYPE = np.dtype(
+    [
+        ("tag", "<u4"),
+        ("tag_index", "<u4"),
+        ("start", "<f8", 3),
+        ("end", "<f8", 3),
+        ("mid", "<f8", 3),
+        ("dir", "<f8", 3),
+        ("length", "<f8"),
+        ("radius", "<f8"),
+    ]
+)
+WIRE_DTYPE = np.dtype(
+    [("tag", "<u4"), ("segments", "<u4"), ("start", "<f8", 3), ("end", "<f8", 3), ("radius", "<f8")]
+)
+SOURCE_DTYPE = np.dtype([("tag", "<u4"), ("segment", "<u4"), ("v_re", "<f8"), ("v_im", "<f8")])
+
+GROUND_FREE = 0
+GROUND_PEC = 1
+
+_P = ctypes.c_void_p
+_I64 = ctypes.c_int64
+_D = ctypes.c_double
+
+
+class _Problem(ctypes.Structure):
+    _fields_ = [
+        ("wires", _P),
+        ("n_wires", _I64),
+        ("sources", _P),
+        ("n_sources", _I64),
+        ("ground", ctypes.c_int),
+        ("freq_hz", _D),
+        ("points", _P),
+        ("n_points", _I64),
+        ("currents", _P),
+        ("feed", _P),
+        ("n_feed", _P),
+        ("pattern", _P),
+        ("pivots", _P),
+        ("status", ctypes.c_int),
+    ]
+
+
+def build() -> str:
+    """Compile liboracle.so with the committed Makefile (gcc, no GPU)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.or_build_geometry.restype = _I64
+        L.or_build_geometry.argtypes = [_P, _I64, _P, _I64]
+        L.or_wire_endpoints.restype = _I64
+        L.or_wire_endpoints.argtypes = [_P, _I64, _P, _I64]
+        L.or_merge_collinear.restype = _I64
+        L.or_merge_collinear.argtypes = [_P, _I64, _P, _I64]
+        L.or_detect_junctions.restype = _I64
+        L.or_detect_junctions.argtypes = [_P, _P, _I64, _D, _P, _P, _P, _I64]
+        L.or_cli_junctions.restype = _I64
+        L.or_cli_junctions.argtypes = [_P, _I64, _P, _I64, _P, _P, _P, _I64]
+        L.or_hallen_rhs.restype = ctypes.c_int
+        L.or_hallen_rhs.argtypes = [_P, _I64, _D, _P, _I64, _P, _P]
+        L.or_excitation.restype = ctypes.c_int
+        L.or_excitation.argtypes = [_P, _I64, _P, _I64, _P]
+        L.or_assemble_z.restype = None
+        L.or_assemble_z.argtypes = [_P, _I64, _D, ctypes.c_int, _P]
+        L.or_solve_hallen.restype = ctypes.c_int
+        L.or_solve_hallen.argtypes = [_P, _I64, _P, _P, _P, _I64, _P, _P, _P, _I64, _P, _P, _P,
+                                      ctypes.c_int, ctypes.c_int]
+        L.or_solve_square.restype = ctypes.c_int
+        L.or_solve_square.argtypes = [_P, _P, _I64, _P, _P, ctypes.c_int]
+        L.or_feedpoints.restype = _I64
+        L.or_feedpoints.argtypes = [_P, _I64, _P, _I64, _P, _P, _I64]
+        L.or_integrate_power.restype = _D
+        L.or_integrate_power.argtypes = [_P, _I64, _P, _D, ctypes.c_int]
+        L.or_radiation_pattern.restype = None
+        L.or_radiation_pattern.argtypes = [_P, _I64, _P, _D, ctypes.c_int, _P, _I64, _P, _P, _P]
+        L.or_rp_card_points.restype = _I64
+        L.or_rp_card_points.argtypes = [ctypes.c_uint32, ctypes.c_uint32, _D, _D, _D, _D, _P]
+        L.or_solve_problem.restype = ctypes.c_int
+        L.or_solve_problem.argtypes = [_P]
+        L.or_solve_problems.restype = None
+        L.or_solve_problems.argtypes = [_P, _I64, ctypes.c_int]
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def wires_array(wires) -> np.ndarray:
+    """wires: iterable of (tag, segments, start3, end3, radius)."""
+    arr = np.zeros(len(wires), dtype=WIRE_DTYPE)
+    for i, (tag, nseg, s, e, r) in enumerate(wires):
+        arr[i] = (tag, nseg, s, e, r)
+    return arr
+
+
+def sources_array(sources) -> np.ndarray:
+    """sources: iterable of (tag, segment, v_complex)."""
+    arr = np.zeros(len(sources), dtype=SOURCE_DTYPE)
+    for i, (tag, seg, v) in enumerate(sources):
+        arr[i] = (tag, seg, complex(v).real, complex(v).imag)
+    return arr
+
+
+class OracleError(RuntimeError):
+    pass
+
+
+def build_geometry(wires: np.ndarray) -> np.ndarray:
+    cap = int(wires["segments"].sum())
+    out = np.zeros(max(cap, 1), dtype=SEG_DTYPE)
+    n = lib().or_build_geometry(_ptr(wires), len(wires), _ptr(out), cap)
+    if n < 0:
+        raise OracleError(f"build_geometry: status {n}")
+    return out[:n]
+
+
+def wire_endpoints(segs: np.ndarray) -> np.ndarray:
+    cnt = lib().or_wire_endpoints(_ptr(segs), len(segs), None, 0)
+    out = np.zeros((max(cnt, 1), 2), dtype=np.int64)
+    lib().or_wire_endpoints(_ptr(segs), len(segs), _ptr(out), cnt)
+    return out[:cnt]
+
+
+def merge_collinear(segs: np.ndarray) -> np.ndarray:
+    cnt = lib().or_merge_collinear(_ptr(segs), len(segs), None, 0)
+    out = np.zeros((max(cnt, 1), 2), dtype=np.int64)
+    lib().or_merge_collinear(_ptr(segs), len(segs), _ptr(out), cnt)
+    return out[:cnt]
+
+
+def detect_junctions(segs, endpoints, tol=1e-6):
+    ep = np.ascontiguousarray(endpoints, dtype=np.int64)
+    cnt = lib().or_detect_junctions(_ptr(segs), _ptr(ep), len(ep), tol, None, None, None, 0)
+    a = np.zeros(max(cnt, 1), np.int64)
+    b = np.zeros(max(cnt, 1), np.int64)
+    s = np.zeros(max(cnt, 1), np.float64)
+    lib().or_detect_junctions(_ptr(segs), _ptr(ep), len(ep), tol, _ptr(a), _ptr(b), _ptr(s), cnt)
+    return a[:cnt], b[:cnt], s[:cnt]
+
+
+def cli_junctions(segs, merged):
+    ep = np.ascontiguousarray(merged, dtype=np.int64)
+    cnt = lib().or_cli_junctions(_ptr(segs), len(segs), _ptr(ep), len(ep), None, None, None, 0)
+    a = np.zeros(max(cnt, 1), np.int64)
+    b = np.zeros(max(cnt, 1), np.int64)
+    s = np.zeros(max(cnt, 1), np.float64)
+    lib().or_cli_junctions(_ptr(segs), len(segs), _ptr(ep), len(ep), _ptr(a), _ptr(b), _ptr(s), cnt)
+    return a[:cnt], b[:cnt], s[:cnt]
+
+
+def hallen_rhs(segs, freq_hz, sources):
+    n = len(segs)
+    rhs = np.zeros(n, np.complex128)
+    cosv = np.zeros(n, np.float64)
+    st = lib().or_hallen_rhs(_ptr(segs), n, freq_hz, _ptr(sources), len(sources), _ptr(rhs), _ptr(cosv))
+    if st != 0:
+        raise OracleError(f"hallen_rhs: status {st}")
+    return rhs, cosv
+
+
+def excitation(segs, sources):
+    v = np.zeros(len(segs), np.complex128)
+    st = lib().or_excitation(_ptr(segs), len(segs), _ptr(sources), len(sources), _ptr(v))
+    if st != 0:
+        raise OracleError(f"excitation: status {st}")
+    return v
+
+
+def assemble_z(segs, freq_hz, ground=GROUND_FREE):
+    n = len(segs)
+    z = np.zeros((n, n), np.complex128)
+    lib().or_assemble_z(_ptr(segs), n, freq_hz, ground, _ptr(z))
+    return z
+
+
+def solve_hallen(z, rhs, cosv, endpoints, ja, jb, js, naive=False, want_gram=False, nthreads=1):
+    n = z.shape[0]
+    z = np.ascontiguousarray(z, np.complex128)
+    rhs = np.ascontiguousarray(rhs, np.complex128)
+    cosv = np.ascontiguousarray(cosv, np.float64)
+    ep = np.ascontiguousarray(endpoints, np.int64).reshape(-1, 2)
+    w = len(ep) if (len(ep) > 0 and n > 0) else (1 if n > 0 else 0)
+    ja = np.ascontiguousarray(ja, np.int64)
+    jb = np.ascontiguousarray(jb, np.int64)
+    js = np.ascontiguousarray(js, np.float64)
+    s = n + w
+    x = np.zeros(s, np.complex128)
+    piv = np.zeros(max(s, 1), np.int32)
+    gram = np.zeros((s, s + 1), np.complex128) if want_gram else None
+    st = lib().or_solve_hallen(_ptr(z), n, _ptr(rhs), _ptr(cosv), _ptr(ep), len(ep), _ptr(ja), _ptr(jb),
+                               _ptr(js), len(ja), _ptr(x), _ptr(piv), _ptr(gram), int(naive), nthreads)
+    if st != 0:
+        raise OracleError(f"solve_hallen: status {st}")
+    return (x, piv[:s], gram) if want_gram else (x, piv[:s])
+
+
+def solve_square(a, b, nthreads=1):
+    s = a.shape[0]
+    a = np.array(a, np.complex128, order="C")
+    b = np.array(b, np.complex128)
+    x = np.zeros(s, np.complex128)
+    piv = np.zeros(max(s, 1), np.int32)
+    st = lib().or_solve_square(_ptr(a), _ptr(b), s, _ptr(x), _ptr(piv), nthreads)
+    return st, x, piv[:s]
+
+
+def feedpoints(segs, sources, currents):
+    out = np.zeros((max(len(sources), 1), 7), np.float64)
+    cur = np.ascontiguousarray(currents, np.complex128)
+    cnt = lib().or_feedpoints(_ptr(segs), len(segs), _ptr(sources), len(sources), _ptr(cur), _ptr(out),
+                              len(sources))
+    return out[:cnt]
+
+
+def integrate_power(segs, currents, freq_hz, ground=GROUND_FREE):
+    cur = np.ascontiguousarray(currents, np.complex128)
+    return lib().or_integrate_power(_ptr(segs), len(segs), _ptr(cur), freq_hz, ground)
+
+
+def radiation_pattern(segs, currents, freq_hz, points, ground=GROUND_FREE, want_fields=False):
+    pts = np.ascontiguousarray(points, np.float64).reshape(-1, 2)
+    cur = np.ascontiguousarray(currents, np.complex128)
+    out = np.zeros((len(pts), 4), np.float64)
+    tot = np.zeros(1, np.float64)
+    uf = np.zeros((len(pts), 2), np.complex128) if want_fields else None
+    lib().or_radiation_pattern(_ptr(segs), len(segs), _ptr(cur), freq_hz, ground, _ptr(pts), len(pts),
+                               _ptr(out), _ptr(tot), _ptr(uf))
+    if want_fields:
+        return out, float(tot[0]), uf
+    return out, float(tot[0])
+
+
+def rp_card_points(n_theta, n_phi, theta0, phi0, d_theta, d_phi):
+    cnt = lib().or_rp_card_points(n_theta, n_phi, theta0, phi0, d_theta, d_phi, None)
+    pts = np.zeros((cnt, 2), np.float64)
+    lib().or_rp_card_points(n_theta, n_phi, theta0, phi0, d_theta, d_phi, _ptr(pts))
+    return pts
+
+
+class Problem:
+    """One per-frequency CLI standard-branch solve (solve_session.rs:1186-1437)."""
+
+    def __init__(self, wires, sources, freq_hz, ground=GROUND_FREE, points=None):
+        self.wires = np.ascontiguousarray(wires)
+        self.sources = np.ascontiguousarray(sources)
+        self.freq_hz = float(freq_hz)
+        self.ground = int(ground)
+        self.points = None if points is None else np.ascontiguousarray(points, np.float64).reshape(-1, 2)
+        n = int(self.wires["segments"].sum())
+        w = len(self.wires)
+        self.currents = np.zeros(n, np.complex128)
+        self.feed = np.zeros((max(len(self.sources), 1), 7), np.float64)
+        self.n_feed = np.zeros(1, np.int64)
+        npts = 0 if self.points is None else len(self.points)
+        self.pattern = np.zeros((max(npts, 1), 4), np.float64)
+        self.pivots = np.zeros(n + w, np.int32)
+        self._s = _Problem(
+            _ptr(self.wires), len(self.wires), _ptr(self.sources), len(self.sources), self.ground,
+            self.freq_hz, _ptr(self.points), npts, _ptr(self.currents), _ptr(self.feed),
+            _ptr(self.n_feed), _ptr(self.pattern), _ptr(self.pivots), 0)
+
+    @property
+    def status(self):
+        return self._s.status
+
+    @property
+    def zin(self):
+        f = self.feed[: int(self.n_feed[0])]
+        return f[:, 5] + 1j * f[:, 6]
+
+
+def solve_problem(p: Problem) -> Problem:
+    lib().or_solve_problem(ctypes.byref(p._s))
+    return p
+
+
+def solve_problems(problems, nthreads: int):
+    arr = (_Problem * len(problems))(*[p._s for p in problems])
+    lib().or_solve_problems(ctypes.cast(arr, _P), len(problems), int(nthreads))
+    for i, p in enumerate(problems):
+        p._s = arr[i]
+    return problems
