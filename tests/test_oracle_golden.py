@@ -1,0 +1,163 @@
+"""Pin the CPU oracle against the reference's own golden corpus and unit tests.
+
+Tolerances follow the printed precision of corpus/reference-results.json:
+impedances carry 6 decimals (we allow 2 units of the last digit: the
+multi-source case's second feed differs from our restatement by 1 unit,
+6e-9 relative, which is the size of libm/platform differences amplified by
+cond(A) ~ 5e6 of the regularised normal equations), pattern gains carry 4
+decimals (we allow 1 unit of the last digit), current magnitudes 7
+significant digits, phases 4 decimals.
+"""
+import numpy as np
+import pytest
+
+from _corpus import deck_arrays, golden_zins, load_cases
+from oracle import oracle as O
+
+CASES = load_cases()
+
+
+def _decimals(v):
+    t = repr(float(v))
+    return len(t.split(".")[1]) if "." in t and "e" not in t else 0
+
+
+def _zin_tol(case, want):
+    """2 units of the last printed digit for 6-decimal regression values;
+    values captured from the reference's Python study (2 decimals, the
+    unregularised least-squares answer) use the case's own absolute gate."""
+    d = min(_decimals(want.real), _decimals(want.imag))
+    if d >= 6:
+        return 2e-6
+    return case["tolerance_gates"]["R_absolute_ohm"]
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_feedpoint_impedance_matches_golden(name):
+    case = CASES[name]
+    wires, sources, _ = deck_arrays(case["deck"])
+    for f, zs in golden_zins(case).items():
+        p = O.solve_problem(O.Problem(wires, sources, f, ground=case["deck"]["ground"]))
+        assert p.status == 0
+        assert len(p.zin) == len(zs)
+        for got, want in zip(p.zin, zs):
+            tol = _zin_tol(case, want)
+            assert abs(got.real - want.real) <= tol, (name, f, got, want, tol)
+            assert abs(got.imag - want.imag) <= tol, (name, f, got, want, tol)
+
+
+@pytest.mark.parametrize("name", [n for n in sorted(CASES) if "pattern_samples" in CASES[n]])
+def test_pattern_samples_match_golden(name):
+    case = CASES[name]
+    wires, sources, _ = deck_arrays(case["deck"])
+    samples = case["pattern_samples"]
+    pts = np.array([[s["theta_deg"], s["phi_deg"]] for s in samples])
+    p = O.Problem(wires, sources, case["deck"]["freqs"][0], ground=case["deck"]["ground"], points=pts)
+    O.solve_problem(p)
+    for s, row in zip(samples, p.pattern):
+        for key, col in (("gain_db", 0), ("gain_v_db", 1), ("gain_h_db", 2), ("axial_ratio", 3)):
+            assert abs(row[col] - s[key]) <= 1.0e-4 + 1e-12, (name, s, row)
+
+
+@pytest.mark.parametrize("name", [n for n in sorted(CASES) if "current_samples" in CASES[n]])
+def test_current_samples_match_golden(name):
+    case = CASES[name]
+    wires, sources, _ = deck_arrays(case["deck"])
+    p = O.solve_problem(O.Problem(wires, sources, case["deck"]["freqs"][0], ground=case["deck"]["ground"]))
+    segs = O.build_geometry(wires)
+    for s in case["current_samples"]:
+        idx = int(np.nonzero((segs["tag"] == s["wire_id"]) & (segs["tag_index"] == s["segment_id"]))[0][0])
+        cur = p.currents[idx]
+        # the report's "amplitude" column is |I| in amperes (7 significant digits)
+        assert abs(abs(cur) - s["amplitude_db"]) <= 1e-6 * abs(s["amplitude_db"]) + 1e-13
+        assert abs(np.degrees(np.angle(cur)) - s["phase_deg"]) <= 1e-4
+
+
+def _yagi():
+    cases = load_cases()
+    return deck_arrays(cases["yagi-5elm-51seg"]["deck"])
+
+
+def test_sparse_gram_is_bit_identical_to_literal_triple_loop():
+    """linear.rs:765-780 literal dense loop vs the structural-zero skip."""
+    for name in ("dipole-freesp-51seg", "yagi-5elm-51seg", "dipole-ground-51seg"):
+        wires, sources, _ = deck_arrays(CASES[name]["deck"])
+        segs = O.build_geometry(wires)
+        f = CASES[name]["deck"]["freqs"][0]
+        rhs, cosv = O.hallen_rhs(segs, f, sources)
+        z = O.assemble_z(segs, f, CASES[name]["deck"]["ground"])
+        m = O.merge_collinear(segs)
+        ja, jb, js = O.cli_junctions(segs, m)
+        x0, p0, g0 = O.solve_hallen(z, rhs, cosv, m, ja, jb, js, naive=True, want_gram=True)
+        x1, p1, g1 = O.solve_hallen(z, rhs, cosv, m, ja, jb, js, naive=False, want_gram=True)
+        assert np.array_equal(g0.view(np.uint64), g1.view(np.uint64))
+        assert np.array_equal(x0.view(np.uint64), x1.view(np.uint64))
+        assert np.array_equal(p0, p1)
+
+
+def test_junction_rows_and_gram_with_junctions_bit_identical():
+    """A bent 3-wire chain (junctions present) through both Gram forms."""
+    wires = O.wires_array([(1, 7, (0, 0, 0), (0, 0, 2.0), 1e-3), (2, 5, (0, 0, 2.0), (1.5, 0, 2.0), 1e-3),
+                           (3, 6, (1.5, 0, 2.0), (1.5, 0, 0.2), 1e-3), (4, 3, (0, 0, 2.0), (-1, 0, 2.5), 1e-3)])
+    sources = O.sources_array([(1, 4, 1.0)])
+    segs = O.build_geometry(wires)
+    rhs, cosv = O.hallen_rhs(segs, 30e6, sources)
+    z = O.assemble_z(segs, 30e6, 1)
+    m = O.merge_collinear(segs)
+    ja, jb, js = O.cli_junctions(segs, m)
+    assert len(ja) == 4  # 3-way node: 3 pairs; one 2-way node: 1
+    x0, p0, g0 = O.solve_hallen(z, rhs, cosv, m, ja, jb, js, naive=True, want_gram=True)
+    x1, p1, g1 = O.solve_hallen(z, rhs, cosv, m, ja, jb, js, naive=False, want_gram=True)
+    assert np.array_equal(g0.view(np.uint64), g1.view(np.uint64))
+    assert np.array_equal(x0.view(np.uint64), x1.view(np.uint64))
+
+
+def test_gepp_known_answers():
+    """linear.rs:1412-1493: 1x1, 2x2 real, 2x2 complex, 3x3 residual, singular."""
+    st, x, _ = O.solve_square(np.array([[2.0]], complex), np.array([4.0], complex))
+    assert st == 0 and abs(x[0] - 2) < 1e-12
+    st, x, _ = O.solve_square(np.array([[3, 1], [1, 2]], complex), np.array([4, 3], complex))
+    assert st == 0 and np.allclose(x, [1, 1], atol=1e-12)
+    st, x, _ = O.solve_square(np.array([[1 + 1j, 0], [0, 2]]), np.array([1 + 1j, 4]))
+    assert st == 0 and np.allclose(x, [1, 2], atol=1e-12)
+    a = np.array([[4 + 1j, 1, -1j], [1, 5 + 2j, 1], [-1j, 1, 3 + 1j]])
+    b = np.array([2 + 1j, 3 - 1j, 1])
+    st, x, _ = O.solve_square(a, b)
+    assert st == 0 and np.abs(a @ x - b).max() < 1e-10
+    st, x, _ = O.solve_square(np.array([[1, 2], [2, 4]], complex), np.array([1, 2], complex))
+    assert st == O.lib().or_solve_square.restype(-1).value if False else st == -1
+
+
+def test_gepp_last_maximum_tie_rule():
+    """Iterator::max_by returns the last of equal maxima (linear.rs:1345)."""
+    a = np.array([[1, 0, 0], [1, 2, 0], [-1, 0, 3]], complex)
+    st, x, piv = O.solve_square(a, np.array([1, 1, 1], complex))
+    assert st == 0 and piv[0] == 2
+
+
+def test_row_parallel_gepp_bit_identical():
+    rng = np.random.default_rng(3)
+    s = 150
+    a = rng.standard_normal((s, s)) + 1j * rng.standard_normal((s, s))
+    b = rng.standard_normal(s) + 1j * rng.standard_normal(s)
+    _, x1, p1 = O.solve_square(a, b, nthreads=1)
+    _, x4, p4 = O.solve_square(a, b, nthreads=4)
+    assert np.array_equal(x1.view(np.uint64), x4.view(np.uint64)) and np.array_equal(p1, p4)
+
+
+def test_hertzian_dipole_and_pec_gain():
+    """farfield.rs:833-974: short element ~1.76 dBi at the equator, deep null on axis."""
+    seg = np.zeros(1, dtype=O.SEG_DTYPE)
+    seg[0]["start"] = (0, 0, -0.005)
+    seg[0]["end"] = (0, 0, 0.005)
+    seg[0]["dir"] = (0, 0, 1)
+    seg[0]["length"] = 0.01
+    seg[0]["radius"] = 1e-4
+    out, _ = O.radiation_pattern(seg, np.array([1.0 + 0j]), 14.2e6, [[90, 0], [0, 0]])
+    assert abs(out[0, 0] - 1.76) < 0.01 and out[1, 0] < -10
+    assert out[0, 2] < -10 and out[0, 1] > 0
+
+
+def test_rp_card_points_order():
+    pts = O.rp_card_points(2, 2, 10.0, 20.0, 30.0, 40.0)
+    assert np.allclose(pts, [[10, 20], [40, 20], [10, 60], [40, 60]])
