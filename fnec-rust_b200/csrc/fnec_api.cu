@@ -1,0 +1,1269 @@
+// fnec_api.cu -- host orchestration and the C ABI of libfnec_cuda.so.
+//
+// Host work is the small, branchy topology of a geometry (wire endpoint
+// runs, collinear merge, junction pairs, constraint rows, resolved sources,
+// feedpoint rows, wire runs for the far field); it follows the reference
+// functions cited inline with the same IEEE arithmetic (built with
+// -ffp-contract=off).  Everything proportional to N^2 or N^3 runs on the
+// device: segment expansion, Hallen RHS, Z fill, Gram, factorisation,
+// solve, feedpoints and the pattern grid.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "fnec_cuda.h"
+#include "fnec_kernels.h"
+#include "fnec_mixed.h"
+
+using namespace fnec;
+
+namespace {
+
+constexpr double PI = 3.14159265358979323846;
+constexpr double C0 = 299792458.0;
+
+struct Err {
+    int code;
+    std::string msg;
+};
+
+}  // namespace
+
+struct fnec_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+};
+
+static int fail(fnec_ctx *c, int code, const std::string &msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+#define CUDA_TRY(ctx, call)                                                                   \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) {                                                              \
+            int code_ = (e_ == cudaErrorMemoryAllocation) ? FNEC_ERR_OUT_OF_MEMORY : FNEC_ERR_CUDA; \
+            return fail((ctx), code_, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+        }                                                                                     \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// host restatements needed for topology (same arithmetic as k_expand_segments)
+// ---------------------------------------------------------------------------
+static DevSeg host_seg(const fnec_wire &gw, uint32_t i) {
+    double dx = gw.end[0] - gw.start[0], dy = gw.end[1] - gw.start[1], dz = gw.end[2] - gw.start[2];
+    double wl = std::sqrt(dx * dx + dy * dy + dz * dz);
+    double nn = (double)gw.segments;
+    double t0 = (double)i / nn, t1 = ((double)i + 1.0) / nn, tm = (t0 + t1) * 0.5;
+    DevSeg s;
+    s.start[0] = gw.start[0] + dx * t0;
+    s.start[1] = gw.start[1] + dy * t0;
+    s.start[2] = gw.start[2] + dz * t0;
+    s.end[0] = gw.start[0] + dx * t1;
+    s.end[1] = gw.start[1] + dy * t1;
+    s.end[2] = gw.start[2] + dz * t1;
+    s.mid[0] = gw.start[0] + dx * tm;
+    s.mid[1] = gw.start[1] + dy * tm;
+    s.mid[2] = gw.start[2] + dz * tm;
+    s.dir[0] = dx / wl;
+    s.dir[1] = dy / wl;
+    s.dir[2] = dz / wl;
+    s.len = wl / nn;
+    s.rad = gw.radius;
+    s.tag = gw.tag;
+    s.tag_index = i + 1;
+    s.pad = 0.0;
+    return s;
+}
+
+static double dist2(const double *a, const double *b) {
+    double d0 = a[0] - b[0], d1 = a[1] - b[1], d2 = a[2] - b[2];
+    return d0 * d0 + d1 * d1 + d2 * d2;
+}
+
+// geometry.rs:227-236
+static bool dir_aligned(const double *a, const double *b, double tol) {
+    double cr[3] = {a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]};
+    double zero[3] = {0, 0, 0};
+    double dot = a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+    return dist2(cr, zero) < tol * tol && dot > 0.0;
+}
+
+namespace {
+
+// Everything the device needs for one antenna, before packing.
+struct HostAnt {
+    std::vector<DevWire> wires;     // empty for caller-provided segments
+    std::vector<DevSeg> segs;       // host copies of the segments
+    int ground = 0;
+    std::vector<std::pair<int64_t, int64_t>> ep;  // column wires (first, last)
+    std::vector<int32_t> comp;      // 2n merged component (first, last) per segment
+    std::vector<int64_t> ja, jb;    // junction rows
+    std::vector<double> js;
+    std::vector<DevSource> srcs;
+    std::vector<DevFeed> feeds;
+    std::vector<DevRun> runs;
+    DevRp rp{};
+    std::vector<double> pts;        // explicit points (theta, phi)
+    std::vector<double> freqs;
+    bool rhs_given = false;         // caller supplies rhs/cos (one unit)
+    std::vector<double> rhs, cosv;  // 2n, n
+    std::vector<double> z;          // caller-supplied Z (2 n^2), else filled on the device
+};
+
+}  // namespace
+
+// geometry.rs:168-185 over the segment list
+static std::vector<std::pair<int64_t, int64_t>> wire_endpoints(const std::vector<DevSeg> &s) {
+    std::vector<std::pair<int64_t, int64_t>> out;
+    uint32_t cur = UINT32_MAX;
+    int64_t first = 0;
+    for (int64_t i = 0; i < (int64_t)s.size(); ++i) {
+        if (s[i].tag != cur) {
+            if (cur != UINT32_MAX) out.push_back({first, i - 1});
+            cur = s[i].tag;
+            first = i;
+        }
+    }
+    if (cur != UINT32_MAX) out.push_back({first, (int64_t)s.size() - 1});
+    return out;
+}
+
+// geometry.rs:200-225
+static std::vector<std::pair<int64_t, int64_t>> merge_collinear(const std::vector<DevSeg> &s) {
+    auto base = wire_endpoints(s);
+    if (base.size() < 2) return base;
+    const double POS_TOL = 1e-6, DIR_TOL = 1e-6;
+    std::vector<std::pair<int64_t, int64_t>> merged;
+    auto cur = base[0];
+    for (size_t k = 1; k < base.size(); ++k) {
+        auto nx = base[k];
+        const DevSeg &a = s[cur.second];
+        const DevSeg &b = s[nx.first];
+        bool contiguous = cur.second + 1 == nx.first;
+        bool connects = dist2(a.end, b.start) < POS_TOL * POS_TOL;
+        bool collinear = dir_aligned(a.dir, b.dir, DIR_TOL);
+        bool same_radius = std::fabs(a.rad - b.rad) < POS_TOL;
+        if (contiguous && connects && collinear && same_radius) {
+            cur.second = nx.second;
+        } else {
+            merged.push_back(cur);
+            cur = nx;
+        }
+    }
+    merged.push_back(cur);
+    return merged;
+}
+
+// geometry.rs:274-339 + solve_session.rs:1386-1400 (cross-component pairs)
+static void cli_junctions(const std::vector<DevSeg> &s,
+                          const std::vector<std::pair<int64_t, int64_t>> &ep, HostAnt &h) {
+    size_t nn = 2 * ep.size();
+    std::vector<int64_t> comp(s.size(), 0);
+    for (size_t c = 0; c < ep.size(); ++c)
+        for (int64_t m = ep[c].first; m <= ep[c].second; ++m) comp[m] = (int64_t)c;
+    for (size_t i = 0; i < nn; ++i) {
+        int64_t si = (i % 2 == 0) ? ep[i / 2].first : ep[i / 2].second;
+        bool st_i = i % 2 == 0;
+        const double *pi = st_i ? s[si].start : s[si].end;
+        for (size_t j = i + 1; j < nn; ++j) {
+            int64_t sj = (j % 2 == 0) ? ep[j / 2].first : ep[j / 2].second;
+            if (si == sj) continue;
+            bool st_j = j % 2 == 0;
+            const double *pj = st_j ? s[sj].start : s[sj].end;
+            double dx = pi[0] - pj[0], dy = pi[1] - pj[1], dz = pi[2] - pj[2];
+            if (std::sqrt(dx * dx + dy * dy + dz * dz) > 1e-6) continue;
+            if (comp[si] == comp[sj]) continue;
+            h.ja.push_back(si);
+            h.jb.push_back(sj);
+            h.js.push_back(st_i == st_j ? 1.0 : -1.0);
+        }
+    }
+}
+
+static int64_t find_seg(const std::vector<DevSeg> &s, uint32_t tag, uint32_t idx) {
+    for (int64_t i = 0; i < (int64_t)s.size(); ++i)
+        if (s[i].tag == tag && s[i].tag_index == idx) return i;
+    return -1;
+}
+
+// Wire runs for the far-field Horner sum: consecutive segments with the
+// same direction and length whose midpoints advance by a constant step.
+static void build_runs(HostAnt &h) {
+    const auto &s = h.segs;
+    int64_t n = (int64_t)s.size();
+    int64_t i = 0;
+    while (i < n) {
+        int64_t j = i + 1;
+        double step[3] = {0, 0, 0};
+        if (j < n) {
+            for (int c = 0; c < 3; ++c) step[c] = s[j].mid[c] - s[i].mid[c];
+        }
+        double sl = std::sqrt(step[0] * step[0] + step[1] * step[1] + step[2] * step[2]);
+        while (j < n) {
+            bool same = s[j].dir[0] == s[i].dir[0] && s[j].dir[1] == s[i].dir[1] &&
+                        s[j].dir[2] == s[i].dir[2] && s[j].len == s[i].len;
+            double e = 0;
+            for (int c = 0; c < 3; ++c) {
+                double pred = s[i].mid[c] + step[c] * (double)(j - i);
+                e = std::max(e, std::fabs(pred - s[j].mid[c]));
+            }
+            double scale = std::max(1.0, std::fabs(s[j].mid[0]) + std::fabs(s[j].mid[1]) + std::fabs(s[j].mid[2]));
+            if (!same || sl == 0.0 || e > 1e-12 * scale) break;
+            ++j;
+        }
+        DevRun r{};
+        for (int c = 0; c < 3; ++c) {
+            r.mid0[c] = s[i].mid[c];
+            r.step[c] = (j - i > 1) ? step[c] : 0.0;
+            r.dir[c] = s[i].dir[c];
+        }
+        r.len = s[i].len;
+        r.first = (int32_t)i;
+        r.count = (int32_t)(j - i);
+        h.runs.push_back(r);
+        i = j;
+    }
+}
+
+// excitation.rs:119-187 source resolution and :78-90 / solve_session.rs:846-917 feed rows.
+static int resolve_sources(HostAnt &h, const fnec_source *src, uint32_t ns, std::string &why) {
+    const auto &s = h.segs;
+    if (ns == 0) return FNEC_OK;
+    std::vector<int64_t> idx(ns);
+    for (uint32_t e = 0; e < ns; ++e) {
+        idx[e] = find_seg(s, src[e].tag, src[e].segment);
+        if (idx[e] < 0) {
+            why = "EX: no segment with tag " + std::to_string(src[e].tag) + ", index " +
+                  std::to_string(src[e].segment);
+            return FNEC_ERR_SEGMENT_NOT_FOUND;
+        }
+    }
+    uint32_t driven = s[idx[0]].tag;
+    std::map<uint32_t, std::pair<int64_t, std::pair<double, double>>> by_tag;
+    by_tag[driven] = {idx[0], {src[0].v_re, src[0].v_im}};
+    for (uint32_t e = 0; e < ns; ++e) {
+        if (src[e].tag == driven) continue;
+        by_tag[src[e].tag] = {idx[e], {src[e].v_re, src[e].v_im}};
+    }
+    for (auto &kv : by_tag) {
+        DevSource d{};
+        d.feed = (int32_t)kv.second.first;
+        d.comp_first = h.comp[2 * d.feed];
+        d.comp_last = h.comp[2 * d.feed + 1];
+        d.v_re = kv.second.second.first;
+        d.v_im = kv.second.second.second;
+        h.srcs.push_back(d);
+    }
+    // feed rows: v_vec[idx] accumulates V/dl of every card on that segment
+    for (uint32_t e = 0; e < ns; ++e) {
+        DevFeed f{};
+        f.seg = (int32_t)idx[e];
+        double re = 0.0, im = 0.0;
+        for (uint32_t q = 0; q < ns; ++q) {
+            if (idx[q] != idx[e]) continue;
+            double dl = s[idx[q]].len;
+            re = re + src[q].v_re / dl;
+            im = im + src[q].v_im / dl;
+        }
+        f.vdl_re = re;
+        f.vdl_im = im;
+        h.feeds.push_back(f);
+    }
+    return FNEC_OK;
+}
+
+static void set_comp(HostAnt &h, const std::vector<std::pair<int64_t, int64_t>> &merged) {
+    h.comp.assign(2 * h.segs.size(), 0);
+    for (auto &c : merged)
+        for (int64_t m = c.first; m <= c.second; ++m) {
+            h.comp[2 * m] = (int32_t)c.first;
+            h.comp[2 * m + 1] = (int32_t)c.second;
+        }
+}
+
+// ---------------------------------------------------------------------------
+// batch
+// ---------------------------------------------------------------------------
+struct fnec_batch {
+    fnec_ctx *ctx = nullptr;
+    int precision = 0;
+    // packed host tables
+    std::vector<DevWire> wires;
+    std::vector<DevSeg> segs;  // uploaded when the batch has no wires
+    bool from_wires = true;
+    std::vector<AntDesc> ants;
+    std::vector<UnitDesc> units;
+    std::vector<int32_t> ibuf;
+    std::vector<DevSource> srcs;
+    std::vector<DevFeed> feeds;
+    std::vector<DevConstraint> cons;
+    std::vector<int32_t> codes;
+    std::vector<DevRun> runs;
+    std::vector<DevRp> rps;
+    std::vector<double> pts;
+    std::vector<int4> fill_tiles, gram_tiles;
+    std::vector<int64_t> feed_row_off;
+    std::vector<double> rhs_given;   // 2 * total rhs
+    std::vector<double> cos_given;
+    bool rhs_given_flag = false;
+    std::vector<double> z_given;  // caller-supplied Z for every unit (fill skipped)
+    std::vector<fnec_unit_info> uinfo;
+    int max_s = 0, max_n = 0;
+    int64_t tot_seg = 0, z_el = 0, a_el = 0, x_el = 0, rhs_el = 0, pat_el = 0, feed_rows = 0;
+    int ff_blocks = 0;
+    size_t ff_smem = 0;
+    uint64_t launches = 0;
+    uint64_t h2d = 0;
+    // device
+    DevWire *d_wires = nullptr;
+    DevSeg *d_segs = nullptr;
+    AntDesc *d_ants = nullptr;
+    UnitDesc *d_units = nullptr;
+    int32_t *d_ibuf = nullptr;
+    DevSource *d_srcs = nullptr;
+    DevFeed *d_feeds = nullptr;
+    DevConstraint *d_cons = nullptr;
+    int32_t *d_codes = nullptr;
+    DevRun *d_runs = nullptr;
+    DevRp *d_rps = nullptr;
+    double *d_pts = nullptr;
+    int4 *d_fill_tiles = nullptr, *d_gram_tiles = nullptr;
+    int64_t *d_feed_row_off = nullptr;
+    double *d_rhs_given = nullptr, *d_cos_given = nullptr, *d_z_given = nullptr;
+    cx *d_z = nullptr, *d_a = nullptr, *d_x = nullptr, *d_rhs = nullptr;
+    double *d_cos = nullptr;
+    int32_t *d_piv = nullptr, *d_status = nullptr;
+    double *d_feed_out = nullptr, *d_fld = nullptr, *d_partials = nullptr, *d_pat = nullptr,
+           *d_total = nullptr;
+    MixedWork mixed;
+    size_t dev_bytes = 0;
+    std::vector<void *> allocs;
+    // packed input arena: one pinned host buffer mirrored by one device buffer
+    unsigned char *h_in = nullptr;
+    unsigned char *d_in = nullptr;
+    size_t in_bytes = 0;
+    // pinned staging of the results
+    unsigned char *h_out = nullptr;
+    size_t out_bytes = 0;
+    // per-phase CUDA events (profiling on)
+    bool profile = false;
+    cudaEvent_t ev[FNEC_N_PHASES + 1] = {};
+    bool ev_made = false;
+};
+
+template <typename T>
+static cudaError_t dalloc(fnec_batch *b, T **p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t e = cudaMalloc((void **)p, sizeof(T) * count);
+    if (e == cudaSuccess) {
+        b->allocs.push_back(*p);
+        b->dev_bytes += sizeof(T) * count;
+    }
+    return e;
+}
+
+template <typename T>
+static cudaError_t up(fnec_batch *b, T *d, const std::vector<T> &h) {
+    if (h.empty()) return cudaSuccess;
+    b->h2d += sizeof(T) * h.size();
+    return cudaMemcpyAsync(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, b->ctx->stream);
+}
+
+static void free_batch(fnec_batch *b) {
+    for (void *p : b->allocs) cudaFree(p);
+    b->allocs.clear();
+    if (b->h_in) cudaFreeHost(b->h_in);
+    if (b->h_out) cudaFreeHost(b->h_out);
+    b->h_in = b->h_out = nullptr;
+    if (b->ev_made)
+        for (auto &e : b->ev) cudaEventDestroy(e);
+    b->ev_made = false;
+    free_mixed(b->mixed);
+}
+
+// Carve the packed input arena: every host table gets a 256-byte aligned
+// slot; the device pointer of the table is the same offset in d_in.
+struct Packer {
+    std::vector<std::pair<const void *, size_t>> parts;
+    std::vector<size_t> offs;
+    size_t total = 0;
+    template <typename T>
+    size_t add(const std::vector<T> &v) {
+        size_t off = total;
+        parts.push_back({v.data(), sizeof(T) * v.size()});
+        offs.push_back(off);
+        total += (sizeof(T) * v.size() + 255) / 256 * 256;
+        return off;
+    }
+};
+
+// Pack host antennas into flat tables and allocate the device side.
+static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, fnec_batch **out,
+                       bool need_solve = true) {
+    fnec_batch *b = new fnec_batch();
+    b->ctx = ctx;
+    b->precision = precision;
+    b->from_wires = !hs.empty() && !hs[0].wires.empty();
+    int64_t ff_req_max = 0, ff_int_max = 0;
+    size_t smem_max = 0;
+    for (size_t ai = 0; ai < hs.size(); ++ai) {
+        HostAnt &h = hs[ai];
+        AntDesc a{};
+        a.seg_off = b->tot_seg;
+        a.n = (int32_t)h.segs.size();
+        a.w = (int32_t)h.ep.size();
+        a.ground = h.ground;
+        int n = a.n;
+        // wires
+        for (auto w : h.wires) {
+            w.seg_off += b->tot_seg;
+            b->wires.push_back(w);
+        }
+        if (!b->from_wires) b->segs.insert(b->segs.end(), h.segs.begin(), h.segs.end());
+        // row_wire (linear.rs:728-733) and the CSR of rows per wire column
+        std::vector<int32_t> row_wire(n, 0);
+        for (size_t q = 0; q < h.ep.size(); ++q)
+            for (int64_t r = h.ep[q].first; r <= h.ep[q].second; ++r) row_wire[r] = (int32_t)q;
+        a.rowwire_off = (int64_t)b->ibuf.size();
+        b->ibuf.insert(b->ibuf.end(), row_wire.begin(), row_wire.end());
+        std::vector<std::vector<int32_t>> rows_of(h.ep.size());
+        for (int r = 0; r < n; ++r) rows_of[row_wire[r]].push_back(r);
+        a.wptr_off = (int64_t)b->ibuf.size();
+        int32_t acc = 0;
+        b->ibuf.push_back(0);
+        for (auto &v : rows_of) {
+            acc += (int32_t)v.size();
+            b->ibuf.push_back(acc);
+        }
+        a.wrow_off = (int64_t)b->ibuf.size();
+        for (auto &v : rows_of) b->ibuf.insert(b->ibuf.end(), v.begin(), v.end());
+        a.comp_off = (int64_t)b->ibuf.size();
+        if (h.comp.empty()) h.comp.assign(2 * n, 0);
+        b->ibuf.insert(b->ibuf.end(), h.comp.begin(), h.comp.end());
+        // constraint rows (linear.rs:744-762): free endpoints first (first,
+        // then last, per wire; skipping junction endpoints), then junctions.
+        std::vector<char> injunc(n, 0);
+        for (size_t t = 0; t < h.ja.size(); ++t) {
+            injunc[h.ja[t]] = 1;
+            injunc[h.jb[t]] = 1;
+        }
+        struct Ent {
+            int64_t col;
+            double val;
+        };
+        std::vector<std::vector<Ent>> crow;
+        for (auto &e : h.ep) {
+            if (!injunc[e.first]) crow.push_back({{e.first, 1.0}});
+            if (!injunc[e.second]) crow.push_back({{e.second, 1.0}});
+        }
+        for (size_t t = 0; t < h.ja.size(); ++t) {
+            if (h.ja[t] == h.jb[t]) crow.push_back({{h.jb[t], h.js[t]}});
+            else crow.push_back({{h.ja[t], 1.0}, {h.jb[t], h.js[t]}});
+        }
+        struct Contrib {
+            int64_t i, j, row;
+            int32_t code;
+        };
+        std::vector<Contrib> cl;
+        for (size_t r = 0; r < crow.size(); ++r)
+            for (auto &u : crow[r])
+                for (auto &v : crow[r]) cl.push_back({u.col, v.col, (int64_t)r, con_code(u.val, v.val)});
+        std::stable_sort(cl.begin(), cl.end(), [](const Contrib &x, const Contrib &y) {
+            return x.i != y.i ? x.i < y.i : (x.j != y.j ? x.j < y.j : x.row < y.row);
+        });
+        a.con_off = (int64_t)b->cons.size();
+        a.conv_off = (int64_t)b->codes.size();
+        int32_t base = 0;
+        for (size_t q = 0; q < cl.size();) {
+            size_t e = q;
+            while (e < cl.size() && cl[e].i == cl[q].i && cl[e].j == cl[q].j) ++e;
+            DevConstraint c{(int32_t)cl[q].i, (int32_t)cl[q].j, base, (int32_t)(e - q)};
+            for (size_t t = q; t < e; ++t) b->codes.push_back(cl[t].code);
+            base += (int32_t)(e - q);
+            b->cons.push_back(c);
+            q = e;
+        }
+        a.n_con = (int32_t)(b->cons.size() - a.con_off);
+        // sources, feeds, runs, rp
+        a.src_off = (int64_t)b->srcs.size();
+        a.n_src = (int32_t)h.srcs.size();
+        b->srcs.insert(b->srcs.end(), h.srcs.begin(), h.srcs.end());
+        a.feed_off = (int64_t)b->feeds.size();
+        a.n_feed = (int32_t)h.feeds.size();
+        b->feeds.insert(b->feeds.end(), h.feeds.begin(), h.feeds.end());
+        a.run_off = (int64_t)b->runs.size();
+        a.n_run = (int32_t)h.runs.size();
+        b->runs.insert(b->runs.end(), h.runs.begin(), h.runs.end());
+        DevRp rp = h.rp;
+        if (!h.pts.empty()) {
+            rp.pts_off = (int64_t)b->pts.size() / 2;
+            rp.n_pts = (int32_t)(h.pts.size() / 2);
+            b->pts.insert(b->pts.end(), h.pts.begin(), h.pts.end());
+        }
+        b->rps.push_back(rp);
+        int64_t n_req = rp.pts_off >= 0 ? rp.n_pts : (int64_t)rp.n_theta * rp.n_phi;
+        int64_t n_int = rp.skip_integral ? 0 : (h.ground == 1 ? 91 : 181) * 360;
+        ff_req_max = std::max(ff_req_max, n_req);
+        ff_int_max = std::max(ff_int_max, n_int);
+        smem_max = std::max(smem_max, sizeof(DevRun) * h.runs.size() + sizeof(cx) * (size_t)n);
+        b->ants.push_back(a);
+        // units
+        int s = n + a.w;
+        for (size_t fi = 0; fi < h.freqs.size(); ++fi) {
+            double f = h.freqs[fi];
+            UnitDesc u{};
+            u.ant = (int32_t)ai;
+            u.n = n;
+            u.s = s;
+            u.freq = f;
+            u.k_fill = 2.0 * PI * f / C0;
+            u.k_rp = 2.0 * PI / (C0 / f);
+            u.z_off = b->z_el;
+            u.a_off = b->a_el;
+            u.x_off = b->x_el;
+            u.rhs_off = b->rhs_el;
+            u.pat_off = b->pat_el;
+            if (need_solve) {
+                b->z_el += (int64_t)n * n;
+                b->a_el += (int64_t)s * (s + 1);
+            }
+            b->x_el += s;
+            b->rhs_el += n;
+            b->pat_el += n_req;
+            fnec_unit_info ui{};
+            ui.antenna = (uint32_t)ai;
+            ui.n = (uint32_t)n;
+            ui.s = (uint32_t)s;
+            ui.n_feed = (uint32_t)a.n_feed;
+            ui.n_points = (uint32_t)n_req;
+            ui.freq_hz = f;
+            ui.pat_off = (uint64_t)u.pat_off;
+            ui.feed_off = (uint64_t)b->feed_rows;
+            ui.cur_off = b->uinfo.empty() ? 0 : b->uinfo.back().cur_off + b->uinfo.back().n;
+            b->feed_row_off.push_back(b->feed_rows);
+            b->feed_rows += a.n_feed;
+            b->uinfo.push_back(ui);
+            b->units.push_back(u);
+            b->max_s = std::max(b->max_s, s);
+            b->max_n = std::max(b->max_n, n);
+            int32_t uidx = (int32_t)(b->units.size() - 1);
+            if (need_solve) {
+                for (int i0 = 0; i0 < n; i0 += 16)
+                    for (int j0 = 0; j0 < n; j0 += 16) b->fill_tiles.push_back(make_int4(uidx, i0, j0, 0));
+                for (int i0 = 0; i0 < n; i0 += 64)
+                    for (int j0 = 0; j0 <= n; j0 += 64) b->gram_tiles.push_back(make_int4(uidx, i0, j0, 0));
+            }
+            if (!h.z.empty()) b->z_given.insert(b->z_given.end(), h.z.begin(), h.z.end());
+            if (h.rhs_given) {
+                b->rhs_given_flag = true;
+                b->rhs_given.insert(b->rhs_given.end(), h.rhs.begin(), h.rhs.end());
+                b->cos_given.insert(b->cos_given.end(), h.cosv.begin(), h.cosv.end());
+            }
+        }
+        b->tot_seg += n;
+    }
+    b->ff_blocks = farfield_max_blocks((int)ff_int_max, (int)ff_req_max);
+    b->ff_smem = smem_max;
+    int nu = (int)b->units.size();
+    cudaError_t e = cudaSuccess;
+    Packer pk;
+    size_t o_wires = pk.add(b->wires), o_segs = pk.add(b->segs), o_ants = pk.add(b->ants),
+           o_units = pk.add(b->units), o_ibuf = pk.add(b->ibuf), o_srcs = pk.add(b->srcs),
+           o_feeds = pk.add(b->feeds), o_cons = pk.add(b->cons), o_codes = pk.add(b->codes),
+           o_runs = pk.add(b->runs), o_rps = pk.add(b->rps), o_pts = pk.add(b->pts),
+           o_ft = pk.add(b->fill_tiles), o_gt = pk.add(b->gram_tiles), o_fro = pk.add(b->feed_row_off),
+           o_rhs = pk.add(b->rhs_given), o_cos = pk.add(b->cos_given), o_z = pk.add(b->z_given);
+    b->in_bytes = pk.total > 0 ? pk.total : 256;
+    e = cudaMallocHost((void **)&b->h_in, b->in_bytes);
+    if (e == cudaSuccess) e = dalloc(b, &b->d_in, b->in_bytes);
+    if (e == cudaSuccess) {
+        for (size_t q = 0; q < pk.parts.size(); ++q)
+            if (pk.parts[q].second) std::memcpy(b->h_in + pk.offs[q], pk.parts[q].first, pk.parts[q].second);
+        b->d_wires = (DevWire *)(b->d_in + o_wires);
+        b->d_ants = (AntDesc *)(b->d_in + o_ants);
+        b->d_units = (UnitDesc *)(b->d_in + o_units);
+        b->d_ibuf = (int32_t *)(b->d_in + o_ibuf);
+        b->d_srcs = (DevSource *)(b->d_in + o_srcs);
+        b->d_feeds = (DevFeed *)(b->d_in + o_feeds);
+        b->d_cons = (DevConstraint *)(b->d_in + o_cons);
+        b->d_codes = (int32_t *)(b->d_in + o_codes);
+        b->d_runs = (DevRun *)(b->d_in + o_runs);
+        b->d_rps = (DevRp *)(b->d_in + o_rps);
+        b->d_pts = (double *)(b->d_in + o_pts);
+        b->d_fill_tiles = (int4 *)(b->d_in + o_ft);
+        b->d_gram_tiles = (int4 *)(b->d_in + o_gt);
+        b->d_feed_row_off = (int64_t *)(b->d_in + o_fro);
+        b->d_rhs_given = (double *)(b->d_in + o_rhs);
+        b->d_cos_given = (double *)(b->d_in + o_cos);
+        b->d_z_given = (double *)(b->d_in + o_z);
+    }
+    // segments: uploaded with the arena for caller-provided geometry,
+    // expanded on the device from the wires otherwise
+    if (!b->from_wires) b->d_segs = (DevSeg *)(b->d_in + o_segs);
+#define DA(p, n)                                             \
+    if (e == cudaSuccess) e = dalloc(b, &b->p, (size_t)(n));
+    if (b->from_wires) DA(d_segs, b->tot_seg);
+    DA(d_z, b->z_el);
+    DA(d_a, b->a_el);
+    DA(d_x, b->x_el);
+    DA(d_rhs, b->rhs_el);
+    DA(d_cos, b->rhs_el);
+    DA(d_piv, b->x_el);
+    DA(d_status, nu);
+    DA(d_feed_out, 7 * b->feed_rows);
+    DA(d_fld, 4 * b->pat_el);
+    DA(d_partials, (int64_t)b->ff_blocks * nu);
+    DA(d_pat, PAT_STRIDE * b->pat_el);
+    DA(d_total, nu);
+#undef DA
+    b->out_bytes = sizeof(cx) * (size_t)b->x_el + sizeof(double) * 7 * (size_t)b->feed_rows +
+                   sizeof(double) * PAT_STRIDE * (size_t)b->pat_el + (sizeof(int32_t) + sizeof(double)) * (size_t)nu +
+                   64;
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_out, b->out_bytes);
+    if (e == cudaSuccess && precision == FNEC_PRECISION_MIXED) {
+        e = alloc_mixed(b->mixed, b->units, b->max_s);
+        b->dev_bytes += b->mixed.bytes;
+    }
+    if (e != cudaSuccess) {
+        free_batch(b);
+        delete b;
+        return fail(ctx, e == cudaErrorMemoryAllocation ? FNEC_ERR_OUT_OF_MEMORY : FNEC_ERR_CUDA,
+                    std::string("batch allocation: ") + cudaGetErrorString(e));
+    }
+    *out = b;
+    int st = fnec_batch_upload(b);
+    if (st != FNEC_OK) {
+        free_batch(b);
+        delete b;
+        *out = nullptr;
+        return st;
+    }
+    return FNEC_OK;
+}
+
+// HostAnt from GW/EX/RP cards: the CLI standard Hallen branch topology
+// (solve_session.rs:1379-1400).
+static int antenna_from_cards(const fnec_antenna &A, HostAnt &h, std::string &why) {
+    if (A.n_wires == 0 || !A.wires) {
+        why = "deck contains no GW (wire) cards";
+        return FNEC_ERR_BAD_ARG;
+    }
+    if (A.ground != FNEC_GROUND_FREE && A.ground != FNEC_GROUND_PEC) {
+        why = "ground must be free space or PEC";
+        return FNEC_ERR_BAD_ARG;
+    }
+    if (A.n_freqs == 0 || !A.freqs_hz) {
+        why = "no frequencies";
+        return FNEC_ERR_BAD_ARG;
+    }
+    h.ground = A.ground;
+    int64_t off = 0;
+    for (uint32_t w = 0; w < A.n_wires; ++w) {
+        const fnec_wire &gw = A.wires[w];
+        if (gw.segments == 0) {
+            why = "GW tag " + std::to_string(gw.tag) + ": segment count must be >= 1";
+            return FNEC_ERR_BAD_ARG;
+        }
+        double dx = gw.end[0] - gw.start[0], dy = gw.end[1] - gw.start[1], dz = gw.end[2] - gw.start[2];
+        if (std::sqrt(dx * dx + dy * dy + dz * dz) == 0.0) {
+            why = "GW tag " + std::to_string(gw.tag) + ": wire has zero length";
+            return FNEC_ERR_BAD_ARG;
+        }
+        DevWire d{};
+        for (int c = 0; c < 3; ++c) {
+            d.start[c] = gw.start[c];
+            d.end[c] = gw.end[c];
+        }
+        d.radius = gw.radius;
+        d.tag = gw.tag;
+        d.nseg = gw.segments;
+        d.seg_off = off;
+        h.wires.push_back(d);
+        for (uint32_t i = 0; i < gw.segments; ++i) h.segs.push_back(host_seg(gw, i));
+        off += gw.segments;
+    }
+    auto merged = merge_collinear(h.segs);
+    h.ep = merged;
+    set_comp(h, merged);
+    cli_junctions(h.segs, merged, h);
+    int st = resolve_sources(h, A.sources, A.n_sources, why);
+    if (st != FNEC_OK) return st;
+    build_runs(h);
+    h.rp.pts_off = -1;
+    if (A.rp) {
+        h.rp.n_theta = (int32_t)std::max<uint32_t>(A.rp->n_theta, 1);
+        h.rp.n_phi = (int32_t)std::max<uint32_t>(A.rp->n_phi, 1);
+        h.rp.theta0 = A.rp->theta0;
+        h.rp.phi0 = A.rp->phi0;
+        h.rp.d_theta = A.rp->d_theta;
+        h.rp.d_phi = A.rp->d_phi;
+    } else {
+        h.rp.n_theta = 0;
+        h.rp.n_phi = 0;
+        h.rp.skip_integral = 1;
+    }
+    h.freqs.assign(A.freqs_hz, A.freqs_hz + A.n_freqs);
+    return FNEC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int fnec_ctx_create(int device, fnec_ctx **out) {
+    if (!out) return FNEC_ERR_BAD_ARG;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) return FNEC_ERR_NO_DEVICE;
+    if (device < 0 || device >= count) return FNEC_ERR_BAD_ARG;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return FNEC_ERR_NO_DEVICE;
+    if (prop.major != 10) return FNEC_ERR_NO_DEVICE;  // built for sm_100a only
+    if (cudaSetDevice(device) != cudaSuccess) return FNEC_ERR_CUDA;
+    fnec_ctx *c = new fnec_ctx();
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return FNEC_ERR_CUDA;
+    }
+    *out = c;
+    return FNEC_OK;
+}
+
+int fnec_ctx_destroy(fnec_ctx *ctx) {
+    if (!ctx) return FNEC_ERR_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return FNEC_OK;
+}
+
+const char *fnec_ctx_last_error(const fnec_ctx *ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+void *fnec_ctx_stream(fnec_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+int fnec_batch_create(fnec_ctx *ctx, const fnec_antenna *antennas, uint32_t n_antennas,
+                      int32_t precision, fnec_batch **out) {
+    if (!ctx || !out || (!antennas && n_antennas)) return FNEC_ERR_BAD_ARG;
+    *out = nullptr;
+    if (precision != FNEC_PRECISION_FP64 && precision != FNEC_PRECISION_MIXED)
+        return fail(ctx, FNEC_ERR_BAD_ARG, "unknown precision");
+    if (precision == FNEC_PRECISION_MIXED && !mixed_available())
+        return fail(ctx, FNEC_ERR_UNSUPPORTED, "mixed precision path not built");
+    cudaSetDevice(ctx->device);
+    std::vector<HostAnt> hs(n_antennas);
+    for (uint32_t a = 0; a < n_antennas; ++a) {
+        std::string why;
+        int st = antenna_from_cards(antennas[a], hs[a], why);
+        if (st != FNEC_OK) return fail(ctx, st, "antenna " + std::to_string(a) + ": " + why);
+    }
+    return build_batch(ctx, hs, precision, out);
+}
+
+int fnec_batch_destroy(fnec_batch *b) {
+    if (!b) return FNEC_ERR_BAD_ARG;
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    free_batch(b);
+    delete b;
+    return FNEC_OK;
+}
+
+int fnec_batch_get_info(const fnec_batch *b, fnec_batch_info *out) {
+    if (!b || !out) return FNEC_ERR_BAD_ARG;
+    out->n_units = (uint32_t)b->units.size();
+    out->max_s = (uint32_t)b->max_s;
+    out->total_currents = b->uinfo.empty() ? 0 : b->uinfo.back().cur_off + b->uinfo.back().n;
+    out->total_feeds = (uint64_t)b->feed_rows;
+    out->total_points = (uint64_t)b->pat_el;
+    out->device_bytes = b->dev_bytes;
+    out->h2d_bytes = b->h2d;
+    out->kernel_launches = b->launches;
+    return FNEC_OK;
+}
+
+int fnec_batch_get_unit_info(const fnec_batch *b, uint32_t unit, fnec_unit_info *out) {
+    if (!b || !out || unit >= b->uinfo.size()) return FNEC_ERR_BAD_ARG;
+    *out = b->uinfo[unit];
+    return FNEC_OK;
+}
+
+int fnec_batch_upload(fnec_batch *b) {
+    if (!b) return FNEC_ERR_BAD_ARG;
+    fnec_ctx *ctx = b->ctx;
+    cudaSetDevice(ctx->device);
+    // one pinned host -> device copy of every input table
+    b->h2d = b->in_bytes;
+    CUDA_TRY(ctx, cudaMemcpyAsync(b->d_in, b->h_in, b->in_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    if (!b->z_given.empty())
+        CUDA_TRY(ctx, cudaMemcpyAsync(b->d_z, b->d_z_given, sizeof(double) * b->z_given.size(),
+                                      cudaMemcpyDeviceToDevice, ctx->stream));
+    if (b->rhs_given_flag) {
+        CUDA_TRY(ctx, cudaMemcpyAsync(b->d_rhs, b->d_rhs_given, sizeof(double) * b->rhs_given.size(),
+                                      cudaMemcpyDeviceToDevice, ctx->stream));
+        CUDA_TRY(ctx, cudaMemcpyAsync(b->d_cos, b->d_cos_given, sizeof(double) * b->cos_given.size(),
+                                      cudaMemcpyDeviceToDevice, ctx->stream));
+    }
+    return FNEC_OK;
+}
+
+int fnec_batch_run(fnec_batch *b) {
+    if (!b) return FNEC_ERR_BAD_ARG;
+    fnec_ctx *ctx = b->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    int nu = (int)b->units.size();
+    uint64_t L = 0;
+    if (nu == 0) return FNEC_OK;
+    auto mark = [&](int k) {
+        if (b->profile) cudaEventRecord(b->ev[k], st);
+    };
+    CUDA_TRY(ctx, cudaMemsetAsync(b->d_status, 0, sizeof(int32_t) * nu, st));
+    CUDA_TRY(ctx, cudaMemsetAsync(b->d_total, 0, sizeof(double) * nu, st));
+    mark(0);
+    if (b->from_wires) {
+        launch_expand_segments(b->d_wires, (int)b->wires.size(), b->d_segs, st);
+        ++L;
+    }
+    mark(1);
+    if (!b->rhs_given_flag) {
+        const double MU0 = 4.0 * PI * 1e-7;
+        const double ETA0 = MU0 * C0;
+        launch_hallen_rhs(b->d_units, nu, b->d_ants, b->d_segs, b->d_ibuf, b->d_srcs, b->d_rhs, b->d_cos,
+                          2.0 * PI / ETA0, st);
+        ++L;
+    }
+    mark(2);
+    if (b->precision == FNEC_PRECISION_MIXED) {
+        MixedMarks mm{b->profile ? &b->ev[3] : nullptr};
+        L += run_mixed(b->mixed, b->d_units, nu, b->units, b->d_ants, b->d_segs, b->d_fill_tiles,
+                       (int)b->fill_tiles.size(), b->d_gram_tiles, (int)b->gram_tiles.size(), b->d_ibuf,
+                       b->d_cons, b->d_codes, b->d_z, b->d_rhs, b->d_cos, b->d_a, b->d_x, b->d_piv,
+                       b->d_status, b->max_s, b->z_given.empty(), mm, st);
+    } else {
+        if (b->z_given.empty()) {
+            launch_fill_exact(b->d_units, b->d_ants, b->d_segs, b->d_fill_tiles, (int)b->fill_tiles.size(),
+                              b->d_z, st);
+            ++L;
+        }
+        mark(3);
+        launch_gram_exact(b->d_units, nu, b->d_ants, b->d_gram_tiles, (int)b->gram_tiles.size(), b->d_ibuf,
+                          b->d_cons, b->d_codes, b->d_z, b->d_rhs, b->d_cos, b->d_a, st);
+        mark(4);
+        launch_factor_exact(b->d_units, nu, b->max_s, 0, b->d_a, b->d_piv, b->d_status, st);
+        mark(5);
+        launch_backsub(b->d_units, nu, b->max_s, b->d_a, b->d_x, b->d_status, st);
+        mark(6);
+        int panels = (b->max_s + 31) / 32;
+        L += 3 + 1 + 3 * panels;
+    }
+    launch_feedpoints(b->d_units, nu, b->d_ants, b->d_segs, b->d_feeds, b->d_x, b->d_status, b->d_feed_out,
+                      b->d_feed_row_off, st);
+    ++L;
+    mark(7);
+    if (b->ff_blocks > 0) {
+        launch_farfield(b->d_units, nu, b->d_ants, b->d_runs, b->d_rps, b->d_pts, b->d_x, b->d_status, b->d_fld,
+                        b->d_partials, b->ff_blocks, b->ff_smem, b->d_pat, b->d_total, st);
+        L += 2;
+    }
+    mark(8);
+    b->launches = L;
+    CUDA_TRY(ctx, cudaGetLastError());
+    return FNEC_OK;
+}
+
+int fnec_batch_set_profiling(fnec_batch *b, int on) {
+    if (!b) return FNEC_ERR_BAD_ARG;
+    cudaSetDevice(b->ctx->device);
+    if (on && !b->ev_made) {
+        for (auto &e : b->ev) CUDA_TRY(b->ctx, cudaEventCreate(&e));
+        b->ev_made = true;
+    }
+    b->profile = on != 0;
+    return FNEC_OK;
+}
+
+int fnec_batch_phase_ms(fnec_batch *b, double *ms) {
+    if (!b || !ms) return FNEC_ERR_BAD_ARG;
+    if (!b->ev_made) return fail(b->ctx, FNEC_ERR_BAD_ARG, "profiling was never enabled");
+    cudaSetDevice(b->ctx->device);
+    CUDA_TRY(b->ctx, cudaEventSynchronize(b->ev[FNEC_N_PHASES]));
+    for (int k = 0; k < FNEC_N_PHASES; ++k) {
+        float f = 0.f;
+        CUDA_TRY(b->ctx, cudaEventElapsedTime(&f, b->ev[k], b->ev[k + 1]));
+        ms[k] = (double)f;
+    }
+    return FNEC_OK;
+}
+
+int fnec_batch_sync(fnec_batch *b) {
+    if (!b) return FNEC_ERR_BAD_ARG;
+    cudaSetDevice(b->ctx->device);
+    CUDA_TRY(b->ctx, cudaStreamSynchronize(b->ctx->stream));
+    return FNEC_OK;
+}
+
+int fnec_batch_read(fnec_batch *b, double *currents, double *feeds, double *pattern, int32_t *status,
+                    double *total_radiated) {
+    if (!b) return FNEC_ERR_BAD_ARG;
+    fnec_ctx *ctx = b->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = ctx->stream;
+    int nu = (int)b->units.size();
+    // device -> pinned staging -> caller arrays
+    unsigned char *hx = b->h_out;
+    unsigned char *hf = hx + sizeof(cx) * (size_t)b->x_el;
+    unsigned char *hp = hf + sizeof(double) * 7 * (size_t)b->feed_rows;
+    unsigned char *hs = hp + sizeof(double) * PAT_STRIDE * (size_t)b->pat_el;
+    unsigned char *ht = hs + sizeof(int32_t) * (size_t)nu;
+    size_t fb = sizeof(double) * 7 * (size_t)b->feed_rows, pb = sizeof(double) * PAT_STRIDE * (size_t)b->pat_el;
+    if (currents) CUDA_TRY(ctx, cudaMemcpyAsync(hx, b->d_x, sizeof(cx) * b->x_el, cudaMemcpyDeviceToHost, st));
+    if (feeds && fb) CUDA_TRY(ctx, cudaMemcpyAsync(hf, b->d_feed_out, fb, cudaMemcpyDeviceToHost, st));
+    if (pattern && pb) CUDA_TRY(ctx, cudaMemcpyAsync(hp, b->d_pat, pb, cudaMemcpyDeviceToHost, st));
+    if (status) CUDA_TRY(ctx, cudaMemcpyAsync(hs, b->d_status, sizeof(int32_t) * nu, cudaMemcpyDeviceToHost, st));
+    if (total_radiated)
+        CUDA_TRY(ctx, cudaMemcpyAsync(ht, b->d_total, sizeof(double) * nu, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    if (currents) {
+        const cx *x = (const cx *)hx;
+        for (int u = 0; u < nu; ++u)
+            std::memcpy(currents + 2 * b->uinfo[u].cur_off, &x[b->units[u].x_off], sizeof(cx) * b->units[u].n);
+    }
+    if (feeds && fb) std::memcpy(feeds, hf, fb);
+    if (pattern && pb) std::memcpy(pattern, hp, pb);
+    if (status) std::memcpy(status, hs, sizeof(int32_t) * nu);
+    if (total_radiated) std::memcpy(total_radiated, ht, sizeof(double) * nu);
+    return FNEC_OK;
+}
+
+int fnec_batch_read_unit(fnec_batch *b, uint32_t unit, double *x, int32_t *pivots) {
+    if (!b || unit >= b->units.size()) return FNEC_ERR_BAD_ARG;
+    fnec_ctx *ctx = b->ctx;
+    cudaSetDevice(ctx->device);
+    const UnitDesc &u = b->units[unit];
+    if (x)
+        CUDA_TRY(ctx, cudaMemcpyAsync(x, b->d_x + u.x_off, sizeof(cx) * u.s, cudaMemcpyDeviceToHost,
+                                      ctx->stream));
+    if (pivots)
+        CUDA_TRY(ctx, cudaMemcpyAsync(pivots, b->d_piv + u.x_off, sizeof(int32_t) * u.s,
+                                      cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return FNEC_OK;
+}
+
+int fnec_batch_read_z(fnec_batch *b, uint32_t unit, double *z) {
+    if (!b || !z || unit >= b->units.size()) return FNEC_ERR_BAD_ARG;
+    fnec_ctx *ctx = b->ctx;
+    cudaSetDevice(ctx->device);
+    const UnitDesc &u = b->units[unit];
+    CUDA_TRY(ctx, cudaMemcpyAsync(z, b->d_z + u.z_off, sizeof(cx) * (size_t)u.n * u.n,
+                                  cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return FNEC_OK;
+}
+
+// ---- reference nec_accel entry points ---------------------------------------
+
+int fnec_fill_zmatrix(fnec_ctx *ctx, const fnec_zsegment *segments, uint64_t n, double freq_hz,
+                      int32_t ground, double *z_out) {
+    if (!ctx || (!segments && n) || (!z_out && n)) return FNEC_ERR_BAD_ARG;
+    if (ground != FNEC_GROUND_FREE && ground != FNEC_GROUND_PEC) return FNEC_ERR_BAD_ARG;
+    if (n == 0) return FNEC_OK;
+    cudaSetDevice(ctx->device);
+    std::vector<DevSeg> hs(n);
+    for (uint64_t i = 0; i < n; ++i) {
+        DevSeg s{};
+        for (int c = 0; c < 3; ++c) {
+            s.mid[c] = segments[i].midpoint[c];
+            s.dir[c] = segments[i].direction[c];
+        }
+        s.len = segments[i].length;
+        s.rad = segments[i].radius;
+        hs[i] = s;
+    }
+    DevSeg *d_s = nullptr;
+    cx *d_z = nullptr;
+    CUDA_TRY(ctx, cudaMalloc(&d_s, sizeof(DevSeg) * n));
+    cudaError_t e = cudaMalloc(&d_z, sizeof(cx) * n * n);
+    if (e != cudaSuccess) {
+        cudaFree(d_s);
+        return fail(ctx, FNEC_ERR_OUT_OF_MEMORY, "fill_zmatrix: Z allocation");
+    }
+    e = cudaMemcpyAsync(d_s, hs.data(), sizeof(DevSeg) * n, cudaMemcpyHostToDevice, ctx->stream);
+    double k = 2.0 * PI * freq_hz / C0;
+    if (e == cudaSuccess) {
+        launch_fill_exact_flat(d_s, (int)n, k, ground, d_z, ctx->stream);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(z_out, d_z, sizeof(cx) * n * n, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    cudaFree(d_s);
+    cudaFree(d_z);
+    if (e != cudaSuccess) return fail(ctx, FNEC_ERR_CUDA, cudaGetErrorString(e));
+    return FNEC_OK;
+}
+
+static int solve_common(fnec_ctx *ctx, const fnec_zsegment *segments, const double *zin, uint64_t n,
+                        const double *rhs, const double *cos_vec, const uint64_t *wire_endpoints, uint64_t w,
+                        const fnec_junction *junctions, uint64_t nj, double freq_hz, int32_t ground,
+                        int32_t precision, double *x_out, int32_t *pivots_out) {
+    if (!ctx || n == 0 || (!segments && !zin) || !rhs || !cos_vec || !x_out) return FNEC_ERR_BAD_ARG;
+    if (ground != FNEC_GROUND_FREE && ground != FNEC_GROUND_PEC) return FNEC_ERR_BAD_ARG;
+    if (w && !wire_endpoints) return FNEC_ERR_BAD_ARG;
+    if (precision == FNEC_PRECISION_MIXED && !mixed_available())
+        return fail(ctx, FNEC_ERR_UNSUPPORTED, "mixed precision path not built");
+    if (nj && !junctions) return FNEC_ERR_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    std::vector<HostAnt> hs(1);
+    HostAnt &h = hs[0];
+    h.ground = ground;
+    for (uint64_t i = 0; i < n; ++i) {
+        DevSeg s{};
+        if (segments) {
+            for (int c = 0; c < 3; ++c) {
+                s.mid[c] = segments[i].midpoint[c];
+                s.dir[c] = segments[i].direction[c];
+            }
+            s.len = segments[i].length;
+            s.rad = segments[i].radius;
+        }
+        h.segs.push_back(s);
+    }
+    if (zin) h.z.assign(zin, zin + 2 * n * n);
+    // linear.rs:689-696: an empty endpoint list means one wire (0, n-1)
+    if (w == 0) {
+        h.ep.push_back({0, (int64_t)n - 1});
+    } else {
+        for (uint64_t q = 0; q < w; ++q) {
+            uint64_t f = wire_endpoints[2 * q], l = wire_endpoints[2 * q + 1];
+            if (f > l || l >= n) return fail(ctx, FNEC_ERR_BAD_ARG, "wire endpoint out of range");
+            h.ep.push_back({(int64_t)f, (int64_t)l});
+        }
+    }
+    for (uint64_t t = 0; t < nj; ++t) {
+        if (junctions[t].seg_a >= n || junctions[t].seg_b >= n)
+            return fail(ctx, FNEC_ERR_BAD_ARG, "junction segment out of range");
+        h.ja.push_back((int64_t)junctions[t].seg_a);
+        h.jb.push_back((int64_t)junctions[t].seg_b);
+        h.js.push_back(junctions[t].sign);
+    }
+    h.rhs_given = true;
+    h.rhs.assign(rhs, rhs + 2 * n);
+    h.cosv.assign(cos_vec, cos_vec + n);
+    h.comp.assign(2 * n, 0);
+    h.rp.pts_off = -1;
+    h.rp.skip_integral = 1;
+    h.freqs.push_back(freq_hz);
+    fnec_batch *b = nullptr;
+    int st = build_batch(ctx, hs, precision, &b);
+    if (st != FNEC_OK) return st;
+    st = fnec_batch_run(b);
+    if (st == FNEC_OK) st = fnec_batch_sync(b);
+    int32_t ust = 0;
+    if (st == FNEC_OK) st = fnec_batch_read(b, nullptr, nullptr, nullptr, &ust, nullptr);
+    if (st == FNEC_OK) st = fnec_batch_read_unit(b, 0, x_out, pivots_out);
+    fnec_batch_destroy(b);
+    if (st != FNEC_OK) return st;
+    if (ust != 0) return fail(ctx, FNEC_ERR_SINGULAR, "singular pivot at column " + std::to_string(-ust - 1));
+    return FNEC_OK;
+}
+
+int fnec_solve_hallen_resident(fnec_ctx *ctx, const fnec_zsegment *segments, uint64_t n,
+                               const double *rhs, const double *cos_vec, const uint64_t *wire_endpoints,
+                               uint64_t w, const fnec_junction *junctions, uint64_t nj, double freq_hz,
+                               int32_t ground, int32_t precision, double *x_out, int32_t *pivots_out) {
+    if (!segments) return FNEC_ERR_BAD_ARG;
+    return solve_common(ctx, segments, nullptr, n, rhs, cos_vec, wire_endpoints, w, junctions, nj, freq_hz,
+                        ground, precision, x_out, pivots_out);
+}
+
+int fnec_solve_hallen(fnec_ctx *ctx, const double *z, uint64_t n, const double *rhs, const double *cos_vec,
+                      const uint64_t *wire_endpoints, uint64_t w, const fnec_junction *junctions, uint64_t nj,
+                      int32_t precision, double *x_out, int32_t *pivots_out) {
+    if (!z) return FNEC_ERR_BAD_ARG;
+    return solve_common(ctx, nullptr, z, n, rhs, cos_vec, wire_endpoints, w, junctions, nj, 1.0,
+                        FNEC_GROUND_FREE, precision, x_out, pivots_out);
+}
+
+static int pattern_common(fnec_ctx *ctx, const fnec_gpu_segment *segments, uint64_t n,
+                          const double *currents, double k_rp, int32_t ground, const double *points,
+                          uint64_t p, bool skip_integral, double total_given, std::vector<double> &pat,
+                          double &total) {
+    if (!ctx || n == 0 || !segments || !currents) return FNEC_ERR_BAD_ARG;
+    if (p && !points) return FNEC_ERR_BAD_ARG;
+    cudaSetDevice(ctx->device);
+    std::vector<HostAnt> hs(1);
+    HostAnt &h = hs[0];
+    h.ground = ground;
+    for (uint64_t i = 0; i < n; ++i) {
+        DevSeg s{};
+        for (int c = 0; c < 3; ++c) {
+            s.mid[c] = segments[i].midpoint[c];
+            s.dir[c] = segments[i].direction[c];
+        }
+        s.len = segments[i].length;
+        s.tag = 1;
+        h.segs.push_back(s);
+    }
+    h.ep.push_back({0, (int64_t)n - 1});
+    h.comp.assign(2 * n, 0);
+    build_runs(h);
+    h.rp.pts_off = -1;
+    if (p) h.pts.assign(points, points + 2 * p);
+    h.rp.skip_integral = skip_integral ? 1 : 0;
+    h.rp.total_given = total_given;
+    h.freqs.push_back(1.0);  // placeholder; k is set below
+    fnec_batch *b = nullptr;
+    int st = build_batch(ctx, hs, FNEC_PRECISION_FP64, &b, false);
+    if (st != FNEC_OK) return st;
+    b->units[0].k_rp = k_rp;
+    cudaStream_t s = ctx->stream;
+    cudaStreamSynchronize(s);
+    cudaError_t e = cudaMemcpyAsync(b->d_units, b->units.data(), sizeof(UnitDesc), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_status, 0, sizeof(int32_t), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_total, 0, sizeof(double), s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_x, currents, sizeof(cx) * n, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        launch_farfield(b->d_units, 1, b->d_ants, b->d_runs, b->d_rps, b->d_pts, b->d_x, b->d_status, b->d_fld,
+                        b->d_partials, b->ff_blocks, b->ff_smem, b->d_pat, b->d_total, s);
+        e = cudaGetLastError();
+    }
+    pat.assign(PAT_STRIDE * (p ? p : 1), 0.0);
+    if (e == cudaSuccess && p)
+        e = cudaMemcpyAsync(pat.data(), b->d_pat, sizeof(double) * PAT_STRIDE * p, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&total, b->d_total, sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    fnec_batch_destroy(b);
+    if (e != cudaSuccess) return fail(ctx, FNEC_ERR_CUDA, cudaGetErrorString(e));
+    return FNEC_OK;
+}
+
+int fnec_rp_farfield_batch(fnec_ctx *ctx, const fnec_gpu_segment *segments, uint64_t n,
+                           const double *currents, double k, double total_radiated, const double *points,
+                           uint64_t p, fnec_rp_result *out) {
+    if (p == 0) return FNEC_OK;
+    if (!out) return FNEC_ERR_BAD_ARG;
+    std::vector<double> pat;
+    double total = 0;
+    int st = pattern_common(ctx, segments, n, currents, k, FNEC_GROUND_FREE, points, p, true, total_radiated,
+                            pat, total);
+    if (st != FNEC_OK) return st;
+    for (uint64_t q = 0; q < p; ++q) {
+        const double *o = &pat[PAT_STRIDE * q];
+        out[q].gain_total_dbi = o[0];
+        out[q].gain_theta_dbi = o[1];
+        out[q].gain_phi_dbi = o[2];
+        out[q].axial_ratio = o[3];
+        out[q].u_theta = o[4];
+        out[q].u_phi = o[5];
+        out[q].theta_deg = points[2 * q];
+        out[q].phi_deg = points[2 * q + 1];
+    }
+    return FNEC_OK;
+}
+
+int fnec_radiation_pattern(fnec_ctx *ctx, const fnec_gpu_segment *segments, uint64_t n,
+                           const double *currents, double freq_hz, int32_t ground, const double *points,
+                           uint64_t p, double *out, double *total_out) {
+    if (p && !out) return FNEC_ERR_BAD_ARG;
+    std::vector<double> pat;
+    double total = 0;
+    int st = pattern_common(ctx, segments, n, currents, 2.0 * PI / (C0 / freq_hz), ground, points, p, false,
+                            0.0, pat, total);
+    if (st != FNEC_OK) return st;
+    for (uint64_t q = 0; q < p; ++q)
+        for (int c = 0; c < 4; ++c) out[4 * q + c] = pat[PAT_STRIDE * q + c];
+    if (total_out) *total_out = total;
+    return FNEC_OK;
+}
+
+int fnec_integrate_radiated_power(fnec_ctx *ctx, const fnec_gpu_segment *segments, uint64_t n,
+                                  const double *currents, double freq_hz, int32_t pec_ground, double *out) {
+    if (!out) return FNEC_ERR_BAD_ARG;
+    std::vector<double> pat;
+    double total = 0;
+    int st = pattern_common(ctx, segments, n, currents, 2.0 * PI / (C0 / freq_hz),
+                            pec_ground ? FNEC_GROUND_PEC : FNEC_GROUND_FREE, nullptr, 0, false, 0.0, pat, total);
+    if (st != FNEC_OK) return st;
+    *out = total;
+    return FNEC_OK;
+}
+
+int fnec_microbench_zmatrix_dispatch(int device, uint64_t n_segments, uint32_t n_dispatches,
+                                     uint64_t *device_init_us, uint64_t *dispatch_min_us,
+                                     uint64_t *dispatch_median_us) {
+    using clk = std::chrono::steady_clock;
+    if (n_segments == 0 || n_dispatches == 0) return FNEC_ERR_BAD_ARG;
+    auto t0 = clk::now();
+    fnec_ctx *ctx = nullptr;
+    int st = fnec_ctx_create(device, &ctx);
+    if (st != FNEC_OK) return st;
+    std::vector<fnec_zsegment> segs(n_segments);
+    double L = 10.0, dl = L / (double)n_segments;
+    for (uint64_t i = 0; i < n_segments; ++i) {
+        fnec_zsegment s{};
+        s.midpoint[2] = -L / 2 + dl * ((double)i + 0.5);
+        s.direction[2] = 1.0;
+        s.length = dl;
+        s.radius = 1e-3;
+        segs[i] = s;
+    }
+    std::vector<double> z(2 * n_segments * n_segments);
+    st = fnec_fill_zmatrix(ctx, segs.data(), n_segments, 14.2e6, FNEC_GROUND_FREE, z.data());
+    auto t1 = clk::now();
+    std::vector<uint64_t> us;
+    for (uint32_t d = 0; d < n_dispatches && st == FNEC_OK; ++d) {
+        auto a = clk::now();
+        st = fnec_fill_zmatrix(ctx, segs.data(), n_segments, 14.2e6, FNEC_GROUND_FREE, z.data());
+        us.push_back((uint64_t)std::chrono::duration_cast<std::chrono::microseconds>(clk::now() - a).count());
+    }
+    fnec_ctx_destroy(ctx);
+    if (st != FNEC_OK) return st;
+    std::sort(us.begin(), us.end());
+    if (device_init_us)
+        *device_init_us = (uint64_t)std::chrono::duration_cast<std::chrono::microseconds>(t1 - t0).count();
+    if (dispatch_min_us) *dispatch_min_us = us.front();
+    if (dispatch_median_us) *dispatch_median_us = us[us.size() / 2];
+    return FNEC_OK;
+}
+
+int fnec_enumerate_devices(int *count, int index, char *name, uint64_t cap) {
+    int c = 0;
+    if (cudaGetDeviceCount(&c) != cudaSuccess) c = 0;
+    if (count) *count = c;
+    if (name && cap > 0) {
+        name[0] = 0;
+        if (index >= 0 && index < c) {
+            cudaDeviceProp p;
+            if (cudaGetDeviceProperties(&p, index) == cudaSuccess) {
+                std::snprintf(name, (size_t)cap, "%s (sm_%d%d)", p.name, p.major, p.minor);
+            }
+        }
+    }
+    return FNEC_OK;
+}
+
+int fnec_dispatch_frequency_point(int request_kind, double freq_hz) {
+    (void)request_kind;
+    (void)freq_hz;
+    int c = 0;
+    if (cudaGetDeviceCount(&c) != cudaSuccess) return 0;
+    return c > 0 ? 1 : 0;
+}
+
+}  // extern "C"

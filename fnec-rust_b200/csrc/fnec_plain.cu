@@ -1,0 +1,702 @@
+// fnec_plain.cu -- plain FP64 Hallen kernels with bit-exact operation order.
+//
+// Every arithmetic operation below is one separately rounded IEEE
+// operation (explicit _rn intrinsics; the file is also built with
+// -fmad=false), issued in the order the reference issues it, and the
+// transcendental calls are correctly rounded (fnec_math.cuh).  Given the
+// same inputs the Gram matrix, the elimination and the back substitution
+// therefore reproduce the reference CPU path bit for bit; pivot order is
+// chosen with the reference's "last maximum by hypot" rule.
+//
+// Kernels (one launch each, all units of a batch at once):
+//   k_expand_segments  geometry.rs:710-754     one CTA per GW wire
+//   k_hallen_rhs       excitation.rs:119-244   one CTA per unit
+//   k_fill_exact       matrix.rs:186-331       16x16 tiles of Z, tile list
+//   k_gram_zz          linear.rs:765-780       64x64 tiles of Z^H [Z | y]
+//   k_gram_ccols       linear.rs:765-780       the -cos(k s) columns (sparse)
+//   k_gram_finish      linear.rs:757-785       constraint rows, then +1e-8 I
+//   k_panel            linear.rs:1343-1370     NB columns, one CTA per unit
+//   k_swap_u12         linear.rs:1358-1369     deferred swaps + U block row
+//   k_trailing         linear.rs:1362-1369     A22 -= L21 U12, 64x64 tiles
+//   k_backsub          linear.rs:1372-1381     one warp per unit
+//   k_feedpoints       solve_session.rs:846-947
+#include "fnec_kernels.h"
+#include "fnec_math.cuh"
+
+namespace fnec {
+
+// Gauss-Legendre tables as written in matrix.rs:39-72 (15 decimal digits).
+__constant__ double c_gl_n4[4] = {-0.861136311594953, -0.339981043584856, 0.339981043584856,
+                                  0.861136311594953};
+__constant__ double c_gl_w4[4] = {0.347854845137454, 0.652145154862626, 0.652145154862626,
+                                  0.347854845137454};
+__constant__ double c_gl_n8[8] = {-0.960289856497536, -0.796666477413627, -0.525532409916329,
+                                  -0.183434642495650, 0.183434642495650,  0.525532409916329,
+                                  0.796666477413627,  0.960289856497536};
+__constant__ double c_gl_w8[8] = {0.101228536290376, 0.222381034453374, 0.313706645877887,
+                                  0.362683783378362, 0.362683783378362, 0.313706645877887,
+                                  0.222381034453374, 0.101228536290376};
+
+// ---------------------------------------------------------------------------
+// geometry
+// ---------------------------------------------------------------------------
+__global__ void k_expand_segments(const DevWire *__restrict__ wires, int nw, DevSeg *segs) {
+    int w = blockIdx.x;
+    if (w >= nw) return;
+    DevWire gw = wires[w];
+    double dx = D_SUB(gw.end[0], gw.start[0]);
+    double dy = D_SUB(gw.end[1], gw.start[1]);
+    double dz = D_SUB(gw.end[2], gw.start[2]);
+    double wl = D_SQRT(D_ADD(D_ADD(D_MUL(dx, dx), D_MUL(dy, dy)), D_MUL(dz, dz)));
+    double dir0 = D_DIV(dx, wl), dir1 = D_DIV(dy, wl), dir2 = D_DIV(dz, wl);
+    double nn = (double)gw.nseg;
+    double seg_len = D_DIV(wl, nn);
+    for (uint32_t i = threadIdx.x; i < gw.nseg; i += blockDim.x) {
+        double t0 = D_DIV((double)i, nn);
+        double t1 = D_DIV(D_ADD((double)i, 1.0), nn);
+        double tm = D_MUL(D_ADD(t0, t1), 0.5);
+        DevSeg s;
+        s.start[0] = D_ADD(gw.start[0], D_MUL(dx, t0));
+        s.start[1] = D_ADD(gw.start[1], D_MUL(dy, t0));
+        s.start[2] = D_ADD(gw.start[2], D_MUL(dz, t0));
+        s.end[0] = D_ADD(gw.start[0], D_MUL(dx, t1));
+        s.end[1] = D_ADD(gw.start[1], D_MUL(dy, t1));
+        s.end[2] = D_ADD(gw.start[2], D_MUL(dz, t1));
+        s.mid[0] = D_ADD(gw.start[0], D_MUL(dx, tm));
+        s.mid[1] = D_ADD(gw.start[1], D_MUL(dy, tm));
+        s.mid[2] = D_ADD(gw.start[2], D_MUL(dz, tm));
+        s.dir[0] = dir0;
+        s.dir[1] = dir1;
+        s.dir[2] = dir2;
+        s.len = seg_len;
+        s.rad = gw.radius;
+        s.tag = gw.tag;
+        s.tag_index = i + 1;
+        s.pad = 0.0;
+        segs[gw.seg_off + i] = s;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Hallen RHS: cos(k s_local) per merged conductor and the delta-gap term
+// -j (2 pi / eta0) V sin(k |s - s_src|) on the source's conductor.
+// ---------------------------------------------------------------------------
+__global__ void k_hallen_rhs(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
+                             const DevSeg *__restrict__ segs, const int32_t *__restrict__ ibuf,
+                             const DevSource *__restrict__ srcs, cx *rhs_buf, double *cos_buf,
+                             double scale) {
+    UnitDesc u = units[blockIdx.x];
+    AntDesc a = ants[u.ant];
+    const DevSeg *sg = segs + a.seg_off;
+    const int32_t *comp = ibuf + a.comp_off;
+    const DevSource *src = srcs + a.src_off;
+    double k = u.k_fill;
+    for (int m = threadIdx.x; m < a.n; m += blockDim.x) {
+        int first = comp[2 * m], last = comp[2 * m + 1];
+        const double *wd = sg[first].dir;
+        double wm0 = D_DIV(D_ADD(sg[first].mid[0], sg[last].mid[0]), 2.0);
+        double wm1 = D_DIV(D_ADD(sg[first].mid[1], sg[last].mid[1]), 2.0);
+        double wm2 = D_DIV(D_ADD(sg[first].mid[2], sg[last].mid[2]), 2.0);
+        double dl0 = D_SUB(sg[m].mid[0], wm0);
+        double dl1 = D_SUB(sg[m].mid[1], wm1);
+        double dl2 = D_SUB(sg[m].mid[2], wm2);
+        double s_local = D_ADD(D_ADD(D_MUL(dl0, wd[0]), D_MUL(dl1, wd[1])), D_MUL(dl2, wd[2]));
+        double sn, cs;
+        cr_sincos(D_MUL(k, s_local), &sn, &cs);
+        cos_buf[u.rhs_off + m] = cs;
+        cx r = cx_make(0.0, 0.0);
+        for (int q = 0; q < a.n_src; ++q) {
+            DevSource s = src[q];
+            if (m < s.comp_first || m > s.comp_last) continue;
+            const DevSeg &f = sg[s.feed];
+            double d0 = D_SUB(sg[m].mid[0], f.mid[0]);
+            double d1 = D_SUB(sg[m].mid[1], f.mid[1]);
+            double d2 = D_SUB(sg[m].mid[2], f.mid[2]);
+            double sd = D_ADD(D_ADD(D_MUL(d0, f.dir[0]), D_MUL(d1, f.dir[1])), D_MUL(d2, f.dir[2]));
+            double ss, sc;
+            cr_sincos(D_MUL(k, fabs(sd)), &ss, &sc);
+            cx t = cx_mul(cx_make(0.0, D_MUL(-scale, ss)), cx_make(s.v_re, s.v_im));
+            r = cx_add(r, t);
+        }
+        rhs_buf[u.rhs_off + m] = r;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Z fill
+// ---------------------------------------------------------------------------
+// G(R) = exp(-jkR)/R with exp(0 + jt) = (cos t, sin t) (num-complex exp)
+__device__ __forceinline__ cx green_k_exact(double r, double k) {
+    double sn, cs;
+    cr_sincos(D_MUL(-k, r), &sn, &cs);
+    return cx_make(D_DIV(cs, r), D_DIV(sn, r));
+}
+
+// matrix.rs:297-331 elem(obs, src, k, is_self)
+__device__ __forceinline__ cx elem_exact(const double *om, const double *od, const double *sm,
+                                         const double *sd, double slen, double srad, double k,
+                                         bool is_self) {
+    double cos_alpha = D_ADD(D_ADD(D_MUL(od[0], sd[0]), D_MUL(od[1], sd[1])), D_MUL(od[2], sd[2]));
+    double half = D_MUL(slen, 0.5);
+    double a = srad;
+    double ire, iim;
+    if (is_self) {
+        double sre = 0.0, sim = 0.0;
+#pragma unroll 1
+        for (int m = 0; m < 4; ++m) {
+            double l = D_MUL(c_gl_n4[m], half);
+            double r_eff = D_SQRT(D_ADD(D_MUL(l, l), D_MUL(a, a)));
+            cx g = green_k_exact(r_eff, k);
+            double dre = D_SUB(g.re, D_DIV(1.0, r_eff));
+            sre = D_ADD(sre, D_MUL(c_gl_w4[m], dre));
+            sim = D_ADD(sim, D_MUL(c_gl_w4[m], g.im));
+        }
+        sre = D_MUL(sre, half);
+        sim = D_MUL(sim, half);
+        double r_end = D_SQRT(D_ADD(D_MUL(half, half), D_MUL(a, a)));
+        double analytic = D_MUL(2.0, cr_log(D_DIV(D_ADD(half, r_end), a)));
+        ire = D_ADD(sre, analytic);
+        iim = sim;
+    } else {
+        double sre = 0.0, sim = 0.0;
+#pragma unroll 1
+        for (int m = 0; m < 8; ++m) {
+            double sc = D_MUL(c_gl_n8[m], half);
+            double rs0 = D_ADD(sm[0], D_MUL(sc, sd[0]));
+            double rs1 = D_ADD(sm[1], D_MUL(sc, sd[1]));
+            double rs2 = D_ADD(sm[2], D_MUL(sc, sd[2]));
+            double r0 = D_SUB(om[0], rs0), r1 = D_SUB(om[1], rs1), r2 = D_SUB(om[2], rs2);
+            double r_sq = D_ADD(D_ADD(D_MUL(r0, r0), D_MUL(r1, r1)), D_MUL(r2, r2));
+            double r_eff = D_SQRT(D_ADD(r_sq, D_MUL(a, a)));
+            cx g = green_k_exact(r_eff, k);
+            sre = D_ADD(sre, D_MUL(c_gl_w8[m], g.re));
+            sim = D_ADD(sim, D_MUL(c_gl_w8[m], g.im));
+        }
+        ire = D_MUL(sre, half);
+        iim = D_MUL(sim, half);
+    }
+    return cx_make(D_MUL(ire, cos_alpha), D_MUL(iim, cos_alpha));
+}
+
+__device__ __forceinline__ cx z_entry_exact(const DevSeg &o, const DevSeg &s, double k, int ground,
+                                            bool is_self) {
+    cx direct = elem_exact(o.mid, o.dir, s.mid, s.dir, s.len, s.rad, k, is_self);
+    cx img = cx_make(0.0, 0.0);
+    if (ground == 1) {
+        // matrix.rs:265-279 image: position (x, y, -z), current (-Jx, -Jy, +Jz)
+        double im_mid[3] = {s.mid[0], s.mid[1], -s.mid[2]};
+        double im_dir[3] = {-s.dir[0], -s.dir[1], s.dir[2]};
+        img = elem_exact(o.mid, o.dir, im_mid, im_dir, s.len, s.rad, k, false);
+    }
+    return cx_add(direct, img);
+}
+
+// One CTA of 256 threads fills a 16x16 tile of one unit's Z.
+__global__ void __launch_bounds__(256) k_fill_exact(const UnitDesc *__restrict__ units,
+                                                    const AntDesc *__restrict__ ants,
+                                                    const DevSeg *__restrict__ segs,
+                                                    const int4 *__restrict__ tiles, cx *zbuf) {
+    __shared__ DevSeg s_obs[16];
+    __shared__ DevSeg s_src[16];
+    int4 t = tiles[blockIdx.x];  // (unit, row0, col0, -)
+    UnitDesc u = units[t.x];
+    AntDesc a = ants[u.ant];
+    int n = a.n;
+    const DevSeg *sg = segs + a.seg_off;
+    int tid = threadIdx.x;
+    if (tid < 16 && t.y + tid < n) s_obs[tid] = sg[t.y + tid];
+    if (tid >= 32 && tid < 48 && t.z + tid - 32 < n) s_src[tid - 32] = sg[t.z + tid - 32];
+    __syncthreads();
+    int ii = tid / 16, jj = tid % 16;
+    int i = t.y + ii, j = t.z + jj;
+    if (i >= n || j >= n) return;
+    cx z = z_entry_exact(s_obs[ii], s_src[jj], u.k_fill, a.ground, i == j);
+    zbuf[u.z_off + (int64_t)i * n + j] = z;
+}
+
+// Fill for caller-provided segments (ZSegmentInput): same arithmetic.
+__global__ void __launch_bounds__(256) k_fill_exact_flat(const DevSeg *__restrict__ sg, int n,
+                                                         double k, int ground, cx *z) {
+    int i = blockIdx.y * 16 + threadIdx.x / 16;
+    int j = blockIdx.x * 16 + threadIdx.x % 16;
+    if (i >= n || j >= n) return;
+    z[(int64_t)i * n + j] = z_entry_exact(sg[i], sg[j], k, ground, i == j);
+}
+
+// ---------------------------------------------------------------------------
+// Gram:  A[i][j] = sum_r conj(M[r][i]) M[r][j]  (r ascending, no FMA)
+// ---------------------------------------------------------------------------
+// Part 1: i < N, j <= N over the Z rows r < N, where column j == N is the
+// RHS y (aty).  64x64 output tile per CTA, 4x4 per thread, k-chunks of 16.
+__global__ void __launch_bounds__(256) k_gram_zz(const UnitDesc *__restrict__ units,
+                                                 const int4 *__restrict__ tiles,
+                                                 const cx *__restrict__ zbuf,
+                                                 const cx *__restrict__ rhs_buf, cx *abuf) {
+    __shared__ cx s_l[16][64];  // conj side: Z[r][i0 + ii]
+    __shared__ cx s_r[16][65];  // right side: B[r][j0 + jj], B = [Z | y]
+    int4 t = tiles[blockIdx.x];
+    UnitDesc u = units[t.x];
+    int n = u.n;
+    int i0 = t.y, j0 = t.z;
+    const cx *z = zbuf + u.z_off;
+    const cx *y = rhs_buf + u.rhs_off;
+    int tid = threadIdx.x;
+    int ty = tid / 16, tx = tid % 16;
+    cx acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = cx_make(0.0, 0.0);
+    for (int r0 = 0; r0 < n; r0 += 16) {
+        // load 16 x 64 of each side (4 elements per thread per side)
+        for (int e = tid; e < 16 * 64; e += 256) {
+            int rr = e / 64, cc = e % 64;
+            int r = r0 + rr;
+            int ci = i0 + cc, cj = j0 + cc;
+            cx lv = cx_make(0.0, 0.0), rv = cx_make(0.0, 0.0);
+            if (r < n) {
+                if (ci < n) lv = z[(int64_t)r * n + ci];
+                if (cj < n) rv = z[(int64_t)r * n + cj];
+                else if (cj == n) rv = y[r];
+            }
+            s_l[rr][cc] = lv;
+            s_r[rr][cc] = rv;
+        }
+        __syncthreads();
+        int kmax = min(16, n - r0);
+        for (int kk = 0; kk < kmax; ++kk) {
+            cx lv[4], rv[4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) lv[a] = s_l[kk][ty + 16 * a];
+#pragma unroll
+            for (int b = 0; b < 4; ++b) rv[b] = s_r[kk][tx + 16 * b];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) acc[a][b] = cx_add(acc[a][b], cx_conj_mul(lv[a], rv[b]));
+        }
+        __syncthreads();
+    }
+    int w1 = u.s + 1;
+    cx *A = abuf + u.a_off;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        int i = i0 + ty + 16 * a;
+        if (i >= n) continue;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            int j = j0 + tx + 16 * b;
+            if (j < n) A[(int64_t)i * w1 + j] = acc[a][b];
+            else if (j == n) A[(int64_t)i * w1 + u.s] = acc[a][b];
+        }
+    }
+}
+
+// Part 2: the homogeneous columns N+w (M[r][N+w] = -cos_r for rows of wire
+// w, zero elsewhere; zero products change neither value nor sign of a sum
+// that starts at +0, so only the wire's rows are visited, in ascending r).
+// grid.x = unit, threads stride over i in [0, N] (i == N is the y column).
+__global__ void k_gram_ccols(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
+                             const int32_t *__restrict__ ibuf, const cx *__restrict__ zbuf,
+                             const cx *__restrict__ rhs_buf, const double *__restrict__ cos_buf,
+                             cx *abuf) {
+    UnitDesc u = units[blockIdx.x];
+    AntDesc a = ants[u.ant];
+    int n = u.n, s = u.s, w1 = s + 1;
+    const cx *z = zbuf + u.z_off;
+    const cx *y = rhs_buf + u.rhs_off;
+    const double *cv = cos_buf + u.rhs_off;
+    const int32_t *wptr = ibuf + a.wptr_off;
+    const int32_t *wrow = ibuf + a.wrow_off;
+    cx *A = abuf + u.a_off;
+    for (int w = 0; w < a.w; ++w) {
+        int b = wptr[w], e = wptr[w + 1];
+        for (int i = threadIdx.x; i <= n; i += blockDim.x) {
+            cx col = cx_make(0.0, 0.0);  // A[i][N+w]  (i < N)
+            cx row = cx_make(0.0, 0.0);  // A[N+w][i]  (i < N), or A[N+w][S] for i == N
+            for (int q = b; q < e; ++q) {
+                int r = wrow[q];
+                cx c = cx_make(-cv[r], 0.0);
+                cx zi = (i < n) ? z[(int64_t)r * n + i] : y[r];
+                if (i < n) col = cx_add(col, cx_conj_mul(zi, c));
+                row = cx_add(row, cx_conj_mul(c, zi));
+            }
+            if (i < n) {
+                A[(int64_t)i * w1 + n + w] = col;
+                A[(int64_t)(n + w) * w1 + i] = row;
+            } else {
+                A[(int64_t)(n + w) * w1 + s] = row;
+            }
+        }
+        // the W x W block: diagonal sum of cos^2 terms, exact zeros elsewhere
+        for (int v = threadIdx.x; v < a.w; v += blockDim.x) {
+            cx d = cx_make(0.0, 0.0);
+            if (v == w) {
+                for (int q = b; q < e; ++q) {
+                    cx c = cx_make(-cv[wrow[q]], 0.0);
+                    d = cx_add(d, cx_conj_mul(c, c));
+                }
+            }
+            A[(int64_t)(n + w) * w1 + n + v] = d;
+        }
+    }
+}
+
+// Part 3: constraint rows (free-end I = 0 rows, then junction rows, in
+// row order), then the Tikhonov term +1e-8 on the diagonal.
+__global__ void k_gram_finish(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
+                              const DevConstraint *__restrict__ cons,
+                              const int32_t *__restrict__ codes, cx *abuf) {
+    UnitDesc u = units[blockIdx.x];
+    AntDesc a = ants[u.ant];
+    int w1 = u.s + 1;
+    cx *A = abuf + u.a_off;
+    const DevConstraint *cg = cons + a.con_off;
+    const int32_t *cc = codes + a.conv_off;
+    for (int g = threadIdx.x; g < a.n_con; g += blockDim.x) {
+        DevConstraint c = cg[g];
+        cx e = A[(int64_t)c.i * w1 + c.j];
+        for (int t = 0; t < c.count; ++t) {
+            int code = cc[c.begin + t];
+            cx uv = cx_make((code & 2) ? -1.0 : 1.0, 0.0);
+            cx vv = cx_make((code & 1) ? -1.0 : 1.0, 0.0);
+            e = cx_add(e, cx_conj_mul(uv, vv));
+        }
+        A[(int64_t)c.i * w1 + c.j] = e;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < u.s; i += blockDim.x) {
+        cx d = A[(int64_t)i * w1 + i];
+        A[(int64_t)i * w1 + i] = cx_add(d, cx_make(1e-8, 0.0));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Blocked GEPP with the reference's per-element operation order.
+// Panel columns c0 .. c0+NB-1 are factored right-looking inside the panel;
+// the row swaps are applied to the trailing columns afterwards, and every
+// trailing element then receives its updates in the same column order as
+// the unblocked loop, so the result is identical to linear.rs:1343-1370.
+// The multipliers f = a[r][c] / a[c][c] are stored in place of a[r][c]
+// (the reference leaves a[r][c] - f*a[c][c] there, which it never reads).
+// ---------------------------------------------------------------------------
+constexpr int NB = 32;
+
+// Pivot reduction: largest hypot, ties resolved to the larger row index
+// (Iterator::max_by keeps the last maximum).
+__device__ __forceinline__ void piv_better(double &bv, int &bi, double v, int i) {
+    if (v > bv || (v == bv && i > bi)) {
+        bv = v;
+        bi = i;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_panel(const UnitDesc *__restrict__ units, int c0,
+                                               cx *abuf, int32_t *piv_buf, int32_t *status) {
+    __shared__ double s_v[8];
+    __shared__ int s_i[8];
+    __shared__ int s_p;
+    __shared__ cx s_prow[NB];
+    int ui = blockIdx.x;
+    UnitDesc u = units[ui];
+    int s = u.s;
+    if (c0 >= s || status[ui] != 0) return;
+    int w1 = s + 1;
+    cx *A = abuf + u.a_off;
+    int32_t *piv = piv_buf + u.x_off;
+    int nb = min(NB, s - c0);
+    int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int c = c0; c < c0 + nb; ++c) {
+        // --- pivot search over rows c..s-1 of column c
+        double bv = -1.0;
+        int bi = -1;
+        for (int r = c + tid; r < s; r += blockDim.x) piv_better(bv, bi, cx_norm(A[(int64_t)r * w1 + c]), r);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double ov = __shfl_down_sync(0xffffffffu, bv, o);
+            int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            piv_better(bv, bi, ov, oi);
+        }
+        if (lane == 0) {
+            s_v[wid] = bv;
+            s_i[wid] = bi;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double v = s_v[0];
+            int p = s_i[0];
+            for (int q = 1; q < (int)(blockDim.x >> 5); ++q) piv_better(v, p, s_v[q], s_i[q]);
+            // linear.rs:1354 singular test on the chosen pivot (NaN never passes <)
+            if (p < 0 || v < 1e-30) {
+                status[ui] = -(c + 1);
+                p = -1;
+            }
+            s_p = p;
+            piv[c] = p;
+        }
+        __syncthreads();
+        int p = s_p;
+        if (p < 0) return;
+        // --- swap rows c and p inside the panel columns
+        if (p != c && tid < nb) {
+            int k = c0 + tid;
+            cx t0 = A[(int64_t)c * w1 + k];
+            A[(int64_t)c * w1 + k] = A[(int64_t)p * w1 + k];
+            A[(int64_t)p * w1 + k] = t0;
+        }
+        __syncthreads();
+        if (tid < nb) s_prow[tid] = A[(int64_t)c * w1 + c0 + tid];
+        __syncthreads();
+        cx diag = s_prow[c - c0];
+        // --- eliminate below the pivot inside the panel
+        for (int r = c + 1 + tid; r < s; r += blockDim.x) {
+            cx *row = A + (int64_t)r * w1;
+            cx f = cx_div(row[c], diag);
+            row[c] = f;
+            for (int k = c + 1; k < c0 + nb; ++k) row[k] = cx_sub(row[k], cx_mul(f, s_prow[k - c0]));
+        }
+        __syncthreads();
+    }
+}
+
+// Deferred swaps and the U12 block row: one thread per trailing column K.
+__global__ void k_swap_u12(const UnitDesc *__restrict__ units, int c0, cx *abuf,
+                           const int32_t *__restrict__ piv_buf, const int32_t *__restrict__ status) {
+    int ui = blockIdx.y;
+    UnitDesc u = units[ui];
+    int s = u.s;
+    if (c0 >= s || status[ui] != 0) return;
+    int nb = min(NB, s - c0);
+    int K = c0 + nb + blockIdx.x * blockDim.x + threadIdx.x;
+    if (K > s) return;  // column s is the right-hand side
+    int w1 = s + 1;
+    cx *A = abuf + u.a_off;
+    const int32_t *piv = piv_buf + u.x_off;
+    cx col[NB];
+#pragma unroll
+    for (int q = 0; q < NB; ++q)
+        if (q < nb) col[q] = A[(int64_t)(c0 + q) * w1 + K];
+    for (int q = 0; q < nb; ++q) {
+        int p = piv[c0 + q];
+        if (p != c0 + q) {
+            // row p lies below the panel or inside it
+            if (p < c0 + nb) {
+                cx t0 = col[q];
+                col[q] = col[p - c0];
+                col[p - c0] = t0;
+            } else {
+                cx t0 = col[q];
+                col[q] = A[(int64_t)p * w1 + K];
+                A[(int64_t)p * w1 + K] = t0;
+            }
+        }
+    }
+    // U12: row c0+q receives the updates of panel columns c0 .. c0+q-1 in order
+    for (int q = 1; q < nb; ++q) {
+        const cx *lrow = A + (int64_t)(c0 + q) * w1 + c0;
+        cx v = col[q];
+        for (int c = 0; c < q; ++c) v = cx_sub(v, cx_mul(lrow[c], col[c]));
+        col[q] = v;
+    }
+#pragma unroll
+    for (int q = 0; q < NB; ++q)
+        if (q < nb) A[(int64_t)(c0 + q) * w1 + K] = col[q];
+}
+
+// A22 -= L21 * U12 with per-element in-order accumulation over the panel.
+// grid.x = tiles of 64x64 over the trailing block, grid.y = unit.
+__global__ void __launch_bounds__(256) k_trailing(const UnitDesc *__restrict__ units, int c0,
+                                                  cx *abuf, const int32_t *__restrict__ status) {
+    extern __shared__ cx s_dyn[];
+    cx(*s_l)[NB + 1] = reinterpret_cast<cx(*)[NB + 1]>(s_dyn);
+    cx(*s_u)[64] = reinterpret_cast<cx(*)[64]>(s_dyn + 64 * (NB + 1));
+    int ui = blockIdx.y;
+    UnitDesc u = units[ui];
+    int s = u.s;
+    if (c0 + NB >= s || status[ui] != 0) return;  // no trailing block (or a failed unit)
+    int r0 = c0 + NB;  // first trailing row/column
+    int rows = s - r0, cols = s + 1 - r0;
+    int tiles_c = (cols + 63) / 64;
+    int tiles_r = (rows + 63) / 64;
+    int tile = blockIdx.x;
+    if (tile >= tiles_r * tiles_c) return;
+    int R0 = r0 + (tile / tiles_c) * 64;
+    int K0 = r0 + (tile % tiles_c) * 64;
+    int w1 = s + 1;
+    cx *A = abuf + u.a_off;
+    int tid = threadIdx.x;
+    for (int e = tid; e < 64 * NB; e += 256) {
+        int rr = e / NB, q = e % NB;
+        int R = R0 + rr;
+        s_l[rr][q] = (R < s) ? A[(int64_t)R * w1 + c0 + q] : cx_make(0.0, 0.0);
+    }
+    for (int e = tid; e < NB * 64; e += 256) {
+        int q = e / 64, cc = e % 64;
+        int K = K0 + cc;
+        s_u[q][cc] = (K <= s) ? A[(int64_t)(c0 + q) * w1 + K] : cx_make(0.0, 0.0);
+    }
+    __syncthreads();
+    int ty = tid / 16, tx = tid % 16;
+    cx acc[4][4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            int R = R0 + ty + 16 * a, K = K0 + tx + 16 * b;
+            acc[a][b] = (R < s && K <= s) ? A[(int64_t)R * w1 + K] : cx_make(0.0, 0.0);
+        }
+    for (int q = 0; q < NB; ++q) {
+        cx lv[4], uv[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) lv[a] = s_l[ty + 16 * a][q];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) uv[b] = s_u[q][tx + 16 * b];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] = cx_sub(acc[a][b], cx_mul(lv[a], uv[b]));
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            int R = R0 + ty + 16 * a, K = K0 + tx + 16 * b;
+            if (R < s && K <= s) A[(int64_t)R * w1 + K] = acc[a][b];
+        }
+}
+
+// Back substitution x_i = (b_i - sum_{j>i} a_ij x_j) / a_ii, j ascending.
+// One warp per unit: the 32 lanes form products a_ij x_j ahead of time and
+// lane 0 subtracts them in order (the subtraction chain is sequential in
+// the reference and stays sequential here).
+__global__ void k_backsub(const UnitDesc *__restrict__ units, const cx *__restrict__ abuf, cx *xbuf,
+                          const int32_t *__restrict__ status) {
+    extern __shared__ cx s_x[];
+    int ui = blockIdx.x;
+    UnitDesc u = units[ui];
+    if (status[ui] != 0) return;
+    int s = u.s, w1 = s + 1;
+    const cx *A = abuf + u.a_off;
+    int lane = threadIdx.x;
+    __shared__ cx s_p[32];
+    for (int i = s - 1; i >= 0; --i) {
+        const cx *row = A + (int64_t)i * w1;
+        cx sum = row[s];
+        for (int j0 = i + 1; j0 < s; j0 += 32) {
+            int j = j0 + lane;
+            if (j < s) s_p[lane] = cx_mul(row[j], s_x[j]);
+            __syncwarp();
+            if (lane == 0) {
+                int cnt = min(32, s - j0);
+                for (int q = 0; q < cnt; ++q) sum = cx_sub(sum, s_p[q]);
+            }
+            __syncwarp();
+        }
+        if (lane == 0) s_x[i] = cx_div(sum, row[i]);
+        __syncwarp();
+    }
+    for (int i = lane; i < s; i += 32) xbuf[u.x_off + i] = s_x[i];
+}
+
+// Feedpoint rows: v_source = v_vec[idx] * dl, Zin = v_source / I[idx] when
+// |I| > 1e-60 (solve_session.rs:911-917).
+__global__ void k_feedpoints(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
+                             const DevSeg *__restrict__ segs, const DevFeed *__restrict__ feeds,
+                             const cx *__restrict__ xbuf, const int32_t *__restrict__ status,
+                             double *feed_out, const int64_t *__restrict__ feed_row_off) {
+    int ui = blockIdx.x;
+    UnitDesc u = units[ui];
+    AntDesc a = ants[u.ant];
+    for (int q = threadIdx.x; q < a.n_feed; q += blockDim.x) {
+        DevFeed f = feeds[a.feed_off + q];
+        double *o = feed_out + 7 * (feed_row_off[ui] + q);
+        if (status[ui] != 0) {
+            for (int t = 0; t < 7; ++t) o[t] = 0.0;
+            continue;
+        }
+        double dl = segs[a.seg_off + f.seg].len;
+        cx vs = cx_make(D_MUL(f.vdl_re, dl), D_MUL(f.vdl_im, dl));
+        cx cur = xbuf[u.x_off + f.seg];
+        cx zin = cx_norm(cur) > 1e-60 ? cx_div(vs, cur) : vs;
+        o[0] = (double)f.seg;
+        o[1] = vs.re;
+        o[2] = vs.im;
+        o[3] = cur.re;
+        o[4] = cur.im;
+        o[5] = zin.re;
+        o[6] = zin.im;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launch wrappers (host)
+// ---------------------------------------------------------------------------
+void launch_expand_segments(const DevWire *wires, int nw, DevSeg *segs, cudaStream_t st) {
+    if (nw > 0) k_expand_segments<<<nw, 64, 0, st>>>(wires, nw, segs);
+}
+void launch_hallen_rhs(const UnitDesc *units, int nu, const AntDesc *ants, const DevSeg *segs,
+                       const int32_t *ibuf, const DevSource *srcs, cx *rhs, double *cosv,
+                       double scale, cudaStream_t st) {
+    if (nu > 0) k_hallen_rhs<<<nu, 128, 0, st>>>(units, ants, segs, ibuf, srcs, rhs, cosv, scale);
+}
+void launch_fill_exact(const UnitDesc *units, const AntDesc *ants, const DevSeg *segs,
+                       const int4 *tiles, int ntiles, cx *z, cudaStream_t st) {
+    if (ntiles > 0) k_fill_exact<<<ntiles, 256, 0, st>>>(units, ants, segs, tiles, z);
+}
+void launch_fill_exact_flat(const DevSeg *segs, int n, double k, int ground, cx *z, cudaStream_t st) {
+    dim3 g((n + 15) / 16, (n + 15) / 16);
+    if (n > 0) k_fill_exact_flat<<<g, 256, 0, st>>>(segs, n, k, ground, z);
+}
+void launch_gram_exact(const UnitDesc *units, int nu, const AntDesc *ants, const int4 *gtiles,
+                       int ngtiles, const int32_t *ibuf, const DevConstraint *cons,
+                       const int32_t *codes, const cx *z, const cx *rhs, const double *cosv, cx *A,
+                       cudaStream_t st) {
+    if (ngtiles > 0) k_gram_zz<<<ngtiles, 256, 0, st>>>(units, gtiles, z, rhs, A);
+    if (nu > 0) {
+        k_gram_ccols<<<nu, 256, 0, st>>>(units, ants, ibuf, z, rhs, cosv, A);
+        k_gram_finish<<<nu, 256, 0, st>>>(units, ants, cons, codes, A);
+    }
+}
+constexpr size_t TRAILING_SMEM = sizeof(cx) * (64 * (NB + 1) + NB * 64);
+
+void launch_factor_exact(const UnitDesc *units, int nu, int max_s, int max_trailing_tiles, cx *A,
+                         int32_t *piv, int32_t *status, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_trailing, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TRAILING_SMEM);
+        attr = true;
+    }
+    for (int c0 = 0; c0 < max_s; c0 += NB) {
+        k_panel<<<nu, 256, 0, st>>>(units, c0, A, piv, status);
+        // columns right of the panel: at least the right-hand side column
+        int rest = max_s + 1 - (c0 + NB);
+        if (rest < 1) rest = 1;
+        {
+            dim3 g1((rest + 127) / 128, nu);
+            k_swap_u12<<<g1, 128, 0, st>>>(units, c0, A, piv, status);
+            int rows = max_s - (c0 + NB);
+            if (rows > 0) {
+                int t = ((rows + 63) / 64) * ((rest + 63) / 64);
+                dim3 g2(t, nu);
+                k_trailing<<<g2, 256, TRAILING_SMEM, st>>>(units, c0, A, status);
+            }
+        }
+    }
+    (void)max_trailing_tiles;
+}
+void launch_backsub(const UnitDesc *units, int nu, int max_s, const cx *A, cx *x,
+                    const int32_t *status, cudaStream_t st) {
+    size_t smem = sizeof(cx) * (size_t)max_s;
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_backsub, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (nu > 0) k_backsub<<<nu, 32, smem, st>>>(units, A, x, status);
+}
+void launch_feedpoints(const UnitDesc *units, int nu, const AntDesc *ants, const DevSeg *segs,
+                       const DevFeed *feeds, const cx *x, const int32_t *status, double *feed_out,
+                       const int64_t *feed_row_off, cudaStream_t st) {
+    if (nu > 0)
+        k_feedpoints<<<nu, 32, 0, st>>>(units, ants, segs, feeds, x, status, feed_out, feed_row_off);
+}
+
+}  // namespace fnec

@@ -1,0 +1,126 @@
+// fnec_types.h -- device-side data layout of a Hallen batch.
+//
+// A batch holds A antennas (geometries) and U units; a unit is one
+// (antenna, frequency) solve.  Everything the kernels touch lives in a few
+// flat device arrays addressed through the descriptors below:
+//
+//   segments   DevSeg[total_segments]          128 B each, one cache line
+//   Z          complex128 N*N per unit          row-major
+//   A          complex128 S*(S+1) per unit      augmented [A | b], row-major
+//   x          complex128 S per unit            solution (currents, C_hom)
+//   rhs, cosv  complex128 N / f64 N per unit    Hallen RHS and cos(k s)
+//
+// S = N + W where W is the number of (merged) wire endpoint pairs.
+#pragma once
+#include <stdint.h>
+
+namespace fnec {
+
+struct DevSeg {          // nec_solver::geometry::Segment (geometry.rs:115-134)
+    double mid[3];
+    double dir[3];
+    double len;
+    double rad;
+    double start[3];
+    double end[3];
+    uint32_t tag;
+    uint32_t tag_index;
+    double pad;
+};
+static_assert(sizeof(DevSeg) == 128, "DevSeg is one 128-byte line");
+
+struct DevWire {         // one GW card, expanded by k_expand_segments
+    double start[3];
+    double end[3];
+    double radius;
+    uint32_t tag;
+    uint32_t nseg;
+    int64_t seg_off;     // global index of its first segment
+};
+
+// A straight run of segments whose midpoints advance by a constant step
+// (every GW card expands into one).  Used by the far-field Horner sum.
+struct DevRun {
+    double mid0[3];      // midpoint of the first segment
+    double step[3];      // midpoint increment between consecutive segments
+    double dir[3];
+    double len;
+    int32_t first;       // antenna-local index of the first segment
+    int32_t count;
+};
+
+struct AntDesc {
+    int64_t seg_off;     // into segments
+    int32_t n;           // segments
+    int32_t w;           // homogeneous columns (merged wires)
+    int64_t rowwire_off; // int32[n]: wire column of each row (linear.rs:728-733)
+    int64_t wrow_off;    // CSR: int32 rows of each wire column, wrow_ptr
+    int64_t wptr_off;    // int32[w+1]
+    int64_t comp_off;    // int32[2n]: merged component (first,last) of each segment
+    int64_t src_off;     // DevSource[n_src] (resolved BTreeMap order)
+    int32_t n_src;
+    int32_t n_con;       // constraint pair groups
+    int64_t con_off;     // DevConstraint groups
+    int64_t conv_off;    // int32 value codes for each group (row order)
+    int64_t feed_off;    // DevFeed[n_feed]
+    int32_t n_feed;
+    int32_t ground;      // 0 free space, 1 PEC image
+    int64_t run_off;     // DevRun[n_run]
+    int32_t n_run;
+    int32_t pad;
+};
+
+struct DevSource {       // one resolved delta-gap source (excitation.rs:171-187)
+    int32_t feed;        // antenna-local segment index
+    int32_t comp_first;  // merged component of the feed segment
+    int32_t comp_last;
+    int32_t pad;
+    double v_re, v_im;
+};
+
+struct DevFeed {         // one EX card row of build_feedpoint_rows
+    int32_t seg;
+    int32_t pad;
+    double vdl_re, vdl_im;   // v_vec[idx] = sum of V/dl on that segment
+};
+
+// One (i, j) entry of the Gram touched by constraint rows; its
+// contributions, in row order, are codes in conv[begin .. begin+count):
+// each code packs (u_val, v_val) with values in {1, -1}.
+struct DevConstraint {
+    int32_t i, j;
+    int32_t begin, count;
+};
+
+struct UnitDesc {
+    int32_t ant;
+    int32_t n;
+    int32_t s;           // n + w
+    int32_t pad;
+    double freq;
+    double k_fill;       // 2*pi*f/c (matrix.rs:194, excitation.rs:165)
+    double k_rp;         // 2*pi/(c/f) (farfield.rs:570-571)
+    int64_t z_off;       // complex elements
+    int64_t a_off;       // complex elements of [A|b]
+    int64_t x_off;       // complex elements
+    int64_t rhs_off;     // complex elements (rhs) and doubles (cosv)
+    int64_t pat_off;     // requested pattern points (4 doubles each)
+    int64_t ff_off;      // far-field partial sums
+};
+
+// Requested pattern points of one antenna: an RP card grid (phi outer,
+// theta inner, farfield.rs:677-699) or an explicit (theta, phi) list.
+struct DevRp {
+    int32_t n_theta, n_phi;
+    double theta0, phi0, d_theta, d_phi;
+    int64_t pts_off;      // >= 0: explicit list of n_pts (theta, phi) pairs
+    int32_t n_pts;
+    int32_t skip_integral;  // 1: use total_given instead of integrating
+    double total_given;
+};
+
+// Constraint-row contribution codes: bit 1 set -> the conj side is -1,
+// bit 0 set -> the other side is -1 (values are 1 or the junction sign).
+inline int32_t con_code(double u, double v) { return (u < 0 ? 2 : 0) | (v < 0 ? 1 : 0); }
+
+}  // namespace fnec

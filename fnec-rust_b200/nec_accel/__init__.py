@@ -1,0 +1,564 @@
+"""Host-side mirror of fnec-rust's ``nec_accel`` crate over libfnec_cuda.so.
+
+The reference's accelerator crate (crates/nec_accel/src/lib.rs:52-96,
+wgpu_device.rs) exposes ``fill_zmatrix_wgpu``, ``solve_hallen_gpu_resident``,
+``run_rp_farfield_batch_wgpu``, ``microbench_zmatrix_dispatch``,
+``enumerate_compute_adapters`` and ``dispatch_frequency_point``.  This module
+keeps those names and argument meanings (segments, rhs, cos_vec, wire
+endpoints, junctions, frequency) and calls the CUDA library through its C
+ABI (include/fnec_cuda.h).  Differences in error behaviour are deliberate:
+where the reference returns ``None`` and lets its caller fall back to the
+CPU, these functions raise :class:`AccelError` -- there is no CPU fallback.
+
+The batched interface (:class:`HallenBatch`) runs whole per-frequency
+solves (solve_session.rs:1186-1437 + the RP grid of :1645) for many
+antennas and frequencies in one device pipeline.
+"""
+from __future__ import annotations
+
+import atexit
+import ctypes
+import os
+import weakref
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfnec_cuda.so")
+
+OK = 0
+ERR_BAD_ARG = -1
+ERR_NO_DEVICE = -2
+ERR_OUT_OF_MEMORY = -3
+ERR_CUDA = -4
+ERR_SINGULAR = -5
+ERR_SEGMENT_NOT_FOUND = -6
+ERR_UNSUPPORTED = -7
+ERR_TIMEOUT = -8
+ERR_BUSY = -9
+
+GROUND_FREE = 0
+GROUND_PEC = 1
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+
+ZSEGMENT_DTYPE = np.dtype([("midpoint", "<f8", 3), ("direction", "<f8", 3), ("length", "<f8"),
+                           ("radius", "<f8")])
+GPU_SEGMENT_DTYPE = np.dtype([("midpoint", "<f8", 3), ("direction", "<f8", 3), ("length", "<f8")])
+RP_RESULT_DTYPE = np.dtype([("u_theta", "<f8"), ("u_phi", "<f8"), ("gain_total_dbi", "<f8"),
+                            ("gain_theta_dbi", "<f8"), ("gain_phi_dbi", "<f8"), ("axial_ratio", "<f8"),
+                            ("theta_deg", "<f8"), ("phi_deg", "<f8")])
+JUNCTION_DTYPE = np.dtype([("seg_a", "<u8"), ("seg_b", "<u8"), ("sign", "<f8")])
+WIRE_DTYPE = np.dtype([("tag", "<u4"), ("segments", "<u4"), ("start", "<f8", 3), ("end", "<f8", 3),
+                       ("radius", "<f8")])
+SOURCE_DTYPE = np.dtype([("tag", "<u4"), ("segment", "<u4"), ("v_re", "<f8"), ("v_im", "<f8")])
+FEED_COLUMNS = ("seg", "v_re", "v_im", "i_re", "i_im", "z_re", "z_im")
+PATTERN_COLUMNS = ("gain_total_dbi", "gain_theta_dbi", "gain_phi_dbi", "axial_ratio", "u_theta", "u_phi")
+
+_P = ctypes.c_void_p
+_U64 = ctypes.c_uint64
+_U32 = ctypes.c_uint32
+_I32 = ctypes.c_int32
+_D = ctypes.c_double
+
+
+class AccelError(RuntimeError):
+    """A failed device call; ``code`` is the library status (FNEC_ERR_*)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"fnec_cuda error {code}: {msg}")
+        self.code = code
+
+
+class _RpCard(ctypes.Structure):
+    _fields_ = [("n_theta", _U32), ("n_phi", _U32), ("theta0", _D), ("phi0", _D), ("d_theta", _D),
+                ("d_phi", _D)]
+
+
+class _Antenna(ctypes.Structure):
+    _fields_ = [("wires", _P), ("n_wires", _U32), ("sources", _P), ("n_sources", _U32), ("ground", _I32),
+                ("n_freqs", _U32), ("freqs_hz", _P), ("rp", _P)]
+
+
+class _UnitInfo(ctypes.Structure):
+    _fields_ = [("antenna", _U32), ("n", _U32), ("s", _U32), ("n_feed", _U32), ("n_points", _U32),
+                ("freq_hz", _D), ("cur_off", _U64), ("feed_off", _U64), ("pat_off", _U64)]
+
+
+class _BatchInfo(ctypes.Structure):
+    _fields_ = [("n_units", _U32), ("max_s", _U32), ("total_currents", _U64), ("total_feeds", _U64),
+                ("total_points", _U64), ("device_bytes", _U64), ("h2d_bytes", _U64),
+                ("kernel_launches", _U64)]
+
+
+# name -> (restype, argtypes); every function declared in include/fnec_cuda.h
+SIGNATURES = {
+    "fnec_ctx_create": (ctypes.c_int, [ctypes.c_int, _P]),
+    "fnec_ctx_destroy": (ctypes.c_int, [_P]),
+    "fnec_ctx_last_error": (ctypes.c_char_p, [_P]),
+    "fnec_ctx_stream": (_P, [_P]),
+    "fnec_fill_zmatrix": (ctypes.c_int, [_P, _P, _U64, _D, _I32, _P]),
+    "fnec_solve_hallen_resident": (ctypes.c_int, [_P, _P, _U64, _P, _P, _P, _U64, _P, _U64, _D, _I32, _I32,
+                                                  _P, _P]),
+    "fnec_solve_hallen": (ctypes.c_int, [_P, _P, _U64, _P, _P, _P, _U64, _P, _U64, _I32, _P, _P]),
+    "fnec_rp_farfield_batch": (ctypes.c_int, [_P, _P, _U64, _P, _D, _D, _P, _U64, _P]),
+    "fnec_radiation_pattern": (ctypes.c_int, [_P, _P, _U64, _P, _D, _I32, _P, _U64, _P, _P]),
+    "fnec_integrate_radiated_power": (ctypes.c_int, [_P, _P, _U64, _P, _D, _I32, _P]),
+    "fnec_microbench_zmatrix_dispatch": (ctypes.c_int, [ctypes.c_int, _U64, _U32, _P, _P, _P]),
+    "fnec_enumerate_devices": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_char_p, _U64]),
+    "fnec_dispatch_frequency_point": (ctypes.c_int, [ctypes.c_int, _D]),
+    "fnec_measure_fp64_peak": (ctypes.c_int, [ctypes.c_int, _P, _P]),
+    "fnec_batch_create": (ctypes.c_int, [_P, _P, _U32, _I32, _P]),
+    "fnec_batch_destroy": (ctypes.c_int, [_P]),
+    "fnec_batch_get_info": (ctypes.c_int, [_P, _P]),
+    "fnec_batch_get_unit_info": (ctypes.c_int, [_P, _U32, _P]),
+    "fnec_batch_upload": (ctypes.c_int, [_P]),
+    "fnec_batch_run": (ctypes.c_int, [_P]),
+    "fnec_batch_sync": (ctypes.c_int, [_P]),
+    "fnec_batch_read": (ctypes.c_int, [_P, _P, _P, _P, _P, _P]),
+    "fnec_batch_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
+    "fnec_batch_phase_ms": (ctypes.c_int, [_P, _P]),
+    "fnec_batch_read_unit": (ctypes.c_int, [_P, _U32, _P, _P]),
+    "fnec_batch_read_z": (ctypes.c_int, [_P, _U32, _P]),
+}
+
+_lib = None
+# Live handles, released in a fixed order at interpreter exit (batches before
+# the contexts they were created on): module teardown order is otherwise
+# arbitrary and a batch must never outlive its context.
+_live_batches = weakref.WeakSet()
+_live_contexts = weakref.WeakSet()
+_shutting_down = False
+
+
+@atexit.register
+def _release_all():
+    global _shutting_down
+    for b in list(_live_batches):
+        b.close()
+    for c in list(_live_contexts):
+        c.close()
+    _shutting_down = True
+
+
+def lib():
+    """Load libfnec_cuda.so (built in-tree by __graft_entry__.build()).
+
+    Raises AccelError if the library is missing: the product path never
+    falls back to a CPU implementation."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise AccelError(ERR_NO_DEVICE, f"{LIB_PATH} is not built")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+class Context:
+    """One device context (CUDA device + stream) of the library."""
+
+    def __init__(self, device: int = 0):
+        h = ctypes.c_void_p()
+        st = lib().fnec_ctx_create(device, ctypes.byref(h))
+        if st != OK:
+            raise AccelError(st, f"fnec_ctx_create(device={device})")
+        self._h = h
+        _live_contexts.add(self)
+
+    @property
+    def handle(self):
+        return self._h
+
+    def check(self, st: int, what: str):
+        if st != OK:
+            msg = lib().fnec_ctx_last_error(self._h)
+            raise AccelError(st, f"{what}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            for b in list(_live_batches):
+                if b.ctx is self:
+                    b.close()
+            lib().fnec_ctx_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        if _shutting_down:
+            return
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+def zsegments_from(segs) -> np.ndarray:
+    """ZSegmentInput records from any array with mid/dir/length/radius fields."""
+    out = np.zeros(len(segs), dtype=ZSEGMENT_DTYPE)
+    names = segs.dtype.names
+    out["midpoint"] = segs["mid"] if "mid" in names else segs["midpoint"]
+    out["direction"] = segs["dir"] if "dir" in names else segs["direction"]
+    out["length"] = segs["length"]
+    out["radius"] = segs["radius"]
+    return out
+
+
+def gpu_segments_from(segs) -> np.ndarray:
+    out = np.zeros(len(segs), dtype=GPU_SEGMENT_DTYPE)
+    names = segs.dtype.names
+    out["midpoint"] = segs["mid"] if "mid" in names else segs["midpoint"]
+    out["direction"] = segs["dir"] if "dir" in names else segs["direction"]
+    out["length"] = segs["length"]
+    return out
+
+
+# --------------------------------------------------------------------------
+# reference nec_accel entry points
+# --------------------------------------------------------------------------
+def fill_zmatrix(segments, freq_hz: float, ground: int = GROUND_FREE, ctx: Optional[Context] = None):
+    """fill_zmatrix_wgpu (wgpu_device.rs:832): the N x N Hallen matrix,
+    complex128, row-major; FP64 and with the PEC image when ground == 1."""
+    ctx = ctx or default_context()
+    segs = np.ascontiguousarray(segments, dtype=ZSEGMENT_DTYPE)
+    n = len(segs)
+    z = np.zeros((n, n), np.complex128)
+    ctx.check(lib().fnec_fill_zmatrix(ctx.handle, _ptr(segs), n, float(freq_hz), int(ground), _ptr(z)),
+              "fill_zmatrix")
+    return z
+
+
+def solve_hallen_gpu_resident(segments, rhs, cos_vec, wire_endpoints, junctions, freq_hz: float,
+                              ground: int = GROUND_FREE, precision: int = PRECISION_FP64,
+                              ctx: Optional[Context] = None, return_pivots: bool = False):
+    """solve_hallen_gpu_resident (wgpu_device.rs:1294-1301): fill, normal
+    equations and elimination on the device; returns x = [I_0..I_{N-1},
+    C_0..C_{W-1}] (and the pivot rows when ``return_pivots``)."""
+    ctx = ctx or default_context()
+    segs = np.ascontiguousarray(segments, dtype=ZSEGMENT_DTYPE)
+    n = len(segs)
+    rhs = np.ascontiguousarray(rhs, np.complex128)
+    cosv = np.ascontiguousarray(cos_vec, np.float64)
+    ep = np.ascontiguousarray(np.asarray(wire_endpoints, dtype=np.uint64).reshape(-1, 2))
+    jn = np.zeros(len(junctions), dtype=JUNCTION_DTYPE)
+    for i, (a, b, s) in enumerate(junctions):
+        jn[i] = (a, b, s)
+    w = max(len(ep), 1)
+    x = np.zeros(n + w, np.complex128)
+    piv = np.zeros(n + w, np.int32)
+    ctx.check(lib().fnec_solve_hallen_resident(ctx.handle, _ptr(segs), n, _ptr(rhs), _ptr(cosv), _ptr(ep),
+                                               len(ep), _ptr(jn), len(jn), float(freq_hz), int(ground),
+                                               int(precision), _ptr(x), _ptr(piv)),
+              "solve_hallen_gpu_resident")
+    return (x, piv) if return_pivots else x
+
+
+def solve_hallen(z, rhs, cos_vec, wire_endpoints, junctions, precision: int = PRECISION_FP64,
+                 ctx: Optional[Context] = None, return_pivots: bool = False):
+    """nec_solver::solve_hallen (linear.rs:672-797) on a given Z matrix."""
+    ctx = ctx or default_context()
+    z = np.ascontiguousarray(z, np.complex128)
+    n = z.shape[0]
+    rhs = np.ascontiguousarray(rhs, np.complex128)
+    cosv = np.ascontiguousarray(cos_vec, np.float64)
+    ep = np.ascontiguousarray(np.asarray(wire_endpoints, dtype=np.uint64).reshape(-1, 2))
+    jn = np.zeros(len(junctions), dtype=JUNCTION_DTYPE)
+    for i, (a, b, s) in enumerate(junctions):
+        jn[i] = (a, b, s)
+    w = max(len(ep), 1)
+    x = np.zeros(n + w, np.complex128)
+    piv = np.zeros(n + w, np.int32)
+    ctx.check(lib().fnec_solve_hallen(ctx.handle, _ptr(z), n, _ptr(rhs), _ptr(cosv), _ptr(ep), len(ep),
+                                      _ptr(jn), len(jn), int(precision), _ptr(x), _ptr(piv)), "solve_hallen")
+    return (x, piv) if return_pivots else x
+
+
+def run_rp_farfield_batch(segments, currents, k: float, total_radiated: float, points,
+                          ctx: Optional[Context] = None) -> np.ndarray:
+    """run_rp_farfield_batch_wgpu (wgpu_device.rs:461-467): RpGpuResult per
+    (theta, phi) point, normalised by the caller's ``total_radiated``."""
+    ctx = ctx or default_context()
+    segs = np.ascontiguousarray(segments, dtype=GPU_SEGMENT_DTYPE)
+    cur = np.ascontiguousarray(currents, np.complex128)
+    pts = np.ascontiguousarray(points, np.float64).reshape(-1, 2)
+    out = np.zeros(len(pts), dtype=RP_RESULT_DTYPE)
+    ctx.check(lib().fnec_rp_farfield_batch(ctx.handle, _ptr(segs), len(segs), _ptr(cur), float(k),
+                                           float(total_radiated), _ptr(pts), len(pts), _ptr(out)),
+              "run_rp_farfield_batch")
+    return out
+
+
+def compute_radiation_pattern(segments, currents, freq_hz: float, points, ground: int = GROUND_FREE,
+                              ctx: Optional[Context] = None):
+    """compute_radiation_pattern (farfield.rs:563-647) with the power
+    integral on the device.  Returns ((p, 4) gains/axial ratio, total)."""
+    ctx = ctx or default_context()
+    segs = np.ascontiguousarray(segments, dtype=GPU_SEGMENT_DTYPE)
+    cur = np.ascontiguousarray(currents, np.complex128)
+    pts = np.ascontiguousarray(points, np.float64).reshape(-1, 2)
+    out = np.zeros((len(pts), 4), np.float64)
+    tot = np.zeros(1, np.float64)
+    ctx.check(lib().fnec_radiation_pattern(ctx.handle, _ptr(segs), len(segs), _ptr(cur), float(freq_hz),
+                                           int(ground), _ptr(pts), len(pts), _ptr(out), _ptr(tot)),
+              "compute_radiation_pattern")
+    return out, float(tot[0])
+
+
+def integrate_radiated_power(segments, currents, freq_hz: float, pec_ground: bool,
+                             ctx: Optional[Context] = None) -> float:
+    """integrate_radiated_power (farfield.rs:409-417)."""
+    ctx = ctx or default_context()
+    segs = np.ascontiguousarray(segments, dtype=GPU_SEGMENT_DTYPE)
+    cur = np.ascontiguousarray(currents, np.complex128)
+    tot = np.zeros(1, np.float64)
+    ctx.check(lib().fnec_integrate_radiated_power(ctx.handle, _ptr(segs), len(segs), _ptr(cur), float(freq_hz),
+                                                  int(bool(pec_ground)), _ptr(tot)),
+              "integrate_radiated_power")
+    return float(tot[0])
+
+
+@dataclass
+class GpuMicrobench:
+    """GpuMicrobench (wgpu_device.rs:1064-1075)."""
+
+    n_segments: int
+    n_dispatches: int
+    device_init_us: int
+    dispatch_min_us: int
+    dispatch_median_us: int
+
+
+def microbench_zmatrix_dispatch(n_segments: int, n_dispatches: int, device: int = 0) -> GpuMicrobench:
+    """microbench_zmatrix_dispatch (wgpu_device.rs:1087)."""
+    a, b, c = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_uint64()
+    st = lib().fnec_microbench_zmatrix_dispatch(device, n_segments, n_dispatches, ctypes.byref(a),
+                                                ctypes.byref(b), ctypes.byref(c))
+    if st != OK:
+        raise AccelError(st, "microbench_zmatrix_dispatch")
+    return GpuMicrobench(n_segments, n_dispatches, a.value, b.value, c.value)
+
+
+def enumerate_compute_adapters() -> list:
+    """enumerate_compute_adapters (wgpu_device.rs:24): CUDA device names."""
+    cnt = ctypes.c_int()
+    lib().fnec_enumerate_devices(ctypes.byref(cnt), -1, None, 0)
+    out = []
+    for i in range(cnt.value):
+        buf = ctypes.create_string_buffer(256)
+        lib().fnec_enumerate_devices(ctypes.byref(cnt), i, buf, 256)
+        out.append({"name": buf.value.decode(), "backend": "cuda", "device_type": "DiscreteGpu"})
+    return out
+
+
+def measure_fp64_peak(device: int = 0):
+    """(fused DFMA, separately rounded DMUL+DADD) TFLOP/s of this GPU."""
+    a, b = ctypes.c_double(), ctypes.c_double()
+    st = lib().fnec_measure_fp64_peak(device, ctypes.byref(a), ctypes.byref(b))
+    if st != OK:
+        raise AccelError(st, "measure_fp64_peak")
+    return a.value, b.value
+
+
+HYBRID_GPU_CANDIDATE = 0
+GPU_ONLY = 1
+
+
+def dispatch_frequency_point(request_kind: int, freq_hz: float) -> str:
+    """dispatch_frequency_point (lib.rs:92): "RunOnGpu" when a device exists."""
+    return "RunOnGpu" if lib().fnec_dispatch_frequency_point(int(request_kind), float(freq_hz)) == 1 \
+        else "NoDevice"
+
+
+# --------------------------------------------------------------------------
+# batched pipeline
+# --------------------------------------------------------------------------
+@dataclass
+class Antenna:
+    """One geometry: GW wires, voltage EX sources, ground, FR frequencies and
+    an optional RP card (n_theta, n_phi, theta0, phi0, d_theta, d_phi)."""
+
+    wires: np.ndarray
+    sources: np.ndarray
+    freqs_hz: Sequence[float]
+    ground: int = GROUND_FREE
+    rp: Optional[tuple] = None
+
+
+def wires_array(wires) -> np.ndarray:
+    """wires: iterable of (tag, segments, start3, end3, radius)."""
+    arr = np.zeros(len(wires), dtype=WIRE_DTYPE)
+    for i, (tag, nseg, s, e, r) in enumerate(wires):
+        arr[i] = (tag, nseg, s, e, r)
+    return arr
+
+
+def sources_array(sources) -> np.ndarray:
+    """sources: iterable of (tag, segment, complex voltage)."""
+    arr = np.zeros(len(sources), dtype=SOURCE_DTYPE)
+    for i, (tag, seg, v) in enumerate(sources):
+        arr[i] = (tag, seg, complex(v).real, complex(v).imag)
+    return arr
+
+
+@dataclass
+class BatchResult:
+    currents: list                 # per unit: complex128[N]
+    feeds: list                    # per unit: (n_feed, 7) array
+    pattern: list                  # per unit: (n_points, 6) array
+    status: np.ndarray             # per unit int32
+    total_radiated: np.ndarray
+    units: list = field(default_factory=list)
+
+
+class HallenBatch:
+    """A planned, device-resident batch of per-frequency Hallen solves."""
+
+    def __init__(self, antennas: Sequence[Antenna], precision: int = PRECISION_FP64,
+                 ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self._keep = []
+        arr = (_Antenna * len(antennas))()
+        for i, a in enumerate(antennas):
+            w = np.ascontiguousarray(a.wires, dtype=WIRE_DTYPE)
+            s = np.ascontiguousarray(a.sources, dtype=SOURCE_DTYPE)
+            f = np.ascontiguousarray(np.asarray(a.freqs_hz, np.float64))
+            rp = None
+            if a.rp is not None:
+                rp = _RpCard(*[int(a.rp[0]), int(a.rp[1])] + [float(v) for v in a.rp[2:6]])
+            self._keep += [w, s, f, rp]
+            arr[i] = _Antenna(_ptr(w), len(w), _ptr(s), len(s), int(a.ground), len(f), _ptr(f),
+                              ctypes.cast(ctypes.pointer(rp), _P) if rp is not None else None)
+        self._keep.append(arr)
+        h = ctypes.c_void_p()
+        self.ctx.check(lib().fnec_batch_create(self.ctx.handle, arr, len(antennas), int(precision),
+                                               ctypes.byref(h)), "batch_create")
+        self._h = h
+        _live_batches.add(self)
+        info = _BatchInfo()
+        lib().fnec_batch_get_info(self._h, ctypes.byref(info))
+        self.info = info
+        self.units = []
+        for u in range(info.n_units):
+            ui = _UnitInfo()
+            lib().fnec_batch_get_unit_info(self._h, u, ctypes.byref(ui))
+            self.units.append({k: getattr(ui, k) for k, _ in _UnitInfo._fields_})
+        # host result buffers, allocated once
+        self._cur = np.zeros(max(info.total_currents, 1), np.complex128)
+        self._feed = np.zeros((max(info.total_feeds, 1), 7), np.float64)
+        self._pat = np.zeros((max(info.total_points, 1), 6), np.float64)
+        self._status = np.zeros(max(info.n_units, 1), np.int32)
+        self._total = np.zeros(max(info.n_units, 1), np.float64)
+
+    def upload(self):
+        self.ctx.check(lib().fnec_batch_upload(self._h), "batch_upload")
+
+    def run(self):
+        self.ctx.check(lib().fnec_batch_run(self._h), "batch_run")
+
+    def sync(self):
+        self.ctx.check(lib().fnec_batch_sync(self._h), "batch_sync")
+
+    @property
+    def kernel_launches(self) -> int:
+        info = _BatchInfo()
+        lib().fnec_batch_get_info(self._h, ctypes.byref(info))
+        return int(info.kernel_launches)
+
+    @property
+    def h2d_bytes(self) -> int:
+        info = _BatchInfo()
+        lib().fnec_batch_get_info(self._h, ctypes.byref(info))
+        return int(info.h2d_bytes)
+
+    def read_raw(self, currents=True, feeds=True, pattern=True):
+        self.ctx.check(lib().fnec_batch_read(self._h, _ptr(self._cur) if currents else None,
+                                             _ptr(self._feed) if feeds else None,
+                                             _ptr(self._pat) if pattern else None, _ptr(self._status),
+                                             _ptr(self._total)), "batch_read")
+        return self._cur, self._feed, self._pat, self._status, self._total
+
+    def d2h_bytes(self, currents=True, feeds=True, pattern=True) -> int:
+        i = self.info
+        b = 4 * i.n_units + 8 * i.n_units
+        if currents:
+            b += 16 * sum(u["s"] for u in self.units)
+        if feeds:
+            b += 56 * i.total_feeds
+        if pattern:
+            b += 48 * i.total_points
+        return int(b)
+
+    def read(self) -> BatchResult:
+        cur, feed, pat, st, tot = self.read_raw()
+        res = BatchResult([], [], [], st[: len(self.units)].copy(), tot[: len(self.units)].copy(), self.units)
+        for u in self.units:
+            res.currents.append(cur[u["cur_off"]: u["cur_off"] + u["n"]].copy())
+            res.feeds.append(feed[u["feed_off"]: u["feed_off"] + u["n_feed"]].copy())
+            res.pattern.append(pat[u["pat_off"]: u["pat_off"] + u["n_points"]].copy())
+        return res
+
+    PHASES = ("expand", "rhs", "fill", "gram", "factor", "solve", "feed", "farfield")
+
+    def set_profiling(self, on: bool = True):
+        self.ctx.check(lib().fnec_batch_set_profiling(self._h, int(on)), "batch_set_profiling")
+
+    def phase_ms(self) -> dict:
+        ms = np.zeros(len(self.PHASES), np.float64)
+        self.ctx.check(lib().fnec_batch_phase_ms(self._h, _ptr(ms)), "batch_phase_ms")
+        return dict(zip(self.PHASES, ms.tolist()))
+
+    def read_unit(self, unit: int):
+        u = self.units[unit]
+        x = np.zeros(u["s"], np.complex128)
+        piv = np.zeros(u["s"], np.int32)
+        self.ctx.check(lib().fnec_batch_read_unit(self._h, unit, _ptr(x), _ptr(piv)), "batch_read_unit")
+        return x, piv
+
+    def read_z(self, unit: int) -> np.ndarray:
+        u = self.units[unit]
+        z = np.zeros((u["n"], u["n"]), np.complex128)
+        self.ctx.check(lib().fnec_batch_read_z(self._h, unit, _ptr(z)), "batch_read_z")
+        return z
+
+    def solve(self) -> BatchResult:
+        self.run()
+        self.sync()
+        return self.read()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fnec_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        if _shutting_down:
+            return
+        try:
+            self.close()
+        except Exception:
+            pass

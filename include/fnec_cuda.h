@@ -1,0 +1,287 @@
+/*
+ * fnec_cuda.h -- C ABI of libfnec_cuda.so, the B200 (sm_100a) backend for
+ * the Hallen method-of-moments hot path of dc0sk/fnec-rust.
+ *
+ * The library replaces the wgpu entry points of the reference's `nec_accel`
+ * crate (crates/nec_accel/src/lib.rs:52-96, wgpu_device.rs) and adds the
+ * batched / device-resident interface the CUDA path is built around.  All
+ * pointers are plain host pointers; sizes are element counts; complex
+ * numbers are interleaved (re, im) doubles.  Every function returns an int
+ * status (FNEC_OK == 0, negative on error); there is no CPU fallback: a
+ * call that cannot run on the GPU returns an error and does nothing else.
+ *
+ * Reference interfaces replaced (file:line within dc0sk/fnec-rust):
+ *   fnec_fill_zmatrix            <- fill_zmatrix_wgpu            crates/nec_accel/src/wgpu_device.rs:832
+ *   fnec_solve_hallen_resident   <- solve_hallen_gpu_resident    crates/nec_accel/src/wgpu_device.rs:1294
+ *   fnec_solve_hallen            <- solve_hallen                 crates/nec_solver/src/linear.rs:672
+ *   fnec_rp_farfield_batch       <- run_rp_farfield_batch_wgpu   crates/nec_accel/src/wgpu_device.rs:461
+ *   fnec_radiation_pattern       <- compute_radiation_pattern    crates/nec_solver/src/farfield.rs:563
+ *   fnec_integrate_radiated_power<- integrate_radiated_power     crates/nec_solver/src/farfield.rs:409
+ *   fnec_microbench_zmatrix_dispatch <- microbench_zmatrix_dispatch crates/nec_accel/src/wgpu_device.rs:1087
+ *   fnec_enumerate_devices       <- enumerate_compute_adapters   crates/nec_accel/src/wgpu_device.rs:24
+ *   fnec_dispatch_frequency_point<- dispatch_frequency_point     crates/nec_accel/src/lib.rs:92
+ *   fnec_batch_*                 <- the per-frequency loop of execute_frequency_sweep /
+ *                                   solve_frequency_point (apps/nec-cli/src/solve_session.rs:1186, :1782)
+ */
+#ifndef FNEC_CUDA_H
+#define FNEC_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------- */
+#define FNEC_OK 0
+#define FNEC_ERR_BAD_ARG (-1)          /* invalid argument / geometry      */
+#define FNEC_ERR_NO_DEVICE (-2)        /* no CUDA device / wrong arch      */
+#define FNEC_ERR_OUT_OF_MEMORY (-3)    /* device allocation failed         */
+#define FNEC_ERR_CUDA (-4)             /* CUDA runtime error               */
+#define FNEC_ERR_SINGULAR (-5)         /* pivot below 1e-30 (linear.rs:1354)*/
+#define FNEC_ERR_SEGMENT_NOT_FOUND (-6)/* EX card without its segment      */
+#define FNEC_ERR_UNSUPPORTED (-7)      /* feature not built                */
+#define FNEC_ERR_TIMEOUT (-8)          /* bounded device wait expired      */
+#define FNEC_ERR_BUSY (-9)             /* admission refused (HBM budget)   */
+
+#define FNEC_GROUND_FREE 0             /* GroundModel::FreeSpace           */
+#define FNEC_GROUND_PEC 1              /* GroundModel::PerfectConductor    */
+
+/* pipeline phases timed by fnec_batch_phase_ms (CUDA events on the
+ * context stream, recorded only while profiling is on) */
+#define FNEC_N_PHASES 8
+#define FNEC_PHASE_EXPAND 0   /* GW -> segments                 */
+#define FNEC_PHASE_RHS 1      /* Hallen RHS and cos(k s)        */
+#define FNEC_PHASE_FILL 2     /* Z fill                         */
+#define FNEC_PHASE_GRAM 3     /* normal equations M^H M + lambda */
+#define FNEC_PHASE_FACTOR 4   /* elimination / factorisation    */
+#define FNEC_PHASE_SOLVE 5    /* back substitution / refinement */
+#define FNEC_PHASE_FEED 6     /* feedpoint rows                 */
+#define FNEC_PHASE_FARFIELD 7 /* pattern grid + power integral  */
+
+#define FNEC_PRECISION_FP64 0          /* plain FP64, bit-exact operation order */
+#define FNEC_PRECISION_MIXED 1         /* FP32 factor + FP64 GMRES refinement   */
+
+/* ---- data records ----------------------------------------------------- */
+
+/* ZSegmentInput (wgpu_device.rs:811-816) */
+typedef struct {
+    double midpoint[3];
+    double direction[3];
+    double length;
+    double radius;
+} fnec_zsegment;
+
+/* GpuSegment (gpu_kernels.rs:52-59) */
+typedef struct {
+    double midpoint[3];
+    double direction[3];
+    double length;
+} fnec_gpu_segment;
+
+/* RpGpuResult (wgpu_device.rs:139-148).  axial_ratio is the Stokes axial
+ * ratio of farfield.rs:659-667 (the CPU path's definition). */
+typedef struct {
+    double u_theta;
+    double u_phi;
+    double gain_total_dbi;
+    double gain_theta_dbi;
+    double gain_phi_dbi;
+    double axial_ratio;
+    double theta_deg;
+    double phi_deg;
+} fnec_rp_result;
+
+/* One junction constraint I[seg_a] + sign * I[seg_b] = 0 (geometry.rs:255-262) */
+typedef struct {
+    uint64_t seg_a;
+    uint64_t seg_b;
+    double sign;
+} fnec_junction;
+
+/* One GW card (geometry.rs:710-754 expands it) */
+typedef struct {
+    uint32_t tag;
+    uint32_t segments;
+    double start[3];
+    double end[3];
+    double radius;
+} fnec_wire;
+
+/* One voltage-source EX card (types 0 and 5), in deck order */
+typedef struct {
+    uint32_t tag;
+    uint32_t segment;
+    double v_re;
+    double v_im;
+} fnec_source;
+
+/* One RP card (farfield.rs:677-699: phi outer, theta inner) */
+typedef struct {
+    uint32_t n_theta;
+    uint32_t n_phi;
+    double theta0;
+    double phi0;
+    double d_theta;
+    double d_phi;
+} fnec_rp_card;
+
+/* One antenna of a batch: its geometry, sources, ground, frequency list and
+ * optional pattern request.  Each frequency is one unit (one solve). */
+typedef struct {
+    const fnec_wire *wires;
+    uint32_t n_wires;
+    const fnec_source *sources;
+    uint32_t n_sources;
+    int32_t ground;
+    uint32_t n_freqs;
+    const double *freqs_hz;
+    const fnec_rp_card *rp; /* NULL: no pattern */
+} fnec_antenna;
+
+/* Per-unit shape, for sizing result buffers. */
+typedef struct {
+    uint32_t antenna;
+    uint32_t n;        /* segments (currents)            */
+    uint32_t s;        /* unknowns N + W                 */
+    uint32_t n_feed;   /* feedpoint rows                 */
+    uint32_t n_points; /* pattern points                 */
+    double freq_hz;
+    uint64_t cur_off;  /* offset (complex) into the currents array of fnec_batch_read */
+    uint64_t feed_off; /* offset (rows of 7 doubles) into the feed array           */
+    uint64_t pat_off;  /* offset (rows of 6 doubles) into the pattern array        */
+} fnec_unit_info;
+
+/* Batch totals. */
+typedef struct {
+    uint32_t n_units;
+    uint32_t max_s;
+    uint64_t total_currents; /* complex entries over all units */
+    uint64_t total_feeds;    /* feed rows                       */
+    uint64_t total_points;   /* pattern rows                    */
+    uint64_t device_bytes;   /* HBM held by the batch           */
+    uint64_t h2d_bytes;      /* input bytes copied by fnec_batch_upload */
+    uint64_t kernel_launches;/* launches issued by one fnec_batch_run  */
+} fnec_batch_info;
+
+typedef struct fnec_ctx fnec_ctx;
+typedef struct fnec_batch fnec_batch;
+
+/* ---- context ---------------------------------------------------------- */
+int fnec_ctx_create(int device, fnec_ctx **out);
+int fnec_ctx_destroy(fnec_ctx *ctx);
+/* Last error message of this context (static storage of the context). */
+const char *fnec_ctx_last_error(const fnec_ctx *ctx);
+/* The context's CUDA stream (cudaStream_t), for callers that order their
+ * own work against the library's. */
+void *fnec_ctx_stream(fnec_ctx *ctx);
+
+/* ---- reference nec_accel entry points ---------------------------------- */
+
+/* fill_zmatrix_wgpu: N x N Hallen matrix, row-major, interleaved complex128
+ * (2*n*n doubles).  Unlike the wgpu path the fill is FP64 and supports the
+ * PEC image (ground = FNEC_GROUND_PEC). */
+int fnec_fill_zmatrix(fnec_ctx *ctx, const fnec_zsegment *segments, uint64_t n, double freq_hz,
+                      int32_t ground, double *z_out);
+
+/* solve_hallen_gpu_resident: fill + normal equations + GEPP on the device.
+ * rhs: 2n doubles; cos_vec: n doubles; wire_endpoints: 2w uint64 (first,
+ * last); junctions: nj records.  x_out: 2(n + w') doubles, w' = max(w, 1)
+ * (linear.rs:691-696 falls back to one wire when w == 0).  pivots_out
+ * (optional, n + w' int32) receives the pivot row of each column. */
+int fnec_solve_hallen_resident(fnec_ctx *ctx, const fnec_zsegment *segments, uint64_t n,
+                               const double *rhs, const double *cos_vec,
+                               const uint64_t *wire_endpoints, uint64_t w,
+                               const fnec_junction *junctions, uint64_t nj, double freq_hz,
+                               int32_t ground, int32_t precision, double *x_out,
+                               int32_t *pivots_out);
+
+/* nec_solver::solve_hallen (linear.rs:672-797) on a caller-supplied Z
+ * (2*n*n doubles, row-major): regularised normal equations + GEPP on the
+ * device.  Arguments as fnec_solve_hallen_resident. */
+int fnec_solve_hallen(fnec_ctx *ctx, const double *z, uint64_t n, const double *rhs,
+                      const double *cos_vec, const uint64_t *wire_endpoints, uint64_t w,
+                      const fnec_junction *junctions, uint64_t nj, int32_t precision,
+                      double *x_out, int32_t *pivots_out);
+
+/* run_rp_farfield_batch_wgpu: pattern at explicit (theta, phi) points with
+ * a caller-supplied normalisation total_radiated (currents: 2n doubles,
+ * points: 2p doubles in degrees). */
+int fnec_rp_farfield_batch(fnec_ctx *ctx, const fnec_gpu_segment *segments, uint64_t n,
+                           const double *currents, double k, double total_radiated,
+                           const double *points, uint64_t p, fnec_rp_result *out);
+
+/* compute_radiation_pattern: the power integral is formed on the device.
+ * out: 4 doubles per point (gain_total, gain_theta, gain_phi, axial ratio);
+ * total_out (optional) receives the integral. */
+int fnec_radiation_pattern(fnec_ctx *ctx, const fnec_gpu_segment *segments, uint64_t n,
+                           const double *currents, double freq_hz, int32_t ground,
+                           const double *points, uint64_t p, double *out, double *total_out);
+
+/* integrate_radiated_power (pec_ground != 0: 91 x 360 upper hemisphere). */
+int fnec_integrate_radiated_power(fnec_ctx *ctx, const fnec_gpu_segment *segments, uint64_t n,
+                                  const double *currents, double freq_hz, int32_t pec_ground,
+                                  double *out);
+
+/* microbench_zmatrix_dispatch: device-init vs dispatch split (microseconds). */
+int fnec_microbench_zmatrix_dispatch(int device, uint64_t n_segments, uint32_t n_dispatches,
+                                     uint64_t *device_init_us, uint64_t *dispatch_min_us,
+                                     uint64_t *dispatch_median_us);
+
+/* enumerate_compute_adapters: number of CUDA devices and, for index `i`,
+ * its name into `name` (NUL-terminated, at most `cap` bytes). */
+int fnec_enumerate_devices(int *count, int index, char *name, uint64_t cap);
+
+/* dispatch_frequency_point: 1 = RunOnGpu (a device is present), 0 = none. */
+int fnec_dispatch_frequency_point(int request_kind, double freq_hz);
+
+/* FP64 pipe peaks of this GPU (no counterpart in the reference): fused
+ * DFMA and separately rounded DMUL+DADD throughput in TFLOP/s, used as the
+ * roofline denominators of the FP64-bound kernels. */
+int fnec_measure_fp64_peak(int device, double *fma_tflops, double *muladd_tflops);
+
+/* ---- batched, device-resident interface ------------------------------- */
+
+/* Plan a batch: host-side topology (endpoints, collinear merge, junctions,
+ * constraint rows, resolved sources, wire runs), device allocation and a
+ * first upload.  Units are ordered antenna-major, frequency-minor. */
+int fnec_batch_create(fnec_ctx *ctx, const fnec_antenna *antennas, uint32_t n_antennas,
+                      int32_t precision, fnec_batch **out);
+int fnec_batch_destroy(fnec_batch *b);
+int fnec_batch_get_info(const fnec_batch *b, fnec_batch_info *out);
+int fnec_batch_get_unit_info(const fnec_batch *b, uint32_t unit, fnec_unit_info *out);
+/* Re-copy the batch's host inputs (wires, tables, frequencies) to the
+ * device (the host->device half of an end-to-end step). */
+int fnec_batch_upload(fnec_batch *b);
+/* Enqueue the whole pipeline on the context stream: segment expansion,
+ * Hallen RHS, Z fill, Gram, factorisation, solve, feedpoints, pattern. */
+int fnec_batch_run(fnec_batch *b);
+/* Wait for the batch (and report per-unit failures as the first error). */
+int fnec_batch_sync(fnec_batch *b);
+/* Copy results to host arrays (any may be NULL):
+ *   currents: 2 * total_currents doubles (unit blocks at cur_off)
+ *   feeds:    7 * total_feeds doubles (seg, V re/im, I re/im, Zin re/im)
+ *   pattern:  6 * total_points doubles (gain_total, gain_theta, gain_phi,
+ *             axial_ratio, u_theta, u_phi)
+ *   status:   n_units int32 (0, or -(column+1) of a singular pivot)
+ *   total_radiated: n_units doubles */
+int fnec_batch_read(fnec_batch *b, double *currents, double *feeds, double *pattern,
+                    int32_t *status, double *total_radiated);
+/* Record CUDA events around each pipeline phase of later runs (on != 0). */
+int fnec_batch_set_profiling(fnec_batch *b, int on);
+/* Milliseconds of each phase of the last profiled run (FNEC_N_PHASES
+ * doubles); waits for that run to finish. */
+int fnec_batch_phase_ms(fnec_batch *b, double *ms);
+
+/* Per-unit solution vector x (currents then homogeneous constants), 2*s
+ * doubles, and the pivot rows (s int32), for parity checks. */
+int fnec_batch_read_unit(fnec_batch *b, uint32_t unit, double *x, int32_t *pivots);
+/* Z matrix (2*n*n doubles) and the augmented normal-equation matrix before
+ * elimination is not kept; the Z of a unit can be read after a run. */
+int fnec_batch_read_z(fnec_batch *b, uint32_t unit, double *z);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,55 @@
+"""CPU checks of the C ABI: the library loads without a GPU, exports every
+function include/fnec_cuda.h declares, the Python mirror binds exactly that
+set, and device entry points fail loudly (no CPU fallback) on a host with
+no CUDA device."""
+import ctypes
+import os
+import re
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "fnec_cuda.h")
+
+
+def header_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fnec_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declares_the_reference_entry_points():
+    names = header_functions()
+    for required in ("fnec_fill_zmatrix", "fnec_solve_hallen_resident", "fnec_solve_hallen",
+                     "fnec_rp_farfield_batch", "fnec_radiation_pattern", "fnec_integrate_radiated_power",
+                     "fnec_microbench_zmatrix_dispatch", "fnec_enumerate_devices",
+                     "fnec_dispatch_frequency_point", "fnec_batch_create", "fnec_batch_run"):
+        assert required in names
+
+
+def test_library_exports_every_declared_symbol():
+    import nec_accel
+
+    L = ctypes.CDLL(nec_accel.LIB_PATH)
+    missing = [n for n in header_functions() if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_python_mirror_binds_exactly_the_header():
+    import nec_accel
+
+    assert sorted(nec_accel.SIGNATURES) == header_functions()
+    nec_accel.lib()
+
+
+def test_no_device_is_an_error_not_a_fallback():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    import nec_accel
+
+    with pytest.raises(nec_accel.AccelError) as ei:
+        nec_accel.Context(0)
+    assert ei.value.code == nec_accel.ERR_NO_DEVICE
+    assert nec_accel.dispatch_frequency_point(nec_accel.GPU_ONLY, 14.2e6) == "NoDevice"
