@@ -38,6 +38,9 @@ ERR_SEGMENT_NOT_FOUND = -6
 ERR_UNSUPPORTED = -7
 ERR_TIMEOUT = -8
 ERR_BUSY = -9
+ERR_TOO_LARGE = -10
+NOALLOC_MAX_SEGMENTS = 4096
+NOALLOC_MAX_POINTS = 65536
 
 GROUND_FREE = 0
 GROUND_PEC = 1
@@ -110,6 +113,7 @@ SIGNATURES = {
     "fnec_enumerate_devices": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_char_p, _U64]),
     "fnec_dispatch_frequency_point": (ctypes.c_int, [ctypes.c_int, _D]),
     "fnec_measure_fp64_peak": (ctypes.c_int, [ctypes.c_int, _P, _P]),
+    "fnec_radiation_pattern_noalloc": (ctypes.c_int, [_P, _U64, _P, _D, _I32, _P, _U64, _P, _P, _P]),
     "fnec_batch_create": (ctypes.c_int, [_P, _P, _U32, _I32, _P]),
     "fnec_batch_destroy": (ctypes.c_int, [_P]),
     "fnec_batch_get_info": (ctypes.c_int, [_P, _P]),
@@ -327,6 +331,15 @@ def compute_radiation_pattern(segments, currents, freq_hz: float, points, ground
                                            int(ground), _ptr(pts), len(pts), _ptr(out), _ptr(tot)),
               "compute_radiation_pattern")
     return out, float(tot[0])
+
+
+def radiation_pattern_noalloc(d_segments: int, n: int, d_currents: int, freq_hz: float, ground: int,
+                              d_points: int, p: int, d_out: int, d_total: int = 0, stream: int = 0) -> int:
+    """The pattern on caller-owned DEVICE buffers with no device allocation
+    (for callers that cannot call cudaMalloc); returns the library status.
+    Pointers are integer device addresses; the caller synchronises."""
+    return lib().fnec_radiation_pattern_noalloc(d_segments, n, d_currents, float(freq_hz), int(ground),
+                                                d_points, p, d_out, d_total or None, stream or None)
 
 
 def integrate_radiated_power(segments, currents, freq_hz: float, pec_ground: bool,

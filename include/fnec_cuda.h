@@ -44,6 +44,7 @@ extern "C" {
 #define FNEC_ERR_UNSUPPORTED (-7)      /* feature not built                */
 #define FNEC_ERR_TIMEOUT (-8)          /* bounded device wait expired      */
 #define FNEC_ERR_BUSY (-9)             /* admission refused (HBM budget)   */
+#define FNEC_ERR_TOO_LARGE (-10)       /* beyond a fixed static maximum    */
 
 #define FNEC_GROUND_FREE 0             /* GroundModel::FreeSpace           */
 #define FNEC_GROUND_PEC 1              /* GroundModel::PerfectConductor    */
@@ -240,6 +241,32 @@ int fnec_dispatch_frequency_point(int request_kind, double freq_hz);
  * DFMA and separately rounded DMUL+DADD throughput in TFLOP/s, used as the
  * roofline denominators of the FP64-bound kernels. */
 int fnec_measure_fp64_peak(int device, double *fma_tflops, double *muladd_tflops);
+
+/* Radiation pattern that allocates no device memory.  No counterpart in
+ * the reference: it serves callers that cannot call cudaMalloc -- a host
+ * framework that owns all device memory through its own pool, a plugin held
+ * to a fixed memory budget, or a real-time loop that cannot take the
+ * implicit synchronisation of cudaMalloc/cudaFree.
+ * Same computation as fnec_radiation_pattern (compute_radiation_pattern
+ * semantics, power integral on the device), but every pointer is a DEVICE
+ * pointer owned by the caller: d_segments (n records), d_currents (2n
+ * doubles), d_points (2p doubles, degrees), d_out (4p doubles: gain_total,
+ * gain_theta, gain_phi, axial_ratio) and d_total (1 double, optional).  The
+ * work is enqueued on `stream` (a cudaStream_t; NULL = legacy default) of
+ * the current device; the caller synchronises.
+ * Scratch lives in a fixed static device array of about 5.6 MB held by
+ * every GPU that loads the library until exit.  The first call on each
+ * device looks its address up (cudaGetSymbolAddress); make that first call
+ * before any stream capture.  Calls that overlap on the GPU (other streams,
+ * other threads) race on the shared scratch and must be serialised.
+ * Limits: n <= FNEC_NOALLOC_MAX_SEGMENTS, p <= FNEC_NOALLOC_MAX_POINTS;
+ * larger sizes return FNEC_ERR_TOO_LARGE without touching the device. */
+#define FNEC_NOALLOC_MAX_SEGMENTS 4096
+#define FNEC_NOALLOC_MAX_POINTS 65536
+int fnec_radiation_pattern_noalloc(const fnec_gpu_segment *d_segments, uint64_t n,
+                                   const double *d_currents, double freq_hz, int32_t ground,
+                                   const double *d_points, uint64_t p, double *d_out,
+                                   double *d_total, void *stream);
 
 /* ---- batched, device-resident interface ------------------------------- */
 
