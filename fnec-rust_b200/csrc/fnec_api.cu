@@ -308,6 +308,7 @@ struct fnec_batch {
     std::vector<DevFeed> feeds;
     std::vector<DevConstraint> cons;
     std::vector<int32_t> codes;
+    std::vector<DevConRow> crows;
     std::vector<DevRun> runs;
     std::vector<DevRp> rps;
     std::vector<double> pts;
@@ -333,6 +334,7 @@ struct fnec_batch {
     DevSource *d_srcs = nullptr;
     DevFeed *d_feeds = nullptr;
     DevConstraint *d_cons = nullptr;
+    DevConRow *d_crows = nullptr;
     int32_t *d_codes = nullptr;
     DevRun *d_runs = nullptr;
     DevRp *d_rps = nullptr;
@@ -471,6 +473,16 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
             if (h.ja[t] == h.jb[t]) crow.push_back({{h.jb[t], h.js[t]}});
             else crow.push_back({{h.ja[t], 1.0}, {h.jb[t], h.js[t]}});
         }
+        a.crow_off = (int64_t)b->crows.size();
+        a.n_crow = (int32_t)crow.size();
+        for (auto &r : crow) {
+            DevConRow d{(int32_t)r[0].col, r.size() > 1 ? (int32_t)r[1].col : -1, r.size() > 1 ? r[1].val : 0.0};
+            if (r.size() == 1 && r[0].val != 1.0) {  // a junction row with seg_a == seg_b
+                d.c1 = d.c0;
+                d.v1 = r[0].val - 1.0;
+            }
+            b->crows.push_back(d);
+        }
         struct Contrib {
             int64_t i, j, row;
             int32_t code;
@@ -582,7 +594,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
            o_units = pk.add(b->units), o_ibuf = pk.add(b->ibuf), o_srcs = pk.add(b->srcs),
            o_feeds = pk.add(b->feeds), o_cons = pk.add(b->cons), o_codes = pk.add(b->codes),
            o_runs = pk.add(b->runs), o_rps = pk.add(b->rps), o_pts = pk.add(b->pts),
-           o_ft = pk.add(b->fill_tiles), o_gt = pk.add(b->gram_tiles), o_fro = pk.add(b->feed_row_off),
+           o_ft = pk.add(b->fill_tiles), o_crows = pk.add(b->crows), o_gt = pk.add(b->gram_tiles), o_fro = pk.add(b->feed_row_off),
            o_rhs = pk.add(b->rhs_given), o_cos = pk.add(b->cos_given), o_z = pk.add(b->z_given);
     b->in_bytes = pk.total > 0 ? pk.total : 256;
     e = cudaMallocHost((void **)&b->h_in, b->in_bytes);
@@ -602,6 +614,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
         b->d_rps = (DevRp *)(b->d_in + o_rps);
         b->d_pts = (double *)(b->d_in + o_pts);
         b->d_fill_tiles = (int4 *)(b->d_in + o_ft);
+        b->d_crows = (DevConRow *)(b->d_in + o_crows);
         b->d_gram_tiles = (int4 *)(b->d_in + o_gt);
         b->d_feed_row_off = (int64_t *)(b->d_in + o_fro);
         b->d_rhs_given = (double *)(b->d_in + o_rhs);
@@ -632,7 +645,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
                    64;
     if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_out, b->out_bytes);
     if (e == cudaSuccess && precision == FNEC_PRECISION_MIXED) {
-        e = alloc_mixed(b->mixed, b->units, b->max_s);
+        e = alloc_mixed(b->mixed, b->units, b->ants, b->max_s);
         b->dev_bytes += b->mixed.bytes;
     }
     if (e != cudaSuccess) {
@@ -851,8 +864,8 @@ int fnec_batch_run(fnec_batch *b) {
         MixedMarks mm{b->profile ? &b->ev[3] : nullptr};
         L += run_mixed(b->mixed, b->d_units, nu, b->units, b->d_ants, b->d_segs, b->d_fill_tiles,
                        (int)b->fill_tiles.size(), b->d_gram_tiles, (int)b->gram_tiles.size(), b->d_ibuf,
-                       b->d_cons, b->d_codes, b->d_z, b->d_rhs, b->d_cos, b->d_a, b->d_x, b->d_piv,
-                       b->d_status, b->max_s, b->z_given.empty(), mm, st);
+                       b->d_crows, b->d_z, b->d_rhs, b->d_cos, b->d_x, b->d_piv, b->d_status, b->max_s,
+                       b->z_given.empty(), mm, st);
     } else {
         if (b->z_given.empty()) {
             launch_fill_exact(b->d_units, b->d_ants, b->d_segs, b->d_fill_tiles, (int)b->fill_tiles.size(),
@@ -961,6 +974,14 @@ int fnec_batch_read_unit(fnec_batch *b, uint32_t unit, double *x, int32_t *pivot
         CUDA_TRY(ctx, cudaMemcpyAsync(pivots, b->d_piv + u.x_off, sizeof(int32_t) * u.s,
                                       cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    return FNEC_OK;
+}
+
+int fnec_batch_read_refinement(fnec_batch *b, int32_t *iters, double *resid) {
+    if (!b) return FNEC_ERR_BAD_ARG;
+    if (b->precision != FNEC_PRECISION_MIXED) return fail(b->ctx, FNEC_ERR_BAD_ARG, "not a mixed-precision batch");
+    cudaSetDevice(b->ctx->device);
+    CUDA_TRY(b->ctx, read_mixed_stats(b->mixed, iters, resid, b->ctx->stream));
     return FNEC_OK;
 }
 

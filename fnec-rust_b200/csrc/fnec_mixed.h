@@ -8,9 +8,27 @@
 
 namespace fnec {
 
+// Per-unit offsets into the mixed path's work buffers, and its refinement
+// statistics (written by the GMRES kernel).
+struct MixedUnit {
+    int64_t a32_off;  // complex64 S*S factor
+    int64_t v_off;    // complex128 Krylov basis
+    int64_t w_off;    // complex128 work vectors
+    int32_t rows;     // N + constraint rows
+    int32_t iters;    // GMRES iterations used
+    double resid;     // final preconditioned relative residual
+};
+
 struct MixedWork {
     size_t bytes = 0;
     void *base = nullptr;
+    MixedUnit *mu = nullptr;
+    float2 *a32 = nullptr;
+    cx *v = nullptr;
+    cx *w = nullptr;
+    int n_units = 0;
+    int max_s = 0;
+    std::vector<MixedUnit> host;
 };
 
 // Phase events the mixed path records after its fill, Gram, factor and
@@ -20,15 +38,16 @@ struct MixedMarks {
 };
 
 bool mixed_available();
-cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &units, int max_s);
+cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &units, const std::vector<AntDesc> &ants,
+                        int max_s);
 void free_mixed(MixedWork &w);
 // Enqueue fill + Gram + factor + refinement for all units; returns the
 // number of kernel launches issued.
 uint64_t run_mixed(MixedWork &w, const UnitDesc *d_units, int nu, const std::vector<UnitDesc> &units,
                    const AntDesc *d_ants, const DevSeg *d_segs, const int4 *fill_tiles, int n_fill,
-                   const int4 *gram_tiles, int n_gram, const int32_t *ibuf, const DevConstraint *cons,
-                   const int32_t *codes, cx *z, const cx *rhs, const double *cosv, cx *A, cx *x,
-                   int32_t *piv, int32_t *status, int max_s, bool do_fill, MixedMarks marks,
-                   cudaStream_t st);
+                   const int4 *gram_tiles, int n_gram, const int32_t *ibuf, const DevConRow *crows, cx *z,
+                   const cx *rhs, const double *cosv, cx *x, int32_t *piv, int32_t *status, int max_s,
+                   bool do_fill, MixedMarks marks, cudaStream_t st);
+cudaError_t read_mixed_stats(MixedWork &w, int32_t *iters, double *resid, cudaStream_t st);
 
 }  // namespace fnec

@@ -459,48 +459,131 @@ __global__ void __launch_bounds__(256) k_panel(const UnitDesc *__restrict__ unit
     }
 }
 
-// Deferred swaps and the U12 block row: one thread per trailing column K.
-__global__ void k_swap_u12(const UnitDesc *__restrict__ units, int c0, cx *abuf,
-                           const int32_t *__restrict__ piv_buf, const int32_t *__restrict__ status) {
+// The same panel factorisation with the panel (rows c0..s-1, NB columns)
+// held in shared memory for the whole kernel: identical operations on
+// identical values, without an L2 round trip in the sequential column loop.
+// Used when (s - c0) * NB * 16 bytes fits in PANEL_SMEM_MAX.
+constexpr int PANEL_SMEM_MAX = 200 * 1024;
+
+__global__ void __launch_bounds__(256) k_panel_smem(const UnitDesc *__restrict__ units, int c0, cx *abuf,
+                                                    int32_t *piv_buf, int32_t *status) {
+    extern __shared__ cx s_pan[];  // [m][NB], m = s - c0
+    __shared__ double s_v[8];
+    __shared__ int s_i[8];
+    __shared__ int s_p;
+    int ui = blockIdx.x;
+    UnitDesc u = units[ui];
+    int s = u.s;
+    if (c0 >= s || status[ui] != 0) return;
+    int w1 = s + 1;
+    cx *A = abuf + u.a_off;
+    int32_t *piv = piv_buf + u.x_off;
+    int nb = min(NB, s - c0);
+    int m = s - c0;
+    int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    for (int e = tid; e < m * nb; e += blockDim.x) {
+        int rr = e / nb, q = e % nb;
+        s_pan[rr * NB + q] = A[(int64_t)(c0 + rr) * w1 + c0 + q];
+    }
+    __syncthreads();
+    for (int c = c0; c < c0 + nb; ++c) {
+        int lc = c - c0;
+        double bv = -1.0;
+        int bi = -1;
+        for (int r = c + tid; r < s; r += blockDim.x) piv_better(bv, bi, cx_norm(s_pan[(r - c0) * NB + lc]), r);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            double ov = __shfl_down_sync(0xffffffffu, bv, o);
+            int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            piv_better(bv, bi, ov, oi);
+        }
+        if (lane == 0) {
+            s_v[wid] = bv;
+            s_i[wid] = bi;
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double v = s_v[0];
+            int p = s_i[0];
+            for (int q = 1; q < (int)(blockDim.x >> 5); ++q) piv_better(v, p, s_v[q], s_i[q]);
+            if (p < 0 || v < 1e-30) {
+                status[ui] = -(c + 1);
+                p = -1;
+            }
+            s_p = p;
+            piv[c] = p;
+        }
+        __syncthreads();
+        int p = s_p;
+        if (p < 0) return;
+        if (p != c && tid < nb) {
+            cx t0 = s_pan[lc * NB + tid];
+            s_pan[lc * NB + tid] = s_pan[(p - c0) * NB + tid];
+            s_pan[(p - c0) * NB + tid] = t0;
+        }
+        __syncthreads();
+        const cx *prow = s_pan + lc * NB;
+        cx diag = prow[lc];
+        for (int r = c + 1 + tid; r < s; r += blockDim.x) {
+            cx *row = s_pan + (r - c0) * NB;
+            cx f = cx_div(row[lc], diag);
+            row[lc] = f;
+            for (int k = lc + 1; k < nb; ++k) row[k] = cx_sub(row[k], cx_mul(f, prow[k]));
+        }
+        __syncthreads();
+    }
+    for (int e = tid; e < m * nb; e += blockDim.x) {
+        int rr = e / nb, q = e % nb;
+        A[(int64_t)(c0 + rr) * w1 + c0 + q] = s_pan[rr * NB + q];
+    }
+}
+
+// Deferred swaps and the U12 block row.  A CTA of 64 threads owns 64
+// trailing columns; their NB panel rows and the panel's L block are staged
+// in shared memory, the swaps are applied in pivot order (rows inside the
+// panel swap in shared memory, rows below it swap with global memory), and
+// row c0+q then receives the updates of panel columns c0..c0+q-1 in order.
+__global__ void __launch_bounds__(64) k_swap_u12(const UnitDesc *__restrict__ units, int c0, cx *abuf,
+                                                 const int32_t *__restrict__ piv_buf,
+                                                 const int32_t *__restrict__ status) {
+    __shared__ cx s_c[NB][64];
+    __shared__ cx s_L[NB][NB];  // read as broadcasts: no padding needed
     int ui = blockIdx.y;
     UnitDesc u = units[ui];
     int s = u.s;
     if (c0 >= s || status[ui] != 0) return;
     int nb = min(NB, s - c0);
-    int K = c0 + nb + blockIdx.x * blockDim.x + threadIdx.x;
-    if (K > s) return;  // column s is the right-hand side
     int w1 = s + 1;
     cx *A = abuf + u.a_off;
     const int32_t *piv = piv_buf + u.x_off;
-    cx col[NB];
-#pragma unroll
-    for (int q = 0; q < NB; ++q)
-        if (q < nb) col[q] = A[(int64_t)(c0 + q) * w1 + K];
-    for (int q = 0; q < nb; ++q) {
-        int p = piv[c0 + q];
-        if (p != c0 + q) {
-            // row p lies below the panel or inside it
+    int t = threadIdx.x;
+    int K = c0 + nb + blockIdx.x * 64 + t;  // column s is the right-hand side
+    if (c0 + nb + blockIdx.x * 64 > s) return;
+    bool live = K <= s;
+    for (int e = t; e < nb * nb; e += 64) s_L[e / nb][e % nb] = A[(int64_t)(c0 + e / nb) * w1 + c0 + e % nb];
+    for (int q = 0; q < nb; ++q) s_c[q][t] = live ? A[(int64_t)(c0 + q) * w1 + K] : cx_make(0.0, 0.0);
+    __syncthreads();
+    if (live) {
+        for (int q = 0; q < nb; ++q) {
+            int p = piv[c0 + q];
+            if (p == c0 + q) continue;
             if (p < c0 + nb) {
-                cx t0 = col[q];
-                col[q] = col[p - c0];
-                col[p - c0] = t0;
+                cx t0 = s_c[q][t];
+                s_c[q][t] = s_c[p - c0][t];
+                s_c[p - c0][t] = t0;
             } else {
-                cx t0 = col[q];
-                col[q] = A[(int64_t)p * w1 + K];
+                cx t0 = s_c[q][t];
+                s_c[q][t] = A[(int64_t)p * w1 + K];
                 A[(int64_t)p * w1 + K] = t0;
             }
         }
+        for (int q = 1; q < nb; ++q) {
+            cx v = s_c[q][t];
+            for (int c = 0; c < q; ++c) v = cx_sub(v, cx_mul(s_L[q][c], s_c[c][t]));
+            s_c[q][t] = v;
+        }
+        for (int q = 0; q < nb; ++q) A[(int64_t)(c0 + q) * w1 + K] = s_c[q][t];
     }
-    // U12: row c0+q receives the updates of panel columns c0 .. c0+q-1 in order
-    for (int q = 1; q < nb; ++q) {
-        const cx *lrow = A + (int64_t)(c0 + q) * w1 + c0;
-        cx v = col[q];
-        for (int c = 0; c < q; ++c) v = cx_sub(v, cx_mul(lrow[c], col[c]));
-        col[q] = v;
-    }
-#pragma unroll
-    for (int q = 0; q < NB; ++q)
-        if (q < nb) A[(int64_t)(c0 + q) * w1 + K] = col[q];
 }
 
 // A22 -= L21 * U12 with per-element in-order accumulation over the panel.
@@ -566,9 +649,11 @@ __global__ void __launch_bounds__(256) k_trailing(const UnitDesc *__restrict__ u
 }
 
 // Back substitution x_i = (b_i - sum_{j>i} a_ij x_j) / a_ii, j ascending.
-// One warp per unit: the 32 lanes form products a_ij x_j ahead of time and
-// lane 0 subtracts them in order (the subtraction chain is sequential in
-// the reference and stays sequential here).
+// One warp per unit.  The products a_ij x_j of a 32-wide chunk are formed
+// in parallel (one per lane, the next chunk's loads issued before the
+// current chunk is consumed); every lane then runs the same sequential
+// subtraction chain over the chunk through shuffles, so the order of the
+// subtractions -- and the result -- is the reference's.
 __global__ void k_backsub(const UnitDesc *__restrict__ units, const cx *__restrict__ abuf, cx *xbuf,
                           const int32_t *__restrict__ status) {
     extern __shared__ cx s_x[];
@@ -578,21 +663,28 @@ __global__ void k_backsub(const UnitDesc *__restrict__ units, const cx *__restri
     int s = u.s, w1 = s + 1;
     const cx *A = abuf + u.a_off;
     int lane = threadIdx.x;
-    __shared__ cx s_p[32];
     for (int i = s - 1; i >= 0; --i) {
         const cx *row = A + (int64_t)i * w1;
         cx sum = row[s];
+        int j = i + 1 + lane;
+        cx p = (j < s) ? cx_mul(row[j], s_x[j]) : cx_make(0.0, 0.0);
         for (int j0 = i + 1; j0 < s; j0 += 32) {
-            int j = j0 + lane;
-            if (j < s) s_p[lane] = cx_mul(row[j], s_x[j]);
-            __syncwarp();
-            if (lane == 0) {
-                int cnt = min(32, s - j0);
-                for (int q = 0; q < cnt; ++q) sum = cx_sub(sum, s_p[q]);
+            int jn = j0 + 32 + lane;
+            cx pn = (jn < s) ? cx_mul(row[jn], s_x[jn]) : cx_make(0.0, 0.0);
+            int cnt = min(32, s - j0);
+            double pr[32], pim[32];
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+                pr[q] = __shfl_sync(0xffffffffu, p.re, q);
+                pim[q] = __shfl_sync(0xffffffffu, p.im, q);
             }
-            __syncwarp();
+#pragma unroll
+            for (int q = 0; q < 32; ++q)
+                if (q < cnt) sum = cx_sub(sum, cx_make(pr[q], pim[q]));
+            p = pn;
         }
-        if (lane == 0) s_x[i] = cx_div(sum, row[i]);
+        cx xi = cx_div(sum, row[i]);
+        if (lane == 0) s_x[i] = xi;
         __syncwarp();
     }
     for (int i = lane; i < s; i += 32) xbuf[u.x_off + i] = s_x[i];
@@ -665,16 +757,21 @@ void launch_factor_exact(const UnitDesc *units, int nu, int max_s, int max_trail
     if (!attr) {
         cudaFuncSetAttribute(k_trailing, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)TRAILING_SMEM);
+        cudaFuncSetAttribute(k_panel_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, PANEL_SMEM_MAX);
         attr = true;
     }
     for (int c0 = 0; c0 < max_s; c0 += NB) {
-        k_panel<<<nu, 256, 0, st>>>(units, c0, A, piv, status);
+        size_t pan = sizeof(cx) * (size_t)(max_s - c0) * NB;
+        if (pan <= (size_t)PANEL_SMEM_MAX)
+            k_panel_smem<<<nu, 256, pan, st>>>(units, c0, A, piv, status);
+        else
+            k_panel<<<nu, 256, 0, st>>>(units, c0, A, piv, status);
         // columns right of the panel: at least the right-hand side column
         int rest = max_s + 1 - (c0 + NB);
         if (rest < 1) rest = 1;
         {
-            dim3 g1((rest + 127) / 128, nu);
-            k_swap_u12<<<g1, 128, 0, st>>>(units, c0, A, piv, status);
+            dim3 g1((rest + 63) / 64, nu);
+            k_swap_u12<<<g1, 64, 0, st>>>(units, c0, A, piv, status);
             int rows = max_s - (c0 + NB);
             if (rows > 0) {
                 int t = ((rows + 63) / 64) * ((rest + 63) / 64);

@@ -67,7 +67,15 @@ struct AntDesc {
     int32_t ground;      // 0 free space, 1 PEC image
     int64_t run_off;     // DevRun[n_run]
     int32_t n_run;
-    int32_t pad;
+    int32_t n_crow;      // constraint rows of M (free ends, then junctions)
+    int64_t crow_off;    // DevConRow[n_crow]
+};
+
+// One constraint row of M (linear.rs:744-762): M[N+q][c0] = 1 and, for a
+// junction row, M[N+q][c1] = v1 (c1 = -1 for a free-end I = 0 row).
+struct DevConRow {
+    int32_t c0, c1;
+    double v1;
 };
 
 struct DevSource {       // one resolved delta-gap source (excitation.rs:171-187)

@@ -126,6 +126,7 @@ SIGNATURES = {
     "fnec_batch_phase_ms": (ctypes.c_int, [_P, _P]),
     "fnec_batch_read_unit": (ctypes.c_int, [_P, _U32, _P, _P]),
     "fnec_batch_read_z": (ctypes.c_int, [_P, _U32, _P]),
+    "fnec_batch_read_refinement": (ctypes.c_int, [_P, _P, _P]),
 }
 
 _lib = None
@@ -551,6 +552,14 @@ class HallenBatch:
         piv = np.zeros(u["s"], np.int32)
         self.ctx.check(lib().fnec_batch_read_unit(self._h, unit, _ptr(x), _ptr(piv)), "batch_read_unit")
         return x, piv
+
+    def refinement_stats(self):
+        """(GMRES iterations, final preconditioned relative residual) per unit
+        of the last run of a mixed-precision batch."""
+        it = np.zeros(len(self.units), np.int32)
+        rs = np.zeros(len(self.units), np.float64)
+        self.ctx.check(lib().fnec_batch_read_refinement(self._h, _ptr(it), _ptr(rs)), "batch_read_refinement")
+        return it, rs
 
     def read_z(self, unit: int) -> np.ndarray:
         u = self.units[unit]

@@ -304,6 +304,9 @@ int fnec_batch_phase_ms(fnec_batch *b, double *ms);
 /* Per-unit solution vector x (currents then homogeneous constants), 2*s
  * doubles, and the pivot rows (s int32), for parity checks. */
 int fnec_batch_read_unit(fnec_batch *b, uint32_t unit, double *x, int32_t *pivots);
+/* Mixed-precision batches: per-unit GMRES iterations (n_units int32) and
+ * final preconditioned relative residual (n_units doubles) of the last run. */
+int fnec_batch_read_refinement(fnec_batch *b, int32_t *iters, double *resid);
 /* Z matrix (2*n*n doubles) and the augmented normal-equation matrix before
  * elimination is not kept; the Z of a unit can be read after a run. */
 int fnec_batch_read_z(fnec_batch *b, uint32_t unit, double *z);

@@ -259,3 +259,17 @@ def test_reference_entry_points(acc):
     assert mb.dispatch_median_us > 0
     assert acc.enumerate_compute_adapters()[0]["name"]
     assert acc.dispatch_frequency_point(acc.GPU_ONLY, f) == "RunOnGpu"
+
+
+def test_uneven_random_antenna_batch_sample(acc):
+    """64 antennas of the uneven 4096-antenna workload generator in one
+    batch (N from tens to hundreds, free space and GN 1 mixed)."""
+    import bench
+
+    wl = bench.uneven_workload(64, seed=7)
+    ants = [acc.Antenna(acc.wires_array(w), acc.sources_array(s), [f], g, None) for w, s, g, f in wl]
+    batch = acc.HallenBatch(ants)
+    res = batch.solve()
+    for u in range(0, 64, 7):
+        w, s, g, f = wl[u]
+        _check_unit(acc, batch, res, u, O.wires_array(w), O.sources_array(s), g, f, None)
