@@ -109,8 +109,8 @@ struct HostAnt {
     std::vector<int32_t> comp;      // 2n merged component (first, last) per segment
     std::vector<int64_t> ja, jb;    // junction rows
     std::vector<double> js;
-    std::vector<DevSource> srcs;
-    std::vector<DevFeed> feeds;
+    std::vector<std::vector<DevSource>> rhs_srcs;  // sources of each right-hand side
+    std::vector<std::vector<DevFeed>> rhs_feeds;   // feed rows of each right-hand side
     std::vector<DevRun> runs;
     DevRp rp{};
     std::vector<double> pts;        // explicit points (theta, phi)
@@ -235,19 +235,13 @@ static void build_runs(HostAnt &h) {
     }
 }
 
-// excitation.rs:119-187 source resolution and :78-90 / solve_session.rs:846-917 feed rows.
-static int resolve_sources(HostAnt &h, const fnec_source *src, uint32_t ns, std::string &why) {
+// excitation.rs:119-187 source resolution and :78-90 / solve_session.rs:846-917
+// feed rows.  With separate == false the EX cards superpose into one
+// right-hand side (a deck); with separate == true every card is its own
+// right-hand side, solved as the single-source deck it stands for.
+static void superposed_rhs(HostAnt &h, const std::vector<int64_t> &idx, const fnec_source *src, uint32_t ns,
+                           std::vector<DevSource> &out_src, std::vector<DevFeed> &out_feed) {
     const auto &s = h.segs;
-    if (ns == 0) return FNEC_OK;
-    std::vector<int64_t> idx(ns);
-    for (uint32_t e = 0; e < ns; ++e) {
-        idx[e] = find_seg(s, src[e].tag, src[e].segment);
-        if (idx[e] < 0) {
-            why = "EX: no segment with tag " + std::to_string(src[e].tag) + ", index " +
-                  std::to_string(src[e].segment);
-            return FNEC_ERR_SEGMENT_NOT_FOUND;
-        }
-    }
     uint32_t driven = s[idx[0]].tag;
     std::map<uint32_t, std::pair<int64_t, std::pair<double, double>>> by_tag;
     by_tag[driven] = {idx[0], {src[0].v_re, src[0].v_im}};
@@ -262,9 +256,9 @@ static int resolve_sources(HostAnt &h, const fnec_source *src, uint32_t ns, std:
         d.comp_last = h.comp[2 * d.feed + 1];
         d.v_re = kv.second.second.first;
         d.v_im = kv.second.second.second;
-        h.srcs.push_back(d);
+        out_src.push_back(d);
     }
-    // feed rows: v_vec[idx] accumulates V/dl of every card on that segment
+    // v_vec[idx] accumulates V/dl of every card on that segment
     for (uint32_t e = 0; e < ns; ++e) {
         DevFeed f{};
         f.seg = (int32_t)idx[e];
@@ -277,7 +271,32 @@ static int resolve_sources(HostAnt &h, const fnec_source *src, uint32_t ns, std:
         }
         f.vdl_re = re;
         f.vdl_im = im;
-        h.feeds.push_back(f);
+        out_feed.push_back(f);
+    }
+}
+
+static int resolve_sources(HostAnt &h, const fnec_source *src, uint32_t ns, bool separate, std::string &why) {
+    const auto &s = h.segs;
+    std::vector<int64_t> idx(ns);
+    for (uint32_t e = 0; e < ns; ++e) {
+        idx[e] = find_seg(s, src[e].tag, src[e].segment);
+        if (idx[e] < 0) {
+            why = "EX: no segment with tag " + std::to_string(src[e].tag) + ", index " +
+                  std::to_string(src[e].segment);
+            return FNEC_ERR_SEGMENT_NOT_FOUND;
+        }
+    }
+    if (ns == 0 || !separate) {
+        h.rhs_srcs.assign(1, {});
+        h.rhs_feeds.assign(1, {});
+        if (ns > 0) superposed_rhs(h, idx, src, ns, h.rhs_srcs[0], h.rhs_feeds[0]);
+        return FNEC_OK;
+    }
+    h.rhs_srcs.assign(ns, {});
+    h.rhs_feeds.assign(ns, {});
+    for (uint32_t e = 0; e < ns; ++e) {
+        std::vector<int64_t> one = {idx[e]};
+        superposed_rhs(h, one, &src[e], 1, h.rhs_srcs[e], h.rhs_feeds[e]);
     }
     return FNEC_OK;
 }
@@ -302,7 +321,8 @@ struct fnec_batch {
     std::vector<DevSeg> segs;  // uploaded when the batch has no wires
     bool from_wires = true;
     std::vector<AntDesc> ants;
-    std::vector<UnitDesc> units;
+    std::vector<UnitDesc> units;   // systems (one factorisation each)
+    std::vector<UnitDesc> solves;  // right-hand sides
     std::vector<int32_t> ibuf;
     std::vector<DevSource> srcs;
     std::vector<DevFeed> feeds;
@@ -320,7 +340,9 @@ struct fnec_batch {
     std::vector<double> z_given;  // caller-supplied Z for every unit (fill skipped)
     std::vector<fnec_unit_info> uinfo;
     int max_s = 0, max_n = 0;
-    int64_t tot_seg = 0, z_el = 0, a_el = 0, x_el = 0, rhs_el = 0, pat_el = 0, feed_rows = 0;
+    int64_t tot_seg = 0, z_el = 0, a_el = 0, x_el = 0, rhs_el = 0, pat_el = 0, feed_rows = 0, cos_el = 0,
+            piv_el = 0;
+    int max_rhs = 1;
     int ff_blocks = 0;
     size_t ff_smem = 0;
     uint64_t launches = 0;
@@ -330,6 +352,7 @@ struct fnec_batch {
     DevSeg *d_segs = nullptr;
     AntDesc *d_ants = nullptr;
     UnitDesc *d_units = nullptr;
+    UnitDesc *d_solves = nullptr;
     int32_t *d_ibuf = nullptr;
     DevSource *d_srcs = nullptr;
     DevFeed *d_feeds = nullptr;
@@ -507,13 +530,32 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
             q = e;
         }
         a.n_con = (int32_t)(b->cons.size() - a.con_off);
-        // sources, feeds, runs, rp
+        // sources and feed rows, grouped by right-hand side (CSR in ibuf)
+        if (h.rhs_srcs.empty()) {
+            h.rhs_srcs.assign(1, {});
+            h.rhs_feeds.assign(1, {});
+        }
+        a.n_rhs = (int32_t)h.rhs_srcs.size();
         a.src_off = (int64_t)b->srcs.size();
-        a.n_src = (int32_t)h.srcs.size();
-        b->srcs.insert(b->srcs.end(), h.srcs.begin(), h.srcs.end());
         a.feed_off = (int64_t)b->feeds.size();
-        a.n_feed = (int32_t)h.feeds.size();
-        b->feeds.insert(b->feeds.end(), h.feeds.begin(), h.feeds.end());
+        a.sptr_off = (int64_t)b->ibuf.size();
+        int32_t cnt = 0;
+        b->ibuf.push_back(0);
+        for (auto &v : h.rhs_srcs) {
+            b->srcs.insert(b->srcs.end(), v.begin(), v.end());
+            cnt += (int32_t)v.size();
+            b->ibuf.push_back(cnt);
+        }
+        a.n_src = cnt;
+        a.fptr_off = (int64_t)b->ibuf.size();
+        cnt = 0;
+        b->ibuf.push_back(0);
+        for (auto &v : h.rhs_feeds) {
+            b->feeds.insert(b->feeds.end(), v.begin(), v.end());
+            cnt += (int32_t)v.size();
+            b->ibuf.push_back(cnt);
+        }
+        a.n_feed = cnt;
         a.run_off = (int64_t)b->runs.size();
         a.n_run = (int32_t)h.runs.size();
         b->runs.insert(b->runs.end(), h.runs.begin(), h.runs.end());
@@ -530,7 +572,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
         ff_int_max = std::max(ff_int_max, n_int);
         smem_max = std::max(smem_max, sizeof(DevRun) * h.runs.size() + sizeof(cx) * (size_t)n);
         b->ants.push_back(a);
-        // units
+        // systems (one per frequency) and their solves (one per right-hand side)
         int s = n + a.w;
         for (size_t fi = 0; fi < h.freqs.size(); ++fi) {
             double f = h.freqs[fi];
@@ -538,38 +580,60 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
             u.ant = (int32_t)ai;
             u.n = n;
             u.s = s;
+            u.rhs = 0;
             u.freq = f;
             u.k_fill = 2.0 * PI * f / C0;
             u.k_rp = 2.0 * PI / (C0 / f);
             u.z_off = b->z_el;
             u.a_off = b->a_el;
-            u.x_off = b->x_el;
-            u.rhs_off = b->rhs_el;
-            u.pat_off = b->pat_el;
+            u.cos_off = b->cos_el;
+            u.piv_off = b->piv_el;
+            u.n_rhs = a.n_rhs;
+            u.sys = (int32_t)b->units.size();
             if (need_solve) {
                 b->z_el += (int64_t)n * n;
                 b->a_el += (int64_t)s * (s + 1);
             }
-            b->x_el += s;
-            b->rhs_el += n;
-            b->pat_el += n_req;
-            fnec_unit_info ui{};
-            ui.antenna = (uint32_t)ai;
-            ui.n = (uint32_t)n;
-            ui.s = (uint32_t)s;
-            ui.n_feed = (uint32_t)a.n_feed;
-            ui.n_points = (uint32_t)n_req;
-            ui.freq_hz = f;
-            ui.pat_off = (uint64_t)u.pat_off;
-            ui.feed_off = (uint64_t)b->feed_rows;
-            ui.cur_off = b->uinfo.empty() ? 0 : b->uinfo.back().cur_off + b->uinfo.back().n;
-            b->feed_row_off.push_back(b->feed_rows);
-            b->feed_rows += a.n_feed;
-            b->uinfo.push_back(ui);
-            b->units.push_back(u);
+            b->cos_el += n;
+            b->piv_el += s;
             b->max_s = std::max(b->max_s, s);
             b->max_n = std::max(b->max_n, n);
-            int32_t uidx = (int32_t)(b->units.size() - 1);
+            b->max_rhs = std::max(b->max_rhs, (int)a.n_rhs);
+            int32_t uidx = u.sys;
+            const int32_t *fptr = &b->ibuf[a.fptr_off];
+            for (int r = 0; r < a.n_rhs; ++r) {
+                UnitDesc v = u;
+                v.rhs = r;
+                v.x_off = b->x_el;
+                v.rhs_off = b->rhs_el;
+                v.pat_off = b->pat_el;
+                if (r == 0) {  // the system points at its first right-hand side
+                    u.x_off = v.x_off;
+                    u.rhs_off = v.rhs_off;
+                    u.pat_off = v.pat_off;
+                }
+                b->x_el += s;
+                b->rhs_el += n;
+                b->pat_el += n_req;
+                int nf = fptr[r + 1] - fptr[r];
+                fnec_unit_info ui{};
+                ui.antenna = (uint32_t)ai;
+                ui.n = (uint32_t)n;
+                ui.s = (uint32_t)s;
+                ui.n_feed = (uint32_t)nf;
+                ui.n_points = (uint32_t)n_req;
+                ui.freq_hz = f;
+                ui.pat_off = (uint64_t)v.pat_off;
+                ui.feed_off = (uint64_t)b->feed_rows;
+                ui.cur_off = b->uinfo.empty() ? 0 : b->uinfo.back().cur_off + b->uinfo.back().n;
+                ui.rhs = (uint32_t)r;
+                ui.system = (uint32_t)uidx;
+                b->feed_row_off.push_back(b->feed_rows);
+                b->feed_rows += nf;
+                b->uinfo.push_back(ui);
+                b->solves.push_back(v);
+            }
+            b->units.push_back(u);
             if (need_solve) {
                 for (int i0 = 0; i0 < n; i0 += 16)
                     for (int j0 = 0; j0 < n; j0 += 16) b->fill_tiles.push_back(make_int4(uidx, i0, j0, 0));
@@ -591,7 +655,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
     cudaError_t e = cudaSuccess;
     Packer pk;
     size_t o_wires = pk.add(b->wires), o_segs = pk.add(b->segs), o_ants = pk.add(b->ants),
-           o_units = pk.add(b->units), o_ibuf = pk.add(b->ibuf), o_srcs = pk.add(b->srcs),
+           o_units = pk.add(b->units), o_solves = pk.add(b->solves), o_ibuf = pk.add(b->ibuf), o_srcs = pk.add(b->srcs),
            o_feeds = pk.add(b->feeds), o_cons = pk.add(b->cons), o_codes = pk.add(b->codes),
            o_runs = pk.add(b->runs), o_rps = pk.add(b->rps), o_pts = pk.add(b->pts),
            o_ft = pk.add(b->fill_tiles), o_crows = pk.add(b->crows), o_gt = pk.add(b->gram_tiles), o_fro = pk.add(b->feed_row_off),
@@ -605,6 +669,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
         b->d_wires = (DevWire *)(b->d_in + o_wires);
         b->d_ants = (AntDesc *)(b->d_in + o_ants);
         b->d_units = (UnitDesc *)(b->d_in + o_units);
+        b->d_solves = (UnitDesc *)(b->d_in + o_solves);
         b->d_ibuf = (int32_t *)(b->d_in + o_ibuf);
         b->d_srcs = (DevSource *)(b->d_in + o_srcs);
         b->d_feeds = (DevFeed *)(b->d_in + o_feeds);
@@ -631,21 +696,21 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
     DA(d_a, b->a_el);
     DA(d_x, b->x_el);
     DA(d_rhs, b->rhs_el);
-    DA(d_cos, b->rhs_el);
-    DA(d_piv, b->x_el);
+    DA(d_cos, b->cos_el);
+    DA(d_piv, b->piv_el);
     DA(d_status, nu);
     DA(d_feed_out, 7 * b->feed_rows);
     DA(d_fld, 4 * b->pat_el);
-    DA(d_partials, (int64_t)b->ff_blocks * nu);
+    DA(d_partials, (int64_t)b->ff_blocks * (int64_t)b->solves.size());
     DA(d_pat, PAT_STRIDE * b->pat_el);
-    DA(d_total, nu);
+    DA(d_total, b->solves.size());
 #undef DA
     b->out_bytes = sizeof(cx) * (size_t)b->x_el + sizeof(double) * 7 * (size_t)b->feed_rows +
-                   sizeof(double) * PAT_STRIDE * (size_t)b->pat_el + (sizeof(int32_t) + sizeof(double)) * (size_t)nu +
-                   64;
+                   sizeof(double) * PAT_STRIDE * (size_t)b->pat_el +
+                   (sizeof(int32_t) + sizeof(double)) * (size_t)(nu + b->solves.size()) + 64;
     if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_out, b->out_bytes);
     if (e == cudaSuccess && precision == FNEC_PRECISION_MIXED) {
-        e = alloc_mixed(b->mixed, b->units, b->ants, b->max_s);
+        e = alloc_mixed(b->mixed, b->units, b->solves, b->ants, b->max_s);
         b->dev_bytes += b->mixed.bytes;
     }
     if (e != cudaSuccess) {
@@ -710,7 +775,7 @@ static int antenna_from_cards(const fnec_antenna &A, HostAnt &h, std::string &wh
     h.ep = merged;
     set_comp(h, merged);
     cli_junctions(h.segs, merged, h);
-    int st = resolve_sources(h, A.sources, A.n_sources, why);
+    int st = resolve_sources(h, A.sources, A.n_sources, A.separate_sources != 0, why);
     if (st != FNEC_OK) return st;
     build_runs(h);
     h.rp.pts_off = -1;
@@ -797,7 +862,8 @@ int fnec_batch_destroy(fnec_batch *b) {
 
 int fnec_batch_get_info(const fnec_batch *b, fnec_batch_info *out) {
     if (!b || !out) return FNEC_ERR_BAD_ARG;
-    out->n_units = (uint32_t)b->units.size();
+    out->n_units = (uint32_t)b->solves.size();
+    out->n_systems = (uint32_t)b->units.size();
     out->max_s = (uint32_t)b->max_s;
     out->total_currents = b->uinfo.empty() ? 0 : b->uinfo.back().cur_off + b->uinfo.back().n;
     out->total_feeds = (uint64_t)b->feed_rows;
@@ -839,13 +905,14 @@ int fnec_batch_run(fnec_batch *b) {
     cudaSetDevice(ctx->device);
     cudaStream_t st = ctx->stream;
     int nu = (int)b->units.size();
+    int ns = (int)b->solves.size();
     uint64_t L = 0;
     if (nu == 0) return FNEC_OK;
     auto mark = [&](int k) {
         if (b->profile) cudaEventRecord(b->ev[k], st);
     };
     CUDA_TRY(ctx, cudaMemsetAsync(b->d_status, 0, sizeof(int32_t) * nu, st));
-    CUDA_TRY(ctx, cudaMemsetAsync(b->d_total, 0, sizeof(double) * nu, st));
+    CUDA_TRY(ctx, cudaMemsetAsync(b->d_total, 0, sizeof(double) * ns, st));
     mark(0);
     if (b->from_wires) {
         launch_expand_segments(b->d_wires, (int)b->wires.size(), b->d_segs, st);
@@ -855,14 +922,14 @@ int fnec_batch_run(fnec_batch *b) {
     if (!b->rhs_given_flag) {
         const double MU0 = 4.0 * PI * 1e-7;
         const double ETA0 = MU0 * C0;
-        launch_hallen_rhs(b->d_units, nu, b->d_ants, b->d_segs, b->d_ibuf, b->d_srcs, b->d_rhs, b->d_cos,
+        launch_hallen_rhs(b->d_solves, ns, b->d_ants, b->d_segs, b->d_ibuf, b->d_srcs, b->d_rhs, b->d_cos,
                           2.0 * PI / ETA0, st);
         ++L;
     }
     mark(2);
     if (b->precision == FNEC_PRECISION_MIXED) {
         MixedMarks mm{b->profile ? &b->ev[3] : nullptr};
-        L += run_mixed(b->mixed, b->d_units, nu, b->units, b->d_ants, b->d_segs, b->d_fill_tiles,
+        L += run_mixed(b->mixed, b->d_units, nu, b->d_solves, ns, b->d_ants, b->d_segs, b->d_fill_tiles,
                        (int)b->fill_tiles.size(), b->d_gram_tiles, (int)b->gram_tiles.size(), b->d_ibuf,
                        b->d_crows, b->d_z, b->d_rhs, b->d_cos, b->d_x, b->d_piv, b->d_status, b->max_s,
                        b->z_given.empty(), mm, st);
@@ -879,16 +946,21 @@ int fnec_batch_run(fnec_batch *b) {
         launch_factor_exact(b->d_units, nu, b->max_s, 0, b->d_a, b->d_piv, b->d_status, st);
         mark(5);
         launch_backsub(b->d_units, nu, b->max_s, b->d_a, b->d_x, b->d_status, st);
+        if (b->max_rhs > 1) {
+            launch_extra_rhs_exact(b->d_solves, ns, b->max_s, b->d_ants, b->d_ibuf, b->d_z, b->d_rhs, b->d_cos,
+                                   b->d_a, b->d_piv, b->d_x, b->d_status, st);
+            L += 2;
+        }
         mark(6);
         int panels = (b->max_s + 31) / 32;
         L += 3 + 1 + 3 * panels;
     }
-    launch_feedpoints(b->d_units, nu, b->d_ants, b->d_segs, b->d_feeds, b->d_x, b->d_status, b->d_feed_out,
-                      b->d_feed_row_off, st);
+    launch_feedpoints(b->d_solves, ns, b->d_ants, b->d_segs, b->d_ibuf, b->d_feeds, b->d_x, b->d_status,
+                      b->d_feed_out, b->d_feed_row_off, st);
     ++L;
     mark(7);
     if (b->ff_blocks > 0) {
-        launch_farfield(b->d_units, nu, b->d_ants, b->d_runs, b->d_rps, b->d_pts, b->d_x, b->d_status, b->d_fld,
+        launch_farfield(b->d_solves, ns, b->d_ants, b->d_runs, b->d_rps, b->d_pts, b->d_x, b->d_status, b->d_fld,
                         b->d_partials, b->ff_blocks, b->ff_smem, b->d_pat, b->d_total, st);
         L += 2;
     }
@@ -935,7 +1007,7 @@ int fnec_batch_read(fnec_batch *b, double *currents, double *feeds, double *patt
     fnec_ctx *ctx = b->ctx;
     cudaSetDevice(ctx->device);
     cudaStream_t st = ctx->stream;
-    int nu = (int)b->units.size();
+    int nu = (int)b->units.size(), ns = (int)b->solves.size();
     // device -> pinned staging -> caller arrays
     unsigned char *hx = b->h_out;
     unsigned char *hf = hx + sizeof(cx) * (size_t)b->x_el;
@@ -948,30 +1020,34 @@ int fnec_batch_read(fnec_batch *b, double *currents, double *feeds, double *patt
     if (pattern && pb) CUDA_TRY(ctx, cudaMemcpyAsync(hp, b->d_pat, pb, cudaMemcpyDeviceToHost, st));
     if (status) CUDA_TRY(ctx, cudaMemcpyAsync(hs, b->d_status, sizeof(int32_t) * nu, cudaMemcpyDeviceToHost, st));
     if (total_radiated)
-        CUDA_TRY(ctx, cudaMemcpyAsync(ht, b->d_total, sizeof(double) * nu, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(ctx, cudaMemcpyAsync(ht, b->d_total, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(ctx, cudaStreamSynchronize(st));
     if (currents) {
         const cx *x = (const cx *)hx;
-        for (int u = 0; u < nu; ++u)
-            std::memcpy(currents + 2 * b->uinfo[u].cur_off, &x[b->units[u].x_off], sizeof(cx) * b->units[u].n);
+        for (int u = 0; u < ns; ++u)
+            std::memcpy(currents + 2 * b->uinfo[u].cur_off, &x[b->solves[u].x_off], sizeof(cx) * b->solves[u].n);
     }
     if (feeds && fb) std::memcpy(feeds, hf, fb);
     if (pattern && pb) std::memcpy(pattern, hp, pb);
-    if (status) std::memcpy(status, hs, sizeof(int32_t) * nu);
-    if (total_radiated) std::memcpy(total_radiated, ht, sizeof(double) * nu);
+    if (status) {  // per solve: the status of its system
+        const int32_t *sst = (const int32_t *)hs;
+        std::vector<int32_t> tmp(sst, sst + nu);
+        for (int u = 0; u < ns; ++u) status[u] = tmp[b->solves[u].sys];
+    }
+    if (total_radiated) std::memcpy(total_radiated, ht, sizeof(double) * ns);
     return FNEC_OK;
 }
 
 int fnec_batch_read_unit(fnec_batch *b, uint32_t unit, double *x, int32_t *pivots) {
-    if (!b || unit >= b->units.size()) return FNEC_ERR_BAD_ARG;
+    if (!b || unit >= b->solves.size()) return FNEC_ERR_BAD_ARG;
     fnec_ctx *ctx = b->ctx;
     cudaSetDevice(ctx->device);
-    const UnitDesc &u = b->units[unit];
+    const UnitDesc &u = b->solves[unit];
     if (x)
         CUDA_TRY(ctx, cudaMemcpyAsync(x, b->d_x + u.x_off, sizeof(cx) * u.s, cudaMemcpyDeviceToHost,
                                       ctx->stream));
     if (pivots)
-        CUDA_TRY(ctx, cudaMemcpyAsync(pivots, b->d_piv + u.x_off, sizeof(int32_t) * u.s,
+        CUDA_TRY(ctx, cudaMemcpyAsync(pivots, b->d_piv + u.piv_off, sizeof(int32_t) * u.s,
                                       cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return FNEC_OK;
@@ -986,10 +1062,10 @@ int fnec_batch_read_refinement(fnec_batch *b, int32_t *iters, double *resid) {
 }
 
 int fnec_batch_read_z(fnec_batch *b, uint32_t unit, double *z) {
-    if (!b || !z || unit >= b->units.size()) return FNEC_ERR_BAD_ARG;
+    if (!b || !z || unit >= b->solves.size()) return FNEC_ERR_BAD_ARG;
     fnec_ctx *ctx = b->ctx;
     cudaSetDevice(ctx->device);
-    const UnitDesc &u = b->units[unit];
+    const UnitDesc &u = b->units[b->solves[unit].sys];
     CUDA_TRY(ctx, cudaMemcpyAsync(z, b->d_z + u.z_off, sizeof(cx) * (size_t)u.n * u.n,
                                   cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
@@ -1152,15 +1228,18 @@ static int pattern_common(fnec_ctx *ctx, const fnec_gpu_segment *segments, uint6
     int st = build_batch(ctx, hs, FNEC_PRECISION_FP64, &b, false);
     if (st != FNEC_OK) return st;
     b->units[0].k_rp = k_rp;
+    b->solves[0].k_rp = k_rp;
     cudaStream_t s = ctx->stream;
     cudaStreamSynchronize(s);
     cudaError_t e = cudaMemcpyAsync(b->d_units, b->units.data(), sizeof(UnitDesc), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->d_solves, b->solves.data(), sizeof(UnitDesc), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_status, 0, sizeof(int32_t), s);
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_total, 0, sizeof(double), s);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(b->d_x, currents, sizeof(cx) * n, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
-        launch_farfield(b->d_units, 1, b->d_ants, b->d_runs, b->d_rps, b->d_pts, b->d_x, b->d_status, b->d_fld,
+        launch_farfield(b->d_solves, 1, b->d_ants, b->d_runs, b->d_rps, b->d_pts, b->d_x, b->d_status, b->d_fld,
                         b->d_partials, b->ff_blocks, b->ff_smem, b->d_pat, b->d_total, s);
         e = cudaGetLastError();
     }

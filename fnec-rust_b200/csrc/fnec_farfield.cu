@@ -94,7 +94,7 @@ __device__ __forceinline__ void field_dir(const DevRun *runs, int n_run, const c
     fp = cx_make(fpr, fpi);
 }
 
-// grid.x: direction blocks, grid.y: unit.  Directions [0, n_int) are the
+// grid.x: direction blocks, grid.y: solve (status is per system).  Directions [0, n_int) are the
 // power-integration grid (theta outer, phi inner, as integrate_power_for_ground
 // iterates); [n_int, n_int + n_req) are the RP card points (phi outer, theta
 // inner, rp_card_points).  Requested fields go to fld_out (4 doubles per
@@ -118,7 +118,7 @@ __global__ void __launch_bounds__(FF_THREADS) k_farfield(
     int total = n_int + n_req;
     int nblocks = (total + FF_THREADS - 1) / FF_THREADS;
     if ((int)blockIdx.x >= nblocks) return;
-    if (status[ui] != 0) {
+    if (status[u.sys] != 0) {
         if (threadIdx.x == 0) partials[(int64_t)ui * max_blocks + blockIdx.x] = 0.0;
         return;
     }
@@ -208,7 +208,7 @@ __global__ void k_gains(const UnitDesc *__restrict__ units, const AntDesc *__res
         else
             for (int b = 0; b < nblocks; ++b) t += partials[(int64_t)ui * max_blocks + b];
         s_total = t;
-        total_out[ui] = status[ui] == 0 ? t : 0.0;
+        total_out[ui] = status[u.sys] == 0 ? t : 0.0;
     }
     __syncthreads();
     double total = s_total;
@@ -217,7 +217,7 @@ __global__ void k_gains(const UnitDesc *__restrict__ units, const AntDesc *__res
         double *o = pat_out + PAT_STRIDE * (u.pat_off + p);
         double th_deg, ph_deg;
         req_point(rp, pts, p, th_deg, ph_deg);
-        if (status[ui] != 0 || (pec && th_deg > 90.0)) {
+        if (status[u.sys] != 0 || (pec && th_deg > 90.0)) {
             o[0] = o[1] = o[2] = -999.99;
             o[3] = o[4] = o[5] = 0.0;
             continue;

@@ -11,7 +11,7 @@ constexpr int PAT_STRIDE = 6;  // gain_total, gain_theta, gain_phi, axial_ratio,
 
 // fnec_plain.cu
 void launch_expand_segments(const DevWire *wires, int nw, DevSeg *segs, cudaStream_t st);
-void launch_hallen_rhs(const UnitDesc *units, int nu, const AntDesc *ants, const DevSeg *segs,
+void launch_hallen_rhs(const UnitDesc *solves, int ns, const AntDesc *ants, const DevSeg *segs,
                        const int32_t *ibuf, const DevSource *srcs, cx *rhs, double *cosv,
                        double scale, cudaStream_t st);
 void launch_fill_exact(const UnitDesc *units, const AntDesc *ants, const DevSeg *segs,
@@ -25,9 +25,12 @@ void launch_factor_exact(const UnitDesc *units, int nu, int max_s, int max_trail
                          int32_t *piv, int32_t *status, cudaStream_t st);
 void launch_backsub(const UnitDesc *units, int nu, int max_s, const cx *A, cx *x,
                     const int32_t *status, cudaStream_t st);
-void launch_feedpoints(const UnitDesc *units, int nu, const AntDesc *ants, const DevSeg *segs,
-                       const DevFeed *feeds, const cx *x, const int32_t *status, double *feed_out,
-                       const int64_t *feed_row_off, cudaStream_t st);
+void launch_feedpoints(const UnitDesc *solves, int ns, const AntDesc *ants, const DevSeg *segs,
+                       const int32_t *ibuf, const DevFeed *feeds, const cx *x, const int32_t *status,
+                       double *feed_out, const int64_t *feed_row_off, cudaStream_t st);
+void launch_extra_rhs_exact(const UnitDesc *solves, int ns, int max_s, const AntDesc *ants, const int32_t *ibuf,
+                            const cx *z, const cx *rhs, const double *cosv, const cx *A, const int32_t *piv,
+                            cx *x, const int32_t *status, cudaStream_t st);
 
 // fnec_farfield.cu
 int farfield_max_blocks(int n_int_max, int n_req_max);

@@ -213,7 +213,7 @@ __global__ void k_gram32_rest(const UnitDesc *__restrict__ units, const AntDesc 
     AntDesc a = ants[u.ant];
     int n = u.n, s = u.s;
     const cx *z = zbuf + u.z_off;
-    const double *cv = cos_buf + u.rhs_off;
+    const double *cv = cos_buf + u.cos_off;
     const int32_t *wptr = ibuf + a.wptr_off, *wrow = ibuf + a.wrow_off;
     float2 *A = a32buf + mus[blockIdx.x].a32_off;
     for (int w = 0; w < a.w; ++w) {
@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(256) k_panel32(const UnitDesc *__restrict__ un
     int s = u.s;
     if (c0 >= s || status[ui] != 0) return;
     float2 *A = a32buf + mus[ui].a32_off;
-    int32_t *piv = piv_buf + u.x_off;
+    int32_t *piv = piv_buf + u.piv_off;
     int nb = min(MNB, s - c0);
     int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int c = c0; c < c0 + nb; ++c) {
@@ -345,7 +345,7 @@ __global__ void __launch_bounds__(256) k_panel32_smem(const UnitDesc *__restrict
     int s = u.s;
     if (c0 >= s || status[ui] != 0) return;
     float2 *A = a32buf + mus[ui].a32_off;
-    int32_t *piv = piv_buf + u.x_off;
+    int32_t *piv = piv_buf + u.piv_off;
     int nb = min(MNB, s - c0), m = s - c0;
     int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int e = tid; e < m * nb; e += blockDim.x) {
@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(64) k_swap_u12_32(const UnitDesc *__restrict__
     bool live = K < s;
     bool trailing = K >= c0 + nb;
     float2 *A = a32buf + mus[ui].a32_off;
-    const int32_t *piv = piv_buf + u.x_off;
+    const int32_t *piv = piv_buf + u.piv_off;
     for (int e = t; e < nb * nb; e += 64) s_L[e / nb][e % nb] = A[(int64_t)(c0 + e / nb) * s + c0 + e % nb];
     for (int q = 0; q < nb; ++q) s_c[q][t] = live ? A[(int64_t)(c0 + q) * s + K] : cf(0.f, 0.f);
     __syncthreads();
@@ -716,9 +716,9 @@ __global__ void __launch_bounds__(256) k_gmres_ir(const UnitDesc *__restrict__ u
     __shared__ cx sh[GM + 1];
     __shared__ double red[8];
     __shared__ int s_stop;
-    int ui = blockIdx.x;
-    if (status[ui] != 0) return;
+    int ui = blockIdx.x;  // one solve (right-hand side)
     UnitDesc u = units[ui];
+    if (status[u.sys] != 0) return;
     AntDesc a = ants[u.ant];
     MixedUnit mu = mus[ui];
     GmresCtx g;
@@ -729,13 +729,13 @@ __global__ void __launch_bounds__(256) k_gmres_ir(const UnitDesc *__restrict__ u
     g.rows = u.n + a.n_crow;
     g.z = zbuf + u.z_off;
     g.y = rhs + u.rhs_off;
-    g.cv = cosv + u.rhs_off;
+    g.cv = cosv + u.cos_off;
     g.rowwire = ibuf + a.rowwire_off;
     g.wptr = ibuf + a.wptr_off;
     g.wrow = ibuf + a.wrow_off;
     g.crows = crows + a.crow_off;
     g.lu = a32buf + mu.a32_off;
-    g.piv = pivbuf + u.x_off;
+    g.piv = pivbuf + u.piv_off;
     int s = g.s;
     cx *W = wbuf + mu.w_off;
     cx *b = W, *x = W + s, *r = W + 2 * s, *w = W + 3 * s;
@@ -878,44 +878,56 @@ __global__ void __launch_bounds__(256) k_gmres_ir(const UnitDesc *__restrict__ u
 
 bool mixed_available() { return true; }
 
-cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &units, const std::vector<AntDesc> &ants,
-                        int max_s) {
-    std::vector<MixedUnit> mu(units.size());
+cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, const std::vector<UnitDesc> &solves,
+                        const std::vector<AntDesc> &ants, int max_s) {
+    std::vector<int64_t> a32_of(systems.size());
     int64_t a32 = 0, v = 0, wk = 0;
-    for (size_t i = 0; i < units.size(); ++i) {
-        const UnitDesc &u = units[i];
+    for (size_t i = 0; i < systems.size(); ++i) {
+        a32_of[i] = a32;
+        a32 += (int64_t)systems[i].s * systems[i].s;
+    }
+    std::vector<MixedUnit> mu(solves.size());
+    for (size_t i = 0; i < solves.size(); ++i) {
+        const UnitDesc &u = solves[i];
         int rows = u.n + ants[u.ant].n_crow;
-        mu[i].a32_off = a32;
+        mu[i].a32_off = a32_of[u.sys];
         mu[i].v_off = v;
         mu[i].w_off = wk;
         mu[i].rows = rows;
         mu[i].iters = 0;
         mu[i].resid = 0.0;
-        a32 += (int64_t)u.s * u.s;
         v += (int64_t)(GM + 1) * u.s;
         wk += 4 * (int64_t)u.s + rows;
     }
+    // systems' descriptors index the factor through the first solve's entry
+    std::vector<MixedUnit> sysmu(systems.size());
+    for (size_t i = 0; i < systems.size(); ++i) sysmu[i].a32_off = a32_of[i];
     size_t b_mu = sizeof(MixedUnit) * (mu.size() + 1);
+    size_t b_smu = sizeof(MixedUnit) * (sysmu.size() + 1);
     size_t b_a32 = sizeof(float2) * (size_t)(a32 + 1);
     size_t b_v = sizeof(cx) * (size_t)(v + 1);
     size_t b_w = sizeof(cx) * (size_t)(wk + 1);
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-    size_t total = al(b_mu) + al(b_a32) + al(b_v) + al(b_w);
+    size_t total = al(b_mu) + al(b_smu) + al(b_a32) + al(b_v) + al(b_w);
     cudaError_t e = cudaMalloc(&w.base, total);
     if (e != cudaSuccess) return e;
     unsigned char *p = (unsigned char *)w.base;
     w.mu = (MixedUnit *)p;
     p += al(b_mu);
+    w.smu = (MixedUnit *)p;
+    p += al(b_smu);
     w.a32 = (float2 *)p;
     p += al(b_a32);
     w.v = (cx *)p;
     p += al(b_v);
     w.w = (cx *)p;
     w.bytes = total;
-    w.n_units = (int)units.size();
+    w.n_units = (int)solves.size();
     w.max_s = max_s;
     w.host = mu;
-    return cudaMemcpy(w.mu, mu.data(), sizeof(MixedUnit) * mu.size(), cudaMemcpyHostToDevice);
+    e = cudaMemcpy(w.mu, mu.data(), sizeof(MixedUnit) * mu.size(), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(w.smu, sysmu.data(), sizeof(MixedUnit) * sysmu.size(), cudaMemcpyHostToDevice);
+    return e;
 }
 
 void free_mixed(MixedWork &w) {
@@ -924,12 +936,11 @@ void free_mixed(MixedWork &w) {
     w.bytes = 0;
 }
 
-uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const std::vector<UnitDesc> &units,
+uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDesc *d_solves, int ns,
                    const AntDesc *d_ants, const DevSeg *d_segs, const int4 *fill_tiles, int n_fill,
                    const int4 *gram_tiles, int n_gram, const int32_t *ibuf, const DevConRow *crows, cx *z,
                    const cx *rhs, const double *cosv, cx *x, int32_t *piv, int32_t *status, int max_s,
                    bool do_fill, MixedMarks marks, cudaStream_t st) {
-    (void)units;
     uint64_t L = 0;
     auto mark = [&](int k) {
         if (marks.ev) cudaEventRecord(marks.ev[k], st);
@@ -939,8 +950,8 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const std::ve
         ++L;
     }
     mark(0);
-    if (n_gram > 0) k_gram32_zz<<<n_gram, 256, 0, st>>>(d_units, mw.mu, gram_tiles, z, mw.a32);
-    k_gram32_rest<<<nu, 256, 0, st>>>(d_units, d_ants, mw.mu, ibuf, crows, z, cosv, mw.a32);
+    if (n_gram > 0) k_gram32_zz<<<n_gram, 256, 0, st>>>(d_units, mw.smu, gram_tiles, z, mw.a32);
+    k_gram32_rest<<<nu, 256, 0, st>>>(d_units, d_ants, mw.smu, ibuf, crows, z, cosv, mw.a32);
     L += 2;
     mark(1);
     static bool attr = false;
@@ -951,17 +962,17 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const std::ve
     for (int c0 = 0; c0 < max_s; c0 += MNB) {
         size_t pan = sizeof(float2) * (size_t)(max_s - c0) * MNB;
         if (pan <= (size_t)PANEL32_SMEM_MAX)
-            k_panel32_smem<<<nu, 256, pan, st>>>(d_units, mw.mu, c0, mw.a32, piv, status);
+            k_panel32_smem<<<nu, 256, pan, st>>>(d_units, mw.smu, c0, mw.a32, piv, status);
         else
-            k_panel32<<<nu, 256, 0, st>>>(d_units, mw.mu, c0, mw.a32, piv, status);
+            k_panel32<<<nu, 256, 0, st>>>(d_units, mw.smu, c0, mw.a32, piv, status);
         dim3 g1((max_s + 63) / 64, nu);  // every column outside the panel
-        k_swap_u12_32<<<g1, 64, 0, st>>>(d_units, mw.mu, c0, mw.a32, piv, status);
+        k_swap_u12_32<<<g1, 64, 0, st>>>(d_units, mw.smu, c0, mw.a32, piv, status);
         int rows = max_s - (c0 + MNB);
         L += 2;
         if (rows > 0) {
             int t = ((rows + 63) / 64) * ((rows + 63) / 64);
             dim3 g2(t, nu);
-            k_trailing32<<<g2, 256, 0, st>>>(d_units, mw.mu, c0, mw.a32, status);
+            k_trailing32<<<g2, 256, 0, st>>>(d_units, mw.smu, c0, mw.a32, status);
             ++L;
         }
     }
@@ -970,8 +981,9 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const std::ve
     for (size_t i = 0; i < mw.host.size(); ++i) max_rows = max_rows > mw.host[i].rows ? max_rows : mw.host[i].rows;
     size_t smem = sizeof(cx) * (size_t)(max_s + max_rows) + sizeof(float2) * (size_t)max_s;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_gmres_ir, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_gmres_ir<<<nu, 256, smem, st>>>(d_units, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x, mw.v,
-                                      mw.w, status);
+    if (ns > 0)
+        k_gmres_ir<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x, mw.v,
+                                          mw.w, status);
     ++L;
     mark(3);
     return L;

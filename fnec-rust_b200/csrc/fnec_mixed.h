@@ -22,7 +22,8 @@ struct MixedUnit {
 struct MixedWork {
     size_t bytes = 0;
     void *base = nullptr;
-    MixedUnit *mu = nullptr;
+    MixedUnit *mu = nullptr;   // per solve
+    MixedUnit *smu = nullptr;  // per system (a32_off only)
     float2 *a32 = nullptr;
     cx *v = nullptr;
     cx *w = nullptr;
@@ -38,12 +39,13 @@ struct MixedMarks {
 };
 
 bool mixed_available();
-cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &units, const std::vector<AntDesc> &ants,
-                        int max_s);
+// systems: one per factorisation; solves: one per right-hand side.
+cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, const std::vector<UnitDesc> &solves,
+                        const std::vector<AntDesc> &ants, int max_s);
 void free_mixed(MixedWork &w);
 // Enqueue fill + Gram + factor + refinement for all units; returns the
 // number of kernel launches issued.
-uint64_t run_mixed(MixedWork &w, const UnitDesc *d_units, int nu, const std::vector<UnitDesc> &units,
+uint64_t run_mixed(MixedWork &w, const UnitDesc *d_units, int nu, const UnitDesc *d_solves, int ns,
                    const AntDesc *d_ants, const DevSeg *d_segs, const int4 *fill_tiles, int n_fill,
                    const int4 *gram_tiles, int n_gram, const int32_t *ibuf, const DevConRow *crows, cx *z,
                    const cx *rhs, const double *cosv, cx *x, int32_t *piv, int32_t *status, int max_s,

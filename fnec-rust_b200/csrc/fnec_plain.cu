@@ -81,15 +81,17 @@ __global__ void k_expand_segments(const DevWire *__restrict__ wires, int nw, Dev
 // Hallen RHS: cos(k s_local) per merged conductor and the delta-gap term
 // -j (2 pi / eta0) V sin(k |s - s_src|) on the source's conductor.
 // ---------------------------------------------------------------------------
-__global__ void k_hallen_rhs(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
+__global__ void k_hallen_rhs(const UnitDesc *__restrict__ solves, const AntDesc *__restrict__ ants,
                              const DevSeg *__restrict__ segs, const int32_t *__restrict__ ibuf,
                              const DevSource *__restrict__ srcs, cx *rhs_buf, double *cos_buf,
                              double scale) {
-    UnitDesc u = units[blockIdx.x];
+    UnitDesc u = solves[blockIdx.x];  // one right-hand side
     AntDesc a = ants[u.ant];
     const DevSeg *sg = segs + a.seg_off;
     const int32_t *comp = ibuf + a.comp_off;
-    const DevSource *src = srcs + a.src_off;
+    const int32_t *sptr = ibuf + a.sptr_off;
+    const DevSource *src = srcs + a.src_off + sptr[u.rhs];
+    int n_src = sptr[u.rhs + 1] - sptr[u.rhs];
     double k = u.k_fill;
     for (int m = threadIdx.x; m < a.n; m += blockDim.x) {
         int first = comp[2 * m], last = comp[2 * m + 1];
@@ -101,11 +103,13 @@ __global__ void k_hallen_rhs(const UnitDesc *__restrict__ units, const AntDesc *
         double dl1 = D_SUB(sg[m].mid[1], wm1);
         double dl2 = D_SUB(sg[m].mid[2], wm2);
         double s_local = D_ADD(D_ADD(D_MUL(dl0, wd[0]), D_MUL(dl1, wd[1])), D_MUL(dl2, wd[2]));
-        double sn, cs;
-        cr_sincos(D_MUL(k, s_local), &sn, &cs);
-        cos_buf[u.rhs_off + m] = cs;
+        if (u.rhs == 0) {  // cos(k s) belongs to the system: written once
+            double sn, cs;
+            cr_sincos(D_MUL(k, s_local), &sn, &cs);
+            cos_buf[u.cos_off + m] = cs;
+        }
         cx r = cx_make(0.0, 0.0);
-        for (int q = 0; q < a.n_src; ++q) {
+        for (int q = 0; q < n_src; ++q) {
             DevSource s = src[q];
             if (m < s.comp_first || m > s.comp_last) continue;
             const DevSeg &f = sg[s.feed];
@@ -305,7 +309,7 @@ __global__ void k_gram_ccols(const UnitDesc *__restrict__ units, const AntDesc *
     int n = u.n, s = u.s, w1 = s + 1;
     const cx *z = zbuf + u.z_off;
     const cx *y = rhs_buf + u.rhs_off;
-    const double *cv = cos_buf + u.rhs_off;
+    const double *cv = cos_buf + u.cos_off;
     const int32_t *wptr = ibuf + a.wptr_off;
     const int32_t *wrow = ibuf + a.wrow_off;
     cx *A = abuf + u.a_off;
@@ -403,7 +407,7 @@ __global__ void __launch_bounds__(256) k_panel(const UnitDesc *__restrict__ unit
     if (c0 >= s || status[ui] != 0) return;
     int w1 = s + 1;
     cx *A = abuf + u.a_off;
-    int32_t *piv = piv_buf + u.x_off;
+    int32_t *piv = piv_buf + u.piv_off;
     int nb = min(NB, s - c0);
     int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     for (int c = c0; c < c0 + nb; ++c) {
@@ -477,7 +481,7 @@ __global__ void __launch_bounds__(256) k_panel_smem(const UnitDesc *__restrict__
     if (c0 >= s || status[ui] != 0) return;
     int w1 = s + 1;
     cx *A = abuf + u.a_off;
-    int32_t *piv = piv_buf + u.x_off;
+    int32_t *piv = piv_buf + u.piv_off;
     int nb = min(NB, s - c0);
     int m = s - c0;
     int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
@@ -555,8 +559,22 @@ __global__ void __launch_bounds__(64) k_swap_u12(const UnitDesc *__restrict__ un
     int nb = min(NB, s - c0);
     int w1 = s + 1;
     cx *A = abuf + u.a_off;
-    const int32_t *piv = piv_buf + u.x_off;
+    const int32_t *piv = piv_buf + u.piv_off;
     int t = threadIdx.x;
+    if (blockIdx.x >= gridDim.x - (c0 + 63) / 64) {
+        // columns left of the panel (earlier panels' multipliers): swaps
+        // only, so that every row of L ends up with the row it belongs to
+        int K = (blockIdx.x - (gridDim.x - (c0 + 63) / 64)) * 64 + t;
+        if (K >= c0) return;
+        for (int q = 0; q < nb; ++q) {
+            int p = piv[c0 + q];
+            if (p == c0 + q) continue;
+            cx t0 = A[(int64_t)(c0 + q) * w1 + K];
+            A[(int64_t)(c0 + q) * w1 + K] = A[(int64_t)p * w1 + K];
+            A[(int64_t)p * w1 + K] = t0;
+        }
+        return;
+    }
     int K = c0 + nb + blockIdx.x * 64 + t;  // column s is the right-hand side
     if (c0 + nb + blockIdx.x * 64 > s) return;
     bool live = K <= s;
@@ -691,18 +709,22 @@ __global__ void k_backsub(const UnitDesc *__restrict__ units, const cx *__restri
 }
 
 // Feedpoint rows: v_source = v_vec[idx] * dl, Zin = v_source / I[idx] when
-// |I| > 1e-60 (solve_session.rs:911-917).
-__global__ void k_feedpoints(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
-                             const DevSeg *__restrict__ segs, const DevFeed *__restrict__ feeds,
-                             const cx *__restrict__ xbuf, const int32_t *__restrict__ status,
-                             double *feed_out, const int64_t *__restrict__ feed_row_off) {
-    int ui = blockIdx.x;
-    UnitDesc u = units[ui];
+// |I| > 1e-60 (solve_session.rs:911-917).  One CTA per solve; its rows are
+// the feed rows of its right-hand side.
+__global__ void k_feedpoints(const UnitDesc *__restrict__ solves, const AntDesc *__restrict__ ants,
+                             const DevSeg *__restrict__ segs, const int32_t *__restrict__ ibuf,
+                             const DevFeed *__restrict__ feeds, const cx *__restrict__ xbuf,
+                             const int32_t *__restrict__ status, double *feed_out,
+                             const int64_t *__restrict__ feed_row_off) {
+    int si = blockIdx.x;
+    UnitDesc u = solves[si];
     AntDesc a = ants[u.ant];
-    for (int q = threadIdx.x; q < a.n_feed; q += blockDim.x) {
-        DevFeed f = feeds[a.feed_off + q];
-        double *o = feed_out + 7 * (feed_row_off[ui] + q);
-        if (status[ui] != 0) {
+    const int32_t *fptr = ibuf + a.fptr_off;
+    int f0 = fptr[u.rhs], nf = fptr[u.rhs + 1] - f0;
+    for (int q = threadIdx.x; q < nf; q += blockDim.x) {
+        DevFeed f = feeds[a.feed_off + f0 + q];
+        double *o = feed_out + 7 * (feed_row_off[si] + q);
+        if (status[u.sys] != 0) {
             for (int t = 0; t < 7; ++t) o[t] = 0.0;
             continue;
         }
@@ -721,15 +743,111 @@ __global__ void k_feedpoints(const UnitDesc *__restrict__ units, const AntDesc *
 }
 
 // ---------------------------------------------------------------------------
+// Further right-hand sides on the factored system (solves with rhs >= 1).
+// The reference re-runs the whole elimination for another source; A does
+// not depend on the source, so its operations on A repeat exactly and only
+// the b column differs.  b = M^H y is formed in the Gram's order; the row
+// swaps, the multipliers (stored in L with all later swaps applied, so row
+// r of L is the row that ends at position r) and the back substitution then
+// give b exactly the sequence of operations the reference's augmented
+// column receives.
+// ---------------------------------------------------------------------------
+__global__ void k_extra_rhs_b(const UnitDesc *__restrict__ solves, const AntDesc *__restrict__ ants,
+                              const int32_t *__restrict__ ibuf, const cx *__restrict__ zbuf,
+                              const cx *__restrict__ rhs_buf, const double *__restrict__ cos_buf, cx *xbuf) {
+    UnitDesc u = solves[blockIdx.y];
+    if (u.rhs == 0) return;
+    AntDesc a = ants[u.ant];
+    int n = u.n;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const cx *z = zbuf + u.z_off;
+    const cx *y = rhs_buf + u.rhs_off;
+    cx *b = xbuf + u.x_off;
+    if (i < n) {
+        cx acc = cx_make(0.0, 0.0);
+        for (int r = 0; r < n; ++r) acc = cx_add(acc, cx_conj_mul(z[(int64_t)r * n + i], y[r]));
+        b[i] = acc;
+    } else if (i < n + a.w) {
+        int w = i - n;
+        const int32_t *wptr = ibuf + a.wptr_off, *wrow = ibuf + a.wrow_off;
+        const double *cv = cos_buf + u.cos_off;
+        cx acc = cx_make(0.0, 0.0);
+        for (int q = wptr[w]; q < wptr[w + 1]; ++q) {
+            int r = wrow[q];
+            acc = cx_add(acc, cx_conj_mul(cx_make(-cv[r], 0.0), y[r]));
+        }
+        b[i] = acc;
+    }
+}
+
+__global__ void k_extra_rhs_solve(const UnitDesc *__restrict__ solves, const cx *__restrict__ abuf,
+                                  const int32_t *__restrict__ piv_buf, cx *xbuf,
+                                  const int32_t *__restrict__ status) {
+    extern __shared__ cx s_b[];
+    UnitDesc u = solves[blockIdx.x];
+    if (u.rhs == 0 || status[u.sys] != 0) return;
+    int s = u.s, w1 = s + 1;
+    const cx *A = abuf + u.a_off;
+    const int32_t *piv = piv_buf + u.piv_off;
+    cx *x = xbuf + u.x_off;
+    int lane = threadIdx.x;
+    for (int i = lane; i < s; i += 32) s_b[i] = x[i];
+    __syncwarp();
+    if (lane == 0)
+        for (int c = 0; c < s; ++c) {
+            int p = piv[c];
+            if (p != c) {
+                cx t0 = s_b[c];
+                s_b[c] = s_b[p];
+                s_b[p] = t0;
+            }
+        }
+    __syncwarp();
+    // forward: row r receives b[r] -= f[r][c] * b[c] for c = 0..r-1 in order
+    for (int c = 0; c < s; ++c) {
+        cx bc = s_b[c];
+        for (int r = c + 1 + lane; r < s; r += 32) s_b[r] = cx_sub(s_b[r], cx_mul(A[(int64_t)r * w1 + c], bc));
+        __syncwarp();
+    }
+    // back substitution, j ascending, as k_backsub
+    for (int i = s - 1; i >= 0; --i) {
+        const cx *row = A + (int64_t)i * w1;
+        cx sum = s_b[i];
+        int j = i + 1 + lane;
+        cx p = (j < s) ? cx_mul(row[j], s_b[j]) : cx_make(0.0, 0.0);
+        for (int j0 = i + 1; j0 < s; j0 += 32) {
+            int jn = j0 + 32 + lane;
+            cx pn = (jn < s) ? cx_mul(row[jn], s_b[jn]) : cx_make(0.0, 0.0);
+            int cnt = min(32, s - j0);
+            double pr[32], pim[32];
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+                pr[q] = __shfl_sync(0xffffffffu, p.re, q);
+                pim[q] = __shfl_sync(0xffffffffu, p.im, q);
+            }
+#pragma unroll
+            for (int q = 0; q < 32; ++q)
+                if (q < cnt) sum = cx_sub(sum, cx_make(pr[q], pim[q]));
+            p = pn;
+        }
+        cx xi = cx_div(sum, row[i]);
+        __syncwarp();
+        if (lane == 0) s_b[i] = xi;
+        __syncwarp();
+    }
+    for (int i = lane; i < s; i += 32) x[i] = s_b[i];
+}
+
+// ---------------------------------------------------------------------------
 // launch wrappers (host)
 // ---------------------------------------------------------------------------
 void launch_expand_segments(const DevWire *wires, int nw, DevSeg *segs, cudaStream_t st) {
     if (nw > 0) k_expand_segments<<<nw, 64, 0, st>>>(wires, nw, segs);
 }
-void launch_hallen_rhs(const UnitDesc *units, int nu, const AntDesc *ants, const DevSeg *segs,
+void launch_hallen_rhs(const UnitDesc *solves, int ns, const AntDesc *ants, const DevSeg *segs,
                        const int32_t *ibuf, const DevSource *srcs, cx *rhs, double *cosv,
                        double scale, cudaStream_t st) {
-    if (nu > 0) k_hallen_rhs<<<nu, 128, 0, st>>>(units, ants, segs, ibuf, srcs, rhs, cosv, scale);
+    if (ns > 0) k_hallen_rhs<<<ns, 128, 0, st>>>(solves, ants, segs, ibuf, srcs, rhs, cosv, scale);
 }
 void launch_fill_exact(const UnitDesc *units, const AntDesc *ants, const DevSeg *segs,
                        const int4 *tiles, int ntiles, cx *z, cudaStream_t st) {
@@ -770,7 +888,8 @@ void launch_factor_exact(const UnitDesc *units, int nu, int max_s, int max_trail
         int rest = max_s + 1 - (c0 + NB);
         if (rest < 1) rest = 1;
         {
-            dim3 g1((rest + 63) / 64, nu);
+            // trailing column blocks, then blocks for the c0 columns on the left
+            dim3 g1((rest + 63) / 64 + (c0 + 63) / 64, nu);
             k_swap_u12<<<g1, 64, 0, st>>>(units, c0, A, piv, status);
             int rows = max_s - (c0 + NB);
             if (rows > 0) {
@@ -789,11 +908,22 @@ void launch_backsub(const UnitDesc *units, int nu, int max_s, const cx *A, cx *x
         cudaFuncSetAttribute(k_backsub, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (nu > 0) k_backsub<<<nu, 32, smem, st>>>(units, A, x, status);
 }
-void launch_feedpoints(const UnitDesc *units, int nu, const AntDesc *ants, const DevSeg *segs,
-                       const DevFeed *feeds, const cx *x, const int32_t *status, double *feed_out,
-                       const int64_t *feed_row_off, cudaStream_t st) {
-    if (nu > 0)
-        k_feedpoints<<<nu, 32, 0, st>>>(units, ants, segs, feeds, x, status, feed_out, feed_row_off);
+void launch_feedpoints(const UnitDesc *solves, int ns, const AntDesc *ants, const DevSeg *segs,
+                       const int32_t *ibuf, const DevFeed *feeds, const cx *x, const int32_t *status,
+                       double *feed_out, const int64_t *feed_row_off, cudaStream_t st) {
+    if (ns > 0)
+        k_feedpoints<<<ns, 32, 0, st>>>(solves, ants, segs, ibuf, feeds, x, status, feed_out, feed_row_off);
+}
+void launch_extra_rhs_exact(const UnitDesc *solves, int ns, int max_s, const AntDesc *ants, const int32_t *ibuf,
+                            const cx *z, const cx *rhs, const double *cosv, const cx *A, const int32_t *piv,
+                            cx *x, const int32_t *status, cudaStream_t st) {
+    if (ns <= 0) return;
+    dim3 g((max_s + 127) / 128, ns);
+    k_extra_rhs_b<<<g, 128, 0, st>>>(solves, ants, ibuf, z, rhs, cosv, x);
+    size_t smem = sizeof(cx) * (size_t)max_s;
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_extra_rhs_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_extra_rhs_solve<<<ns, 32, smem, st>>>(solves, A, piv, x, status);
 }
 
 }  // namespace fnec

@@ -57,8 +57,11 @@ struct AntDesc {
     int64_t wrow_off;    // CSR: int32 rows of each wire column, wrow_ptr
     int64_t wptr_off;    // int32[w+1]
     int64_t comp_off;    // int32[2n]: merged component (first,last) of each segment
-    int64_t src_off;     // DevSource[n_src] (resolved BTreeMap order)
+    int64_t src_off;     // DevSource[n_src] (resolved BTreeMap order), grouped by right-hand side
     int32_t n_src;
+    int32_t n_rhs;       // right-hand sides per system
+    int64_t sptr_off;    // int32[n_rhs+1]: sources of right-hand side r = srcs[sptr[r] .. sptr[r+1])
+    int64_t fptr_off;    // int32[n_rhs+1]: feed rows of right-hand side r
     int32_t n_con;       // constraint pair groups
     int64_t con_off;     // DevConstraint groups
     int64_t conv_off;    // int32 value codes for each group (row order)
@@ -100,20 +103,29 @@ struct DevConstraint {
     int32_t begin, count;
 };
 
+// A system is one (antenna, frequency): one Z, one normal-equation matrix,
+// one factorisation.  A solve is one right-hand side of a system (the
+// superposed EX cards of a deck, or -- for served requests -- each source
+// position separately); solves share their system's factor.  Kernels that
+// work per system and kernels that work per solve both take UnitDesc
+// arrays: a solve's descriptor is its system's with the per-solve offsets.
 struct UnitDesc {
     int32_t ant;
     int32_t n;
     int32_t s;           // n + w
-    int32_t pad;
+    int32_t rhs;         // right-hand side index of a solve (0 for a system)
     double freq;
     double k_fill;       // 2*pi*f/c (matrix.rs:194, excitation.rs:165)
     double k_rp;         // 2*pi/(c/f) (farfield.rs:570-571)
-    int64_t z_off;       // complex elements
-    int64_t a_off;       // complex elements of [A|b]
-    int64_t x_off;       // complex elements
-    int64_t rhs_off;     // complex elements (rhs) and doubles (cosv)
-    int64_t pat_off;     // requested pattern points (4 doubles each)
-    int64_t ff_off;      // far-field partial sums
+    int64_t z_off;       // complex elements of Z (per system)
+    int64_t a_off;       // complex elements of [A|b] (per system)
+    int64_t x_off;       // complex elements of the solution (per solve; a system: its solve 0)
+    int64_t rhs_off;     // complex elements of the Hallen RHS (per solve; a system: its solve 0)
+    int64_t cos_off;     // doubles of cos(k s) (per system)
+    int64_t piv_off;     // int32 pivot rows (per system)
+    int64_t pat_off;     // requested pattern points (per solve)
+    int32_t n_rhs;       // right-hand sides of the system
+    int32_t sys;         // system index of a solve
 };
 
 // Requested pattern points of one antenna: an RP card grid (phi outer,

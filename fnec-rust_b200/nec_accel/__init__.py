@@ -82,18 +82,19 @@ class _RpCard(ctypes.Structure):
 
 class _Antenna(ctypes.Structure):
     _fields_ = [("wires", _P), ("n_wires", _U32), ("sources", _P), ("n_sources", _U32), ("ground", _I32),
-                ("n_freqs", _U32), ("freqs_hz", _P), ("rp", _P)]
+                ("n_freqs", _U32), ("freqs_hz", _P), ("rp", _P), ("separate_sources", _U32)]
 
 
 class _UnitInfo(ctypes.Structure):
     _fields_ = [("antenna", _U32), ("n", _U32), ("s", _U32), ("n_feed", _U32), ("n_points", _U32),
-                ("freq_hz", _D), ("cur_off", _U64), ("feed_off", _U64), ("pat_off", _U64)]
+                ("freq_hz", _D), ("cur_off", _U64), ("feed_off", _U64), ("pat_off", _U64), ("rhs", _U32),
+                ("system", _U32)]
 
 
 class _BatchInfo(ctypes.Structure):
     _fields_ = [("n_units", _U32), ("max_s", _U32), ("total_currents", _U64), ("total_feeds", _U64),
                 ("total_points", _U64), ("device_bytes", _U64), ("h2d_bytes", _U64),
-                ("kernel_launches", _U64)]
+                ("kernel_launches", _U64), ("n_systems", _U32)]
 
 
 # name -> (restype, argtypes); every function declared in include/fnec_cuda.h
@@ -421,6 +422,7 @@ class Antenna:
     freqs_hz: Sequence[float]
     ground: int = GROUND_FREE
     rp: Optional[tuple] = None
+    separate_sources: bool = False  # each source its own right-hand side on one factorisation
 
 
 def wires_array(wires) -> np.ndarray:
@@ -466,7 +468,8 @@ class HallenBatch:
                 rp = _RpCard(*[int(a.rp[0]), int(a.rp[1])] + [float(v) for v in a.rp[2:6]])
             self._keep += [w, s, f, rp]
             arr[i] = _Antenna(_ptr(w), len(w), _ptr(s), len(s), int(a.ground), len(f), _ptr(f),
-                              ctypes.cast(ctypes.pointer(rp), _P) if rp is not None else None)
+                              ctypes.cast(ctypes.pointer(rp), _P) if rp is not None else None,
+                              int(bool(a.separate_sources)))
         self._keep.append(arr)
         h = ctypes.c_void_p()
         self.ctx.check(lib().fnec_batch_create(self.ctx.handle, arr, len(antennas), int(precision),
@@ -518,7 +521,7 @@ class HallenBatch:
 
     def d2h_bytes(self, currents=True, feeds=True, pattern=True) -> int:
         i = self.info
-        b = 4 * i.n_units + 8 * i.n_units
+        b = 4 * i.n_systems + 8 * i.n_units
         if currents:
             b += 16 * sum(u["s"] for u in self.units)
         if feeds:

@@ -139,9 +139,15 @@ typedef struct {
     uint32_t n_freqs;
     const double *freqs_hz;
     const fnec_rp_card *rp; /* NULL: no pattern */
+    /* 0: the EX cards superpose into one right-hand side (a deck's
+     * semantics).  1: every card is its own right-hand side -- solved as the
+     * single-source deck it stands for -- and all of them reuse the one
+     * factorisation of each frequency. */
+    uint32_t separate_sources;
 } fnec_antenna;
 
-/* Per-unit shape, for sizing result buffers. */
+/* Per-unit shape, for sizing result buffers.  A unit is one solve: one
+ * right-hand side of one (antenna, frequency) system. */
 typedef struct {
     uint32_t antenna;
     uint32_t n;        /* segments (currents)            */
@@ -152,6 +158,8 @@ typedef struct {
     uint64_t cur_off;  /* offset (complex) into the currents array of fnec_batch_read */
     uint64_t feed_off; /* offset (rows of 7 doubles) into the feed array           */
     uint64_t pat_off;  /* offset (rows of 6 doubles) into the pattern array        */
+    uint32_t rhs;      /* right-hand side index within its system                  */
+    uint32_t system;   /* (antenna, frequency) system index: the factorisation     */
 } fnec_unit_info;
 
 /* Batch totals. */
@@ -164,6 +172,7 @@ typedef struct {
     uint64_t device_bytes;   /* HBM held by the batch           */
     uint64_t h2d_bytes;      /* input bytes copied by fnec_batch_upload */
     uint64_t kernel_launches;/* launches issued by one fnec_batch_run  */
+    uint32_t n_systems;      /* factorisations (antenna, frequency)     */
 } fnec_batch_info;
 
 typedef struct fnec_ctx fnec_ctx;

@@ -145,3 +145,15 @@ def test_mixed_uneven_random_antenna_batch_sample(acc):
         _check(res, batch, u, O.wires_array(w), O.sources_array(s), g, f, None, errs)
     it, rs = batch.refinement_stats()
     assert it.max() <= 96
+
+
+def test_mixed_extra_right_hand_sides(acc):
+    wl = [(1, 21, (0, 0, 1.0), (0, 0, 6.0), 1e-3), (2, 15, (1.2, 0, 1.0), (1.2, 0, 5.0), 1e-3)]
+    srcs = [(1, 11, 1.0), (2, 8, 0.5 - 0.25j), (1, 3, 1.0), (2, 14, 1j)]
+    w = O.wires_array(wl)
+    b = acc.HallenBatch([acc.Antenna(w.view(acc.WIRE_DTYPE), O.sources_array(srcs).view(acc.SOURCE_DTYPE), [24e6],
+                                     1, None, separate_sources=True)], precision=acc.PRECISION_MIXED)
+    res = b.solve()
+    errs = {}
+    for r, src in enumerate(srcs):
+        _check(res, b, r, w, O.sources_array([src]), 1, 24e6, None, errs)

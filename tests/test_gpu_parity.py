@@ -273,3 +273,33 @@ def test_uneven_random_antenna_batch_sample(acc):
     for u in range(0, 64, 7):
         w, s, g, f = wl[u]
         _check_unit(acc, batch, res, u, O.wires_array(w), O.sources_array(s), g, f, None)
+
+
+def test_extra_right_hand_sides_reuse_the_factor_bit_exactly(acc):
+    """separate_sources: three source positions on one factorisation per
+    frequency.  Solve r must be bit-identical to the single-source deck
+    solved on its own (the reference re-runs the whole elimination for a
+    new source; only the b column differs), and match the oracle."""
+    wl = [(1, 21, (0, 0, 1.0), (0, 0, 6.0), 1e-3), (2, 15, (1.2, 0, 1.0), (1.2, 0, 5.0), 1e-3),
+          (3, 9, (0, 0, 6.0), (1.2, 0, 6.5), 1e-3)]
+    srcs = [(1, 11, 1.0), (2, 8, 0.5 - 0.25j), (3, 2, 1.0)]
+    w = O.wires_array(wl)
+    freqs = [20e6, 26e6]
+    for ground in (0, 1):
+        multi = acc.HallenBatch([acc.Antenna(w.view(acc.WIRE_DTYPE), O.sources_array(srcs).view(acc.SOURCE_DTYPE),
+                                             freqs, ground, (9, 3, 0.0, 0.0, 10.0, 60.0), separate_sources=True)])
+        rm = multi.solve()
+        assert len(rm.currents) == len(freqs) * len(srcs)
+        for fi, f in enumerate(freqs):
+            for r, src in enumerate(srcs):
+                one = acc.HallenBatch([acc.Antenna(w.view(acc.WIRE_DTYPE), O.sources_array([src]).view(acc.SOURCE_DTYPE),
+                                                   [f], ground, (9, 3, 0.0, 0.0, 10.0, 60.0))])
+                ro = one.solve()
+                u = fi * len(srcs) + r
+                xm, _ = multi.read_unit(u)
+                xo, _ = one.read_unit(0)
+                assert np.array_equal(xm.view(np.uint64), xo.view(np.uint64)), (fi, r)
+                assert np.array_equal(rm.feeds[u], ro.feeds[0])
+                assert np.array_equal(rm.pattern[u], ro.pattern[0])
+                _check_unit(acc, one, ro, 0, w, O.sources_array([src]), ground, f,
+                            O.rp_card_points(9, 3, 0, 0, 10, 60))
