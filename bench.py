@@ -112,6 +112,39 @@ def uneven_workload(n_ant: int = 4096, seed: int = 7):
     return out
 
 
+def mesh_workload(cells: int = 46, seed: int = 5, f0: float = 14.2e6):
+    """Junctioned wire mesh over PEC ground: a square grid of cells x cells
+    cells with edge 0.05 lambda in the plane z = 0.25 lambda, node positions
+    jittered by a seeded +-1 % of the pitch, every cell edge a 2-segment wire
+    of radius 1 mm (row edges first, then column edges, in tag order), and a
+    1 V source on the first segment of the row edge nearest the grid centre.
+    Every interior node joins four wire ends, so junction rows are pairwise
+    (C(4,2) = 6 per interior node, geometry.rs:274-339)."""
+    lam = C0 / f0
+    pitch = 0.05 * lam
+    rng = np.random.default_rng(seed)
+    nn = cells + 1
+    jit = rng.uniform(-0.01, 0.01, size=(nn, nn, 2)) * pitch
+    node = np.zeros((nn, nn, 3))
+    for i in range(nn):
+        for j in range(nn):
+            node[i, j] = (i * pitch + jit[i, j, 0], j * pitch + jit[i, j, 1], 0.25 * lam)
+    wires = []
+    tag = 1
+    centre = None
+    for j in range(nn):          # row edges: along x
+        for i in range(cells):
+            wires.append((tag, 2, tuple(node[i, j]), tuple(node[i + 1, j]), 1e-3))
+            if j == nn // 2 and i == cells // 2:
+                centre = tag
+            tag += 1
+    for i in range(nn):          # column edges: along y
+        for j in range(cells):
+            wires.append((tag, 2, tuple(node[i, j]), tuple(node[i, j + 1]), 1e-3))
+            tag += 1
+    return wires, [(centre, 1, 1.0)], f0
+
+
 def algorithmic_flops(n, s, n_dir):
     """Algorithmic work of each phase summed over units (real flops; a
     complex multiply-add is 8: 4 multiplies + 4 adds).  n, s, n_dir are
@@ -199,6 +232,9 @@ def reference_units(args):
         wires, sources, freqs, rp = sweep_workload(n_freqs=args.freqs)
         return [(wires, sources, 0, f, rp) for f in freqs], "sweep5: 5-wire parallel array, N=255 (S=260), " \
             f"{len(freqs)} freqs 13.0-15.5 MHz, RP 91x361 per freq"
+    if args.workload == "mesh":
+        wl, src, f = mesh_workload(args.cells)
+        return [(wl, src, 1, f, None)], f"mesh: {args.cells}x{args.cells} cells over PEC ground"
     wl = uneven_workload(args.antennas)
     return [(w, src, g, f, None) for w, src, g, f in wl], f"uneven: {len(wl)} random antennas, one frequency each"
 
@@ -244,8 +280,10 @@ def main():
                     help="mixed: time the chosen form and the plain FP64 form; fp64: plain only")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--freqs", type=int, default=201, help="sweep points (201 = the workload; fewer = profiling)")
-    ap.add_argument("--workload", default="sweep5", choices=["sweep5", "uneven"],
-                    help="sweep5: the 5-wire frequency sweep (headline); uneven: 4096 random antennas")
+    ap.add_argument("--workload", default="sweep5", choices=["sweep5", "uneven", "mesh"],
+                    help="sweep5: the 5-wire frequency sweep (headline); uneven: 4096 random antennas; "
+                         "mesh: the junctioned wire mesh over ground (one large solve)")
+    ap.add_argument("--cells", type=int, default=46, help="mesh workload size (cells per side)")
     ap.add_argument("--antennas", type=int, default=4096, help="uneven workload size")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -275,6 +313,14 @@ def main():
                 f"RP 91x361 per freq")
         ref_units = [(wires, sources, acc.GROUND_FREE, f, rp) for f in freqs]
         data = "synthetic (seeded 5-element array, seed 11)"
+    elif args.workload == "mesh":
+        wl, src, f = mesh_workload(args.cells)
+        ants = [acc.Antenna(acc.wires_array(wl), acc.sources_array(src), [f], acc.GROUND_PEC, None)]
+        n_seg = 2 * len(wl)
+        desc = (f"mesh: {args.cells}x{args.cells} cells of 2-segment wires over PEC ground (GN 1), N={n_seg}, "
+                f"W={len(wl)}, one frequency 14.2 MHz, no pattern")
+        ref_units = [(wl, src, acc.GROUND_PEC, f, None)]
+        data = "synthetic (seeded jittered mesh, seed 5)"
     else:
         wl = uneven_workload(args.antennas)
         ants = [acc.Antenna(acc.wires_array(w), acc.sources_array(src), [f], g, None) for w, src, g, f in wl]
@@ -429,7 +475,11 @@ def main():
             line["mixed_gate"] = gate
             line["mixed_vs_fp64"] = line["form_mixed"]["value"] / line["form_fp64"]["value"]
         res = H["res"]
-        if not args.no_cpu_baseline:
+        if args.workload == "mesh" and args.cells > 12:
+            line["cpu_baseline"] = {"value": None, "unit": "solves/s", "cores": os.cpu_count() or 1, "kind": "port",
+                                    "sample": "not run: the faithful single-threaded CPU solve of this mesh takes "
+                                              "hours (2.9e13 flops of naive Gram + 5.8e12 of GEPP)"}
+        elif not args.no_cpu_baseline:
             threads = os.cpu_count() or 1
             n_units = min(units, max(threads, 4))
             rate, dt, probs, idx = cpu_oracle_units(ref_units, n_units, threads)

@@ -343,6 +343,7 @@ struct fnec_batch {
     int64_t tot_seg = 0, z_el = 0, a_el = 0, x_el = 0, rhs_el = 0, pat_el = 0, feed_rows = 0, cos_el = 0,
             piv_el = 0;
     int max_rhs = 1;
+    int max_w = 0;
     int ff_blocks = 0;
     size_t ff_smem = 0;
     uint64_t launches = 0;
@@ -572,6 +573,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
         ff_int_max = std::max(ff_int_max, n_int);
         smem_max = std::max(smem_max, sizeof(DevRun) * h.runs.size() + sizeof(cx) * (size_t)n);
         b->ants.push_back(a);
+        b->max_w = std::max(b->max_w, (int)a.w);
         // systems (one per frequency) and their solves (one per right-hand side)
         int s = n + a.w;
         for (size_t fi = 0; fi < h.freqs.size(); ++fi) {
@@ -932,7 +934,7 @@ int fnec_batch_run(fnec_batch *b) {
         L += run_mixed(b->mixed, b->d_units, nu, b->d_solves, ns, b->d_ants, b->d_segs, b->d_fill_tiles,
                        (int)b->fill_tiles.size(), b->d_gram_tiles, (int)b->gram_tiles.size(), b->d_ibuf,
                        b->d_crows, b->d_z, b->d_rhs, b->d_cos, b->d_x, b->d_piv, b->d_status, b->max_s,
-                       b->z_given.empty(), mm, st);
+                       b->z_given.empty(), b->max_w, mm, st);
     } else {
         if (b->z_given.empty()) {
             launch_fill_exact(b->d_units, b->d_ants, b->d_segs, b->d_fill_tiles, (int)b->fill_tiles.size(),
@@ -940,7 +942,7 @@ int fnec_batch_run(fnec_batch *b) {
             ++L;
         }
         mark(3);
-        launch_gram_exact(b->d_units, nu, b->d_ants, b->d_gram_tiles, (int)b->gram_tiles.size(), b->d_ibuf,
+        launch_gram_exact(b->d_units, nu, b->max_w, b->d_ants, b->d_gram_tiles, (int)b->gram_tiles.size(), b->d_ibuf,
                           b->d_cons, b->d_codes, b->d_z, b->d_rhs, b->d_cos, b->d_a, st);
         mark(4);
         launch_factor_exact(b->d_units, nu, b->max_s, 0, b->d_a, b->d_piv, b->d_status, st);

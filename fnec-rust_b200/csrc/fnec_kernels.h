@@ -17,7 +17,7 @@ void launch_hallen_rhs(const UnitDesc *solves, int ns, const AntDesc *ants, cons
 void launch_fill_exact(const UnitDesc *units, const AntDesc *ants, const DevSeg *segs,
                        const int4 *tiles, int ntiles, cx *z, cudaStream_t st);
 void launch_fill_exact_flat(const DevSeg *segs, int n, double k, int ground, cx *z, cudaStream_t st);
-void launch_gram_exact(const UnitDesc *units, int nu, const AntDesc *ants, const int4 *gtiles,
+void launch_gram_exact(const UnitDesc *units, int nu, int max_w, const AntDesc *ants, const int4 *gtiles,
                        int ngtiles, const int32_t *ibuf, const DevConstraint *cons,
                        const int32_t *codes, const cx *z, const cx *rhs, const double *cosv, cx *A,
                        cudaStream_t st);

@@ -204,39 +204,47 @@ __global__ void __launch_bounds__(256) k_gram32_zz(const UnitDesc *__restrict__ 
     }
 }
 
-// cos columns, constraint rows and lambda (one CTA per unit)
-__global__ void k_gram32_rest(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
-                              const MixedUnit *__restrict__ mus, const int32_t *__restrict__ ibuf,
-                              const DevConRow *__restrict__ crows, const cx *__restrict__ zbuf,
-                              const double *__restrict__ cos_buf, float2 *a32buf) {
-    UnitDesc u = units[blockIdx.x];
+// cos columns (grid.x = wire column, grid.y = system)
+__global__ void k_gram32_ccols(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
+                               const MixedUnit *__restrict__ mus, const int32_t *__restrict__ ibuf,
+                               const cx *__restrict__ zbuf, const double *__restrict__ cos_buf, float2 *a32buf) {
+    UnitDesc u = units[blockIdx.y];
     AntDesc a = ants[u.ant];
+    int w = blockIdx.x;
+    if (w >= a.w) return;
     int n = u.n, s = u.s;
     const cx *z = zbuf + u.z_off;
     const double *cv = cos_buf + u.cos_off;
     const int32_t *wptr = ibuf + a.wptr_off, *wrow = ibuf + a.wrow_off;
-    float2 *A = a32buf + mus[blockIdx.x].a32_off;
-    for (int w = 0; w < a.w; ++w) {
-        int b = wptr[w], e = wptr[w + 1];
-        for (int i = threadIdx.x; i < n; i += blockDim.x) {
-            double cr = 0, ci = 0;
-            for (int q = b; q < e; ++q) {
-                int r = wrow[q];
-                cx zi = z[(int64_t)r * n + i];
-                cr += -cv[r] * zi.re;
-                ci += -cv[r] * zi.im;
-            }
-            A[(int64_t)i * s + n + w] = cf((float)cr, (float)-ci);   // conj(Z) * (-cos)
-            A[(int64_t)(n + w) * s + i] = cf((float)cr, (float)ci);  // (-cos) * Z
+    float2 *A = a32buf + mus[blockIdx.y].a32_off;
+    int b = wptr[w], e = wptr[w + 1];
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        double cr = 0, ci = 0;
+        for (int q = b; q < e; ++q) {
+            int r = wrow[q];
+            cx zi = z[(int64_t)r * n + i];
+            cr += -cv[r] * zi.re;
+            ci += -cv[r] * zi.im;
         }
-        for (int v = threadIdx.x; v < a.w; v += blockDim.x) {
-            double d = 0;
-            if (v == w)
-                for (int q = b; q < e; ++q) d += cv[wrow[q]] * cv[wrow[q]];
-            A[(int64_t)(n + w) * s + n + v] = cf((float)d, 0.f);
-        }
+        A[(int64_t)i * s + n + w] = cf((float)cr, (float)-ci);   // conj(Z) * (-cos)
+        A[(int64_t)(n + w) * s + i] = cf((float)cr, (float)ci);  // (-cos) * Z
     }
-    __syncthreads();
+    for (int v = threadIdx.x; v < a.w; v += blockDim.x) {
+        double d = 0;
+        if (v == w)
+            for (int q = b; q < e; ++q) d += cv[wrow[q]] * cv[wrow[q]];
+        A[(int64_t)(n + w) * s + n + v] = cf((float)d, 0.f);
+    }
+}
+
+// constraint rows (in row order) and lambda; one CTA per system
+__global__ void k_gram32_rest(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
+                              const MixedUnit *__restrict__ mus, const DevConRow *__restrict__ crows,
+                              float2 *a32buf) {
+    UnitDesc u = units[blockIdx.x];
+    AntDesc a = ants[u.ant];
+    int s = u.s;
+    float2 *A = a32buf + mus[blockIdx.x].a32_off;
     if (threadIdx.x == 0) {
         const DevConRow *cr = crows + a.crow_off;
         for (int q = 0; q < a.n_crow; ++q) {
@@ -707,7 +715,8 @@ __global__ void __launch_bounds__(256) k_gmres_ir(const UnitDesc *__restrict__ u
                                                   const DevConRow *__restrict__ crows, const cx *__restrict__ zbuf,
                                                   const cx *__restrict__ rhs, const double *__restrict__ cosv,
                                                   const float2 *__restrict__ a32buf, const int32_t *__restrict__ pivbuf,
-                                                  cx *xbuf, cx *vbuf, cx *wbuf, const int32_t *__restrict__ status) {
+                                                  cx *xbuf, cx *vbuf, cx *wbuf, const int32_t *__restrict__ status,
+                                                  int staged) {
     extern __shared__ unsigned char s_dyn[];
     __shared__ cx sH[(GM + 1) * GM];
     __shared__ double scs[GM];
@@ -742,7 +751,8 @@ __global__ void __launch_bounds__(256) k_gmres_ir(const UnitDesc *__restrict__ u
     g.t = W + 4 * s;
     cx *V = vbuf + mu.v_off;
     int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
-    cx *sv = reinterpret_cast<cx *>(s_dyn);
+    // staging vectors: shared memory when they fit, else the solve's work area
+    cx *sv = staged ? reinterpret_cast<cx *>(s_dyn) : W + 4 * s + g.rows;
     cx *stv = sv + s;
     float2 *sy = reinterpret_cast<float2 *>(stv + g.rows);
 
@@ -897,7 +907,7 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
         mu[i].iters = 0;
         mu[i].resid = 0.0;
         v += (int64_t)(GM + 1) * u.s;
-        wk += 4 * (int64_t)u.s + rows;
+        wk += 6 * (int64_t)u.s + 2 * (int64_t)rows;  // 4 vectors + rows, then the unstaged copies
     }
     // systems' descriptors index the factor through the first solve's entry
     std::vector<MixedUnit> sysmu(systems.size());
@@ -940,7 +950,7 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
                    const AntDesc *d_ants, const DevSeg *d_segs, const int4 *fill_tiles, int n_fill,
                    const int4 *gram_tiles, int n_gram, const int32_t *ibuf, const DevConRow *crows, cx *z,
                    const cx *rhs, const double *cosv, cx *x, int32_t *piv, int32_t *status, int max_s,
-                   bool do_fill, MixedMarks marks, cudaStream_t st) {
+                   bool do_fill, int max_w, MixedMarks marks, cudaStream_t st) {
     uint64_t L = 0;
     auto mark = [&](int k) {
         if (marks.ev) cudaEventRecord(marks.ev[k], st);
@@ -951,8 +961,12 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     }
     mark(0);
     if (n_gram > 0) k_gram32_zz<<<n_gram, 256, 0, st>>>(d_units, mw.smu, gram_tiles, z, mw.a32);
-    k_gram32_rest<<<nu, 256, 0, st>>>(d_units, d_ants, mw.smu, ibuf, crows, z, cosv, mw.a32);
-    L += 2;
+    {
+        dim3 g(max_w > 0 ? max_w : 1, nu);
+        k_gram32_ccols<<<g, 256, 0, st>>>(d_units, d_ants, mw.smu, ibuf, z, cosv, mw.a32);
+    }
+    k_gram32_rest<<<nu, 256, 0, st>>>(d_units, d_ants, mw.smu, crows, mw.a32);
+    L += 3;
     mark(1);
     static bool attr = false;
     if (!attr) {
@@ -980,10 +994,12 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     int max_rows = 0;
     for (size_t i = 0; i < mw.host.size(); ++i) max_rows = max_rows > mw.host[i].rows ? max_rows : mw.host[i].rows;
     size_t smem = sizeof(cx) * (size_t)(max_s + max_rows) + sizeof(float2) * (size_t)max_s;
+    int staged = smem <= 200 * 1024;
+    if (!staged) smem = 0;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_gmres_ir, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (ns > 0)
         k_gmres_ir<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x, mw.v,
-                                          mw.w, status);
+                                          mw.w, status, staged);
     ++L;
     mark(3);
     return L;

@@ -299,13 +299,16 @@ __global__ void __launch_bounds__(256) k_gram_zz(const UnitDesc *__restrict__ un
 // Part 2: the homogeneous columns N+w (M[r][N+w] = -cos_r for rows of wire
 // w, zero elsewhere; zero products change neither value nor sign of a sum
 // that starts at +0, so only the wire's rows are visited, in ascending r).
-// grid.x = unit, threads stride over i in [0, N] (i == N is the y column).
+// grid.x = wire column w, grid.y = unit; threads stride over i in [0, N]
+// (i == N is the y column).
 __global__ void k_gram_ccols(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
                              const int32_t *__restrict__ ibuf, const cx *__restrict__ zbuf,
                              const cx *__restrict__ rhs_buf, const double *__restrict__ cos_buf,
                              cx *abuf) {
-    UnitDesc u = units[blockIdx.x];
+    UnitDesc u = units[blockIdx.y];
     AntDesc a = ants[u.ant];
+    int w = blockIdx.x;
+    if (w >= a.w) return;
     int n = u.n, s = u.s, w1 = s + 1;
     const cx *z = zbuf + u.z_off;
     const cx *y = rhs_buf + u.rhs_off;
@@ -313,36 +316,34 @@ __global__ void k_gram_ccols(const UnitDesc *__restrict__ units, const AntDesc *
     const int32_t *wptr = ibuf + a.wptr_off;
     const int32_t *wrow = ibuf + a.wrow_off;
     cx *A = abuf + u.a_off;
-    for (int w = 0; w < a.w; ++w) {
-        int b = wptr[w], e = wptr[w + 1];
-        for (int i = threadIdx.x; i <= n; i += blockDim.x) {
-            cx col = cx_make(0.0, 0.0);  // A[i][N+w]  (i < N)
-            cx row = cx_make(0.0, 0.0);  // A[N+w][i]  (i < N), or A[N+w][S] for i == N
+    int b = wptr[w], e = wptr[w + 1];
+    for (int i = threadIdx.x; i <= n; i += blockDim.x) {
+        cx col = cx_make(0.0, 0.0);  // A[i][N+w]  (i < N)
+        cx row = cx_make(0.0, 0.0);  // A[N+w][i]  (i < N), or A[N+w][S] for i == N
+        for (int q = b; q < e; ++q) {
+            int r = wrow[q];
+            cx c = cx_make(-cv[r], 0.0);
+            cx zi = (i < n) ? z[(int64_t)r * n + i] : y[r];
+            if (i < n) col = cx_add(col, cx_conj_mul(zi, c));
+            row = cx_add(row, cx_conj_mul(c, zi));
+        }
+        if (i < n) {
+            A[(int64_t)i * w1 + n + w] = col;
+            A[(int64_t)(n + w) * w1 + i] = row;
+        } else {
+            A[(int64_t)(n + w) * w1 + s] = row;
+        }
+    }
+    // the W x W block row of this wire: cos^2 sum on the diagonal, exact zeros elsewhere
+    for (int v = threadIdx.x; v < a.w; v += blockDim.x) {
+        cx d = cx_make(0.0, 0.0);
+        if (v == w) {
             for (int q = b; q < e; ++q) {
-                int r = wrow[q];
-                cx c = cx_make(-cv[r], 0.0);
-                cx zi = (i < n) ? z[(int64_t)r * n + i] : y[r];
-                if (i < n) col = cx_add(col, cx_conj_mul(zi, c));
-                row = cx_add(row, cx_conj_mul(c, zi));
-            }
-            if (i < n) {
-                A[(int64_t)i * w1 + n + w] = col;
-                A[(int64_t)(n + w) * w1 + i] = row;
-            } else {
-                A[(int64_t)(n + w) * w1 + s] = row;
+                cx c = cx_make(-cv[wrow[q]], 0.0);
+                d = cx_add(d, cx_conj_mul(c, c));
             }
         }
-        // the W x W block: diagonal sum of cos^2 terms, exact zeros elsewhere
-        for (int v = threadIdx.x; v < a.w; v += blockDim.x) {
-            cx d = cx_make(0.0, 0.0);
-            if (v == w) {
-                for (int q = b; q < e; ++q) {
-                    cx c = cx_make(-cv[wrow[q]], 0.0);
-                    d = cx_add(d, cx_conj_mul(c, c));
-                }
-            }
-            A[(int64_t)(n + w) * w1 + n + v] = d;
-        }
+        A[(int64_t)(n + w) * w1 + n + v] = d;
     }
 }
 
@@ -857,13 +858,14 @@ void launch_fill_exact_flat(const DevSeg *segs, int n, double k, int ground, cx 
     dim3 g((n + 15) / 16, (n + 15) / 16);
     if (n > 0) k_fill_exact_flat<<<g, 256, 0, st>>>(segs, n, k, ground, z);
 }
-void launch_gram_exact(const UnitDesc *units, int nu, const AntDesc *ants, const int4 *gtiles,
+void launch_gram_exact(const UnitDesc *units, int nu, int max_w, const AntDesc *ants, const int4 *gtiles,
                        int ngtiles, const int32_t *ibuf, const DevConstraint *cons,
                        const int32_t *codes, const cx *z, const cx *rhs, const double *cosv, cx *A,
                        cudaStream_t st) {
     if (ngtiles > 0) k_gram_zz<<<ngtiles, 256, 0, st>>>(units, gtiles, z, rhs, A);
     if (nu > 0) {
-        k_gram_ccols<<<nu, 256, 0, st>>>(units, ants, ibuf, z, rhs, cosv, A);
+        dim3 g(max_w > 0 ? max_w : 1, nu);
+        k_gram_ccols<<<g, 256, 0, st>>>(units, ants, ibuf, z, rhs, cosv, A);
         k_gram_finish<<<nu, 256, 0, st>>>(units, ants, cons, codes, A);
     }
 }

@@ -157,3 +157,14 @@ def test_mixed_extra_right_hand_sides(acc):
     errs = {}
     for r, src in enumerate(srcs):
         _check(res, b, r, w, O.sources_array([src]), 1, 24e6, None, errs)
+
+
+def test_mixed_junctioned_mesh(acc):
+    import bench
+
+    wl, src, f = bench.mesh_workload(6)
+    w, s = O.wires_array(wl), O.sources_array(src)
+    b = acc.HallenBatch([acc.Antenna(w.view(acc.WIRE_DTYPE), s.view(acc.SOURCE_DTYPE), [f], 1, None)],
+                        precision=acc.PRECISION_MIXED)
+    res = b.solve()
+    _check(res, b, 0, w, s, 1, f, None, {})

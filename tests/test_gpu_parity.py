@@ -303,3 +303,28 @@ def test_extra_right_hand_sides_reuse_the_factor_bit_exactly(acc):
                 assert np.array_equal(rm.pattern[u], ro.pattern[0])
                 _check_unit(acc, one, ro, 0, w, O.sources_array([src]), ground, f,
                             O.rp_card_points(9, 3, 0, 0, 10, 60))
+
+
+@pytest.mark.parametrize("cells", [3, 6])
+def test_junctioned_mesh_over_ground(acc, cells):
+    """The mesh workload at small size: every interior node joins four wire
+    ends (6 pairwise junction rows each), GN 1 images, bit-exact solve given
+    the oracle's Z, and end-to-end parity."""
+    import bench
+
+    wl, src, f = bench.mesh_workload(cells)
+    w = O.wires_array(wl)
+    s = O.sources_array(src)
+    batch = acc.HallenBatch([acc.Antenna(w.view(acc.WIRE_DTYPE), s.view(acc.SOURCE_DTYPE), [f], 1,
+                                         (10, 4, 0.0, 0.0, 10.0, 90.0))])
+    res = batch.solve()
+    _check_unit(acc, batch, res, 0, w, s, 1, f, O.rp_card_points(10, 4, 0, 0, 10, 90))
+    segs = O.build_geometry(w)
+    rhs, cosv = O.hallen_rhs(segs, f, s)
+    z = O.assemble_z(segs, f, 1)
+    m = O.merge_collinear(segs)
+    ja, jb, js = O.cli_junctions(segs, m)
+    x0, p0 = O.solve_hallen(z, rhs, cosv, m, ja, jb, js)
+    x1, p1 = acc.solve_hallen(z, rhs, cosv, m, list(zip(ja, jb, js)), return_pivots=True)
+    assert np.array_equal(p0, p1)
+    assert np.array_equal(x0.view(np.uint64), x1.view(np.uint64))
