@@ -668,29 +668,65 @@ __global__ void __launch_bounds__(256) k_trailing(const UnitDesc *__restrict__ u
 }
 
 // Back substitution x_i = (b_i - sum_{j>i} a_ij x_j) / a_ii, j ascending.
-// One warp per unit.  The products a_ij x_j of a 32-wide chunk are formed
-// in parallel (one per lane, the next chunk's loads issued before the
-// current chunk is consumed); every lane then runs the same sequential
-// subtraction chain over the chunk through shuffles, so the order of the
-// subtractions -- and the result -- is the reference's.
-__global__ void k_backsub(const UnitDesc *__restrict__ units, const cx *__restrict__ abuf, cx *xbuf,
-                          const int32_t *__restrict__ status) {
-    extern __shared__ cx s_x[];
-    int ui = blockIdx.x;
-    UnitDesc u = units[ui];
-    if (status[ui] != 0) return;
-    int s = u.s, w1 = s + 1;
-    const cx *A = abuf + u.a_off;
-    int lane = threadIdx.x;
+// One warp per unit.  The subtraction chain is sequential in the reference
+// and stays sequential here; what is parallel is the memory stream.  The
+// products a_ij x_j of a 32-wide chunk are formed one per lane, every lane
+// runs the same in-order chain over the chunk through shuffles, and the U
+// entries of the next BS_DEPTH chunks (in exactly the order the chain will
+// consume them, across row boundaries) are already in flight while a chunk
+// is consumed.  b_i and a_ii are fetched one row ahead.  x lives in shared
+// memory and may alias b: b_i is read before x_i is written, and only
+// x_j, j > i, is read after.
+constexpr int BS_DEPTH = 8;
+constexpr size_t BS_SMEM_MAX = 220 * 1024;  // x staged in shared memory up to S = 14080
+
+struct ChunkCursor {  // (row i, first column j0) of the next 32-wide chunk
+    int i, j0;
+    __device__ void next(int s) {
+        j0 += 32;
+        while (i >= 0 && j0 >= s) {
+            --i;
+            j0 = i + 1;
+        }
+    }
+};
+
+__device__ __forceinline__ cx ld_cx(const cx *p) { return *p; }
+
+__device__ __forceinline__ void backsub_rows(const cx *A, int s, int w1, const cx *bv, int64_t b_stride,
+                                             cx *s_x) {
+    int lane = threadIdx.x & 31;
+    ChunkCursor pf{s - 1, s - 32};  // positioned before the first chunk
+    pf.next(s);
+    cx u[BS_DEPTH];
+#pragma unroll
+    for (int q = 0; q < BS_DEPTH; ++q) {
+        int j = pf.j0 + lane;
+        u[q] = (pf.i >= 0 && j < s) ? A[(int64_t)pf.i * w1 + j] : cx_make(0.0, 0.0);
+        if (pf.i >= 0) pf.next(s);
+    }
+    cx b_next = ld_cx(bv + (int64_t)(s - 1) * b_stride);
+    cx d_next = A[(int64_t)(s - 1) * w1 + (s - 1)];
     for (int i = s - 1; i >= 0; --i) {
-        const cx *row = A + (int64_t)i * w1;
-        cx sum = row[s];
-        int j = i + 1 + lane;
-        cx p = (j < s) ? cx_mul(row[j], s_x[j]) : cx_make(0.0, 0.0);
+        cx sum = b_next, di = d_next;
+        if (i > 0) {
+            b_next = ld_cx(bv + (int64_t)(i - 1) * b_stride);
+            d_next = A[(int64_t)(i - 1) * w1 + (i - 1)];
+        }
         for (int j0 = i + 1; j0 < s; j0 += 32) {
-            int jn = j0 + 32 + lane;
-            cx pn = (jn < s) ? cx_mul(row[jn], s_x[jn]) : cx_make(0.0, 0.0);
-            int cnt = min(32, s - j0);
+            cx uv = u[0];
+#pragma unroll
+            for (int q = 0; q < BS_DEPTH - 1; ++q) u[q] = u[q + 1];
+            {
+                int j = pf.j0 + lane;
+                u[BS_DEPTH - 1] = (pf.i >= 0 && j < s) ? A[(int64_t)pf.i * w1 + j] : cx_make(0.0, 0.0);
+                if (pf.i >= 0) pf.next(s);
+            }
+            // Lanes past the row end contribute +0: sum - (+0) == sum
+            // exactly for every sum (-0, infinities and NaN included), so
+            // the chain needs no predicate.
+            int j = j0 + lane;
+            cx p = (j < s) ? cx_mul(uv, s_x[j]) : cx_make(0.0, 0.0);
             double pr[32], pim[32];
 #pragma unroll
             for (int q = 0; q < 32; ++q) {
@@ -698,15 +734,29 @@ __global__ void k_backsub(const UnitDesc *__restrict__ units, const cx *__restri
                 pim[q] = __shfl_sync(0xffffffffu, p.im, q);
             }
 #pragma unroll
-            for (int q = 0; q < 32; ++q)
-                if (q < cnt) sum = cx_sub(sum, cx_make(pr[q], pim[q]));
-            p = pn;
+            for (int q = 0; q < 32; ++q) sum = cx_sub(sum, cx_make(pr[q], pim[q]));
         }
-        cx xi = cx_div(sum, row[i]);
+        cx xi = cx_div(sum, di);
+        __syncwarp();
         if (lane == 0) s_x[i] = xi;
         __syncwarp();
     }
-    for (int i = lane; i < s; i += 32) xbuf[u.x_off + i] = s_x[i];
+}
+
+// staged == 0 (systems whose x does not fit in shared memory): x is built
+// in place in global memory; __syncwarp orders the warp's accesses there too.
+__global__ void k_backsub(const UnitDesc *__restrict__ units, const cx *__restrict__ abuf, cx *xbuf,
+                          const int32_t *__restrict__ status, int staged) {
+    extern __shared__ cx s_xs[];
+    int ui = blockIdx.x;
+    UnitDesc u = units[ui];
+    if (status[ui] != 0) return;
+    int s = u.s, w1 = s + 1;
+    const cx *A = abuf + u.a_off;
+    cx *xs = staged ? s_xs : xbuf + u.x_off;
+    backsub_rows(A, s, w1, A + s, w1, xs);
+    if (staged)
+        for (int i = threadIdx.x; i < s; i += 32) xbuf[u.x_off + i] = s_xs[i];
 }
 
 // Feedpoint rows: v_source = v_vec[idx] * dl, Zin = v_source / I[idx] when
@@ -783,16 +833,18 @@ __global__ void k_extra_rhs_b(const UnitDesc *__restrict__ solves, const AntDesc
 
 __global__ void k_extra_rhs_solve(const UnitDesc *__restrict__ solves, const cx *__restrict__ abuf,
                                   const int32_t *__restrict__ piv_buf, cx *xbuf,
-                                  const int32_t *__restrict__ status) {
-    extern __shared__ cx s_b[];
+                                  const int32_t *__restrict__ status, int staged) {
+    extern __shared__ cx s_bs[];
     UnitDesc u = solves[blockIdx.x];
     if (u.rhs == 0 || status[u.sys] != 0) return;
     int s = u.s, w1 = s + 1;
     const cx *A = abuf + u.a_off;
     const int32_t *piv = piv_buf + u.piv_off;
     cx *x = xbuf + u.x_off;
+    cx *s_b = staged ? s_bs : x;  // unstaged: work in place in global memory
     int lane = threadIdx.x;
-    for (int i = lane; i < s; i += 32) s_b[i] = x[i];
+    if (staged)
+        for (int i = lane; i < s; i += 32) s_b[i] = x[i];
     __syncwarp();
     if (lane == 0)
         for (int c = 0; c < s; ++c) {
@@ -810,33 +862,10 @@ __global__ void k_extra_rhs_solve(const UnitDesc *__restrict__ solves, const cx 
         for (int r = c + 1 + lane; r < s; r += 32) s_b[r] = cx_sub(s_b[r], cx_mul(A[(int64_t)r * w1 + c], bc));
         __syncwarp();
     }
-    // back substitution, j ascending, as k_backsub
-    for (int i = s - 1; i >= 0; --i) {
-        const cx *row = A + (int64_t)i * w1;
-        cx sum = s_b[i];
-        int j = i + 1 + lane;
-        cx p = (j < s) ? cx_mul(row[j], s_b[j]) : cx_make(0.0, 0.0);
-        for (int j0 = i + 1; j0 < s; j0 += 32) {
-            int jn = j0 + 32 + lane;
-            cx pn = (jn < s) ? cx_mul(row[jn], s_b[jn]) : cx_make(0.0, 0.0);
-            int cnt = min(32, s - j0);
-            double pr[32], pim[32];
-#pragma unroll
-            for (int q = 0; q < 32; ++q) {
-                pr[q] = __shfl_sync(0xffffffffu, p.re, q);
-                pim[q] = __shfl_sync(0xffffffffu, p.im, q);
-            }
-#pragma unroll
-            for (int q = 0; q < 32; ++q)
-                if (q < cnt) sum = cx_sub(sum, cx_make(pr[q], pim[q]));
-            p = pn;
-        }
-        cx xi = cx_div(sum, row[i]);
-        __syncwarp();
-        if (lane == 0) s_b[i] = xi;
-        __syncwarp();
-    }
-    for (int i = lane; i < s; i += 32) x[i] = s_b[i];
+    // back substitution, j ascending, as k_backsub (x overwrites b in place)
+    backsub_rows(A, s, w1, s_b, 1, s_b);
+    if (staged)
+        for (int i = lane; i < s; i += 32) x[i] = s_b[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -906,9 +935,11 @@ void launch_factor_exact(const UnitDesc *units, int nu, int max_s, int max_trail
 void launch_backsub(const UnitDesc *units, int nu, int max_s, const cx *A, cx *x,
                     const int32_t *status, cudaStream_t st) {
     size_t smem = sizeof(cx) * (size_t)max_s;
+    int staged = smem <= BS_SMEM_MAX;
+    if (!staged) smem = 0;
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_backsub, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (nu > 0) k_backsub<<<nu, 32, smem, st>>>(units, A, x, status);
+    if (nu > 0) k_backsub<<<nu, 32, smem, st>>>(units, A, x, status, staged);
 }
 void launch_feedpoints(const UnitDesc *solves, int ns, const AntDesc *ants, const DevSeg *segs,
                        const int32_t *ibuf, const DevFeed *feeds, const cx *x, const int32_t *status,
@@ -923,9 +954,11 @@ void launch_extra_rhs_exact(const UnitDesc *solves, int ns, int max_s, const Ant
     dim3 g((max_s + 127) / 128, ns);
     k_extra_rhs_b<<<g, 128, 0, st>>>(solves, ants, ibuf, z, rhs, cosv, x);
     size_t smem = sizeof(cx) * (size_t)max_s;
+    int staged = smem <= BS_SMEM_MAX;
+    if (!staged) smem = 0;
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_extra_rhs_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_extra_rhs_solve<<<ns, 32, smem, st>>>(solves, A, piv, x, status);
+    k_extra_rhs_solve<<<ns, 32, smem, st>>>(solves, A, piv, x, status, staged);
 }
 
 }  // namespace fnec
