@@ -372,6 +372,8 @@ struct fnec_batch {
     double *d_feed_out = nullptr, *d_fld = nullptr, *d_partials = nullptr, *d_pat = nullptr,
            *d_total = nullptr;
     MixedWork mixed;
+    GridPlan grid;
+    std::vector<int32_t> grid_order;
     size_t dev_bytes = 0;
     std::vector<void *> allocs;
     // packed input arena: one pinned host buffer mirrored by one device buffer
@@ -706,6 +708,26 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
     DA(d_partials, (int64_t)b->ff_blocks * (int64_t)b->solves.size());
     DA(d_pat, PAT_STRIDE * b->pat_el);
     DA(d_total, b->solves.size());
+    {
+        // grid-wide panels: units by s, tallest first
+        std::vector<int32_t> &ord = b->grid_order;
+        ord.resize(nu);
+        for (int i = 0; i < nu; ++i) ord[i] = i;
+        std::stable_sort(ord.begin(), ord.end(), [&](int32_t x, int32_t y) { return b->units[x].s > b->units[y].s; });
+        b->grid.s_desc.resize(nu);
+        for (int i = 0; i < nu; ++i) b->grid.s_desc[i] = b->units[ord[i]].s;
+        b->grid.steps = (b->max_s + 31) / 32;
+        cudaDeviceGetAttribute(&b->grid.sms, cudaDevAttrMultiProcessorCount, ctx->device);
+        if (b->max_s > 400) {  // some panel may outgrow one CTA's shared memory
+            unsigned char *xg = nullptr, *sy = nullptr;
+            if (e == cudaSuccess) e = dalloc(b, &b->grid.d_order, (size_t)nu);
+            if (e == cudaSuccess) e = up(b, b->grid.d_order, ord);
+            if (e == cudaSuccess) e = dalloc(b, &xg, grid_xchg_bytes());
+            if (e == cudaSuccess) e = dalloc(b, &sy, grid_sync_bytes(b->grid.steps));
+            b->grid.d_xchg = xg;
+            b->grid.d_sync = sy;
+        }
+    }
 #undef DA
     b->out_bytes = sizeof(cx) * (size_t)b->x_el + sizeof(double) * 7 * (size_t)b->feed_rows +
                    sizeof(double) * PAT_STRIDE * (size_t)b->pat_el +
@@ -934,7 +956,7 @@ int fnec_batch_run(fnec_batch *b) {
         L += run_mixed(b->mixed, b->d_units, nu, b->d_solves, ns, b->d_ants, b->d_segs, b->d_fill_tiles,
                        (int)b->fill_tiles.size(), b->d_gram_tiles, (int)b->gram_tiles.size(), b->d_ibuf,
                        b->d_crows, b->d_z, b->d_rhs, b->d_cos, b->d_x, b->d_piv, b->d_status, b->max_s,
-                       b->z_given.empty(), b->max_w, mm, st);
+                       b->z_given.empty(), b->max_w, b->grid, mm, st);
     } else {
         if (b->z_given.empty()) {
             launch_fill_exact(b->d_units, b->d_ants, b->d_segs, b->d_fill_tiles, (int)b->fill_tiles.size(),
@@ -945,7 +967,7 @@ int fnec_batch_run(fnec_batch *b) {
         launch_gram_exact(b->d_units, nu, b->max_w, b->d_ants, b->d_gram_tiles, (int)b->gram_tiles.size(), b->d_ibuf,
                           b->d_cons, b->d_codes, b->d_z, b->d_rhs, b->d_cos, b->d_a, st);
         mark(4);
-        launch_factor_exact(b->d_units, nu, b->max_s, 0, b->d_a, b->d_piv, b->d_status, st);
+        launch_factor_exact(b->d_units, nu, b->max_s, b->grid, b->d_a, b->d_piv, b->d_status, st);
         mark(5);
         launch_backsub(b->d_units, nu, b->max_s, b->d_a, b->d_x, b->d_status, st);
         if (b->max_rhs > 1) {

@@ -2,12 +2,31 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <vector>
+
 #include "fnec_math.cuh"
 #include "fnec_types.h"
 
 namespace fnec {
 
 constexpr int PAT_STRIDE = 6;  // gain_total, gain_theta, gain_phi, axial_ratio, u_theta, u_phi
+
+// Units whose panels are too tall for one CTA's shared memory are factored
+// by the grid-wide panel kernel (fnec_grid.cuh).  Built once per batch.
+struct GridPlan {
+    int32_t *d_order = nullptr;  // unit indices, s descending
+    std::vector<int> s_desc;     // their s (host copy)
+    void *d_xchg = nullptr;      // GRID_PANEL_MAX_UNITS exchange areas (complex128-sized)
+    void *d_sync = nullptr;      // GridSync words: panel steps x GRID_PANEL_MAX_UNITS
+    int steps = 0;               // panel steps the sync words cover
+    int sms = 0;                 // SMs of the device
+};
+size_t grid_xchg_bytes();        // bytes of d_xchg
+size_t grid_sync_bytes(int steps);
+// How the panel at column c0 is factored (fnec_plain.cu): the number of
+// units that take the grid-wide kernel (0 none, -1 infeasible) and its shape.
+int plan_grid_panel(const GridPlan &gp, int c0, int thr_rows, int pnb, size_t elem, const void *kernel,
+                    int *G_out, size_t *smem_out);
 
 // fnec_plain.cu
 void launch_expand_segments(const DevWire *wires, int nw, DevSeg *segs, cudaStream_t st);
@@ -21,7 +40,7 @@ void launch_gram_exact(const UnitDesc *units, int nu, int max_w, const AntDesc *
                        int ngtiles, const int32_t *ibuf, const DevConstraint *cons,
                        const int32_t *codes, const cx *z, const cx *rhs, const double *cosv, cx *A,
                        cudaStream_t st);
-void launch_factor_exact(const UnitDesc *units, int nu, int max_s, int max_trailing_tiles, cx *A,
+void launch_factor_exact(const UnitDesc *units, int nu, int max_s, const GridPlan &gp, cx *A,
                          int32_t *piv, int32_t *status, cudaStream_t st);
 void launch_backsub(const UnitDesc *units, int nu, int max_s, const cx *A, cx *x,
                     const int32_t *status, cudaStream_t st);

@@ -19,8 +19,11 @@
 // a handful of iterations because the FP32 factor's errors concentrate in
 // few directions.  The error against the FP64 oracle is reported per unit
 // (iterations and final residual are kept for inspection).
+#include <algorithm>
+#include <climits>
 #include <vector>
 
+#include "fnec_grid.cuh"
 #include "fnec_mixed.h"
 
 namespace fnec {
@@ -273,7 +276,8 @@ __device__ __forceinline__ void piv_better32(float &bv, int &bi, float v, int i)
 }
 
 __global__ void __launch_bounds__(256) k_panel32(const UnitDesc *__restrict__ units, const MixedUnit *__restrict__ mus,
-                                                 int c0, float2 *a32buf, int32_t *piv_buf, int32_t *status) {
+                                                 int c0, float2 *a32buf, int32_t *piv_buf, int32_t *status,
+                                                 int skip_m) {
     __shared__ float s_v[8];
     __shared__ int s_i[8];
     __shared__ int s_p;
@@ -281,7 +285,7 @@ __global__ void __launch_bounds__(256) k_panel32(const UnitDesc *__restrict__ un
     int ui = blockIdx.x;
     UnitDesc u = units[ui];
     int s = u.s;
-    if (c0 >= s || status[ui] != 0) return;
+    if (c0 >= s || s - c0 > skip_m || status[ui] != 0) return;  // skip_m: taller panels go grid-wide
     float2 *A = a32buf + mus[ui].a32_off;
     int32_t *piv = piv_buf + u.piv_off;
     int nb = min(MNB, s - c0);
@@ -343,7 +347,7 @@ constexpr int PANEL32_SMEM_MAX = 200 * 1024;
 
 __global__ void __launch_bounds__(256) k_panel32_smem(const UnitDesc *__restrict__ units,
                                                       const MixedUnit *__restrict__ mus, int c0, float2 *a32buf,
-                                                      int32_t *piv_buf, int32_t *status) {
+                                                      int32_t *piv_buf, int32_t *status, int skip_m) {
     extern __shared__ float2 s_pan32[];
     __shared__ float s_v[8];
     __shared__ int s_i[8];
@@ -351,7 +355,7 @@ __global__ void __launch_bounds__(256) k_panel32_smem(const UnitDesc *__restrict
     int ui = blockIdx.x;
     UnitDesc u = units[ui];
     int s = u.s;
-    if (c0 >= s || status[ui] != 0) return;
+    if (c0 >= s || s - c0 > skip_m || status[ui] != 0) return;  // skip_m: taller panels go grid-wide
     float2 *A = a32buf + mus[ui].a32_off;
     int32_t *piv = piv_buf + u.piv_off;
     int nb = min(MNB, s - c0), m = s - c0;
@@ -419,6 +423,33 @@ __global__ void __launch_bounds__(256) k_panel32_smem(const UnitDesc *__restrict
 // Row swaps on every column outside the panel, then U12 for the trailing
 // ones; 64 columns per CTA with their panel rows and the L block staged in
 // shared memory.
+// Panels taller than one CTA's shared memory, over many CTAs (fnec_grid.cuh).
+struct MixedPanelOps {
+    using E = float2;
+    using V = float;
+    static constexpr float V_NONE = -1.f;
+    __device__ static float key(float2 a) { return a.x * a.x + a.y * a.y; }
+    __device__ static void better(float &bv, int &bi, float v, int i) { piv_better32(bv, bi, v, i); }
+    __device__ static float2 div(float2 a, float2 b) { return cf_div(a, b); }
+    __device__ static float2 sub_mul(float2 acc, float2 f, float2 p) { return cf_sub(acc, cf_mul(f, p)); }
+    __device__ static bool singular(float v) { return !(v > 0.f); }
+    __device__ static float2 load_cg(const float2 *p) { return __ldcg(p); }
+};
+
+__global__ void __launch_bounds__(256) k_panel32_grid(const UnitDesc *__restrict__ units,
+                                                      const MixedUnit *__restrict__ mus,
+                                                      const int32_t *__restrict__ order, int c0, float2 *a32buf,
+                                                      int32_t *piv_buf, int32_t *status, PanelXchg<float2> *xg,
+                                                      GridSync *gs) {
+    extern __shared__ float2 s_gpan32[];
+    int ui = order[blockIdx.y];
+    UnitDesc u = units[ui];
+    if (status[ui] != 0) return;
+    panel_grid_body<MixedPanelOps, MNB, 256>(a32buf + mus[ui].a32_off, (int64_t)u.s, u.s, c0, piv_buf + u.piv_off,
+                                             &status[ui], xg + blockIdx.y, gs + blockIdx.y, (int)gridDim.x,
+                                             (int)blockIdx.x, s_gpan32);
+}
+
 __global__ void __launch_bounds__(64) k_swap_u12_32(const UnitDesc *__restrict__ units,
                                                     const MixedUnit *__restrict__ mus, int c0, float2 *a32buf,
                                                     const int32_t *__restrict__ piv_buf,
@@ -950,7 +981,7 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
                    const AntDesc *d_ants, const DevSeg *d_segs, const int4 *fill_tiles, int n_fill,
                    const int4 *gram_tiles, int n_gram, const int32_t *ibuf, const DevConRow *crows, cx *z,
                    const cx *rhs, const double *cosv, cx *x, int32_t *piv, int32_t *status, int max_s,
-                   bool do_fill, int max_w, MixedMarks marks, cudaStream_t st) {
+                   bool do_fill, int max_w, const GridPlan &gp, MixedMarks marks, cudaStream_t st) {
     uint64_t L = 0;
     auto mark = [&](int k) {
         if (marks.ev) cudaEventRecord(marks.ev[k], st);
@@ -968,17 +999,44 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     k_gram32_rest<<<nu, 256, 0, st>>>(d_units, d_ants, mw.smu, crows, mw.a32);
     L += 3;
     mark(1);
-    static bool attr = false;
+    static bool attr = false, attr_grid = false;
     if (!attr) {
         cudaFuncSetAttribute(k_panel32_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, PANEL32_SMEM_MAX);
         attr = true;
     }
+    if (!attr_grid) {
+        cudaFuncSetAttribute(k_panel32_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
+        attr_grid = true;
+    }
+    const int thr_rows = PANEL32_SMEM_MAX / (int)(MNB * sizeof(float2));
+    if (gp.d_sync) cudaMemsetAsync(gp.d_sync, 0, grid_sync_bytes(gp.steps), st);
     for (int c0 = 0; c0 < max_s; c0 += MNB) {
-        size_t pan = sizeof(float2) * (size_t)(max_s - c0) * MNB;
-        if (pan <= (size_t)PANEL32_SMEM_MAX)
-            k_panel32_smem<<<nu, 256, pan, st>>>(d_units, mw.smu, c0, mw.a32, piv, status);
-        else
-            k_panel32<<<nu, 256, 0, st>>>(d_units, mw.smu, c0, mw.a32, piv, status);
+        int G = 0;
+        size_t gsm = 0;
+        int nl = plan_grid_panel(gp, c0, thr_rows, MNB, sizeof(float2), (const void *)k_panel32_grid, &G, &gsm);
+        if (nl > 0) {
+            PanelXchg<float2> *xg = static_cast<PanelXchg<float2> *>(gp.d_xchg);
+            GridSync *gs = static_cast<GridSync *>(gp.d_sync) + (size_t)(c0 / MNB) * GRID_PANEL_MAX_UNITS;
+            const int32_t *ord = gp.d_order;
+            const MixedUnit *smu = mw.smu;
+            float2 *a32 = mw.a32;
+            void *args[] = {(void *)&d_units, (void *)&smu, (void *)&ord, (void *)&c0, (void *)&a32,
+                            (void *)&piv, (void *)&status, (void *)&xg, (void *)&gs};
+            if (cudaLaunchCooperativeKernel((const void *)k_panel32_grid, dim3(G, nl), dim3(256), args, gsm, st) ==
+                cudaSuccess) {
+                int m_rest = std::min(max_s - c0, thr_rows);
+                k_panel32_smem<<<nu, 256, sizeof(float2) * (size_t)m_rest * MNB, st>>>(d_units, mw.smu, c0, mw.a32,
+                                                                                       piv, status, thr_rows);
+            } else {
+                (void)cudaGetLastError();
+                k_panel32<<<nu, 256, 0, st>>>(d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX);
+            }
+        } else if (nl == 0) {
+            size_t pan = sizeof(float2) * (size_t)(max_s - c0) * MNB;
+            k_panel32_smem<<<nu, 256, pan, st>>>(d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX);
+        } else {
+            k_panel32<<<nu, 256, 0, st>>>(d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX);
+        }
         dim3 g1((max_s + 63) / 64, nu);  // every column outside the panel
         k_swap_u12_32<<<g1, 64, 0, st>>>(d_units, mw.smu, c0, mw.a32, piv, status);
         int rows = max_s - (c0 + MNB);

@@ -16,10 +16,12 @@
 //   k_gram_ccols       linear.rs:765-780       the -cos(k s) columns (sparse)
 //   k_gram_finish      linear.rs:757-785       constraint rows, then +1e-8 I
 //   k_panel            linear.rs:1343-1370     NB columns, one CTA per unit
+//   k_panel_grid       linear.rs:1343-1370     NB columns of a tall panel, many CTAs
 //   k_swap_u12         linear.rs:1358-1369     deferred swaps + U block row
 //   k_trailing         linear.rs:1362-1369     A22 -= L21 U12, 64x64 tiles
 //   k_backsub          linear.rs:1372-1381     one warp per unit
 //   k_feedpoints       solve_session.rs:846-947
+#include "fnec_grid.cuh"
 #include "fnec_kernels.h"
 #include "fnec_math.cuh"
 
@@ -397,7 +399,7 @@ __device__ __forceinline__ void piv_better(double &bv, int &bi, double v, int i)
 }
 
 __global__ void __launch_bounds__(256) k_panel(const UnitDesc *__restrict__ units, int c0,
-                                               cx *abuf, int32_t *piv_buf, int32_t *status) {
+                                               cx *abuf, int32_t *piv_buf, int32_t *status, int skip_m) {
     __shared__ double s_v[8];
     __shared__ int s_i[8];
     __shared__ int s_p;
@@ -405,7 +407,7 @@ __global__ void __launch_bounds__(256) k_panel(const UnitDesc *__restrict__ unit
     int ui = blockIdx.x;
     UnitDesc u = units[ui];
     int s = u.s;
-    if (c0 >= s || status[ui] != 0) return;
+    if (c0 >= s || s - c0 > skip_m || status[ui] != 0) return;  // skip_m: taller panels go grid-wide
     int w1 = s + 1;
     cx *A = abuf + u.a_off;
     int32_t *piv = piv_buf + u.piv_off;
@@ -471,7 +473,7 @@ __global__ void __launch_bounds__(256) k_panel(const UnitDesc *__restrict__ unit
 constexpr int PANEL_SMEM_MAX = 200 * 1024;
 
 __global__ void __launch_bounds__(256) k_panel_smem(const UnitDesc *__restrict__ units, int c0, cx *abuf,
-                                                    int32_t *piv_buf, int32_t *status) {
+                                                    int32_t *piv_buf, int32_t *status, int skip_m) {
     extern __shared__ cx s_pan[];  // [m][NB], m = s - c0
     __shared__ double s_v[8];
     __shared__ int s_i[8];
@@ -479,7 +481,7 @@ __global__ void __launch_bounds__(256) k_panel_smem(const UnitDesc *__restrict__
     int ui = blockIdx.x;
     UnitDesc u = units[ui];
     int s = u.s;
-    if (c0 >= s || status[ui] != 0) return;
+    if (c0 >= s || s - c0 > skip_m || status[ui] != 0) return;  // skip_m: taller panels go grid-wide
     int w1 = s + 1;
     cx *A = abuf + u.a_off;
     int32_t *piv = piv_buf + u.piv_off;
@@ -541,6 +543,37 @@ __global__ void __launch_bounds__(256) k_panel_smem(const UnitDesc *__restrict__
         int rr = e / nb, q = e % nb;
         A[(int64_t)(c0 + rr) * w1 + c0 + q] = s_pan[rr * NB + q];
     }
+}
+
+// Panels taller than one CTA's shared memory: the grid-wide panel of
+// fnec_grid.cuh over gridDim.x CTAs per unit (gridDim.y units, the tallest
+// first), launched cooperatively.  Bit-identical to k_panel.
+struct ExactPanelOps {
+    using E = cx;
+    using V = double;
+    static constexpr double V_NONE = -1.0;
+    __device__ static double key(cx a) { return cx_norm(a); }
+    __device__ static void better(double &bv, int &bi, double v, int i) { piv_better(bv, bi, v, i); }
+    __device__ static cx div(cx a, cx b) { return cx_div(a, b); }
+    __device__ static cx sub_mul(cx acc, cx f, cx p) { return cx_sub(acc, cx_mul(f, p)); }
+    __device__ static bool singular(double v) { return v < 1e-30; }  // linear.rs:1354
+    __device__ static cx load_cg(const cx *p) {
+        double2 d = __ldcg(reinterpret_cast<const double2 *>(p));
+        return cx_make(d.x, d.y);
+    }
+};
+
+__global__ void __launch_bounds__(256) k_panel_grid(const UnitDesc *__restrict__ units,
+                                                    const int32_t *__restrict__ order, int c0, cx *abuf,
+                                                    int32_t *piv_buf, int32_t *status, PanelXchg<cx> *xg,
+                                                    GridSync *gs) {
+    extern __shared__ cx s_gpan[];
+    int ui = order[blockIdx.y];
+    UnitDesc u = units[ui];
+    if (status[ui] != 0) return;
+    panel_grid_body<ExactPanelOps, NB, 256>(abuf + u.a_off, (int64_t)u.s + 1, u.s, c0, piv_buf + u.piv_off,
+                                            &status[ui], xg + blockIdx.y, gs + blockIdx.y, (int)gridDim.x,
+                                            (int)blockIdx.x, s_gpan);
 }
 
 // Deferred swaps and the U12 block row.  A CTA of 64 threads owns 64
@@ -900,21 +933,77 @@ void launch_gram_exact(const UnitDesc *units, int nu, int max_w, const AntDesc *
 }
 constexpr size_t TRAILING_SMEM = sizeof(cx) * (64 * (NB + 1) + NB * 64);
 
-void launch_factor_exact(const UnitDesc *units, int nu, int max_s, int max_trailing_tiles, cx *A,
+size_t grid_xchg_bytes() { return sizeof(PanelXchg<cx>) * GRID_PANEL_MAX_UNITS; }
+size_t grid_sync_bytes(int steps) { return sizeof(GridSync) * GRID_PANEL_MAX_UNITS * (size_t)(steps > 0 ? steps : 1); }
+
+// Chooses how the panel at column c0 is factored.  Units whose panel
+// (s - c0 rows) exceeds one CTA's shared memory (thr_rows) go to the
+// grid-wide kernel when they are few enough to be co-resident; the rest use
+// the one-CTA shared-memory kernel.  Returns the number of grid units
+// (0: none; -1: not possible, every unit takes the one-CTA global kernel)
+// and the CTAs per grid unit and their shared memory.
+int plan_grid_panel(const GridPlan &gp, int c0, int thr_rows, int pnb, size_t elem, const void *kernel,
+                    int *G_out, size_t *smem_out) {
+    int nl = 0;
+    while (nl < (int)gp.s_desc.size() && gp.s_desc[nl] - c0 > thr_rows) ++nl;
+    if (nl == 0) return 0;
+    if (nl > GRID_PANEL_MAX_UNITS || !gp.d_xchg || !gp.d_sync || gp.sms <= 0) return -1;
+    const int m_max = gp.s_desc[0] - c0;
+    const size_t cta_cap = 96 * 1024;  // two CTAs per SM
+    const int r_cap = (int)(cta_cap / (pnb * elem));
+    int G = std::max(1, gp.sms / nl);
+    G = std::min(G, (m_max + 31) / 32);
+    G = std::max(G, (m_max + r_cap - 1) / r_cap);
+    if (G > GRID_PANEL_MAX_CTAS) return -1;
+    int R = (m_max + G - 1) / G;
+    size_t smem = (size_t)R * pnb * elem;
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, 256, smem) != cudaSuccess) return -1;
+    if ((int64_t)G * nl > (int64_t)per_sm * gp.sms) return -1;
+    *G_out = G;
+    *smem_out = smem;
+    return nl;
+}
+
+void launch_factor_exact(const UnitDesc *units, int nu, int max_s, const GridPlan &gp, cx *A,
                          int32_t *piv, int32_t *status, cudaStream_t st) {
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_trailing, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)TRAILING_SMEM);
         cudaFuncSetAttribute(k_panel_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, PANEL_SMEM_MAX);
+        cudaFuncSetAttribute(k_panel_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
         attr = true;
     }
+    const int thr_rows = PANEL_SMEM_MAX / (int)(NB * sizeof(cx));
+    if (gp.d_sync) cudaMemsetAsync(gp.d_sync, 0, grid_sync_bytes(gp.steps), st);
     for (int c0 = 0; c0 < max_s; c0 += NB) {
-        size_t pan = sizeof(cx) * (size_t)(max_s - c0) * NB;
-        if (pan <= (size_t)PANEL_SMEM_MAX)
-            k_panel_smem<<<nu, 256, pan, st>>>(units, c0, A, piv, status);
-        else
-            k_panel<<<nu, 256, 0, st>>>(units, c0, A, piv, status);
+        int G = 0;
+        size_t gsm = 0;
+        int nl = plan_grid_panel(gp, c0, thr_rows, NB, sizeof(cx), (const void *)k_panel_grid, &G, &gsm);
+        if (nl > 0) {
+            int step = c0 / NB;
+            PanelXchg<cx> *xg = static_cast<PanelXchg<cx> *>(gp.d_xchg);
+            GridSync *gs = static_cast<GridSync *>(gp.d_sync) + (size_t)step * GRID_PANEL_MAX_UNITS;
+            const int32_t *ord = gp.d_order;
+            void *args[] = {(void *)&units, (void *)&ord, (void *)&c0, (void *)&A, (void *)&piv,
+                            (void *)&status, (void *)&xg, (void *)&gs};
+            if (cudaLaunchCooperativeKernel((const void *)k_panel_grid, dim3(G, nl), dim3(256), args, gsm, st) ==
+                cudaSuccess) {
+                // the rest: one CTA each, panels of at most thr_rows rows
+                int m_rest = std::min(max_s - c0, thr_rows);
+                k_panel_smem<<<nu, 256, sizeof(cx) * (size_t)m_rest * NB, st>>>(units, c0, A, piv, status,
+                                                                                 thr_rows);
+            } else {
+                (void)cudaGetLastError();  // not co-resident after all: one CTA per unit
+                k_panel<<<nu, 256, 0, st>>>(units, c0, A, piv, status, INT_MAX);
+            }
+        } else if (nl == 0) {
+            size_t pan = sizeof(cx) * (size_t)(max_s - c0) * NB;
+            k_panel_smem<<<nu, 256, pan, st>>>(units, c0, A, piv, status, INT_MAX);
+        } else {
+            k_panel<<<nu, 256, 0, st>>>(units, c0, A, piv, status, INT_MAX);
+        }
         // columns right of the panel: at least the right-hand side column
         int rest = max_s + 1 - (c0 + NB);
         if (rest < 1) rest = 1;
@@ -930,7 +1019,6 @@ void launch_factor_exact(const UnitDesc *units, int nu, int max_s, int max_trail
             }
         }
     }
-    (void)max_trailing_tiles;
 }
 void launch_backsub(const UnitDesc *units, int nu, int max_s, const cx *A, cx *x,
                     const int32_t *status, cudaStream_t st) {

@@ -46,6 +46,11 @@ extern "C" {
 #define FNEC_ERR_BUSY (-9)             /* admission refused (HBM budget)   */
 #define FNEC_ERR_TOO_LARGE (-10)       /* beyond a fixed static maximum    */
 
+/* Per-unit status word of a batch (fnec_batch_read): 0, -(column+1) of a
+ * singular pivot, or FNEC_UNIT_TIMEOUT when a wait between the CTAs of a
+ * grid-wide kernel ran out of time (the unit's results are void). */
+#define FNEC_UNIT_TIMEOUT 0x40000000
+
 #define FNEC_GROUND_FREE 0             /* GroundModel::FreeSpace           */
 #define FNEC_GROUND_PEC 1              /* GroundModel::PerfectConductor    */
 
@@ -300,7 +305,8 @@ int fnec_batch_sync(fnec_batch *b);
  *   feeds:    7 * total_feeds doubles (seg, V re/im, I re/im, Zin re/im)
  *   pattern:  6 * total_points doubles (gain_total, gain_theta, gain_phi,
  *             axial_ratio, u_theta, u_phi)
- *   status:   n_units int32 (0, or -(column+1) of a singular pivot)
+ *   status:   n_units int32 (0, -(column+1) of a singular pivot, or
+ *             FNEC_UNIT_TIMEOUT)
  *   total_radiated: n_units doubles */
 int fnec_batch_read(fnec_batch *b, double *currents, double *feeds, double *pattern,
                     int32_t *status, double *total_radiated);
