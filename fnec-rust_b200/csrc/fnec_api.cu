@@ -509,6 +509,21 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
             }
             b->crows.push_back(d);
         }
+        {
+            // transpose: the constraint rows touching each segment column
+            std::vector<std::vector<int32_t>> cc(a.n);
+            for (int32_t q = 0; q < a.n_crow; ++q) {
+                const DevConRow &d = b->crows[a.crow_off + q];
+                cc[d.c0].push_back(q);
+                if (d.c1 >= 0 && d.c1 != d.c0) cc[d.c1].push_back(q);
+            }
+            a.ccptr_off = (int64_t)b->ibuf.size();
+            int32_t acc = 0;
+            b->ibuf.push_back(0);
+            for (auto &v : cc) b->ibuf.push_back(acc += (int32_t)v.size());
+            a.ccq_off = (int64_t)b->ibuf.size();
+            for (auto &v : cc) b->ibuf.insert(b->ibuf.end(), v.begin(), v.end());
+        }
         struct Contrib {
             int64_t i, j, row;
             int32_t code;

@@ -747,7 +747,7 @@ __global__ void __launch_bounds__(256) k_gmres_ir(const UnitDesc *__restrict__ u
                                                   const cx *__restrict__ rhs, const double *__restrict__ cosv,
                                                   const float2 *__restrict__ a32buf, const int32_t *__restrict__ pivbuf,
                                                   cx *xbuf, cx *vbuf, cx *wbuf, const int32_t *__restrict__ status,
-                                                  int staged) {
+                                                  int staged, int skip_s, int only) {
     extern __shared__ unsigned char s_dyn[];
     __shared__ cx sH[(GM + 1) * GM];
     __shared__ double scs[GM];
@@ -758,7 +758,8 @@ __global__ void __launch_bounds__(256) k_gmres_ir(const UnitDesc *__restrict__ u
     __shared__ int s_stop;
     int ui = blockIdx.x;  // one solve (right-hand side)
     UnitDesc u = units[ui];
-    if (status[u.sys] != 0) return;
+    if (status[u.sys] != 0 || u.s >= skip_s) return;  // skip_s: refined grid-wide
+    if (only >= 0 && ui != only) return;
     AntDesc a = ants[u.ant];
     MixedUnit mu = mus[ui];
     GmresCtx g;
@@ -915,6 +916,473 @@ __global__ void __launch_bounds__(256) k_gmres_ir(const UnitDesc *__restrict__ u
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// GMRES for large systems: the same iteration as k_gmres_ir, spread over
+// the whole GPU (one cooperative launch per solve).  Every CTA runs the
+// same control flow; scalars (inner products, norms, the Hessenberg
+// column, the Givens rotations, the stopping test) are reduced in a fixed
+// order and recomputed identically in every CTA, so all CTAs take the same
+// branches.  Vectors are split element-wise over all threads; the phases
+// that read another CTA's elements are separated by grid barriers
+// (fnec_grid.cuh) and read through L2.
+//   A v      row pass t = M v (a warp per row), then M^H t as column sums
+//            over row chunks (a warp per 64 columns x GG_RC rows) reduced
+//            in chunk order, plus the sparse constraint and cos columns
+//   P^-1     gather through the factor's row permutation, then blocked
+//            forward / backward substitution: the owner CTA of each 32-row
+//            block solves its diagonal block, one barrier, every CTA
+//            updates the blocks it owns
+// ---------------------------------------------------------------------------
+constexpr int GG_RC = 256;           // rows per column-sum chunk of M^H t
+constexpr int GG_MIN_S = 1536;       // solves this large go grid-wide ...
+constexpr int GG_MAX_SOLVES = 16;    // ... when there are at most this many
+constexpr int GG_MAX_CTAS = 296;
+
+__device__ __forceinline__ cx ldcg_cx(const cx *p) {
+    double2 d = __ldcg(reinterpret_cast<const double2 *>(p));
+    return {d.x, d.y};
+}
+
+struct GGrid {
+    GmresCtx g;
+    const int32_t *ccptr, *ccq, *perm;
+    cx *part;
+    float2 *y;
+    cx *red;
+    GridSync *gs;
+    int32_t *status;
+    int G, cta, tid, lane, wid, gt, T, gw, TW;
+    unsigned epoch, redk;
+};
+
+__device__ __forceinline__ bool gg_sync(GGrid &c) {
+    if (grid_barrier(c.gs, (unsigned)c.G, ++c.epoch)) return true;
+    if (c.tid == 0) atomicExch(c.status, FNEC_STATUS_GRID_TIMEOUT);
+    return false;
+}
+#define GG_SYNC(c)          \
+    if (!gg_sync(c)) return false
+
+// out = M^H (M v) + lambda v; with v == nullptr, out = M^H [y; 0] (the
+// right-hand side b).
+__device__ bool gg_apply(GGrid &c, const cx *v, cx *out) {
+    const GmresCtx &g = c.g;
+    if (v) {
+        for (int r = c.gw; r < g.n; r += c.TW) {
+            const cx *zr = g.z + (int64_t)r * g.n;
+            cx acc = {0, 0};
+#pragma unroll 4
+            for (int col = c.lane; col < g.n; col += 32) acc = zadd(acc, zmul(zr[col], ldcg_cx(v + col)));
+            acc = warp_sum(acc);
+            if (c.lane == 0) {
+                cx cvv = ldcg_cx(v + g.n + g.rowwire[r]);
+                g.t[r] = {acc.re - g.cv[r] * cvv.re, acc.im - g.cv[r] * cvv.im};
+            }
+        }
+        for (int q = c.gt; q < g.nc; q += c.T) {
+            DevConRow cr = g.crows[q];
+            cx val = ldcg_cx(v + cr.c0);
+            if (cr.c1 >= 0) val = zadd(val, zscale(ldcg_cx(v + cr.c1), cr.v1));
+            g.t[g.n + q] = val;
+        }
+    } else {
+        for (int r = c.gt; r < g.n; r += c.T) g.t[r] = g.y[r];
+        for (int q = c.gt; q < g.nc; q += c.T) g.t[g.n + q] = {0, 0};
+    }
+    GG_SYNC(c);
+    const int ncb = (g.n + 63) / 64, nch = (g.n + GG_RC - 1) / GG_RC;
+    for (int it = c.gw; it < ncb * nch; it += c.TW) {
+        int cb = it % ncb, ch = it / ncb;
+        int c0 = cb * 64 + c.lane, c1 = c0 + 32;
+        int r0 = ch * GG_RC, r1 = min(g.n, r0 + GG_RC);
+        cx a0 = {0, 0}, a1 = {0, 0};
+        if (c1 < g.n) {
+            for (int r = r0; r < r1; ++r) {
+                cx tr = ldcg_cx(g.t + r);
+                const cx *zr = g.z + (int64_t)r * g.n;
+                a0 = zadd(a0, zcmul(zr[c0], tr));
+                a1 = zadd(a1, zcmul(zr[c1], tr));
+            }
+        } else if (c0 < g.n) {
+            for (int r = r0; r < r1; ++r) a0 = zadd(a0, zcmul(g.z[(int64_t)r * g.n + c0], ldcg_cx(g.t + r)));
+        }
+        if (c0 < g.n) c.part[(int64_t)ch * g.n + c0] = a0;
+        if (c1 < g.n) c.part[(int64_t)ch * g.n + c1] = a1;
+    }
+    GG_SYNC(c);
+    for (int col = c.gt; col < g.n; col += c.T) {
+        cx acc = {0, 0};
+        for (int ch = 0; ch < nch; ++ch) acc = zadd(acc, ldcg_cx(c.part + (int64_t)ch * g.n + col));
+        for (int k = c.ccptr[col]; k < c.ccptr[col + 1]; ++k) {
+            int q = c.ccq[k];
+            DevConRow cr = g.crows[q];
+            double coef = (cr.c0 == col ? 1.0 : 0.0) + (cr.c1 == col ? cr.v1 : 0.0);
+            acc = zadd(acc, zscale(ldcg_cx(g.t + g.n + q), coef));
+        }
+        if (v) acc = zadd(acc, zscale(ldcg_cx(v + col), 1e-8));
+        out[col] = acc;
+    }
+    for (int w = c.gt; w < g.w; w += c.T) {
+        cx acc = {0, 0};
+        for (int k = g.wptr[w]; k < g.wptr[w + 1]; ++k) {
+            int r = g.wrow[k];
+            acc = zadd(acc, zscale(ldcg_cx(g.t + r), -g.cv[r]));
+        }
+        if (v) acc = zadd(acc, zscale(ldcg_cx(v + g.n + w), 1e-8));
+        out[g.n + w] = acc;
+    }
+    GG_SYNC(c);
+    return true;
+}
+
+// out = (L U)^-1 P in (the caller has synchronised after writing in)
+__device__ bool gg_prec(GGrid &c, const cx *in, cx *out) {
+    const GmresCtx &g = c.g;
+    const int s = g.s, nblk = (s + 31) / 32;
+    __shared__ float2 s_yb[32];
+    for (int i = c.gt; i < s; i += c.T) {
+        cx v = ldcg_cx(in + c.perm[i]);
+        c.y[i] = cf((float)v.re, (float)v.im);
+    }
+    GG_SYNC(c);
+    // forward, unit lower triangular
+    for (int bk = 0; bk < nblk; ++bk) {
+        const int c0 = bk * 32, nb = min(32, s - c0);
+        if (bk % c.G == c.cta && c.wid == 0) {
+            float2 yl = c.lane < nb ? __ldcg(c.y + c0 + c.lane) : cf(0.f, 0.f);
+            const float2 *lrow = g.lu + (int64_t)(c0 + (c.lane < nb ? c.lane : 0)) * s + c0;
+            float2 lr[32];
+#pragma unroll
+            for (int q = 0; q < 32; ++q) lr[q] = (q < nb) ? lrow[q] : cf(0.f, 0.f);
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+                float yr = __shfl_sync(0xffffffffu, yl.x, q), yi = __shfl_sync(0xffffffffu, yl.y, q);
+                if (c.lane > q && c.lane < nb) yl = cf_sub(yl, cf_mul(lr[q], cf(yr, yi)));
+            }
+            if (c.lane < nb) c.y[c0 + c.lane] = yl;
+        }
+        GG_SYNC(c);
+        if (c.tid < nb) s_yb[c.tid] = __ldcg(c.y + c0 + c.tid);
+        __syncthreads();
+        // owned blocks q > bk: q = bk+1+d with q % G == cta
+        int q0 = bk + 1 + ((c.cta - (bk + 1)) % c.G + c.G) % c.G;
+        int nown = q0 < nblk ? (nblk - 1 - q0) / c.G + 1 : 0;
+        for (int e = c.tid; e < nown * 32; e += blockDim.x) {
+            int r = (q0 + (e >> 5) * c.G) * 32 + (e & 31);
+            if (r >= s) continue;
+            const float2 *lrow = g.lu + (int64_t)r * s + c0;
+            float2 acc = __ldcg(c.y + r);
+            if (nb == 32) {
+                float2 lr[32];
+#pragma unroll
+                for (int k = 0; k < 32; ++k) lr[k] = lrow[k];
+#pragma unroll
+                for (int k = 0; k < 32; ++k) acc = cf_sub(acc, cf_mul(lr[k], s_yb[k]));
+            } else {
+                for (int k = 0; k < nb; ++k) acc = cf_sub(acc, cf_mul(lrow[k], s_yb[k]));
+            }
+            c.y[r] = acc;
+        }
+        __syncthreads();
+    }
+    // backward, upper triangular with its diagonal
+    for (int bk = nblk - 1; bk >= 0; --bk) {
+        const int c0 = bk * 32, nb = min(32, s - c0);
+        if (bk % c.G == c.cta && c.wid == 0) {
+            float2 yl = c.lane < nb ? __ldcg(c.y + c0 + c.lane) : cf(0.f, 0.f);
+            const float2 *urow = g.lu + (int64_t)(c0 + (c.lane < nb ? c.lane : 0)) * s + c0;
+            float2 ur[32];
+#pragma unroll
+            for (int q = 0; q < 32; ++q) ur[q] = (q < nb) ? urow[q] : cf(1.f, 0.f);
+#pragma unroll
+            for (int q = 31; q >= 0; --q) {
+                if (q < nb) {
+                    if (c.lane == q) yl = cf_div(yl, ur[q]);
+                    float yr = __shfl_sync(0xffffffffu, yl.x, q), yi = __shfl_sync(0xffffffffu, yl.y, q);
+                    if (c.lane < q) yl = cf_sub(yl, cf_mul(ur[q], cf(yr, yi)));
+                }
+            }
+            if (c.lane < nb) c.y[c0 + c.lane] = yl;
+        }
+        GG_SYNC(c);
+        if (bk == 0) break;
+        if (c.tid < nb) s_yb[c.tid] = __ldcg(c.y + c0 + c.tid);
+        __syncthreads();
+        // owned blocks q < bk: q = cta, cta + G, ...
+        int nown = c.cta < bk ? (bk - 1 - c.cta) / c.G + 1 : 0;
+        for (int e = c.tid; e < nown * 32; e += blockDim.x) {
+            int r = (c.cta + (e >> 5) * c.G) * 32 + (e & 31);
+            const float2 *urow = g.lu + (int64_t)r * s + c0;
+            float2 acc = __ldcg(c.y + r);
+            if (nb == 32) {
+                float2 ur[32];
+#pragma unroll
+                for (int k = 0; k < 32; ++k) ur[k] = urow[k];
+#pragma unroll
+                for (int k = 0; k < 32; ++k) acc = cf_sub(acc, cf_mul(ur[k], s_yb[k]));
+            } else {
+                for (int k = 0; k < nb; ++k) acc = cf_sub(acc, cf_mul(urow[k], s_yb[k]));
+            }
+            c.y[r] = acc;
+        }
+        __syncthreads();
+    }
+    for (int i = c.gt; i < s; i += c.T) {
+        float2 v = __ldcg(c.y + i);
+        out[i] = {(double)v.x, (double)v.y};
+    }
+    GG_SYNC(c);
+    return true;
+}
+
+// h[i] = <V_i, vn> for i <= j (h in shared memory, identical in every CTA)
+__device__ bool gg_dots(GGrid &c, const cx *V, int j, const cx *vn, cx *h, cx (*s_wp)[GM + 1]) {
+    const int s = c.g.s;
+    cx *red = c.red + (size_t)(c.redk & 1) * c.G * (GM + 1);
+    ++c.redk;
+    for (int i = 0; i <= j; ++i) {
+        const cx *vi = V + (int64_t)i * s;
+        cx acc = {0, 0};
+        for (int k = c.gt; k < s; k += c.T) acc = zadd(acc, zcmul(ldcg_cx(vi + k), ldcg_cx(vn + k)));
+        acc = warp_sum(acc);
+        if (c.lane == 0) s_wp[c.wid][i] = acc;
+    }
+    __syncthreads();
+    if (c.tid <= j) {
+        cx a = {0, 0};
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) a = zadd(a, s_wp[q][c.tid]);
+        red[c.cta * (GM + 1) + c.tid] = a;
+    }
+    GG_SYNC(c);
+    if (c.tid <= j) {
+        cx a = {0, 0};
+        for (int q = 0; q < c.G; ++q) a = zadd(a, ldcg_cx(red + q * (GM + 1) + c.tid));
+        h[c.tid] = a;
+    }
+    __syncthreads();
+    return true;
+}
+
+// |v| (identical in every CTA)
+__device__ bool gg_norm(GGrid &c, const cx *v, double *out, double *s_red) {
+    const int s = c.g.s;
+    cx *red = c.red + (size_t)(c.redk & 1) * c.G * (GM + 1);
+    ++c.redk;
+    double a = 0;
+    for (int k = c.gt; k < s; k += c.T) {
+        cx x = ldcg_cx(v + k);
+        a += x.re * x.re + x.im * x.im;
+    }
+    a = block_sum(a, s_red);
+    if (c.tid == 0) red[c.cta * (GM + 1)] = {a, 0.0};
+    GG_SYNC(c);
+    if (c.tid == 0) {
+        double t = 0;
+        for (int q = 0; q < c.G; ++q) t += __ldcg(reinterpret_cast<const double *>(red + q * (GM + 1)));
+        s_red[8] = sqrt(t);
+    }
+    __syncthreads();
+    *out = s_red[8];
+    __syncthreads();
+    return true;
+}
+
+__device__ bool gmres_grid_body(GGrid &c, const UnitDesc &u, MixedUnit *mus, int ui, cx *xbuf, cx *W, cx *V) {
+    __shared__ cx sH[(GM + 1) * GM];
+    __shared__ double scs[GM];
+    __shared__ cx ssn[GM];
+    __shared__ cx sg[GM + 1];
+    __shared__ cx sh[GM + 1];
+    __shared__ cx shp[GM + 1];
+    __shared__ cx s_wp[8][GM + 1];
+    __shared__ double s_red[9];
+    __shared__ int s_stop;
+    const int s = c.g.s, tid = c.tid;
+    cx *b = W, *x = W + s, *r = W + 2 * s, *w = W + 3 * s;
+    if (!gg_apply(c, nullptr, b)) return false;
+    if (!gg_prec(c, b, x)) return false;
+    double bnorm;
+    if (!gg_norm(c, x, &bnorm, s_red)) return false;
+    int iters = 0;
+    double rel = 1.0;
+    for (int outer = 0; outer < MAX_OUTER; ++outer) {
+        if (!gg_apply(c, x, w)) return false;
+        for (int i = c.gt; i < s; i += c.T) r[i] = zsub(ldcg_cx(b + i), ldcg_cx(w + i));
+        GG_SYNC(c);
+        if (!gg_prec(c, r, V)) return false;
+        double beta;
+        if (!gg_norm(c, V, &beta, s_red)) return false;
+        rel = bnorm > 0 ? beta / bnorm : 0.0;
+        if (rel <= GMRES_TOL || beta == 0.0) break;
+        for (int i = c.gt; i < s; i += c.T) V[i] = zscale(V[i], 1.0 / beta);
+        if (tid == 0) {
+            sg[0] = {beta, 0};
+            for (int q = 1; q <= GM; ++q) sg[q] = {0, 0};
+        }
+        GG_SYNC(c);
+        int jend = GM - 1;
+        for (int j = 0; j < GM; ++j) {
+            cx *vj = V + (int64_t)j * s, *vn = V + (int64_t)(j + 1) * s;
+            if (!gg_apply(c, vj, w)) return false;
+            if (!gg_prec(c, w, vn)) return false;
+            if (tid <= j) sh[tid] = {0, 0};
+            __syncthreads();
+            for (int pass = 0; pass < 2; ++pass) {
+                if (!gg_dots(c, V, j, vn, shp, s_wp)) return false;
+                for (int k = c.gt; k < s; k += c.T) {
+                    cx vv = vn[k];
+                    for (int i = 0; i <= j; ++i) vv = zsub(vv, zmul(shp[i], V[(int64_t)i * s + k]));
+                    vn[k] = vv;
+                }
+                if (tid <= j) sh[tid] = zadd(sh[tid], shp[tid]);
+                __syncthreads();
+            }
+            if (tid <= j) sH[tid * GM + j] = sh[tid];
+            double hn;
+            if (!gg_norm(c, vn, &hn, s_red)) return false;
+            if (tid == 0) {
+                sH[(j + 1) * GM + j] = {hn, 0};
+                for (int i = 0; i < j; ++i) {
+                    cx h0 = sH[i * GM + j], h1 = sH[(i + 1) * GM + j];
+                    cx t0 = zadd(zscale(h0, scs[i]), zmul(ssn[i], h1));
+                    cx sc = {ssn[i].re, -ssn[i].im};
+                    sH[(i + 1) * GM + j] = zsub(zscale(h1, scs[i]), zmul(sc, h0));
+                    sH[i * GM + j] = t0;
+                }
+                cx aa = sH[j * GM + j];
+                double bb = hn;
+                double na = sqrt(aa.re * aa.re + aa.im * aa.im);
+                double nu = sqrt(na * na + bb * bb);
+                double cc;
+                cx sn;
+                if (na == 0.0) {
+                    cc = 0.0;
+                    sn = {1.0, 0.0};
+                    sH[j * GM + j] = {bb, 0};
+                } else {
+                    cc = na / nu;
+                    cx ph = {aa.re / na, aa.im / na};
+                    sn = zscale(ph, bb / nu);
+                    sH[j * GM + j] = zscale(ph, nu);
+                }
+                scs[j] = cc;
+                ssn[j] = sn;
+                cx gj = sg[j];
+                cx sc = {sn.re, -sn.im};
+                sg[j + 1] = zscale(zmul(sc, gj), -1.0);
+                sg[j] = zscale(gj, cc);
+                double res = sqrt(sg[j + 1].re * sg[j + 1].re + sg[j + 1].im * sg[j + 1].im);
+                s_stop = (res <= GMRES_TOL * bnorm || hn == 0.0) ? 1 : 0;
+            }
+            __syncthreads();
+            if (hn > 0.0)
+                for (int k = c.gt; k < s; k += c.T) vn[k] = zscale(vn[k], 1.0 / hn);
+            GG_SYNC(c);
+            ++iters;
+            if (s_stop) {
+                jend = j;
+                break;
+            }
+        }
+        if (tid == 0) {
+            for (int i = jend; i >= 0; --i) {
+                cx acc = sg[i];
+                for (int k = i + 1; k <= jend; ++k) acc = zsub(acc, zmul(sH[i * GM + k], sh[k]));
+                sh[i] = zdiv(acc, sH[i * GM + i]);
+            }
+        }
+        __syncthreads();
+        for (int k = c.gt; k < s; k += c.T) {
+            cx vv = x[k];
+            for (int i = 0; i <= jend; ++i) vv = zadd(vv, zmul(sh[i], V[(int64_t)i * s + k]));
+            x[k] = vv;
+        }
+        GG_SYNC(c);
+    }
+    for (int i = c.gt; i < s; i += c.T) xbuf[u.x_off + i] = x[i];
+    if (c.cta == 0 && tid == 0) {
+        mus[ui].iters = iters;
+        mus[ui].resid = rel;
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(256) k_gmres_grid(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
+                                                    MixedUnit *mus, int ui, const int32_t *__restrict__ ibuf,
+                                                    const DevConRow *__restrict__ crows, const cx *__restrict__ zbuf,
+                                                    const cx *__restrict__ rhs, const double *__restrict__ cosv,
+                                                    const float2 *__restrict__ a32buf, const int32_t *__restrict__ pivbuf,
+                                                    cx *xbuf, cx *vbuf, cx *wbuf, int32_t *status,
+                                                    const int32_t *__restrict__ perm, cx *part, float2 *ybuf, cx *red,
+                                                    GridSync *gs) {
+    UnitDesc u = units[ui];
+    if (status[u.sys] != 0) return;
+    AntDesc a = ants[u.ant];
+    MixedUnit mu = mus[ui];
+    GGrid c;
+    c.g.n = u.n;
+    c.g.s = u.s;
+    c.g.w = a.w;
+    c.g.nc = a.n_crow;
+    c.g.rows = u.n + a.n_crow;
+    c.g.z = zbuf + u.z_off;
+    c.g.y = rhs + u.rhs_off;
+    c.g.cv = cosv + u.cos_off;
+    c.g.rowwire = ibuf + a.rowwire_off;
+    c.g.wptr = ibuf + a.wptr_off;
+    c.g.wrow = ibuf + a.wrow_off;
+    c.g.crows = crows + a.crow_off;
+    c.g.lu = a32buf + mu.a32_off;
+    c.g.piv = pivbuf + u.piv_off;
+    cx *W = wbuf + mu.w_off;
+    c.g.t = W + 4 * u.s;
+    c.ccptr = ibuf + a.ccptr_off;
+    c.ccq = ibuf + a.ccq_off;
+    c.perm = perm;
+    c.part = part;
+    c.y = ybuf;
+    c.red = red;
+    c.gs = gs;
+    c.status = &status[u.sys];
+    c.G = gridDim.x;
+    c.cta = blockIdx.x;
+    c.tid = threadIdx.x;
+    c.lane = threadIdx.x & 31;
+    c.wid = threadIdx.x >> 5;
+    c.gt = blockIdx.x * blockDim.x + threadIdx.x;
+    c.T = gridDim.x * blockDim.x;
+    c.gw = c.gt >> 5;
+    c.TW = c.T >> 5;
+    c.epoch = 0;
+    c.redk = 0;
+    gmres_grid_body(c, u, mus, ui, xbuf, W, vbuf + mu.v_off);
+}
+
+// The row permutation of the factor: perm[i] = source row of row i after
+// the swaps piv[0..s) (applied in order, in shared memory when it fits).
+__global__ void k_perm_from_piv(const UnitDesc *__restrict__ units, int ui, const int32_t *__restrict__ pivbuf,
+                                int32_t *perm, int staged) {
+    extern __shared__ int32_t s_perm_dyn[];
+    UnitDesc u = units[ui];
+    const int32_t *piv = pivbuf + u.piv_off;
+    int32_t *s_perm = staged ? s_perm_dyn : perm;
+    for (int i = threadIdx.x; i < u.s; i += blockDim.x) s_perm[i] = i;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        for (int c = 0; c < u.s; ++c) {
+            int p = piv[c];
+            if (p >= 0 && p != c) {
+                int t0 = s_perm[c];
+                s_perm[c] = s_perm[p];
+                s_perm[p] = t0;
+            }
+        }
+    __syncthreads();
+    if (!staged) return;
+    for (int i = threadIdx.x; i < u.s; i += blockDim.x) perm[i] = s_perm[i];
+}
+
 }  // namespace
 
 bool mixed_available() { return true; }
@@ -966,6 +1434,47 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
     w.n_units = (int)solves.size();
     w.max_s = max_s;
     w.host = mu;
+    w.grid_solves.clear();
+    w.grid_s.clear();
+    for (size_t i = 0; i < solves.size(); ++i)
+        if (solves[i].s >= GG_MIN_S) {
+            w.grid_solves.push_back((int)i);
+            w.grid_s.push_back(solves[i].s);
+        }
+    if (w.grid_solves.size() > (size_t)GG_MAX_SOLVES) {
+        w.grid_solves.clear();
+        w.grid_s.clear();
+    }
+    if (!w.grid_solves.empty()) {
+        int64_t smax = 0, partmax = 0;
+        for (int i : w.grid_solves) {
+            const UnitDesc &u = solves[i];
+            smax = std::max<int64_t>(smax, u.s);
+            partmax = std::max<int64_t>(partmax, (int64_t)((u.n + GG_RC - 1) / GG_RC) * u.n);
+        }
+        size_t b_perm = sizeof(int32_t) * (size_t)smax, b_part = sizeof(cx) * (size_t)partmax,
+               b_y = sizeof(float2) * (size_t)smax, b_red = sizeof(cx) * 2 * GG_MAX_CTAS * (GM + 1),
+               b_sync = sizeof(GridSync) * w.grid_solves.size();
+        size_t gt = al(b_perm) + al(b_part) + al(b_y) + al(b_red) + al(b_sync);
+        e = cudaMalloc(&w.grid_base, gt);
+        if (e != cudaSuccess) return e;
+        unsigned char *q = (unsigned char *)w.grid_base;
+        w.g_perm = (int32_t *)q;
+        q += al(b_perm);
+        w.g_part = (cx *)q;
+        q += al(b_part);
+        w.g_y = (float2 *)q;
+        q += al(b_y);
+        w.g_red = (cx *)q;
+        q += al(b_red);
+        w.g_sync = q;
+        w.bytes += gt;
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gmres_grid, 256, 0);
+        w.grid_ctas = std::min(GG_MAX_CTAS, sms * std::min(per_sm, 1));
+    }
     e = cudaMemcpy(w.mu, mu.data(), sizeof(MixedUnit) * mu.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(w.smu, sysmu.data(), sizeof(MixedUnit) * sysmu.size(), cudaMemcpyHostToDevice);
     return e;
@@ -973,6 +1482,8 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
 
 void free_mixed(MixedWork &w) {
     if (w.base) cudaFree(w.base);
+    if (w.grid_base) cudaFree(w.grid_base);
+    w.grid_base = nullptr;
     w.base = nullptr;
     w.bytes = 0;
 }
@@ -1057,8 +1568,37 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_gmres_ir, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (ns > 0)
         k_gmres_ir<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x, mw.v,
-                                          mw.w, status, staged);
+                                          mw.w, status, staged, mw.grid_solves.empty() ? INT_MAX : GG_MIN_S, -1);
     ++L;
+    if (!mw.grid_solves.empty()) {
+        cudaMemsetAsync(mw.g_sync, 0, sizeof(GridSync) * mw.grid_solves.size(), st);
+        for (size_t k = 0; k < mw.grid_solves.size(); ++k) {
+            int ui = mw.grid_solves[k];
+            size_t psm = sizeof(int32_t) * (size_t)mw.grid_s[k];
+            int pst = psm <= 200 * 1024;
+            if (!pst) psm = 0;
+            if (psm > 48 * 1024)
+                cudaFuncSetAttribute(k_perm_from_piv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm);
+            k_perm_from_piv<<<1, 256, psm, st>>>(d_solves, ui, piv, mw.g_perm, pst);
+            GridSync *gs = static_cast<GridSync *>(mw.g_sync) + k;
+            MixedUnit *mus = mw.mu;
+            float2 *a32 = mw.a32;
+            cx *vb = mw.v, *wb = mw.w;
+            const int32_t *perm = mw.g_perm;
+            void *args[] = {(void *)&d_solves, (void *)&d_ants, (void *)&mus, (void *)&ui, (void *)&ibuf,
+                            (void *)&crows, (void *)&z, (void *)&rhs, (void *)&cosv, (void *)&a32,
+                            (void *)&piv, (void *)&x, (void *)&vb, (void *)&wb, (void *)&status,
+                            (void *)&perm, (void *)&mw.g_part, (void *)&mw.g_y, (void *)&mw.g_red, (void *)&gs};
+            if (mw.grid_ctas <= 0 ||
+                cudaLaunchCooperativeKernel((const void *)k_gmres_grid, dim3(mw.grid_ctas), dim3(256), args, 0, st) !=
+                    cudaSuccess) {
+                (void)cudaGetLastError();  // not co-resident: refine this solve in one CTA
+                k_gmres_ir<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x,
+                                                  mw.v, mw.w, status, staged, INT_MAX, ui);
+            }
+            L += 2;
+        }
+    }
     mark(3);
     return L;
 }

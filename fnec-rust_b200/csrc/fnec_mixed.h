@@ -30,6 +30,16 @@ struct MixedWork {
     int n_units = 0;
     int max_s = 0;
     std::vector<MixedUnit> host;
+    // large solves refined by the grid-wide GMRES, one cooperative launch each
+    std::vector<int> grid_solves;
+    std::vector<int> grid_s;       // their s
+    void *grid_base = nullptr;     // scratch shared by those launches
+    int32_t *g_perm = nullptr;
+    cx *g_part = nullptr;
+    float2 *g_y = nullptr;
+    cx *g_red = nullptr;
+    void *g_sync = nullptr;
+    int grid_ctas = 0;
 };
 
 // Phase events the mixed path records after its fill, Gram, factor and

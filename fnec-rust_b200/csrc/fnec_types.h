@@ -72,6 +72,8 @@ struct AntDesc {
     int32_t n_run;
     int32_t n_crow;      // constraint rows of M (free ends, then junctions)
     int64_t crow_off;    // DevConRow[n_crow]
+    int64_t ccptr_off;   // int32[n+1]: CSR of the constraint rows touching each column
+    int64_t ccq_off;     // int32: those rows (ascending), ccptr-indexed
 };
 
 // One constraint row of M (linear.rs:744-762): M[N+q][c0] = 1 and, for a

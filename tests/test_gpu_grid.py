@@ -56,16 +56,20 @@ def test_grid_panel_several_units(acc):
         _check_unit(acc, batch, res, u, w, s, 1, f, O.rp_card_points(5, 4, 0, 0, 20, 90))
 
 
-def test_grid_panel_mixed(acc):
-    """Mesh of 14x14 cells (S = 1260) in the mixed form: its first panels
-    run grid-wide in FP32; the refined result meets the 1e-6 gate against
-    the plain GPU path (itself pinned to the oracle above)."""
-    w, s, f = _mesh(14)
+def test_grid_panel_and_gmres_mixed(acc):
+    """Mesh of 18x18 cells (S = 2052) in the mixed form, two copies in one
+    batch: the first panels run grid-wide in FP32 and both solves are
+    refined by the grid-wide GMRES (one cooperative launch each).  The
+    result meets the 1e-6 gate against the plain GPU path (itself pinned to
+    the oracle above)."""
+    w, s, f = _mesh(18)
     ant = acc.Antenna(w.view(acc.WIRE_DTYPE), s.view(acc.SOURCE_DTYPE), [f], 1, None)
     plain = acc.HallenBatch([ant])
     rp = plain.solve()
     mixed = acc.HallenBatch([ant, ant], precision=acc.PRECISION_MIXED)
     rm = mixed.solve()
+    it, rs = mixed.refinement_stats()
+    assert np.all(it > 0) and np.all(rs <= 1e-9)
     assert np.all(rm.status == 0) and np.all(rp.status == 0)
     zp = complex(*rp.feeds[0][0, 5:7])
     for u in range(2):
