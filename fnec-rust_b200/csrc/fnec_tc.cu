@@ -1,0 +1,504 @@
+// fnec_tc.cu -- 3xTF32 tensor-core GEMM on the 5th-generation tensor cores.
+//
+// D = A B^T over K, both operands K-major FP32, each split once into
+// hi = tf32(x) and lo = x - hi; D = A_hi B_hi^T + A_hi B_lo^T + A_lo B_hi^T
+// recovers FP32-level accuracy (the dropped A_lo B_lo^T term is ~2^-22 of
+// the product) at tensor-core rate.  One CTA computes one 128x128 tile:
+//   warp 0   TMA producer: 4 boxes (A_hi, A_lo, B_hi, B_lo) of 128 rows x
+//            32 floats (128 B, SWIZZLE_128B) per k-block, 3-stage ring
+//   warp 1   MMA issuer: tcgen05.mma.cta_group::1.kind::tf32, M=128 N=128
+//            K=8, 12 per k-block, accumulator in TMEM (128 columns)
+//   warps 2-5  epilogue: tcgen05.ld of their TMEM lane quarter, then the
+//            caller's epilogue (store, or the complex Gram combine)
+// Operands live in "K-blocked" stacks: a [rows][32] float array where
+// k-block kb of an operand row block starts kb * kstride rows after the
+// first, so one tensor map serves every unit of an uneven batch.
+// Every wait is bounded (2 s of global time); a CTA that gives up marks
+// its unit FNEC_UNIT_TIMEOUT, drains its copies and MMAs and frees TMEM.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "fnec_cuda.h"
+#include "fnec_grid.cuh"
+#include "fnec_tc.h"
+
+namespace fnec {
+namespace {
+
+constexpr int BM = 128, BN = 128, BK = 32;
+constexpr int STAGES = 3;
+constexpr int BOX_BYTES = BM * BK * 4;         // 16 KB
+constexpr int STAGE_BYTES = 4 * BOX_BYTES;    // A_hi, A_lo, B_hi, B_lo
+constexpr int TMEM_COLS = 128;
+constexpr int TC_THREADS = 192;
+constexpr unsigned long long TC_WAIT_NS = 2000000000ull;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait.  false: the CTA is aborting (abort word set by another role)
+// or this wait ran out of time (it then sets the abort word).
+__device__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_word) {
+    unsigned long long t0 = gtimer_ns();
+    for (uint32_t it = 1;; ++it) {
+        if (mbar_try(bar, parity)) return true;
+        if (*abort_word) return false;
+        if ((it & 63) == 0 && gtimer_ns() - t0 > TC_WAIT_NS) {
+            *abort_word = 1;
+            return false;
+        }
+    }
+}
+// Bounded wait that ignores the abort word (draining after an abort).
+__device__ void mbar_drain(uint32_t bar, uint32_t parity) {
+    unsigned long long t0 = gtimer_ns();
+    for (uint32_t it = 1;; ++it) {
+        if (mbar_try(bar, parity)) return;
+        if ((it & 63) == 0 && gtimer_ns() - t0 > TC_WAIT_NS) return;
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+            dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+// Shared-memory matrix descriptor of a K-major operand tile written by TMA
+// with SWIZZLE_128B: rows of 128 B, 8-row groups 1024 B apart (SBO), the
+// swizzle applied on absolute address bits, so a K step inside the 128 B
+// row is a plain start-address offset.
+__device__ __forceinline__ uint64_t sw128_kmajor_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr & 0x3FFFFu) >> 4);  // start address, 16 B units
+    d |= (uint64_t)1 << 16;                    // leading byte offset (unused here)
+    d |= (uint64_t)(1024 >> 4) << 32;          // stride byte offset
+    d |= (uint64_t)1 << 46;                    // descriptor version
+    d |= (uint64_t)2 << 61;                    // SWIZZLE_128B
+    return d;
+}
+
+// Instruction descriptor: D f32, A and B tf32, both K-major, M=128, N=128.
+constexpr uint32_t IDESC_TF32_128x128 =
+    (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(IDESC_TF32_128x128), "r"(acc));
+}
+__device__ __forceinline__ void mma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// -- epilogues ------------------------------------------------------------
+// row: 0..127 inside the tile; v: 32 consecutive columns starting at col.
+__device__ __forceinline__ void epi_store(const TcTile &t, const TcEpilogue &ep, int row, int col, const float (&v)[32]) {
+    int64_t R = (int64_t)t.ti * BM + row;
+    if (R >= ep.m) return;
+    float *c = ep.c + R * ep.ldc;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        int64_t C = (int64_t)t.tj * BN + col + j;
+        if (C < ep.n) c[C] = v[j];
+    }
+}
+
+// The complex Gram A = Z^H Z from D = T T^T with T[2c+s][k] = (Re, Im) Z[k][c]:
+//   A[c][c'] = (D[2c][2c'] + D[2c+1][2c'+1], D[2c][2c'+1] - D[2c+1][2c']).
+// Lanes 2i and 2i+1 hold rows 2c and 2c+1; the even lane writes complex
+// columns 0..7 of the chunk, the odd lane 8..15.  Off-diagonal tiles also
+// write the mirrored entries A[c'][c] = conj(A[c][c']).
+__device__ __forceinline__ void epi_gram(const TcTile &t, const TcEpilogue &ep, int row, int col, const float (&v)[32],
+                                         int lane) {
+    float p[32];
+#pragma unroll
+    for (int j = 0; j < 32; ++j) p[j] = __shfl_xor_sync(0xffffffffu, v[j], 1);
+    const bool odd = lane & 1;
+    const UnitDesc u = ep.units[t.unit];
+    const int n = u.n, s = u.s;
+    float2 *A = ep.a32 + ep.mus[t.unit].a32_off;
+    const int c = (t.ti * BM + row) >> 1;
+    const int c1 = ((t.tj * BN + col) >> 1) + (odd ? 8 : 0);
+    if (c >= n) return;
+    float2 out[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        float e0 = odd ? p[16 + 2 * q] : v[2 * q];
+        float e1 = odd ? p[17 + 2 * q] : v[2 * q + 1];
+        float o0 = odd ? v[16 + 2 * q] : p[2 * q];
+        float o1 = odd ? v[17 + 2 * q] : p[2 * q + 1];
+        out[q] = make_float2(e0 + o1, e1 - o0);
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+        if (c1 + q < n) A[(int64_t)c * s + c1 + q] = out[q];
+    if (t.ti != t.tj) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q)
+            if (c1 + q < n) A[(int64_t)(c1 + q) * s + c] = make_float2(out[q].x, -out[q].y);
+    }
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_tc_gemm(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+              const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
+              const TcTile *__restrict__ tiles, TcEpilogue ep) {
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t s_bar[2 * STAGES + 1];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_abort;
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const TcTile t = tiles[blockIdx.x];
+    const uint32_t sbase = smem_u32(smem);
+    auto full = [&](int st) { return smem_u32(&s_bar[st]); };
+    auto empty = [&](int st) { return smem_u32(&s_bar[STAGES + st]); };
+    const uint32_t tfull = smem_u32(&s_bar[2 * STAGES]);
+    volatile int *abort_word = &s_abort;
+    if (threadIdx.x == 0) {
+        for (int i = 0; i < 2 * STAGES + 1; ++i) mbar_init(smem_u32(&s_bar[i]), 1);
+        s_abort = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            int issued = 0;
+            for (int kb = 0; kb < t.kblocks; ++kb) {
+                const int st = kb % STAGES;
+                const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+                if (kb >= STAGES && !mbar_wait(empty(st), ph ^ 1u, abort_word)) break;
+                const uint32_t dst = sbase + st * STAGE_BYTES;
+                mbar_expect_tx(full(st), STAGE_BYTES);
+                const int ya = t.a_row + kb * t.a_kstride, yb = t.b_row + kb * t.b_kstride;
+                tma_load_2d(dst, &mAh, 0, ya, full(st));
+                tma_load_2d(dst + BOX_BYTES, &mAl, 0, ya, full(st));
+                tma_load_2d(dst + 2 * BOX_BYTES, &mBh, 0, yb, full(st));
+                tma_load_2d(dst + 3 * BOX_BYTES, &mBl, 0, yb, full(st));
+                issued = kb + 1;
+            }
+            if (*abort_word)  // let the copies already issued land before the CTA exits
+                for (int kb = issued - 1; kb >= 0 && kb >= issued - STAGES; --kb)
+                    mbar_drain(full(kb % STAGES), (uint32_t)(kb / STAGES) & 1u);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            for (int kb = 0; kb < t.kblocks; ++kb) {
+                const int st = kb % STAGES;
+                const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+                if (!mbar_wait(full(st), ph, abort_word)) break;
+                tc_fence_after();
+                const uint32_t a_hi = sbase + st * STAGE_BYTES, a_lo = a_hi + BOX_BYTES;
+                const uint32_t b_hi = a_hi + 2 * BOX_BYTES, b_lo = a_hi + 3 * BOX_BYTES;
+#pragma unroll
+                for (int kk = 0; kk < BK / 8; ++kk) {
+                    const uint32_t off = kk * 32;  // 8 tf32 = 32 B along the swizzled row
+                    const uint64_t dah = sw128_kmajor_desc(a_hi + off), dal = sw128_kmajor_desc(a_lo + off);
+                    const uint64_t dbh = sw128_kmajor_desc(b_hi + off), dbl = sw128_kmajor_desc(b_lo + off);
+                    mma_tf32(tmem, dah, dbh, (kb | kk) != 0);
+                    mma_tf32(tmem, dah, dbl, 1u);
+                    mma_tf32(tmem, dal, dbh, 1u);
+                }
+                mma_commit(empty(st));
+            }
+            mma_commit(tfull);  // arrives once every MMA issued above has completed
+            if (*abort_word) mbar_drain(tfull, 0);
+        }
+    } else {
+        const bool ok = mbar_wait(tfull, 0, abort_word);
+        tc_fence_after();
+        if (ok) {
+            const int q = warp & 3;  // TMEM lane quarter this warp may access
+            const int row = q * 32 + lane;
+#pragma unroll 1
+            for (int cc = 0; cc < BN / 32; ++cc) {
+                float v[32];
+                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(cc * 32), v);
+                if (EPI == TC_EPI_STORE) epi_store(t, ep, row, cc * 32, v);
+                else epi_gram(t, ep, row, cc * 32, v, lane);
+            }
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+    if (threadIdx.x == 0 && *abort_word && ep.status) atomicExch(&ep.status[ep.status_of_tile ? t.unit : 0],
+                                                                 FNEC_UNIT_TIMEOUT);
+}
+
+// -- operand preparation -----------------------------------------------------
+__device__ __forceinline__ void split_tf32(float x, float &hi, float &lo) {
+    uint32_t h;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+    hi = __uint_as_float(h);
+    lo = x - hi;
+}
+
+// Row-major FP32 [rows][k] -> K-blocked hi/lo stacks (zero padded to
+// kblocks * 32 columns and rpad rows per k-block).
+__global__ void k_split_rows(const float *__restrict__ src, int rows, int k, int rpad, float *hi, float *lo) {
+    int kb = blockIdx.y, r = blockIdx.x * 8 + (threadIdx.x >> 5), j = threadIdx.x & 31;
+    if (r >= rpad) return;
+    int kk = kb * 32 + j;
+    float x = (r < rows && kk < k) ? src[(int64_t)r * k + kk] : 0.f;
+    float h, l;
+    split_tf32(x, h, l);
+    int64_t o = ((int64_t)kb * rpad + r) * 32 + j;
+    hi[o] = h;
+    lo[o] = l;
+}
+
+// Z (FP64 complex, N x N, row-major) -> the Gram operand T[2c+s][k] =
+// (Re, Im) Z[k][c] as K-blocked hi/lo stacks, one unit per blockIdx.z.
+// A 32 (k) x 16 (c) tile of Z is transposed through shared memory.
+__global__ void k_split_gram(const UnitDesc *__restrict__ units, const TcGramUnit *__restrict__ gu,
+                             const cx *__restrict__ zbuf, float *hi, float *lo) {
+    __shared__ float s_t[32][33];  // [2c+s local][k local]
+    const int ui = blockIdx.z;
+    const TcGramUnit g = gu[ui];
+    const UnitDesc u = units[g.unit];
+    const int n = u.n;
+    const int k0 = blockIdx.y * 32, c0 = blockIdx.x * 16;
+    if (k0 >= g.kblocks * 32 || 2 * c0 >= g.rpad) return;
+    const cx *z = zbuf + u.z_off;
+    const int tid = threadIdx.x;  // 256 threads
+    for (int e = tid; e < 32 * 16; e += 256) {
+        int kk = e / 16, cc = e % 16, k = k0 + kk, c = c0 + cc;
+        cx v = (k < n && c < n) ? z[(int64_t)k * n + c] : cx{0.0, 0.0};
+        s_t[2 * cc][kk] = (float)v.re;
+        s_t[2 * cc + 1][kk] = (float)v.im;
+    }
+    __syncthreads();
+    for (int e = tid; e < 32 * 32; e += 256) {
+        int rr = e / 32, kk = e % 32;
+        float h, l;
+        split_tf32(s_t[rr][kk], h, l);
+        int64_t o = ((int64_t)g.base + (int64_t)blockIdx.y * g.rpad + 2 * c0 + rr) * 32 + kk;
+        hi[o] = h;
+        lo[o] = l;
+    }
+}
+
+// -- host --------------------------------------------------------------------
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::once_flag g_encode_once;
+
+bool make_map(CUtensorMap *m, const float *base, int64_t rows) {
+    std::call_once(g_encode_once, [] {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    });
+    if (!g_encode || rows <= 0) return false;
+    cuuint64_t dims[2] = {32, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {32 * sizeof(float)};
+    cuuint32_t box[2] = {32, (cuuint32_t)BM};
+    cuuint32_t es[2] = {1, 1};
+    return g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(base), dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+size_t tc_smem_bytes() { return (size_t)STAGES * STAGE_BYTES + 1024; }
+
+template <int EPI>
+cudaError_t launch_tc(const CUtensorMap &ah, const CUtensorMap &al, const CUtensorMap &bh, const CUtensorMap &bl,
+                      const TcTile *tiles, int ntiles, const TcEpilogue &ep, cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)tc_smem_bytes());
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    if (ntiles <= 0) return cudaSuccess;
+    k_tc_gemm<EPI><<<ntiles, TC_THREADS, tc_smem_bytes(), st>>>(ah, al, bh, bl, tiles, ep);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+// Gram plan: per unit the operand base row, padded rows and k-blocks; the
+// tile list (upper triangle of 128x128 real tiles).
+cudaError_t tc_gram_plan(const std::vector<UnitDesc> &systems, TcGramPlan &p) {
+    p.units.clear();
+    p.tiles.clear();
+    int64_t rows = 0;
+    for (size_t i = 0; i < systems.size(); ++i) {
+        const int n = systems[i].n;
+        if (n <= 0) continue;
+        TcGramUnit g;
+        g.unit = (int)i;
+        g.kblocks = (n + 31) / 32;
+        g.rpad = ((2 * n + BM - 1) / BM) * BM;
+        g.base = rows;
+        rows += (int64_t)g.kblocks * g.rpad;
+        const int nt = g.rpad / BM;
+        for (int ti = 0; ti < nt; ++ti)
+            for (int tj = ti; tj < nt; ++tj) {
+                TcTile t;
+                t.a_row = (int32_t)(g.base + ti * BM);
+                t.b_row = (int32_t)(g.base + tj * BM);
+                t.a_kstride = t.b_kstride = g.rpad;
+                t.kblocks = g.kblocks;
+                t.unit = (int)i;
+                t.ti = ti;
+                t.tj = tj;
+                p.tiles.push_back(t);
+            }
+        p.units.push_back(g);
+    }
+    p.rows = rows;
+    return cudaSuccess;
+}
+
+bool tc_gram_maps(TcGramPlan &p, const float *hi, const float *lo) {
+    p.ready = make_map(&p.m_hi, hi, p.rows) && make_map(&p.m_lo, lo, p.rows);
+    return p.ready;
+}
+
+cudaError_t tc_gram_run(const TcGramPlan &p, const UnitDesc *d_units, const TcGramUnit *d_gu, const TcTile *d_tiles,
+                        const MixedUnit *d_mus, const cx *z, float *hi, float *lo, float2 *a32, int32_t *status,
+                        int max_n, cudaStream_t st) {
+    if (p.units.empty()) return cudaSuccess;
+    int max_kb = (max_n + 31) / 32, max_cb = (max_n + 15) / 16;
+    dim3 g(max_cb, max_kb, (unsigned)p.units.size());
+    k_split_gram<<<g, 256, 0, st>>>(d_units, d_gu, z, hi, lo);
+    TcEpilogue ep{};
+    ep.units = d_units;
+    ep.mus = d_mus;
+    ep.a32 = a32;
+    ep.status = status;
+    ep.status_of_tile = 1;
+    return launch_tc<TC_EPI_GRAM>(p.m_hi, p.m_lo, p.m_hi, p.m_lo, d_tiles, (int)p.tiles.size(), ep, st);
+}
+
+}  // namespace fnec
+
+using namespace fnec;
+
+extern "C" int fnec_selftest_tf32x3_gemm(int32_t device, uint64_t m, uint64_t n, uint64_t k, const float *a,
+                                         const float *b, float *c) {
+    if (!a || !b || !c || m == 0 || n == 0 || k == 0) return FNEC_ERR_BAD_ARG;
+    if (m > (1u << 16) || n > (1u << 16) || k > (1u << 16)) return FNEC_ERR_TOO_LARGE;
+    if (cudaSetDevice(device) != cudaSuccess) return FNEC_ERR_NO_DEVICE;
+    const int kb = (int)((k + 31) / 32);
+    const int mp = (int)((m + BM - 1) / BM) * BM, np = (int)((n + BN - 1) / BN) * BN;
+    float *da = nullptr, *db = nullptr, *dc = nullptr, *ops = nullptr;
+    TcTile *dt = nullptr;
+    int32_t *dst = nullptr;
+    size_t opa = (size_t)kb * mp * 32, opb = (size_t)kb * np * 32;
+    int rc = FNEC_OK;
+    std::vector<TcTile> tiles;
+    for (int ti = 0; ti < mp / BM; ++ti)
+        for (int tj = 0; tj < np / BN; ++tj) {
+            TcTile t;
+            t.a_row = ti * BM;
+            t.b_row = tj * BN;
+            t.a_kstride = mp;
+            t.b_kstride = np;
+            t.kblocks = kb;
+            t.unit = 0;
+            t.ti = ti;
+            t.tj = tj;
+            tiles.push_back(t);
+        }
+    do {
+        if (cudaMalloc(&da, sizeof(float) * m * k) != cudaSuccess || cudaMalloc(&db, sizeof(float) * n * k) != cudaSuccess ||
+            cudaMalloc(&dc, sizeof(float) * m * n) != cudaSuccess ||
+            cudaMalloc(&ops, sizeof(float) * 2 * (opa + opb)) != cudaSuccess ||
+            cudaMalloc(&dt, sizeof(TcTile) * tiles.size()) != cudaSuccess || cudaMalloc(&dst, sizeof(int32_t)) != cudaSuccess) {
+            rc = FNEC_ERR_OUT_OF_MEMORY;
+            break;
+        }
+        cudaMemcpy(da, a, sizeof(float) * m * k, cudaMemcpyHostToDevice);
+        cudaMemcpy(db, b, sizeof(float) * n * k, cudaMemcpyHostToDevice);
+        cudaMemcpy(dt, tiles.data(), sizeof(TcTile) * tiles.size(), cudaMemcpyHostToDevice);
+        cudaMemset(dst, 0, sizeof(int32_t));
+        float *ah = ops, *al = ops + opa, *bh = ops + 2 * opa, *bl = ops + 2 * opa + opb;
+        k_split_rows<<<dim3(mp / 8, kb), 256>>>(da, (int)m, (int)k, mp, ah, al);
+        k_split_rows<<<dim3(np / 8, kb), 256>>>(db, (int)n, (int)k, np, bh, bl);
+        CUtensorMap mah, mal, mbh, mbl;
+        if (!make_map(&mah, ah, (int64_t)kb * mp) || !make_map(&mal, al, (int64_t)kb * mp) ||
+            !make_map(&mbh, bh, (int64_t)kb * np) || !make_map(&mbl, bl, (int64_t)kb * np)) {
+            rc = FNEC_ERR_UNSUPPORTED;
+            break;
+        }
+        TcEpilogue ep{};
+        ep.c = dc;
+        ep.ldc = (int64_t)n;
+        ep.m = (int64_t)m;
+        ep.n = (int64_t)n;
+        ep.status = dst;
+        ep.status_of_tile = 0;
+        if (launch_tc<TC_EPI_STORE>(mah, mal, mbh, mbl, dt, (int)tiles.size(), ep, 0) != cudaSuccess) {
+            rc = FNEC_ERR_CUDA;
+            break;
+        }
+        if (cudaDeviceSynchronize() != cudaSuccess) {
+            rc = FNEC_ERR_CUDA;
+            break;
+        }
+        int32_t stv = 0;
+        cudaMemcpy(&stv, dst, sizeof(int32_t), cudaMemcpyDeviceToHost);
+        if (stv != 0) {
+            rc = FNEC_ERR_TIMEOUT;
+            break;
+        }
+        cudaMemcpy(c, dc, sizeof(float) * m * n, cudaMemcpyDeviceToHost);
+    } while (0);
+    cudaFree(da);
+    cudaFree(db);
+    cudaFree(dc);
+    cudaFree(ops);
+    cudaFree(dt);
+    cudaFree(dst);
+    return rc;
+}

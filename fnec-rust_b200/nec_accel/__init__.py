@@ -114,6 +114,8 @@ SIGNATURES = {
     "fnec_enumerate_devices": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_char_p, _U64]),
     "fnec_dispatch_frequency_point": (ctypes.c_int, [ctypes.c_int, _D]),
     "fnec_measure_fp64_peak": (ctypes.c_int, [ctypes.c_int, _P, _P]),
+    "fnec_selftest_tf32x3_gemm": (ctypes.c_int, [ctypes.c_int32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
+                                                 _P, _P, _P]),
     "fnec_radiation_pattern_noalloc": (ctypes.c_int, [_P, _U64, _P, _D, _I32, _P, _U64, _P, _P, _P]),
     "fnec_batch_create": (ctypes.c_int, [_P, _P, _U32, _I32, _P]),
     "fnec_batch_destroy": (ctypes.c_int, [_P]),
@@ -388,6 +390,21 @@ def enumerate_compute_adapters() -> list:
         lib().fnec_enumerate_devices(ctypes.byref(cnt), i, buf, 256)
         out.append({"name": buf.value.decode(), "backend": "cuda", "device_type": "DiscreteGpu"})
     return out
+
+
+def selftest_tf32x3_gemm(a: np.ndarray, b: np.ndarray, device: int = 0) -> np.ndarray:
+    """C = A B^T through the 3xTF32 tensor-core GEMM (A: m x k, B: n x k, FP32)."""
+    a = np.ascontiguousarray(a, np.float32)
+    b = np.ascontiguousarray(b, np.float32)
+    m, k = a.shape
+    n, k2 = b.shape
+    if k != k2:
+        raise ValueError("inner dimensions differ")
+    c = np.empty((m, n), np.float32)
+    st = lib().fnec_selftest_tf32x3_gemm(device, m, n, k, _ptr(a), _ptr(b), _ptr(c))
+    if st != 0:
+        raise AccelError(st, "selftest_tf32x3_gemm")
+    return c
 
 
 def measure_fp64_peak(device: int = 0):

@@ -256,6 +256,12 @@ int fnec_dispatch_frequency_point(int request_kind, double freq_hz);
  * roofline denominators of the FP64-bound kernels. */
 int fnec_measure_fp64_peak(int device, double *fma_tflops, double *muladd_tflops);
 
+/* Self-test of the 3xTF32 tensor-core GEMM that forms the mixed form's
+ * Gram matrix (no counterpart in the reference): C = A B^T with A (m x k),
+ * B (n x k) and C (m x n) row-major FP32 host arrays.  m, n, k <= 65536. */
+int fnec_selftest_tf32x3_gemm(int32_t device, uint64_t m, uint64_t n, uint64_t k, const float *a,
+                              const float *b, float *c);
+
 /* Radiation pattern that allocates no device memory.  No counterpart in
  * the reference: it serves callers that cannot call cudaMalloc -- a host
  * framework that owns all device memory through its own pool, a plugin held
