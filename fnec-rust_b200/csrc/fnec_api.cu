@@ -733,10 +733,10 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
         for (int i = 0; i < nu; ++i) b->grid.s_desc[i] = b->units[ord[i]].s;
         b->grid.steps = (b->max_s + 31) / 32;
         cudaDeviceGetAttribute(&b->grid.sms, cudaDevAttrMultiProcessorCount, ctx->device);
-        if (b->max_s > 400) {  // some panel may outgrow one CTA's shared memory
+        if (e == cudaSuccess) e = dalloc(b, &b->grid.d_order, (size_t)nu);
+        if (e == cudaSuccess) e = up(b, b->grid.d_order, ord);
+        if (b->max_s > 380) {  // some panel may outgrow one CTA's shared memory
             unsigned char *xg = nullptr, *sy = nullptr;
-            if (e == cudaSuccess) e = dalloc(b, &b->grid.d_order, (size_t)nu);
-            if (e == cudaSuccess) e = up(b, b->grid.d_order, ord);
             if (e == cudaSuccess) e = dalloc(b, &xg, grid_xchg_bytes());
             if (e == cudaSuccess) e = dalloc(b, &sy, grid_sync_bytes(b->grid.steps));
             b->grid.d_xchg = xg;
@@ -982,7 +982,7 @@ int fnec_batch_run(fnec_batch *b) {
         launch_gram_exact(b->d_units, nu, b->max_w, b->d_ants, b->d_gram_tiles, (int)b->gram_tiles.size(), b->d_ibuf,
                           b->d_cons, b->d_codes, b->d_z, b->d_rhs, b->d_cos, b->d_a, st);
         mark(4);
-        launch_factor_exact(b->d_units, nu, b->max_s, b->grid, b->d_a, b->d_piv, b->d_status, st);
+        L += launch_factor_exact(b->d_units, nu, b->max_s, b->grid, b->d_a, b->d_piv, b->d_status, st);
         mark(5);
         launch_backsub(b->d_units, nu, b->max_s, b->d_a, b->d_x, b->d_status, st);
         if (b->max_rhs > 1) {
@@ -991,8 +991,7 @@ int fnec_batch_run(fnec_batch *b) {
             L += 2;
         }
         mark(6);
-        int panels = (b->max_s + 31) / 32;
-        L += 3 + 1 + 3 * panels;
+        L += 3 + 1;  // Gram (3 kernels) and the back substitution
     }
     launch_feedpoints(b->d_solves, ns, b->d_ants, b->d_segs, b->d_ibuf, b->d_feeds, b->d_x, b->d_status,
                       b->d_feed_out, b->d_feed_row_off, st);

@@ -23,6 +23,13 @@ struct GridPlan {
 };
 size_t grid_xchg_bytes();        // bytes of d_xchg
 size_t grid_sync_bytes(int steps);
+// The units still active at panel step c0 (s > c0), in ranges [i0, i1) of
+// the s-descending order whose panel heights m = s - c0 share a power-of-two
+// class (<= 64, <= 128, ...); m_max is the range's tallest.  Starts at i_begin.
+struct StepClass {
+    int i0, i1, m_max;
+};
+void step_classes(const GridPlan &gp, int c0, int i_begin, std::vector<StepClass> &out);
 // How the panel at column c0 is factored (fnec_plain.cu): the number of
 // units that take the grid-wide kernel (0 none, -1 infeasible) and its shape.
 int plan_grid_panel(const GridPlan &gp, int c0, int thr_rows, int pnb, size_t elem, const void *kernel,
@@ -40,8 +47,9 @@ void launch_gram_exact(const UnitDesc *units, int nu, int max_w, const AntDesc *
                        int ngtiles, const int32_t *ibuf, const DevConstraint *cons,
                        const int32_t *codes, const cx *z, const cx *rhs, const double *cosv, cx *A,
                        cudaStream_t st);
-void launch_factor_exact(const UnitDesc *units, int nu, int max_s, const GridPlan &gp, cx *A,
-                         int32_t *piv, int32_t *status, cudaStream_t st);
+// returns the number of kernel launches issued
+uint64_t launch_factor_exact(const UnitDesc *units, int nu, int max_s, const GridPlan &gp, cx *A,
+                             int32_t *piv, int32_t *status, cudaStream_t st);
 void launch_backsub(const UnitDesc *units, int nu, int max_s, const cx *A, cx *x,
                     const int32_t *status, cudaStream_t st);
 void launch_feedpoints(const UnitDesc *solves, int ns, const AntDesc *ants, const DevSeg *segs,

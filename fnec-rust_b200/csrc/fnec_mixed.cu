@@ -25,6 +25,7 @@
 
 #include "fnec_grid.cuh"
 #include "fnec_mixed.h"
+#include "fnec_tc.h"
 
 namespace fnec {
 
@@ -241,28 +242,30 @@ __global__ void k_gram32_ccols(const UnitDesc *__restrict__ units, const AntDesc
 }
 
 // constraint rows (in row order) and lambda; one CTA per system
+// Constraint rows and the regulariser: A[c][c'] += m_qc m_qc' over the
+// constraint rows q touching column c (its CSR), then A[c][c] += 1e-8.
+// One thread owns each row c of A, so the updates need no atomics.
 __global__ void k_gram32_rest(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
-                              const MixedUnit *__restrict__ mus, const DevConRow *__restrict__ crows,
-                              float2 *a32buf) {
+                              const MixedUnit *__restrict__ mus, const int32_t *__restrict__ ibuf,
+                              const DevConRow *__restrict__ crows, float2 *a32buf) {
     UnitDesc u = units[blockIdx.x];
     AntDesc a = ants[u.ant];
-    int s = u.s;
+    int s = u.s, n = u.n;
     float2 *A = a32buf + mus[blockIdx.x].a32_off;
-    if (threadIdx.x == 0) {
-        const DevConRow *cr = crows + a.crow_off;
-        for (int q = 0; q < a.n_crow; ++q) {
-            int c0 = cr[q].c0, c1 = cr[q].c1;
-            float v1 = (float)cr[q].v1;
-            A[(int64_t)c0 * s + c0].x += 1.f;
-            if (c1 >= 0) {
-                A[(int64_t)c0 * s + c1].x += v1;
-                A[(int64_t)c1 * s + c0].x += v1;
-                A[(int64_t)c1 * s + c1].x += v1 * v1;
+    const DevConRow *cr = crows + a.crow_off;
+    const int32_t *ccptr = ibuf + a.ccptr_off, *ccq = ibuf + a.ccq_off;
+    for (int c = threadIdx.x; c < s; c += blockDim.x) {
+        float2 *row = A + (int64_t)c * s;
+        if (c < n)
+            for (int k = ccptr[c]; k < ccptr[c + 1]; ++k) {
+                DevConRow r = cr[ccq[k]];
+                float v1 = (float)r.v1;
+                float mc = (r.c0 == c ? 1.f : 0.f) + (r.c1 == c ? v1 : 0.f);
+                row[r.c0].x += mc * (r.c1 == r.c0 ? 1.f + v1 : 1.f);
+                if (r.c1 >= 0 && r.c1 != r.c0) row[r.c1].x += mc * v1;
             }
-        }
+        row[c].x += 1e-8f;
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < s; i += blockDim.x) A[(int64_t)i * s + i].x += 1e-8f;
 }
 
 // ---------------------------------------------------------------------------
@@ -277,12 +280,12 @@ __device__ __forceinline__ void piv_better32(float &bv, int &bi, float v, int i)
 
 __global__ void __launch_bounds__(256) k_panel32(const UnitDesc *__restrict__ units, const MixedUnit *__restrict__ mus,
                                                  int c0, float2 *a32buf, int32_t *piv_buf, int32_t *status,
-                                                 int skip_m) {
+                                                 int skip_m, const int32_t *__restrict__ order, int base) {
     __shared__ float s_v[8];
     __shared__ int s_i[8];
     __shared__ int s_p;
     __shared__ float2 s_prow[MNB];
-    int ui = blockIdx.x;
+    int ui = order[base + blockIdx.x];
     UnitDesc u = units[ui];
     int s = u.s;
     if (c0 >= s || s - c0 > skip_m || status[ui] != 0) return;  // skip_m: taller panels go grid-wide
@@ -347,12 +350,15 @@ constexpr int PANEL32_SMEM_MAX = 200 * 1024;
 
 __global__ void __launch_bounds__(256) k_panel32_smem(const UnitDesc *__restrict__ units,
                                                       const MixedUnit *__restrict__ mus, int c0, float2 *a32buf,
-                                                      int32_t *piv_buf, int32_t *status, int skip_m) {
+                                                      int32_t *piv_buf, int32_t *status, int skip_m, const int32_t *__restrict__ order, int base) {
+    // panel rows padded to PS = MNB + 1 entries: a column read by consecutive
+    // rows then falls on distinct banks
+    constexpr int PS = MNB + 1;
     extern __shared__ float2 s_pan32[];
     __shared__ float s_v[8];
     __shared__ int s_i[8];
     __shared__ int s_p;
-    int ui = blockIdx.x;
+    int ui = order[base + blockIdx.x];
     UnitDesc u = units[ui];
     int s = u.s;
     if (c0 >= s || s - c0 > skip_m || status[ui] != 0) return;  // skip_m: taller panels go grid-wide
@@ -360,9 +366,10 @@ __global__ void __launch_bounds__(256) k_panel32_smem(const UnitDesc *__restrict
     int32_t *piv = piv_buf + u.piv_off;
     int nb = min(MNB, s - c0), m = s - c0;
     int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int nw = blockDim.x >> 5;
     for (int e = tid; e < m * nb; e += blockDim.x) {
         int rr = e / nb, q = e % nb;
-        s_pan32[rr * MNB + q] = A[(int64_t)(c0 + rr) * s + c0 + q];
+        s_pan32[rr * PS + q] = A[(int64_t)(c0 + rr) * s + c0 + q];
     }
     __syncthreads();
     for (int c = c0; c < c0 + nb; ++c) {
@@ -370,7 +377,7 @@ __global__ void __launch_bounds__(256) k_panel32_smem(const UnitDesc *__restrict
         float bv = -1.f;
         int bi = -1;
         for (int r = c + tid; r < s; r += blockDim.x) {
-            float2 v = s_pan32[(r - c0) * MNB + lc];
+            float2 v = s_pan32[(r - c0) * PS + lc];
             piv_better32(bv, bi, v.x * v.x + v.y * v.y, r);
         }
 #pragma unroll
@@ -387,7 +394,7 @@ __global__ void __launch_bounds__(256) k_panel32_smem(const UnitDesc *__restrict
         if (tid == 0) {
             float v = s_v[0];
             int p = s_i[0];
-            for (int q = 1; q < (int)(blockDim.x >> 5); ++q) piv_better32(v, p, s_v[q], s_i[q]);
+            for (int q = 1; q < nw; ++q) piv_better32(v, p, s_v[q], s_i[q]);
             if (p < 0 || !(v > 0.f)) {
                 status[ui] = -(c + 1);
                 p = -1;
@@ -399,24 +406,27 @@ __global__ void __launch_bounds__(256) k_panel32_smem(const UnitDesc *__restrict
         int p = s_p;
         if (p < 0) return;
         if (p != c && tid < nb) {
-            float2 t0 = s_pan32[lc * MNB + tid];
-            s_pan32[lc * MNB + tid] = s_pan32[(p - c0) * MNB + tid];
-            s_pan32[(p - c0) * MNB + tid] = t0;
+            float2 t0 = s_pan32[lc * PS + tid];
+            s_pan32[lc * PS + tid] = s_pan32[(p - c0) * PS + tid];
+            s_pan32[(p - c0) * PS + tid] = t0;
         }
         __syncthreads();
-        const float2 *prow = s_pan32 + lc * MNB;
-        float2 diag = prow[lc];
-        for (int r = c + 1 + tid; r < s; r += blockDim.x) {
-            float2 *row = s_pan32 + (r - c0) * MNB;
-            float2 f = cf_div(row[lc], diag);
-            row[lc] = f;
-            for (int k = lc + 1; k < nb; ++k) row[k] = cf_sub(row[k], cf_mul(f, prow[k]));
+        // elimination: a warp per row, a lane per panel column
+        const float2 pj = lane < nb ? s_pan32[lc * PS + lane] : cf(0.f, 0.f);
+        const float2 diag = s_pan32[lc * PS + lc];
+#pragma unroll 4
+        for (int r = c + 1 + wid; r < s; r += nw) {
+            float2 *row = s_pan32 + (r - c0) * PS;
+            float2 x = lane < nb ? row[lane] : cf(0.f, 0.f);
+            float2 f = cf_div(make_float2(__shfl_sync(0xffffffffu, x.x, lc), __shfl_sync(0xffffffffu, x.y, lc)), diag);
+            if (lane == lc) row[lc] = f;
+            else if (lane > lc && lane < nb) row[lane] = cf_sub(x, cf_mul(f, pj));
         }
         __syncthreads();
     }
     for (int e = tid; e < m * nb; e += blockDim.x) {
         int rr = e / nb, q = e % nb;
-        A[(int64_t)(c0 + rr) * s + c0 + q] = s_pan32[rr * MNB + q];
+        A[(int64_t)(c0 + rr) * s + c0 + q] = s_pan32[rr * PS + q];
     }
 }
 
@@ -453,10 +463,10 @@ __global__ void __launch_bounds__(256) k_panel32_grid(const UnitDesc *__restrict
 __global__ void __launch_bounds__(64) k_swap_u12_32(const UnitDesc *__restrict__ units,
                                                     const MixedUnit *__restrict__ mus, int c0, float2 *a32buf,
                                                     const int32_t *__restrict__ piv_buf,
-                                                    const int32_t *__restrict__ status) {
+                                                    const int32_t *__restrict__ status, const int32_t *__restrict__ order, int base) {
     __shared__ float2 s_c[MNB][64];
     __shared__ float2 s_L[MNB][MNB + 1];
-    int ui = blockIdx.y;
+    int ui = order[base + blockIdx.y];
     UnitDesc u = units[ui];
     int s = u.s;
     if (c0 >= s || status[ui] != 0) return;
@@ -496,10 +506,10 @@ __global__ void __launch_bounds__(64) k_swap_u12_32(const UnitDesc *__restrict__
 }
 
 __global__ void __launch_bounds__(256) k_trailing32(const UnitDesc *__restrict__ units, const MixedUnit *__restrict__ mus,
-                                                    int c0, float2 *a32buf, const int32_t *__restrict__ status) {
+                                                    int c0, float2 *a32buf, const int32_t *__restrict__ status, const int32_t *__restrict__ order, int base) {
     __shared__ float2 s_l[64][MNB + 1];
     __shared__ float2 s_u[MNB][64];
-    int ui = blockIdx.y;
+    int ui = order[base + blockIdx.y];
     UnitDesc u = units[ui];
     int s = u.s;
     if (c0 + MNB >= s || status[ui] != 0) return;
@@ -648,35 +658,45 @@ __device__ void apply_A(const GmresCtx &g, const cx *v, cx *out, cx *sv, cx *st)
 // out = (L U)^-1 P in with the complex64 factor, blocked by 32 columns:
 // one warp solves each 32x32 diagonal block from registers (each lane holds
 // its row of the block), then all threads update the remaining rows with
-// fully unrolled, independent loads.  in/out are FP64, sy is smem (S).
-__device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, float2 *sy) {
+// fully unrolled, independent loads.  The factor is stored in FP32 but the
+// substitution runs in FP64: the preconditioner is then one fixed linear
+// operator (the stored L U) to FP64 rounding, so the preconditioned
+// residual GMRES minimises and tests is measured without an FP32 floor.
+// in/out are FP64, sy is shared memory (S).
+__device__ __forceinline__ cx f2z(float2 a) { return {(double)a.x, (double)a.y}; }
+
+__device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, cx *sy) {
     int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     int s = g.s;
-    for (int i = tid; i < s; i += blockDim.x) sy[i] = cf((float)in[i].re, (float)in[i].im);
+    for (int i = tid; i < s; i += blockDim.x) sy[i] = in[i];
     __syncthreads();
     if (tid == 0)
         for (int c = 0; c < s; ++c) {
             int p = g.piv[c];
             if (p != c) {
-                float2 t0 = sy[c];
+                cx t0 = sy[c];
                 sy[c] = sy[p];
                 sy[p] = t0;
             }
         }
     __syncthreads();
-    // forward: unit lower triangular
+    // forward: unit lower triangular (factor rows read 8 entries at a time
+    // to keep the register footprint small enough for several CTAs per SM)
     for (int c0 = 0; c0 < s; c0 += 32) {
         int nb = min(32, s - c0);
         if (wid == 0) {
-            float2 yl = lane < nb ? sy[c0 + lane] : cf(0.f, 0.f);
+            cx yl = lane < nb ? sy[c0 + lane] : cx{0, 0};
             const float2 *lrow = g.lu + (int64_t)(c0 + (lane < nb ? lane : 0)) * s + c0;
-            float2 lr[32];
+#pragma unroll 1
+            for (int c8 = 0; c8 < 32; c8 += 8) {
+                float2 lr[8];
 #pragma unroll
-            for (int c = 0; c < 32; ++c) lr[c] = (c < nb) ? lrow[c] : cf(0.f, 0.f);
+                for (int c = 0; c < 8; ++c) lr[c] = (c8 + c < nb) ? lrow[c8 + c] : cf(0.f, 0.f);
 #pragma unroll
-            for (int c = 0; c < 32; ++c) {
-                float yr = __shfl_sync(0xffffffffu, yl.x, c), yi = __shfl_sync(0xffffffffu, yl.y, c);
-                if (lane > c && lane < nb) yl = cf_sub(yl, cf_mul(lr[c], cf(yr, yi)));
+                for (int c = 0; c < 8; ++c) {
+                    double yr = __shfl_sync(0xffffffffu, yl.re, c8 + c), yi = __shfl_sync(0xffffffffu, yl.im, c8 + c);
+                    if (lane > c8 + c && lane < nb) yl = zsub(yl, zmul(f2z(lr[c]), cx{yr, yi}));
+                }
             }
             if (lane < nb) sy[c0 + lane] = yl;
         }
@@ -684,12 +704,15 @@ __device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, float2 *sy)
         if (nb == 32) {
             for (int r = c0 + 32 + tid; r < s; r += blockDim.x) {
                 const float2 *lrow = g.lu + (int64_t)r * s + c0;
-                float2 lr[32];
+                cx acc = sy[r];
 #pragma unroll
-                for (int c = 0; c < 32; ++c) lr[c] = lrow[c];
-                float2 acc = sy[r];
+                for (int c8 = 0; c8 < 32; c8 += 8) {
+                    float2 lr[8];
 #pragma unroll
-                for (int c = 0; c < 32; ++c) acc = cf_sub(acc, cf_mul(lr[c], sy[c0 + c]));
+                    for (int c = 0; c < 8; ++c) lr[c] = lrow[c8 + c];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) acc = zsub(acc, zmul(f2z(lr[c]), sy[c0 + c8 + c]));
+                }
                 sy[r] = acc;
             }
         }
@@ -699,17 +722,21 @@ __device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, float2 *sy)
     for (int c1 = s; c1 > 0; c1 -= 32) {
         int c0 = max(0, c1 - 32), nb = c1 - c0;
         if (wid == 0) {
-            float2 yl = lane < nb ? sy[c0 + lane] : cf(0.f, 0.f);
+            cx yl = lane < nb ? sy[c0 + lane] : cx{0, 0};
             const float2 *urow = g.lu + (int64_t)(c0 + (lane < nb ? lane : 0)) * s + c0;
-            float2 ur[32];
+#pragma unroll 1
+            for (int c8 = 24; c8 >= 0; c8 -= 8) {
+                float2 ur[8];
 #pragma unroll
-            for (int c = 0; c < 32; ++c) ur[c] = (c < nb) ? urow[c] : cf(1.f, 0.f);
+                for (int c = 0; c < 8; ++c) ur[c] = (c8 + c < nb) ? urow[c8 + c] : cf(1.f, 0.f);
 #pragma unroll
-            for (int c = 31; c >= 0; --c) {
-                if (c < nb) {
-                    if (lane == c) yl = cf_div(yl, ur[c]);
-                    float yr = __shfl_sync(0xffffffffu, yl.x, c), yi = __shfl_sync(0xffffffffu, yl.y, c);
-                    if (lane < c) yl = cf_sub(yl, cf_mul(ur[c], cf(yr, yi)));
+                for (int c = 7; c >= 0; --c) {
+                    const int cc = c8 + c;
+                    if (cc < nb) {
+                        if (lane == cc) yl = zdiv(yl, f2z(ur[c]));
+                        double yr = __shfl_sync(0xffffffffu, yl.re, cc), yi = __shfl_sync(0xffffffffu, yl.im, cc);
+                        if (lane < cc) yl = zsub(yl, zmul(f2z(ur[c]), cx{yr, yi}));
+                    }
                 }
             }
             if (lane < nb) sy[c0 + lane] = yl;
@@ -717,21 +744,24 @@ __device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, float2 *sy)
         __syncthreads();
         for (int r = tid; r < c0; r += blockDim.x) {
             const float2 *urow = g.lu + (int64_t)r * s + c0;
-            float2 acc = sy[r];
+            cx acc = sy[r];
             if (nb == 32) {
-                float2 ur[32];
 #pragma unroll
-                for (int c = 0; c < 32; ++c) ur[c] = urow[c];
+                for (int c8 = 0; c8 < 32; c8 += 8) {
+                    float2 ur[8];
 #pragma unroll
-                for (int c = 0; c < 32; ++c) acc = cf_sub(acc, cf_mul(ur[c], sy[c0 + c]));
+                    for (int c = 0; c < 8; ++c) ur[c] = urow[c8 + c];
+#pragma unroll
+                    for (int c = 0; c < 8; ++c) acc = zsub(acc, zmul(f2z(ur[c]), sy[c0 + c8 + c]));
+                }
             } else {
-                for (int c = 0; c < nb; ++c) acc = cf_sub(acc, cf_mul(urow[c], sy[c0 + c]));
+                for (int c = 0; c < nb; ++c) acc = zsub(acc, zmul(f2z(urow[c]), sy[c0 + c]));
             }
             sy[r] = acc;
         }
         __syncthreads();
     }
-    for (int i = tid; i < s; i += blockDim.x) out[i] = {(double)sy[i].x, (double)sy[i].y};
+    for (int i = tid; i < s; i += blockDim.x) out[i] = sy[i];
     __syncthreads();
 }
 
@@ -741,7 +771,7 @@ __device__ double vnorm(const cx *v, int s, double *red) {
     return sqrt(block_sum(a, red));
 }
 
-__global__ void __launch_bounds__(256) k_gmres_ir(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
+__global__ void __launch_bounds__(256, 3) k_gmres_ir(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
                                                   MixedUnit *mus, const int32_t *__restrict__ ibuf,
                                                   const DevConRow *__restrict__ crows, const cx *__restrict__ zbuf,
                                                   const cx *__restrict__ rhs, const double *__restrict__ cosv,
@@ -786,7 +816,7 @@ __global__ void __launch_bounds__(256) k_gmres_ir(const UnitDesc *__restrict__ u
     // staging vectors: shared memory when they fit, else the solve's work area
     cx *sv = staged ? reinterpret_cast<cx *>(s_dyn) : W + 4 * s + g.rows;
     cx *stv = sv + s;
-    float2 *sy = reinterpret_cast<float2 *>(stv + g.rows);
+    cx *sy = stv + g.rows;
 
     // b = M^H y (y is zero on the constraint rows)
     for (int i = tid; i < g.rows; i += blockDim.x) g.t[i] = i < g.n ? g.y[i] : cx{0, 0};
@@ -948,7 +978,7 @@ struct GGrid {
     GmresCtx g;
     const int32_t *ccptr, *ccq, *perm;
     cx *part;
-    float2 *y;
+    cx *y;
     cx *red;
     GridSync *gs;
     int32_t *status;
@@ -1036,34 +1066,32 @@ __device__ bool gg_apply(GGrid &c, const cx *v, cx *out) {
     return true;
 }
 
-// out = (L U)^-1 P in (the caller has synchronised after writing in)
+// out = (L U)^-1 P in (the caller has synchronised after writing in);
+// FP64 substitution with the FP32 factor, as apply_prec.
 __device__ bool gg_prec(GGrid &c, const cx *in, cx *out) {
     const GmresCtx &g = c.g;
     const int s = g.s, nblk = (s + 31) / 32;
-    __shared__ float2 s_yb[32];
-    for (int i = c.gt; i < s; i += c.T) {
-        cx v = ldcg_cx(in + c.perm[i]);
-        c.y[i] = cf((float)v.re, (float)v.im);
-    }
+    __shared__ cx s_yb[32];
+    for (int i = c.gt; i < s; i += c.T) c.y[i] = ldcg_cx(in + c.perm[i]);
     GG_SYNC(c);
     // forward, unit lower triangular
     for (int bk = 0; bk < nblk; ++bk) {
         const int c0 = bk * 32, nb = min(32, s - c0);
         if (bk % c.G == c.cta && c.wid == 0) {
-            float2 yl = c.lane < nb ? __ldcg(c.y + c0 + c.lane) : cf(0.f, 0.f);
+            cx yl = c.lane < nb ? ldcg_cx(c.y + c0 + c.lane) : cx{0, 0};
             const float2 *lrow = g.lu + (int64_t)(c0 + (c.lane < nb ? c.lane : 0)) * s + c0;
             float2 lr[32];
 #pragma unroll
             for (int q = 0; q < 32; ++q) lr[q] = (q < nb) ? lrow[q] : cf(0.f, 0.f);
 #pragma unroll
             for (int q = 0; q < 32; ++q) {
-                float yr = __shfl_sync(0xffffffffu, yl.x, q), yi = __shfl_sync(0xffffffffu, yl.y, q);
-                if (c.lane > q && c.lane < nb) yl = cf_sub(yl, cf_mul(lr[q], cf(yr, yi)));
+                double yr = __shfl_sync(0xffffffffu, yl.re, q), yi = __shfl_sync(0xffffffffu, yl.im, q);
+                if (c.lane > q && c.lane < nb) yl = zsub(yl, zmul(f2z(lr[q]), cx{yr, yi}));
             }
             if (c.lane < nb) c.y[c0 + c.lane] = yl;
         }
         GG_SYNC(c);
-        if (c.tid < nb) s_yb[c.tid] = __ldcg(c.y + c0 + c.tid);
+        if (c.tid < nb) s_yb[c.tid] = ldcg_cx(c.y + c0 + c.tid);
         __syncthreads();
         // owned blocks q > bk: q = bk+1+d with q % G == cta
         int q0 = bk + 1 + ((c.cta - (bk + 1)) % c.G + c.G) % c.G;
@@ -1072,15 +1100,15 @@ __device__ bool gg_prec(GGrid &c, const cx *in, cx *out) {
             int r = (q0 + (e >> 5) * c.G) * 32 + (e & 31);
             if (r >= s) continue;
             const float2 *lrow = g.lu + (int64_t)r * s + c0;
-            float2 acc = __ldcg(c.y + r);
+            cx acc = ldcg_cx(c.y + r);
             if (nb == 32) {
                 float2 lr[32];
 #pragma unroll
                 for (int k = 0; k < 32; ++k) lr[k] = lrow[k];
 #pragma unroll
-                for (int k = 0; k < 32; ++k) acc = cf_sub(acc, cf_mul(lr[k], s_yb[k]));
+                for (int k = 0; k < 32; ++k) acc = zsub(acc, zmul(f2z(lr[k]), s_yb[k]));
             } else {
-                for (int k = 0; k < nb; ++k) acc = cf_sub(acc, cf_mul(lrow[k], s_yb[k]));
+                for (int k = 0; k < nb; ++k) acc = zsub(acc, zmul(f2z(lrow[k]), s_yb[k]));
             }
             c.y[r] = acc;
         }
@@ -1090,7 +1118,7 @@ __device__ bool gg_prec(GGrid &c, const cx *in, cx *out) {
     for (int bk = nblk - 1; bk >= 0; --bk) {
         const int c0 = bk * 32, nb = min(32, s - c0);
         if (bk % c.G == c.cta && c.wid == 0) {
-            float2 yl = c.lane < nb ? __ldcg(c.y + c0 + c.lane) : cf(0.f, 0.f);
+            cx yl = c.lane < nb ? ldcg_cx(c.y + c0 + c.lane) : cx{0, 0};
             const float2 *urow = g.lu + (int64_t)(c0 + (c.lane < nb ? c.lane : 0)) * s + c0;
             float2 ur[32];
 #pragma unroll
@@ -1098,40 +1126,37 @@ __device__ bool gg_prec(GGrid &c, const cx *in, cx *out) {
 #pragma unroll
             for (int q = 31; q >= 0; --q) {
                 if (q < nb) {
-                    if (c.lane == q) yl = cf_div(yl, ur[q]);
-                    float yr = __shfl_sync(0xffffffffu, yl.x, q), yi = __shfl_sync(0xffffffffu, yl.y, q);
-                    if (c.lane < q) yl = cf_sub(yl, cf_mul(ur[q], cf(yr, yi)));
+                    if (c.lane == q) yl = zdiv(yl, f2z(ur[q]));
+                    double yr = __shfl_sync(0xffffffffu, yl.re, q), yi = __shfl_sync(0xffffffffu, yl.im, q);
+                    if (c.lane < q) yl = zsub(yl, zmul(f2z(ur[q]), cx{yr, yi}));
                 }
             }
             if (c.lane < nb) c.y[c0 + c.lane] = yl;
         }
         GG_SYNC(c);
         if (bk == 0) break;
-        if (c.tid < nb) s_yb[c.tid] = __ldcg(c.y + c0 + c.tid);
+        if (c.tid < nb) s_yb[c.tid] = ldcg_cx(c.y + c0 + c.tid);
         __syncthreads();
         // owned blocks q < bk: q = cta, cta + G, ...
         int nown = c.cta < bk ? (bk - 1 - c.cta) / c.G + 1 : 0;
         for (int e = c.tid; e < nown * 32; e += blockDim.x) {
             int r = (c.cta + (e >> 5) * c.G) * 32 + (e & 31);
             const float2 *urow = g.lu + (int64_t)r * s + c0;
-            float2 acc = __ldcg(c.y + r);
+            cx acc = ldcg_cx(c.y + r);
             if (nb == 32) {
                 float2 ur[32];
 #pragma unroll
                 for (int k = 0; k < 32; ++k) ur[k] = urow[k];
 #pragma unroll
-                for (int k = 0; k < 32; ++k) acc = cf_sub(acc, cf_mul(ur[k], s_yb[k]));
+                for (int k = 0; k < 32; ++k) acc = zsub(acc, zmul(f2z(ur[k]), s_yb[k]));
             } else {
-                for (int k = 0; k < nb; ++k) acc = cf_sub(acc, cf_mul(urow[k], s_yb[k]));
+                for (int k = 0; k < nb; ++k) acc = zsub(acc, zmul(f2z(urow[k]), s_yb[k]));
             }
             c.y[r] = acc;
         }
         __syncthreads();
     }
-    for (int i = c.gt; i < s; i += c.T) {
-        float2 v = __ldcg(c.y + i);
-        out[i] = {(double)v.x, (double)v.y};
-    }
+    for (int i = c.gt; i < s; i += c.T) out[i] = ldcg_cx(c.y + i);
     GG_SYNC(c);
     return true;
 }
@@ -1314,7 +1339,7 @@ __global__ void __launch_bounds__(256) k_gmres_grid(const UnitDesc *__restrict__
                                                     const cx *__restrict__ rhs, const double *__restrict__ cosv,
                                                     const float2 *__restrict__ a32buf, const int32_t *__restrict__ pivbuf,
                                                     cx *xbuf, cx *vbuf, cx *wbuf, int32_t *status,
-                                                    const int32_t *__restrict__ perm, cx *part, float2 *ybuf, cx *red,
+                                                    const int32_t *__restrict__ perm, cx *part, cx *ybuf, cx *red,
                                                     GridSync *gs) {
     UnitDesc u = units[ui];
     if (status[u.sys] != 0) return;
@@ -1453,7 +1478,7 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
             partmax = std::max<int64_t>(partmax, (int64_t)((u.n + GG_RC - 1) / GG_RC) * u.n);
         }
         size_t b_perm = sizeof(int32_t) * (size_t)smax, b_part = sizeof(cx) * (size_t)partmax,
-               b_y = sizeof(float2) * (size_t)smax, b_red = sizeof(cx) * 2 * GG_MAX_CTAS * (GM + 1),
+               b_y = sizeof(cx) * (size_t)smax, b_red = sizeof(cx) * 2 * GG_MAX_CTAS * (GM + 1),
                b_sync = sizeof(GridSync) * w.grid_solves.size();
         size_t gt = al(b_perm) + al(b_part) + al(b_y) + al(b_red) + al(b_sync);
         e = cudaMalloc(&w.grid_base, gt);
@@ -1463,7 +1488,7 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
         q += al(b_perm);
         w.g_part = (cx *)q;
         q += al(b_part);
-        w.g_y = (float2 *)q;
+        w.g_y = (cx *)q;
         q += al(b_y);
         w.g_red = (cx *)q;
         q += al(b_red);
@@ -1475,6 +1500,44 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_gmres_grid, 256, 0);
         w.grid_ctas = std::min(GG_MAX_CTAS, sms * std::min(per_sm, 1));
     }
+    {
+        // tensor-core Gram: operand stacks, per-unit layout and the tile list
+        TcGramPlan *p = new TcGramPlan();
+        tc_gram_plan(systems, *p);
+        if (!p->units.empty()) {
+            size_t b_st = sizeof(float) * 32 * (size_t)p->rows;
+            size_t b_gu = sizeof(TcGramUnit) * p->units.size(), b_t = sizeof(TcTile) * p->tiles.size();
+            size_t tot = 2 * al(b_st) + al(b_gu) + al(b_t);
+            e = cudaMalloc(&w.tc_base, tot);
+            if (e != cudaSuccess) {
+                delete p;
+                return e;
+            }
+            unsigned char *q = (unsigned char *)w.tc_base;
+            w.tc_hi = (float *)q;
+            q += al(b_st);
+            w.tc_lo = (float *)q;
+            q += al(b_st);
+            w.tc_gu = q;
+            q += al(b_gu);
+            w.tc_tiles = q;
+            w.bytes += tot;
+            e = cudaMemcpy(w.tc_gu, p->units.data(), b_gu, cudaMemcpyHostToDevice);
+            if (e == cudaSuccess) e = cudaMemcpy(w.tc_tiles, p->tiles.data(), b_t, cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) {
+                delete p;
+                return e;
+            }
+            if (!tc_gram_maps(*p, w.tc_hi, w.tc_lo)) {
+                delete p;
+                return cudaErrorNotSupported;  // no tensor-map encoder in this driver
+            }
+            for (const UnitDesc &u : systems) w.tc_max_n = std::max(w.tc_max_n, u.n);
+            w.tc = p;
+        } else {
+            delete p;
+        }
+    }
     e = cudaMemcpy(w.mu, mu.data(), sizeof(MixedUnit) * mu.size(), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(w.smu, sysmu.data(), sizeof(MixedUnit) * sysmu.size(), cudaMemcpyHostToDevice);
     return e;
@@ -1484,6 +1547,10 @@ void free_mixed(MixedWork &w) {
     if (w.base) cudaFree(w.base);
     if (w.grid_base) cudaFree(w.grid_base);
     w.grid_base = nullptr;
+    if (w.tc_base) cudaFree(w.tc_base);
+    w.tc_base = nullptr;
+    delete w.tc;
+    w.tc = nullptr;
     w.base = nullptr;
     w.bytes = 0;
 }
@@ -1502,12 +1569,18 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         ++L;
     }
     mark(0);
-    if (n_gram > 0) k_gram32_zz<<<n_gram, 256, 0, st>>>(d_units, mw.smu, gram_tiles, z, mw.a32);
+    if (mw.tc) {
+        tc_gram_run(*mw.tc, d_units, static_cast<const TcGramUnit *>(mw.tc_gu), static_cast<const TcTile *>(mw.tc_tiles),
+                    mw.smu, z, mw.tc_hi, mw.tc_lo, mw.a32, status, mw.tc_max_n, st);
+        ++L;
+    } else if (n_gram > 0) {
+        k_gram32_zz<<<n_gram, 256, 0, st>>>(d_units, mw.smu, gram_tiles, z, mw.a32);
+    }
     {
         dim3 g(max_w > 0 ? max_w : 1, nu);
         k_gram32_ccols<<<g, 256, 0, st>>>(d_units, d_ants, mw.smu, ibuf, z, cosv, mw.a32);
     }
-    k_gram32_rest<<<nu, 256, 0, st>>>(d_units, d_ants, mw.smu, crows, mw.a32);
+    k_gram32_rest<<<nu, 256, 0, st>>>(d_units, d_ants, mw.smu, ibuf, crows, mw.a32);
     L += 3;
     mark(1);
     static bool attr = false, attr_grid = false;
@@ -1519,50 +1592,59 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         cudaFuncSetAttribute(k_panel32_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
         attr_grid = true;
     }
-    const int thr_rows = PANEL32_SMEM_MAX / (int)(MNB * sizeof(float2));
+    const int thr_rows = PANEL32_SMEM_MAX / (int)((MNB + 1) * sizeof(float2));
+    const int32_t *ord = gp.d_order;
     if (gp.d_sync) cudaMemsetAsync(gp.d_sync, 0, grid_sync_bytes(gp.steps), st);
+    std::vector<StepClass> cls;
     for (int c0 = 0; c0 < max_s; c0 += MNB) {
-        int G = 0;
-        size_t gsm = 0;
-        int nl = plan_grid_panel(gp, c0, thr_rows, MNB, sizeof(float2), (const void *)k_panel32_grid, &G, &gsm);
-        if (nl > 0) {
-            PanelXchg<float2> *xg = static_cast<PanelXchg<float2> *>(gp.d_xchg);
-            GridSync *gs = static_cast<GridSync *>(gp.d_sync) + (size_t)(c0 / MNB) * GRID_PANEL_MAX_UNITS;
-            const int32_t *ord = gp.d_order;
-            const MixedUnit *smu = mw.smu;
-            float2 *a32 = mw.a32;
-            void *args[] = {(void *)&d_units, (void *)&smu, (void *)&ord, (void *)&c0, (void *)&a32,
-                            (void *)&piv, (void *)&status, (void *)&xg, (void *)&gs};
-            if (cudaLaunchCooperativeKernel((const void *)k_panel32_grid, dim3(G, nl), dim3(256), args, gsm, st) ==
-                cudaSuccess) {
-                int m_rest = std::min(max_s - c0, thr_rows);
-                k_panel32_smem<<<nu, 256, sizeof(float2) * (size_t)m_rest * MNB, st>>>(d_units, mw.smu, c0, mw.a32,
-                                                                                       piv, status, thr_rows);
-            } else {
-                (void)cudaGetLastError();
-                k_panel32<<<nu, 256, 0, st>>>(d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX);
+        // panels as in the plain path: tallest grid-wide (or one CTA from
+        // global memory), the rest one CTA from shared memory per size class
+        int n_thr = 0;
+        while (n_thr < (int)gp.s_desc.size() && gp.s_desc[n_thr] - c0 > thr_rows) ++n_thr;
+        if (n_thr > 0) {
+            int G = 0;
+            size_t gsm = 0;
+            bool done = false;
+            if (plan_grid_panel(gp, c0, thr_rows, MNB, sizeof(float2), (const void *)k_panel32_grid, &G, &gsm) ==
+                n_thr) {
+                PanelXchg<float2> *xg = static_cast<PanelXchg<float2> *>(gp.d_xchg);
+                GridSync *gs = static_cast<GridSync *>(gp.d_sync) + (size_t)(c0 / MNB) * GRID_PANEL_MAX_UNITS;
+                const MixedUnit *smu = mw.smu;
+                float2 *a32 = mw.a32;
+                void *args[] = {(void *)&d_units, (void *)&smu, (void *)&ord, (void *)&c0, (void *)&a32,
+                                (void *)&piv, (void *)&status, (void *)&xg, (void *)&gs};
+                done = cudaLaunchCooperativeKernel((const void *)k_panel32_grid, dim3(G, n_thr), dim3(256), args, gsm,
+                                                   st) == cudaSuccess;
+                if (!done) (void)cudaGetLastError();
             }
-        } else if (nl == 0) {
-            size_t pan = sizeof(float2) * (size_t)(max_s - c0) * MNB;
-            k_panel32_smem<<<nu, 256, pan, st>>>(d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX);
-        } else {
-            k_panel32<<<nu, 256, 0, st>>>(d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX);
-        }
-        dim3 g1((max_s + 63) / 64, nu);  // every column outside the panel
-        k_swap_u12_32<<<g1, 64, 0, st>>>(d_units, mw.smu, c0, mw.a32, piv, status);
-        int rows = max_s - (c0 + MNB);
-        L += 2;
-        if (rows > 0) {
-            int t = ((rows + 63) / 64) * ((rows + 63) / 64);
-            dim3 g2(t, nu);
-            k_trailing32<<<g2, 256, 0, st>>>(d_units, mw.smu, c0, mw.a32, status);
+            if (!done) k_panel32<<<n_thr, 256, 0, st>>>(d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX, ord, 0);
             ++L;
+        }
+        step_classes(gp, c0, n_thr, cls);
+        for (const StepClass &c : cls) {
+            k_panel32_smem<<<c.i1 - c.i0, 256, sizeof(float2) * (size_t)c.m_max * (MNB + 1), st>>>(
+                d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX, ord, c.i0);
+            ++L;
+        }
+        step_classes(gp, c0, 0, cls);
+        for (const StepClass &c : cls) {
+            int m = c.m_max;
+            dim3 g1((m + c0 + 63) / 64, c.i1 - c.i0);  // every column outside the panel
+            k_swap_u12_32<<<g1, 64, 0, st>>>(d_units, mw.smu, c0, mw.a32, piv, status, ord, c.i0);
+            ++L;
+            int rows = m - MNB;
+            if (rows > 0) {
+                int t = ((rows + 63) / 64) * ((rows + 63) / 64);
+                dim3 g2(t, c.i1 - c.i0);
+                k_trailing32<<<g2, 256, 0, st>>>(d_units, mw.smu, c0, mw.a32, status, ord, c.i0);
+                ++L;
+            }
         }
     }
     mark(2);
     int max_rows = 0;
     for (size_t i = 0; i < mw.host.size(); ++i) max_rows = max_rows > mw.host[i].rows ? max_rows : mw.host[i].rows;
-    size_t smem = sizeof(cx) * (size_t)(max_s + max_rows) + sizeof(float2) * (size_t)max_s;
+    size_t smem = sizeof(cx) * (size_t)(2 * max_s + max_rows);
     int staged = smem <= 200 * 1024;
     if (!staged) smem = 0;
     if (smem > 48 * 1024) cudaFuncSetAttribute(k_gmres_ir, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

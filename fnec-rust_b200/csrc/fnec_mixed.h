@@ -8,6 +8,8 @@
 
 namespace fnec {
 
+struct TcGramPlan;
+
 // Per-unit offsets into the mixed path's work buffers, and its refinement
 // statistics (written by the GMRES kernel).
 struct MixedUnit {
@@ -36,10 +38,16 @@ struct MixedWork {
     void *grid_base = nullptr;     // scratch shared by those launches
     int32_t *g_perm = nullptr;
     cx *g_part = nullptr;
-    float2 *g_y = nullptr;
+    cx *g_y = nullptr;
     cx *g_red = nullptr;
     void *g_sync = nullptr;
     int grid_ctas = 0;
+    // the Gram block Z^H Z on the tensor cores (fnec_tc.cu)
+    TcGramPlan *tc = nullptr;
+    void *tc_base = nullptr;
+    float *tc_hi = nullptr, *tc_lo = nullptr;
+    void *tc_gu = nullptr, *tc_tiles = nullptr;
+    int tc_max_n = 0;
 };
 
 // Phase events the mixed path records after its fill, Gram, factor and

@@ -399,12 +399,12 @@ __device__ __forceinline__ void piv_better(double &bv, int &bi, double v, int i)
 }
 
 __global__ void __launch_bounds__(256) k_panel(const UnitDesc *__restrict__ units, int c0,
-                                               cx *abuf, int32_t *piv_buf, int32_t *status, int skip_m) {
+                                               cx *abuf, int32_t *piv_buf, int32_t *status, int skip_m, const int32_t *__restrict__ order, int base) {
     __shared__ double s_v[8];
     __shared__ int s_i[8];
     __shared__ int s_p;
     __shared__ cx s_prow[NB];
-    int ui = blockIdx.x;
+    int ui = order[base + blockIdx.x];
     UnitDesc u = units[ui];
     int s = u.s;
     if (c0 >= s || s - c0 > skip_m || status[ui] != 0) return;  // skip_m: taller panels go grid-wide
@@ -473,12 +473,17 @@ __global__ void __launch_bounds__(256) k_panel(const UnitDesc *__restrict__ unit
 constexpr int PANEL_SMEM_MAX = 200 * 1024;
 
 __global__ void __launch_bounds__(256) k_panel_smem(const UnitDesc *__restrict__ units, int c0, cx *abuf,
-                                                    int32_t *piv_buf, int32_t *status, int skip_m) {
-    extern __shared__ cx s_pan[];  // [m][NB], m = s - c0
+                                                    int32_t *piv_buf, int32_t *status, int skip_m, const int32_t *__restrict__ order, int base) {
+    // rows padded to PS = NB + 1 entries (distinct banks down a column); the
+    // elimination runs a warp per row and a lane per panel column.  Each
+    // element still receives f = a_rc / a_cc and a_rk -= f a_ck in column
+    // order, as in k_panel.
+    constexpr int PS = NB + 1;
+    extern __shared__ cx s_pan[];  // [m][PS], m = s - c0
     __shared__ double s_v[8];
     __shared__ int s_i[8];
     __shared__ int s_p;
-    int ui = blockIdx.x;
+    int ui = order[base + blockIdx.x];
     UnitDesc u = units[ui];
     int s = u.s;
     if (c0 >= s || s - c0 > skip_m || status[ui] != 0) return;  // skip_m: taller panels go grid-wide
@@ -488,16 +493,17 @@ __global__ void __launch_bounds__(256) k_panel_smem(const UnitDesc *__restrict__
     int nb = min(NB, s - c0);
     int m = s - c0;
     int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int nw = blockDim.x >> 5;
     for (int e = tid; e < m * nb; e += blockDim.x) {
         int rr = e / nb, q = e % nb;
-        s_pan[rr * NB + q] = A[(int64_t)(c0 + rr) * w1 + c0 + q];
+        s_pan[rr * PS + q] = A[(int64_t)(c0 + rr) * w1 + c0 + q];
     }
     __syncthreads();
     for (int c = c0; c < c0 + nb; ++c) {
         int lc = c - c0;
         double bv = -1.0;
         int bi = -1;
-        for (int r = c + tid; r < s; r += blockDim.x) piv_better(bv, bi, cx_norm(s_pan[(r - c0) * NB + lc]), r);
+        for (int r = c + tid; r < s; r += blockDim.x) piv_better(bv, bi, cx_norm(s_pan[(r - c0) * PS + lc]), r);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             double ov = __shfl_down_sync(0xffffffffu, bv, o);
@@ -512,7 +518,7 @@ __global__ void __launch_bounds__(256) k_panel_smem(const UnitDesc *__restrict__
         if (tid == 0) {
             double v = s_v[0];
             int p = s_i[0];
-            for (int q = 1; q < (int)(blockDim.x >> 5); ++q) piv_better(v, p, s_v[q], s_i[q]);
+            for (int q = 1; q < nw; ++q) piv_better(v, p, s_v[q], s_i[q]);
             if (p < 0 || v < 1e-30) {
                 status[ui] = -(c + 1);
                 p = -1;
@@ -524,24 +530,27 @@ __global__ void __launch_bounds__(256) k_panel_smem(const UnitDesc *__restrict__
         int p = s_p;
         if (p < 0) return;
         if (p != c && tid < nb) {
-            cx t0 = s_pan[lc * NB + tid];
-            s_pan[lc * NB + tid] = s_pan[(p - c0) * NB + tid];
-            s_pan[(p - c0) * NB + tid] = t0;
+            cx t0 = s_pan[lc * PS + tid];
+            s_pan[lc * PS + tid] = s_pan[(p - c0) * PS + tid];
+            s_pan[(p - c0) * PS + tid] = t0;
         }
         __syncthreads();
-        const cx *prow = s_pan + lc * NB;
-        cx diag = prow[lc];
-        for (int r = c + 1 + tid; r < s; r += blockDim.x) {
-            cx *row = s_pan + (r - c0) * NB;
-            cx f = cx_div(row[lc], diag);
-            row[lc] = f;
-            for (int k = lc + 1; k < nb; ++k) row[k] = cx_sub(row[k], cx_mul(f, prow[k]));
+        const cx pj = lane < nb ? s_pan[lc * PS + lane] : cx_make(0.0, 0.0);
+        const cx diag = s_pan[lc * PS + lc];
+#pragma unroll 2
+        for (int r = c + 1 + wid; r < s; r += nw) {
+            cx *row = s_pan + (r - c0) * PS;
+            cx x = lane < nb ? row[lane] : cx_make(0.0, 0.0);
+            cx f = lane == lc ? cx_div(x, diag) : x;  // one division, then broadcast
+            f = cx_make(__shfl_sync(0xffffffffu, f.re, lc), __shfl_sync(0xffffffffu, f.im, lc));
+            if (lane == lc) row[lc] = f;
+            else if (lane > lc && lane < nb) row[lane] = cx_sub(x, cx_mul(f, pj));
         }
         __syncthreads();
     }
     for (int e = tid; e < m * nb; e += blockDim.x) {
         int rr = e / nb, q = e % nb;
-        A[(int64_t)(c0 + rr) * w1 + c0 + q] = s_pan[rr * NB + q];
+        A[(int64_t)(c0 + rr) * w1 + c0 + q] = s_pan[rr * PS + q];
     }
 }
 
@@ -583,10 +592,10 @@ __global__ void __launch_bounds__(256) k_panel_grid(const UnitDesc *__restrict__
 // row c0+q then receives the updates of panel columns c0..c0+q-1 in order.
 __global__ void __launch_bounds__(64) k_swap_u12(const UnitDesc *__restrict__ units, int c0, cx *abuf,
                                                  const int32_t *__restrict__ piv_buf,
-                                                 const int32_t *__restrict__ status) {
+                                                 const int32_t *__restrict__ status, const int32_t *__restrict__ order, int base) {
     __shared__ cx s_c[NB][64];
     __shared__ cx s_L[NB][NB];  // read as broadcasts: no padding needed
-    int ui = blockIdx.y;
+    int ui = order[base + blockIdx.y];
     UnitDesc u = units[ui];
     int s = u.s;
     if (c0 >= s || status[ui] != 0) return;
@@ -641,11 +650,11 @@ __global__ void __launch_bounds__(64) k_swap_u12(const UnitDesc *__restrict__ un
 // A22 -= L21 * U12 with per-element in-order accumulation over the panel.
 // grid.x = tiles of 64x64 over the trailing block, grid.y = unit.
 __global__ void __launch_bounds__(256) k_trailing(const UnitDesc *__restrict__ units, int c0,
-                                                  cx *abuf, const int32_t *__restrict__ status) {
+                                                  cx *abuf, const int32_t *__restrict__ status, const int32_t *__restrict__ order, int base) {
     extern __shared__ cx s_dyn[];
     cx(*s_l)[NB + 1] = reinterpret_cast<cx(*)[NB + 1]>(s_dyn);
     cx(*s_u)[64] = reinterpret_cast<cx(*)[64]>(s_dyn + 64 * (NB + 1));
-    int ui = blockIdx.y;
+    int ui = order[base + blockIdx.y];
     UnitDesc u = units[ui];
     int s = u.s;
     if (c0 + NB >= s || status[ui] != 0) return;  // no trailing block (or a failed unit)
@@ -965,8 +974,23 @@ int plan_grid_panel(const GridPlan &gp, int c0, int thr_rows, int pnb, size_t el
     return nl;
 }
 
-void launch_factor_exact(const UnitDesc *units, int nu, int max_s, const GridPlan &gp, cx *A,
-                         int32_t *piv, int32_t *status, cudaStream_t st) {
+void step_classes(const GridPlan &gp, int c0, int i_begin, std::vector<StepClass> &out) {
+    out.clear();
+    int i = i_begin, n = (int)gp.s_desc.size();
+    while (i < n && gp.s_desc[i] > c0) {
+        int m = gp.s_desc[i] - c0, hi = 64;
+        while (hi < m) hi *= 2;
+        int lo = hi == 64 ? 0 : hi / 2;  // the class holds heights (lo, hi]
+        StepClass c{i, i, m};
+        while (i < n && gp.s_desc[i] - c0 > lo) ++i;  // s descending: the class is a run
+        c.i1 = i;
+        out.push_back(c);
+    }
+}
+
+uint64_t launch_factor_exact(const UnitDesc *units, int nu, int max_s, const GridPlan &gp, cx *A,
+                             int32_t *piv, int32_t *status, cudaStream_t st) {
+    uint64_t L = 0;
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_trailing, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -975,50 +999,58 @@ void launch_factor_exact(const UnitDesc *units, int nu, int max_s, const GridPla
         cudaFuncSetAttribute(k_panel_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
         attr = true;
     }
-    const int thr_rows = PANEL_SMEM_MAX / (int)(NB * sizeof(cx));
+    (void)nu;
+    const int thr_rows = PANEL_SMEM_MAX / (int)((NB + 1) * sizeof(cx));
+    const int32_t *ord = gp.d_order;
     if (gp.d_sync) cudaMemsetAsync(gp.d_sync, 0, grid_sync_bytes(gp.steps), st);
+    std::vector<StepClass> cls;
     for (int c0 = 0; c0 < max_s; c0 += NB) {
-        int G = 0;
-        size_t gsm = 0;
-        int nl = plan_grid_panel(gp, c0, thr_rows, NB, sizeof(cx), (const void *)k_panel_grid, &G, &gsm);
-        if (nl > 0) {
-            int step = c0 / NB;
-            PanelXchg<cx> *xg = static_cast<PanelXchg<cx> *>(gp.d_xchg);
-            GridSync *gs = static_cast<GridSync *>(gp.d_sync) + (size_t)step * GRID_PANEL_MAX_UNITS;
-            const int32_t *ord = gp.d_order;
-            void *args[] = {(void *)&units, (void *)&ord, (void *)&c0, (void *)&A, (void *)&piv,
-                            (void *)&status, (void *)&xg, (void *)&gs};
-            if (cudaLaunchCooperativeKernel((const void *)k_panel_grid, dim3(G, nl), dim3(256), args, gsm, st) ==
-                cudaSuccess) {
-                // the rest: one CTA each, panels of at most thr_rows rows
-                int m_rest = std::min(max_s - c0, thr_rows);
-                k_panel_smem<<<nu, 256, sizeof(cx) * (size_t)m_rest * NB, st>>>(units, c0, A, piv, status,
-                                                                                 thr_rows);
-            } else {
-                (void)cudaGetLastError();  // not co-resident after all: one CTA per unit
-                k_panel<<<nu, 256, 0, st>>>(units, c0, A, piv, status, INT_MAX);
+        // panels: the tallest units (m > thr_rows) grid-wide or one CTA each
+        // from global memory, the rest one CTA each from shared memory, in
+        // size classes so that short panels do not reserve tall panels' memory
+        int n_thr = 0;
+        while (n_thr < (int)gp.s_desc.size() && gp.s_desc[n_thr] - c0 > thr_rows) ++n_thr;
+        if (n_thr > 0) {
+            int G = 0;
+            size_t gsm = 0;
+            bool done = false;
+            if (plan_grid_panel(gp, c0, thr_rows, NB, sizeof(cx), (const void *)k_panel_grid, &G, &gsm) == n_thr) {
+                PanelXchg<cx> *xg = static_cast<PanelXchg<cx> *>(gp.d_xchg);
+                GridSync *gs = static_cast<GridSync *>(gp.d_sync) + (size_t)(c0 / NB) * GRID_PANEL_MAX_UNITS;
+                void *args[] = {(void *)&units, (void *)&ord, (void *)&c0, (void *)&A, (void *)&piv,
+                                (void *)&status, (void *)&xg, (void *)&gs};
+                done = cudaLaunchCooperativeKernel((const void *)k_panel_grid, dim3(G, n_thr), dim3(256), args, gsm,
+                                                   st) == cudaSuccess;
+                if (!done) (void)cudaGetLastError();  // not co-resident after all
             }
-        } else if (nl == 0) {
-            size_t pan = sizeof(cx) * (size_t)(max_s - c0) * NB;
-            k_panel_smem<<<nu, 256, pan, st>>>(units, c0, A, piv, status, INT_MAX);
-        } else {
-            k_panel<<<nu, 256, 0, st>>>(units, c0, A, piv, status, INT_MAX);
+            if (!done) k_panel<<<n_thr, 256, 0, st>>>(units, c0, A, piv, status, INT_MAX, ord, 0);
+            ++L;
         }
-        // columns right of the panel: at least the right-hand side column
-        int rest = max_s + 1 - (c0 + NB);
-        if (rest < 1) rest = 1;
-        {
-            // trailing column blocks, then blocks for the c0 columns on the left
-            dim3 g1((rest + 63) / 64 + (c0 + 63) / 64, nu);
-            k_swap_u12<<<g1, 64, 0, st>>>(units, c0, A, piv, status);
-            int rows = max_s - (c0 + NB);
+        step_classes(gp, c0, n_thr, cls);
+        for (const StepClass &c : cls) {
+            k_panel_smem<<<c.i1 - c.i0, 256, sizeof(cx) * (size_t)c.m_max * (NB + 1), st>>>(units, c0, A, piv, status,
+                                                                                      INT_MAX, ord, c.i0);
+            ++L;
+        }
+        // deferred swaps + U12, then the trailing update, by size class
+        step_classes(gp, c0, 0, cls);
+        for (const StepClass &c : cls) {
+            int m = c.m_max;
+            int rest = m + 1 - NB;  // columns right of the panel, at least the right-hand side
+            if (rest < 1) rest = 1;
+            dim3 g1((rest + 63) / 64 + (c0 + 63) / 64, c.i1 - c.i0);
+            k_swap_u12<<<g1, 64, 0, st>>>(units, c0, A, piv, status, ord, c.i0);
+            ++L;
+            int rows = m - NB;
             if (rows > 0) {
                 int t = ((rows + 63) / 64) * ((rest + 63) / 64);
-                dim3 g2(t, nu);
-                k_trailing<<<g2, 256, TRAILING_SMEM, st>>>(units, c0, A, status);
+                dim3 g2(t, c.i1 - c.i0);
+                k_trailing<<<g2, 256, TRAILING_SMEM, st>>>(units, c0, A, status, ord, c.i0);
+                ++L;
             }
         }
     }
+    return L;
 }
 void launch_backsub(const UnitDesc *units, int nu, int max_s, const cx *A, cx *x,
                     const int32_t *status, cudaStream_t st) {

@@ -272,11 +272,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 }
 
 // -- operand preparation -----------------------------------------------------
+// x = hi + lo with both parts tf32 values, each rounded to nearest: the
+// tensor core then uses lo as given (it would otherwise drop lo's low 13
+// bits), so x is carried to ~2^-23 relative instead of ~2^-22.
 __device__ __forceinline__ void split_tf32(float x, float &hi, float &lo) {
-    uint32_t h;
+    uint32_t h, l;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
     hi = __uint_as_float(h);
-    lo = x - hi;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(x - hi));
+    lo = __uint_as_float(l);
 }
 
 // Row-major FP32 [rows][k] -> K-blocked hi/lo stacks (zero padded to

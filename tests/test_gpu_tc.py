@@ -1,8 +1,9 @@
 """The 3xTF32 tensor-core GEMM (tcgen05 + TMA) against a float64 product.
 
 3xTF32 keeps the hi*hi, hi*lo and lo*hi products of the tf32 splits, so
-its error is that of an FP32 GEMM: bounded here by 1e-6 of the row-norm x
-column-norm scale of each entry.
+its error is that of an FP32 GEMM: a random-walk accumulation error of
+about sqrt(k) * 6e-8 of the row-norm x column-norm scale of each entry,
+bounded here by 1e-7 * (sqrt(k) + 1).
 """
 import numpy as np
 import pytest
@@ -26,7 +27,7 @@ def test_tf32x3_gemm_matches_float64(acc, m, n, k):
     ref = a.astype(np.float64) @ b.astype(np.float64).T
     scale = np.outer(np.linalg.norm(a, axis=1), np.linalg.norm(b, axis=1))
     err = np.abs(c - ref) / scale
-    assert err.max() <= 1e-6, err.max()
+    assert err.max() <= 1e-7 * (np.sqrt(k) + 1), err.max()
 
 
 def test_tf32x3_beats_plain_tf32(acc):
