@@ -437,6 +437,49 @@ struct Packer {
 };
 
 // Pack host antennas into flat tables and allocate the device side.
+// Far-field coverage maps (see DevRp): requested points whose (theta, phi)
+// equal a power-integration direction's -- evaluated with the same
+// expressions as the far-field kernel -- reuse that direction's field.
+// Integration rows with sin(theta) == 0 are never evaluated (theta = 0), and
+// the last row is left out as well; PEC points below the horizon need no
+// field at all.
+static void ff_cover_maps(const DevRp &rp, const double *pts, int ground, std::vector<int32_t> &i2r,
+                          std::vector<int32_t> &xr) {
+    const bool pec = ground == 1;
+    const int n_th = pec ? 91 : 181;
+    const double th_max = pec ? 90.0 : 180.0;
+    const int n_int = rp.skip_integral ? 0 : n_th * 360;
+    const int n_req = rp.pts_off >= 0 ? rp.n_pts : rp.n_theta * rp.n_phi;
+    i2r.assign(n_int, -1);
+    xr.clear();
+    for (int p = 0; p < n_req; ++p) {
+        double th, ph;
+        if (rp.pts_off >= 0) {
+            th = pts[2 * p];
+            ph = pts[2 * p + 1];
+        } else {
+            int ip = p / rp.n_theta, it = p % rp.n_theta;
+            th = rp.theta0 + (double)it * rp.d_theta;
+            ph = rp.phi0 + (double)ip * rp.d_phi;
+        }
+        if (pec && th > 90.0) continue;  // clamped to -999.99 without a field
+        bool covered = false;
+        if (n_int > 0 && th >= 0.0 && ph >= 0.0 && ph < 360.0) {
+            double step = th_max / ((double)n_th - 1.0);
+            long it = std::lround(th / step), ip = std::lround(ph);
+            if (it >= 1 && it < n_th - 1 && ip >= 0 && ip < 360) {
+                double th_i = (double)it * th_max / ((double)n_th - 1.0), ph_i = (double)ip;
+                int d = (int)(it * 360 + ip);
+                if (th_i == th && ph_i == ph && i2r[d] < 0) {
+                    i2r[d] = p;
+                    covered = true;
+                }
+            }
+        }
+        if (!covered) xr.push_back(p);
+    }
+}
+
 static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, fnec_batch **out,
                        bool need_solve = true) {
     fnec_batch *b = new fnec_batch();
@@ -582,6 +625,15 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
             rp.pts_off = (int64_t)b->pts.size() / 2;
             rp.n_pts = (int32_t)(h.pts.size() / 2);
             b->pts.insert(b->pts.end(), h.pts.begin(), h.pts.end());
+        }
+        {
+            std::vector<int32_t> i2r, xr;
+            ff_cover_maps(rp, h.pts.data(), h.ground, i2r, xr);
+            rp.i2r_off = (int64_t)b->ibuf.size();
+            b->ibuf.insert(b->ibuf.end(), i2r.begin(), i2r.end());
+            rp.xr_off = (int64_t)b->ibuf.size();
+            b->ibuf.insert(b->ibuf.end(), xr.begin(), xr.end());
+            rp.n_xr = (int32_t)xr.size();
         }
         b->rps.push_back(rp);
         int64_t n_req = rp.pts_off >= 0 ? rp.n_pts : (int64_t)rp.n_theta * rp.n_phi;
@@ -998,7 +1050,7 @@ int fnec_batch_run(fnec_batch *b) {
     ++L;
     mark(7);
     if (b->ff_blocks > 0) {
-        launch_farfield(b->d_solves, ns, b->d_ants, b->d_runs, b->d_rps, b->d_pts, b->d_x, b->d_status, b->d_fld,
+        launch_farfield(b->d_solves, ns, b->d_ants, b->d_runs, b->d_rps, b->d_pts, b->d_ibuf, b->d_x, b->d_status, b->d_fld,
                         b->d_partials, b->ff_blocks, b->ff_smem, b->d_pat, b->d_total, st);
         L += 2;
     }
@@ -1277,7 +1329,7 @@ static int pattern_common(fnec_ctx *ctx, const fnec_gpu_segment *segments, uint6
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(b->d_x, currents, sizeof(cx) * n, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
-        launch_farfield(b->d_solves, 1, b->d_ants, b->d_runs, b->d_rps, b->d_pts, b->d_x, b->d_status, b->d_fld,
+        launch_farfield(b->d_solves, 1, b->d_ants, b->d_runs, b->d_rps, b->d_pts, b->d_ibuf, b->d_x, b->d_status, b->d_fld,
                         b->d_partials, b->ff_blocks, b->ff_smem, b->d_pat, b->d_total, s);
         e = cudaGetLastError();
     }

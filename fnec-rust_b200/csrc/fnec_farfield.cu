@@ -54,56 +54,131 @@ __device__ __forceinline__ void unit_vectors_dev(double th_deg, double ph_deg, d
     phh[2] = 0.0;
 }
 
-// Field of one direction: Horner sum over the antenna's runs (+ images).
-__device__ __forceinline__ void field_dir(const DevRun *runs, int n_run, const cx *cur, double k,
-                                          bool pec, const double *rh, const double *thh,
-                                          const double *phh, cx &ft, cx &fp) {
-    double ftr = 0, fti = 0, fpr = 0, fpi = 0;
+// Fields of two directions at once: Horner sums over the antenna's runs
+// (+ images).  The two recurrences are independent, so each current load
+// from shared memory feeds 8 FMAs on two dependency chains.
+__device__ __forceinline__ void field_dir2(const DevRun *runs, int n_run, const cx *cur, double k, bool pec,
+                                           const double *rh0, const double *th0, const double *ph0,
+                                           const double *rh1, const double *th1, const double *ph1, cx &ft0,
+                                           cx &fp0, cx &ft1, cx &fp1) {
+    double a_tr = 0, a_ti = 0, a_pr = 0, a_pi = 0;
+    double b_tr = 0, b_ti = 0, b_pr = 0, b_pi = 0;
     for (int q = 0; q < n_run; ++q) {
         const DevRun &R = runs[q];
         for (int img = 0; img < (pec ? 2 : 1); ++img) {
             double m0 = R.mid0[0], m1 = R.mid0[1], m2 = img ? -R.mid0[2] : R.mid0[2];
             double s0 = R.step[0], s1 = R.step[1], s2 = img ? -R.step[2] : R.step[2];
             double d0 = img ? -R.dir[0] : R.dir[0], d1 = img ? -R.dir[1] : R.dir[1], d2 = R.dir[2];
-            double p0 = k * (m0 * rh[0] + m1 * rh[1] + m2 * rh[2]);
-            double dp = k * (s0 * rh[0] + s1 * rh[1] + s2 * rh[2]);
-            double e0s, e0c, zs, zc;
-            sincos(p0, &e0s, &e0c);
-            sincos(dp, &zs, &zc);
+            double pa = k * (m0 * rh0[0] + m1 * rh0[1] + m2 * rh0[2]);
+            double da = k * (s0 * rh0[0] + s1 * rh0[1] + s2 * rh0[2]);
+            double pb = k * (m0 * rh1[0] + m1 * rh1[1] + m2 * rh1[2]);
+            double db = k * (s0 * rh1[0] + s1 * rh1[1] + s2 * rh1[2]);
+            double eas, eac, zas, zac, ebs, ebc, zbs, zbc;
+            sincos(pa, &eas, &eac);
+            sincos(da, &zas, &zac);
+            sincos(pb, &ebs, &ebc);
+            sincos(db, &zbs, &zbc);
             const cx *I = cur + R.first;
             int c = R.count;
-            double ar = I[c - 1].re, ai = I[c - 1].im;
+            cx last = I[c - 1];
+            double ar = last.re, ai = last.im, br = last.re, bi = last.im;
             for (int n = c - 2; n >= 0; --n) {
-                double nr = fma(ar, zc, fma(-ai, zs, I[n].re));
-                double ni = fma(ar, zs, fma(ai, zc, I[n].im));
-                ar = nr;
-                ai = ni;
+                cx v = I[n];
+                double nar = fma(ar, zac, fma(-ai, zas, v.re));
+                double nai = fma(ar, zas, fma(ai, zac, v.im));
+                double nbr = fma(br, zbc, fma(-bi, zbs, v.re));
+                double nbi = fma(br, zbs, fma(bi, zbc, v.im));
+                ar = nar;
+                ai = nai;
+                br = nbr;
+                bi = nbi;
             }
-            // F = exp(j p0) * acc * L
-            double fr = (e0c * ar - e0s * ai) * R.len;
-            double fi = (e0c * ai + e0s * ar) * R.len;
-            double pt = d0 * thh[0] + d1 * thh[1] + d2 * thh[2];
-            double pp = d0 * phh[0] + d1 * phh[1] + d2 * phh[2];
-            ftr = fma(fr, pt, ftr);
-            fti = fma(fi, pt, fti);
-            fpr = fma(fr, pp, fpr);
-            fpi = fma(fi, pp, fpi);
+            // F = exp(j p0) * acc * L, projected on theta-hat and phi-hat
+            double fr = (eac * ar - eas * ai) * R.len, fi = (eac * ai + eas * ar) * R.len;
+            double gr = (ebc * br - ebs * bi) * R.len, gi = (ebc * bi + ebs * br) * R.len;
+            double pta = d0 * th0[0] + d1 * th0[1] + d2 * th0[2];
+            double ppa = d0 * ph0[0] + d1 * ph0[1] + d2 * ph0[2];
+            double ptb = d0 * th1[0] + d1 * th1[1] + d2 * th1[2];
+            double ppb = d0 * ph1[0] + d1 * ph1[1] + d2 * ph1[2];
+            a_tr = fma(fr, pta, a_tr);
+            a_ti = fma(fi, pta, a_ti);
+            a_pr = fma(fr, ppa, a_pr);
+            a_pi = fma(fi, ppa, a_pi);
+            b_tr = fma(gr, ptb, b_tr);
+            b_ti = fma(gi, ptb, b_ti);
+            b_pr = fma(gr, ppb, b_pr);
+            b_pi = fma(gi, ppb, b_pi);
         }
     }
-    ft = cx_make(ftr, fti);
-    fp = cx_make(fpr, fpi);
+    ft0 = cx_make(a_tr, a_ti);
+    fp0 = cx_make(a_pr, a_pi);
+    ft1 = cx_make(b_tr, b_ti);
+    fp1 = cx_make(b_pr, b_pi);
 }
 
-// grid.x: direction blocks, grid.y: solve (status is per system).  Directions [0, n_int) are the
-// power-integration grid (theta outer, phi inner, as integrate_power_for_ground
-// iterates); [n_int, n_int + n_req) are the RP card points (phi outer, theta
-// inner, rp_card_points).  Requested fields go to fld_out (4 doubles per
-// point); each block writes one partial integral.
+// One direction's role: an integration direction (weight, and possibly the
+// requested point that coincides with it) or a requested point of its own.
+struct FfDir {
+    bool live;       // a field is needed
+    bool integ;      // contributes to the power integral with weight wgt
+    double wgt;
+    int req;         // requested point written with this field (-1: none)
+    bool below;      // requested point below a PEC ground: zeros
+    double th, ph;   // degrees
+};
+
+__device__ __forceinline__ FfDir ff_dir(int d, int n_int, int n_xr, int n_th, double th_max, bool pec,
+                                        const DevRp &rp, const double *pts, const int32_t *ibuf) {
+    FfDir r{false, false, 0.0, -1, false, 0.0, 0.0};
+    if (d < n_int) {
+        int it = d / 360, ip = d % 360;
+        r.th = (double)it * th_max / ((double)n_th - 1.0);
+        r.ph = (double)ip;
+        double sin_t = sin(r.th * RADS_PER_DEG);
+        double d_theta = (th_max * RADS_PER_DEG) / ((double)n_th - 1.0);
+        double d_phi = 2.0 * 3.14159265358979323846 / 360.0;
+        double w_t = (it == 0 || it == n_th - 1) ? 0.5 * d_theta : d_theta;
+        // farfield.rs:441 skips sin(theta) == 0 rows
+        if (sin_t != 0.0) {
+            r.live = r.integ = true;
+            r.wgt = sin_t * w_t * d_phi;
+            r.req = rp.i2r_off >= 0 ? ibuf[rp.i2r_off + d] : -1;
+        }
+    } else if (d < n_int + n_xr) {
+        int p = rp.i2r_off >= 0 ? ibuf[rp.xr_off + (d - n_int)] : d - n_int;
+        req_point(rp, pts, p, r.th, r.ph);
+        r.req = p;
+        r.below = pec && r.th > 90.0;
+        r.live = !r.below;
+    }
+    return r;
+}
+
+__device__ __forceinline__ void ff_store(double *fld_out, const UnitDesc &u, const FfDir &r, cx ft, cx fp) {
+    if (r.req < 0) return;
+    double *o = fld_out + 4 * (u.pat_off + r.req);
+    if (r.below) {
+        o[0] = o[1] = o[2] = o[3] = 0.0;
+        return;
+    }
+    o[0] = ft.re;
+    o[1] = ft.im;
+    o[2] = fp.re;
+    o[3] = fp.im;
+}
+
+// grid.x: direction blocks, grid.y: solve (status is per system).  Each
+// thread takes directions d and d + FF_THREADS of its block's 2*FF_THREADS.
+// Directions [0, n_int) are the power-integration grid (theta outer, phi
+// inner, as integrate_power_for_ground iterates); [n_int, n_int + n_xr)
+// the requested points not already covered by an integration direction.
+// Requested fields go to fld_out (4 doubles per point); each block writes
+// one partial integral.
 __global__ void __launch_bounds__(FF_THREADS) k_farfield(
     const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
     const DevRun *__restrict__ runs_all, const DevRp *__restrict__ rps, const double *__restrict__ pts,
-    const cx *__restrict__ xbuf, const int32_t *__restrict__ status, double *fld_out, double *partials,
-    int max_blocks, int staged) {
+    const int32_t *__restrict__ ibuf, const cx *__restrict__ xbuf, const int32_t *__restrict__ status,
+    double *fld_out, double *partials, int max_blocks, int staged) {
     extern __shared__ unsigned char s_raw[];
     __shared__ double s_red[FF_THREADS / 32];
     int ui = blockIdx.y;
@@ -115,8 +190,9 @@ __global__ void __launch_bounds__(FF_THREADS) k_farfield(
     double th_max = pec ? 90.0 : 180.0;
     int n_int = rp.skip_integral ? 0 : n_th * 360;
     int n_req = rp.pts_off >= 0 ? rp.n_pts : rp.n_theta * rp.n_phi;
-    int total = n_int + n_req;
-    int nblocks = (total + FF_THREADS - 1) / FF_THREADS;
+    int n_xr = rp.i2r_off >= 0 ? rp.n_xr : n_req;
+    int total = n_int + n_xr;
+    int nblocks = (total + 2 * FF_THREADS - 1) / (2 * FF_THREADS);
     if ((int)blockIdx.x >= nblocks) return;
     if (status[u.sys] != 0) {
         if (threadIdx.x == 0) partials[(int64_t)ui * max_blocks + blockIdx.x] = 0.0;
@@ -135,44 +211,23 @@ __global__ void __launch_bounds__(FF_THREADS) k_farfield(
     }
     __syncthreads();
 
-    int d = blockIdx.x * FF_THREADS + threadIdx.x;
+    const int d0 = blockIdx.x * 2 * FF_THREADS + threadIdx.x, d1 = d0 + FF_THREADS;
+    FfDir r0 = ff_dir(d0, n_int, n_xr, n_th, th_max, pec, rp, pts, ibuf);
+    FfDir r1 = ff_dir(d1, n_int, n_xr, n_th, th_max, pec, rp, pts, ibuf);
     double contrib = 0.0;
-    if (d < total) {
-        double th_deg, ph_deg;
-        bool integ = d < n_int;
-        double wgt = 0.0;
-        if (integ) {
-            int it = d / 360, ip = d % 360;
-            th_deg = (double)it * th_max / ((double)n_th - 1.0);
-            ph_deg = (double)ip;
-            double sin_t = sin(th_deg * RADS_PER_DEG);
-            double d_theta = (th_max * RADS_PER_DEG) / ((double)n_th - 1.0);
-            double d_phi = 2.0 * 3.14159265358979323846 / 360.0;
-            double w_t = (it == 0 || it == n_th - 1) ? 0.5 * d_theta : d_theta;
-            wgt = (sin_t == 0.0) ? 0.0 : sin_t * w_t * d_phi;
-            if (sin_t == 0.0) integ = false;  // farfield.rs:441 skips sin(theta) == 0 rows
-        } else {
-            req_point(rp, pts, d - n_int, th_deg, ph_deg);
-        }
-        bool below = !integ && d >= n_int && pec && th_deg > 90.0;
-        if ((integ || d >= n_int) && !below) {
-            double rh[3], thh[3], phh[3];
-            unit_vectors_dev(th_deg, ph_deg, rh, thh, phh);
-            cx ft, fp;
-            field_dir(s_runs, a.n_run, s_cur, u.k_rp, pec, rh, thh, phh, ft, fp);
-            if (integ) {
-                contrib = (ft.re * ft.re + ft.im * ft.im + fp.re * fp.re + fp.im * fp.im) * wgt;
-            } else {
-                double *o = fld_out + 4 * (u.pat_off + (d - n_int));
-                o[0] = ft.re;
-                o[1] = ft.im;
-                o[2] = fp.re;
-                o[3] = fp.im;
-            }
-        } else if (below) {
-            double *o = fld_out + 4 * (u.pat_off + (d - n_int));
-            o[0] = o[1] = o[2] = o[3] = 0.0;
-        }
+    if (r0.live || r1.live) {
+        double rh0[3], th0[3], ph0[3], rh1[3], th1[3], ph1[3];
+        unit_vectors_dev(r0.th, r0.ph, rh0, th0, ph0);
+        unit_vectors_dev(r1.th, r1.ph, rh1, th1, ph1);
+        cx ft0, fp0, ft1, fp1;
+        field_dir2(s_runs, a.n_run, s_cur, u.k_rp, pec, rh0, th0, ph0, rh1, th1, ph1, ft0, fp0, ft1, fp1);
+        if (r0.integ) contrib += (ft0.re * ft0.re + ft0.im * ft0.im + fp0.re * fp0.re + fp0.im * fp0.im) * r0.wgt;
+        if (r1.integ) contrib += (ft1.re * ft1.re + ft1.im * ft1.im + fp1.re * fp1.re + fp1.im * fp1.im) * r1.wgt;
+        ff_store(fld_out, u, r0, ft0, fp0);
+        ff_store(fld_out, u, r1, ft1, fp1);
+    } else {
+        ff_store(fld_out, u, r0, cx_make(0.0, 0.0), cx_make(0.0, 0.0));
+        ff_store(fld_out, u, r1, cx_make(0.0, 0.0), cx_make(0.0, 0.0));
     }
     // deterministic block reduction of the integral contributions
 #pragma unroll
@@ -201,7 +256,8 @@ __global__ void k_gains(const UnitDesc *__restrict__ units, const AntDesc *__res
     bool pec = a.ground == 1;
     int n_int = rp.skip_integral ? 0 : (pec ? 91 : 181) * 360;
     int n_req = rp.pts_off >= 0 ? rp.n_pts : rp.n_theta * rp.n_phi;
-    int nblocks = (n_int + n_req + FF_THREADS - 1) / FF_THREADS;
+    int n_xr = rp.i2r_off >= 0 ? rp.n_xr : n_req;
+    int nblocks = (n_int + n_xr + 2 * FF_THREADS - 1) / (2 * FF_THREADS);
     if (threadIdx.x == 0) {
         double t = 0.0;
         if (rp.skip_integral) t = rp.total_given;
@@ -246,11 +302,11 @@ __global__ void k_gains(const UnitDesc *__restrict__ units, const AntDesc *__res
 }
 
 int farfield_max_blocks(int n_int_max, int n_req_max) {
-    return (n_int_max + n_req_max + FF_THREADS - 1) / FF_THREADS;
+    return (n_int_max + n_req_max + 2 * FF_THREADS - 1) / (2 * FF_THREADS);
 }
 
 void launch_farfield(const UnitDesc *units, int nu, const AntDesc *ants, const DevRun *runs,
-                     const DevRp *rps, const double *pts, const cx *x, const int32_t *status,
+                     const DevRp *rps, const double *pts, const int32_t *ibuf, const cx *x, const int32_t *status,
                      double *fld,
                      double *partials, int max_blocks, size_t smem, double *pat_out,
                      double *total_out, cudaStream_t st) {
@@ -260,7 +316,7 @@ void launch_farfield(const UnitDesc *units, int nu, const AntDesc *ants, const D
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_farfield, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     dim3 g(max_blocks, nu);
-    k_farfield<<<g, FF_THREADS, smem, st>>>(units, ants, runs, rps, pts, x, status, fld, partials,
+    k_farfield<<<g, FF_THREADS, smem, st>>>(units, ants, runs, rps, pts, ibuf, x, status, fld, partials,
                                             max_blocks, staged);
     k_gains<<<nu, 256, 0, st>>>(units, ants, rps, pts, status, fld, partials, max_blocks, pat_out,
                                 total_out);

@@ -61,8 +61,10 @@ void launch_extra_rhs_exact(const UnitDesc *solves, int ns, int max_s, const Ant
 
 // fnec_farfield.cu
 int farfield_max_blocks(int n_int_max, int n_req_max);
+// ibuf: the int32 buffer the DevRp coverage maps index (may be null when
+// every DevRp has i2r_off < 0)
 void launch_farfield(const UnitDesc *units, int nu, const AntDesc *ants, const DevRun *runs,
-                     const DevRp *rps, const double *pts, const cx *x, const int32_t *status,
+                     const DevRp *rps, const double *pts, const int32_t *ibuf, const cx *x, const int32_t *status,
                      double *fld, double *partials, int max_blocks, size_t smem, double *pat_out,
                      double *total_out, cudaStream_t st);
 

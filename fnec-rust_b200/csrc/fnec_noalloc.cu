@@ -29,7 +29,7 @@ namespace {
 
 constexpr int NA_MAX_SEGMENTS = FNEC_NOALLOC_MAX_SEGMENTS;
 constexpr int NA_MAX_POINTS = FNEC_NOALLOC_MAX_POINTS;
-constexpr int NA_MAX_BLOCKS = 1024;  // >= (181*360 + NA_MAX_POINTS + 127) / 128
+constexpr int NA_MAX_BLOCKS = 1024;  // >= (181*360 + NA_MAX_POINTS + 255) / 256 far-field blocks
 
 struct NoallocScratch {
     UnitDesc unit;
@@ -124,6 +124,8 @@ __global__ void k_na_setup(NoallocScratch *S, const fnec_gpu_segment *__restrict
     rp.pts_off = 0;
     rp.n_pts = p;
     rp.skip_integral = 0;
+    rp.i2r_off = -1;  // no coverage maps: every requested point on its own
+    rp.n_xr = p;
     S->rp = rp;
     S->status = 0;
     S->total = 0.0;
@@ -161,7 +163,7 @@ extern "C" int fnec_radiation_pattern_noalloc(const fnec_gpu_segment *d_segments
     int max_blocks = farfield_max_blocks(n_int, (int)p);
     // n_run <= n bounds the staged run table
     size_t smem = sizeof(DevRun) * (size_t)n + sizeof(cx) * (size_t)n;
-    launch_farfield(&S->unit, 1, &S->ant, S->runs, &S->rp, d_points, reinterpret_cast<const cx *>(d_currents),
+    launch_farfield(&S->unit, 1, &S->ant, S->runs, &S->rp, d_points, nullptr, reinterpret_cast<const cx *>(d_currents),
                     &S->status, S->fld, S->partials, max_blocks, smem, S->pat, &S->total, s);
     int rb = (int)((p + 255) / 256);
     k_na_repack<<<rb > 0 ? rb : 1, 256, 0, s>>>(S, (int)p, d_out, d_total);

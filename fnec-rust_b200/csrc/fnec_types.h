@@ -139,6 +139,15 @@ struct DevRp {
     int32_t n_pts;
     int32_t skip_integral;  // 1: use total_given instead of integrating
     double total_given;
+    // Requested points that coincide with a power-integration direction
+    // reuse its field: i2r (int32[n_int], -1 = none) maps integration
+    // directions to requested points; the other requested points are
+    // listed in xr (int32[n_xr]).  i2r_off < 0: no maps, every requested
+    // point is computed on its own (n_xr = all of them, in order).
+    int64_t i2r_off;
+    int64_t xr_off;
+    int32_t n_xr;
+    int32_t pad_rp;
 };
 
 // Constraint-row contribution codes: bit 1 set -> the conj side is -1,
