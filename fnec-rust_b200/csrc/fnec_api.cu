@@ -371,6 +371,8 @@ struct fnec_batch {
     int32_t *d_piv = nullptr, *d_status = nullptr;
     double *d_feed_out = nullptr, *d_fld = nullptr, *d_partials = nullptr, *d_pat = nullptr,
            *d_total = nullptr;
+    cx *d_cur = nullptr;           // compact currents (read into pinned memory)
+    int64_t *d_cur_off = nullptr;  // per solve: its first entry in d_cur
     MixedWork mixed;
     GridPlan grid;
     std::vector<int32_t> grid_order;
@@ -776,6 +778,14 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
     DA(d_pat, PAT_STRIDE * b->pat_el);
     DA(d_total, b->solves.size());
     {
+        int64_t tc = b->uinfo.empty() ? 0 : b->uinfo.back().cur_off + b->uinfo.back().n;
+        std::vector<int64_t> co(b->uinfo.size());
+        for (size_t u = 0; u < co.size(); ++u) co[u] = b->uinfo[u].cur_off;
+        DA(d_cur, tc);
+        DA(d_cur_off, co.size());
+        if (e == cudaSuccess) e = up(b, b->d_cur_off, co);
+    }
+    {
         // grid-wide panels: units by s, tallest first
         std::vector<int32_t> &ord = b->grid_order;
         ord.resize(nu);
@@ -1091,6 +1101,41 @@ int fnec_batch_sync(fnec_batch *b) {
     return FNEC_OK;
 }
 
+namespace fnec {
+// currents of every solve, compacted (the c_hom tail of each x dropped)
+__global__ void k_gather_currents(const UnitDesc *__restrict__ solves, const int64_t *__restrict__ cur_off,
+                                  const cx *__restrict__ x, cx *cur) {
+    const UnitDesc u = solves[blockIdx.x];
+    for (int i = threadIdx.x; i < u.n; i += blockDim.x) cur[cur_off[blockIdx.x] + i] = x[u.x_off + i];
+}
+}  // namespace fnec
+
+// Page-locked host memory (cudaMallocHost or registered): copies into it
+// need no staging.
+static bool is_pinned(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+extern "C" int fnec_host_alloc(uint64_t bytes, void **out) {
+    if (!out) return FNEC_ERR_BAD_ARG;
+    *out = nullptr;
+    if (cudaMallocHost(out, bytes ? bytes : 1) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return FNEC_ERR_OUT_OF_MEMORY;
+    }
+    return FNEC_OK;
+}
+
+extern "C" int fnec_host_free(void *p) {
+    if (p && cudaFreeHost(p) != cudaSuccess) return FNEC_ERR_CUDA;
+    return FNEC_OK;
+}
+
 int fnec_batch_read(fnec_batch *b, double *currents, double *feeds, double *pattern, int32_t *status,
                     double *total_radiated) {
     if (!b) return FNEC_ERR_BAD_ARG;
@@ -1105,26 +1150,39 @@ int fnec_batch_read(fnec_batch *b, double *currents, double *feeds, double *patt
     unsigned char *hs = hp + sizeof(double) * PAT_STRIDE * (size_t)b->pat_el;
     unsigned char *ht = hs + sizeof(int32_t) * (size_t)nu;
     size_t fb = sizeof(double) * 7 * (size_t)b->feed_rows, pb = sizeof(double) * PAT_STRIDE * (size_t)b->pat_el;
-    if (currents) CUDA_TRY(ctx, cudaMemcpyAsync(hx, b->d_x, sizeof(cx) * b->x_el, cudaMemcpyDeviceToHost, st));
-    if (feeds && fb) CUDA_TRY(ctx, cudaMemcpyAsync(hf, b->d_feed_out, fb, cudaMemcpyDeviceToHost, st));
-    if (pattern && pb) CUDA_TRY(ctx, cudaMemcpyAsync(hp, b->d_pat, pb, cudaMemcpyDeviceToHost, st));
+    const int64_t tc = b->uinfo.empty() ? 0 : b->uinfo.back().cur_off + b->uinfo.back().n;
+    // caller arrays in page-locked memory are written directly; others
+    // through the pinned staging buffer
+    const bool pc = currents && is_pinned(currents), pf = feeds && fb && is_pinned(feeds),
+               pp = pattern && pb && is_pinned(pattern), pt = total_radiated && is_pinned(total_radiated);
+    if (currents && pc && tc > 0) {
+        k_gather_currents<<<ns, 128, 0, st>>>(b->d_solves, b->d_cur_off, b->d_x, b->d_cur);
+        CUDA_TRY(ctx, cudaMemcpyAsync(currents, b->d_cur, sizeof(cx) * tc, cudaMemcpyDeviceToHost, st));
+    } else if (currents) {
+        CUDA_TRY(ctx, cudaMemcpyAsync(hx, b->d_x, sizeof(cx) * b->x_el, cudaMemcpyDeviceToHost, st));
+    }
+    if (feeds && fb)
+        CUDA_TRY(ctx, cudaMemcpyAsync(pf ? (void *)feeds : (void *)hf, b->d_feed_out, fb, cudaMemcpyDeviceToHost, st));
+    if (pattern && pb)
+        CUDA_TRY(ctx, cudaMemcpyAsync(pp ? (void *)pattern : (void *)hp, b->d_pat, pb, cudaMemcpyDeviceToHost, st));
     if (status) CUDA_TRY(ctx, cudaMemcpyAsync(hs, b->d_status, sizeof(int32_t) * nu, cudaMemcpyDeviceToHost, st));
     if (total_radiated)
-        CUDA_TRY(ctx, cudaMemcpyAsync(ht, b->d_total, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(ctx, cudaMemcpyAsync(pt ? (void *)total_radiated : (void *)ht, b->d_total, sizeof(double) * ns,
+                                      cudaMemcpyDeviceToHost, st));
     CUDA_TRY(ctx, cudaStreamSynchronize(st));
-    if (currents) {
+    if (currents && !pc) {
         const cx *x = (const cx *)hx;
         for (int u = 0; u < ns; ++u)
             std::memcpy(currents + 2 * b->uinfo[u].cur_off, &x[b->solves[u].x_off], sizeof(cx) * b->solves[u].n);
     }
-    if (feeds && fb) std::memcpy(feeds, hf, fb);
-    if (pattern && pb) std::memcpy(pattern, hp, pb);
+    if (feeds && fb && !pf) std::memcpy(feeds, hf, fb);
+    if (pattern && pb && !pp) std::memcpy(pattern, hp, pb);
     if (status) {  // per solve: the status of its system
         const int32_t *sst = (const int32_t *)hs;
         std::vector<int32_t> tmp(sst, sst + nu);
         for (int u = 0; u < ns; ++u) status[u] = tmp[b->solves[u].sys];
     }
-    if (total_radiated) std::memcpy(total_radiated, ht, sizeof(double) * ns);
+    if (total_radiated && !pt) std::memcpy(total_radiated, ht, sizeof(double) * ns);
     return FNEC_OK;
 }
 

@@ -114,6 +114,8 @@ SIGNATURES = {
     "fnec_enumerate_devices": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_char_p, _U64]),
     "fnec_dispatch_frequency_point": (ctypes.c_int, [ctypes.c_int, _D]),
     "fnec_measure_fp64_peak": (ctypes.c_int, [ctypes.c_int, _P, _P]),
+    "fnec_host_alloc": (ctypes.c_int, [ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
+    "fnec_host_free": (ctypes.c_int, [_P]),
     "fnec_selftest_tf32x3_gemm": (ctypes.c_int, [ctypes.c_int32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
                                                  _P, _P, _P]),
     "fnec_radiation_pattern_noalloc": (ctypes.c_int, [_P, _U64, _P, _D, _I32, _P, _U64, _P, _P, _P]),
@@ -501,12 +503,14 @@ class HallenBatch:
             ui = _UnitInfo()
             lib().fnec_batch_get_unit_info(self._h, u, ctypes.byref(ui))
             self.units.append({k: getattr(ui, k) for k, _ in _UnitInfo._fields_})
-        # host result buffers, allocated once
-        self._cur = np.zeros(max(info.total_currents, 1), np.complex128)
-        self._feed = np.zeros((max(info.total_feeds, 1), 7), np.float64)
-        self._pat = np.zeros((max(info.total_points, 1), 6), np.float64)
-        self._status = np.zeros(max(info.n_units, 1), np.int32)
-        self._total = np.zeros(max(info.n_units, 1), np.float64)
+        # host result buffers, allocated once in page-locked memory: the
+        # library copies straight into them
+        self._host = []
+        self._cur = self._pinned((max(info.total_currents, 1),), np.complex128)
+        self._feed = self._pinned((max(info.total_feeds, 1), 7), np.float64)
+        self._pat = self._pinned((max(info.total_points, 1), 6), np.float64)
+        self._status = self._pinned((max(info.n_units, 1),), np.int32)
+        self._total = self._pinned((max(info.n_units, 1),), np.float64)
 
     def upload(self):
         self.ctx.check(lib().fnec_batch_upload(self._h), "batch_upload")
@@ -547,13 +551,16 @@ class HallenBatch:
             b += 48 * i.total_points
         return int(b)
 
-    def read(self) -> BatchResult:
+    def read(self, copy: bool = True) -> BatchResult:
+        """Results of the last run.  copy=False returns views of the batch's
+        page-locked result buffers: valid until the next read or close."""
         cur, feed, pat, st, tot = self.read_raw()
-        res = BatchResult([], [], [], st[: len(self.units)].copy(), tot[: len(self.units)].copy(), self.units)
+        cp = (lambda a: a.copy()) if copy else (lambda a: a)
+        res = BatchResult([], [], [], cp(st[: len(self.units)]), cp(tot[: len(self.units)]), self.units)
         for u in self.units:
-            res.currents.append(cur[u["cur_off"]: u["cur_off"] + u["n"]].copy())
-            res.feeds.append(feed[u["feed_off"]: u["feed_off"] + u["n_feed"]].copy())
-            res.pattern.append(pat[u["pat_off"]: u["pat_off"] + u["n_points"]].copy())
+            res.currents.append(cp(cur[u["cur_off"]: u["cur_off"] + u["n"]]))
+            res.feeds.append(cp(feed[u["feed_off"]: u["feed_off"] + u["n_feed"]]))
+            res.pattern.append(cp(pat[u["pat_off"]: u["pat_off"] + u["n_points"]]))
         return res
 
     PHASES = ("expand", "rhs", "fill", "gram", "factor", "solve", "feed", "farfield")
@@ -592,10 +599,23 @@ class HallenBatch:
         self.sync()
         return self.read()
 
+    def _pinned(self, shape, dtype):
+        nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        p = ctypes.c_void_p()
+        st = lib().fnec_host_alloc(nbytes, ctypes.byref(p))
+        if st != 0:
+            raise AccelError(st, "host_alloc")
+        self._host.append(p)
+        buf = (ctypes.c_char * nbytes).from_address(p.value)
+        return np.frombuffer(buf, dtype=dtype).reshape(shape)
+
     def close(self):
         if getattr(self, "_h", None):
             lib().fnec_batch_destroy(self._h)
             self._h = None
+        for p in getattr(self, "_host", []):
+            lib().fnec_host_free(p)
+        self._host = []
 
     def __del__(self):
         if _shutting_down:

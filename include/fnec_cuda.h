@@ -256,6 +256,12 @@ int fnec_dispatch_frequency_point(int request_kind, double freq_hz);
  * roofline denominators of the FP64-bound kernels. */
 int fnec_measure_fp64_peak(int device, double *fma_tflops, double *muladd_tflops);
 
+/* Page-locked host memory (no counterpart in the reference).  Result arrays
+ * passed to fnec_batch_read in such memory are written by direct device
+ * copies, without the staging copy pageable memory needs. */
+int fnec_host_alloc(uint64_t bytes, void **out);
+int fnec_host_free(void *p);
+
 /* Self-test of the 3xTF32 tensor-core GEMM that forms the mixed form's
  * Gram matrix (no counterpart in the reference): C = A B^T with A (m x k),
  * B (n x k) and C (m x n) row-major FP32 host arrays.  m, n, k <= 65536. */
