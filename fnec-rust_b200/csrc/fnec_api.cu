@@ -375,6 +375,12 @@ struct fnec_batch {
     int64_t *d_cur_off = nullptr;  // per solve: its first entry in d_cur
     MixedWork mixed;
     GridPlan grid;
+    // execution: the stream every operation of the batch is enqueued on;
+    // pooled batches take device memory from the stream-ordered pool and
+    // borrow their pinned host arenas (the server's lanes)
+    cudaStream_t st = nullptr;
+    bool pooled = false;
+    bool allow_grid = true;
     std::vector<int32_t> grid_order;
     size_t dev_bytes = 0;
     std::vector<void *> allocs;
@@ -395,7 +401,8 @@ template <typename T>
 static cudaError_t dalloc(fnec_batch *b, T **p, size_t count) {
     *p = nullptr;
     if (count == 0) count = 1;
-    cudaError_t e = cudaMalloc((void **)p, sizeof(T) * count);
+    cudaError_t e = b->pooled ? cudaMallocAsync((void **)p, sizeof(T) * count, b->st)
+                              : cudaMalloc((void **)p, sizeof(T) * count);
     if (e == cudaSuccess) {
         b->allocs.push_back(*p);
         b->dev_bytes += sizeof(T) * count;
@@ -407,19 +414,24 @@ template <typename T>
 static cudaError_t up(fnec_batch *b, T *d, const std::vector<T> &h) {
     if (h.empty()) return cudaSuccess;
     b->h2d += sizeof(T) * h.size();
-    return cudaMemcpyAsync(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, b->ctx->stream);
+    return cudaMemcpyAsync(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, b->st);
 }
 
 static void free_batch(fnec_batch *b) {
-    for (void *p : b->allocs) cudaFree(p);
+    for (void *p : b->allocs) {
+        if (b->pooled) cudaFreeAsync(p, b->st);
+        else cudaFree(p);
+    }
     b->allocs.clear();
-    if (b->h_in) cudaFreeHost(b->h_in);
-    if (b->h_out) cudaFreeHost(b->h_out);
+    if (!b->pooled) {  // pooled batches borrow their lane's pinned arenas
+        if (b->h_in) cudaFreeHost(b->h_in);
+        if (b->h_out) cudaFreeHost(b->h_out);
+    }
     b->h_in = b->h_out = nullptr;
     if (b->ev_made)
         for (auto &e : b->ev) cudaEventDestroy(e);
     b->ev_made = false;
-    free_mixed(b->mixed);
+    free_mixed(b->mixed, DevAlloc{b->st, b->pooled});
 }
 
 // Carve the packed input arena: every host table gets a 256-byte aligned
@@ -482,10 +494,42 @@ static void ff_cover_maps(const DevRp &rp, const double *pts, int ground, std::v
     }
 }
 
+// Where a batch runs: the context's stream with its own allocations (the
+// default), or a server lane's stream with pooled device memory and the
+// lane's pinned arenas.
+struct PinnedArena {
+    unsigned char *p = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t need) {
+        if (need <= cap) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+        size_t grow = need + need / 2;  // geometric growth: few reallocations
+        cudaError_t e = cudaMallocHost((void **)&p, grow);
+        if (e == cudaSuccess) cap = grow;
+        return e;
+    }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        cap = 0;
+    }
+};
+struct BatchPlace {
+    cudaStream_t st = nullptr;  // null: the context's stream
+    bool pooled = false;
+    bool allow_grid = true;
+    PinnedArena *in = nullptr, *out = nullptr;  // pooled only
+};
+
 static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, fnec_batch **out,
-                       bool need_solve = true) {
+                       bool need_solve = true, const BatchPlace &place = BatchPlace()) {
     fnec_batch *b = new fnec_batch();
     b->ctx = ctx;
+    b->st = place.st ? place.st : ctx->stream;
+    b->pooled = place.pooled;
+    b->allow_grid = place.allow_grid;
     b->precision = precision;
     b->from_wires = !hs.empty() && !hs[0].wires.empty();
     int64_t ff_req_max = 0, ff_int_max = 0;
@@ -734,7 +778,12 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
            o_ft = pk.add(b->fill_tiles), o_crows = pk.add(b->crows), o_gt = pk.add(b->gram_tiles), o_fro = pk.add(b->feed_row_off),
            o_rhs = pk.add(b->rhs_given), o_cos = pk.add(b->cos_given), o_z = pk.add(b->z_given);
     b->in_bytes = pk.total > 0 ? pk.total : 256;
-    e = cudaMallocHost((void **)&b->h_in, b->in_bytes);
+    if (b->pooled) {
+        e = place.in->ensure(b->in_bytes);
+        b->h_in = place.in->p;
+    } else {
+        e = cudaMallocHost((void **)&b->h_in, b->in_bytes);
+    }
     if (e == cudaSuccess) e = dalloc(b, &b->d_in, b->in_bytes);
     if (e == cudaSuccess) {
         for (size_t q = 0; q < pk.parts.size(); ++q)
@@ -797,7 +846,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
         cudaDeviceGetAttribute(&b->grid.sms, cudaDevAttrMultiProcessorCount, ctx->device);
         if (e == cudaSuccess) e = dalloc(b, &b->grid.d_order, (size_t)nu);
         if (e == cudaSuccess) e = up(b, b->grid.d_order, ord);
-        if (b->max_s > 380) {  // some panel may outgrow one CTA's shared memory
+        if (b->max_s > 380 && b->allow_grid) {  // some panel may outgrow one CTA's shared memory
             unsigned char *xg = nullptr, *sy = nullptr;
             if (e == cudaSuccess) e = dalloc(b, &xg, grid_xchg_bytes());
             if (e == cudaSuccess) e = dalloc(b, &sy, grid_sync_bytes(b->grid.steps));
@@ -809,9 +858,17 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
     b->out_bytes = sizeof(cx) * (size_t)b->x_el + sizeof(double) * 7 * (size_t)b->feed_rows +
                    sizeof(double) * PAT_STRIDE * (size_t)b->pat_el +
                    (sizeof(int32_t) + sizeof(double)) * (size_t)(nu + b->solves.size()) + 64;
-    if (e == cudaSuccess) e = cudaMallocHost((void **)&b->h_out, b->out_bytes);
+    if (e == cudaSuccess) {
+        if (b->pooled) {
+            e = place.out->ensure(b->out_bytes);
+            b->h_out = place.out->p;
+        } else {
+            e = cudaMallocHost((void **)&b->h_out, b->out_bytes);
+        }
+    }
     if (e == cudaSuccess && precision == FNEC_PRECISION_MIXED) {
-        e = alloc_mixed(b->mixed, b->units, b->solves, b->ants, b->max_s);
+        e = alloc_mixed(b->mixed, b->units, b->solves, b->ants, b->max_s, DevAlloc{b->st, b->pooled},
+                        b->allow_grid);
         b->dev_bytes += b->mixed.bytes;
     }
     if (e != cudaSuccess) {
@@ -955,7 +1012,7 @@ int fnec_batch_create(fnec_ctx *ctx, const fnec_antenna *antennas, uint32_t n_an
 int fnec_batch_destroy(fnec_batch *b) {
     if (!b) return FNEC_ERR_BAD_ARG;
     cudaSetDevice(b->ctx->device);
-    cudaStreamSynchronize(b->ctx->stream);
+    cudaStreamSynchronize(b->st);
     free_batch(b);
     delete b;
     return FNEC_OK;
@@ -987,15 +1044,15 @@ int fnec_batch_upload(fnec_batch *b) {
     cudaSetDevice(ctx->device);
     // one pinned host -> device copy of every input table
     b->h2d = b->in_bytes;
-    CUDA_TRY(ctx, cudaMemcpyAsync(b->d_in, b->h_in, b->in_bytes, cudaMemcpyHostToDevice, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(b->d_in, b->h_in, b->in_bytes, cudaMemcpyHostToDevice, b->st));
     if (!b->z_given.empty())
         CUDA_TRY(ctx, cudaMemcpyAsync(b->d_z, b->d_z_given, sizeof(double) * b->z_given.size(),
-                                      cudaMemcpyDeviceToDevice, ctx->stream));
+                                      cudaMemcpyDeviceToDevice, b->st));
     if (b->rhs_given_flag) {
         CUDA_TRY(ctx, cudaMemcpyAsync(b->d_rhs, b->d_rhs_given, sizeof(double) * b->rhs_given.size(),
-                                      cudaMemcpyDeviceToDevice, ctx->stream));
+                                      cudaMemcpyDeviceToDevice, b->st));
         CUDA_TRY(ctx, cudaMemcpyAsync(b->d_cos, b->d_cos_given, sizeof(double) * b->cos_given.size(),
-                                      cudaMemcpyDeviceToDevice, ctx->stream));
+                                      cudaMemcpyDeviceToDevice, b->st));
     }
     return FNEC_OK;
 }
@@ -1004,7 +1061,7 @@ int fnec_batch_run(fnec_batch *b) {
     if (!b) return FNEC_ERR_BAD_ARG;
     fnec_ctx *ctx = b->ctx;
     cudaSetDevice(ctx->device);
-    cudaStream_t st = ctx->stream;
+    cudaStream_t st = b->st;
     int nu = (int)b->units.size();
     int ns = (int)b->solves.size();
     uint64_t L = 0;
@@ -1097,7 +1154,7 @@ int fnec_batch_phase_ms(fnec_batch *b, double *ms) {
 int fnec_batch_sync(fnec_batch *b) {
     if (!b) return FNEC_ERR_BAD_ARG;
     cudaSetDevice(b->ctx->device);
-    CUDA_TRY(b->ctx, cudaStreamSynchronize(b->ctx->stream));
+    CUDA_TRY(b->ctx, cudaStreamSynchronize(b->st));
     return FNEC_OK;
 }
 
@@ -1141,7 +1198,7 @@ int fnec_batch_read(fnec_batch *b, double *currents, double *feeds, double *patt
     if (!b) return FNEC_ERR_BAD_ARG;
     fnec_ctx *ctx = b->ctx;
     cudaSetDevice(ctx->device);
-    cudaStream_t st = ctx->stream;
+    cudaStream_t st = b->st;
     int nu = (int)b->units.size(), ns = (int)b->solves.size();
     // device -> pinned staging -> caller arrays
     unsigned char *hx = b->h_out;
@@ -1193,11 +1250,11 @@ int fnec_batch_read_unit(fnec_batch *b, uint32_t unit, double *x, int32_t *pivot
     const UnitDesc &u = b->solves[unit];
     if (x)
         CUDA_TRY(ctx, cudaMemcpyAsync(x, b->d_x + u.x_off, sizeof(cx) * u.s, cudaMemcpyDeviceToHost,
-                                      ctx->stream));
+                                      b->st));
     if (pivots)
         CUDA_TRY(ctx, cudaMemcpyAsync(pivots, b->d_piv + u.piv_off, sizeof(int32_t) * u.s,
-                                      cudaMemcpyDeviceToHost, ctx->stream));
-    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+                                      cudaMemcpyDeviceToHost, b->st));
+    CUDA_TRY(ctx, cudaStreamSynchronize(b->st));
     return FNEC_OK;
 }
 
@@ -1205,7 +1262,7 @@ int fnec_batch_read_refinement(fnec_batch *b, int32_t *iters, double *resid) {
     if (!b) return FNEC_ERR_BAD_ARG;
     if (b->precision != FNEC_PRECISION_MIXED) return fail(b->ctx, FNEC_ERR_BAD_ARG, "not a mixed-precision batch");
     cudaSetDevice(b->ctx->device);
-    CUDA_TRY(b->ctx, read_mixed_stats(b->mixed, iters, resid, b->ctx->stream));
+    CUDA_TRY(b->ctx, read_mixed_stats(b->mixed, iters, resid, b->st));
     return FNEC_OK;
 }
 
@@ -1215,8 +1272,8 @@ int fnec_batch_read_z(fnec_batch *b, uint32_t unit, double *z) {
     cudaSetDevice(ctx->device);
     const UnitDesc &u = b->units[b->solves[unit].sys];
     CUDA_TRY(ctx, cudaMemcpyAsync(z, b->d_z + u.z_off, sizeof(cx) * (size_t)u.n * u.n,
-                                  cudaMemcpyDeviceToHost, ctx->stream));
-    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+                                  cudaMemcpyDeviceToHost, b->st));
+    CUDA_TRY(ctx, cudaStreamSynchronize(b->st));
     return FNEC_OK;
 }
 
@@ -1515,3 +1572,430 @@ int fnec_dispatch_frequency_point(int request_kind, double freq_hz) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Serving: requests (one antenna deck each) batched continuously over lanes.
+//
+// A host thread owns the device side.  Each lane is a CUDA stream that runs
+// one batch at a time; whenever a lane is free and requests are queued, the
+// thread admits requests in arrival order while the device bytes of the
+// batches in flight stay within the HBM budget, plans them as one batch
+// (stream-ordered pool allocations, the lane's pinned arenas), and enqueues
+// upload + solve + result copies on the lane.  Requests that arrive while
+// other batches run are admitted as soon as a lane and memory are free, and
+// the lanes' kernels overlap on the device.  A request's systems keep Z and
+// the factor on the device for all of its right-hand sides (one per source
+// position) and its pattern.
+// ---------------------------------------------------------------------------
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct ServerReq {
+    uint64_t ticket = 0;
+    HostAnt host;
+    fnec_request_out out{};
+    int64_t bytes = 0;
+    uint32_t n_solves = 0, n = 0, n_points = 0;
+    Clock::time_point t_submit, t_done;
+    int32_t state = FNEC_REQ_QUEUED;
+};
+
+struct Lane {
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    fnec_batch *b = nullptr;
+    std::vector<ServerReq *> reqs;
+    int64_t bytes = 0;
+    PinnedArena in, out;
+};
+
+// Upper bound of the device bytes one request's batch needs (Z, the
+// factor, solution and work vectors, Gram operand stacks, pattern buffers).
+int64_t request_bytes(const HostAnt &h, int precision) {
+    const int64_t n = (int64_t)h.segs.size(), w = (int64_t)h.ep.size(), s = n + w;
+    const int64_t f = (int64_t)h.freqs.size(), r = (int64_t)std::max<size_t>(h.rhs_srcs.size(), 1);
+    const int64_t rows = n + 2 * w + (int64_t)h.ja.size();
+    const int64_t pts = h.rp.pts_off >= 0 ? (int64_t)h.pts.size() / 2 : (int64_t)h.rp.n_theta * h.rp.n_phi;
+    const int64_t n_int = h.rp.skip_integral ? 0 : (h.ground == 1 ? 91 : 181) * 360;
+    int64_t b = 0;
+    b += 16 * n * n * f;                                   // Z
+    b += 160 * n + 256 * w + 64 * rows + 4 * n_int;        // geometry, tables, coverage maps
+    b += (16 * s + 16 * n + 8 * n + 64) * f * r;           // x, rhs, cos, feeds
+    b += (48 + 32) * pts * f * r + 8 * 1024 * f * r;      // pattern, fields, partials
+    if (precision == FNEC_PRECISION_MIXED) {
+        int64_t kb = (n + 31) / 32, rp = ((2 * n + 127) / 128) * 128;
+        b += 8 * s * s * f;                                // FP32 factor
+        b += 2 * 128 * kb * rp * f + 64 * kb * kb * f;     // Gram operand stacks (hi, lo), tiles
+        b += 16 * (25 * s + 6 * s + 2 * rows) * f * r;     // GMRES basis and work vectors
+    } else {
+        b += 16 * s * (s + 1) * f + 4 * s * f;             // FP64 factor, pivots
+    }
+    if (s > 380) b += (int64_t)grid_xchg_bytes() + (int64_t)grid_sync_bytes((int)((s + 31) / 32));  // grid panels
+    if (precision == FNEC_PRECISION_MIXED && s >= 1536)   // grid-wide GMRES scratch
+        b += 16 * n * ((n + 255) / 256) + 64 * s + 16 * 2 * 296 * 25 + 4096;
+    return b + (1 << 20);
+}
+
+}  // namespace
+
+struct fnec_server {
+    fnec_ctx own;  // the loop's private context (its own error string)
+    fnec_server_config cfg{};
+    std::mutex mu;
+    std::condition_variable cv;       // wakes the loop
+    std::condition_variable done_cv;  // wakes waiters
+    std::deque<ServerReq *> queue;
+    std::unordered_map<uint64_t, ServerReq *> live;
+    std::vector<Lane> lanes;
+    int64_t in_flight = 0;
+    uint64_t next_ticket = 1;
+    bool stop = false;
+    std::thread loop;
+    // statistics since the last reset
+    std::vector<double> lat_ms;
+    uint64_t submitted = 0, completed = 0, failed = 0, solves = 0, batches = 0, launches = 0;
+    int64_t peak_bytes = 0;
+    uint64_t max_batch_seen = 0;
+};
+
+namespace {
+
+// Copies a finished lane's results into its requests' output arrays.
+void server_complete(fnec_server *S, Lane &L, bool ok) {
+    fnec_batch *b = L.b;
+    const unsigned char *hx = b->h_out;
+    const unsigned char *hf = hx + sizeof(cx) * (size_t)b->x_el;
+    const unsigned char *hp = hf + sizeof(double) * 7 * (size_t)b->feed_rows;
+    const int32_t *hst = (const int32_t *)(hp + sizeof(double) * PAT_STRIDE * (size_t)b->pat_el);
+    const cx *x = (const cx *)hx;
+    std::vector<uint32_t> k_of(L.reqs.size(), 0);    // next solve slot of each request
+    std::vector<size_t> row_of(L.reqs.size(), 0);    // next feed row of each request
+    for (size_t u = 0; u < b->solves.size(); ++u) {
+        const fnec_unit_info &ui = b->uinfo[u];
+        ServerReq *r = L.reqs[ui.antenna];
+        const uint32_t k = k_of[ui.antenna]++;
+        const size_t row0 = row_of[ui.antenna];
+        row_of[ui.antenna] += ui.n_feed;
+        const int32_t st = ok ? hst[b->solves[u].sys] : FNEC_ERR_CUDA;
+        if (r->out.status) r->out.status[k] = st;
+        if (!ok) continue;
+        if (r->out.currents)
+            std::memcpy(r->out.currents + 2 * (size_t)k * r->n, &x[b->solves[u].x_off], sizeof(cx) * ui.n);
+        if (r->out.feeds && ui.n_feed)
+            std::memcpy(r->out.feeds + 7 * row0, hf + sizeof(double) * 7 * ui.feed_off,
+                        sizeof(double) * 7 * ui.n_feed);
+        if (r->out.pattern && ui.n_points)
+            std::memcpy(r->out.pattern + (size_t)PAT_STRIDE * k * r->n_points,
+                        hp + sizeof(double) * PAT_STRIDE * ui.pat_off, sizeof(double) * PAT_STRIDE * ui.n_points);
+    }
+    const auto now = Clock::now();
+    for (ServerReq *r : L.reqs) {
+        r->t_done = now;
+        r->state = ok ? FNEC_REQ_DONE : FNEC_ERR_CUDA;
+        if (ok) {
+            S->lat_ms.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
+            ++S->completed;
+            S->solves += r->n_solves;
+        } else {
+            ++S->failed;
+        }
+    }
+    S->launches += b->launches;
+    free_batch(b);  // pooled: the frees are ordered on the lane's stream
+    delete b;
+    L.b = nullptr;
+    L.reqs.clear();
+    S->in_flight -= L.bytes;
+    L.bytes = 0;
+}
+
+// Enqueue the device -> pinned copies of every result of a lane's batch.
+cudaError_t enqueue_results(fnec_batch *b) {
+    unsigned char *hx = b->h_out;
+    unsigned char *hf = hx + sizeof(cx) * (size_t)b->x_el;
+    unsigned char *hp = hf + sizeof(double) * 7 * (size_t)b->feed_rows;
+    unsigned char *hs = hp + sizeof(double) * PAT_STRIDE * (size_t)b->pat_el;
+    size_t fb = sizeof(double) * 7 * (size_t)b->feed_rows, pb = sizeof(double) * PAT_STRIDE * (size_t)b->pat_el;
+    cudaError_t e = cudaMemcpyAsync(hx, b->d_x, sizeof(cx) * b->x_el, cudaMemcpyDeviceToHost, b->st);
+    if (e == cudaSuccess && fb) e = cudaMemcpyAsync(hf, b->d_feed_out, fb, cudaMemcpyDeviceToHost, b->st);
+    if (e == cudaSuccess && pb) e = cudaMemcpyAsync(hp, b->d_pat, pb, cudaMemcpyDeviceToHost, b->st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(hs, b->d_status, sizeof(int32_t) * b->units.size(), cudaMemcpyDeviceToHost, b->st);
+    return e;
+}
+
+void server_loop(fnec_server *S) {
+    cudaSetDevice(S->own.device);
+    std::unique_lock<std::mutex> lk(S->mu);
+    for (;;) {
+        bool progress = false;
+        for (Lane &L : S->lanes) {  // completions
+            if (!L.b) continue;
+            cudaError_t q = cudaEventQuery(L.done);
+            if (q == cudaErrorNotReady) continue;
+            server_complete(S, L, q == cudaSuccess);
+            progress = true;
+        }
+        if (progress) S->done_cv.notify_all();
+        bool busy = false;
+        for (Lane &L : S->lanes) busy = busy || L.b;
+        if (S->stop && S->queue.empty() && !busy) break;
+        // admissions: a free lane takes queued requests in arrival order
+        for (Lane &L : S->lanes) {
+            if (L.b || S->queue.empty()) continue;
+            std::vector<ServerReq *> take;
+            int64_t bytes = 0;
+            while (!S->queue.empty() && take.size() < S->cfg.max_batch) {
+                ServerReq *r = S->queue.front();
+                if (S->in_flight + bytes + r->bytes > (int64_t)S->cfg.hbm_budget_bytes) break;
+                bytes += r->bytes;
+                take.push_back(r);
+                S->queue.pop_front();
+            }
+            if (take.empty()) break;  // the head waits for memory: arrival order is kept
+            for (ServerReq *r : take) r->state = FNEC_REQ_RUNNING;
+            S->in_flight += bytes;
+            L.bytes = bytes;
+            lk.unlock();
+            std::vector<HostAnt> hs;
+            hs.reserve(take.size());
+            for (ServerReq *r : take) hs.push_back(r->host);
+            BatchPlace place;
+            place.st = L.st;
+            place.pooled = true;
+            place.allow_grid = S->lanes.size() == 1;  // cooperative kernels need the whole device
+            place.in = &L.in;
+            place.out = &L.out;
+            fnec_batch *b = nullptr;
+            int st = build_batch(&S->own, hs, S->cfg.precision, &b, true, place);
+            cudaError_t e = cudaSuccess;
+            if (st == FNEC_OK) st = fnec_batch_run(b);
+            if (st == FNEC_OK) e = enqueue_results(b);
+            if (st == FNEC_OK && e == cudaSuccess) e = cudaEventRecord(L.done, L.st);
+            lk.lock();
+            if (st == FNEC_OK && e == cudaSuccess) {
+                L.b = b;
+                L.reqs = take;
+                ++S->batches;
+                S->max_batch_seen = std::max<uint64_t>(S->max_batch_seen, take.size());
+                S->peak_bytes = std::max(S->peak_bytes, S->in_flight);
+            } else {
+                if (b) {
+                    cudaStreamSynchronize(L.st);
+                    free_batch(b);
+                    delete b;
+                }
+                S->in_flight -= L.bytes;
+                L.bytes = 0;
+                const auto now = Clock::now();
+                for (ServerReq *r : take) {
+                    r->state = st != FNEC_OK ? st : FNEC_ERR_CUDA;
+                    r->t_done = now;
+                    if (r->out.status)
+                        for (uint32_t k = 0; k < r->n_solves; ++k) r->out.status[k] = r->state;
+                    ++S->failed;
+                }
+                S->done_cv.notify_all();
+            }
+            progress = true;
+        }
+        if (!progress) {
+            busy = false;
+            for (Lane &L : S->lanes) busy = busy || L.b;
+            // poll the lanes every 20 us while work is in flight, else sleep until woken
+            if (busy) S->cv.wait_for(lk, std::chrono::microseconds(20));
+            else S->cv.wait_for(lk, std::chrono::milliseconds(50));
+        }
+    }
+}
+
+}  // namespace
+
+int fnec_server_create(fnec_ctx *ctx, const fnec_server_config *cfg, fnec_server **out) {
+    if (!ctx || !cfg || !out) return FNEC_ERR_BAD_ARG;
+    *out = nullptr;
+    if (cfg->precision != FNEC_PRECISION_FP64 && cfg->precision != FNEC_PRECISION_MIXED)
+        return fail(ctx, FNEC_ERR_BAD_ARG, "precision must be FP64 or MIXED");
+    if (cfg->lanes < 1 || cfg->lanes > 16 || cfg->max_batch < 1 || cfg->hbm_budget_bytes == 0)
+        return fail(ctx, FNEC_ERR_BAD_ARG, "lanes 1..16, max_batch >= 1 and a nonzero HBM budget");
+    cudaSetDevice(ctx->device);
+    fnec_server *S = new fnec_server();
+    S->own.device = ctx->device;
+    S->own.stream = ctx->stream;
+    S->cfg = *cfg;
+    if (S->cfg.queue_cap == 0) S->cfg.queue_cap = 1u << 20;
+    S->lanes.resize(cfg->lanes);
+    for (Lane &L : S->lanes) {
+        if (cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming) != cudaSuccess) {
+            for (Lane &M : S->lanes) {
+                if (M.done) cudaEventDestroy(M.done);
+                if (M.st) cudaStreamDestroy(M.st);
+            }
+            delete S;
+            return fail(ctx, FNEC_ERR_CUDA, "lane stream creation failed");
+        }
+    }
+    // keep pool memory freed by finished batches cached for the next ones
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    S->loop = std::thread(server_loop, S);
+    *out = S;
+    return FNEC_OK;
+}
+
+int fnec_server_destroy(fnec_server *S) {
+    if (!S) return FNEC_ERR_BAD_ARG;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+    }
+    S->cv.notify_all();
+    if (S->loop.joinable()) S->loop.join();
+    cudaSetDevice(S->own.device);
+    for (Lane &L : S->lanes) {
+        cudaStreamSynchronize(L.st);
+        L.in.release();
+        L.out.release();
+        cudaEventDestroy(L.done);
+        cudaStreamDestroy(L.st);
+    }
+    for (auto &kv : S->live) delete kv.second;
+    delete S;
+    return FNEC_OK;
+}
+
+int fnec_request_shape(fnec_ctx *ctx, const fnec_antenna *req, int32_t precision, fnec_request_info *out) {
+    if (!ctx || !req || !out) return FNEC_ERR_BAD_ARG;
+    HostAnt h;
+    std::string why;
+    int st = antenna_from_cards(*req, h, why);
+    if (st != FNEC_OK) return fail(ctx, st, why);
+    out->n_segments = (uint32_t)h.segs.size();
+    out->n_rhs = (uint32_t)std::max<size_t>(h.rhs_srcs.size(), 1);
+    out->n_solves = out->n_rhs * (uint32_t)h.freqs.size();
+    uint32_t fr = 0;
+    for (auto &v : h.rhs_feeds) fr += (uint32_t)v.size();
+    out->n_feed_rows = fr * (uint32_t)h.freqs.size();
+    out->n_points = h.rp.pts_off >= 0 ? (uint32_t)(h.pts.size() / 2) : (uint32_t)(h.rp.n_theta * h.rp.n_phi);
+    out->pad = 0;
+    out->device_bytes = (uint64_t)request_bytes(h, precision);
+    return FNEC_OK;
+}
+
+int fnec_server_submit(fnec_server *S, const fnec_antenna *req, const fnec_request_out *out, uint64_t *ticket) {
+    if (!S || !req || !out || !ticket) return FNEC_ERR_BAD_ARG;
+    ServerReq *r = new ServerReq();
+    std::string why;
+    int st = antenna_from_cards(*req, r->host, why);
+    if (st != FNEC_OK) {
+        delete r;
+        return st;
+    }
+    r->out = *out;
+    r->n = (uint32_t)r->host.segs.size();
+    r->n_solves = (uint32_t)(std::max<size_t>(r->host.rhs_srcs.size(), 1) * r->host.freqs.size());
+    r->n_points = r->host.rp.pts_off >= 0 ? (uint32_t)(r->host.pts.size() / 2)
+                                          : (uint32_t)(r->host.rp.n_theta * r->host.rp.n_phi);
+    r->bytes = request_bytes(r->host, S->cfg.precision);
+    if (r->bytes > (int64_t)S->cfg.hbm_budget_bytes) {
+        delete r;
+        return FNEC_ERR_TOO_LARGE;
+    }
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (S->queue.size() >= S->cfg.queue_cap) {
+            delete r;
+            return FNEC_ERR_BUSY;
+        }
+        r->ticket = S->next_ticket++;
+        r->t_submit = Clock::now();
+        S->queue.push_back(r);
+        S->live[r->ticket] = r;
+        ++S->submitted;
+        *ticket = r->ticket;
+    }
+    S->cv.notify_all();
+    return FNEC_OK;
+}
+
+int fnec_server_poll(fnec_server *S, uint64_t ticket, int32_t *state, double *latency_ms) {
+    if (!S || !state) return FNEC_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->live.find(ticket);
+    if (it == S->live.end()) return FNEC_ERR_BAD_ARG;
+    ServerReq *r = it->second;
+    *state = r->state;
+    if (r->state == FNEC_REQ_DONE || r->state < 0) {
+        if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+        S->live.erase(it);
+        delete r;
+    }
+    return FNEC_OK;
+}
+
+int fnec_server_wait(fnec_server *S, uint64_t ticket, double timeout_ms, int32_t *state, double *latency_ms) {
+    if (!S || !state) return FNEC_ERR_BAD_ARG;
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->live.find(ticket);
+    if (it == S->live.end()) return FNEC_ERR_BAD_ARG;
+    ServerReq *r = it->second;
+    const auto until = Clock::now() + std::chrono::microseconds((int64_t)(timeout_ms * 1000.0));
+    while (!(r->state == FNEC_REQ_DONE || r->state < 0)) {
+        if (S->done_cv.wait_until(lk, until) == std::cv_status::timeout &&
+            !(r->state == FNEC_REQ_DONE || r->state < 0)) {
+            *state = r->state;
+            return FNEC_ERR_TIMEOUT;
+        }
+    }
+    *state = r->state;
+    if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+    S->live.erase(it);
+    delete r;
+    return FNEC_OK;
+}
+
+int fnec_server_stats(fnec_server *S, fnec_server_stats_t *out, int32_t reset) {
+    if (!S || !out) return FNEC_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lk(S->mu);
+    std::vector<double> v = S->lat_ms;
+    std::sort(v.begin(), v.end());
+    auto pct = [&](double q) {
+        if (v.empty()) return 0.0;
+        double i = std::ceil(q * (double)v.size()) - 1.0;
+        return v[(size_t)std::min<double>((double)v.size() - 1, std::max(0.0, i))];
+    };
+    out->submitted = S->submitted;
+    out->completed = S->completed;
+    out->failed = S->failed;
+    out->solves = S->solves;
+    out->batches = S->batches;
+    out->queued = S->queue.size();
+    out->in_flight_bytes = (uint64_t)std::max<int64_t>(S->in_flight, 0);
+    out->peak_in_flight_bytes = (uint64_t)S->peak_bytes;
+    out->max_batch = S->max_batch_seen;
+    out->kernel_launches = S->launches;
+    out->p50_ms = pct(0.50);
+    out->p99_ms = pct(0.99);
+    out->max_ms = v.empty() ? 0.0 : v.back();
+    double sum = 0;
+    for (double x : v) sum += x;
+    out->mean_ms = v.empty() ? 0.0 : sum / (double)v.size();
+    if (reset) {
+        S->lat_ms.clear();
+        S->submitted = S->completed = S->failed = S->solves = S->batches = S->launches = 0;
+        S->peak_bytes = S->in_flight;
+        S->max_batch_seen = 0;
+    }
+    return FNEC_OK;
+}

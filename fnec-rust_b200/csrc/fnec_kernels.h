@@ -11,6 +11,21 @@ namespace fnec {
 
 constexpr int PAT_STRIDE = 6;  // gain_total, gain_theta, gain_phi, axial_ratio, u_theta, u_phi
 
+// Device allocations of a batch: plain cudaMalloc, or the stream-ordered
+// pool (cudaMallocAsync on the batch's stream) for server lanes.
+struct DevAlloc {
+    cudaStream_t st;
+    bool pooled;
+    cudaError_t alloc(void **p, size_t bytes) const {
+        return pooled ? cudaMallocAsync(p, bytes, st) : cudaMalloc(p, bytes);
+    }
+    void release(void *p) const {
+        if (!p) return;
+        if (pooled) cudaFreeAsync(p, st);
+        else cudaFree(p);
+    }
+};
+
 // Units whose panels are too tall for one CTA's shared memory are factored
 // by the grid-wide panel kernel (fnec_grid.cuh).  Built once per batch.
 struct GridPlan {

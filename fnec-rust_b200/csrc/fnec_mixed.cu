@@ -1413,7 +1413,7 @@ __global__ void k_perm_from_piv(const UnitDesc *__restrict__ units, int ui, cons
 bool mixed_available() { return true; }
 
 cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, const std::vector<UnitDesc> &solves,
-                        const std::vector<AntDesc> &ants, int max_s) {
+                        const std::vector<AntDesc> &ants, int max_s, const DevAlloc &dev, bool allow_grid) {
     std::vector<int64_t> a32_of(systems.size());
     int64_t a32 = 0, v = 0, wk = 0;
     for (size_t i = 0; i < systems.size(); ++i) {
@@ -1443,7 +1443,7 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
     size_t b_w = sizeof(cx) * (size_t)(wk + 1);
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
     size_t total = al(b_mu) + al(b_smu) + al(b_a32) + al(b_v) + al(b_w);
-    cudaError_t e = cudaMalloc(&w.base, total);
+    cudaError_t e = dev.alloc(&w.base, total);
     if (e != cudaSuccess) return e;
     unsigned char *p = (unsigned char *)w.base;
     w.mu = (MixedUnit *)p;
@@ -1466,7 +1466,7 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
             w.grid_solves.push_back((int)i);
             w.grid_s.push_back(solves[i].s);
         }
-    if (w.grid_solves.size() > (size_t)GG_MAX_SOLVES) {
+    if (w.grid_solves.size() > (size_t)GG_MAX_SOLVES || !allow_grid) {
         w.grid_solves.clear();
         w.grid_s.clear();
     }
@@ -1481,7 +1481,7 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
                b_y = sizeof(cx) * (size_t)smax, b_red = sizeof(cx) * 2 * GG_MAX_CTAS * (GM + 1),
                b_sync = sizeof(GridSync) * w.grid_solves.size();
         size_t gt = al(b_perm) + al(b_part) + al(b_y) + al(b_red) + al(b_sync);
-        e = cudaMalloc(&w.grid_base, gt);
+        e = dev.alloc(&w.grid_base, gt);
         if (e != cudaSuccess) return e;
         unsigned char *q = (unsigned char *)w.grid_base;
         w.g_perm = (int32_t *)q;
@@ -1508,7 +1508,7 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
             size_t b_st = sizeof(float) * 32 * (size_t)p->rows;
             size_t b_gu = sizeof(TcGramUnit) * p->units.size(), b_t = sizeof(TcTile) * p->tiles.size();
             size_t tot = 2 * al(b_st) + al(b_gu) + al(b_t);
-            e = cudaMalloc(&w.tc_base, tot);
+            e = dev.alloc(&w.tc_base, tot);
             if (e != cudaSuccess) {
                 delete p;
                 return e;
@@ -1522,8 +1522,8 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
             q += al(b_gu);
             w.tc_tiles = q;
             w.bytes += tot;
-            e = cudaMemcpy(w.tc_gu, p->units.data(), b_gu, cudaMemcpyHostToDevice);
-            if (e == cudaSuccess) e = cudaMemcpy(w.tc_tiles, p->tiles.data(), b_t, cudaMemcpyHostToDevice);
+            e = cudaMemcpyAsync(w.tc_gu, p->units.data(), b_gu, cudaMemcpyHostToDevice, dev.st);
+            if (e == cudaSuccess) e = cudaMemcpyAsync(w.tc_tiles, p->tiles.data(), b_t, cudaMemcpyHostToDevice, dev.st);
             if (e != cudaSuccess) {
                 delete p;
                 return e;
@@ -1538,16 +1538,17 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
             delete p;
         }
     }
-    e = cudaMemcpy(w.mu, mu.data(), sizeof(MixedUnit) * mu.size(), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(w.smu, sysmu.data(), sizeof(MixedUnit) * sysmu.size(), cudaMemcpyHostToDevice);
+    e = cudaMemcpyAsync(w.mu, mu.data(), sizeof(MixedUnit) * mu.size(), cudaMemcpyHostToDevice, dev.st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(w.smu, sysmu.data(), sizeof(MixedUnit) * sysmu.size(), cudaMemcpyHostToDevice, dev.st);
     return e;
 }
 
-void free_mixed(MixedWork &w) {
-    if (w.base) cudaFree(w.base);
-    if (w.grid_base) cudaFree(w.grid_base);
+void free_mixed(MixedWork &w, const DevAlloc &dev) {
+    dev.release(w.base);
+    dev.release(w.grid_base);
+    dev.release(w.tc_base);
     w.grid_base = nullptr;
-    if (w.tc_base) cudaFree(w.tc_base);
     w.tc_base = nullptr;
     delete w.tc;
     w.tc = nullptr;

@@ -58,9 +58,10 @@ struct MixedMarks {
 
 bool mixed_available();
 // systems: one per factorisation; solves: one per right-hand side.
+// allow_grid: large solves may take the grid-wide (cooperative) GMRES
 cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, const std::vector<UnitDesc> &solves,
-                        const std::vector<AntDesc> &ants, int max_s);
-void free_mixed(MixedWork &w);
+                        const std::vector<AntDesc> &ants, int max_s, const DevAlloc &dev, bool allow_grid);
+void free_mixed(MixedWork &w, const DevAlloc &dev);
 // Enqueue fill + Gram + factor + refinement for all units; returns the
 // number of kernel launches issued.
 uint64_t run_mixed(MixedWork &w, const UnitDesc *d_units, int nu, const UnitDesc *d_solves, int ns,

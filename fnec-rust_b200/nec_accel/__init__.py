@@ -97,6 +97,26 @@ class _BatchInfo(ctypes.Structure):
                 ("kernel_launches", _U64), ("n_systems", _U32)]
 
 
+class _ServerConfig(ctypes.Structure):
+    _fields_ = [("precision", _I32), ("lanes", _I32), ("hbm_budget_bytes", _U64), ("max_batch", _U32),
+                ("queue_cap", _U32)]
+
+
+class _RequestOut(ctypes.Structure):
+    _fields_ = [("currents", _P), ("feeds", _P), ("pattern", _P), ("status", _P)]
+
+
+class _RequestInfo(ctypes.Structure):
+    _fields_ = [("n_segments", _U32), ("n_rhs", _U32), ("n_solves", _U32), ("n_feed_rows", _U32),
+                ("n_points", _U32), ("pad", _U32), ("device_bytes", _U64)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [("submitted", _U64), ("completed", _U64), ("failed", _U64), ("solves", _U64), ("batches", _U64),
+                ("queued", _U64), ("in_flight_bytes", _U64), ("peak_in_flight_bytes", _U64), ("max_batch", _U64),
+                ("kernel_launches", _U64), ("p50_ms", _D), ("p99_ms", _D), ("mean_ms", _D), ("max_ms", _D)]
+
+
 # name -> (restype, argtypes); every function declared in include/fnec_cuda.h
 SIGNATURES = {
     "fnec_ctx_create": (ctypes.c_int, [ctypes.c_int, _P]),
@@ -115,6 +135,13 @@ SIGNATURES = {
     "fnec_dispatch_frequency_point": (ctypes.c_int, [ctypes.c_int, _D]),
     "fnec_measure_fp64_peak": (ctypes.c_int, [ctypes.c_int, _P, _P]),
     "fnec_host_alloc": (ctypes.c_int, [ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
+    "fnec_server_create": (ctypes.c_int, [_P, _P, _P]),
+    "fnec_server_destroy": (ctypes.c_int, [_P]),
+    "fnec_request_shape": (ctypes.c_int, [_P, _P, _I32, _P]),
+    "fnec_server_submit": (ctypes.c_int, [_P, _P, _P, _P]),
+    "fnec_server_poll": (ctypes.c_int, [_P, _U64, _P, _P]),
+    "fnec_server_wait": (ctypes.c_int, [_P, _U64, _D, _P, _P]),
+    "fnec_server_stats": (ctypes.c_int, [_P, _P, _I32]),
     "fnec_host_free": (ctypes.c_int, [_P]),
     "fnec_selftest_tf32x3_gemm": (ctypes.c_int, [ctypes.c_int32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
                                                  _P, _P, _P]),
@@ -139,6 +166,7 @@ _lib = None
 # the contexts they were created on): module teardown order is otherwise
 # arbitrary and a batch must never outlive its context.
 _live_batches = weakref.WeakSet()
+_live_servers = weakref.WeakSet()
 _live_contexts = weakref.WeakSet()
 _shutting_down = False
 
@@ -146,6 +174,8 @@ _shutting_down = False
 @atexit.register
 def _release_all():
     global _shutting_down
+    for v in list(_live_servers):
+        v.close()
     for b in list(_live_batches):
         b.close()
     for c in list(_live_contexts):
@@ -197,6 +227,9 @@ class Context:
 
     def close(self):
         if getattr(self, "_h", None):
+            for v in list(_live_servers):
+                if v.ctx is self:
+                    v.close()
             for b in list(_live_batches):
                 if b.ctx is self:
                     b.close()
@@ -470,6 +503,20 @@ class BatchResult:
     units: list = field(default_factory=list)
 
 
+def _antenna_struct(a, keep: list):
+    """The C fnec_antenna of an Antenna; the arrays it points to go to keep."""
+    w = np.ascontiguousarray(a.wires, dtype=WIRE_DTYPE)
+    s = np.ascontiguousarray(a.sources, dtype=SOURCE_DTYPE)
+    f = np.ascontiguousarray(np.asarray(a.freqs_hz, np.float64))
+    rp = None
+    if a.rp is not None:
+        rp = _RpCard(*[int(a.rp[0]), int(a.rp[1])] + [float(v) for v in a.rp[2:6]])
+    keep += [w, s, f, rp]
+    return _Antenna(_ptr(w), len(w), _ptr(s), len(s), int(a.ground), len(f), _ptr(f),
+                    ctypes.cast(ctypes.pointer(rp), _P) if rp is not None else None,
+                    int(bool(a.separate_sources)))
+
+
 class HallenBatch:
     """A planned, device-resident batch of per-frequency Hallen solves."""
 
@@ -479,16 +526,7 @@ class HallenBatch:
         self._keep = []
         arr = (_Antenna * len(antennas))()
         for i, a in enumerate(antennas):
-            w = np.ascontiguousarray(a.wires, dtype=WIRE_DTYPE)
-            s = np.ascontiguousarray(a.sources, dtype=SOURCE_DTYPE)
-            f = np.ascontiguousarray(np.asarray(a.freqs_hz, np.float64))
-            rp = None
-            if a.rp is not None:
-                rp = _RpCard(*[int(a.rp[0]), int(a.rp[1])] + [float(v) for v in a.rp[2:6]])
-            self._keep += [w, s, f, rp]
-            arr[i] = _Antenna(_ptr(w), len(w), _ptr(s), len(s), int(a.ground), len(f), _ptr(f),
-                              ctypes.cast(ctypes.pointer(rp), _P) if rp is not None else None,
-                              int(bool(a.separate_sources)))
+            arr[i] = _antenna_struct(a, self._keep)
         self._keep.append(arr)
         h = ctypes.c_void_p()
         self.ctx.check(lib().fnec_batch_create(self.ctx.handle, arr, len(antennas), int(precision),
@@ -616,6 +654,125 @@ class HallenBatch:
         for p in getattr(self, "_host", []):
             lib().fnec_host_free(p)
         self._host = []
+
+    def __del__(self):
+        if _shutting_down:
+            return
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE = 0, 1, 2
+
+
+class Request:
+    """One submitted request: its output arrays and, once done, its latency."""
+
+    def __init__(self, antenna, info, currents, feeds, pattern):
+        self.antenna = antenna
+        self.info = info
+        self.n_solves = info.n_solves
+        self.currents = np.zeros((info.n_solves, info.n_segments), np.complex128) if currents else None
+        self.feeds = np.zeros((max(info.n_feed_rows, 1), 7), np.float64) if feeds else None
+        self.pattern = (np.zeros((info.n_solves, info.n_points, 6), np.float64)
+                        if (pattern and info.n_points) else None)
+        self.status = np.zeros(info.n_solves, np.int32)
+        self.ticket = None
+        self.latency_ms = None
+        self.state = REQ_QUEUED
+        self._keep = []
+
+    def feed_z(self, solve: int = 0) -> complex:
+        """Feedpoint impedance of a solve's first feed row (columns 5, 6)."""
+        rows_per = len(self.feeds) // max(self.n_solves, 1)
+        r = self.feeds[solve * rows_per]
+        return complex(r[5], r[6])
+
+
+class Server:
+    """Continuous-batching solve server (fnec_server_*): submit decks as they
+    arrive; a host thread admits them by HBM budget onto `lanes` concurrent
+    streams and delivers each request's results into its arrays."""
+
+    def __init__(self, precision: int = PRECISION_MIXED, lanes: int = 2, hbm_budget_bytes: int = 32 << 30,
+                 max_batch: int = 64, queue_cap: int = 0, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        self.precision = int(precision)
+        cfg = _ServerConfig(self.precision, int(lanes), int(hbm_budget_bytes), int(max_batch), int(queue_cap))
+        h = ctypes.c_void_p()
+        self.ctx.check(lib().fnec_server_create(self.ctx.handle, ctypes.byref(cfg), ctypes.byref(h)),
+                       "server_create")
+        self._h = h
+        self._pending = {}
+        _live_servers.add(self)
+
+    def shape(self, antenna):
+        keep = []
+        a = _antenna_struct(antenna, keep)
+        info = _RequestInfo()
+        self.ctx.check(lib().fnec_request_shape(self.ctx.handle, ctypes.byref(a), self.precision,
+                                                ctypes.byref(info)), "request_shape")
+        return info
+
+    def submit(self, antenna, currents: bool = True, feeds: bool = True, pattern: bool = True) -> Request:
+        keep = []
+        a = _antenna_struct(antenna, keep)
+        req = Request(antenna, self.shape(antenna), currents, feeds, pattern)
+        req._keep = keep
+        out = _RequestOut(_ptr(req.currents), _ptr(req.feeds), _ptr(req.pattern), _ptr(req.status))
+        t = ctypes.c_uint64()
+        st = lib().fnec_server_submit(self._h, ctypes.byref(a), ctypes.byref(out), ctypes.byref(t))
+        if st != 0:
+            raise AccelError(st, "server_submit")
+        req.ticket = t.value
+        self._pending[req.ticket] = req  # keeps the output arrays alive until done
+        return req
+
+    def _finish(self, req, state, lat):
+        req.state = state
+        if state == REQ_DONE or state < 0:
+            req.latency_ms = lat
+            self._pending.pop(req.ticket, None)
+        if state < 0:
+            raise AccelError(state, "request failed")
+
+    def poll(self, req: Request) -> bool:
+        if req.state == REQ_DONE:
+            return True
+        state, lat = ctypes.c_int32(), ctypes.c_double()
+        st = lib().fnec_server_poll(self._h, req.ticket, ctypes.byref(state), ctypes.byref(lat))
+        if st != 0:
+            raise AccelError(st, "server_poll")
+        self._finish(req, state.value, lat.value)
+        return req.state == REQ_DONE
+
+    def wait(self, req: Request, timeout_ms: float = 120000.0) -> Request:
+        if req.state == REQ_DONE:
+            return req
+        state, lat = ctypes.c_int32(), ctypes.c_double()
+        st = lib().fnec_server_wait(self._h, req.ticket, float(timeout_ms), ctypes.byref(state), ctypes.byref(lat))
+        if st != 0:
+            raise AccelError(st, "server_wait")
+        self._finish(req, state.value, lat.value)
+        return req
+
+    def stats(self, reset: bool = False) -> dict:
+        s = _ServerStats()
+        self.ctx.check(lib().fnec_server_stats(self._h, ctypes.byref(s), int(reset)), "server_stats")
+        return {k: getattr(s, k) for k, _ in _ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fnec_server_destroy(self._h)  # finishes queued and running requests
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
     def __del__(self):
         if _shutting_down:

@@ -256,6 +256,79 @@ int fnec_dispatch_frequency_point(int request_kind, double freq_hz);
  * roofline denominators of the FP64-bound kernels. */
 int fnec_measure_fp64_peak(int device, double *fma_tflops, double *muladd_tflops);
 
+/* ---- serving: continuous batching of solve requests -------------------
+ * No counterpart in the reference (its sweep loop calls the backend once
+ * per frequency).  A server owns `lanes` CUDA streams and a host thread:
+ * submitted requests (one fnec_antenna deck each; every voltage source a
+ * separate right-hand side when separate_sources is set) queue in arrival
+ * order; whenever a lane is free the thread admits queued requests while the
+ * device bytes of the batches in flight (each request's admission estimate,
+ * fnec_request_info.device_bytes) stay within hbm_budget_bytes, solves them
+ * as one batch -- Z and its factor stay on the device for all of a request's
+ * right-hand sides and its pattern -- and copies the results into the
+ * request's output arrays.  Requests arriving while batches run are admitted
+ * as lanes and memory free up; the lanes' kernels overlap on the device.
+ * With more than one lane the grid-wide (cooperative) kernels are not used. */
+typedef struct fnec_server fnec_server;
+
+typedef struct {
+    int32_t precision;         /* FNEC_PRECISION_FP64 or FNEC_PRECISION_MIXED */
+    int32_t lanes;             /* concurrent batches (streams), 1..16        */
+    uint64_t hbm_budget_bytes; /* device bytes the batches in flight may use */
+    uint32_t max_batch;        /* requests per batch                          */
+    uint32_t queue_cap;        /* queued requests before submit is BUSY (0: 2^20) */
+} fnec_server_config;
+
+/* Output arrays of one request, caller-owned, written before the request
+ * reports DONE (any may be NULL).  Solve k = frequency * n_rhs + rhs. */
+typedef struct {
+    double *currents; /* n_solves x n_segments complex (interleaved)         */
+    double *feeds;    /* n_feed_rows x 7 (as fnec_batch_read), solve order    */
+    double *pattern;  /* n_solves x n_points x 6 (as fnec_batch_read)         */
+    int32_t *status;  /* n_solves: 0, -(column+1) singular, or an error code  */
+} fnec_request_out;
+
+typedef struct {
+    uint32_t n_segments;
+    uint32_t n_rhs;
+    uint32_t n_solves;
+    uint32_t n_feed_rows;
+    uint32_t n_points;
+    uint32_t pad;
+    uint64_t device_bytes; /* admission estimate (upper bound) of the footprint */
+} fnec_request_info;
+
+typedef struct {
+    uint64_t submitted, completed, failed;
+    uint64_t solves;          /* right-hand sides of completed requests */
+    uint64_t batches;
+    uint64_t queued;
+    uint64_t in_flight_bytes, peak_in_flight_bytes;
+    uint64_t max_batch;       /* largest batch formed                      */
+    uint64_t kernel_launches; /* kernels launched for the completed batches */
+    double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> results delivered */
+} fnec_server_stats_t;
+
+#define FNEC_REQ_QUEUED 0
+#define FNEC_REQ_RUNNING 1
+#define FNEC_REQ_DONE 2
+
+int fnec_server_create(fnec_ctx *ctx, const fnec_server_config *cfg, fnec_server **out);
+/* Finishes every queued and running request, then releases the server. */
+int fnec_server_destroy(fnec_server *s);
+/* Output sizes and admission footprint of a request (host planning only). */
+int fnec_request_shape(fnec_ctx *ctx, const fnec_antenna *req, int32_t precision, fnec_request_info *out);
+/* Queue a request; BUSY when the queue is full, TOO_LARGE when it alone
+ * exceeds the budget.  The deck is copied; the output arrays must stay
+ * valid until the request is done. */
+int fnec_server_submit(fnec_server *s, const fnec_antenna *req, const fnec_request_out *out, uint64_t *ticket);
+/* state: FNEC_REQ_* or a negative error; a finished request (done or
+ * failed) is released by the call that reports it. */
+int fnec_server_poll(fnec_server *s, uint64_t ticket, int32_t *state, double *latency_ms);
+int fnec_server_wait(fnec_server *s, uint64_t ticket, double timeout_ms, int32_t *state, double *latency_ms);
+/* Latency percentiles over completed requests since the last reset. */
+int fnec_server_stats(fnec_server *s, fnec_server_stats_t *out, int32_t reset);
+
 /* Page-locked host memory (no counterpart in the reference).  Result arrays
  * passed to fnec_batch_read in such memory are written by direct device
  * copies, without the staging copy pageable memory needs. */
