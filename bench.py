@@ -112,6 +112,60 @@ def uneven_workload(n_ant: int = 4096, seed: int = 7):
     return out
 
 
+SERVE_RP = (91, 361, 0.0, 0.0, 1.0, 1.0)  # theta 0-90 x phi 0-360, 1 degree steps
+
+
+def serve_requests(n_req: int, seed: int = 13, n_cap: int = 4096, sigma: float = 0.75):
+    """Served request stream: each request is a random wire antenna like the
+    uneven batch's (1-8 straight wires, endpoints in a 20 m cube, radius
+    log-uniform 0.5-5 mm, one frequency log-uniform 3-30 MHz, free space or
+    GN 1 with probability 1/2) whose total segment count N is drawn
+    lognormal with median 150 (sigma 0.75, capped at n_cap) and split over
+    the wires in odd counts of at least 3.  It carries 1-4 source positions
+    (uniform): the centre segment of wire 1 and distinct random segments,
+    each a separate right-hand side; half of the requests ask for the
+    91 x 361 pattern.  The CLI guards of the uneven generator apply."""
+    rng = np.random.default_rng(seed)
+    out = []
+    while len(out) < n_req:
+        n_tot = int(min(n_cap, max(11, round(float(np.exp(rng.normal(np.log(150.0), sigma)))))))
+        nw = int(rng.integers(1, 9))
+        nw = max(1, min(nw, n_tot // 3))
+        share = rng.dirichlet(np.ones(nw))
+        counts = [max(3, int(round(n_tot * f))) for f in share]
+        counts = [c if c % 2 else c + 1 for c in counts]
+        wires = []
+        for t in range(nw):
+            p0 = rng.uniform([-10.0, -10.0, 0.0], [10.0, 10.0, 20.0])
+            p1 = rng.uniform([-10.0, -10.0, 0.0], [10.0, 10.0, 20.0])
+            rad = float(np.exp(rng.uniform(np.log(0.5e-3), np.log(5e-3))))
+            wires.append((t + 1, counts[t], tuple(p0), tuple(p1), rad))
+        ground = int(rng.integers(0, 2))
+        f = float(np.exp(rng.uniform(np.log(3e6), np.log(30e6))))
+        n_src = int(rng.integers(1, 5))
+        srcs = [(1, (wires[0][1] + 1) // 2)]
+        while len(srcs) < n_src:
+            t = int(rng.integers(0, nw))
+            cand = (t + 1, int(rng.integers(1, wires[t][1] + 1)))
+            if cand not in srcs:
+                srcs.append(cand)
+        ok = all(min(w[2][2], w[3][2]) > 1e-9 for w in wires)
+        for tag, seg in srcs:
+            w = wires[tag - 1]
+            ok = ok and np.linalg.norm(np.subtract(w[3], w[2])) / w[1] / w[4] >= 2.0
+        for i in range(nw):
+            for j in range(i + 1, nw):
+                dist, sp, tp = _seg_closest(np.array(wires[i][2]), np.array(wires[i][3]),
+                                            np.array(wires[j][2]), np.array(wires[j][3]))
+                if dist <= 1e-7 and 1e-6 < sp < 1 - 1e-6 and 1e-6 < tp < 1 - 1e-6:
+                    ok = False
+        if not ok:
+            continue
+        rp = SERVE_RP if rng.random() < 0.5 else None
+        out.append((wires, [(tag, seg, 1.0) for tag, seg in srcs], ground, f, rp))
+    return out
+
+
 def mesh_workload(cells: int = 46, seed: int = 5, f0: float = 14.2e6):
     """Junctioned wire mesh over PEC ground: a square grid of cells x cells
     cells with edge 0.05 lambda in the plane z = 0.25 lambda, node positions

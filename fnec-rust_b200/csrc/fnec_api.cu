@@ -815,7 +815,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
     if (e == cudaSuccess) e = dalloc(b, &b->p, (size_t)(n));
     if (b->from_wires) DA(d_segs, b->tot_seg);
     DA(d_z, b->z_el);
-    DA(d_a, b->a_el);
+    DA(d_a, precision == FNEC_PRECISION_MIXED ? 1 : b->a_el);  // the mixed form factors in FP32
     DA(d_x, b->x_el);
     DA(d_rhs, b->rhs_el);
     DA(d_cos, b->cos_el);
@@ -1627,6 +1627,8 @@ int64_t request_bytes(const HostAnt &h, int precision) {
     int64_t b = 0;
     b += 16 * n * n * f;                                   // Z
     b += 160 * n + 256 * w + 64 * rows + 4 * n_int;        // geometry, tables, coverage maps
+    b += n * n / 16 + 64 * ((n + 63) / 64) * ((n + 64) / 64);  // fill and Gram tile lists
+    b += 16 * n * f * r;                                   // compact currents for pinned reads
     b += (16 * s + 16 * n + 8 * n + 64) * f * r;           // x, rhs, cos, feeds
     b += (48 + 32) * pts * f * r + 8 * 1024 * f * r;      // pattern, fields, partials
     if (precision == FNEC_PRECISION_MIXED) {

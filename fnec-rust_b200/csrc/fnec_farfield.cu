@@ -314,7 +314,7 @@ void launch_farfield(const UnitDesc *units, int nu, const AntDesc *ants, const D
     int staged = smem <= 200 * 1024;
     if (!staged) smem = 0;
     if (smem > 48 * 1024)
-        cudaFuncSetAttribute(k_farfield, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        set_smem_limit_once(k_farfield, 200 * 1024);
     dim3 g(max_blocks, nu);
     k_farfield<<<g, FF_THREADS, smem, st>>>(units, ants, runs, rps, pts, ibuf, x, status, fld, partials,
                                             max_blocks, staged);

@@ -11,6 +11,16 @@ namespace fnec {
 
 constexpr int PAT_STRIDE = 6;  // gain_total, gain_theta, gain_phi, axial_ratio, u_theta, u_phi
 
+// Raise a kernel's dynamic shared-memory limit to its largest use, once per
+// process.  The limit is a per-function attribute shared by every thread
+// and stream: setting it to each launch's own size would let a concurrent
+// launch (another server lane) lower it under a larger one.
+void set_smem_limit_once(const void *kernel, int bytes);  // fnec_plain.cu
+template <class K>
+inline void set_smem_limit_once(K kernel, int bytes) {
+    set_smem_limit_once(reinterpret_cast<const void *>(kernel), bytes);
+}
+
 // Device allocations of a batch: plain cudaMalloc, or the stream-ordered
 // pool (cudaMallocAsync on the batch's stream) for server lanes.
 struct DevAlloc {

@@ -1648,7 +1648,7 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     size_t smem = sizeof(cx) * (size_t)(2 * max_s + max_rows);
     int staged = smem <= 200 * 1024;
     if (!staged) smem = 0;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(k_gmres_ir, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (smem > 48 * 1024) set_smem_limit_once(k_gmres_ir, 200 * 1024);
     if (ns > 0)
         k_gmres_ir<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x, mw.v,
                                           mw.w, status, staged, mw.grid_solves.empty() ? INT_MAX : GG_MIN_S, -1);
@@ -1661,7 +1661,7 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
             int pst = psm <= 200 * 1024;
             if (!pst) psm = 0;
             if (psm > 48 * 1024)
-                cudaFuncSetAttribute(k_perm_from_piv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psm);
+                set_smem_limit_once(k_perm_from_piv, 200 * 1024);
             k_perm_from_piv<<<1, 256, psm, st>>>(d_solves, ui, piv, mw.g_perm, pst);
             GridSync *gs = static_cast<GridSync *>(mw.g_sync) + k;
             MixedUnit *mus = mw.mu;

@@ -21,6 +21,11 @@
 //   k_trailing         linear.rs:1362-1369     A22 -= L21 U12, 64x64 tiles
 //   k_backsub          linear.rs:1372-1381     one warp per unit
 //   k_feedpoints       solve_session.rs:846-947
+#include <algorithm>
+#include <climits>
+#include <mutex>
+#include <unordered_set>
+
 #include "fnec_grid.cuh"
 #include "fnec_kernels.h"
 #include "fnec_math.cuh"
@@ -942,6 +947,13 @@ void launch_gram_exact(const UnitDesc *units, int nu, int max_w, const AntDesc *
 }
 constexpr size_t TRAILING_SMEM = sizeof(cx) * (64 * (NB + 1) + NB * 64);
 
+void set_smem_limit_once(const void *kernel, int bytes) {
+    static std::mutex mu;
+    static std::unordered_set<const void *> done;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done.insert(kernel).second) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
 size_t grid_xchg_bytes() { return sizeof(PanelXchg<cx>) * GRID_PANEL_MAX_UNITS; }
 size_t grid_sync_bytes(int steps) { return sizeof(GridSync) * GRID_PANEL_MAX_UNITS * (size_t)(steps > 0 ? steps : 1); }
 
@@ -1058,7 +1070,7 @@ void launch_backsub(const UnitDesc *units, int nu, int max_s, const cx *A, cx *x
     int staged = smem <= BS_SMEM_MAX;
     if (!staged) smem = 0;
     if (smem > 48 * 1024)
-        cudaFuncSetAttribute(k_backsub, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        set_smem_limit_once(k_backsub, (int)BS_SMEM_MAX);
     if (nu > 0) k_backsub<<<nu, 32, smem, st>>>(units, A, x, status, staged);
 }
 void launch_feedpoints(const UnitDesc *solves, int ns, const AntDesc *ants, const DevSeg *segs,
@@ -1077,7 +1089,7 @@ void launch_extra_rhs_exact(const UnitDesc *solves, int ns, int max_s, const Ant
     int staged = smem <= BS_SMEM_MAX;
     if (!staged) smem = 0;
     if (smem > 48 * 1024)
-        cudaFuncSetAttribute(k_extra_rhs_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        set_smem_limit_once(k_extra_rhs_solve, (int)BS_SMEM_MAX);
     k_extra_rhs_solve<<<ns, 32, smem, st>>>(solves, A, piv, x, status, staged);
 }
 

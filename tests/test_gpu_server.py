@@ -1,0 +1,111 @@
+"""The serving loop (fnec_server_*): continuous batching over CUDA-stream
+lanes with admission by HBM budget.
+
+Each request is a random antenna deck with 1-4 source positions (separate
+right-hand sides on one factorisation) and an optional 91 x 361 pattern.
+Requests submitted together are batched and their batches overlap on the
+device; every result must equal the result of solving that deck alone:
+bit for bit in the plain FP64 form (its per-unit arithmetic does not depend
+on what else is in the batch), and within the 1e-6 feedpoint gate in the
+mixed form.
+"""
+import numpy as np
+import pytest
+
+import bench
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def acc():
+    import nec_accel
+
+    return nec_accel
+
+
+def _antennas(acc, n, seed, n_cap=400):
+    out = []
+    for wires, srcs, ground, f, rp in bench.serve_requests(n, seed=seed, n_cap=n_cap):
+        out.append(acc.Antenna(acc.wires_array(wires), acc.sources_array(srcs), [f], ground, rp,
+                               separate_sources=True))
+    return out
+
+
+def _serve(acc, ants, precision, **kw):
+    with acc.Server(precision, **kw) as srv:
+        reqs = [srv.submit(a) for a in ants]
+        for r in reqs:
+            srv.wait(r)
+        stats = srv.stats()
+    return reqs, stats
+
+
+def _alone(acc, a, precision):
+    b = acc.HallenBatch([a], precision=precision)
+    res = b.solve()
+    b.close()
+    return res
+
+
+def test_server_fp64_results_equal_solving_alone(acc):
+    ants = _antennas(acc, 16, seed=21)
+    reqs, stats = _serve(acc, ants, acc.PRECISION_FP64, lanes=2, max_batch=6)
+    assert stats["completed"] == len(ants) and stats["failed"] == 0
+    assert stats["batches"] >= 3  # 16 requests, at most 6 per batch
+    for a, r in zip(ants, reqs):
+        res = _alone(acc, a, acc.PRECISION_FP64)
+        assert r.n_solves == len(res.currents) == len(a.sources)
+        assert np.array_equal(r.status, res.status)
+        for k in range(r.n_solves):
+            assert np.array_equal(r.currents[k].view(np.uint64), res.currents[k].view(np.uint64))
+        assert np.array_equal(r.feeds, np.concatenate(res.feeds))
+        if r.pattern is not None:
+            for k in range(r.n_solves):
+                assert np.array_equal(r.pattern[k], res.pattern[k])
+        assert r.latency_ms is not None and r.latency_ms > 0.0
+
+
+def test_server_mixed_results_within_gate(acc):
+    ants = _antennas(acc, 12, seed=22)
+    mixed, stats = _serve(acc, ants, acc.PRECISION_MIXED, lanes=3, max_batch=4)
+    plain, _ = _serve(acc, ants, acc.PRECISION_FP64, lanes=1, max_batch=12)
+    assert stats["completed"] == len(ants)
+    for a, rm, rp in zip(ants, mixed, plain):
+        alone = _alone(acc, a, acc.PRECISION_MIXED)
+        for k in range(rm.n_solves):
+            zm, zp = rm.feed_z(k), rp.feed_z(k)
+            za = complex(*alone.feeds[k][0, 5:7])
+            assert abs(zm - zp) <= 1e-6 * abs(zp)
+            assert abs(zm - za) <= 1e-6 * abs(za)
+
+
+def test_server_admission_respects_budget(acc):
+    ants = _antennas(acc, 10, seed=23)
+    with acc.Server(acc.PRECISION_FP64, lanes=2, max_batch=8) as probe:
+        need = [probe.shape(a).device_bytes for a in ants]
+    budget = max(need)
+    reqs, stats = _serve(acc, ants, acc.PRECISION_FP64, lanes=2, max_batch=8, hbm_budget_bytes=budget)
+    assert stats["completed"] == len(ants)
+    assert stats["peak_in_flight_bytes"] <= budget
+    assert all(np.all(r.status == 0) for r in reqs)
+
+
+def test_server_rejects_request_above_budget(acc):
+    ants = _antennas(acc, 1, seed=24)
+    with acc.Server(acc.PRECISION_FP64, lanes=1, hbm_budget_bytes=1 << 20) as srv:
+        with pytest.raises(acc.AccelError) as e:
+            srv.submit(ants[0])
+        assert e.value.code == acc.ERR_TOO_LARGE
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_request_footprint_bounds_the_batch(acc, precision):
+    """The admission estimate is an upper bound of what a batch allocates."""
+    ants = _antennas(acc, 6, seed=25, n_cap=1500)
+    with acc.Server(precision, lanes=1) as srv:
+        for a in ants:
+            est = srv.shape(a).device_bytes
+            b = acc.HallenBatch([a], precision=precision)
+            assert b.info.device_bytes <= est, (b.info.device_bytes, est)
+            b.close()
