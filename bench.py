@@ -289,6 +289,10 @@ def reference_units(args):
     if args.workload == "mesh":
         wl, src, f = mesh_workload(args.cells)
         return [(wl, src, 1, f, None)], f"mesh: {args.cells}x{args.cells} cells over PEC ground"
+    if args.workload == "serve":
+        reqs = serve_requests(512, seed=13)
+        return ([(w, [s], g, f, rp) for w, srcs, g, f, rp in reqs for s in srcs],
+                "serve: random antennas, N lognormal (median 150), 1-4 source positions, half with 91x361 RP")
     wl = uneven_workload(args.antennas)
     return [(w, src, g, f, None) for w, src, g, f in wl], f"uneven: {len(wl)} random antennas, one frequency each"
 
@@ -324,6 +328,118 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_serve(args, acc, ctx, rank, local, dist):
+    """The served request stream: requests arrive as a Poisson process at
+    each offered rate; the submitting loop replays the arrival times and the
+    server (continuous batching over `lanes` streams, HBM-budget admission)
+    returns each request's currents, feedpoints and pattern into host
+    arrays.  Latency is submit -> results delivered, measured by the server.
+    Every number here is end to end (host decks in, host arrays out)."""
+    import torch
+
+    rates = [float(r) for r in args.rates.split(",")]
+    rng = np.random.default_rng(29)
+    n_pool = int(min(4000, max(rates) * args.serve_seconds))
+    pool = serve_requests(n_pool, seed=13)
+    ants = [acc.Antenna(acc.wires_array(w), acc.sources_array(srcs), [f], g, rp, separate_sources=True)
+            for w, srcs, g, f, rp in pool]
+    warm = ants[: min(64, len(ants))]
+    forms = {"mixed": acc.PRECISION_MIXED, "fp64": acc.PRECISION_FP64}
+    if args.precision == "fp64":
+        forms = {"fp64": acc.PRECISION_FP64}
+    elif args.precision == "mixed-only":
+        forms = {"mixed": acc.PRECISION_MIXED}
+    res = {}
+    feeds = {}
+    clocks = None
+    for name, prec in forms.items():
+        srv = acc.Server(prec, lanes=args.lanes, hbm_budget_bytes=int(args.budget_gb * (1 << 30)), max_batch=256,
+                         ctx=ctx)
+        for _ in range(max(1, args.warmup)):
+            for r in [srv.submit(a) for a in warm]:
+                srv.wait(r)
+        res[name] = []
+        for k, rate in enumerate(rates):
+            n = int(min(len(ants), max(8, rate * args.serve_seconds)))
+            gaps = rng.exponential(1.0 / rate, size=n)
+            arrive = np.cumsum(gaps) - gaps[0]
+            srv.stats(reset=True)
+            sampler = clock_sampler(local) if (name == "mixed" or len(forms) == 1) and k == len(rates) - 1 else None
+            reqs = []
+            t0 = time.perf_counter()
+            for i in range(n):
+                while time.perf_counter() - t0 < arrive[i]:
+                    pass
+                reqs.append(srv.submit(ants[i]))
+            t_sub = time.perf_counter() - t0
+            for r in reqs:
+                srv.wait(r)
+            wall = time.perf_counter() - t0
+            if sampler is not None:
+                clocks = clock_summary(sampler)
+            st = srv.stats()
+            res[name].append({"offered_req_per_s": rate, "requests": n,
+                              "achieved_submit_req_per_s": n / t_sub if t_sub > 0 else None,
+                              "solves": int(st["solves"]), "wall_s": wall,
+                              "solves_per_s": st["solves"] / wall, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                              "mean_ms": st["mean_ms"], "batches": int(st["batches"]),
+                              "max_batch": int(st["max_batch"]), "peak_in_flight_gb": st["peak_in_flight_bytes"] / 1e9,
+                              "kernel_launches": int(st["kernel_launches"]), "h2d": int(st["h2d_bytes"]),
+                              "d2h": int(st["d2h_bytes"]), "failed": int(st["failed"]),
+                              "loop_host_ms": {"plan": st["plan_ms"], "launch": st["launch_ms"],
+                                               "collect": st["collect_ms"]}})
+            if k == len(rates) - 1:
+                feeds[name] = [r.feeds.copy() for r in reqs]
+        srv.close()
+    if rank != 0:
+        return
+    gate = None
+    if "mixed" in feeds and "fp64" in feeds:
+        dz = 0.0
+        for a, b in zip(feeds["mixed"], feeds["fp64"]):
+            zm = a[:, 5] + 1j * a[:, 6]
+            zp = b[:, 5] + 1j * b[:, 6]
+            dz = max(dz, float(np.max(np.abs(zm - zp) / np.abs(zp))))
+        gate = {"max_rel_dzin_mixed_vs_fp64_gpu": dz, "gate": 1e-6, "passed": bool(dz <= 1e-6)}
+    head = "mixed" if ("mixed" in res and (gate is None or gate["passed"])) else "fp64"
+    H = res[head][-1]
+    line = {
+        "metric": METRIC, "value": H["solves_per_s"] * args.gpus, "unit": "solves/s", "n_gpus": args.gpus,
+        "steps": H["requests"], "warmup": max(1, args.warmup) * len(warm), "ms_per_step": 1e3 * H["wall_s"] / H["requests"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if head == "fp64" else "f32+f64",
+        "data": "synthetic (seeded served request stream, seed 13; Poisson arrivals, seed 29)",
+        "config": {"workload": f"serve: Poisson requests at {rates} req/s, random antennas (N lognormal median 150, "
+                               f"cap 4096), 1-4 source positions each, half with a 91x361 pattern",
+                   "precision": head, "lanes": args.lanes, "hbm_budget_gb": args.budget_gb,
+                   "step": "one request", "l2": "per-batch working sets differ; no flush between requests",
+                   "parallelism": f"replicas x{args.gpus} (no collective)"},
+        "latency_ms": {"p50": H["p50_ms"], "p99": H["p99_ms"], "what": "request submit -> results in host arrays",
+                       "offered_req_per_s": H["offered_req_per_s"]},
+        "e2e": {"value": H["solves_per_s"] * args.gpus, "unit": "solves/s",
+                "h2d_bytes_per_step": int(H["h2d"] / max(H["requests"], 1)),
+                "d2h_bytes_per_step": int(H["d2h"] / max(H["requests"], 1))},
+        "gpu_launches": H["kernel_launches"],
+        "roofline": {"kernel": None, "bound": None, "achieved": None, "peak": None, "unit": None, "frac": None,
+                     "traffic": None, "note": "the served stream runs the batch kernels; their rooflines are "
+                                              "reported by --workload uneven and sweep5"},
+        "clocks": clocks,
+        "rates": res,
+    }
+    if gate is not None:
+        line["mixed_gate"] = gate
+        line["mixed_vs_fp64"] = res["mixed"][-1]["solves_per_s"] / res["fp64"][-1]["solves_per_s"]
+    if not args.no_cpu_baseline:
+        ref_units, _ = reference_units(args)
+        threads = os.cpu_count() or 1
+        n_units = min(len(ref_units), max(threads, 4))
+        rate, dt, _, _ = cpu_oracle_units(ref_units, n_units, threads)
+        line["cpu_baseline"] = {"value": rate, "unit": "solves/s", "cores": threads, "kind": "port",
+                                "sample": f"{n_units} single-source decks of the request stream, one per thread, "
+                                          f"{dt:.1f} s wall"}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -335,9 +451,14 @@ def main():
                          "mixed-only: the chosen form alone, no accuracy gate (for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--freqs", type=int, default=201, help="sweep points (201 = the workload; fewer = profiling)")
-    ap.add_argument("--workload", default="sweep5", choices=["sweep5", "uneven", "mesh"],
+    ap.add_argument("--workload", default="sweep5", choices=["sweep5", "uneven", "mesh", "serve"],
                     help="sweep5: the 5-wire frequency sweep (headline); uneven: 4096 random antennas; "
-                         "mesh: the junctioned wire mesh over ground (one large solve)")
+                         "mesh: the junctioned wire mesh over ground (one large solve); serve: a Poisson "
+                         "request stream through the continuous-batching server")
+    ap.add_argument("--rates", default="100,1000,5000,20000", help="serve: offered request rates (req/s)")
+    ap.add_argument("--serve-seconds", type=float, default=2.0, help="serve: arrival window per rate")
+    ap.add_argument("--lanes", type=int, default=4, help="serve: concurrent batches")
+    ap.add_argument("--budget-gb", type=float, default=64.0, help="serve: HBM budget of the batches in flight")
     ap.add_argument("--cells", type=int, default=46, help="mesh workload size (cells per side)")
     ap.add_argument("--antennas", type=int, default=4096, help="uneven workload size")
     args = ap.parse_args()
@@ -361,6 +482,13 @@ def main():
     import nec_accel as acc
 
     ctx = acc.Context(local)
+    if args.workload == "serve":
+        run_serve(args, acc, ctx, rank, local, dist)
+        ctx.close()
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
     if args.workload == "sweep5":
         wires, sources, freqs, rp = sweep_workload(n_freqs=args.freqs)
         ants = [acc.Antenna(acc.wires_array(wires), acc.sources_array(sources), freqs, acc.GROUND_FREE, rp)]

@@ -16,6 +16,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "fnec_cuda.h"
@@ -534,6 +535,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
     b->from_wires = !hs.empty() && !hs[0].wires.empty();
     int64_t ff_req_max = 0, ff_int_max = 0;
     size_t smem_max = 0;
+    std::map<std::tuple<int32_t, int32_t, double, double, double, double, int32_t, int>, DevRp> map_cache;
     for (size_t ai = 0; ai < hs.size(); ++ai) {
         HostAnt &h = hs[ai];
         AntDesc a{};
@@ -673,13 +675,25 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
             b->pts.insert(b->pts.end(), h.pts.begin(), h.pts.end());
         }
         {
-            std::vector<int32_t> i2r, xr;
-            ff_cover_maps(rp, h.pts.data(), h.ground, i2r, xr);
-            rp.i2r_off = (int64_t)b->ibuf.size();
-            b->ibuf.insert(b->ibuf.end(), i2r.begin(), i2r.end());
-            rp.xr_off = (int64_t)b->ibuf.size();
-            b->ibuf.insert(b->ibuf.end(), xr.begin(), xr.end());
-            rp.n_xr = (int32_t)xr.size();
+            // antennas with the same RP card and ground share one copy of the maps
+            const bool card = rp.pts_off < 0;
+            const auto key = std::make_tuple(rp.n_theta, rp.n_phi, rp.theta0, rp.phi0, rp.d_theta, rp.d_phi,
+                                             rp.skip_integral, h.ground);
+            auto hit = card ? map_cache.find(key) : map_cache.end();
+            if (hit != map_cache.end()) {
+                rp.i2r_off = hit->second.i2r_off;
+                rp.xr_off = hit->second.xr_off;
+                rp.n_xr = hit->second.n_xr;
+            } else {
+                std::vector<int32_t> i2r, xr;
+                ff_cover_maps(rp, h.pts.data(), h.ground, i2r, xr);
+                rp.i2r_off = (int64_t)b->ibuf.size();
+                b->ibuf.insert(b->ibuf.end(), i2r.begin(), i2r.end());
+                rp.xr_off = (int64_t)b->ibuf.size();
+                b->ibuf.insert(b->ibuf.end(), xr.begin(), xr.end());
+                rp.n_xr = (int32_t)xr.size();
+                if (card) map_cache[key] = rp;
+            }
         }
         b->rps.push_back(rp);
         int64_t n_req = rp.pts_off >= 0 ? rp.n_pts : (int64_t)rp.n_theta * rp.n_phi;
@@ -1069,6 +1083,16 @@ int fnec_batch_run(fnec_batch *b) {
     auto mark = [&](int k) {
         if (b->profile) cudaEventRecord(b->ev[k], st);
     };
+    const char *failed = nullptr;  // the first phase whose launches failed
+    std::string detail;
+    auto check = [&](const char *phase) {
+        if (!failed && cudaPeekAtLastError() != cudaSuccess) failed = phase;
+    };
+    {
+        cudaError_t pre = cudaGetLastError();
+        if (pre != cudaSuccess)
+            return fail(ctx, FNEC_ERR_CUDA, std::string("an earlier call left an error: ") + cudaGetErrorString(pre));
+    }
     CUDA_TRY(ctx, cudaMemsetAsync(b->d_status, 0, sizeof(int32_t) * nu, st));
     CUDA_TRY(ctx, cudaMemsetAsync(b->d_total, 0, sizeof(double) * ns, st));
     mark(0);
@@ -1086,11 +1110,14 @@ int fnec_batch_run(fnec_batch *b) {
     }
     mark(2);
     if (b->precision == FNEC_PRECISION_MIXED) {
+        check("segments and right-hand sides");
         MixedMarks mm{b->profile ? &b->ev[3] : nullptr};
         L += run_mixed(b->mixed, b->d_units, nu, b->d_solves, ns, b->d_ants, b->d_segs, b->d_fill_tiles,
                        (int)b->fill_tiles.size(), b->d_gram_tiles, (int)b->gram_tiles.size(), b->d_ibuf,
                        b->d_crows, b->d_z, b->d_rhs, b->d_cos, b->d_x, b->d_piv, b->d_status, b->max_s,
                        b->z_given.empty(), b->max_w, b->grid, mm, st);
+        if (!failed && mm.failed_phase) failed = mm.failed_phase;
+        if (mm.detail[0]) detail = mm.detail;
     } else {
         if (b->z_given.empty()) {
             launch_fill_exact(b->d_units, b->d_ants, b->d_segs, b->d_fill_tiles, (int)b->fill_tiles.size(),
@@ -1111,10 +1138,12 @@ int fnec_batch_run(fnec_batch *b) {
         }
         mark(6);
         L += 3 + 1;  // Gram (3 kernels) and the back substitution
+        check("fill, Gram, factor and solve");
     }
     launch_feedpoints(b->d_solves, ns, b->d_ants, b->d_segs, b->d_ibuf, b->d_feeds, b->d_x, b->d_status,
                       b->d_feed_out, b->d_feed_row_off, st);
     ++L;
+    check("feedpoints");
     mark(7);
     if (b->ff_blocks > 0) {
         launch_farfield(b->d_solves, ns, b->d_ants, b->d_runs, b->d_rps, b->d_pts, b->d_ibuf, b->d_x, b->d_status, b->d_fld,
@@ -1122,8 +1151,12 @@ int fnec_batch_run(fnec_batch *b) {
         L += 2;
     }
     mark(8);
+    check("far field");
     b->launches = L;
-    CUDA_TRY(ctx, cudaGetLastError());
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return fail(ctx, FNEC_ERR_CUDA, std::string(failed ? failed : "run") + ": " + cudaGetErrorString(e) +
+                                            (detail.empty() ? "" : " [" + detail + "]"));
     return FNEC_OK;
 }
 
@@ -1662,9 +1695,12 @@ struct fnec_server {
     std::thread loop;
     // statistics since the last reset
     std::vector<double> lat_ms;
-    uint64_t submitted = 0, completed = 0, failed = 0, solves = 0, batches = 0, launches = 0;
+    uint64_t submitted = 0, completed = 0, failed = 0, solves = 0, batches = 0, launches = 0, h2d = 0, d2h = 0;
     int64_t peak_bytes = 0;
     uint64_t max_batch_seen = 0;
+    double plan_ms = 0, launch_ms = 0, collect_ms = 0;  // host time of the loop's three jobs
+    std::string last_err;  // the most recent failure, for fnec_server_last_error
+    std::string err_copy;
 };
 
 namespace {
@@ -1710,6 +1746,9 @@ void server_complete(fnec_server *S, Lane &L, bool ok) {
         }
     }
     S->launches += b->launches;
+    S->h2d += b->in_bytes;
+    S->d2h += sizeof(cx) * (size_t)b->x_el + sizeof(double) * 7 * (size_t)b->feed_rows +
+              sizeof(double) * PAT_STRIDE * (size_t)b->pat_el + sizeof(int32_t) * b->units.size();
     free_batch(b);  // pooled: the frees are ordered on the lane's stream
     delete b;
     L.b = nullptr;
@@ -1742,7 +1781,10 @@ void server_loop(fnec_server *S) {
             if (!L.b) continue;
             cudaError_t q = cudaEventQuery(L.done);
             if (q == cudaErrorNotReady) continue;
+            if (q != cudaSuccess) S->last_err = std::string("lane batch: ") + cudaGetErrorString(q);
+            const auto c0 = Clock::now();
             server_complete(S, L, q == cudaSuccess);
+            S->collect_ms += std::chrono::duration<double, std::milli>(Clock::now() - c0).count();
             progress = true;
         }
         if (progress) S->done_cv.notify_all();
@@ -1776,12 +1818,19 @@ void server_loop(fnec_server *S) {
             place.in = &L.in;
             place.out = &L.out;
             fnec_batch *b = nullptr;
+            const auto t0 = Clock::now();
             int st = build_batch(&S->own, hs, S->cfg.precision, &b, true, place);
+            const auto t1 = Clock::now();
             cudaError_t e = cudaSuccess;
             if (st == FNEC_OK) st = fnec_batch_run(b);
             if (st == FNEC_OK) e = enqueue_results(b);
             if (st == FNEC_OK && e == cudaSuccess) e = cudaEventRecord(L.done, L.st);
+            const auto t2 = Clock::now();
             lk.lock();
+            S->plan_ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
+            S->launch_ms += std::chrono::duration<double, std::milli>(t2 - t1).count();
+            if (st != FNEC_OK) S->last_err = "batch of " + std::to_string(take.size()) + " requests: " + S->own.err;
+            else if (e != cudaSuccess) S->last_err = std::string("result copies: ") + cudaGetErrorString(e);
             if (st == FNEC_OK && e == cudaSuccess) {
                 L.b = b;
                 L.reqs = take;
@@ -1987,6 +2036,11 @@ int fnec_server_stats(fnec_server *S, fnec_server_stats_t *out, int32_t reset) {
     out->peak_in_flight_bytes = (uint64_t)S->peak_bytes;
     out->max_batch = S->max_batch_seen;
     out->kernel_launches = S->launches;
+    out->h2d_bytes = S->h2d;
+    out->d2h_bytes = S->d2h;
+    out->plan_ms = S->plan_ms;
+    out->launch_ms = S->launch_ms;
+    out->collect_ms = S->collect_ms;
     out->p50_ms = pct(0.50);
     out->p99_ms = pct(0.99);
     out->max_ms = v.empty() ? 0.0 : v.back();
@@ -1995,9 +2049,17 @@ int fnec_server_stats(fnec_server *S, fnec_server_stats_t *out, int32_t reset) {
     out->mean_ms = v.empty() ? 0.0 : sum / (double)v.size();
     if (reset) {
         S->lat_ms.clear();
-        S->submitted = S->completed = S->failed = S->solves = S->batches = S->launches = 0;
+        S->submitted = S->completed = S->failed = S->solves = S->batches = S->launches = S->h2d = S->d2h = 0;
         S->peak_bytes = S->in_flight;
         S->max_batch_seen = 0;
+        S->plan_ms = S->launch_ms = S->collect_ms = 0;
     }
     return FNEC_OK;
+}
+
+const char *fnec_server_last_error(fnec_server *S) {
+    if (!S) return "";
+    std::lock_guard<std::mutex> lk(S->mu);
+    S->err_copy = S->last_err;
+    return S->err_copy.c_str();
 }

@@ -312,9 +312,11 @@ void launch_farfield(const UnitDesc *units, int nu, const AntDesc *ants, const D
                      double *total_out, cudaStream_t st) {
     if (nu <= 0 || max_blocks <= 0) return;
     int staged = smem <= 200 * 1024;
+    if (staged && smem > 0) {  // static + dynamic above 48 KB needs the raised limit
+        int lim = set_smem_limit_once(k_farfield, 200 * 1024);
+        if (lim < 0 || (size_t)lim < smem) staged = 0;
+    }
     if (!staged) smem = 0;
-    if (smem > 48 * 1024)
-        set_smem_limit_once(k_farfield, 200 * 1024);
     dim3 g(max_blocks, nu);
     k_farfield<<<g, FF_THREADS, smem, st>>>(units, ants, runs, rps, pts, ibuf, x, status, fld, partials,
                                             max_blocks, staged);

@@ -15,10 +15,11 @@ constexpr int PAT_STRIDE = 6;  // gain_total, gain_theta, gain_phi, axial_ratio,
 // process.  The limit is a per-function attribute shared by every thread
 // and stream: setting it to each launch's own size would let a concurrent
 // launch (another server lane) lower it under a larger one.
-void set_smem_limit_once(const void *kernel, int bytes);  // fnec_plain.cu
+// Returns the kernel's resulting limit (bytes), or -1 if it could not be raised.
+int set_smem_limit_once(const void *kernel, int bytes);  // fnec_plain.cu
 template <class K>
-inline void set_smem_limit_once(K kernel, int bytes) {
-    set_smem_limit_once(reinterpret_cast<const void *>(kernel), bytes);
+inline int set_smem_limit_once(K kernel, int bytes) {
+    return set_smem_limit_once(reinterpret_cast<const void *>(kernel), bytes);
 }
 
 // Device allocations of a batch: plain cudaMalloc, or the stream-ordered

@@ -1560,9 +1560,11 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
                    const AntDesc *d_ants, const DevSeg *d_segs, const int4 *fill_tiles, int n_fill,
                    const int4 *gram_tiles, int n_gram, const int32_t *ibuf, const DevConRow *crows, cx *z,
                    const cx *rhs, const double *cosv, cx *x, int32_t *piv, int32_t *status, int max_s,
-                   bool do_fill, int max_w, const GridPlan &gp, MixedMarks marks, cudaStream_t st) {
+                   bool do_fill, int max_w, const GridPlan &gp, MixedMarks &marks, cudaStream_t st) {
     uint64_t L = 0;
+    static const char *const phase_name[4] = {"fill", "gram", "factor", "refinement"};
     auto mark = [&](int k) {
+        if (!marks.failed_phase && cudaPeekAtLastError() != cudaSuccess) marks.failed_phase = phase_name[k];
         if (marks.ev) cudaEventRecord(marks.ev[k], st);
     };
     if (do_fill && n_fill > 0) {
@@ -1647,11 +1649,19 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     for (size_t i = 0; i < mw.host.size(); ++i) max_rows = max_rows > mw.host[i].rows ? max_rows : mw.host[i].rows;
     size_t smem = sizeof(cx) * (size_t)(2 * max_s + max_rows);
     int staged = smem <= 200 * 1024;
+    if (staged && smem > 0) {  // static + dynamic above 48 KB needs the raised limit
+        int lim = set_smem_limit_once(k_gmres_ir, 200 * 1024);
+        if (lim < 0 || (size_t)lim < smem) staged = 0;
+    }
     if (!staged) smem = 0;
-    if (smem > 48 * 1024) set_smem_limit_once(k_gmres_ir, 200 * 1024);
-    if (ns > 0)
+    if (ns > 0) {
         k_gmres_ir<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x, mw.v,
                                           mw.w, status, staged, mw.grid_solves.empty() ? INT_MAX : GG_MIN_S, -1);
+        cudaError_t le = cudaPeekAtLastError();
+        if (le != cudaSuccess && !marks.detail[0])
+            std::snprintf(marks.detail, sizeof(marks.detail), "GMRES launch: %d solves, %zu B shared (%s), max_s %d, rows %d",
+                          ns, smem, staged ? "staged" : "unstaged", max_s, max_rows);
+    }
     ++L;
     if (!mw.grid_solves.empty()) {
         cudaMemsetAsync(mw.g_sync, 0, sizeof(GridSync) * mw.grid_solves.size(), st);
@@ -1659,9 +1669,11 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
             int ui = mw.grid_solves[k];
             size_t psm = sizeof(int32_t) * (size_t)mw.grid_s[k];
             int pst = psm <= 200 * 1024;
+            if (pst && psm > 0) {
+                int lim = set_smem_limit_once(k_perm_from_piv, 200 * 1024);
+                if (lim < 0 || (size_t)lim < psm) pst = 0;
+            }
             if (!pst) psm = 0;
-            if (psm > 48 * 1024)
-                set_smem_limit_once(k_perm_from_piv, 200 * 1024);
             k_perm_from_piv<<<1, 256, psm, st>>>(d_solves, ui, piv, mw.g_perm, pst);
             GridSync *gs = static_cast<GridSync *>(mw.g_sync) + k;
             MixedUnit *mus = mw.mu;

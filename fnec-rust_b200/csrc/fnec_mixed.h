@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstdio>
 #include <vector>
 
 #include "fnec_kernels.h"
@@ -54,6 +55,8 @@ struct MixedWork {
 // refinement phases (ev[0..3]); null when profiling is off.
 struct MixedMarks {
     cudaEvent_t *ev;
+    const char *failed_phase = nullptr;  // set by run_mixed: the first phase whose launches failed
+    char detail[160] = {0};               // the failed launch's shape, when known
 };
 
 bool mixed_available();
@@ -68,7 +71,7 @@ uint64_t run_mixed(MixedWork &w, const UnitDesc *d_units, int nu, const UnitDesc
                    const AntDesc *d_ants, const DevSeg *d_segs, const int4 *fill_tiles, int n_fill,
                    const int4 *gram_tiles, int n_gram, const int32_t *ibuf, const DevConRow *crows, cx *z,
                    const cx *rhs, const double *cosv, cx *x, int32_t *piv, int32_t *status, int max_s,
-                   bool do_fill, int max_w, const GridPlan &gp, MixedMarks marks, cudaStream_t st);
+                   bool do_fill, int max_w, const GridPlan &gp, MixedMarks &marks, cudaStream_t st);
 cudaError_t read_mixed_stats(MixedWork &w, int32_t *iters, double *resid, cudaStream_t st);
 
 }  // namespace fnec

@@ -22,9 +22,10 @@
 //   k_backsub          linear.rs:1372-1381     one warp per unit
 //   k_feedpoints       solve_session.rs:846-947
 #include <algorithm>
+#include <cstdio>
 #include <climits>
 #include <mutex>
-#include <unordered_set>
+#include <unordered_map>
 
 #include "fnec_grid.cuh"
 #include "fnec_kernels.h"
@@ -947,11 +948,26 @@ void launch_gram_exact(const UnitDesc *units, int nu, int max_w, const AntDesc *
 }
 constexpr size_t TRAILING_SMEM = sizeof(cx) * (64 * (NB + 1) + NB * 64);
 
-void set_smem_limit_once(const void *kernel, int bytes) {
+int set_smem_limit_once(const void *kernel, int bytes) {
     static std::mutex mu;
-    static std::unordered_set<const void *> done;
+    static std::unordered_map<const void *, int> done;
     std::lock_guard<std::mutex> lk(mu);
-    if (done.insert(kernel).second) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    auto it = done.find(kernel);
+    if (it != done.end()) return it->second;
+    int got = -1;
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) {
+        got = bytes;
+    } else {
+        (void)cudaGetLastError();  // leave no error behind for the launch checks
+        std::fprintf(stderr, "fnec: shared-memory limit %d B refused (%s); kernels fall back to global staging\n",
+                     bytes, cudaGetErrorString(e));
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, kernel) == cudaSuccess) got = fa.maxDynamicSharedSizeBytes;
+        else (void)cudaGetLastError();
+    }
+    done[kernel] = got;
+    return got;
 }
 
 size_t grid_xchg_bytes() { return sizeof(PanelXchg<cx>) * GRID_PANEL_MAX_UNITS; }
@@ -1068,9 +1084,11 @@ void launch_backsub(const UnitDesc *units, int nu, int max_s, const cx *A, cx *x
                     const int32_t *status, cudaStream_t st) {
     size_t smem = sizeof(cx) * (size_t)max_s;
     int staged = smem <= BS_SMEM_MAX;
+    if (staged && smem > 0) {  // static + dynamic above 48 KB needs the raised limit
+        int lim = set_smem_limit_once(k_backsub, (int)BS_SMEM_MAX);
+        if (lim < 0 || (size_t)lim < smem) staged = 0;
+    }
     if (!staged) smem = 0;
-    if (smem > 48 * 1024)
-        set_smem_limit_once(k_backsub, (int)BS_SMEM_MAX);
     if (nu > 0) k_backsub<<<nu, 32, smem, st>>>(units, A, x, status, staged);
 }
 void launch_feedpoints(const UnitDesc *solves, int ns, const AntDesc *ants, const DevSeg *segs,
@@ -1087,9 +1105,11 @@ void launch_extra_rhs_exact(const UnitDesc *solves, int ns, int max_s, const Ant
     k_extra_rhs_b<<<g, 128, 0, st>>>(solves, ants, ibuf, z, rhs, cosv, x);
     size_t smem = sizeof(cx) * (size_t)max_s;
     int staged = smem <= BS_SMEM_MAX;
+    if (staged && smem > 0) {  // static + dynamic above 48 KB needs the raised limit
+        int lim = set_smem_limit_once(k_extra_rhs_solve, (int)BS_SMEM_MAX);
+        if (lim < 0 || (size_t)lim < smem) staged = 0;
+    }
     if (!staged) smem = 0;
-    if (smem > 48 * 1024)
-        set_smem_limit_once(k_extra_rhs_solve, (int)BS_SMEM_MAX);
     k_extra_rhs_solve<<<ns, 32, smem, st>>>(solves, A, piv, x, status, staged);
 }
 

@@ -114,7 +114,8 @@ class _RequestInfo(ctypes.Structure):
 class _ServerStats(ctypes.Structure):
     _fields_ = [("submitted", _U64), ("completed", _U64), ("failed", _U64), ("solves", _U64), ("batches", _U64),
                 ("queued", _U64), ("in_flight_bytes", _U64), ("peak_in_flight_bytes", _U64), ("max_batch", _U64),
-                ("kernel_launches", _U64), ("p50_ms", _D), ("p99_ms", _D), ("mean_ms", _D), ("max_ms", _D)]
+                ("kernel_launches", _U64), ("h2d_bytes", _U64), ("d2h_bytes", _U64),
+                ("plan_ms", _D), ("launch_ms", _D), ("collect_ms", _D), ("p50_ms", _D), ("p99_ms", _D), ("mean_ms", _D), ("max_ms", _D)]
 
 
 # name -> (restype, argtypes); every function declared in include/fnec_cuda.h
@@ -142,6 +143,7 @@ SIGNATURES = {
     "fnec_server_poll": (ctypes.c_int, [_P, _U64, _P, _P]),
     "fnec_server_wait": (ctypes.c_int, [_P, _U64, _D, _P, _P]),
     "fnec_server_stats": (ctypes.c_int, [_P, _P, _I32]),
+    "fnec_server_last_error": (ctypes.c_char_p, [_P]),
     "fnec_host_free": (ctypes.c_int, [_P]),
     "fnec_selftest_tf32x3_gemm": (ctypes.c_int, [ctypes.c_int32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
                                                  _P, _P, _P]),
@@ -736,7 +738,8 @@ class Server:
             req.latency_ms = lat
             self._pending.pop(req.ticket, None)
         if state < 0:
-            raise AccelError(state, "request failed")
+            msg = lib().fnec_server_last_error(self._h)
+            raise AccelError(state, f"request failed: {msg.decode() if msg else ''}")
 
     def poll(self, req: Request) -> bool:
         if req.state == REQ_DONE:

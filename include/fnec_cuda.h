@@ -306,6 +306,9 @@ typedef struct {
     uint64_t in_flight_bytes, peak_in_flight_bytes;
     uint64_t max_batch;       /* largest batch formed                      */
     uint64_t kernel_launches; /* kernels launched for the completed batches */
+    uint64_t h2d_bytes, d2h_bytes; /* host <-> device bytes of those batches */
+    double plan_ms, launch_ms, collect_ms; /* the loop thread's host time: batch planning,
+                                              enqueueing, result delivery */
     double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> results delivered */
 } fnec_server_stats_t;
 
@@ -326,6 +329,8 @@ int fnec_server_submit(fnec_server *s, const fnec_antenna *req, const fnec_reque
  * failed) is released by the call that reports it. */
 int fnec_server_poll(fnec_server *s, uint64_t ticket, int32_t *state, double *latency_ms);
 int fnec_server_wait(fnec_server *s, uint64_t ticket, double timeout_ms, int32_t *state, double *latency_ms);
+/* The server's most recent failure (valid until the next call). */
+const char *fnec_server_last_error(fnec_server *s);
 /* Latency percentiles over completed requests since the last reset. */
 int fnec_server_stats(fnec_server *s, fnec_server_stats_t *out, int32_t reset);
 
