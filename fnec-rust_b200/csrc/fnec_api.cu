@@ -382,6 +382,11 @@ struct fnec_batch {
     cudaStream_t st = nullptr;
     bool pooled = false;
     bool allow_grid = true;
+    unsigned char *stage = nullptr;  // page-locked staging of uploads (pooled batches)
+    size_t stage_cap = 0, stage_used = 0;
+    double alloc_ms = 0;  // host time spent allocating (device pool, pinned arenas, mixed work)
+    double t_dev = 0, t_copy = 0, t_pinned = 0, t_mixed = 0;  // its parts: device allocations,
+                                                             // table uploads, pinned arenas, mixed work
     std::vector<int32_t> grid_order;
     size_t dev_bytes = 0;
     std::vector<void *> allocs;
@@ -402,8 +407,10 @@ template <typename T>
 static cudaError_t dalloc(fnec_batch *b, T **p, size_t count) {
     *p = nullptr;
     if (count == 0) count = 1;
+    const auto t0 = std::chrono::steady_clock::now();
     cudaError_t e = b->pooled ? cudaMallocAsync((void **)p, sizeof(T) * count, b->st)
                               : cudaMalloc((void **)p, sizeof(T) * count);
+    b->t_dev += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     if (e == cudaSuccess) {
         b->allocs.push_back(*p);
         b->dev_bytes += sizeof(T) * count;
@@ -415,7 +422,11 @@ template <typename T>
 static cudaError_t up(fnec_batch *b, T *d, const std::vector<T> &h) {
     if (h.empty()) return cudaSuccess;
     b->h2d += sizeof(T) * h.size();
-    return cudaMemcpyAsync(d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, b->st);
+    const auto t0 = std::chrono::steady_clock::now();
+    DevAlloc dev{b->st, b->pooled, b->stage, b->stage_cap, &b->stage_used};
+    cudaError_t e = dev.upload(d, h.data(), sizeof(T) * h.size());
+    b->t_copy += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+    return e;
 }
 
 static void free_batch(fnec_batch *b) {
@@ -522,6 +533,7 @@ struct BatchPlace {
     bool pooled = false;
     bool allow_grid = true;
     PinnedArena *in = nullptr, *out = nullptr;  // pooled only
+    PinnedArena *aux = nullptr;                 // pooled only: staging of the other uploads
 };
 
 static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, fnec_batch **out,
@@ -531,6 +543,10 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
     b->st = place.st ? place.st : ctx->stream;
     b->pooled = place.pooled;
     b->allow_grid = place.allow_grid;
+    if (place.aux) {
+        b->stage = place.aux->p;
+        b->stage_cap = place.aux->cap;
+    }
     b->precision = precision;
     b->from_wires = !hs.empty() && !hs[0].wires.empty();
     int64_t ff_req_max = 0, ff_int_max = 0;
@@ -792,9 +808,11 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
            o_ft = pk.add(b->fill_tiles), o_crows = pk.add(b->crows), o_gt = pk.add(b->gram_tiles), o_fro = pk.add(b->feed_row_off),
            o_rhs = pk.add(b->rhs_given), o_cos = pk.add(b->cos_given), o_z = pk.add(b->z_given);
     b->in_bytes = pk.total > 0 ? pk.total : 256;
+    const auto ta0 = std::chrono::steady_clock::now();
     if (b->pooled) {
         e = place.in->ensure(b->in_bytes);
         b->h_in = place.in->p;
+        b->t_pinned += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta0).count();
     } else {
         e = cudaMallocHost((void **)&b->h_in, b->in_bytes);
     }
@@ -874,15 +892,22 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
                    (sizeof(int32_t) + sizeof(double)) * (size_t)(nu + b->solves.size()) + 64;
     if (e == cudaSuccess) {
         if (b->pooled) {
+            const auto tp = std::chrono::steady_clock::now();
             e = place.out->ensure(b->out_bytes);
             b->h_out = place.out->p;
+            b->t_pinned += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tp).count();
         } else {
             e = cudaMallocHost((void **)&b->h_out, b->out_bytes);
         }
     }
     if (e == cudaSuccess && precision == FNEC_PRECISION_MIXED) {
-        e = alloc_mixed(b->mixed, b->units, b->solves, b->ants, b->max_s, DevAlloc{b->st, b->pooled},
-                        b->allow_grid);
+        const auto tm = std::chrono::steady_clock::now();
+        e = alloc_mixed(b->mixed, b->units, b->solves, b->ants, b->max_s,
+                        DevAlloc{b->st, b->pooled, b->stage, b->stage_cap, &b->stage_used}, b->allow_grid);
+        b->t_mixed += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tm).count();
+    }
+    b->alloc_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta0).count();
+    if (e == cudaSuccess && precision == FNEC_PRECISION_MIXED) {
         b->dev_bytes += b->mixed.bytes;
     }
     if (e != cudaSuccess) {
@@ -1609,16 +1634,17 @@ int fnec_dispatch_frequency_point(int request_kind, double freq_hz) {
 // ---------------------------------------------------------------------------
 // Serving: requests (one antenna deck each) batched continuously over lanes.
 //
-// A host thread owns the device side.  Each lane is a CUDA stream that runs
-// one batch at a time; whenever a lane is free and requests are queued, the
-// thread admits requests in arrival order while the device bytes of the
+// Each lane is a CUDA stream driven by its own host thread.  A lane that is
+// free takes queued requests in arrival order while the device bytes of the
 // batches in flight stay within the HBM budget, plans them as one batch
-// (stream-ordered pool allocations, the lane's pinned arenas), and enqueues
-// upload + solve + result copies on the lane.  Requests that arrive while
-// other batches run are admitted as soon as a lane and memory are free, and
-// the lanes' kernels overlap on the device.  A request's systems keep Z and
-// the factor on the device for all of its right-hand sides (one per source
-// position) and its pattern.
+// (stream-ordered pool allocations), enqueues upload + solve + result copies
+// on its stream, sleeps on the completion event, and delivers the results.
+// Requests that arrive while other batches run are taken by the next free
+// lane; the lanes' planning, kernels and copies overlap.  A request's systems
+// keep Z and the factor on the device for all of its right-hand sides (one
+// per source position) and its pattern.  Results land in a page-locked slab
+// of the server: requests submitted with output arrays get a copy, the others
+// read the slab in place until they are released.
 // ---------------------------------------------------------------------------
 #include <condition_variable>
 #include <deque>
@@ -1630,23 +1656,32 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+struct Slab {  // page-locked results of one batch, shared by its requests
+    PinnedArena mem;
+    int refs = 0;
+};
+
 struct ServerReq {
     uint64_t ticket = 0;
     HostAnt host;
     fnec_request_out out{};
+    bool copy_out = false;
     int64_t bytes = 0;
-    uint32_t n_solves = 0, n = 0, n_points = 0;
+    uint32_t n_solves = 0, n = 0, s = 0, n_points = 0, n_feed_rows = 0;
     Clock::time_point t_submit, t_done;
     int32_t state = FNEC_REQ_QUEUED;
+    // results in place (no output arrays): offsets into the slab
+    Slab *slab = nullptr;
+    size_t x_off = 0, feed_row = 0, pat_row = 0;  // complex / feed rows / pattern rows
+    size_t hf_off = 0, hp_off = 0;                // byte offsets of the feed and pattern blocks
+    std::vector<int32_t> status;
 };
 
 struct Lane {
     cudaStream_t st = nullptr;
     cudaEvent_t done = nullptr;
-    fnec_batch *b = nullptr;
-    std::vector<ServerReq *> reqs;
-    int64_t bytes = 0;
-    PinnedArena in, out;
+    PinnedArena in, aux;
+    std::thread worker;
 };
 
 // Upper bound of the device bytes one request's batch needs (Z, the
@@ -1678,86 +1713,107 @@ int64_t request_bytes(const HostAnt &h, int precision) {
     return b + (1 << 20);
 }
 
+bool finished(const ServerReq *r) { return r->state == FNEC_REQ_DONE || r->state < 0; }
+
+constexpr size_t SERVER_IN_ARENA = 128ull << 20;  // packed inputs of one batch
+constexpr size_t SERVER_AUX_ARENA = 64ull << 20;  // its other uploads
+constexpr size_t SERVER_SLAB = 512ull << 20;      // results of one batch (grows for larger ones)
+
 }  // namespace
 
 struct fnec_server {
-    fnec_ctx own;  // the loop's private context (its own error string)
+    int device = 0;
     fnec_server_config cfg{};
     std::mutex mu;
-    std::condition_variable cv;       // wakes the loop
+    std::condition_variable work_cv;  // wakes lanes: a request queued, memory freed, stop
     std::condition_variable done_cv;  // wakes waiters
     std::deque<ServerReq *> queue;
+    std::deque<uint64_t> done_q;  // finished tickets, in completion order
     std::unordered_map<uint64_t, ServerReq *> live;
     std::vector<Lane> lanes;
+    std::vector<Slab *> slabs_free, slabs_all;
+    size_t max_slabs = 0;  // page-locked result slabs, at most (lanes and unreleased requests share them)
     int64_t in_flight = 0;
     uint64_t next_ticket = 1;
     bool stop = false;
-    std::thread loop;
     // statistics since the last reset
     std::vector<double> lat_ms;
     uint64_t submitted = 0, completed = 0, failed = 0, solves = 0, batches = 0, launches = 0, h2d = 0, d2h = 0;
     int64_t peak_bytes = 0;
     uint64_t max_batch_seen = 0;
-    double plan_ms = 0, launch_ms = 0, collect_ms = 0;  // host time of the loop's three jobs
+    double plan_ms = 0, launch_ms = 0, collect_ms = 0;  // host time of the lanes' three jobs
+    double alloc_ms = 0;                                // of plan_ms: allocation
+    double t_dev = 0, t_copy = 0, t_pinned = 0, t_mixed = 0;
     std::string last_err;  // the most recent failure, for fnec_server_last_error
     std::string err_copy;
 };
 
 namespace {
 
-// Copies a finished lane's results into its requests' output arrays.
-void server_complete(fnec_server *S, Lane &L, bool ok) {
-    fnec_batch *b = L.b;
+void slab_unref(fnec_server *S, Slab *sl) {  // S->mu held
+    if (sl && --sl->refs == 0) S->slabs_free.push_back(sl);
+}
+
+// Takes the next batch (arrival order, within budget and max_batch); S->mu held.
+std::vector<ServerReq *> admit(fnec_server *S, int64_t &bytes) {
+    std::vector<ServerReq *> take;
+    bytes = 0;
+    while (!S->queue.empty() && take.size() < S->cfg.max_batch) {
+        ServerReq *r = S->queue.front();
+        if (S->in_flight + bytes + r->bytes > (int64_t)S->cfg.hbm_budget_bytes) break;
+        bytes += r->bytes;
+        take.push_back(r);
+        S->queue.pop_front();
+    }
+    return take;
+}
+
+// Distribute a finished batch's results (in the slab b->h_out) to its requests.
+void deliver(fnec_batch *b, const std::vector<ServerReq *> &take, Slab *slab, bool ok) {
     const unsigned char *hx = b->h_out;
-    const unsigned char *hf = hx + sizeof(cx) * (size_t)b->x_el;
-    const unsigned char *hp = hf + sizeof(double) * 7 * (size_t)b->feed_rows;
-    const int32_t *hst = (const int32_t *)(hp + sizeof(double) * PAT_STRIDE * (size_t)b->pat_el);
+    const size_t f_off = sizeof(cx) * (size_t)b->x_el;
+    const size_t p_off = f_off + sizeof(double) * 7 * (size_t)b->feed_rows;
+    const int32_t *hst = (const int32_t *)(hx + p_off + sizeof(double) * PAT_STRIDE * (size_t)b->pat_el);
     const cx *x = (const cx *)hx;
-    std::vector<uint32_t> k_of(L.reqs.size(), 0);    // next solve slot of each request
-    std::vector<size_t> row_of(L.reqs.size(), 0);    // next feed row of each request
+    struct Next {
+        uint32_t k = 0;    // next solve of the request
+        size_t row = 0;    // its next feed row
+    };
+    std::vector<Next> next(take.size());
     for (size_t u = 0; u < b->solves.size(); ++u) {
         const fnec_unit_info &ui = b->uinfo[u];
-        ServerReq *r = L.reqs[ui.antenna];
-        const uint32_t k = k_of[ui.antenna]++;
-        const size_t row0 = row_of[ui.antenna];
-        row_of[ui.antenna] += ui.n_feed;
-        const int32_t st = ok ? hst[b->solves[u].sys] : FNEC_ERR_CUDA;
-        if (r->out.status) r->out.status[k] = st;
-        if (!ok) continue;
+        ServerReq *r = take[ui.antenna];
+        const uint32_t k = next[ui.antenna].k++;
+        const size_t row0 = next[ui.antenna].row;
+        next[ui.antenna].row += ui.n_feed;
+        r->status[k] = ok ? hst[b->solves[u].sys] : FNEC_ERR_CUDA;
+        if (k == 0) {  // a request's solves are consecutive: its first solve locates its blocks
+            r->slab = slab;
+            r->x_off = (size_t)b->solves[u].x_off;
+            r->feed_row = (size_t)ui.feed_off;
+            r->pat_row = (size_t)ui.pat_off;
+            r->hf_off = f_off;
+            r->hp_off = p_off;
+        }
+        if (!ok || !r->copy_out) continue;
+        if (r->out.status) r->out.status[k] = r->status[k];
         if (r->out.currents)
             std::memcpy(r->out.currents + 2 * (size_t)k * r->n, &x[b->solves[u].x_off], sizeof(cx) * ui.n);
         if (r->out.feeds && ui.n_feed)
-            std::memcpy(r->out.feeds + 7 * row0, hf + sizeof(double) * 7 * ui.feed_off,
+            std::memcpy(r->out.feeds + 7 * row0, hx + f_off + sizeof(double) * 7 * ui.feed_off,
                         sizeof(double) * 7 * ui.n_feed);
         if (r->out.pattern && ui.n_points)
             std::memcpy(r->out.pattern + (size_t)PAT_STRIDE * k * r->n_points,
-                        hp + sizeof(double) * PAT_STRIDE * ui.pat_off, sizeof(double) * PAT_STRIDE * ui.n_points);
+                        hx + p_off + sizeof(double) * PAT_STRIDE * ui.pat_off,
+                        sizeof(double) * PAT_STRIDE * ui.n_points);
     }
-    const auto now = Clock::now();
-    for (ServerReq *r : L.reqs) {
-        r->t_done = now;
-        r->state = ok ? FNEC_REQ_DONE : FNEC_ERR_CUDA;
-        if (ok) {
-            S->lat_ms.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
-            ++S->completed;
-            S->solves += r->n_solves;
-        } else {
-            ++S->failed;
-        }
-    }
-    S->launches += b->launches;
-    S->h2d += b->in_bytes;
-    S->d2h += sizeof(cx) * (size_t)b->x_el + sizeof(double) * 7 * (size_t)b->feed_rows +
-              sizeof(double) * PAT_STRIDE * (size_t)b->pat_el + sizeof(int32_t) * b->units.size();
-    free_batch(b);  // pooled: the frees are ordered on the lane's stream
-    delete b;
-    L.b = nullptr;
-    L.reqs.clear();
-    S->in_flight -= L.bytes;
-    L.bytes = 0;
+    if (!ok)
+        for (ServerReq *r : take)
+            if (r->out.status)
+                for (uint32_t k = 0; k < r->n_solves; ++k) r->out.status[k] = FNEC_ERR_CUDA;
 }
 
-// Enqueue the device -> pinned copies of every result of a lane's batch.
+// Enqueue the device -> slab copies of every result of a batch.
 cudaError_t enqueue_results(fnec_batch *b) {
     unsigned char *hx = b->h_out;
     unsigned char *hf = hx + sizeof(cx) * (size_t)b->x_el;
@@ -1772,98 +1828,118 @@ cudaError_t enqueue_results(fnec_batch *b) {
     return e;
 }
 
-void server_loop(fnec_server *S) {
-    cudaSetDevice(S->own.device);
-    std::unique_lock<std::mutex> lk(S->mu);
+void lane_worker(fnec_server *S, Lane *L) {
+    cudaSetDevice(S->device);
+    fnec_ctx own;  // this lane's private context: its own error string
+    own.device = S->device;
+    own.stream = L->st;
     for (;;) {
-        bool progress = false;
-        for (Lane &L : S->lanes) {  // completions
-            if (!L.b) continue;
-            cudaError_t q = cudaEventQuery(L.done);
-            if (q == cudaErrorNotReady) continue;
-            if (q != cudaSuccess) S->last_err = std::string("lane batch: ") + cudaGetErrorString(q);
-            const auto c0 = Clock::now();
-            server_complete(S, L, q == cudaSuccess);
-            S->collect_ms += std::chrono::duration<double, std::milli>(Clock::now() - c0).count();
-            progress = true;
-        }
-        if (progress) S->done_cv.notify_all();
-        bool busy = false;
-        for (Lane &L : S->lanes) busy = busy || L.b;
-        if (S->stop && S->queue.empty() && !busy) break;
-        // admissions: a free lane takes queued requests in arrival order
-        for (Lane &L : S->lanes) {
-            if (L.b || S->queue.empty()) continue;
-            std::vector<ServerReq *> take;
-            int64_t bytes = 0;
-            while (!S->queue.empty() && take.size() < S->cfg.max_batch) {
-                ServerReq *r = S->queue.front();
-                if (S->in_flight + bytes + r->bytes > (int64_t)S->cfg.hbm_budget_bytes) break;
-                bytes += r->bytes;
-                take.push_back(r);
-                S->queue.pop_front();
+        std::vector<ServerReq *> take;
+        int64_t bytes = 0;
+        Slab *slab = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            for (;;) {
+                // a result slab must be free (or creatable) before requests are taken:
+                // allocating page-locked memory while other lanes run stalls them all
+                const bool slab_ok = !S->slabs_free.empty() || S->slabs_all.size() < S->max_slabs;
+                if (slab_ok) {
+                    take = admit(S, bytes);
+                    if (!take.empty()) break;
+                }
+                if (S->stop && S->queue.empty()) return;
+                S->work_cv.wait(lk);
             }
-            if (take.empty()) break;  // the head waits for memory: arrival order is kept
             for (ServerReq *r : take) r->state = FNEC_REQ_RUNNING;
             S->in_flight += bytes;
-            L.bytes = bytes;
-            lk.unlock();
-            std::vector<HostAnt> hs;
-            hs.reserve(take.size());
-            for (ServerReq *r : take) hs.push_back(r->host);
-            BatchPlace place;
-            place.st = L.st;
-            place.pooled = true;
-            place.allow_grid = S->lanes.size() == 1;  // cooperative kernels need the whole device
-            place.in = &L.in;
-            place.out = &L.out;
-            fnec_batch *b = nullptr;
-            const auto t0 = Clock::now();
-            int st = build_batch(&S->own, hs, S->cfg.precision, &b, true, place);
-            const auto t1 = Clock::now();
-            cudaError_t e = cudaSuccess;
-            if (st == FNEC_OK) st = fnec_batch_run(b);
-            if (st == FNEC_OK) e = enqueue_results(b);
-            if (st == FNEC_OK && e == cudaSuccess) e = cudaEventRecord(L.done, L.st);
-            const auto t2 = Clock::now();
-            lk.lock();
-            S->plan_ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
-            S->launch_ms += std::chrono::duration<double, std::milli>(t2 - t1).count();
-            if (st != FNEC_OK) S->last_err = "batch of " + std::to_string(take.size()) + " requests: " + S->own.err;
-            else if (e != cudaSuccess) S->last_err = std::string("result copies: ") + cudaGetErrorString(e);
-            if (st == FNEC_OK && e == cudaSuccess) {
-                L.b = b;
-                L.reqs = take;
-                ++S->batches;
-                S->max_batch_seen = std::max<uint64_t>(S->max_batch_seen, take.size());
-                S->peak_bytes = std::max(S->peak_bytes, S->in_flight);
+            S->peak_bytes = std::max(S->peak_bytes, S->in_flight);
+            if (!S->slabs_free.empty()) {
+                slab = S->slabs_free.back();
+                S->slabs_free.pop_back();
             } else {
-                if (b) {
-                    cudaStreamSynchronize(L.st);
-                    free_batch(b);
-                    delete b;
-                }
-                S->in_flight -= L.bytes;
-                L.bytes = 0;
-                const auto now = Clock::now();
-                for (ServerReq *r : take) {
-                    r->state = st != FNEC_OK ? st : FNEC_ERR_CUDA;
-                    r->t_done = now;
-                    if (r->out.status)
-                        for (uint32_t k = 0; k < r->n_solves; ++k) r->out.status[k] = r->state;
+                slab = new Slab();
+                S->slabs_all.push_back(slab);
+            }
+        }
+        std::vector<HostAnt> hs;
+        hs.reserve(take.size());
+        for (ServerReq *r : take) hs.push_back(r->host);
+        BatchPlace place;
+        place.st = L->st;
+        place.pooled = true;
+        place.allow_grid = S->lanes.size() == 1;  // cooperative kernels need the whole device
+        place.in = &L->in;
+        place.out = &slab->mem;
+        place.aux = &L->aux;
+        fnec_batch *b = nullptr;
+        const auto t0 = Clock::now();
+        int st = build_batch(&own, hs, S->cfg.precision, &b, true, place);
+        const auto t1 = Clock::now();
+        cudaError_t e = cudaSuccess;
+        if (st == FNEC_OK) st = fnec_batch_run(b);
+        if (st == FNEC_OK) e = enqueue_results(b);
+        if (st == FNEC_OK && e == cudaSuccess) e = cudaEventRecord(L->done, L->st);
+        const auto t2 = Clock::now();
+        if (st == FNEC_OK && e == cudaSuccess) e = cudaEventSynchronize(L->done);  // the thread sleeps
+        const bool ok = st == FNEC_OK && e == cudaSuccess;
+        const auto t3 = Clock::now();
+        if (b) deliver(b, take, slab, ok);
+        const auto t4 = Clock::now();
+        uint64_t launches = 0, h2d = 0, d2h = 0;
+        double alloc_ms = 0, t_dev = 0, t_copy = 0, t_pinned = 0, t_mixed = 0;
+        if (b) {
+            alloc_ms = b->alloc_ms;
+            t_dev = b->t_dev;
+            t_copy = b->t_copy;
+            t_pinned = b->t_pinned;
+            t_mixed = b->t_mixed;
+            launches = b->launches;
+            h2d = b->in_bytes;
+            d2h = sizeof(cx) * (size_t)b->x_el + sizeof(double) * 7 * (size_t)b->feed_rows +
+                  sizeof(double) * PAT_STRIDE * (size_t)b->pat_el + sizeof(int32_t) * b->units.size();
+            if (!ok) cudaStreamSynchronize(L->st);
+            free_batch(b);  // pooled: the frees are ordered on the lane's stream
+            delete b;
+        }
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->plan_ms += std::chrono::duration<double, std::milli>(t1 - t0).count();
+            S->alloc_ms += alloc_ms;
+            S->t_dev += t_dev;
+            S->t_copy += t_copy;
+            S->t_pinned += t_pinned;
+            S->t_mixed += t_mixed;
+            S->launch_ms += std::chrono::duration<double, std::milli>(t2 - t1).count();
+            S->collect_ms += std::chrono::duration<double, std::milli>(t4 - t3).count();
+            if (!ok) {
+                if (st != FNEC_OK) S->last_err = "batch of " + std::to_string(take.size()) + " requests: " + own.err;
+                else S->last_err = std::string("lane batch: ") + cudaGetErrorString(e);
+            }
+            S->in_flight -= bytes;
+            ++S->batches;
+            S->max_batch_seen = std::max<uint64_t>(S->max_batch_seen, take.size());
+            S->launches += launches;
+            S->h2d += h2d;
+            S->d2h += d2h;
+            const auto now = Clock::now();
+            for (ServerReq *r : take) {
+                r->t_done = now;
+                r->state = ok ? FNEC_REQ_DONE : (st != FNEC_OK ? st : FNEC_ERR_CUDA);
+                if (ok) {
+                    S->lat_ms.push_back(std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count());
+                    ++S->completed;
+                    S->solves += r->n_solves;
+                    if (!r->copy_out) ++slab->refs;  // read in place until released
+                } else {
                     ++S->failed;
                 }
-                S->done_cv.notify_all();
+                if (r->copy_out || !ok) r->slab = nullptr;
+                S->done_q.push_back(r->ticket);
             }
-            progress = true;
+            if (slab->refs == 0) S->slabs_free.push_back(slab);
         }
-        if (!progress) {
-            busy = false;
-            for (Lane &L : S->lanes) busy = busy || L.b;
-            // poll the lanes every 20 us while work is in flight, else sleep until woken
-            if (busy) S->cv.wait_for(lk, std::chrono::microseconds(20));
-            else S->cv.wait_for(lk, std::chrono::milliseconds(50));
-        }
+        S->done_cv.notify_all();
+        S->work_cv.notify_all();  // memory freed: the queue head may fit now
     }
 }
 
@@ -1878,14 +1954,13 @@ int fnec_server_create(fnec_ctx *ctx, const fnec_server_config *cfg, fnec_server
         return fail(ctx, FNEC_ERR_BAD_ARG, "lanes 1..16, max_batch >= 1 and a nonzero HBM budget");
     cudaSetDevice(ctx->device);
     fnec_server *S = new fnec_server();
-    S->own.device = ctx->device;
-    S->own.stream = ctx->stream;
+    S->device = ctx->device;
     S->cfg = *cfg;
     if (S->cfg.queue_cap == 0) S->cfg.queue_cap = 1u << 20;
     S->lanes.resize(cfg->lanes);
     for (Lane &L : S->lanes) {
         if (cudaStreamCreateWithFlags(&L.st, cudaStreamNonBlocking) != cudaSuccess ||
-            cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming) != cudaSuccess) {
+            cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming | cudaEventBlockingSync) != cudaSuccess) {
             for (Lane &M : S->lanes) {
                 if (M.done) cudaEventDestroy(M.done);
                 if (M.st) cudaStreamDestroy(M.st);
@@ -1900,7 +1975,20 @@ int fnec_server_create(fnec_ctx *ctx, const fnec_server_config *cfg, fnec_server
         uint64_t keep = UINT64_MAX;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
     }
-    S->loop = std::thread(server_loop, S);
+    // page-locked arenas sized for typical batches up front: growing one later
+    // frees the old arena, which waits for the whole device
+    for (Lane &L : S->lanes) {
+        L.in.ensure((size_t)SERVER_IN_ARENA);
+        L.aux.ensure((size_t)SERVER_AUX_ARENA);
+    }
+    S->max_slabs = (size_t)cfg->lanes + 4;
+    for (size_t i = 0; i < S->max_slabs; ++i) {
+        Slab *sl = new Slab();
+        sl->mem.ensure((size_t)SERVER_SLAB);
+        S->slabs_all.push_back(sl);
+        S->slabs_free.push_back(sl);
+    }
+    for (Lane &L : S->lanes) L.worker = std::thread(lane_worker, S, &L);
     *out = S;
     return FNEC_OK;
 }
@@ -1911,17 +1999,22 @@ int fnec_server_destroy(fnec_server *S) {
         std::lock_guard<std::mutex> lk(S->mu);
         S->stop = true;
     }
-    S->cv.notify_all();
-    if (S->loop.joinable()) S->loop.join();
-    cudaSetDevice(S->own.device);
+    S->work_cv.notify_all();
+    for (Lane &L : S->lanes)
+        if (L.worker.joinable()) L.worker.join();
+    cudaSetDevice(S->device);
     for (Lane &L : S->lanes) {
         cudaStreamSynchronize(L.st);
         L.in.release();
-        L.out.release();
+        L.aux.release();
         cudaEventDestroy(L.done);
         cudaStreamDestroy(L.st);
     }
     for (auto &kv : S->live) delete kv.second;
+    for (Slab *sl : S->slabs_all) {
+        sl->mem.release();
+        delete sl;
+    }
     delete S;
     return FNEC_OK;
 }
@@ -1944,8 +2037,9 @@ int fnec_request_shape(fnec_ctx *ctx, const fnec_antenna *req, int32_t precision
     return FNEC_OK;
 }
 
-int fnec_server_submit(fnec_server *S, const fnec_antenna *req, const fnec_request_out *out, uint64_t *ticket) {
-    if (!S || !req || !out || !ticket) return FNEC_ERR_BAD_ARG;
+int fnec_server_submit(fnec_server *S, const fnec_antenna *req, const fnec_request_out *out, uint64_t *ticket,
+                       fnec_request_info *info) {
+    if (!S || !req || !ticket) return FNEC_ERR_BAD_ARG;
     ServerReq *r = new ServerReq();
     std::string why;
     int st = antenna_from_cards(*req, r->host, why);
@@ -1953,12 +2047,29 @@ int fnec_server_submit(fnec_server *S, const fnec_antenna *req, const fnec_reque
         delete r;
         return st;
     }
-    r->out = *out;
-    r->n = (uint32_t)r->host.segs.size();
-    r->n_solves = (uint32_t)(std::max<size_t>(r->host.rhs_srcs.size(), 1) * r->host.freqs.size());
-    r->n_points = r->host.rp.pts_off >= 0 ? (uint32_t)(r->host.pts.size() / 2)
-                                          : (uint32_t)(r->host.rp.n_theta * r->host.rp.n_phi);
-    r->bytes = request_bytes(r->host, S->cfg.precision);
+    if (out) {
+        r->out = *out;
+        r->copy_out = true;
+    }
+    const HostAnt &h = r->host;
+    r->n = (uint32_t)h.segs.size();
+    r->s = r->n + (uint32_t)h.ep.size();
+    r->n_solves = (uint32_t)(std::max<size_t>(h.rhs_srcs.size(), 1) * h.freqs.size());
+    r->n_points = h.rp.pts_off >= 0 ? (uint32_t)(h.pts.size() / 2) : (uint32_t)(h.rp.n_theta * h.rp.n_phi);
+    uint32_t fr = 0;
+    for (auto &v : h.rhs_feeds) fr += (uint32_t)v.size();
+    r->n_feed_rows = fr * (uint32_t)h.freqs.size();
+    r->status.assign(r->n_solves, 0);
+    r->bytes = request_bytes(h, S->cfg.precision);
+    if (info) {
+        info->n_segments = r->n;
+        info->n_rhs = (uint32_t)std::max<size_t>(h.rhs_srcs.size(), 1);
+        info->n_solves = r->n_solves;
+        info->n_feed_rows = r->n_feed_rows;
+        info->n_points = r->n_points;
+        info->pad = 0;
+        info->device_bytes = (uint64_t)r->bytes;
+    }
     if (r->bytes > (int64_t)S->cfg.hbm_budget_bytes) {
         delete r;
         return FNEC_ERR_TOO_LARGE;
@@ -1976,7 +2087,7 @@ int fnec_server_submit(fnec_server *S, const fnec_antenna *req, const fnec_reque
         ++S->submitted;
         *ticket = r->ticket;
     }
-    S->cv.notify_all();
+    S->work_cv.notify_one();
     return FNEC_OK;
 }
 
@@ -1987,11 +2098,8 @@ int fnec_server_poll(fnec_server *S, uint64_t ticket, int32_t *state, double *la
     if (it == S->live.end()) return FNEC_ERR_BAD_ARG;
     ServerReq *r = it->second;
     *state = r->state;
-    if (r->state == FNEC_REQ_DONE || r->state < 0) {
-        if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
-        S->live.erase(it);
-        delete r;
-    }
+    if (finished(r) && latency_ms)
+        *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
     return FNEC_OK;
 }
 
@@ -2002,17 +2110,71 @@ int fnec_server_wait(fnec_server *S, uint64_t ticket, double timeout_ms, int32_t
     if (it == S->live.end()) return FNEC_ERR_BAD_ARG;
     ServerReq *r = it->second;
     const auto until = Clock::now() + std::chrono::microseconds((int64_t)(timeout_ms * 1000.0));
-    while (!(r->state == FNEC_REQ_DONE || r->state < 0)) {
-        if (S->done_cv.wait_until(lk, until) == std::cv_status::timeout &&
-            !(r->state == FNEC_REQ_DONE || r->state < 0)) {
+    while (!finished(r)) {
+        if (S->done_cv.wait_until(lk, until) == std::cv_status::timeout && !finished(r)) {
             *state = r->state;
             return FNEC_ERR_TIMEOUT;
         }
     }
     *state = r->state;
     if (latency_ms) *latency_ms = std::chrono::duration<double, std::milli>(r->t_done - r->t_submit).count();
+    return FNEC_OK;
+}
+
+int fnec_server_next_done(fnec_server *S, double timeout_ms, uint64_t *ticket) {
+    if (!S || !ticket) return FNEC_ERR_BAD_ARG;
+    std::unique_lock<std::mutex> lk(S->mu);
+    const auto until = Clock::now() + std::chrono::microseconds((int64_t)(timeout_ms * 1000.0));
+    for (;;) {
+        while (!S->done_q.empty() && !S->live.count(S->done_q.front())) S->done_q.pop_front();  // released
+        if (!S->done_q.empty()) break;
+        if (S->done_cv.wait_until(lk, until) == std::cv_status::timeout) {
+            while (!S->done_q.empty() && !S->live.count(S->done_q.front())) S->done_q.pop_front();
+            if (S->done_q.empty()) return FNEC_ERR_TIMEOUT;
+            break;
+        }
+    }
+    *ticket = S->done_q.front();
+    S->done_q.pop_front();
+    return FNEC_OK;
+}
+
+int fnec_server_result(fnec_server *S, uint64_t ticket, fnec_request_result *out) {
+    if (!S || !out) return FNEC_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->live.find(ticket);
+    if (it == S->live.end()) return FNEC_ERR_BAD_ARG;
+    ServerReq *r = it->second;
+    if (!finished(r)) return FNEC_ERR_BUSY;
+    std::memset(out, 0, sizeof(*out));
+    out->n_solves = r->n_solves;
+    out->n_segments = r->n;
+    out->n_feed_rows = r->n_feed_rows;
+    out->n_points = r->n_points;
+    out->status = r->status.data();
+    if (r->slab && r->state == FNEC_REQ_DONE) {
+        const unsigned char *base = r->slab->mem.p;
+        out->currents = (const double *)(base + sizeof(cx) * r->x_off);
+        out->cur_stride = r->s;
+        out->feeds = (const double *)(base + r->hf_off + sizeof(double) * 7 * r->feed_row);
+        out->pattern = r->n_points ? (const double *)(base + r->hp_off + sizeof(double) * PAT_STRIDE * r->pat_row)
+                                   : nullptr;
+    }
+    return FNEC_OK;
+}
+
+int fnec_server_release(fnec_server *S, uint64_t ticket) {
+    if (!S) return FNEC_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->live.find(ticket);
+    if (it == S->live.end()) return FNEC_ERR_BAD_ARG;
+    ServerReq *r = it->second;
+    if (!finished(r)) return FNEC_ERR_BUSY;
+    const bool freed = r->slab && r->slab->refs == 1;
+    slab_unref(S, r->slab);
     S->live.erase(it);
     delete r;
+    if (freed) S->work_cv.notify_all();  // a lane may be waiting for a slab
     return FNEC_OK;
 }
 
@@ -2041,6 +2203,11 @@ int fnec_server_stats(fnec_server *S, fnec_server_stats_t *out, int32_t reset) {
     out->plan_ms = S->plan_ms;
     out->launch_ms = S->launch_ms;
     out->collect_ms = S->collect_ms;
+    out->alloc_ms = S->alloc_ms;
+    out->alloc_device_ms = S->t_dev;
+    out->alloc_upload_ms = S->t_copy;
+    out->alloc_pinned_ms = S->t_pinned;
+    out->alloc_mixed_ms = S->t_mixed;
     out->p50_ms = pct(0.50);
     out->p99_ms = pct(0.99);
     out->max_ms = v.empty() ? 0.0 : v.back();
@@ -2052,7 +2219,8 @@ int fnec_server_stats(fnec_server *S, fnec_server_stats_t *out, int32_t reset) {
         S->submitted = S->completed = S->failed = S->solves = S->batches = S->launches = S->h2d = S->d2h = 0;
         S->peak_bytes = S->in_flight;
         S->max_batch_seen = 0;
-        S->plan_ms = S->launch_ms = S->collect_ms = 0;
+        S->plan_ms = S->launch_ms = S->collect_ms = S->alloc_ms = 0;
+        S->t_dev = S->t_copy = S->t_pinned = S->t_mixed = 0;
     }
     return FNEC_OK;
 }

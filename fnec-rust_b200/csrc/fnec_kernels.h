@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <cstring>
 #include <vector>
 
 #include "fnec_math.cuh"
@@ -27,8 +28,23 @@ inline int set_smem_limit_once(K kernel, int bytes) {
 struct DevAlloc {
     cudaStream_t st;
     bool pooled;
+    // optional page-locked staging for uploads (a server lane's): copies go
+    // through it asynchronously instead of from pageable memory
+    unsigned char *stage = nullptr;
+    size_t stage_cap = 0;
+    size_t *stage_used = nullptr;
     cudaError_t alloc(void **p, size_t bytes) const {
         return pooled ? cudaMallocAsync(p, bytes, st) : cudaMalloc(p, bytes);
+    }
+    cudaError_t upload(void *dst, const void *src, size_t bytes) const {
+        if (bytes == 0) return cudaSuccess;
+        if (stage && stage_used && *stage_used + bytes <= stage_cap) {
+            unsigned char *s = stage + *stage_used;
+            std::memcpy(s, src, bytes);
+            *stage_used += (bytes + 255) / 256 * 256;
+            return cudaMemcpyAsync(dst, s, bytes, cudaMemcpyHostToDevice, st);
+        }
+        return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
     }
     void release(void *p) const {
         if (!p) return;

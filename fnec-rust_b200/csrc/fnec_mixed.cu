@@ -1522,8 +1522,8 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
             q += al(b_gu);
             w.tc_tiles = q;
             w.bytes += tot;
-            e = cudaMemcpyAsync(w.tc_gu, p->units.data(), b_gu, cudaMemcpyHostToDevice, dev.st);
-            if (e == cudaSuccess) e = cudaMemcpyAsync(w.tc_tiles, p->tiles.data(), b_t, cudaMemcpyHostToDevice, dev.st);
+            e = dev.upload(w.tc_gu, p->units.data(), b_gu);
+            if (e == cudaSuccess) e = dev.upload(w.tc_tiles, p->tiles.data(), b_t);
             if (e != cudaSuccess) {
                 delete p;
                 return e;
@@ -1538,9 +1538,9 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
             delete p;
         }
     }
-    e = cudaMemcpyAsync(w.mu, mu.data(), sizeof(MixedUnit) * mu.size(), cudaMemcpyHostToDevice, dev.st);
+    e = dev.upload(w.mu, mu.data(), sizeof(MixedUnit) * mu.size());
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(w.smu, sysmu.data(), sizeof(MixedUnit) * sysmu.size(), cudaMemcpyHostToDevice, dev.st);
+        e = dev.upload(w.smu, sysmu.data(), sizeof(MixedUnit) * sysmu.size());
     return e;
 }
 

@@ -17,6 +17,7 @@ antennas and frequencies in one device pipeline.
 from __future__ import annotations
 
 import atexit
+import time
 import ctypes
 import os
 import weakref
@@ -111,11 +112,18 @@ class _RequestInfo(ctypes.Structure):
                 ("n_points", _U32), ("pad", _U32), ("device_bytes", _U64)]
 
 
+class _RequestResult(ctypes.Structure):
+    _fields_ = [("currents", _P), ("cur_stride", _U64), ("feeds", _P), ("pattern", _P), ("status", _P),
+                ("n_solves", _U32), ("n_segments", _U32), ("n_feed_rows", _U32), ("n_points", _U32)]
+
+
 class _ServerStats(ctypes.Structure):
     _fields_ = [("submitted", _U64), ("completed", _U64), ("failed", _U64), ("solves", _U64), ("batches", _U64),
                 ("queued", _U64), ("in_flight_bytes", _U64), ("peak_in_flight_bytes", _U64), ("max_batch", _U64),
                 ("kernel_launches", _U64), ("h2d_bytes", _U64), ("d2h_bytes", _U64),
-                ("plan_ms", _D), ("launch_ms", _D), ("collect_ms", _D), ("p50_ms", _D), ("p99_ms", _D), ("mean_ms", _D), ("max_ms", _D)]
+                ("plan_ms", _D), ("launch_ms", _D), ("collect_ms", _D), ("alloc_ms", _D),
+                ("alloc_device_ms", _D), ("alloc_upload_ms", _D), ("alloc_pinned_ms", _D), ("alloc_mixed_ms", _D),
+                ("p50_ms", _D), ("p99_ms", _D), ("mean_ms", _D), ("max_ms", _D)]
 
 
 # name -> (restype, argtypes); every function declared in include/fnec_cuda.h
@@ -139,7 +147,10 @@ SIGNATURES = {
     "fnec_server_create": (ctypes.c_int, [_P, _P, _P]),
     "fnec_server_destroy": (ctypes.c_int, [_P]),
     "fnec_request_shape": (ctypes.c_int, [_P, _P, _I32, _P]),
-    "fnec_server_submit": (ctypes.c_int, [_P, _P, _P, _P]),
+    "fnec_server_submit": (ctypes.c_int, [_P, _P, _P, _P, _P]),
+    "fnec_server_result": (ctypes.c_int, [_P, _U64, _P]),
+    "fnec_server_next_done": (ctypes.c_int, [_P, _D, _P]),
+    "fnec_server_release": (ctypes.c_int, [_P, _U64]),
     "fnec_server_poll": (ctypes.c_int, [_P, _U64, _P, _P]),
     "fnec_server_wait": (ctypes.c_int, [_P, _U64, _D, _P, _P]),
     "fnec_server_stats": (ctypes.c_int, [_P, _P, _I32]),
@@ -669,34 +680,82 @@ class HallenBatch:
 REQ_QUEUED, REQ_RUNNING, REQ_DONE = 0, 1, 2
 
 
-class Request:
-    """One submitted request: its output arrays and, once done, its latency."""
+def _view(ptr, dtype, shape, strides=None):
+    """A numpy view of library-owned host memory (no copy)."""
+    dt = np.dtype(dtype)
+    if strides is None:
+        nbytes = int(np.prod(shape)) * dt.itemsize
+    else:
+        nbytes = sum((n - 1) * st for n, st in zip(shape, strides)) + dt.itemsize if all(shape) else 0
+    if nbytes == 0 or not ptr:
+        return np.zeros(shape, dt)
+    buf = (ctypes.c_char * nbytes).from_address(ptr)
+    return np.ndarray(shape, dt, buffer=buf, strides=strides)
 
-    def __init__(self, antenna, info, currents, feeds, pattern):
+
+class Request:
+    """One submitted request.  With copy_out its results are copied into
+    its own arrays (currents, feeds, pattern, status); otherwise they are
+    read in place from the server's page-locked memory (result()) until
+    release()."""
+
+    def __init__(self, server, antenna, copy_out, currents, feeds, pattern):
+        self.server = server
         self.antenna = antenna
-        self.info = info
-        self.n_solves = info.n_solves
-        self.currents = np.zeros((info.n_solves, info.n_segments), np.complex128) if currents else None
-        self.feeds = np.zeros((max(info.n_feed_rows, 1), 7), np.float64) if feeds else None
-        self.pattern = (np.zeros((info.n_solves, info.n_points, 6), np.float64)
-                        if (pattern and info.n_points) else None)
-        self.status = np.zeros(info.n_solves, np.int32)
+        self.copy_out = copy_out
+        self.info = _RequestInfo()
+        self.want = (currents, feeds, pattern)
+        self.currents = self.feeds = self.pattern = self.status = None
         self.ticket = None
         self.latency_ms = None
         self.state = REQ_QUEUED
         self._keep = []
 
+    def _alloc(self):
+        i = self.info
+        c, f, p = self.want
+        self.currents = np.zeros((i.n_solves, i.n_segments), np.complex128) if c else None
+        self.feeds = np.zeros((max(i.n_feed_rows, 1), 7), np.float64) if f else None
+        self.pattern = np.zeros((i.n_solves, i.n_points, 6), np.float64) if (p and i.n_points) else None
+        self.status = np.zeros(i.n_solves, np.int32)
+
+    @property
+    def n_solves(self):
+        return self.info.n_solves
+
+    def result(self):
+        """(currents, feeds, pattern, status) of a finished request; views of
+        server memory (valid until release) unless submitted with copy_out."""
+        if self.copy_out:
+            return self.currents, self.feeds, self.pattern, self.status
+        r = _RequestResult()
+        st = lib().fnec_server_result(self.server._h, self.ticket, ctypes.byref(r))
+        if st != 0:
+            raise AccelError(st, "server_result")
+        cur = _view(r.currents, np.complex128, (r.n_solves, r.n_segments), (16 * r.cur_stride, 16))
+        feeds = _view(r.feeds, np.float64, (r.n_feed_rows, 7))
+        pat = _view(r.pattern, np.float64, (r.n_solves, r.n_points, 6)) if r.n_points else None
+        status = _view(r.status, np.int32, (r.n_solves,))
+        return cur, feeds, pat, status
+
     def feed_z(self, solve: int = 0) -> complex:
         """Feedpoint impedance of a solve's first feed row (columns 5, 6)."""
-        rows_per = len(self.feeds) // max(self.n_solves, 1)
-        r = self.feeds[solve * rows_per]
+        feeds = self.result()[1]
+        rows_per = len(feeds) // max(self.n_solves, 1)
+        r = feeds[solve * rows_per]
         return complex(r[5], r[6])
+
+    def release(self):
+        if self.ticket is not None and self.server._h:
+            lib().fnec_server_release(self.server._h, self.ticket)
+            self.server._pending.pop(self.ticket, None)
+        self.ticket = None
 
 
 class Server:
     """Continuous-batching solve server (fnec_server_*): submit decks as they
-    arrive; a host thread admits them by HBM budget onto `lanes` concurrent
-    streams and delivers each request's results into its arrays."""
+    arrive; lanes (each a CUDA stream with its own host thread) admit them by
+    HBM budget and deliver each request's results."""
 
     def __init__(self, precision: int = PRECISION_MIXED, lanes: int = 2, hbm_budget_bytes: int = 32 << 30,
                  max_batch: int = 64, queue_cap: int = 0, ctx: Optional[Context] = None):
@@ -718,25 +777,33 @@ class Server:
                                                 ctypes.byref(info)), "request_shape")
         return info
 
-    def submit(self, antenna, currents: bool = True, feeds: bool = True, pattern: bool = True) -> Request:
+    def submit(self, antenna, copy_out: bool = False, currents: bool = True, feeds: bool = True,
+               pattern: bool = True, tag=None) -> Request:
+        """Queue a deck; `tag` is kept on the Request (e.g. the caller's index)."""
         keep = []
         a = _antenna_struct(antenna, keep)
-        req = Request(antenna, self.shape(antenna), currents, feeds, pattern)
+        req = Request(self, antenna, copy_out, currents, feeds, pattern)
+        req.tag = tag
         req._keep = keep
-        out = _RequestOut(_ptr(req.currents), _ptr(req.feeds), _ptr(req.pattern), _ptr(req.status))
+        out = None
+        if copy_out:
+            self.ctx.check(lib().fnec_request_shape(self.ctx.handle, ctypes.byref(a), self.precision,
+                                                    ctypes.byref(req.info)), "request_shape")
+            req._alloc()
+            out = _RequestOut(_ptr(req.currents), _ptr(req.feeds), _ptr(req.pattern), _ptr(req.status))
         t = ctypes.c_uint64()
-        st = lib().fnec_server_submit(self._h, ctypes.byref(a), ctypes.byref(out), ctypes.byref(t))
+        st = lib().fnec_server_submit(self._h, ctypes.byref(a), ctypes.byref(out) if out is not None else None,
+                                      ctypes.byref(t), ctypes.byref(req.info))
         if st != 0:
             raise AccelError(st, "server_submit")
         req.ticket = t.value
-        self._pending[req.ticket] = req  # keeps the output arrays alive until done
+        self._pending[req.ticket] = req  # keeps output arrays alive until released
         return req
 
     def _finish(self, req, state, lat):
         req.state = state
         if state == REQ_DONE or state < 0:
             req.latency_ms = lat
-            self._pending.pop(req.ticket, None)
         if state < 0:
             msg = lib().fnec_server_last_error(self._h)
             raise AccelError(state, f"request failed: {msg.decode() if msg else ''}")
@@ -761,6 +828,25 @@ class Server:
         self._finish(req, state.value, lat.value)
         return req
 
+    def next_done(self, timeout_ms: float = 1000.0) -> Optional[Request]:
+        """The next finished request in completion order (None on timeout)."""
+        t = ctypes.c_uint64()
+        st = lib().fnec_server_next_done(self._h, float(timeout_ms), ctypes.byref(t))
+        if st == ERR_TIMEOUT:
+            return None
+        if st != 0:
+            raise AccelError(st, "server_next_done")
+        req = self._pending.get(t.value)
+        t_end = time.monotonic() + 1.0
+        while req is None and time.monotonic() < t_end:  # its submit() is still returning
+            time.sleep(0)
+            req = self._pending.get(t.value)
+        if req is not None:
+            state, lat = ctypes.c_int32(), ctypes.c_double()
+            lib().fnec_server_poll(self._h, req.ticket, ctypes.byref(state), ctypes.byref(lat))
+            self._finish(req, state.value, lat.value)
+        return req
+
     def stats(self, reset: bool = False) -> dict:
         s = _ServerStats()
         self.ctx.check(lib().fnec_server_stats(self._h, ctypes.byref(s), int(reset)), "server_stats")
@@ -770,6 +856,7 @@ class Server:
         if getattr(self, "_h", None):
             lib().fnec_server_destroy(self._h)  # finishes queued and running requests
             self._h = None
+            self._pending.clear()
 
     def __enter__(self):
         return self

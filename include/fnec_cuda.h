@@ -261,14 +261,17 @@ int fnec_measure_fp64_peak(int device, double *fma_tflops, double *muladd_tflops
  * per frequency).  A server owns `lanes` CUDA streams and a host thread:
  * submitted requests (one fnec_antenna deck each; every voltage source a
  * separate right-hand side when separate_sources is set) queue in arrival
- * order; whenever a lane is free the thread admits queued requests while the
- * device bytes of the batches in flight (each request's admission estimate,
- * fnec_request_info.device_bytes) stay within hbm_budget_bytes, solves them
- * as one batch -- Z and its factor stay on the device for all of a request's
- * right-hand sides and its pattern -- and copies the results into the
- * request's output arrays.  Requests arriving while batches run are admitted
- * as lanes and memory free up; the lanes' kernels overlap on the device.
- * With more than one lane the grid-wide (cooperative) kernels are not used. */
+ * order; whenever a lane (each driven by its own host thread) is free it
+ * admits queued requests while the device bytes of the batches in flight
+ * (each request's admission estimate, fnec_request_info.device_bytes) stay
+ * within hbm_budget_bytes, solves them as one batch -- Z and its factor stay
+ * on the device for all of a request's right-hand sides and its pattern --
+ * and delivers the results: copied into the request's output arrays when it
+ * gave some, else readable in place in the server's page-locked memory
+ * (fnec_server_result) until fnec_server_release.  Requests arriving while
+ * batches run are admitted as lanes and memory free up; the lanes' planning,
+ * kernels and copies overlap.  With more than one lane the grid-wide
+ * (cooperative) kernels are not used. */
 typedef struct fnec_server fnec_server;
 
 typedef struct {
@@ -307,8 +310,10 @@ typedef struct {
     uint64_t max_batch;       /* largest batch formed                      */
     uint64_t kernel_launches; /* kernels launched for the completed batches */
     uint64_t h2d_bytes, d2h_bytes; /* host <-> device bytes of those batches */
-    double plan_ms, launch_ms, collect_ms; /* the loop thread's host time: batch planning,
+    double plan_ms, launch_ms, collect_ms; /* the lanes' host time: batch planning,
                                               enqueueing, result delivery */
+    double alloc_ms;                       /* of plan_ms: allocations          */
+    double alloc_device_ms, alloc_upload_ms, alloc_pinned_ms, alloc_mixed_ms; /* its parts */
     double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> results delivered */
 } fnec_server_stats_t;
 
@@ -322,13 +327,38 @@ int fnec_server_destroy(fnec_server *s);
 /* Output sizes and admission footprint of a request (host planning only). */
 int fnec_request_shape(fnec_ctx *ctx, const fnec_antenna *req, int32_t precision, fnec_request_info *out);
 /* Queue a request; BUSY when the queue is full, TOO_LARGE when it alone
- * exceeds the budget.  The deck is copied; the output arrays must stay
- * valid until the request is done. */
-int fnec_server_submit(fnec_server *s, const fnec_antenna *req, const fnec_request_out *out, uint64_t *ticket);
-/* state: FNEC_REQ_* or a negative error; a finished request (done or
- * failed) is released by the call that reports it. */
+ * exceeds the budget.  The deck is copied.  out (may be NULL): output
+ * arrays, which must stay valid until the request is done.  info (may be
+ * NULL) receives the request's shape. */
+int fnec_server_submit(fnec_server *s, const fnec_antenna *req, const fnec_request_out *out, uint64_t *ticket,
+                       fnec_request_info *info);
+/* state: FNEC_REQ_* or a negative error. */
 int fnec_server_poll(fnec_server *s, uint64_t ticket, int32_t *state, double *latency_ms);
 int fnec_server_wait(fnec_server *s, uint64_t ticket, double timeout_ms, int32_t *state, double *latency_ms);
+
+/* The next finished request (done or failed) in completion order; each
+ * finished request not yet released is reported once here, whatever
+ * poll/wait also saw. */
+int fnec_server_next_done(fnec_server *s, double timeout_ms, uint64_t *ticket);
+
+/* A finished request's results, in place in the server's page-locked
+ * memory (NULL arrays when it was submitted with output arrays, or failed);
+ * valid until fnec_server_release.  Solve k's currents start at
+ * currents + 2 * k * cur_stride doubles (n_segments complex values). */
+typedef struct {
+    const double *currents;
+    uint64_t cur_stride;
+    const double *feeds;   /* n_feed_rows x 7  */
+    const double *pattern; /* n_solves x n_points x 6 */
+    const int32_t *status; /* n_solves         */
+    uint32_t n_solves, n_segments, n_feed_rows, n_points;
+} fnec_request_result;
+int fnec_server_result(fnec_server *s, uint64_t ticket, fnec_request_result *out);
+/* Forget a finished request (BUSY while it runs); its in-place results go.
+ * Requests read in place hold their batch's result slab: a server keeps at
+ * most lanes + 4 slabs (allocated up front), so lanes wait for releases when
+ * all are held. */
+int fnec_server_release(fnec_server *s, uint64_t ticket);
 /* The server's most recent failure (valid until the next call). */
 const char *fnec_server_last_error(fnec_server *s);
 /* Latency percentiles over completed requests since the last reset. */
