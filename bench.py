@@ -215,6 +215,97 @@ def algorithmic_flops(n, s, n_dir):
     }
 
 
+FILL_FLOPS_PER_SAMPLE = 60.0  # one G(R) sample: sqrt + sincos + 2 divisions + ~26 add/mul, in FP64 ops
+SINCOS_FLOPS = 40.0           # one FP64 sincos, in FP64 ops
+
+
+def measured_peaks():
+    """HBM copy bandwidth and dense BF16 tensor throughput measured on this
+    pool's B200s (MEASURED_PEAKS.json beside this file); TF32 tensor
+    throughput is half the BF16 rate."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            m = json.load(fh)
+        hbm = float(m.get("hbm_gbs"))
+        bf16 = float(m.get("bf16_tflops"))
+        src = "MEASURED_PEAKS.json"
+    except Exception:
+        hbm, bf16, src = 6650.0, 1590.0, "fallback (no MEASURED_PEAKS.json)"
+    return {"hbm_gbs": hbm, "bf16_tflops": bf16, "tf32_tflops": bf16 / 2.0, "source": src}
+
+
+def ff_directions(ground, rp):
+    """Far-field directions evaluated per solve: the power-integration grid
+    plus the requested points that do not coincide with one of its
+    directions (theta 0, the last theta row, phi >= 360 are evaluated on
+    their own)."""
+    n_th, th_max = (91, 90.0) if ground == 1 else (181, 180.0)
+    n_int = n_th * 360
+    if rp is None:
+        return n_int
+    nt, nph, t0, p0, dt, dp = rp
+    th = t0 + np.arange(nt) * dt
+    ph = p0 + np.arange(nph) * dp
+    step = th_max / (n_th - 1)
+    on_t = (np.abs(th / step - np.round(th / step)) < 1e-12) & (th >= step) & (th <= th_max - step)
+    if ground == 1:
+        on_t &= th <= 90.0
+    on_p = (np.abs(ph - np.round(ph)) < 1e-12) & (ph >= 0) & (ph < 360)
+    below = (th > 90.0).sum() * nph if ground == 1 else 0
+    return n_int + nt * nph - int(on_t.sum()) * int(on_p.sum()) - int(below)
+
+
+def phase_rooflines(form, o, n, s, g, d, shapes, fma, muladd, ffma, peaks, runs):
+    """Achieved rate and fraction of the measured peak of every phase.
+    Work models (per unit): fill 60 FP64 ops per G(R) sample (8 N^2 - 4 N
+    samples, doubled over GN 1); Gram 8 N^2 (N+1) flops (plain) or the
+    3xTF32 tensor-core flops issued on the upper-triangle 128x128 tiles
+    (mixed); factor (8/3) S^3 flops; solve: plain back substitution 8 S^2
+    flops on a serial chain, mixed GMRES HBM bytes (iterations + 2) x
+    (32 N^2 + 8 S^2) (FP64 Z read twice, FP32 factor once per apply); far
+    field 8 N flops per direction plus 2 sincos per (direction, wire run)."""
+    ph = o["phase"]
+    exact = form == "fp64"
+    samples = float(np.sum((8 * n * n - 4 * n) * (1 + g)))
+    res = {}
+
+    def put(k, achieved, peak, unit, bound, src):
+        ms = ph.get(k, 0.0)
+        if not ms:
+            res[k] = {"bound": bound, "achieved": None, "peak": peak, "unit": unit, "frac": None, "peak_source": src}
+            return
+        a = achieved / (ms * 1e-3)
+        res[k] = {"bound": bound, "achieved": a, "peak": peak, "unit": unit, "frac": a / peak, "peak_source": src}
+
+    p64 = (muladd, "DMUL+DADD measured by fnec_measure_fp64_peak (the exact path issues no FMA)") if exact else \
+          (fma, "DFMA measured by fnec_measure_fp64_peak")
+    put("fill", samples * FILL_FLOPS_PER_SAMPLE / 1e12, p64[0], "TFLOP/s", "fp64", p64[1])
+    if exact:
+        put("gram", float(np.sum(8 * n * n * (n + 1))) / 1e12, muladd, "TFLOP/s", "fp64", p64[1])
+        put("factor", float(np.sum(8 * s ** 3 / 3)) / 1e12, muladd, "TFLOP/s", "fp64", p64[1])
+        put("solve", float(np.sum(8 * s * s)) / 1e12, muladd, "TFLOP/s", "latency (serial chain)", p64[1])
+    else:
+        kb = np.ceil(n / 32)
+        nt = np.ceil(2 * n / 128)
+        tc = float(np.sum(nt * (nt + 1) / 2 * 128 * 128 * kb * 32 * 2 * 3))
+        put("gram", tc / 1e12, peaks["tf32_tflops"], "TFLOP/s", "tensor (tf32)",
+            "half the BF16 rate of " + peaks["source"])
+        put("factor", float(np.sum(8 * s ** 3 / 3)) / 1e12, ffma, "TFLOP/s", "fp32",
+            "FFMA measured by fnec_measure_fp32_peak")
+        it = o.get("gmres_iters")
+        n_s = np.array([u["n"] for u in shapes], np.float64)
+        s_s = np.array([u["s"] for u in shapes], np.float64)
+        its = it if it is not None and len(it) == len(n_s) else np.full(len(n_s), 5.0)
+        byt = float(np.sum((its + 2) * (32 * n_s * n_s + 8 * s_s * s_s)))
+        put("solve", byt / 1e9, peaks["hbm_gbs"], "GB/s", "hbm", peaks["source"])
+    dd = np.asarray(d, np.float64)
+    nr = np.asarray(runs, np.float64)
+    put("farfield", float(np.sum(dd * (8 * n + 2 * SINCOS_FLOPS * nr))) / 1e12, fma, "TFLOP/s", "fp64",
+        "DFMA measured by fnec_measure_fp64_peak")
+    return res
+
+
 def clock_sampler(device: int):
     q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -601,36 +692,27 @@ def main():
             it, rs = batch.refinement_stats()
             out[form]["gmres"] = {"iters_mean": float(it.mean()), "iters_max": int(it.max()),
                                   "resid_max": float(rs.max())}
+            out[form]["gmres_iters"] = it.astype(np.float64)
         batch.close()
 
     if rank == 0:
         fma_tf, muladd_tf = acc.measure_fp64_peak(local)
-        n_u = [u["n"] for u in shapes]
-        s_u = [u["s"] for u in shapes]
-        d_u = [(0 if u["n_points"] == 0 else (181 * 360 if ref_units[i][2] == 0 else 91 * 360) + u["n_points"])
-               for i, u in enumerate(shapes)]
+        ffma_tf = acc.measure_fp32_peak(local)
+        peaks = measured_peaks()
+        n_u = np.array([u["n"] for u in shapes], np.float64)
+        s_u = np.array([u["s"] for u in shapes], np.float64)
+        g_u = np.array([ref_units[i][2] if i < len(ref_units) else 0 for i in range(len(shapes))], np.float64)
+        d_u = [ff_directions(ref_units[i][2], ref_units[i][4]) if u["n_points"] else 0 for i, u in enumerate(shapes)]
         flops = algorithmic_flops(n_u, s_u, d_u)
+        w_u = [len(ref_units[i][0]) if i < len(ref_units) else 1 for i in range(len(shapes))]
+        rr = {form: phase_rooflines(form, out[form], n_u, s_u, g_u, d_u, shapes, fma_tf, muladd_tf, ffma_tf, peaks,
+                                    w_u) for form in forms}
         head = out[forms[0]]
         phase = head["phase"]
         dom = max(("fill", "gram", "factor", "solve", "farfield"), key=lambda k: phase[k])
-        dom_ms = phase[dom]
-        if dom in ("gram", "factor") and forms[0] == "fp64":
-            achieved = flops[dom] / (dom_ms * 1e-3) / 1e12
-            peak = muladd_tf if dom in ("gram", "factor") else fma_tf
-            roof = {"kernel": dom, "bound": "fp64", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": achieved / peak, "traffic": None,
-                    "peak_source": "measured in this run by fnec_measure_fp64_peak ("
-                                   + ("DMUL+DADD, the exact path issues no FMA" if peak == muladd_tf else "DFMA")
-                                   + "); MEASURED_PEAKS.json holds no FP64 figure"}
-        elif dom == "farfield":
-            achieved = flops["farfield"] / (dom_ms * 1e-3) / 1e12
-            roof = {"kernel": "farfield", "bound": "fp64", "achieved": achieved, "peak": fma_tf,
-                    "unit": "TFLOP/s", "frac": achieved / fma_tf, "traffic": None,
-                    "peak_source": "measured in this run by fnec_measure_fp64_peak (DFMA); MEASURED_PEAKS.json "
-                                   "holds no FP64 figure"}
-        else:
-            roof = {"kernel": dom, "bound": "fp64", "achieved": None, "peak": fma_tf, "unit": "TFLOP/s",
-                    "frac": None, "traffic": None, "note": "see phase_ms"}
+        roof = dict(rr[forms[0]][dom])
+        roof["kernel"] = dom
+        roof["traffic"] = None
         samples = flops["fill_samples"]
         # accuracy of the chosen form against the plain FP64 GPU path (all units)
         gate = None
@@ -667,7 +749,9 @@ def main():
             "phase_ms": {k: round(v, 4) for k, v in phase.items()},
             "phase_detail": {"fill_gsamples_per_s": samples / (phase["fill"] * 1e-3) / 1e9
                              if phase["fill"] else None,
-                             "fp64_peak_tflops": {"dfma": fma_tf, "dmul_dadd": muladd_tf}},
+                             "measured_peaks": {"fp64_dfma_tflops": fma_tf, "fp64_dmul_dadd_tflops": muladd_tf,
+                                                "fp32_ffma_tflops": ffma_tf, **peaks}},
+            "phase_rooflines": rr,
             "clocks": head["clocks"],
         }
         for form in forms:

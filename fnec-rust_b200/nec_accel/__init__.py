@@ -143,6 +143,7 @@ SIGNATURES = {
     "fnec_enumerate_devices": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_char_p, _U64]),
     "fnec_dispatch_frequency_point": (ctypes.c_int, [ctypes.c_int, _D]),
     "fnec_measure_fp64_peak": (ctypes.c_int, [ctypes.c_int, _P, _P]),
+    "fnec_measure_fp32_peak": (ctypes.c_int, [ctypes.c_int, _P]),
     "fnec_host_alloc": (ctypes.c_int, [ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p)]),
     "fnec_server_create": (ctypes.c_int, [_P, _P, _P]),
     "fnec_server_destroy": (ctypes.c_int, [_P]),
@@ -453,6 +454,15 @@ def selftest_tf32x3_gemm(a: np.ndarray, b: np.ndarray, device: int = 0) -> np.nd
     if st != 0:
         raise AccelError(st, "selftest_tf32x3_gemm")
     return c
+
+
+def measure_fp32_peak(device: int = 0) -> float:
+    """FP32 FFMA throughput of the GPU in TFLOP/s."""
+    a = ctypes.c_double()
+    st = lib().fnec_measure_fp32_peak(device, ctypes.byref(a))
+    if st != 0:
+        raise AccelError(st, "measure_fp32_peak")
+    return a.value
 
 
 def measure_fp64_peak(device: int = 0):

@@ -255,6 +255,9 @@ int fnec_dispatch_frequency_point(int request_kind, double freq_hz);
  * DFMA and separately rounded DMUL+DADD throughput in TFLOP/s, used as the
  * roofline denominators of the FP64-bound kernels. */
 int fnec_measure_fp64_peak(int device, double *fma_tflops, double *muladd_tflops);
+/* FP32 FFMA throughput in TFLOP/s (no counterpart in the reference): the
+ * roofline denominator of the mixed form's FP32 factorisation. */
+int fnec_measure_fp32_peak(int device, double *ffma_tflops);
 
 /* ---- serving: continuous batching of solve requests -------------------
  * No counterpart in the reference (its sweep loop calls the backend once
