@@ -256,6 +256,20 @@ def ff_directions(ground, rp):
     return n_int + nt * nph - int(on_t.sum()) * int(on_p.sum()) - int(below)
 
 
+def dram_traffic(phase, form, units):
+    """DRAM bytes of one run of a phase, scaled by units from the per-unit
+    figure of an ncu capture committed under profiles/ (None if none)."""
+    key = {("solve", "mixed"): "solve_mixed", ("farfield", "mixed"): "farfield", ("farfield", "fp64"): "farfield",
+           ("fill", "fp64"): "fill_fp64"}.get((phase, form))
+    try:
+        with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "traffic.json")) as fh:
+            t = json.load(fh)
+        e = t[key]
+        return float(e["bytes_per_unit"]) * units, "profiles/" + e["capture"]
+    except Exception:
+        return None, None
+
+
 def phase_rooflines(form, o, n, s, g, d, shapes, fma, muladd, ffma, peaks, runs):
     """Achieved rate and fraction of the measured peak of every phase.
     Work models (per unit): fill 60 FP64 ops per G(R) sample (8 N^2 - 4 N
@@ -712,7 +726,7 @@ def main():
         dom = max(("fill", "gram", "factor", "solve", "farfield"), key=lambda k: phase[k])
         roof = dict(rr[forms[0]][dom])
         roof["kernel"] = dom
-        roof["traffic"] = None
+        roof["traffic"], roof["traffic_source"] = dram_traffic(dom, forms[0], units)
         samples = flops["fill_samples"]
         # accuracy of the chosen form against the plain FP64 GPU path (all units)
         gate = None
