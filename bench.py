@@ -590,6 +590,9 @@ def main():
     ap.add_argument("--budget-gb", type=float, default=64.0, help="serve: HBM budget of the batches in flight")
     ap.add_argument("--cells", type=int, default=46, help="mesh workload size (cells per side)")
     ap.add_argument("--antennas", type=int, default=4096, help="uneven workload size")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="skip the autotuner (default schedule; the pipeline is still graph-captured)")
+    ap.add_argument("--tune-reps", type=int, default=2, help="timed runs per candidate schedule")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -701,7 +704,15 @@ def main():
         prec = acc.PRECISION_MIXED if form == "mixed" else acc.PRECISION_FP64
         batch = acc.HallenBatch(ants, precision=prec, ctx=ctx)
         shapes = batch.units
+        # schedule: the autotuner's pick (timed before, outside the timed region)
+        tune = None if args.no_tune else batch.tune(reps=args.tune_reps)
         out[form] = measure(batch, with_clocks=(form == forms[0]))
+        st, nodes = batch.graph_state()
+        out[form]["schedule"] = {"schedule": batch.schedule,
+                                 "graph": {1: "replayed", 0: "eager", -1: "capture refused"}[st],
+                                 "graph_kernels": nodes}
+        if tune is not None:
+            out[form]["schedule"]["tune"] = {k: tune[k] for k in ("candidates", "default_ms", "best_ms", "key")}
         if form == "mixed":
             it, rs = batch.refinement_stats()
             out[form]["gmres"] = {"iters_mean": float(it.mean()), "iters_max": int(it.max()),
@@ -776,6 +787,7 @@ def main():
                                     "phase_ms": {k: round(v, 4) for k, v in o["phase"].items()}}
             if "gmres" in o:
                 line[f"form_{form}"]["gmres"] = o["gmres"]
+            line[f"form_{form}"]["schedule"] = o["schedule"]
         if gate is not None:
             line["mixed_gate"] = gate
             line["mixed_vs_fp64"] = line["form_mixed"]["value"] / line["form_fp64"]["value"]

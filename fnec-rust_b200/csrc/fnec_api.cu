@@ -15,6 +15,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -119,6 +120,12 @@ struct HostAnt {
     bool rhs_given = false;         // caller supplies rhs/cos (one unit)
     std::vector<double> rhs, cosv;  // 2n, n
     std::vector<double> z;          // caller-supplied Z (2 n^2), else filled on the device
+    // degree-2 conductor-path form (solve_session.rs:1338-1378)
+    bool paths = false;
+    std::vector<int32_t> path_of;   // column (path) of each row
+    std::vector<double> arc;        // 2n: signed arc length of each midpoint, then its sign
+    std::vector<int64_t> free_ends; // 2 per path: I = 0 rows
+    int64_t cols() const { return paths ? (int64_t)free_ends.size() / 2 : (int64_t)ep.size(); }
 };
 
 }  // namespace
@@ -189,6 +196,103 @@ static void cli_junctions(const std::vector<DevSeg> &s,
             h.js.push_back(st_i == st_j ? 1.0 : -1.0);
         }
     }
+}
+
+// geometry.rs:404-584 (build_conductor_paths) and the guard of
+// solve_session.rs:1338-1340: the per-tag wires are joined through
+// endpoint nodes where exactly two ends meet (within 1e-6 m) into open
+// chains.  Returns true -- and fills the path form of h -- only when every
+// node has degree <= 2, no chain is closed, and some chain is not a plain
+// forward run of ascending segments; otherwise h is left as it was.
+static bool conductor_paths(HostAnt &h) {
+    const auto &s = h.segs;
+    const auto wires = wire_endpoints(s);
+    const int64_t nw = (int64_t)wires.size(), n = (int64_t)s.size();
+    if (nw == 0) return false;
+    auto point = [&](int64_t id) -> const double * {  // endpoint id = 2 wire + (0 start, 1 end)
+        return id % 2 == 0 ? s[wires[id / 2].first].start : s[wires[id / 2].second].end;
+    };
+    // nodes: coincident endpoints, numbered in order of their first endpoint
+    std::vector<int64_t> node(2 * nw, -1);
+    std::vector<std::vector<int64_t>> members;
+    for (int64_t id = 0; id < 2 * nw; ++id) {
+        if (node[id] >= 0) continue;
+        node[id] = (int64_t)members.size();
+        members.push_back({id});
+        for (int64_t j = 0; j < 2 * nw; ++j)
+            if (node[j] < 0 && dist2(point(id), point(j)) < 1e-6 * 1e-6) {
+                node[j] = node[id];
+                members.back().push_back(j);
+            }
+    }
+    std::vector<int64_t> up(nw);
+    for (int64_t i = 0; i < nw; ++i) up[i] = i;
+    auto root = [&](int64_t x) {
+        while (up[x] != x) x = up[x];
+        return x;
+    };
+    for (auto &m : members) {
+        if (m.size() >= 3) return false;  // T/Y junction
+        if (m.size() == 2) {
+            if (m[0] / 2 == m[1] / 2) return false;  // a wire closed on itself
+            up[root(m[0] / 2)] = root(m[1] / 2);
+        }
+    }
+    std::vector<int32_t> path_of(n, 0);
+    std::vector<double> smid(n, 0.0), sgn(n, 1.0);
+    std::vector<int64_t> fends;
+    std::vector<char> seen(nw, 0);
+    bool nontrivial = false;
+    int32_t np = 0;
+    std::vector<int64_t> roots(nw);
+    for (int64_t i = 0; i < nw; ++i) roots[i] = root(i);
+    for (int64_t r = 0; r < nw; ++r) {  // chains in ascending order of their root wire
+        std::vector<int64_t> ends;
+        for (int64_t wi = 0; wi < nw; ++wi)
+            if (roots[wi] == r)
+                for (int e = 0; e < 2; ++e)
+                    if (members[node[2 * wi + e]].size() == 1) ends.push_back(2 * wi + e);
+        bool any = false;
+        for (int64_t wi = 0; wi < nw && !any; ++wi) any = roots[wi] == r;
+        if (!any) continue;
+        if (ends.size() != 2) return false;  // a closed chain
+        std::vector<int64_t> order;
+        double arc = 0.0;
+        int64_t cur = ends[0] / 2, enter = ends[0] % 2;
+        for (;;) {
+            seen[cur] = 1;
+            const double sg = enter == 0 ? 1.0 : -1.0;
+            const int64_t f = wires[cur].first, l = wires[cur].second;
+            for (int64_t t = 0; t <= l - f; ++t) {
+                const int64_t m = enter == 0 ? f + t : l - t;
+                if (sg != 1.0 || (!order.empty() && m != order.back() + 1)) nontrivial = true;
+                smid[m] = arc + s[m].len * 0.5;
+                arc += s[m].len;
+                sgn[m] = sg;
+                path_of[m] = np;
+                order.push_back(m);
+            }
+            const auto &at = members[node[2 * cur + (1 - enter)]];
+            if (at.size() == 1) break;
+            int64_t next = -1;
+            for (int64_t id : at)
+                if (id / 2 != cur && !seen[id / 2]) next = id;
+            if (next < 0) break;
+            cur = next / 2;
+            enter = next % 2;
+        }
+        for (int64_t m : order) smid[m] = smid[m] - arc * 0.5;
+        fends.push_back(order.front());
+        fends.push_back(order.back());
+        ++np;
+    }
+    if (!nontrivial) return false;
+    h.paths = true;
+    h.path_of = std::move(path_of);
+    h.arc.assign(smid.begin(), smid.end());
+    h.arc.insert(h.arc.end(), sgn.begin(), sgn.end());
+    h.free_ends = std::move(fends);
+    return true;
 }
 
 static int64_t find_seg(const std::vector<DevSeg> &s, uint32_t tag, uint32_t idx) {
@@ -286,6 +390,35 @@ static int resolve_sources(HostAnt &h, const fnec_source *src, uint32_t ns, bool
                   std::to_string(src[e].segment);
             return FNEC_ERR_SEGMENT_NOT_FOUND;
         }
+    }
+    if (h.paths) {
+        // excitation.rs:303-333: every voltage card, in deck order, drives
+        // its own path (no per-tag merging); feed rows as in the plain form
+        std::vector<DevSource> all;
+        for (uint32_t e = 0; e < ns; ++e) {
+            DevSource d{};
+            d.feed = (int32_t)idx[e];
+            d.comp_first = d.comp_last = -1;
+            d.v_re = src[e].v_re;
+            d.v_im = src[e].v_im;
+            all.push_back(d);
+        }
+        std::vector<DevSource> none;
+        if (ns == 0 || !separate) {
+            h.rhs_srcs.assign(1, all);
+            h.rhs_feeds.assign(1, {});
+            if (ns > 0) superposed_rhs(h, idx, src, ns, none, h.rhs_feeds[0]);
+            return FNEC_OK;
+        }
+        h.rhs_srcs.assign(ns, {});
+        h.rhs_feeds.assign(ns, {});
+        for (uint32_t e = 0; e < ns; ++e) {
+            h.rhs_srcs[e] = {all[e]};
+            std::vector<int64_t> one = {idx[e]};
+            superposed_rhs(h, one, &src[e], 1, none, h.rhs_feeds[e]);
+            none.clear();
+        }
+        return FNEC_OK;
     }
     if (ns == 0 || !separate) {
         h.rhs_srcs.assign(1, {});
@@ -401,6 +534,13 @@ struct fnec_batch {
     bool profile = false;
     cudaEvent_t ev[FNEC_N_PHASES + 1] = {};
     bool ev_made = false;
+    // schedule and its CUDA graph
+    fnec_schedule sched = {1, 1, 1, 1, 1, 1};
+    cudaGraphExec_t gexec = nullptr;
+    int graph_state = FNEC_GRAPH_NONE;
+    uint64_t graph_launches = 0;  // launches the graph replays
+    uint64_t n_runs = 0;  // fnec_batch_run calls
+    std::string graph_why;        // why capture was refused
 };
 
 template <typename T>
@@ -440,6 +580,8 @@ static void free_batch(fnec_batch *b) {
         if (b->h_out) cudaFreeHost(b->h_out);
     }
     b->h_in = b->h_out = nullptr;
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
     if (b->ev_made)
         for (auto &e : b->ev) cudaEventDestroy(e);
     b->ev_made = false;
@@ -528,6 +670,10 @@ struct PinnedArena {
         cap = 0;
     }
 };
+extern "C" {
+static void schedule_from_cache(fnec_batch *b);  // defined with the C API below
+}
+
 struct BatchPlace {
     cudaStream_t st = nullptr;  // null: the context's stream
     bool pooled = false;
@@ -557,7 +703,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
         AntDesc a{};
         a.seg_off = b->tot_seg;
         a.n = (int32_t)h.segs.size();
-        a.w = (int32_t)h.ep.size();
+        a.w = (int32_t)h.cols();
         a.ground = h.ground;
         int n = a.n;
         // wires
@@ -570,9 +716,10 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
         std::vector<int32_t> row_wire(n, 0);
         for (size_t q = 0; q < h.ep.size(); ++q)
             for (int64_t r = h.ep[q].first; r <= h.ep[q].second; ++r) row_wire[r] = (int32_t)q;
+        if (h.paths) row_wire = h.path_of;  // linear.rs:851-856: one column per path
         a.rowwire_off = (int64_t)b->ibuf.size();
         b->ibuf.insert(b->ibuf.end(), row_wire.begin(), row_wire.end());
-        std::vector<std::vector<int32_t>> rows_of(h.ep.size());
+        std::vector<std::vector<int32_t>> rows_of(a.w);
         for (int r = 0; r < n; ++r) rows_of[row_wire[r]].push_back(r);
         a.wptr_off = (int64_t)b->ibuf.size();
         int32_t acc = 0;
@@ -602,6 +749,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
             if (!injunc[e.first]) crow.push_back({{e.first, 1.0}});
             if (!injunc[e.second]) crow.push_back({{e.second, 1.0}});
         }
+        for (int64_t fe : h.free_ends) crow.push_back({{fe, 1.0}});  // linear.rs:859-864 (path form)
         for (size_t t = 0; t < h.ja.size(); ++t) {
             if (h.ja[t] == h.jb[t]) crow.push_back({{h.jb[t], h.js[t]}});
             else crow.push_back({{h.ja[t], 1.0}, {h.jb[t], h.js[t]}});
@@ -717,6 +865,11 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
         ff_req_max = std::max(ff_req_max, n_req);
         ff_int_max = std::max(ff_int_max, n_int);
         smem_max = std::max(smem_max, sizeof(DevRun) * h.runs.size() + sizeof(cx) * (size_t)n);
+        if (h.paths) {
+            a.paths = 1;
+            a.arc_off = (int64_t)b->pts.size();  // 2n doubles (n arc lengths, n signs): pairs stay aligned
+            b->pts.insert(b->pts.end(), h.arc.begin(), h.arc.end());
+        }
         b->ants.push_back(a);
         b->max_w = std::max(b->max_w, (int)a.w);
         // systems (one per frequency) and their solves (one per right-hand side)
@@ -917,6 +1070,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
                     std::string("batch allocation: ") + cudaGetErrorString(e));
     }
     *out = b;
+    schedule_from_cache(b);
     int st = fnec_batch_upload(b);
     if (st != FNEC_OK) {
         free_batch(b);
@@ -969,9 +1123,11 @@ static int antenna_from_cards(const fnec_antenna &A, HostAnt &h, std::string &wh
         off += gw.segments;
     }
     auto merged = merge_collinear(h.segs);
-    h.ep = merged;
     set_comp(h, merged);
-    cli_junctions(h.segs, merged, h);
+    if (!conductor_paths(h)) {  // the standard branch (solve_session.rs:1379-1400)
+        h.ep = merged;
+        cli_junctions(h.segs, merged, h);
+    }
     int st = resolve_sources(h, A.sources, A.n_sources, A.separate_sources != 0, why);
     if (st != FNEC_OK) return st;
     build_runs(h);
@@ -1096,10 +1252,10 @@ int fnec_batch_upload(fnec_batch *b) {
     return FNEC_OK;
 }
 
-int fnec_batch_run(fnec_batch *b) {
-    if (!b) return FNEC_ERR_BAD_ARG;
+// Enqueue the pipeline's launches on the batch stream (eagerly, or into
+// the graph being captured on it).
+static int run_pipeline(fnec_batch *b) {
     fnec_ctx *ctx = b->ctx;
-    cudaSetDevice(ctx->device);
     cudaStream_t st = b->st;
     int nu = (int)b->units.size();
     int ns = (int)b->solves.size();
@@ -1129,7 +1285,7 @@ int fnec_batch_run(fnec_batch *b) {
     if (!b->rhs_given_flag) {
         const double MU0 = 4.0 * PI * 1e-7;
         const double ETA0 = MU0 * C0;
-        launch_hallen_rhs(b->d_solves, ns, b->d_ants, b->d_segs, b->d_ibuf, b->d_srcs, b->d_rhs, b->d_cos,
+        launch_hallen_rhs(b->d_solves, ns, b->d_ants, b->d_segs, b->d_ibuf, b->d_srcs, b->d_pts, b->d_rhs, b->d_cos,
                           2.0 * PI / ETA0, st);
         ++L;
     }
@@ -1185,6 +1341,71 @@ int fnec_batch_run(fnec_batch *b) {
     return FNEC_OK;
 }
 
+// Capture the pipeline from the batch stream into a graph.  Capture may be
+// refused (a launch form the driver does not record); the batch then keeps
+// launching eagerly and says why.
+static void capture_pipeline(fnec_batch *b) {
+    fnec_ctx *ctx = b->ctx;
+    const std::string saved = ctx->err;
+    cudaStream_t st = b->st;
+    cudaError_t e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        b->graph_state = FNEC_GRAPH_FAILED;
+        b->graph_why = std::string("begin capture: ") + cudaGetErrorString(e);
+        return;
+    }
+    int rc = run_pipeline(b);
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(st, &g);
+    cudaGraphExec_t ex = nullptr;
+    std::string why;
+    if (rc != FNEC_OK) why = "capture: " + ctx->err;
+    else if (e != cudaSuccess || !g) why = std::string("end capture: ") + cudaGetErrorString(e);
+    else if ((e = cudaGraphInstantiateWithFlags(&ex, g, 0)) != cudaSuccess)
+        why = std::string("instantiate: ") + cudaGetErrorString(e);
+    if (g) cudaGraphDestroy(g);
+    if (!why.empty() || !ex) {
+        (void)cudaGetLastError();
+        if (ex) cudaGraphExecDestroy(ex);
+        ctx->err = saved;
+        b->graph_state = FNEC_GRAPH_FAILED;
+        b->graph_why = why;
+        return;
+    }
+    b->gexec = ex;
+    b->graph_state = FNEC_GRAPH_READY;
+    b->graph_launches = b->launches;
+}
+
+static void drop_graph(fnec_batch *b) {
+    if (b->gexec) cudaGraphExecDestroy(b->gexec);
+    b->gexec = nullptr;
+    b->graph_state = FNEC_GRAPH_NONE;
+    b->graph_why.clear();
+}
+
+int fnec_batch_run(fnec_batch *b) {
+    if (!b) return FNEC_ERR_BAD_ARG;
+    fnec_ctx *ctx = b->ctx;
+    cudaSetDevice(ctx->device);
+    if (b->units.empty()) return FNEC_OK;
+    const bool graph = b->sched.graph != 0 && !b->profile && b->graph_state != FNEC_GRAPH_FAILED &&
+                       (b->sched.graph == 2 || b->n_runs >= 1);
+    ++b->n_runs;
+    if (!graph) return run_pipeline(b);
+    if (!b->gexec) {
+        cudaError_t pre = cudaGetLastError();
+        if (pre != cudaSuccess)
+            return fail(ctx, FNEC_ERR_CUDA, std::string("an earlier call left an error: ") + cudaGetErrorString(pre));
+        capture_pipeline(b);
+        if (!b->gexec) return run_pipeline(b);
+    }
+    CUDA_TRY(ctx, cudaGraphLaunch(b->gexec, b->st));
+    b->launches = b->graph_launches;
+    return FNEC_OK;
+}
+
 int fnec_batch_set_profiling(fnec_batch *b, int on) {
     if (!b) return FNEC_ERR_BAD_ARG;
     cudaSetDevice(b->ctx->device);
@@ -1213,6 +1434,286 @@ int fnec_batch_sync(fnec_batch *b) {
     if (!b) return FNEC_ERR_BAD_ARG;
     cudaSetDevice(b->ctx->device);
     CUDA_TRY(b->ctx, cudaStreamSynchronize(b->st));
+    return FNEC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// schedules, the autotuner and its cache
+// ---------------------------------------------------------------------------
+
+static bool schedule_valid(const fnec_schedule &s) {
+    auto bit = [](int32_t v) { return v == 0 || v == 1; };
+    return bit(s.grid_panels) && (s.class_shift == 1 || s.class_shift == 2) && bit(s.gram_tensor) &&
+           (s.gmres_cluster == 1 || s.gmres_cluster == 2 || s.gmres_cluster == 4 || s.gmres_cluster == 8) &&
+           bit(s.grid_gmres) && s.graph >= 0 && s.graph <= 2;
+}
+
+// Make the batch launch as s says (s valid); drops a captured graph when
+// anything the pipeline's launches depend on changes.
+static void apply_schedule(fnec_batch *b, const fnec_schedule &s) {
+    fnec_schedule t = s;
+    if (t.gmres_cluster > b->mixed.cluster_max) t.gmres_cluster = b->mixed.cluster_max;
+    const bool same_launches = t.grid_panels == b->sched.grid_panels && t.class_shift == b->sched.class_shift &&
+                               t.gram_tensor == b->sched.gram_tensor && t.gmres_cluster == b->sched.gmres_cluster &&
+                               t.grid_gmres == b->sched.grid_gmres;
+    if (!same_launches || (t.graph == 0) != (b->sched.graph == 0)) drop_graph(b);
+    b->sched = t;
+    b->grid.grid_on = t.grid_panels != 0;
+    b->grid.class_shift = t.class_shift;
+    b->mixed.use_tc = t.gram_tensor != 0;
+    b->mixed.cluster_c = t.gmres_cluster < 1 ? 1 : t.gmres_cluster;
+    b->mixed.grid_on = t.grid_gmres != 0;
+}
+
+static int ceil_log2(int64_t v) {
+    int k = 0;
+    while (((int64_t)1 << k) < v) ++k;
+    return k;
+}
+
+// Batches whose launch structure is alike share a key: precision, SM count,
+// solve count, largest and mean system size (log2 buckets) and which
+// optional kernels the plan holds.
+static std::string tune_key(const fnec_batch *b) {
+    int64_t ssum = 0;
+    for (const UnitDesc &u : b->units) ssum += u.s;
+    const int64_t nu = (int64_t)b->units.size();
+    char k[96];
+    std::snprintf(k, sizeof(k), "p%d.sm%d.ns%d.nu%d.smax%d.smean%d.gp%d.gg%d.tc%d.cm%d", b->precision, b->grid.sms,
+                  ceil_log2((int64_t)b->solves.size()), ceil_log2(nu), ceil_log2(b->max_s),
+                  ceil_log2(nu ? ssum / nu : 0), b->grid.d_xchg ? 1 : 0, b->mixed.grid_solves.empty() ? 0 : 1,
+                  b->mixed.tc ? 1 : 0, b->mixed.cluster_max);
+    return k;
+}
+
+static std::mutex g_tune_mu;
+static std::map<std::string, fnec_schedule> g_tune_cache;
+
+static void schedule_from_cache(fnec_batch *b) {
+    fnec_schedule s;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(tune_key(b));
+        if (it == g_tune_cache.end()) return;
+        s = it->second;
+    }
+    apply_schedule(b, s);
+}
+
+int fnec_batch_get_schedule(const fnec_batch *b, fnec_schedule *out) {
+    if (!b || !out) return FNEC_ERR_BAD_ARG;
+    *out = b->sched;
+    return FNEC_OK;
+}
+
+int fnec_batch_set_schedule(fnec_batch *b, const fnec_schedule *s) {
+    if (!b || !s) return FNEC_ERR_BAD_ARG;
+    if (!schedule_valid(*s)) return fail(b->ctx, FNEC_ERR_BAD_ARG, "schedule field out of range");
+    cudaSetDevice(b->ctx->device);
+    apply_schedule(b, *s);
+    return FNEC_OK;
+}
+
+int fnec_batch_graph_state(const fnec_batch *b, int32_t *state, uint64_t *nodes) {
+    if (!b) return FNEC_ERR_BAD_ARG;
+    if (state) *state = b->graph_state;
+    if (nodes) *nodes = b->graph_state == FNEC_GRAPH_READY ? b->graph_launches : 0;
+    return FNEC_OK;
+}
+
+// Median device time (ms) of reps runs under s after one warm-up run, or
+// a negative value if a run failed.
+static double time_schedule(fnec_batch *b, const fnec_schedule &s, uint32_t reps, cudaEvent_t *ev) {
+    apply_schedule(b, s);
+    if (fnec_batch_run(b) != FNEC_OK || cudaStreamSynchronize(b->st) != cudaSuccess) return -1.0;
+    std::vector<float> ms(reps);
+    for (uint32_t r = 0; r < reps; ++r) {
+        cudaEventRecord(ev[0], b->st);
+        if (fnec_batch_run(b) != FNEC_OK) return -1.0;
+        cudaEventRecord(ev[1], b->st);
+        if (cudaEventSynchronize(ev[1]) != cudaSuccess) return -1.0;
+        cudaEventElapsedTime(&ms[r], ev[0], ev[1]);
+    }
+    std::sort(ms.begin(), ms.end());
+    return (double)ms[reps / 2];
+}
+
+int fnec_batch_tune(fnec_batch *b, uint32_t reps, fnec_tune_report *out) {
+    if (!b) return FNEC_ERR_BAD_ARG;
+    fnec_ctx *ctx = b->ctx;
+    cudaSetDevice(ctx->device);
+    const std::string key = tune_key(b);
+    fnec_tune_report rep = {};
+    std::snprintf(rep.key, sizeof(rep.key), "%s", key.c_str());
+    fnec_schedule start = b->sched;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            start = it->second;
+            rep.from_cache = 1;
+        }
+    }
+    if (reps == 0 || b->units.empty()) {
+        apply_schedule(b, start);
+        rep.best = b->sched;
+        if (out) *out = rep;
+        return FNEC_OK;
+    }
+    CUDA_TRY(ctx, cudaStreamSynchronize(b->st));
+    cudaEvent_t ev[2];
+    CUDA_TRY(ctx, cudaEventCreate(&ev[0]));
+    if (cudaEventCreate(&ev[1]) != cudaSuccess) {
+        cudaEventDestroy(ev[0]);
+        return fail(ctx, FNEC_ERR_CUDA, "tune: event creation failed");
+    }
+    const bool prof = b->profile;
+    b->profile = false;
+    // graph capture first (the other fields are then timed as they will run)
+    fnec_schedule best = start;
+    best.graph = 2;
+    double best_ms = time_schedule(b, best, reps, ev);
+    if (b->graph_state != FNEC_GRAPH_READY || best_ms < 0) {
+        best.graph = 0;
+        best_ms = time_schedule(b, best, reps, ev);
+    } else {
+        fnec_schedule eager = best;
+        eager.graph = 0;
+        double t = time_schedule(b, eager, reps, ev);
+        ++rep.candidates;
+        if (t >= 0 && t < 0.98 * best_ms) {
+            best = eager;
+            best_ms = t;
+        }
+    }
+    ++rep.candidates;
+    if (best_ms < 0) {
+        cudaEventDestroy(ev[0]);
+        cudaEventDestroy(ev[1]);
+        b->profile = prof;
+        apply_schedule(b, start);
+        return fail(ctx, FNEC_ERR_CUDA, "tune: the starting schedule failed to run: " + ctx->err);
+    }
+    rep.default_ms = best_ms;
+    // coordinate descent over the launch-shape fields that can matter here
+    struct Knob {
+        int32_t fnec_schedule::*f;
+        std::vector<int32_t> v;
+    };
+    std::vector<Knob> knobs;
+    const bool mixed = b->precision == FNEC_PRECISION_MIXED;
+    if (mixed && b->mixed.tc) knobs.push_back({&fnec_schedule::gram_tensor, {1, 0}});
+    if (mixed && b->mixed.cluster_max > 1) {
+        std::vector<int32_t> c;
+        for (int v = 1; v <= b->mixed.cluster_max; v *= 2) c.push_back(v);
+        knobs.push_back({&fnec_schedule::gmres_cluster, c});
+    }
+    if (mixed && !b->mixed.grid_solves.empty()) knobs.push_back({&fnec_schedule::grid_gmres, {1, 0}});
+    if (b->grid.d_xchg) knobs.push_back({&fnec_schedule::grid_panels, {1, 0}});
+    if (b->units.size() > 1) knobs.push_back({&fnec_schedule::class_shift, {1, 2}});
+    for (const Knob &k : knobs) {
+        for (int32_t v : k.v) {
+            if (best.*(k.f) == v) continue;
+            fnec_schedule c = best;
+            c.*(k.f) = v;
+            double t = time_schedule(b, c, reps, ev);
+            ++rep.candidates;
+            if (t >= 0 && t < 0.98 * best_ms) {  // 2 % margin against timing noise
+                best = c;
+                best_ms = t;
+            }
+        }
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    b->profile = prof;
+    (void)cudaGetLastError();  // a refused candidate's launch error
+    if (best.graph) best.graph = 1;
+    apply_schedule(b, best);
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        g_tune_cache[key] = b->sched;
+    }
+    rep.best = b->sched;
+    rep.best_ms = best_ms;
+    if (out) *out = rep;
+    return FNEC_OK;
+}
+
+static const char *const SCHED_FIELDS[] = {"grid_panels", "class_shift", "gram_tensor",
+                                           "gmres_cluster", "grid_gmres", "graph"};
+static int32_t *sched_field(fnec_schedule &s, int i) {
+    int32_t *f[] = {&s.grid_panels, &s.class_shift, &s.gram_tensor, &s.gmres_cluster, &s.grid_gmres, &s.graph};
+    return f[i];
+}
+
+int fnec_tune_cache_save(const char *path) {
+    if (!path) return FNEC_ERR_BAD_ARG;
+    std::FILE *f = std::fopen(path, "w");
+    if (!f) return FNEC_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (auto &kv : g_tune_cache) {
+        fnec_schedule s = kv.second;
+        std::fprintf(f, "%s", kv.first.c_str());
+        for (int i = 0; i < 6; ++i) std::fprintf(f, " %s=%d", SCHED_FIELDS[i], (int)*sched_field(s, i));
+        std::fprintf(f, "\n");
+    }
+    return std::fclose(f) == 0 ? FNEC_OK : FNEC_ERR_BAD_ARG;
+}
+
+int fnec_tune_cache_load(const char *path) {
+    if (!path) return FNEC_ERR_BAD_ARG;
+    std::FILE *f = std::fopen(path, "r");
+    if (!f) return FNEC_ERR_BAD_ARG;
+    std::map<std::string, fnec_schedule> got;
+    char line[512];
+    int rc = FNEC_OK;
+    while (std::fgets(line, sizeof(line), f)) {
+        char *save = nullptr;
+        char *tok = strtok_r(line, " \t\r\n", &save);
+        if (!tok || tok[0] == '#') continue;
+        std::string key = tok;
+        fnec_schedule s = {1, 1, 1, 1, 1, 1};
+        int seen = 0;
+        while ((tok = strtok_r(nullptr, " \t\r\n", &save))) {
+            char *eq = std::strchr(tok, '=');
+            if (!eq) {
+                rc = FNEC_ERR_BAD_ARG;
+                break;
+            }
+            *eq = 0;
+            int i = 0;
+            while (i < 6 && std::strcmp(tok, SCHED_FIELDS[i]) != 0) ++i;
+            if (i == 6) {
+                rc = FNEC_ERR_BAD_ARG;
+                break;
+            }
+            *sched_field(s, i) = (int32_t)std::atoi(eq + 1);
+            seen |= 1 << i;
+        }
+        if (rc != FNEC_OK || seen != 0x3f || !schedule_valid(s)) {
+            rc = FNEC_ERR_BAD_ARG;
+            break;
+        }
+        got[key] = s;
+    }
+    std::fclose(f);
+    if (rc != FNEC_OK) return rc;  // a malformed file changes nothing
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    for (auto &kv : got) g_tune_cache[kv.first] = kv.second;
+    return FNEC_OK;
+}
+
+int fnec_tune_cache_clear(void) {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache.clear();
+    return FNEC_OK;
+}
+
+int fnec_tune_cache_size(uint32_t *n) {
+    if (!n) return FNEC_ERR_BAD_ARG;
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    *n = (uint32_t)g_tune_cache.size();
     return FNEC_OK;
 }
 
@@ -1687,7 +2188,7 @@ struct Lane {
 // Upper bound of the device bytes one request's batch needs (Z, the
 // factor, solution and work vectors, Gram operand stacks, pattern buffers).
 int64_t request_bytes(const HostAnt &h, int precision) {
-    const int64_t n = (int64_t)h.segs.size(), w = (int64_t)h.ep.size(), s = n + w;
+    const int64_t n = (int64_t)h.segs.size(), w = h.cols(), s = n + w;
     const int64_t f = (int64_t)h.freqs.size(), r = (int64_t)std::max<size_t>(h.rhs_srcs.size(), 1);
     const int64_t rows = n + 2 * w + (int64_t)h.ja.size();
     const int64_t pts = h.rp.pts_off >= 0 ? (int64_t)h.pts.size() / 2 : (int64_t)h.rp.n_theta * h.rp.n_phi;
@@ -2053,7 +2554,7 @@ int fnec_server_submit(fnec_server *S, const fnec_antenna *req, const fnec_reque
     }
     const HostAnt &h = r->host;
     r->n = (uint32_t)h.segs.size();
-    r->s = r->n + (uint32_t)h.ep.size();
+    r->s = r->n + (uint32_t)h.cols();
     r->n_solves = (uint32_t)(std::max<size_t>(h.rhs_srcs.size(), 1) * h.freqs.size());
     r->n_points = h.rp.pts_off >= 0 ? (uint32_t)(h.pts.size() / 2) : (uint32_t)(h.rp.n_theta * h.rp.n_phi);
     uint32_t fr = 0;

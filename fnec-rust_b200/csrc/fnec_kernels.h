@@ -62,16 +62,25 @@ struct GridPlan {
     void *d_sync = nullptr;      // GridSync words: panel steps x GRID_PANEL_MAX_UNITS
     int steps = 0;               // panel steps the sync words cover
     int sms = 0;                 // SMs of the device
+    // schedule (set per batch, the autotuner's choices)
+    bool grid_on = true;         // tall panels grid-wide (else one CTA from global memory)
+    int class_shift = 1;         // size classes of panel heights: (2^k x lo, hi]
 };
 size_t grid_xchg_bytes();        // bytes of d_xchg
 size_t grid_sync_bytes(int steps);
 // The units still active at panel step c0 (s > c0), in ranges [i0, i1) of
-// the s-descending order whose panel heights m = s - c0 share a power-of-two
-// class (<= 64, <= 128, ...); m_max is the range's tallest.  Starts at i_begin.
+// the s-descending order whose panel heights m = s - c0 share a size class
+// (<= 64, then powers of 2^class_shift above it); m_max is the range's
+// tallest.  Starts at i_begin.
 struct StepClass {
     int i0, i1, m_max;
 };
 void step_classes(const GridPlan &gp, int c0, int i_begin, std::vector<StepClass> &out);
+// A cooperative launch (every CTA co-resident) issued through
+// cudaLaunchKernelExC so that stream capture records it as a cooperative
+// kernel node.
+cudaError_t launch_cooperative(const void *kernel, dim3 grid, dim3 block, void **args, size_t smem,
+                               cudaStream_t st);
 // How the panel at column c0 is factored (fnec_plain.cu): the number of
 // units that take the grid-wide kernel (0 none, -1 infeasible) and its shape.
 int plan_grid_panel(const GridPlan &gp, int c0, int thr_rows, int pnb, size_t elem, const void *kernel,
@@ -79,8 +88,9 @@ int plan_grid_panel(const GridPlan &gp, int c0, int thr_rows, int pnb, size_t el
 
 // fnec_plain.cu
 void launch_expand_segments(const DevWire *wires, int nw, DevSeg *segs, cudaStream_t st);
+// dtab: the batch's double table (path arc lengths and signs, AntDesc::arc_off)
 void launch_hallen_rhs(const UnitDesc *solves, int ns, const AntDesc *ants, const DevSeg *segs,
-                       const int32_t *ibuf, const DevSource *srcs, cx *rhs, double *cosv,
+                       const int32_t *ibuf, const DevSource *srcs, const double *dtab, cx *rhs, double *cosv,
                        double scale, cudaStream_t st);
 void launch_fill_exact(const UnitDesc *units, const AntDesc *ants, const DevSeg *segs,
                        const int4 *tiles, int ntiles, cx *z, cudaStream_t st);

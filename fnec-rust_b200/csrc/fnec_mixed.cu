@@ -777,7 +777,7 @@ __global__ void __launch_bounds__(256, 3) k_gmres_ir(const UnitDesc *__restrict_
                                                   const cx *__restrict__ rhs, const double *__restrict__ cosv,
                                                   const float2 *__restrict__ a32buf, const int32_t *__restrict__ pivbuf,
                                                   cx *xbuf, cx *vbuf, cx *wbuf, const int32_t *__restrict__ status,
-                                                  int staged, int skip_s, int only) {
+                                                  int staged, int skip_s, int only, int min_s) {
     extern __shared__ unsigned char s_dyn[];
     __shared__ cx sH[(GM + 1) * GM];
     __shared__ double scs[GM];
@@ -788,7 +788,7 @@ __global__ void __launch_bounds__(256, 3) k_gmres_ir(const UnitDesc *__restrict_
     __shared__ int s_stop;
     int ui = blockIdx.x;  // one solve (right-hand side)
     UnitDesc u = units[ui];
-    if (status[u.sys] != 0 || u.s >= skip_s) return;  // skip_s: refined grid-wide
+    if (status[u.sys] != 0 || u.s >= skip_s || u.s < min_s) return;  // refined grid-wide / by clusters
     if (only >= 0 && ui != only) return;
     AntDesc a = ants[u.ant];
     MixedUnit mu = mus[ui];
@@ -983,10 +983,28 @@ struct GGrid {
     GridSync *gs;
     int32_t *status;
     int G, cta, tid, lane, wid, gt, T, gw, TW;
+    int rc;       // rows per column-sum chunk of M^H t
+    int cluster;  // 1: the G CTAs are one thread-block cluster (hardware barrier)
     unsigned epoch, redk;
 };
 
+// Rows per column-sum chunk: enough (column block, row chunk) items to keep
+// every warp busy, at least 32 rows and at most 256.
+__host__ __device__ __forceinline__ int gg_row_chunk(int n, int total_warps) {
+    int ncb = (n + 63) / 64;
+    int rc = (int)(((int64_t)n * ncb + 4 * total_warps - 1) / (4 * total_warps));
+    return rc < 32 ? 32 : (rc > 256 ? 256 : rc);
+}
+
+__device__ __forceinline__ void cluster_barrier() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
 __device__ __forceinline__ bool gg_sync(GGrid &c) {
+    if (c.cluster) {  // a hardware barrier: every CTA of the cluster takes the same path
+        cluster_barrier();
+        return true;
+    }
     if (grid_barrier(c.gs, (unsigned)c.G, ++c.epoch)) return true;
     if (c.tid == 0) atomicExch(c.status, FNEC_STATUS_GRID_TIMEOUT);
     return false;
@@ -1021,11 +1039,11 @@ __device__ bool gg_apply(GGrid &c, const cx *v, cx *out) {
         for (int q = c.gt; q < g.nc; q += c.T) g.t[g.n + q] = {0, 0};
     }
     GG_SYNC(c);
-    const int ncb = (g.n + 63) / 64, nch = (g.n + GG_RC - 1) / GG_RC;
+    const int ncb = (g.n + 63) / 64, nch = (g.n + c.rc - 1) / c.rc;
     for (int it = c.gw; it < ncb * nch; it += c.TW) {
         int cb = it % ncb, ch = it / ncb;
         int c0 = cb * 64 + c.lane, c1 = c0 + 32;
-        int r0 = ch * GG_RC, r1 = min(g.n, r0 + GG_RC);
+        int r0 = ch * c.rc, r1 = min(g.n, r0 + c.rc);
         cx a0 = {0, 0}, a1 = {0, 0};
         if (c1 < g.n) {
             for (int r = r0; r < r1; ++r) {
@@ -1080,13 +1098,16 @@ __device__ bool gg_prec(GGrid &c, const cx *in, cx *out) {
         if (bk % c.G == c.cta && c.wid == 0) {
             cx yl = c.lane < nb ? ldcg_cx(c.y + c0 + c.lane) : cx{0, 0};
             const float2 *lrow = g.lu + (int64_t)(c0 + (c.lane < nb ? c.lane : 0)) * s + c0;
-            float2 lr[32];
+#pragma unroll 1
+            for (int q8 = 0; q8 < 32; q8 += 8) {
+                float2 lr[8];
 #pragma unroll
-            for (int q = 0; q < 32; ++q) lr[q] = (q < nb) ? lrow[q] : cf(0.f, 0.f);
+                for (int q = 0; q < 8; ++q) lr[q] = (q8 + q < nb) ? lrow[q8 + q] : cf(0.f, 0.f);
 #pragma unroll
-            for (int q = 0; q < 32; ++q) {
-                double yr = __shfl_sync(0xffffffffu, yl.re, q), yi = __shfl_sync(0xffffffffu, yl.im, q);
-                if (c.lane > q && c.lane < nb) yl = zsub(yl, zmul(f2z(lr[q]), cx{yr, yi}));
+                for (int q = 0; q < 8; ++q) {
+                    double yr = __shfl_sync(0xffffffffu, yl.re, q8 + q), yi = __shfl_sync(0xffffffffu, yl.im, q8 + q);
+                    if (c.lane > q8 + q && c.lane < nb) yl = zsub(yl, zmul(f2z(lr[q]), cx{yr, yi}));
+                }
             }
             if (c.lane < nb) c.y[c0 + c.lane] = yl;
         }
@@ -1102,11 +1123,14 @@ __device__ bool gg_prec(GGrid &c, const cx *in, cx *out) {
             const float2 *lrow = g.lu + (int64_t)r * s + c0;
             cx acc = ldcg_cx(c.y + r);
             if (nb == 32) {
-                float2 lr[32];
 #pragma unroll
-                for (int k = 0; k < 32; ++k) lr[k] = lrow[k];
+                for (int k8 = 0; k8 < 32; k8 += 8) {
+                    float2 lr[8];
 #pragma unroll
-                for (int k = 0; k < 32; ++k) acc = zsub(acc, zmul(f2z(lr[k]), s_yb[k]));
+                    for (int k = 0; k < 8; ++k) lr[k] = lrow[k8 + k];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) acc = zsub(acc, zmul(f2z(lr[k]), s_yb[k8 + k]));
+                }
             } else {
                 for (int k = 0; k < nb; ++k) acc = zsub(acc, zmul(f2z(lrow[k]), s_yb[k]));
             }
@@ -1120,15 +1144,19 @@ __device__ bool gg_prec(GGrid &c, const cx *in, cx *out) {
         if (bk % c.G == c.cta && c.wid == 0) {
             cx yl = c.lane < nb ? ldcg_cx(c.y + c0 + c.lane) : cx{0, 0};
             const float2 *urow = g.lu + (int64_t)(c0 + (c.lane < nb ? c.lane : 0)) * s + c0;
-            float2 ur[32];
+#pragma unroll 1
+            for (int q8 = 24; q8 >= 0; q8 -= 8) {
+                float2 ur[8];
 #pragma unroll
-            for (int q = 0; q < 32; ++q) ur[q] = (q < nb) ? urow[q] : cf(1.f, 0.f);
+                for (int q = 0; q < 8; ++q) ur[q] = (q8 + q < nb) ? urow[q8 + q] : cf(1.f, 0.f);
 #pragma unroll
-            for (int q = 31; q >= 0; --q) {
-                if (q < nb) {
-                    if (c.lane == q) yl = zdiv(yl, f2z(ur[q]));
-                    double yr = __shfl_sync(0xffffffffu, yl.re, q), yi = __shfl_sync(0xffffffffu, yl.im, q);
-                    if (c.lane < q) yl = zsub(yl, zmul(f2z(ur[q]), cx{yr, yi}));
+                for (int q = 7; q >= 0; --q) {
+                    const int qq = q8 + q;
+                    if (qq < nb) {
+                        if (c.lane == qq) yl = zdiv(yl, f2z(ur[q]));
+                        double yr = __shfl_sync(0xffffffffu, yl.re, qq), yi = __shfl_sync(0xffffffffu, yl.im, qq);
+                        if (c.lane < qq) yl = zsub(yl, zmul(f2z(ur[q]), cx{yr, yi}));
+                    }
                 }
             }
             if (c.lane < nb) c.y[c0 + c.lane] = yl;
@@ -1144,11 +1172,14 @@ __device__ bool gg_prec(GGrid &c, const cx *in, cx *out) {
             const float2 *urow = g.lu + (int64_t)r * s + c0;
             cx acc = ldcg_cx(c.y + r);
             if (nb == 32) {
-                float2 ur[32];
 #pragma unroll
-                for (int k = 0; k < 32; ++k) ur[k] = urow[k];
+                for (int k8 = 0; k8 < 32; k8 += 8) {
+                    float2 ur[8];
 #pragma unroll
-                for (int k = 0; k < 32; ++k) acc = zsub(acc, zmul(f2z(ur[k]), s_yb[k]));
+                    for (int k = 0; k < 8; ++k) ur[k] = urow[k8 + k];
+#pragma unroll
+                    for (int k = 0; k < 8; ++k) acc = zsub(acc, zmul(f2z(ur[k]), s_yb[k8 + k]));
+                }
             } else {
                 for (int k = 0; k < nb; ++k) acc = zsub(acc, zmul(f2z(urow[k]), s_yb[k]));
             }
@@ -1381,6 +1412,101 @@ __global__ void __launch_bounds__(256) k_gmres_grid(const UnitDesc *__restrict__
     c.TW = c.T >> 5;
     c.epoch = 0;
     c.redk = 0;
+    c.rc = GG_RC;
+    c.cluster = 0;
+    gmres_grid_body(c, u, mus, ui, xbuf, W, vbuf + mu.v_off);
+}
+
+constexpr int GC_MAX_S = 8192;  // cluster GMRES: the permutation is built in shared memory
+
+// Scratch (complex128 units) of one solve of the cluster GMRES: column-sum
+// partials, the substitution vector, the reduction slots and the row
+// permutation (int32).
+__host__ __device__ __forceinline__ int64_t gc_scratch(int n, int s, int C) {
+    int rc = gg_row_chunk(n, C * 8);
+    int64_t nch = (n + rc - 1) / rc;
+    return nch * n + s + 2LL * C * (GM + 1) + (s + 3) / 4;
+}
+
+__device__ __forceinline__ unsigned cluster_rank() {
+    unsigned r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// The grid-wide GMRES iteration on one thread-block cluster per solve: the
+// cluster's C CTAs split the vectors and the matrix passes, synchronise with
+// the hardware cluster barrier and exchange through L2.  Solves with S at or
+// above skip_s (refined grid-wide) or above GC_MAX_S are left to the others.
+__global__ void __launch_bounds__(256, 2) k_gmres_cluster(
+    const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants, MixedUnit *mus,
+    const int32_t *__restrict__ ibuf, const DevConRow *__restrict__ crows, const cx *__restrict__ zbuf,
+    const cx *__restrict__ rhs, const double *__restrict__ cosv, const float2 *__restrict__ a32buf,
+    const int32_t *__restrict__ pivbuf, cx *xbuf, cx *vbuf, cx *wbuf, int32_t *status, cx *cscratch, int C,
+    int skip_s) {
+    extern __shared__ int32_t s_pperm[];
+    const int ui = blockIdx.x / C;
+    UnitDesc u = units[ui];
+    if (status[u.sys] != 0 || u.s >= skip_s || u.s > GC_MAX_S) return;  // the whole cluster leaves
+    AntDesc a = ants[u.ant];
+    MixedUnit mu = mus[ui];
+    GGrid c;
+    c.g.n = u.n;
+    c.g.s = u.s;
+    c.g.w = a.w;
+    c.g.nc = a.n_crow;
+    c.g.rows = u.n + a.n_crow;
+    c.g.z = zbuf + u.z_off;
+    c.g.y = rhs + u.rhs_off;
+    c.g.cv = cosv + u.cos_off;
+    c.g.rowwire = ibuf + a.rowwire_off;
+    c.g.wptr = ibuf + a.wptr_off;
+    c.g.wrow = ibuf + a.wrow_off;
+    c.g.crows = crows + a.crow_off;
+    c.g.lu = a32buf + mu.a32_off;
+    c.g.piv = pivbuf + u.piv_off;
+    cx *W = wbuf + mu.w_off;
+    c.g.t = W + 4 * u.s;
+    c.ccptr = ibuf + a.ccptr_off;
+    c.ccq = ibuf + a.ccq_off;
+    c.G = C;
+    c.cta = (int)cluster_rank();
+    c.tid = threadIdx.x;
+    c.lane = threadIdx.x & 31;
+    c.wid = threadIdx.x >> 5;
+    c.gt = c.cta * blockDim.x + threadIdx.x;
+    c.T = C * blockDim.x;
+    c.gw = c.gt >> 5;
+    c.TW = c.T >> 5;
+    c.epoch = 0;
+    c.redk = 0;
+    c.rc = gg_row_chunk(u.n, C * 8);
+    c.cluster = 1;
+    c.gs = nullptr;
+    c.status = &status[u.sys];
+    cx *cs = cscratch + mu.cs_off;
+    const int64_t nch = (u.n + c.rc - 1) / c.rc;
+    c.part = cs;
+    c.y = cs + nch * u.n;
+    c.red = c.y + u.s;
+    int32_t *perm = reinterpret_cast<int32_t *>(c.red + 2 * C * (GM + 1));
+    c.perm = perm;
+    if (c.cta == 0) {  // the factor's row permutation, applied in order in shared memory
+        for (int i = threadIdx.x; i < u.s; i += blockDim.x) s_pperm[i] = i;
+        __syncthreads();
+        if (threadIdx.x == 0)
+            for (int k = 0; k < u.s; ++k) {
+                int p = c.g.piv[k];
+                if (p >= 0 && p != k) {
+                    int t0 = s_pperm[k];
+                    s_pperm[k] = s_pperm[p];
+                    s_pperm[p] = t0;
+                }
+            }
+        __syncthreads();
+        for (int i = threadIdx.x; i < u.s; i += blockDim.x) perm[i] = s_pperm[i];
+    }
+    cluster_barrier();
     gmres_grid_body(c, u, mus, ui, xbuf, W, vbuf + mu.v_off);
 }
 
@@ -1430,6 +1556,7 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
         mu[i].rows = rows;
         mu[i].iters = 0;
         mu[i].resid = 0.0;
+        mu[i].cs_off = -1;
         v += (int64_t)(GM + 1) * u.s;
         wk += 6 * (int64_t)u.s + 2 * (int64_t)rows;  // 4 vectors + rows, then the unstaged copies
     }
@@ -1501,6 +1628,28 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
         w.grid_ctas = std::min(GG_MAX_CTAS, sms * std::min(per_sm, 1));
     }
     {
+        // cluster GMRES when one CTA per solve cannot fill the GPU
+        int device = 0, sms = 0;
+        cudaGetDevice(&device);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        const int capacity = 3 * sms;  // one-CTA solves resident at once (3 CTAs per SM)
+        int C = 1;
+        while (C < 8 && (int64_t)solves.size() * C * 2 <= capacity) C *= 2;
+        w.cluster_max = C;
+        w.cluster_c = 1;  // one CTA per solve unless the tuner measures better
+        if (C > 1) {
+            int64_t tot = 0;
+            for (size_t i = 0; i < solves.size(); ++i) {
+                mu[i].cs_off = tot;
+                tot += gc_scratch(solves[i].n, solves[i].s, C);
+            }
+            e = dev.alloc(&w.c_base, sizeof(cx) * (size_t)(tot + 1));
+            if (e != cudaSuccess) return e;
+            w.c_scratch = (cx *)w.c_base;
+            w.bytes += sizeof(cx) * (size_t)(tot + 1);
+        }
+    }
+    {
         // tensor-core Gram: operand stacks, per-unit layout and the tile list
         TcGramPlan *p = new TcGramPlan();
         tc_gram_plan(systems, *p);
@@ -1548,6 +1697,9 @@ void free_mixed(MixedWork &w, const DevAlloc &dev) {
     dev.release(w.base);
     dev.release(w.grid_base);
     dev.release(w.tc_base);
+    dev.release(w.c_base);
+    w.c_base = nullptr;
+    w.c_scratch = nullptr;
     w.grid_base = nullptr;
     w.tc_base = nullptr;
     delete w.tc;
@@ -1572,7 +1724,7 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         ++L;
     }
     mark(0);
-    if (mw.tc) {
+    if (mw.tc && mw.use_tc) {
         tc_gram_run(*mw.tc, d_units, static_cast<const TcGramUnit *>(mw.tc_gu), static_cast<const TcTile *>(mw.tc_tiles),
                     mw.smu, z, mw.tc_hi, mw.tc_lo, mw.a32, status, mw.tc_max_n, st);
         ++L;
@@ -1616,8 +1768,8 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
                 float2 *a32 = mw.a32;
                 void *args[] = {(void *)&d_units, (void *)&smu, (void *)&ord, (void *)&c0, (void *)&a32,
                                 (void *)&piv, (void *)&status, (void *)&xg, (void *)&gs};
-                done = cudaLaunchCooperativeKernel((const void *)k_panel32_grid, dim3(G, n_thr), dim3(256), args, gsm,
-                                                   st) == cudaSuccess;
+                done = launch_cooperative((const void *)k_panel32_grid, dim3(G, n_thr), dim3(256), args, gsm, st) ==
+                       cudaSuccess;
                 if (!done) (void)cudaGetLastError();
             }
             if (!done) k_panel32<<<n_thr, 256, 0, st>>>(d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX, ord, 0);
@@ -1654,16 +1806,42 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         if (lim < 0 || (size_t)lim < smem) staged = 0;
     }
     if (!staged) smem = 0;
+    const bool grid_refine = mw.grid_on && !mw.grid_solves.empty();
+    const int skip_s = grid_refine ? GG_MIN_S : INT_MAX;
+    int min_s = 0;  // solves below this are refined by the cluster kernel
+    if (ns > 0 && mw.cluster_c > 1) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(ns * mw.cluster_c));
+        cfg.blockDim = dim3(256);
+        cfg.dynamicSmemBytes = sizeof(int32_t) * (size_t)std::min(max_s, GC_MAX_S);
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)mw.cluster_c;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        set_smem_limit_once(k_gmres_cluster, (int)(sizeof(int32_t) * GC_MAX_S));
+        if (cudaLaunchKernelEx(&cfg, k_gmres_cluster, d_solves, d_ants, mw.mu, ibuf, crows, (const cx *)z, rhs, cosv,
+                               (const float2 *)mw.a32, (const int32_t *)piv, x, mw.v, mw.w, status, mw.c_scratch,
+                               mw.cluster_c, skip_s) == cudaSuccess) {
+            min_s = GC_MAX_S + 1;
+            ++L;
+        } else {
+            (void)cudaGetLastError();  // clusters not schedulable: one CTA per solve
+        }
+    }
     if (ns > 0) {
         k_gmres_ir<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x, mw.v,
-                                          mw.w, status, staged, mw.grid_solves.empty() ? INT_MAX : GG_MIN_S, -1);
+                                          mw.w, status, staged, skip_s, -1, min_s);
         cudaError_t le = cudaPeekAtLastError();
         if (le != cudaSuccess && !marks.detail[0])
             std::snprintf(marks.detail, sizeof(marks.detail), "GMRES launch: %d solves, %zu B shared (%s), max_s %d, rows %d",
                           ns, smem, staged ? "staged" : "unstaged", max_s, max_rows);
     }
     ++L;
-    if (!mw.grid_solves.empty()) {
+    if (grid_refine) {
         cudaMemsetAsync(mw.g_sync, 0, sizeof(GridSync) * mw.grid_solves.size(), st);
         for (size_t k = 0; k < mw.grid_solves.size(); ++k) {
             int ui = mw.grid_solves[k];
@@ -1685,11 +1863,11 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
                             (void *)&piv, (void *)&x, (void *)&vb, (void *)&wb, (void *)&status,
                             (void *)&perm, (void *)&mw.g_part, (void *)&mw.g_y, (void *)&mw.g_red, (void *)&gs};
             if (mw.grid_ctas <= 0 ||
-                cudaLaunchCooperativeKernel((const void *)k_gmres_grid, dim3(mw.grid_ctas), dim3(256), args, 0, st) !=
+                launch_cooperative((const void *)k_gmres_grid, dim3(mw.grid_ctas), dim3(256), args, 0, st) !=
                     cudaSuccess) {
                 (void)cudaGetLastError();  // not co-resident: refine this solve in one CTA
                 k_gmres_ir<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x,
-                                                  mw.v, mw.w, status, staged, INT_MAX, ui);
+                                                  mw.v, mw.w, status, staged, INT_MAX, ui, 0);
             }
             L += 2;
         }

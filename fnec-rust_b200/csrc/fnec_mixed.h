@@ -20,6 +20,7 @@ struct MixedUnit {
     int32_t rows;     // N + constraint rows
     int32_t iters;    // GMRES iterations used
     double resid;     // final preconditioned relative residual
+    int64_t cs_off;   // complex128 scratch of the cluster GMRES (-1: none)
 };
 
 struct MixedWork {
@@ -43,6 +44,14 @@ struct MixedWork {
     cx *g_red = nullptr;
     void *g_sync = nullptr;
     int grid_ctas = 0;
+    // GMRES spread over thread-block clusters of cluster_c CTAs per solve
+    // (when there are too few solves to fill the GPU one CTA each)
+    int cluster_c = 1;    // in use (1: one CTA per solve); the tuner picks it
+    int cluster_max = 1;  // largest cluster the scratch was sized for
+    bool use_tc = true;   // Gram on the tensor cores (else the FP32 SIMT kernel); the tuner picks it
+    bool grid_on = true;  // grid_solves refine grid-wide (else one CTA each); the tuner picks it
+    cx *c_scratch = nullptr;
+    void *c_base = nullptr;
     // the Gram block Z^H Z on the tensor cores (fnec_tc.cu)
     TcGramPlan *tc = nullptr;
     void *tc_base = nullptr;

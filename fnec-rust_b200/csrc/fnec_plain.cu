@@ -91,8 +91,8 @@ __global__ void k_expand_segments(const DevWire *__restrict__ wires, int nw, Dev
 // ---------------------------------------------------------------------------
 __global__ void k_hallen_rhs(const UnitDesc *__restrict__ solves, const AntDesc *__restrict__ ants,
                              const DevSeg *__restrict__ segs, const int32_t *__restrict__ ibuf,
-                             const DevSource *__restrict__ srcs, cx *rhs_buf, double *cos_buf,
-                             double scale) {
+                             const DevSource *__restrict__ srcs, const double *__restrict__ dtab,
+                             cx *rhs_buf, double *cos_buf, double scale) {
     UnitDesc u = solves[blockIdx.x];  // one right-hand side
     AntDesc a = ants[u.ant];
     const DevSeg *sg = segs + a.seg_off;
@@ -101,6 +101,33 @@ __global__ void k_hallen_rhs(const UnitDesc *__restrict__ solves, const AntDesc 
     const DevSource *src = srcs + a.src_off + sptr[u.rhs];
     int n_src = sptr[u.rhs + 1] - sptr[u.rhs];
     double k = u.k_fill;
+    if (a.paths) {
+        // build_hallen_rhs_paths (excitation.rs:264-341): cos(k s) and the
+        // source terms along each path's signed arc length s, times the
+        // traversal signs; every EX card drives its whole path
+        const double *s_mid = dtab + a.arc_off, *sgn = s_mid + a.n;
+        const int32_t *col = ibuf + a.rowwire_off;
+        for (int m = threadIdx.x; m < a.n; m += blockDim.x) {
+            if (u.rhs == 0) {
+                double sn, cs;
+                cr_sincos(D_MUL(k, s_mid[m]), &sn, &cs);
+                cos_buf[u.cos_off + m] = D_MUL(sgn[m], cs);
+            }
+            cx r = cx_make(0.0, 0.0);
+            for (int q = 0; q < n_src; ++q) {
+                DevSource s = src[q];
+                if (col[m] != col[s.feed]) continue;
+                double ds = fabs(D_SUB(s_mid[m], s_mid[s.feed]));
+                double ss, sc;
+                cr_sincos(D_MUL(k, ds), &ss, &sc);
+                cx t = cx_mul(cx_make(0.0, D_MUL(-scale, ss)), cx_make(s.v_re, s.v_im));
+                double f = D_MUL(sgn[m], sgn[s.feed]);
+                r = cx_add(r, cx_make(D_MUL(t.re, f), D_MUL(t.im, f)));
+            }
+            rhs_buf[u.rhs_off + m] = r;
+        }
+        return;
+    }
     for (int m = threadIdx.x; m < a.n; m += blockDim.x) {
         int first = comp[2 * m], last = comp[2 * m + 1];
         const double *wd = sg[first].dir;
@@ -923,9 +950,9 @@ void launch_expand_segments(const DevWire *wires, int nw, DevSeg *segs, cudaStre
     if (nw > 0) k_expand_segments<<<nw, 64, 0, st>>>(wires, nw, segs);
 }
 void launch_hallen_rhs(const UnitDesc *solves, int ns, const AntDesc *ants, const DevSeg *segs,
-                       const int32_t *ibuf, const DevSource *srcs, cx *rhs, double *cosv,
+                       const int32_t *ibuf, const DevSource *srcs, const double *dtab, cx *rhs, double *cosv,
                        double scale, cudaStream_t st) {
-    if (ns > 0) k_hallen_rhs<<<ns, 128, 0, st>>>(solves, ants, segs, ibuf, srcs, rhs, cosv, scale);
+    if (ns > 0) k_hallen_rhs<<<ns, 128, 0, st>>>(solves, ants, segs, ibuf, srcs, dtab, rhs, cosv, scale);
 }
 void launch_fill_exact(const UnitDesc *units, const AntDesc *ants, const DevSeg *segs,
                        const int4 *tiles, int ntiles, cx *z, cudaStream_t st) {
@@ -984,7 +1011,7 @@ int plan_grid_panel(const GridPlan &gp, int c0, int thr_rows, int pnb, size_t el
     int nl = 0;
     while (nl < (int)gp.s_desc.size() && gp.s_desc[nl] - c0 > thr_rows) ++nl;
     if (nl == 0) return 0;
-    if (nl > GRID_PANEL_MAX_UNITS || !gp.d_xchg || !gp.d_sync || gp.sms <= 0) return -1;
+    if (!gp.grid_on || nl > GRID_PANEL_MAX_UNITS || !gp.d_xchg || !gp.d_sync || gp.sms <= 0) return -1;
     const int m_max = gp.s_desc[0] - c0;
     const size_t cta_cap = 96 * 1024;  // two CTAs per SM
     const int r_cap = (int)(cta_cap / (pnb * elem));
@@ -1002,13 +1029,29 @@ int plan_grid_panel(const GridPlan &gp, int c0, int thr_rows, int pnb, size_t el
     return nl;
 }
 
+cudaError_t launch_cooperative(const void *kernel, dim3 grid, dim3 block, void **args, size_t smem,
+                               cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelExC(&cfg, kernel, args);
+}
+
 void step_classes(const GridPlan &gp, int c0, int i_begin, std::vector<StepClass> &out) {
     out.clear();
     int i = i_begin, n = (int)gp.s_desc.size();
     while (i < n && gp.s_desc[i] > c0) {
+        const int f = 1 << gp.class_shift;
         int m = gp.s_desc[i] - c0, hi = 64;
-        while (hi < m) hi *= 2;
-        int lo = hi == 64 ? 0 : hi / 2;  // the class holds heights (lo, hi]
+        while (hi < m) hi *= f;
+        int lo = hi == 64 ? 0 : hi / f;  // the class holds heights (lo, hi]
         StepClass c{i, i, m};
         while (i < n && gp.s_desc[i] - c0 > lo) ++i;  // s descending: the class is a run
         c.i1 = i;
@@ -1047,8 +1090,8 @@ uint64_t launch_factor_exact(const UnitDesc *units, int nu, int max_s, const Gri
                 GridSync *gs = static_cast<GridSync *>(gp.d_sync) + (size_t)(c0 / NB) * GRID_PANEL_MAX_UNITS;
                 void *args[] = {(void *)&units, (void *)&ord, (void *)&c0, (void *)&A, (void *)&piv,
                                 (void *)&status, (void *)&xg, (void *)&gs};
-                done = cudaLaunchCooperativeKernel((const void *)k_panel_grid, dim3(G, n_thr), dim3(256), args, gsm,
-                                                   st) == cudaSuccess;
+                done = launch_cooperative((const void *)k_panel_grid, dim3(G, n_thr), dim3(256), args, gsm, st) ==
+                       cudaSuccess;
                 if (!done) (void)cudaGetLastError();  // not co-resident after all
             }
             if (!done) k_panel<<<n_thr, 256, 0, st>>>(units, c0, A, piv, status, INT_MAX, ord, 0);

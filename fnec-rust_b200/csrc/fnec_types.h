@@ -74,6 +74,12 @@ struct AntDesc {
     int64_t crow_off;    // DevConRow[n_crow]
     int64_t ccptr_off;   // int32[n+1]: CSR of the constraint rows touching each column
     int64_t ccq_off;     // int32: those rows (ascending), ccptr-indexed
+    // degree-2 conductor paths (solve_session.rs:1338-1378): one column per
+    // path (rowwire), I = 0 rows at the two free ends of each path, and
+    // cos / source terms along the signed arc length of each path
+    int32_t paths;       // 1: the path form; 0: merged straight wires
+    int32_t pad_a;
+    int64_t arc_off;     // doubles: s_mid[n] (signed arc length), then sign[n]
 };
 
 // One constraint row of M (linear.rs:744-762): M[N+q][c0] = 1 and, for a
@@ -85,7 +91,7 @@ struct DevConRow {
 
 struct DevSource {       // one resolved delta-gap source (excitation.rs:171-187)
     int32_t feed;        // antenna-local segment index
-    int32_t comp_first;  // merged component of the feed segment
+    int32_t comp_first;  // merged component of the feed segment (path form: unused)
     int32_t comp_last;
     int32_t pad;
     double v_re, v_im;

@@ -173,6 +173,14 @@ SIGNATURES = {
     "fnec_batch_read_unit": (ctypes.c_int, [_P, _U32, _P, _P]),
     "fnec_batch_read_z": (ctypes.c_int, [_P, _U32, _P]),
     "fnec_batch_read_refinement": (ctypes.c_int, [_P, _P, _P]),
+    "fnec_batch_get_schedule": (ctypes.c_int, [_P, _P]),
+    "fnec_batch_set_schedule": (ctypes.c_int, [_P, _P]),
+    "fnec_batch_graph_state": (ctypes.c_int, [_P, _P, _P]),
+    "fnec_batch_tune": (ctypes.c_int, [_P, _U32, _P]),
+    "fnec_tune_cache_save": (ctypes.c_int, [ctypes.c_char_p]),
+    "fnec_tune_cache_load": (ctypes.c_int, [ctypes.c_char_p]),
+    "fnec_tune_cache_clear": (ctypes.c_int, []),
+    "fnec_tune_cache_size": (ctypes.c_int, [_P]),
 }
 
 _lib = None
@@ -540,6 +548,45 @@ def _antenna_struct(a, keep: list):
                     int(bool(a.separate_sources)))
 
 
+class _Schedule(ctypes.Structure):
+    _fields_ = [("grid_panels", ctypes.c_int32), ("class_shift", ctypes.c_int32), ("gram_tensor", ctypes.c_int32),
+                ("gmres_cluster", ctypes.c_int32), ("grid_gmres", ctypes.c_int32), ("graph", ctypes.c_int32)]
+
+
+class _TuneReport(ctypes.Structure):
+    _fields_ = [("best", _Schedule), ("default_ms", ctypes.c_double), ("best_ms", ctypes.c_double),
+                ("candidates", ctypes.c_uint32), ("from_cache", ctypes.c_uint32), ("key", ctypes.c_char * 96)]
+
+
+GRAPH_NONE, GRAPH_READY, GRAPH_FAILED = 0, 1, -1
+
+
+def _sched_dict(s: _Schedule) -> dict:
+    return {k: int(getattr(s, k)) for k, _ in _Schedule._fields_}
+
+
+def tune_cache_save(path: str):
+    """Write the process-wide tuning cache (shape key -> schedule) as text."""
+    if lib().fnec_tune_cache_save(str(path).encode()) != OK:
+        raise AccelError(ERR_BAD_ARG, f"tune_cache_save: cannot write {path}")
+
+
+def tune_cache_load(path: str):
+    """Merge a saved tuning cache; a malformed file changes nothing."""
+    if lib().fnec_tune_cache_load(str(path).encode()) != OK:
+        raise AccelError(ERR_BAD_ARG, f"tune_cache_load: cannot read {path} (missing or malformed)")
+
+
+def tune_cache_clear():
+    lib().fnec_tune_cache_clear()
+
+
+def tune_cache_size() -> int:
+    n = ctypes.c_uint32()
+    lib().fnec_tune_cache_size(ctypes.byref(n))
+    return int(n.value)
+
+
 class HallenBatch:
     """A planned, device-resident batch of per-frequency Hallen solves."""
 
@@ -581,6 +628,38 @@ class HallenBatch:
 
     def sync(self):
         self.ctx.check(lib().fnec_batch_sync(self._h), "batch_sync")
+
+    @property
+    def schedule(self) -> dict:
+        """How the pipeline launches (grid_panels, class_shift, gram_tensor,
+        gmres_cluster, grid_gmres, graph)."""
+        s = _Schedule()
+        self.ctx.check(lib().fnec_batch_get_schedule(self._h, ctypes.byref(s)), "batch_get_schedule")
+        return _sched_dict(s)
+
+    @schedule.setter
+    def schedule(self, values: dict):
+        s = _Schedule()
+        lib().fnec_batch_get_schedule(self._h, ctypes.byref(s))
+        for k, v in values.items():
+            if k not in dict(_Schedule._fields_):
+                raise KeyError(k)
+            setattr(s, k, int(v))
+        self.ctx.check(lib().fnec_batch_set_schedule(self._h, ctypes.byref(s)), "batch_set_schedule")
+
+    def graph_state(self):
+        """(GRAPH_NONE | GRAPH_READY | GRAPH_FAILED, kernel launches per replay)."""
+        st, n = ctypes.c_int32(), ctypes.c_uint64()
+        self.ctx.check(lib().fnec_batch_graph_state(self._h, ctypes.byref(st), ctypes.byref(n)), "batch_graph_state")
+        return int(st.value), int(n.value)
+
+    def tune(self, reps: int = 3) -> dict:
+        """Time candidate schedules on this batch, keep the fastest and cache
+        it for batches of the same shape (reps=0: apply a cached one only)."""
+        r = _TuneReport()
+        self.ctx.check(lib().fnec_batch_tune(self._h, int(reps), ctypes.byref(r)), "batch_tune")
+        return {"best": _sched_dict(r.best), "default_ms": r.default_ms, "best_ms": r.best_ms,
+                "candidates": int(r.candidates), "from_cache": bool(r.from_cache), "key": r.key.decode()}
 
     @property
     def kernel_launches(self) -> int:

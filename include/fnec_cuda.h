@@ -449,6 +449,65 @@ int fnec_batch_read_refinement(fnec_batch *b, int32_t *iters, double *resid);
  * elimination is not kept; the Z of a unit can be read after a run. */
 int fnec_batch_read_z(fnec_batch *b, uint32_t unit, double *z);
 
+/* ---- schedules, CUDA graphs and the autotuner --------------------------
+ *
+ * How a batch's pipeline is launched.  None of these choices changes a
+ * result bit of the plain FP64 form (its per-unit arithmetic is the same
+ * under every schedule); the mixed form stays within its refinement
+ * tolerance under every schedule. */
+typedef struct {
+    int32_t grid_panels;   /* 1: panels too tall for one CTA's shared memory are
+                              factored grid-wide (cooperative launch); 0: one CTA
+                              from global memory                                  */
+    int32_t class_shift;   /* panel and trailing launches group units whose
+                              remaining heights share a 2^class_shift size class
+                              (1 or 2)                                            */
+    int32_t gram_tensor;   /* mixed: 1 Gram Z^H Z as 3xTF32 tcgen05 tiles; 0 FP32
+                              SIMT tiles                                          */
+    int32_t gmres_cluster; /* mixed: CTAs per refinement solve (1, 2, 4 or 8; a
+                              thread-block cluster when > 1)                      */
+    int32_t grid_gmres;    /* mixed: 1 very large solves refine grid-wide        */
+    int32_t graph;         /* 0 launch eagerly; 1 capture the pipeline as a CUDA
+                              graph at the second run and replay it afterwards;
+                              2 capture at the first run                          */
+} fnec_schedule;
+
+/* Graph state of a batch (fnec_batch_graph_state). */
+#define FNEC_GRAPH_NONE 0     /* not captured (eager launches)                 */
+#define FNEC_GRAPH_READY 1    /* runs replay the captured graph                */
+#define FNEC_GRAPH_FAILED (-1)/* capture was refused; runs launch eagerly      */
+
+typedef struct {
+    fnec_schedule best;     /* the schedule set on the batch                  */
+    double default_ms;      /* device ms of one run under the starting schedule */
+    double best_ms;         /* ... under the chosen one                       */
+    uint32_t candidates;    /* schedules timed                                 */
+    uint32_t from_cache;    /* 1: the batch's shape was already in the cache   */
+    char key[96];           /* shape key of the tuning cache                   */
+} fnec_tune_report;
+
+int fnec_batch_get_schedule(const fnec_batch *b, fnec_schedule *out);
+/* Change the schedule (validated: FNEC_ERR_BAD_ARG for values out of range;
+ * cluster sizes above what the batch planned for are lowered); drops a
+ * captured graph. */
+int fnec_batch_set_schedule(fnec_batch *b, const fnec_schedule *s);
+/* state: FNEC_GRAPH_*; nodes: kernel launches one replay issues. */
+int fnec_batch_graph_state(const fnec_batch *b, int32_t *state, uint64_t *nodes);
+/* Time the batch under candidate schedules (coordinate descent over the
+ * fields above, reps timed runs each after one warm-up, median device time
+ * on the batch stream), set the fastest and record it in the process-wide
+ * tuning cache under the batch's shape key.  Batches created later with
+ * the same key start from the cached schedule.  With reps == 0 the cached
+ * schedule is applied if present and nothing is timed. */
+int fnec_batch_tune(fnec_batch *b, uint32_t reps, fnec_tune_report *out);
+/* The tuning cache as a text file: one "key field=value ..." line per
+ * shape.  load merges (later lines win); clear empties the cache. */
+int fnec_tune_cache_save(const char *path);
+int fnec_tune_cache_load(const char *path);
+int fnec_tune_cache_clear(void);
+/* Number of cached shapes. */
+int fnec_tune_cache_size(uint32_t *n);
+
 #ifdef __cplusplus
 }
 #endif

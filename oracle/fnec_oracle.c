@@ -373,6 +373,176 @@ int or_hallen_rhs(const or_seg *segs, int64_t n, double freq_hz, const or_source
     return OR_OK;
 }
 
+/* geometry.rs:404-584 build_conductor_paths: wires (per-tag runs) joined
+ * through degree-2 endpoint nodes into open chains.  Outputs per segment
+ * its path (in path order), traversal sign and signed arc length of its
+ * midpoint from the path centre; free_ends holds each path's (first,
+ * last) traversed segment.  Returns the number of paths, or -1 where the
+ * reference returns None (a node of degree >= 3, a wire closed on itself,
+ * a chain without exactly two free ends).  *nontrivial = 1 if some path
+ * is not a forward run of ascending segments (ConductorPath::is_trivial). */
+static int64_t uf_find(int64_t *parent, int64_t x) {
+    int64_t r = x;
+    while (parent[r] != r) r = parent[r];
+    while (parent[x] != x) {
+        int64_t nx = parent[x];
+        parent[x] = r;
+        x = nx;
+    }
+    return r;
+}
+
+int64_t or_conductor_paths(const or_seg *segs, int64_t n, int64_t *path_of, double *sign,
+                           double *s_mid, int64_t *free_ends, int *nontrivial) {
+    int64_t w = or_wire_endpoints(segs, n, NULL, 0);
+    *nontrivial = 0;
+    if (w <= 0) return 0;
+    int64_t *ep = (int64_t *)malloc(sizeof(int64_t) * 2 * (size_t)w);
+    or_wire_endpoints(segs, n, ep, w);
+    const double TOL = 1e-6;
+    /* endpoint id = 2 wi + end (0 start of its first segment, 1 end of its last) */
+    int64_t ne = 2 * w;
+    int64_t *node_of = (int64_t *)malloc(sizeof(int64_t) * (size_t)ne);
+    int64_t *node_cnt = (int64_t *)calloc((size_t)ne, sizeof(int64_t));
+    int64_t *node_mem = (int64_t *)malloc(sizeof(int64_t) * 2 * (size_t)ne); /* first two members */
+    for (int64_t i = 0; i < ne; ++i) node_of[i] = -1;
+    int64_t nodes = 0;
+    int64_t ret = 0;
+#define EP_POINT(id) ((id) % 2 == 0 ? segs[ep[2 * ((id) / 2)]].start : segs[ep[2 * ((id) / 2) + 1]].end)
+    for (int64_t id = 0; id < ne; ++id) {
+        if (node_of[id] >= 0) continue;
+        int64_t nd = nodes++;
+        node_of[id] = nd;
+        node_mem[2 * nd] = id;
+        node_cnt[nd] = 1;
+        const double *p = EP_POINT(id);
+        for (int64_t j = 0; j < ne; ++j) {
+            if (node_of[j] >= 0) continue;
+            if (dist2(p, EP_POINT(j)) < TOL * TOL) {
+                node_of[j] = nd;
+                if (node_cnt[nd] < 2) node_mem[2 * nd + node_cnt[nd]] = j;
+                node_cnt[nd]++;
+            }
+        }
+    }
+#undef EP_POINT
+    int64_t *parent = (int64_t *)malloc(sizeof(int64_t) * (size_t)w);
+    int64_t *root = (int64_t *)malloc(sizeof(int64_t) * (size_t)w);
+    char *visited = (char *)calloc((size_t)w, 1);
+    for (int64_t nd = 0; nd < nodes; ++nd)
+        if (node_cnt[nd] >= 3) {
+            ret = -1;
+            goto done;
+        }
+    for (int64_t i = 0; i < w; ++i) parent[i] = i;
+    for (int64_t nd = 0; nd < nodes; ++nd) {
+        if (node_cnt[nd] != 2) continue;
+        int64_t a = node_mem[2 * nd] / 2, b = node_mem[2 * nd + 1] / 2;
+        if (a == b) {
+            ret = -1;
+            goto done;
+        }
+        int64_t ra = uf_find(parent, a), rb = uf_find(parent, b);
+        parent[ra] = rb;
+    }
+    for (int64_t i = 0; i < w; ++i) root[i] = uf_find(parent, i);
+    /* components in ascending root order (BTreeMap), wires ascending within */
+    for (int64_t r = 0; r < w; ++r) {
+        int64_t fe[2], nfe = 0, any = 0;
+        for (int64_t wi = 0; wi < w; ++wi) {
+            if (root[wi] != r) continue;
+            any = 1;
+            for (int e = 0; e < 2; ++e)
+                if (node_cnt[node_of[2 * wi + e]] == 1) {
+                    if (nfe < 2) fe[nfe] = 2 * wi + e;
+                    nfe++;
+                }
+        }
+        if (!any) continue;
+        if (nfe != 2) {
+            ret = -1;
+            goto done;
+        }
+        int64_t pi = ret++;
+        int64_t cur = fe[0] / 2, enter = fe[0] % 2;
+        double arc = 0.0;
+        int64_t first_seg = -1, last_seg = -1, prev = -1, cnt = 0;
+        int64_t *walked = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n > 0 ? n : 1));
+        for (;;) {
+            visited[cur] = 1;
+            int64_t f = ep[2 * cur], l = ep[2 * cur + 1];
+            double sg = enter == 0 ? 1.0 : -1.0;
+            for (int64_t t = 0; t <= l - f; ++t) {
+                int64_t m = enter == 0 ? f + t : l - t;
+                double half = segs[m].length * 0.5;
+                s_mid[m] = arc + half; /* arc length from the path start, re-centred below */
+                arc += segs[m].length;
+                path_of[m] = pi;
+                sign[m] = sg;
+                if (sg != 1.0 || (prev >= 0 && m != prev + 1)) *nontrivial = 1;
+                if (first_seg < 0) first_seg = m;
+                last_seg = m;
+                prev = m;
+                walked[cnt++] = m;
+            }
+            int64_t exit_id = 2 * cur + (1 - enter);
+            int64_t nd = node_of[exit_id];
+            if (node_cnt[nd] == 1) break;
+            int64_t nxt = -1;
+            for (int q = 0; q < 2; ++q) {
+                int64_t mid = node_mem[2 * nd + q];
+                if (mid / 2 != cur && !visited[mid / 2]) nxt = mid;
+            }
+            if (nxt < 0) break;
+            cur = nxt / 2;
+            enter = nxt % 2;
+        }
+        for (int64_t t = 0; t < cnt; ++t) s_mid[walked[t]] = s_mid[walked[t]] - arc * 0.5;
+        free(walked);
+        free_ends[2 * pi] = first_seg;
+        free_ends[2 * pi + 1] = last_seg;
+    }
+done:
+    free(ep);
+    free(node_of);
+    free(node_cnt);
+    free(node_mem);
+    free(parent);
+    free(root);
+    free(visited);
+    return ret;
+}
+
+/* excitation.rs:264-341 build_hallen_rhs_paths: cos(k s) along each path
+ * with the traversal sign; every voltage EX card, in deck order, drives
+ * its whole path with the sign of its feed segment. */
+int or_hallen_rhs_paths(const or_seg *segs, int64_t n, double freq_hz, const or_source *src,
+                        int64_t ns, const int64_t *path_of, const double *sign, const double *s_mid,
+                        double *rhs, double *cosv) {
+    const double MU0 = 4.0 * OR_PI * 1e-7;
+    const double ETA0 = MU0 * C0;
+    double k = 2.0 * OR_PI * freq_hz / C0;
+    double scale = 2.0 * OR_PI / ETA0;
+    for (int64_t m = 0; m < n; ++m) {
+        cosv[m] = sign[m] * cos(k * s_mid[m]);
+        rhs[2 * m] = 0.0;
+        rhs[2 * m + 1] = 0.0;
+    }
+    for (int64_t e = 0; e < ns; ++e) {
+        int64_t fi = find_seg(segs, n, src[e].tag, src[e].segment);
+        if (fi < 0) return OR_ERR_SEGMENT_NOT_FOUND;
+        c64 vsrc = cmk(src[e].v_re, src[e].v_im);
+        double feed_sign = sign[fi];
+        for (int64_t m = 0; m < n; ++m) {
+            if (path_of[m] != path_of[fi]) continue;
+            double ds = fabs(s_mid[m] - s_mid[fi]);
+            c64 t = crs(sign[m] * feed_sign, cmul(cmk(0.0, -scale * sin(k * ds)), vsrc));
+            cst(&rhs[2 * m], cadd(cld(&rhs[2 * m]), t));
+        }
+    }
+    return OR_OK;
+}
+
 /* ------------------------------------------------------------------------- */
 /* Z-matrix fill                                                              */
 /* ------------------------------------------------------------------------- */
@@ -603,6 +773,11 @@ int or_solve_square(double *a, double *b, int64_t s, double *x, int32_t *pivots,
  * started at +0 never changes its value or its sign under round-to-nearest,
  * so the skipped form is value-identical (checked bit-for-bit by the tests).
  * Per element, the surviving terms are still added in ascending r. */
+static int solve_core(const double *z, int64_t n, const double *rhs, const double *cosv,
+                      const int64_t *row_wire, int64_t w, const int64_t *cc0, const int64_t *cc1,
+                      const double *cv1, int64_t nc, double *x, int32_t *pivots, double *gram, int naive,
+                      int nthreads);
+
 int or_solve_hallen(const double *z, int64_t n, const double *rhs, const double *cosv,
                     const int64_t *ep_in, int64_t w_in, const int64_t *ja, const int64_t *jb,
                     const double *jsign, int64_t nj, double *x, int32_t *pivots, double *gram,
@@ -632,7 +807,6 @@ int or_solve_hallen(const double *z, int64_t n, const double *rhs, const double 
         if (!injunc[ep[2 * q + 1]]) nfree++;
     }
     int64_t rows = n + nfree + nj;
-    int64_t cols = n + w;
     int64_t *row_wire = (int64_t *)calloc((size_t)(n > 0 ? n : 1), sizeof(int64_t));
     for (int64_t q = 0; q < w; ++q)
         for (int64_t r = ep[2 * q]; r <= ep[2 * q + 1]; ++r) row_wire[r] = q;
@@ -663,7 +837,45 @@ int or_solve_hallen(const double *z, int64_t n, const double *rhs, const double 
         cv1[crow] = jsign[t];
         crow++;
     }
+    (void)rows;
+    int st = solve_core(z, n, rhs, cosv, row_wire, w, cc0, cc1, cv1, nc, x, pivots, gram, naive, nthreads);
+    free(cc0);
+    free(cc1);
+    free(cv1);
+    free(row_wire);
+    free(injunc);
+    return st;
+}
 
+/* linear.rs:823-894 solve_hallen_paths: one homogeneous column per path
+ * (path_of), I = 0 rows only at the listed free-end segments (in order),
+ * no junction rows; the normal equations and elimination as solve_hallen. */
+int or_solve_hallen_paths(const double *z, int64_t n, const double *rhs, const double *cosv,
+                          const int64_t *path_of, const int64_t *free_ends, int64_t n_free, double *x,
+                          int32_t *pivots, double *gram, int naive, int nthreads) {
+    int64_t w = 0;
+    for (int64_t m = 0; m < n; ++m)
+        if (path_of[m] + 1 > w) w = path_of[m] + 1;
+    int64_t *cc1 = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n_free + 1));
+    double *cv1 = (double *)malloc(sizeof(double) * (size_t)(n_free + 1));
+    for (int64_t q = 0; q < n_free; ++q) {
+        cc1[q] = -1;
+        cv1[q] = 0.0;
+    }
+    int st = solve_core(z, n, rhs, cosv, path_of, w, free_ends, cc1, cv1, n_free, x, pivots, gram, naive, nthreads);
+    free(cc1);
+    free(cv1);
+    return st;
+}
+
+/* The normal equations (MᴴM + 1e-8 I) x = Mᴴy of M = [Z | -cos columns]
+ * over constraint rows (cc0, cc1, cv1), then GEPP. */
+static int solve_core(const double *z, int64_t n, const double *rhs, const double *cosv,
+                      const int64_t *row_wire, int64_t w, const int64_t *cc0, const int64_t *cc1,
+                      const double *cv1, int64_t nc, double *x, int32_t *pivots, double *gram, int naive,
+                      int nthreads) {
+    int64_t rows = n + nc;
+    int64_t cols = n + w;
     int64_t aw = cols + 1;
     c64 *aug = (c64 *)calloc((size_t)(cols * aw + 1), sizeof(c64));
 
@@ -736,11 +948,6 @@ int or_solve_hallen(const double *z, int64_t n, const double *rhs, const double 
         for (int64_t i = 0; i < cols; ++i) cst(&x[2 * i], xx[i]);
     free(xx);
     free(aug);
-    free(cc0);
-    free(cc1);
-    free(cv1);
-    free(row_wire);
-    free(injunc);
     return st;
 }
 
@@ -940,6 +1147,49 @@ int or_solve_problem(or_problem *p) {
     }
     double *rhs = (double *)malloc(sizeof(double) * 2 * (size_t)n);
     double *cosv = (double *)malloc(sizeof(double) * (size_t)n);
+    /* solve_session.rs:1338-1378: decks with a non-trivial degree-2
+     * conductor path take the path solve */
+    {
+        int64_t *path_of = (int64_t *)malloc(sizeof(int64_t) * (size_t)n);
+        double *sgn = (double *)malloc(sizeof(double) * (size_t)n);
+        double *smid = (double *)malloc(sizeof(double) * (size_t)n);
+        int64_t *fe = (int64_t *)malloc(sizeof(int64_t) * 2 * (size_t)n);
+        int nontrivial = 0;
+        int64_t np = or_conductor_paths(segs, n, path_of, sgn, smid, fe, &nontrivial);
+        int st = OR_OK;
+        int taken = np >= 0 && nontrivial;
+        if (taken) {
+            st = or_hallen_rhs_paths(segs, n, p->freq_hz, p->sources, p->n_sources, path_of, sgn, smid, rhs,
+                                     cosv);
+            double *x = (double *)malloc(sizeof(double) * 2 * (size_t)(n + np));
+            double *z = NULL;
+            if (st == OR_OK) {
+                z = (double *)malloc(sizeof(double) * 2 * (size_t)(n * n));
+                or_assemble_z(segs, n, p->freq_hz, p->ground, z);
+                st = or_solve_hallen_paths(z, n, rhs, cosv, path_of, fe, 2 * np, x, p->pivots, NULL, 0, 1);
+            }
+            if (st == OR_OK) {
+                memcpy(p->currents, x, sizeof(double) * 2 * (size_t)n);
+                int64_t nf = or_feedpoints(segs, n, p->sources, p->n_sources, x, p->feed, p->n_sources);
+                if (p->n_feed) *p->n_feed = nf;
+                if (p->n_points > 0 && p->points && p->pattern)
+                    or_radiation_pattern(segs, n, x, p->freq_hz, p->ground, p->points, p->n_points, p->pattern,
+                                         NULL, NULL);
+            }
+            free(x);
+            free(z);
+        }
+        free(path_of);
+        free(sgn);
+        free(smid);
+        free(fe);
+        if (taken) {
+            free(segs);
+            free(rhs);
+            free(cosv);
+            return p->status = st;
+        }
+    }
     int st = or_hallen_rhs(segs, n, p->freq_hz, p->sources, p->n_sources, rhs, cosv);
     if (st != OR_OK) {
         free(segs);

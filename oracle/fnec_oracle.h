@@ -95,6 +95,20 @@ void or_z_element(const or_seg *obs, const or_seg *src, double freq_hz, int grou
  * n+w int32 pivot rows.  gram (optional): 2*S*(S+1) doubles, the augmented
  * [A|b] before elimination.  naive != 0 runs the literal dense triple loop
  * over M; naive == 0 skips structural zeros (value-identical, see .c). */
+/* geometry.rs:404-584 build_conductor_paths.  Per segment: path index,
+ * traversal sign, signed arc length from the path centre; free_ends: 2 per
+ * path (capacity 2n).  Returns the path count, -1 for None (degree >= 3,
+ * closed loop).  *nontrivial: some path is reversed or non-contiguous. */
+int64_t or_conductor_paths(const or_seg *segs, int64_t n, int64_t *path_of, double *sign,
+                           double *s_mid, int64_t *free_ends, int *nontrivial);
+/* excitation.rs:264-341 build_hallen_rhs_paths. */
+int or_hallen_rhs_paths(const or_seg *segs, int64_t n, double freq_hz, const or_source *src,
+                        int64_t ns, const int64_t *path_of, const double *sign, const double *s_mid,
+                        double *rhs, double *cosv);
+/* linear.rs:823-894 solve_hallen_paths; x holds n + paths complex values. */
+int or_solve_hallen_paths(const double *z, int64_t n, const double *rhs, const double *cosv,
+                          const int64_t *path_of, const int64_t *free_ends, int64_t n_free, double *x,
+                          int32_t *pivots, double *gram, int naive, int nthreads);
 int or_solve_hallen(const double *z, int64_t n, const double *rhs, const double *cosv,
                     const int64_t *ep, int64_t w, const int64_t *ja, const int64_t *jb,
                     const double *jsign, int64_t nj, double *x, int32_t *pivots,

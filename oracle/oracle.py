@@ -95,6 +95,13 @@ def lib():
         L.or_solve_hallen.restype = ctypes.c_int
         L.or_solve_hallen.argtypes = [_P, _I64, _P, _P, _P, _I64, _P, _P, _P, _I64, _P, _P, _P,
                                       ctypes.c_int, ctypes.c_int]
+        L.or_conductor_paths.restype = _I64
+        L.or_conductor_paths.argtypes = [_P, _I64, _P, _P, _P, _P, _P]
+        L.or_hallen_rhs_paths.restype = ctypes.c_int
+        L.or_hallen_rhs_paths.argtypes = [_P, _I64, _D, _P, _I64, _P, _P, _P, _P, _P]
+        L.or_solve_hallen_paths.restype = ctypes.c_int
+        L.or_solve_hallen_paths.argtypes = [_P, _I64, _P, _P, _P, _P, _I64, _P, _P, _P, ctypes.c_int,
+                                            ctypes.c_int]
         L.or_solve_square.restype = ctypes.c_int
         L.or_solve_square.argtypes = [_P, _P, _I64, _P, _P, ctypes.c_int]
         L.or_feedpoints.restype = _I64
@@ -226,6 +233,66 @@ def solve_hallen(z, rhs, cosv, endpoints, ja, jb, js, naive=False, want_gram=Fal
     return (x, piv[:s], gram) if want_gram else (x, piv[:s])
 
 
+class ConductorPaths:
+    """build_conductor_paths (geometry.rs:404-584) for a segment list:
+    per-segment path index, traversal sign and signed arc length, the free
+    ends (2 per path) and whether some path is non-trivial."""
+
+    def __init__(self, path_of, sign, s_mid, free_ends, nontrivial):
+        self.path_of, self.sign, self.s_mid = path_of, sign, s_mid
+        self.free_ends = free_ends
+        self.nontrivial = nontrivial
+
+    def __len__(self):
+        return len(self.free_ends)
+
+    def segs(self, p):
+        """Segments of path p in traversal order (signed arc length ascending)."""
+        idx = np.nonzero(self.path_of == p)[0]
+        return idx[np.argsort(self.s_mid[idx], kind="stable")]
+
+
+def conductor_paths(segs):
+    """ConductorPaths, or None where the reference returns None."""
+    n = len(segs)
+    path_of = np.zeros(max(n, 1), np.int64)
+    sign = np.zeros(max(n, 1), np.float64)
+    s_mid = np.zeros(max(n, 1), np.float64)
+    fe = np.zeros((max(n, 1), 2), np.int64)
+    nt = ctypes.c_int(0)
+    cnt = lib().or_conductor_paths(_ptr(segs), n, _ptr(path_of), _ptr(sign), _ptr(s_mid), _ptr(fe), ctypes.byref(nt))
+    if cnt < 0:
+        return None
+    return ConductorPaths(path_of[:n], sign[:n], s_mid[:n], fe[:cnt], bool(nt.value))
+
+
+def hallen_rhs_paths(segs, freq_hz, sources, paths: ConductorPaths):
+    n = len(segs)
+    rhs = np.zeros(n, np.complex128)
+    cosv = np.zeros(n, np.float64)
+    st = lib().or_hallen_rhs_paths(_ptr(segs), n, freq_hz, _ptr(sources), len(sources), _ptr(paths.path_of),
+                                   _ptr(paths.sign), _ptr(paths.s_mid), _ptr(rhs), _ptr(cosv))
+    if st != 0:
+        raise OracleError(f"hallen_rhs_paths: status {st}")
+    return rhs, cosv
+
+
+def solve_hallen_paths(z, rhs, cosv, paths: ConductorPaths, nthreads=1):
+    n = z.shape[0]
+    z = np.ascontiguousarray(z, np.complex128)
+    rhs = np.ascontiguousarray(rhs, np.complex128)
+    cosv = np.ascontiguousarray(cosv, np.float64)
+    fe = np.ascontiguousarray(paths.free_ends, np.int64).reshape(-1)
+    s = n + len(paths)
+    x = np.zeros(s, np.complex128)
+    piv = np.zeros(max(s, 1), np.int32)
+    st = lib().or_solve_hallen_paths(_ptr(z), n, _ptr(rhs), _ptr(cosv), _ptr(paths.path_of), _ptr(fe), len(fe),
+                                     _ptr(x), _ptr(piv), None, 0, nthreads)
+    if st != 0:
+        raise OracleError(f"solve_hallen_paths: status {st}")
+    return x, piv[:s]
+
+
 def solve_square(a, b, nthreads=1):
     s = a.shape[0]
     a = np.array(a, np.complex128, order="C")
@@ -270,7 +337,9 @@ def rp_card_points(n_theta, n_phi, theta0, phi0, d_theta, d_phi):
 
 
 class Problem:
-    """One per-frequency CLI standard-branch solve (solve_session.rs:1186-1437)."""
+    """One per-frequency CLI Hallen solve (solve_session.rs:1186-1437): the
+    degree-2 conductor-path branch when some path is non-trivial
+    (:1338-1378), else the standard branch."""
 
     def __init__(self, wires, sources, freq_hz, ground=GROUND_FREE, points=None):
         self.wires = np.ascontiguousarray(wires)

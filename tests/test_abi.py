@@ -53,3 +53,36 @@ def test_no_device_is_an_error_not_a_fallback():
         nec_accel.Context(0)
     assert ei.value.code == nec_accel.ERR_NO_DEVICE
     assert nec_accel.dispatch_frequency_point(nec_accel.GPU_ONLY, 14.2e6) == "NoDevice"
+
+
+def test_tune_cache_file_round_trip(tmp_path):
+    """The tuning cache is host state: its text file loads, saves and
+    refuses malformed input without changing the cache."""
+    import nec_accel as acc
+
+    acc.tune_cache_clear()
+    good = tmp_path / "tune.txt"
+    good.write_text("# shape key, then every schedule field\n"
+                    "p1.sm148.ns8.nu8.smax9.smean8.gp0.gg0.tc1.cm1 grid_panels=1 class_shift=2 gram_tensor=0 "
+                    "gmres_cluster=1 grid_gmres=1 graph=1\n"
+                    "p0.sm148.ns12.nu12.smax10.smean8.gp1.gg0.tc0.cm1 grid_panels=0 class_shift=1 gram_tensor=1 "
+                    "gmres_cluster=1 grid_gmres=1 graph=0\n")
+    acc.tune_cache_load(good)
+    assert acc.tune_cache_size() == 2
+    out = tmp_path / "saved.txt"
+    acc.tune_cache_save(out)
+    lines = sorted(out.read_text().split("\n")[:-1])
+    assert lines == sorted(l for l in good.read_text().split("\n")[1:] if l)
+    bad = tmp_path / "bad.txt"
+    for text in ("k grid_panels=1 class_shift=3 gram_tensor=1 gmres_cluster=1 grid_gmres=1 graph=1\n",  # range
+                 "k grid_panels=1 class_shift=1 gram_tensor=1 gmres_cluster=3 grid_gmres=1 graph=1\n",  # cluster
+                 "k grid_panels=1 class_shift=1\n",  # fields missing
+                 "k grid_panels=1 tile=7 class_shift=1 gram_tensor=1 gmres_cluster=1 grid_gmres=1 graph=1\n"):
+        bad.write_text(text)
+        with pytest.raises(acc.AccelError):
+            acc.tune_cache_load(bad)
+        assert acc.tune_cache_size() == 2
+    with pytest.raises(acc.AccelError):
+        acc.tune_cache_load(tmp_path / "absent.txt")
+    acc.tune_cache_clear()
+    assert acc.tune_cache_size() == 0
