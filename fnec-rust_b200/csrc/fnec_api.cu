@@ -2205,6 +2205,7 @@ int64_t request_bytes(const HostAnt &h, int precision) {
         b += 8 * s * s * f;                                // FP32 factor
         b += 2 * 128 * kb * rp * f + 64 * kb * kb * f;     // Gram operand stacks (hi, lo), tiles
         b += 16 * (25 * s + 6 * s + 2 * rows) * f * r;     // GMRES basis and work vectors
+        b += (16 * (((n + 31) / 32) * n + 2 * s + 512) + 4) * f * r;  // cluster GMRES scratch, launch order
     } else {
         b += 16 * s * (s + 1) * f + 4 * s * f;             // FP64 factor, pivots
     }

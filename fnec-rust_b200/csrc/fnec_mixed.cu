@@ -348,15 +348,18 @@ __global__ void __launch_bounds__(256) k_panel32(const UnitDesc *__restrict__ un
 // The FP32 panel held in shared memory (rows c0..s-1, MNB columns).
 constexpr int PANEL32_SMEM_MAX = 200 * 1024;
 
-__global__ void __launch_bounds__(256) k_panel32_smem(const UnitDesc *__restrict__ units,
-                                                      const MixedUnit *__restrict__ mus, int c0, float2 *a32buf,
-                                                      int32_t *piv_buf, int32_t *status, int skip_m, const int32_t *__restrict__ order, int base) {
+// NT threads: 256, or 1024 for tall panels (fewer rows per warp on the
+// column-serial critical path of the largest units).
+template <int NT>
+__global__ void __launch_bounds__(NT) k_panel32_smem(const UnitDesc *__restrict__ units,
+                                                     const MixedUnit *__restrict__ mus, int c0, float2 *a32buf,
+                                                     int32_t *piv_buf, int32_t *status, int skip_m, const int32_t *__restrict__ order, int base) {
     // panel rows padded to PS = MNB + 1 entries: a column read by consecutive
     // rows then falls on distinct banks
     constexpr int PS = MNB + 1;
     extern __shared__ float2 s_pan32[];
-    __shared__ float s_v[8];
-    __shared__ int s_i[8];
+    __shared__ float s_v[NT / 32];
+    __shared__ int s_i[NT / 32];
     __shared__ int s_p;
     int ui = order[base + blockIdx.x];
     UnitDesc u = units[ui];
@@ -372,14 +375,16 @@ __global__ void __launch_bounds__(256) k_panel32_smem(const UnitDesc *__restrict
         s_pan32[rr * PS + q] = A[(int64_t)(c0 + rr) * s + c0 + q];
     }
     __syncthreads();
+    // pivot candidates of the first column; later columns get theirs from
+    // the elimination pass of the column before (the tie rule is order-free)
+    float bv = -1.f;
+    int bi = -1;
+    for (int r = c0 + tid; r < s; r += blockDim.x) {
+        float2 v = s_pan32[(r - c0) * PS];
+        piv_better32(bv, bi, v.x * v.x + v.y * v.y, r);
+    }
     for (int c = c0; c < c0 + nb; ++c) {
         int lc = c - c0;
-        float bv = -1.f;
-        int bi = -1;
-        for (int r = c + tid; r < s; r += blockDim.x) {
-            float2 v = s_pan32[(r - c0) * PS + lc];
-            piv_better32(bv, bi, v.x * v.x + v.y * v.y, r);
-        }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) {
             float ov = __shfl_down_sync(0xffffffffu, bv, o);
@@ -411,19 +416,31 @@ __global__ void __launch_bounds__(256) k_panel32_smem(const UnitDesc *__restrict
             s_pan32[(p - c0) * PS + tid] = t0;
         }
         __syncthreads();
-        // elimination: a warp per row, a lane per panel column
+        // elimination: a warp per row, a lane per panel column; the
+        // multiplier is x times the pivot's reciprocal (one division per
+        // column), and the updated next column feeds its pivot search
         const float2 pj = lane < nb ? s_pan32[lc * PS + lane] : cf(0.f, 0.f);
         const float2 diag = s_pan32[lc * PS + lc];
+        const float dn = 1.0f / (diag.x * diag.x + diag.y * diag.y);
+        const float2 dinv = cf(diag.x * dn, -diag.y * dn);
+        const int nx = lc + 1;
+        bv = -1.f;
+        bi = -1;
 #pragma unroll 4
         for (int r = c + 1 + wid; r < s; r += nw) {
             float2 *row = s_pan32 + (r - c0) * PS;
             float2 x = lane < nb ? row[lane] : cf(0.f, 0.f);
-            float2 f = cf_div(make_float2(__shfl_sync(0xffffffffu, x.x, lc), __shfl_sync(0xffffffffu, x.y, lc)), diag);
+            float2 f = cf_mul(make_float2(__shfl_sync(0xffffffffu, x.x, lc), __shfl_sync(0xffffffffu, x.y, lc)), dinv);
+            float2 y = cf_sub(x, cf_mul(f, pj));
             if (lane == lc) row[lc] = f;
-            else if (lane > lc && lane < nb) row[lane] = cf_sub(x, cf_mul(f, pj));
+            else if (lane > lc && lane < nb) row[lane] = y;
+            if (nx < nb) piv_better32(bv, bi, __shfl_sync(0xffffffffu, y.x * y.x + y.y * y.y, nx), r);
         }
-        __syncthreads();
+        // no barrier here: the next column's first barrier orders these
+        // writes before its swap, and s_v is rewritten only after this
+        // column's reads of it
     }
+    __syncthreads();
     for (int e = tid; e < m * nb; e += blockDim.x) {
         int rr = e / nb, q = e % nb;
         A[(int64_t)(c0 + rr) * s + c0 + q] = s_pan32[rr * PS + q];
@@ -574,6 +591,7 @@ struct GmresCtx {
     const DevConRow *crows;
     const float2 *lu;
     const int32_t *piv;
+    const int32_t *perm = nullptr;  // the row permutation of piv, if built (then P in = in[perm])
     cx *t;  // rows
 };
 
@@ -599,43 +617,55 @@ __device__ double block_sum(double v, double *red) {
 }
 
 // out = M^H (M v) + lambda v   (v, out: S).  v and the row vector t are
-// staged in shared memory (sv: S, st: rows) so the two passes over Z only
-// wait on Z itself.
-__device__ void apply_A(const GmresCtx &g, const cx *v, cx *out, cx *sv, cx *st) {
-    int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5, nw = blockDim.x >> 5;
+// staged in shared memory (sv: S, st: rows; so: N accumulators).  Z is
+// streamed once from HBM: each block of ARB rows is first reduced into
+// t (a warp per row) and then, right away and still in L1/L2, folded into
+// the column sums M^H t (a thread per column), so the second use of every
+// row costs no HBM traffic.
+constexpr int ARB = 16;  // rows per block (2 per warp)
+__device__ void apply_A(const GmresCtx &g, const cx *v, cx *out, cx *sv, cx *st, cx *so) {
+    int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int n = g.n;
     for (int i = tid; i < g.s; i += blockDim.x) sv[i] = v[i];
+    for (int c = tid; c < n; c += blockDim.x) so[c] = {0, 0};
     __syncthreads();
-    for (int r = wid; r < g.n; r += nw) {
-        cx acc = {0, 0};
-        const cx *zr = g.z + (int64_t)r * g.n;
+    for (int rb = 0; rb < n; rb += ARB) {
+        for (int r = rb + wid; r < rb + ARB && r < n; r += 8) {
+            cx acc = {0, 0};
+            const cx *zr = g.z + (int64_t)r * n;
 #pragma unroll 4
-        for (int c = lane; c < g.n; c += 32) acc = zadd(acc, zmul(zr[c], sv[c]));
-        acc = warp_sum(acc);
-        if (lane == 0) {
-            cx cvv = sv[g.n + g.rowwire[r]];
-            st[r] = {acc.re - g.cv[r] * cvv.re, acc.im - g.cv[r] * cvv.im};
+            for (int c = lane; c < n; c += 32) acc = zadd(acc, zmul(zr[c], sv[c]));
+            acc = warp_sum(acc);
+            if (lane == 0) {
+                cx cvv = sv[n + g.rowwire[r]];
+                st[r] = {acc.re - g.cv[r] * cvv.re, acc.im - g.cv[r] * cvv.im};
+            }
         }
+        __syncthreads();
+        const int re = min(rb + ARB, n);
+        for (int c = tid; c < n; c += blockDim.x) {
+            const cx *zc = g.z + (int64_t)rb * n + c;
+            cx a0 = so[c], a1 = {0, 0};
+            int r = rb;
+#pragma unroll 4
+            for (; r + 2 <= re; r += 2, zc += 2 * (int64_t)n) {
+                a0 = zadd(a0, zcmul(zc[0], st[r]));
+                a1 = zadd(a1, zcmul(zc[n], st[r + 1]));
+            }
+            if (r < re) a0 = zadd(a0, zcmul(zc[0], st[r]));
+            so[c] = zadd(a0, a1);
+        }
+        // no barrier: st rows of the next block are disjoint, and so[c] is
+        // only ever touched by the thread that owns column c
     }
     for (int q = tid; q < g.nc; q += blockDim.x) {
         DevConRow c = g.crows[q];
         cx val = sv[c.c0];
         if (c.c1 >= 0) val = zadd(val, zscale(sv[c.c1], c.v1));
-        st[g.n + q] = val;
+        st[n + q] = val;
     }
     __syncthreads();
-    for (int c = tid; c < g.n; c += blockDim.x) {
-        cx a0 = {0, 0}, a1 = {0, 0}, a2 = {0, 0}, a3 = {0, 0};
-        int r = 0;
-        for (; r + 4 <= g.n; r += 4) {
-            a0 = zadd(a0, zcmul(g.z[(int64_t)r * g.n + c], st[r]));
-            a1 = zadd(a1, zcmul(g.z[(int64_t)(r + 1) * g.n + c], st[r + 1]));
-            a2 = zadd(a2, zcmul(g.z[(int64_t)(r + 2) * g.n + c], st[r + 2]));
-            a3 = zadd(a3, zcmul(g.z[(int64_t)(r + 3) * g.n + c], st[r + 3]));
-        }
-        for (; r < g.n; ++r) a0 = zadd(a0, zcmul(g.z[(int64_t)r * g.n + c], st[r]));
-        cx acc = zadd(zadd(a0, a1), zadd(a2, a3));
-        out[c] = zadd(acc, zscale(sv[c], 1e-8));
-    }
+    for (int c = tid; c < n; c += blockDim.x) out[c] = zadd(so[c], zscale(sv[c], 1e-8));
     for (int w = tid; w < g.w; w += blockDim.x) {
         cx acc = {0, 0};
         for (int q = g.wptr[w]; q < g.wptr[w + 1]; ++q) {
@@ -668,17 +698,21 @@ __device__ __forceinline__ cx f2z(float2 a) { return {(double)a.x, (double)a.y};
 __device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, cx *sy) {
     int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     int s = g.s;
-    for (int i = tid; i < s; i += blockDim.x) sy[i] = in[i];
-    __syncthreads();
-    if (tid == 0)
-        for (int c = 0; c < s; ++c) {
-            int p = g.piv[c];
-            if (p != c) {
-                cx t0 = sy[c];
-                sy[c] = sy[p];
-                sy[p] = t0;
+    if (g.perm) {
+        for (int i = tid; i < s; i += blockDim.x) sy[i] = in[g.perm[i]];
+    } else {
+        for (int i = tid; i < s; i += blockDim.x) sy[i] = in[i];
+        __syncthreads();
+        if (tid == 0)
+            for (int c = 0; c < s; ++c) {
+                int p = g.piv[c];
+                if (p != c) {
+                    cx t0 = sy[c];
+                    sy[c] = sy[p];
+                    sy[p] = t0;
+                }
             }
-        }
+    }
     __syncthreads();
     // forward: unit lower triangular (factor rows read 8 entries at a time
     // to keep the register footprint small enough for several CTAs per SM)
@@ -777,7 +811,8 @@ __global__ void __launch_bounds__(256, 3) k_gmres_ir(const UnitDesc *__restrict_
                                                   const cx *__restrict__ rhs, const double *__restrict__ cosv,
                                                   const float2 *__restrict__ a32buf, const int32_t *__restrict__ pivbuf,
                                                   cx *xbuf, cx *vbuf, cx *wbuf, const int32_t *__restrict__ status,
-                                                  int staged, int skip_s, int only, int min_s) {
+                                                  int staged, int skip_s, int only, int min_s,
+                                                  const int32_t *__restrict__ s_order) {
     extern __shared__ unsigned char s_dyn[];
     __shared__ cx sH[(GM + 1) * GM];
     __shared__ double scs[GM];
@@ -786,7 +821,7 @@ __global__ void __launch_bounds__(256, 3) k_gmres_ir(const UnitDesc *__restrict_
     __shared__ cx sh[GM + 1];
     __shared__ double red[8];
     __shared__ int s_stop;
-    int ui = blockIdx.x;  // one solve (right-hand side)
+    int ui = s_order ? s_order[blockIdx.x] : (int)blockIdx.x;  // one solve (right-hand side)
     UnitDesc u = units[ui];
     if (status[u.sys] != 0 || u.s >= skip_s || u.s < min_s) return;  // refined grid-wide / by clusters
     if (only >= 0 && ui != only) return;
@@ -817,6 +852,24 @@ __global__ void __launch_bounds__(256, 3) k_gmres_ir(const UnitDesc *__restrict_
     cx *sv = staged ? reinterpret_cast<cx *>(s_dyn) : W + 4 * s + g.rows;
     cx *stv = sv + s;
     cx *sy = stv + g.rows;
+    if (staged) {
+        // the pivots' row permutation, built once: each preconditioner
+        // application then gathers in parallel instead of swapping serially
+        int32_t *perm = reinterpret_cast<int32_t *>(sy + s);
+        for (int i = tid; i < s; i += blockDim.x) perm[i] = i;
+        __syncthreads();
+        if (tid == 0)
+            for (int c = 0; c < s; ++c) {
+                int p = g.piv[c];
+                if (p != c) {
+                    int t0 = perm[c];
+                    perm[c] = perm[p];
+                    perm[p] = t0;
+                }
+            }
+        __syncthreads();
+        g.perm = perm;
+    }
 
     // b = M^H y (y is zero on the constraint rows)
     for (int i = tid; i < g.rows; i += blockDim.x) g.t[i] = i < g.n ? g.y[i] : cx{0, 0};
@@ -837,7 +890,7 @@ __global__ void __launch_bounds__(256, 3) k_gmres_ir(const UnitDesc *__restrict_
     int iters = 0;
     double rel = 1.0;
     for (int outer = 0; outer < MAX_OUTER; ++outer) {
-        apply_A(g, x, w, sv, stv);
+        apply_A(g, x, w, sv, stv, sy);
         for (int i = tid; i < s; i += blockDim.x) r[i] = zsub(b[i], w[i]);
         __syncthreads();
         apply_prec(g, r, V, sy);
@@ -854,7 +907,7 @@ __global__ void __launch_bounds__(256, 3) k_gmres_ir(const UnitDesc *__restrict_
         int jend = GM - 1;
         for (int j = 0; j < GM; ++j) {
             cx *vj = V + (int64_t)j * s, *vn = V + (int64_t)(j + 1) * s;
-            apply_A(g, vj, w, sv, stv);
+            apply_A(g, vj, w, sv, stv, sy);
             apply_prec(g, w, vn, sy);
             // classical Gram-Schmidt, twice
             if (tid <= j) sh[tid] = {0, 0};
@@ -1569,10 +1622,18 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
     size_t b_v = sizeof(cx) * (size_t)(v + 1);
     size_t b_w = sizeof(cx) * (size_t)(wk + 1);
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
-    size_t total = al(b_mu) + al(b_smu) + al(b_a32) + al(b_v) + al(b_w);
+    size_t b_ord = sizeof(int32_t) * (solves.size() + 1);
+    size_t total = al(b_mu) + al(b_smu) + al(b_a32) + al(b_v) + al(b_w) + al(b_ord);
     cudaError_t e = dev.alloc(&w.base, total);
     if (e != cudaSuccess) return e;
     unsigned char *p = (unsigned char *)w.base;
+    // refinement CTAs take the largest solves first (longest-first
+    // scheduling shortens the tail of the one-launch refinement)
+    std::vector<int32_t> lpt(solves.size());
+    for (size_t i = 0; i < lpt.size(); ++i) lpt[i] = (int32_t)i;
+    std::stable_sort(lpt.begin(), lpt.end(), [&](int32_t x, int32_t y) {
+        return (int64_t)solves[x].n * solves[x].n > (int64_t)solves[y].n * solves[y].n;
+    });
     w.mu = (MixedUnit *)p;
     p += al(b_mu);
     w.smu = (MixedUnit *)p;
@@ -1582,6 +1643,8 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
     w.v = (cx *)p;
     p += al(b_v);
     w.w = (cx *)p;
+    p += al(b_w);
+    w.s_order = (int32_t *)p;
     w.bytes = total;
     w.n_units = (int)solves.size();
     w.max_s = max_s;
@@ -1687,7 +1750,8 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
             delete p;
         }
     }
-    e = dev.upload(w.mu, mu.data(), sizeof(MixedUnit) * mu.size());
+    e = dev.upload(w.s_order, lpt.data(), sizeof(int32_t) * lpt.size());
+    if (e == cudaSuccess) e = dev.upload(w.mu, mu.data(), sizeof(MixedUnit) * mu.size());
     if (e == cudaSuccess)
         e = dev.upload(w.smu, sysmu.data(), sizeof(MixedUnit) * sysmu.size());
     return e;
@@ -1740,7 +1804,8 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     mark(1);
     static bool attr = false, attr_grid = false;
     if (!attr) {
-        cudaFuncSetAttribute(k_panel32_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, PANEL32_SMEM_MAX);
+        cudaFuncSetAttribute(k_panel32_smem<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, PANEL32_SMEM_MAX);
+        cudaFuncSetAttribute(k_panel32_smem<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, PANEL32_SMEM_MAX);
         attr = true;
     }
     if (!attr_grid) {
@@ -1777,8 +1842,13 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         }
         step_classes(gp, c0, n_thr, cls);
         for (const StepClass &c : cls) {
-            k_panel32_smem<<<c.i1 - c.i0, 256, sizeof(float2) * (size_t)c.m_max * (MNB + 1), st>>>(
-                d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX, ord, c.i0);
+            const size_t psm = sizeof(float2) * (size_t)c.m_max * (MNB + 1);
+            if (c.m_max > 256)
+                k_panel32_smem<1024><<<c.i1 - c.i0, 1024, psm, st>>>(d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX,
+                                                                   ord, c.i0);
+            else
+                k_panel32_smem<256><<<c.i1 - c.i0, 256, psm, st>>>(d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX,
+                                                                 ord, c.i0);
             ++L;
         }
         step_classes(gp, c0, 0, cls);
@@ -1799,7 +1869,7 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     mark(2);
     int max_rows = 0;
     for (size_t i = 0; i < mw.host.size(); ++i) max_rows = max_rows > mw.host[i].rows ? max_rows : mw.host[i].rows;
-    size_t smem = sizeof(cx) * (size_t)(2 * max_s + max_rows);
+    size_t smem = sizeof(cx) * (size_t)(2 * max_s + max_rows) + sizeof(int32_t) * (size_t)max_s;  // + perm
     int staged = smem <= 200 * 1024;
     if (staged && smem > 0) {  // static + dynamic above 48 KB needs the raised limit
         int lim = set_smem_limit_once(k_gmres_ir, 200 * 1024);
@@ -1834,7 +1904,7 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     }
     if (ns > 0) {
         k_gmres_ir<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x, mw.v,
-                                          mw.w, status, staged, skip_s, -1, min_s);
+                                          mw.w, status, staged, skip_s, -1, min_s, mw.s_order);
         cudaError_t le = cudaPeekAtLastError();
         if (le != cudaSuccess && !marks.detail[0])
             std::snprintf(marks.detail, sizeof(marks.detail), "GMRES launch: %d solves, %zu B shared (%s), max_s %d, rows %d",
@@ -1867,7 +1937,7 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
                     cudaSuccess) {
                 (void)cudaGetLastError();  // not co-resident: refine this solve in one CTA
                 k_gmres_ir<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x,
-                                                  mw.v, mw.w, status, staged, INT_MAX, ui, 0);
+                                                  mw.v, mw.w, status, staged, INT_MAX, ui, 0, mw.s_order);
             }
             L += 2;
         }

@@ -29,6 +29,7 @@ struct MixedWork {
     MixedUnit *mu = nullptr;   // per solve
     MixedUnit *smu = nullptr;  // per system (a32_off only)
     float2 *a32 = nullptr;
+    int32_t *s_order = nullptr;  // solves by decreasing N^2 (refinement launch order)
     cx *v = nullptr;
     cx *w = nullptr;
     int n_units = 0;

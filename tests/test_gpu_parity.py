@@ -58,7 +58,10 @@ def _check_unit(acc, batch, res, u, wires, sources, ground, freq, pts):
     else:
         assert np.abs(cur - p.currents).max() / peak <= CUR_TOL
     _, piv = batch.read_unit(u)
-    assert np.array_equal(piv, p.pivots)
+    # the oracle's pivot buffer has room for n + (GW cards) rows; the solve
+    # uses n + (columns): merged wires, or conductor paths in the path form
+    assert len(piv) == batch.units[u]["s"] <= len(p.pivots)
+    assert np.array_equal(piv, p.pivots[: len(piv)])
     if pts is not None:
         g = res.pattern[u][:, :4]
         ref = p.pattern
