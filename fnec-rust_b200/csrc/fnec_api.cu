@@ -535,7 +535,7 @@ struct fnec_batch {
     cudaEvent_t ev[FNEC_N_PHASES + 1] = {};
     bool ev_made = false;
     // schedule and its CUDA graph
-    fnec_schedule sched = {1, 1, 1, 1, 1, 1};
+    fnec_schedule sched = {1, 1, 1, 1, 1, 1, 1, 1};
     cudaGraphExec_t gexec = nullptr;
     int graph_state = FNEC_GRAPH_NONE;
     uint64_t graph_launches = 0;  // launches the graph replays
@@ -1445,7 +1445,8 @@ static bool schedule_valid(const fnec_schedule &s) {
     auto bit = [](int32_t v) { return v == 0 || v == 1; };
     return bit(s.grid_panels) && (s.class_shift == 1 || s.class_shift == 2) && bit(s.gram_tensor) &&
            (s.gmres_cluster == 1 || s.gmres_cluster == 2 || s.gmres_cluster == 4 || s.gmres_cluster == 8) &&
-           bit(s.grid_gmres) && s.graph >= 0 && s.graph <= 2;
+           bit(s.grid_gmres) && s.graph >= 0 && s.graph <= 2 &&
+           (s.factor_streams == 1 || s.factor_streams == 2 || s.factor_streams == 4) && bit(s.unit_factor);
 }
 
 // Make the batch launch as s says (s valid); drops a captured graph when
@@ -1455,7 +1456,8 @@ static void apply_schedule(fnec_batch *b, const fnec_schedule &s) {
     if (t.gmres_cluster > b->mixed.cluster_max) t.gmres_cluster = b->mixed.cluster_max;
     const bool same_launches = t.grid_panels == b->sched.grid_panels && t.class_shift == b->sched.class_shift &&
                                t.gram_tensor == b->sched.gram_tensor && t.gmres_cluster == b->sched.gmres_cluster &&
-                               t.grid_gmres == b->sched.grid_gmres;
+                               t.grid_gmres == b->sched.grid_gmres && t.factor_streams == b->sched.factor_streams &&
+                               t.unit_factor == b->sched.unit_factor;
     if (!same_launches || (t.graph == 0) != (b->sched.graph == 0)) drop_graph(b);
     b->sched = t;
     b->grid.grid_on = t.grid_panels != 0;
@@ -1463,6 +1465,8 @@ static void apply_schedule(fnec_batch *b, const fnec_schedule &s) {
     b->mixed.use_tc = t.gram_tensor != 0;
     b->mixed.cluster_c = t.gmres_cluster < 1 ? 1 : t.gmres_cluster;
     b->mixed.grid_on = t.grid_gmres != 0;
+    b->grid.factor_streams = t.factor_streams;
+    b->grid.unit_factor = t.unit_factor != 0;
 }
 
 static int ceil_log2(int64_t v) {
@@ -1611,6 +1615,9 @@ int fnec_batch_tune(fnec_batch *b, uint32_t reps, fnec_tune_report *out) {
     if (mixed && !b->mixed.grid_solves.empty()) knobs.push_back({&fnec_schedule::grid_gmres, {1, 0}});
     if (b->grid.d_xchg) knobs.push_back({&fnec_schedule::grid_panels, {1, 0}});
     if (b->units.size() > 1) knobs.push_back({&fnec_schedule::class_shift, {1, 2}});
+    if (mixed && !b->grid.s_desc.empty() && b->grid.s_desc.back() <= 256)
+        knobs.push_back({&fnec_schedule::unit_factor, {1, 0}});
+    if (mixed && b->mixed.fmade) knobs.push_back({&fnec_schedule::factor_streams, {1, 2, 4}});
     for (const Knob &k : knobs) {
         for (int32_t v : k.v) {
             if (best.*(k.f) == v) continue;
@@ -1640,10 +1647,13 @@ int fnec_batch_tune(fnec_batch *b, uint32_t reps, fnec_tune_report *out) {
     return FNEC_OK;
 }
 
-static const char *const SCHED_FIELDS[] = {"grid_panels", "class_shift", "gram_tensor",
-                                           "gmres_cluster", "grid_gmres", "graph"};
+constexpr int N_SCHED_FIELDS = 8;
+static const char *const SCHED_FIELDS[N_SCHED_FIELDS] = {"grid_panels", "class_shift", "gram_tensor",
+                                                         "gmres_cluster", "grid_gmres", "graph",
+                                                         "factor_streams", "unit_factor"};
 static int32_t *sched_field(fnec_schedule &s, int i) {
-    int32_t *f[] = {&s.grid_panels, &s.class_shift, &s.gram_tensor, &s.gmres_cluster, &s.grid_gmres, &s.graph};
+    int32_t *f[N_SCHED_FIELDS] = {&s.grid_panels, &s.class_shift, &s.gram_tensor,    &s.gmres_cluster,
+                                  &s.grid_gmres,  &s.graph,       &s.factor_streams, &s.unit_factor};
     return f[i];
 }
 
@@ -1655,7 +1665,7 @@ int fnec_tune_cache_save(const char *path) {
     for (auto &kv : g_tune_cache) {
         fnec_schedule s = kv.second;
         std::fprintf(f, "%s", kv.first.c_str());
-        for (int i = 0; i < 6; ++i) std::fprintf(f, " %s=%d", SCHED_FIELDS[i], (int)*sched_field(s, i));
+        for (int i = 0; i < N_SCHED_FIELDS; ++i) std::fprintf(f, " %s=%d", SCHED_FIELDS[i], (int)*sched_field(s, i));
         std::fprintf(f, "\n");
     }
     return std::fclose(f) == 0 ? FNEC_OK : FNEC_ERR_BAD_ARG;
@@ -1673,7 +1683,7 @@ int fnec_tune_cache_load(const char *path) {
         char *tok = strtok_r(line, " \t\r\n", &save);
         if (!tok || tok[0] == '#') continue;
         std::string key = tok;
-        fnec_schedule s = {1, 1, 1, 1, 1, 1};
+        fnec_schedule s = {1, 1, 1, 1, 1, 1, 1, 1};
         int seen = 0;
         while ((tok = strtok_r(nullptr, " \t\r\n", &save))) {
             char *eq = std::strchr(tok, '=');
@@ -1683,15 +1693,15 @@ int fnec_tune_cache_load(const char *path) {
             }
             *eq = 0;
             int i = 0;
-            while (i < 6 && std::strcmp(tok, SCHED_FIELDS[i]) != 0) ++i;
-            if (i == 6) {
+            while (i < N_SCHED_FIELDS && std::strcmp(tok, SCHED_FIELDS[i]) != 0) ++i;
+            if (i == N_SCHED_FIELDS) {
                 rc = FNEC_ERR_BAD_ARG;
                 break;
             }
             *sched_field(s, i) = (int32_t)std::atoi(eq + 1);
             seen |= 1 << i;
         }
-        if (rc != FNEC_OK || seen != 0x3f || !schedule_valid(s)) {
+        if (rc != FNEC_OK || seen != (1 << N_SCHED_FIELDS) - 1 || !schedule_valid(s)) {
             rc = FNEC_ERR_BAD_ARG;
             break;
         }

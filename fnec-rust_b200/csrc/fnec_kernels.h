@@ -65,6 +65,8 @@ struct GridPlan {
     // schedule (set per batch, the autotuner's choices)
     bool grid_on = true;         // tall panels grid-wide (else one CTA from global memory)
     int class_shift = 1;         // size classes of panel heights: (2^k x lo, hi]
+    int factor_streams = 1;      // mixed factor: groups of units factored on concurrent streams
+    bool unit_factor = true;     // mixed factor: small units factored whole, one CTA each
 };
 size_t grid_xchg_bytes();        // bytes of d_xchg
 size_t grid_sync_bytes(int steps);
@@ -75,7 +77,8 @@ size_t grid_sync_bytes(int steps);
 struct StepClass {
     int i0, i1, m_max;
 };
-void step_classes(const GridPlan &gp, int c0, int i_begin, std::vector<StepClass> &out);
+// i_end >= 0 stops at that position of the order.
+void step_classes(const GridPlan &gp, int c0, int i_begin, std::vector<StepClass> &out, int i_end = -1);
 // A cooperative launch (every CTA co-resident) issued through
 // cudaLaunchKernelExC so that stream capture records it as a cooperative
 // kernel node.

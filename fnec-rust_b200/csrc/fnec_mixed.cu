@@ -348,38 +348,29 @@ __global__ void __launch_bounds__(256) k_panel32(const UnitDesc *__restrict__ un
 // The FP32 panel held in shared memory (rows c0..s-1, MNB columns).
 constexpr int PANEL32_SMEM_MAX = 200 * 1024;
 
-// NT threads: 256, or 1024 for tall panels (fewer rows per warp on the
-// column-serial critical path of the largest units).
+// The FP32 panel of one unit (rows c0..s-1, MNB columns) factored from
+// shared memory by a CTA of NT threads: pivot search, row swap, and
+// elimination with the pivot's reciprocal, a warp per row.  The next
+// column's pivot search is folded into each elimination pass (the tie rule
+// is order-free).  Writes the panel and its pivots back to global memory;
+// returns false (with the unit's status set) for a singular panel.
 template <int NT>
-__global__ void __launch_bounds__(NT) k_panel32_smem(const UnitDesc *__restrict__ units,
-                                                     const MixedUnit *__restrict__ mus, int c0, float2 *a32buf,
-                                                     int32_t *piv_buf, int32_t *status, int skip_m, const int32_t *__restrict__ order, int base) {
+__device__ bool panel32_body(float2 *A, int s, int c0, int32_t *piv, int32_t *status_u, float2 *s_pan32,
+                             float *s_v, int *s_i, int *s_p) {
     // panel rows padded to PS = MNB + 1 entries: a column read by consecutive
     // rows then falls on distinct banks
     constexpr int PS = MNB + 1;
-    extern __shared__ float2 s_pan32[];
-    __shared__ float s_v[NT / 32];
-    __shared__ int s_i[NT / 32];
-    __shared__ int s_p;
-    int ui = order[base + blockIdx.x];
-    UnitDesc u = units[ui];
-    int s = u.s;
-    if (c0 >= s || s - c0 > skip_m || status[ui] != 0) return;  // skip_m: taller panels go grid-wide
-    float2 *A = a32buf + mus[ui].a32_off;
-    int32_t *piv = piv_buf + u.piv_off;
+    constexpr int nw = NT / 32;
     int nb = min(MNB, s - c0), m = s - c0;
     int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
-    const int nw = blockDim.x >> 5;
-    for (int e = tid; e < m * nb; e += blockDim.x) {
+    for (int e = tid; e < m * nb; e += NT) {
         int rr = e / nb, q = e % nb;
         s_pan32[rr * PS + q] = A[(int64_t)(c0 + rr) * s + c0 + q];
     }
     __syncthreads();
-    // pivot candidates of the first column; later columns get theirs from
-    // the elimination pass of the column before (the tie rule is order-free)
     float bv = -1.f;
     int bi = -1;
-    for (int r = c0 + tid; r < s; r += blockDim.x) {
+    for (int r = c0 + tid; r < s; r += NT) {
         float2 v = s_pan32[(r - c0) * PS];
         piv_better32(bv, bi, v.x * v.x + v.y * v.y, r);
     }
@@ -401,24 +392,21 @@ __global__ void __launch_bounds__(NT) k_panel32_smem(const UnitDesc *__restrict_
             int p = s_i[0];
             for (int q = 1; q < nw; ++q) piv_better32(v, p, s_v[q], s_i[q]);
             if (p < 0 || !(v > 0.f)) {
-                status[ui] = -(c + 1);
+                *status_u = -(c + 1);
                 p = -1;
             }
-            s_p = p;
+            *s_p = p;
             piv[c] = p;
         }
         __syncthreads();
-        int p = s_p;
-        if (p < 0) return;
+        int p = *s_p;
+        if (p < 0) return false;
         if (p != c && tid < nb) {
             float2 t0 = s_pan32[lc * PS + tid];
             s_pan32[lc * PS + tid] = s_pan32[(p - c0) * PS + tid];
             s_pan32[(p - c0) * PS + tid] = t0;
         }
         __syncthreads();
-        // elimination: a warp per row, a lane per panel column; the
-        // multiplier is x times the pivot's reciprocal (one division per
-        // column), and the updated next column feeds its pivot search
         const float2 pj = lane < nb ? s_pan32[lc * PS + lane] : cf(0.f, 0.f);
         const float2 diag = s_pan32[lc * PS + lc];
         const float dn = 1.0f / (diag.x * diag.x + diag.y * diag.y);
@@ -441,9 +429,145 @@ __global__ void __launch_bounds__(NT) k_panel32_smem(const UnitDesc *__restrict_
         // column's reads of it
     }
     __syncthreads();
-    for (int e = tid; e < m * nb; e += blockDim.x) {
+    for (int e = tid; e < m * nb; e += NT) {
         int rr = e / nb, q = e % nb;
         A[(int64_t)(c0 + rr) * s + c0 + q] = s_pan32[rr * PS + q];
+    }
+    return true;
+}
+
+// The panel step of every unit of a size class, one CTA of NT threads per
+// unit: 256, or 1024 for tall panels (fewer rows per warp on the
+// column-serial critical path of the largest units).
+template <int NT>
+__global__ void __launch_bounds__(NT) k_panel32_smem(const UnitDesc *__restrict__ units,
+                                                     const MixedUnit *__restrict__ mus, int c0, float2 *a32buf,
+                                                     int32_t *piv_buf, int32_t *status, int skip_m, const int32_t *__restrict__ order, int base) {
+    extern __shared__ float2 s_pan32[];
+    __shared__ float s_v[NT / 32];
+    __shared__ int s_i[NT / 32];
+    __shared__ int s_p;
+    int ui = order[base + blockIdx.x];
+    UnitDesc u = units[ui];
+    int s = u.s;
+    if (c0 >= s || s - c0 > skip_m || status[ui] != 0) return;  // skip_m: taller panels go grid-wide
+    panel32_body<NT>(a32buf + mus[ui].a32_off, s, c0, piv_buf + u.piv_off, &status[ui], s_pan32, s_v, s_i, &s_p);
+}
+
+// The whole FP32 blocked GEPP of one small unit (S <= FU_MAX_S) per CTA:
+// the panel, swap/U12 and trailing steps of the per-step kernels
+// (k_panel32_smem, k_swap_u12_32, k_trailing32) with the same per-element
+// operations in the same order -- so the factor is bit-identical -- but
+// without a kernel boundary or a global round trip between steps.
+constexpr int FU_MAX_S = 256;
+constexpr int FU_THREADS = 256;
+constexpr size_t FU_SMEM = sizeof(float2) * (size_t)(MNB * (MNB + 1) + MNB * FU_THREADS);  // swap stage, the largest
+
+__global__ void __launch_bounds__(FU_THREADS, 3) k_factor32_unit(const UnitDesc *__restrict__ units,
+                                                                const MixedUnit *__restrict__ mus, float2 *a32buf,
+                                                                int32_t *piv_buf, int32_t *status,
+                                                                const int32_t *__restrict__ order, int base) {
+    extern __shared__ float2 s_fu[];
+    __shared__ float s_v[FU_THREADS / 32];
+    __shared__ int s_i[FU_THREADS / 32];
+    __shared__ int s_p;
+    const int ui = order[base + blockIdx.x];
+    const UnitDesc u = units[ui];
+    const int s = u.s;
+    if (status[ui] != 0) return;
+    float2 *A = a32buf + mus[ui].a32_off;
+    int32_t *piv = piv_buf + u.piv_off;
+    const int tid = threadIdx.x;
+    for (int c0 = 0; c0 < s; c0 += MNB) {
+        if (!panel32_body<FU_THREADS>(A, s, c0, piv, &status[ui], s_fu, s_v, s_i, &s_p)) return;
+        __syncthreads();
+        // row swaps on every column outside the panel, U12 = L11^-1 A12 on
+        // the trailing ones (as k_swap_u12_32, a thread per column)
+        const int nb = min(MNB, s - c0);
+        float2(*s_L)[MNB + 1] = reinterpret_cast<float2(*)[MNB + 1]>(s_fu);
+        float2(*s_c)[FU_THREADS] = reinterpret_cast<float2(*)[FU_THREADS]>(s_fu + MNB * (MNB + 1));
+        for (int e = tid; e < nb * nb; e += FU_THREADS) s_L[e / nb][e % nb] = A[(int64_t)(c0 + e / nb) * s + c0 + e % nb];
+        __syncthreads();
+        for (int k0 = 0; k0 < s - nb; k0 += FU_THREADS) {
+            const int idx = k0 + tid;
+            const int K = idx < c0 ? idx : idx + nb;  // skip the panel columns
+            if (K < s) {
+                const bool trailing = K >= c0 + nb;
+                for (int q = 0; q < nb; ++q) s_c[q][tid] = A[(int64_t)(c0 + q) * s + K];
+                for (int q = 0; q < nb; ++q) {
+                    int p = piv[c0 + q];
+                    if (p == c0 + q) continue;
+                    if (p < c0 + nb) {
+                        float2 t0 = s_c[q][tid];
+                        s_c[q][tid] = s_c[p - c0][tid];
+                        s_c[p - c0][tid] = t0;
+                    } else {
+                        float2 t0 = s_c[q][tid];
+                        s_c[q][tid] = A[(int64_t)p * s + K];
+                        A[(int64_t)p * s + K] = t0;
+                    }
+                }
+                if (trailing)
+                    for (int q = 1; q < nb; ++q) {
+                        float2 v = s_c[q][tid];
+                        for (int c = 0; c < q; ++c) v = cf_sub(v, cf_mul(s_L[q][c], s_c[c][tid]));
+                        s_c[q][tid] = v;
+                    }
+                for (int q = 0; q < nb; ++q) A[(int64_t)(c0 + q) * s + K] = s_c[q][tid];
+            }
+        }
+        __syncthreads();
+        // trailing update A22 -= L21 U12 (as k_trailing32, 64x64 tiles)
+        if (c0 + MNB < s) {
+            const int r0 = c0 + MNB, rows = s - r0;
+            const int tiles = (rows + 63) / 64;
+            float2(*s_l)[MNB + 1] = reinterpret_cast<float2(*)[MNB + 1]>(s_fu);
+            float2(*s_u)[64] = reinterpret_cast<float2(*)[64]>(s_fu + 64 * (MNB + 1));
+            const int ty = tid / 16, tx = tid % 16;
+            for (int tile = 0; tile < tiles * tiles; ++tile) {
+                const int R0 = r0 + (tile / tiles) * 64, K0 = r0 + (tile % tiles) * 64;
+                for (int e = tid; e < 64 * MNB; e += FU_THREADS) {
+                    int rr = e / MNB, q = e % MNB, R = R0 + rr;
+                    s_l[rr][q] = (R < s) ? A[(int64_t)R * s + c0 + q] : cf(0.f, 0.f);
+                }
+                for (int e = tid; e < MNB * 64; e += FU_THREADS) {
+                    int q = e / 64, cc = e % 64, K = K0 + cc;
+                    s_u[q][cc] = (K < s) ? A[(int64_t)(c0 + q) * s + K] : cf(0.f, 0.f);
+                }
+                __syncthreads();
+                float2 acc[4][4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        int R = R0 + ty + 16 * a, K = K0 + tx + 16 * b;
+                        acc[a][b] = (R < s && K < s) ? A[(int64_t)R * s + K] : cf(0.f, 0.f);
+                    }
+#pragma unroll 4
+                for (int q = 0; q < MNB; ++q) {
+                    float2 lv[4], uv[4];
+#pragma unroll
+                    for (int a = 0; a < 4; ++a) lv[a] = s_l[ty + 16 * a][q];
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) uv[b] = s_u[q][tx + 16 * b];
+#pragma unroll
+                    for (int a = 0; a < 4; ++a)
+#pragma unroll
+                        for (int b = 0; b < 4; ++b) {
+                            acc[a][b].x = fmaf(-lv[a].x, uv[b].x, fmaf(lv[a].y, uv[b].y, acc[a][b].x));
+                            acc[a][b].y = fmaf(-lv[a].x, uv[b].y, fmaf(-lv[a].y, uv[b].x, acc[a][b].y));
+                        }
+                }
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        int R = R0 + ty + 16 * a, K = K0 + tx + 16 * b;
+                        if (R < s && K < s) A[(int64_t)R * s + K] = acc[a][b];
+                    }
+                __syncthreads();
+            }
+        }
     }
 }
 
@@ -1750,6 +1874,15 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
             delete p;
         }
     }
+    if (systems.size() >= 4 && !w.fmade) {  // concurrent factor groups
+        bool ok = true;
+        for (int g = 0; g + 1 < MixedWork::MAX_FACTOR_STREAMS && ok; ++g)
+            ok = cudaStreamCreateWithFlags(&w.fstream[g], cudaStreamNonBlocking) == cudaSuccess;
+        for (int g = 0; g < MixedWork::MAX_FACTOR_STREAMS && ok; ++g)
+            ok = cudaEventCreateWithFlags(&w.fevent[g], cudaEventDisableTiming) == cudaSuccess;
+        w.fmade = ok;
+        if (!ok) (void)cudaGetLastError();  // one stream: the groups run in sequence
+    }
     e = dev.upload(w.s_order, lpt.data(), sizeof(int32_t) * lpt.size());
     if (e == cudaSuccess) e = dev.upload(w.mu, mu.data(), sizeof(MixedUnit) * mu.size());
     if (e == cudaSuccess)
@@ -1758,6 +1891,11 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
 }
 
 void free_mixed(MixedWork &w, const DevAlloc &dev) {
+    for (auto &s : w.fstream)
+        if (s) cudaStreamDestroy(s), s = nullptr;
+    for (auto &e : w.fevent)
+        if (e) cudaEventDestroy(e), e = nullptr;
+    w.fmade = false;
     dev.release(w.base);
     dev.release(w.grid_base);
     dev.release(w.tc_base);
@@ -1815,17 +1953,67 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     const int thr_rows = PANEL32_SMEM_MAX / (int)((MNB + 1) * sizeof(float2));
     const int32_t *ord = gp.d_order;
     if (gp.d_sync) cudaMemsetAsync(gp.d_sync, 0, grid_sync_bytes(gp.steps), st);
+    // Units (in decreasing s) are split into up to factor_streams groups of
+    // about equal work (sum of s^3), each factored on its own stream: the
+    // column-serial panel chain of the tallest units then overlaps the
+    // many short units' work instead of leaving the GPU idle.
+    const int nu_all = (int)gp.s_desc.size();
+    // units with S <= FU_MAX_S (the tail of the order) are factored whole,
+    // one CTA each, in one launch on a stream of their own
+    int i_unit = nu_all;
+    if (gp.unit_factor)
+        while (i_unit > 0 && gp.s_desc[i_unit - 1] <= FU_MAX_S) --i_unit;
+    const bool unit_launch = i_unit < nu_all;
+    int G = std::max(1, std::min(gp.factor_streams, MixedWork::MAX_FACTOR_STREAMS) - (unit_launch ? 1 : 0));
+    if (!mw.fmade || i_unit < 2 * G) G = 1;
+    std::vector<int> gb(1, 0);
+    if (G > 1) {
+        // units whose panels outgrow one CTA (grid-wide or global-memory
+        // panels, one exchange area) all stay in the first group
+        int n_tall = 0;
+        while (n_tall < i_unit && gp.s_desc[n_tall] > thr_rows) ++n_tall;
+        double tot = 0, acc = 0;
+        for (int i = 0; i < i_unit; ++i) tot += (double)gp.s_desc[i] * gp.s_desc[i] * gp.s_desc[i];
+        for (int i = 0; i < i_unit && (int)gb.size() < G; ++i) {
+            acc += (double)gp.s_desc[i] * gp.s_desc[i] * gp.s_desc[i];
+            if (acc >= tot * (double)gb.size() / G && i + 1 < i_unit && i + 1 >= n_tall) gb.push_back(i + 1);
+        }
+    }
+    gb.push_back(i_unit);
+    G = (int)gb.size() - 1;
+    // streams: the per-step groups on st, fstream[0..G-2]; the whole-unit
+    // launch on the next one (or st when there is no stream to spare)
+    const bool unit_own = unit_launch && mw.fmade && G - 1 < MixedWork::MAX_FACTOR_STREAMS - 1 && i_unit > 0;
+    const int n_side = (G - 1) + (unit_own ? 1 : 0);
+    if (n_side > 0) {
+        cudaEventRecord(mw.fevent[0], st);
+        for (int g = 0; g < n_side; ++g) cudaStreamWaitEvent(mw.fstream[g], mw.fevent[0], 0);
+    }
+    if (unit_launch) {
+        static bool fu_attr = false;
+        if (!fu_attr) {
+            cudaFuncSetAttribute(k_factor32_unit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FU_SMEM);
+            fu_attr = true;
+        }
+        cudaStream_t us = unit_own ? mw.fstream[G - 1] : st;
+        k_factor32_unit<<<nu_all - i_unit, FU_THREADS, FU_SMEM, us>>>(d_units, mw.smu, mw.a32, piv, status, ord, i_unit);
+        ++L;
+    }
     std::vector<StepClass> cls;
-    for (int c0 = 0; c0 < max_s; c0 += MNB) {
+    for (int grp = 0; grp < G && i_unit > 0; ++grp) {
+    const int gi0 = gb[grp], gi1 = gb[grp + 1];
+    cudaStream_t fs = grp == 0 ? st : mw.fstream[grp - 1];
+    for (int c0 = 0; gi0 < gi1 && c0 < gp.s_desc[gi0]; c0 += MNB) {
         // panels as in the plain path: tallest grid-wide (or one CTA from
         // global memory), the rest one CTA from shared memory per size class
-        int n_thr = 0;
-        while (n_thr < (int)gp.s_desc.size() && gp.s_desc[n_thr] - c0 > thr_rows) ++n_thr;
+        int n_thr = gi0;
+        while (n_thr < gi1 && gp.s_desc[n_thr] - c0 > thr_rows) ++n_thr;
+        n_thr -= gi0;  // only the first group (the tallest units) can have any
         if (n_thr > 0) {
-            int G = 0;
+            int Gp = 0;
             size_t gsm = 0;
             bool done = false;
-            if (plan_grid_panel(gp, c0, thr_rows, MNB, sizeof(float2), (const void *)k_panel32_grid, &G, &gsm) ==
+            if (plan_grid_panel(gp, c0, thr_rows, MNB, sizeof(float2), (const void *)k_panel32_grid, &Gp, &gsm) ==
                 n_thr) {
                 PanelXchg<float2> *xg = static_cast<PanelXchg<float2> *>(gp.d_xchg);
                 GridSync *gs = static_cast<GridSync *>(gp.d_sync) + (size_t)(c0 / MNB) * GRID_PANEL_MAX_UNITS;
@@ -1833,38 +2021,43 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
                 float2 *a32 = mw.a32;
                 void *args[] = {(void *)&d_units, (void *)&smu, (void *)&ord, (void *)&c0, (void *)&a32,
                                 (void *)&piv, (void *)&status, (void *)&xg, (void *)&gs};
-                done = launch_cooperative((const void *)k_panel32_grid, dim3(G, n_thr), dim3(256), args, gsm, st) ==
+                done = launch_cooperative((const void *)k_panel32_grid, dim3(Gp, n_thr), dim3(256), args, gsm, fs) ==
                        cudaSuccess;
                 if (!done) (void)cudaGetLastError();
             }
-            if (!done) k_panel32<<<n_thr, 256, 0, st>>>(d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX, ord, 0);
+            if (!done) k_panel32<<<n_thr, 256, 0, fs>>>(d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX, ord, gi0);
             ++L;
         }
-        step_classes(gp, c0, n_thr, cls);
+        step_classes(gp, c0, gi0 + n_thr, cls, gi1);
         for (const StepClass &c : cls) {
             const size_t psm = sizeof(float2) * (size_t)c.m_max * (MNB + 1);
             if (c.m_max > 256)
-                k_panel32_smem<1024><<<c.i1 - c.i0, 1024, psm, st>>>(d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX,
+                k_panel32_smem<1024><<<c.i1 - c.i0, 1024, psm, fs>>>(d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX,
                                                                    ord, c.i0);
             else
-                k_panel32_smem<256><<<c.i1 - c.i0, 256, psm, st>>>(d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX,
+                k_panel32_smem<256><<<c.i1 - c.i0, 256, psm, fs>>>(d_units, mw.smu, c0, mw.a32, piv, status, INT_MAX,
                                                                  ord, c.i0);
             ++L;
         }
-        step_classes(gp, c0, 0, cls);
+        step_classes(gp, c0, gi0, cls, gi1);
         for (const StepClass &c : cls) {
             int m = c.m_max;
             dim3 g1((m + c0 + 63) / 64, c.i1 - c.i0);  // every column outside the panel
-            k_swap_u12_32<<<g1, 64, 0, st>>>(d_units, mw.smu, c0, mw.a32, piv, status, ord, c.i0);
+            k_swap_u12_32<<<g1, 64, 0, fs>>>(d_units, mw.smu, c0, mw.a32, piv, status, ord, c.i0);
             ++L;
             int rows = m - MNB;
             if (rows > 0) {
                 int t = ((rows + 63) / 64) * ((rows + 63) / 64);
                 dim3 g2(t, c.i1 - c.i0);
-                k_trailing32<<<g2, 256, 0, st>>>(d_units, mw.smu, c0, mw.a32, status, ord, c.i0);
+                k_trailing32<<<g2, 256, 0, fs>>>(d_units, mw.smu, c0, mw.a32, status, ord, c.i0);
                 ++L;
             }
         }
+    }
+    }
+    for (int g = 0; g < n_side; ++g) {  // join the side streams back into the batch stream
+        cudaEventRecord(mw.fevent[g + 1], mw.fstream[g]);
+        cudaStreamWaitEvent(st, mw.fevent[g + 1], 0);
     }
     mark(2);
     int max_rows = 0;

@@ -51,6 +51,12 @@ struct MixedWork {
     int cluster_max = 1;  // largest cluster the scratch was sized for
     bool use_tc = true;   // Gram on the tensor cores (else the FP32 SIMT kernel); the tuner picks it
     bool grid_on = true;  // grid_solves refine grid-wide (else one CTA each); the tuner picks it
+    // concurrent factor groups: the batch stream plus these, forked and
+    // joined with events (parallel branches of a captured graph)
+    static constexpr int MAX_FACTOR_STREAMS = 4;
+    cudaStream_t fstream[MAX_FACTOR_STREAMS - 1] = {};
+    cudaEvent_t fevent[MAX_FACTOR_STREAMS] = {};
+    bool fmade = false;
     cx *c_scratch = nullptr;
     void *c_base = nullptr;
     // the Gram block Z^H Z on the tensor cores (fnec_tc.cu)

@@ -1044,9 +1044,9 @@ cudaError_t launch_cooperative(const void *kernel, dim3 grid, dim3 block, void *
     return cudaLaunchKernelExC(&cfg, kernel, args);
 }
 
-void step_classes(const GridPlan &gp, int c0, int i_begin, std::vector<StepClass> &out) {
+void step_classes(const GridPlan &gp, int c0, int i_begin, std::vector<StepClass> &out, int i_end) {
     out.clear();
-    int i = i_begin, n = (int)gp.s_desc.size();
+    int i = i_begin, n = i_end < 0 ? (int)gp.s_desc.size() : std::min(i_end, (int)gp.s_desc.size());
     while (i < n && gp.s_desc[i] > c0) {
         const int f = 1 << gp.class_shift;
         int m = gp.s_desc[i] - c0, hi = 64;

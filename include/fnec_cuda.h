@@ -470,6 +470,12 @@ typedef struct {
     int32_t graph;         /* 0 launch eagerly; 1 capture the pipeline as a CUDA
                               graph at the second run and replay it afterwards;
                               2 capture at the first run                          */
+    int32_t factor_streams;/* mixed: the factor's units in 1, 2 or 4 groups of
+                              about equal work, each on its own stream (parallel
+                              branches of the graph)                              */
+    int32_t unit_factor;   /* mixed: 1 units with S <= 256 are factored whole,
+                              one CTA each, in one launch beside the per-step
+                              launches of the larger units                        */
 } fnec_schedule;
 
 /* Graph state of a batch (fnec_batch_graph_state). */

@@ -97,7 +97,8 @@ def test_graph_capture_and_replay(acc, plain_ants):
 
 def test_schedule_rejects_out_of_range(acc, plain_ants):
     b = acc.HallenBatch(plain_ants[:2], precision=acc.PRECISION_FP64)
-    for bad in ({"class_shift": 3}, {"gmres_cluster": 3}, {"graph": 5}, {"grid_panels": -1}):
+    for bad in ({"class_shift": 3}, {"gmres_cluster": 3}, {"graph": 5}, {"grid_panels": -1}, {"factor_streams": 3},
+                {"unit_factor": 2}):
         with pytest.raises(acc.AccelError) as e:
             b.schedule = bad
         assert e.value.code == acc.ERR_BAD_ARG
@@ -108,6 +109,8 @@ def test_schedule_rejects_out_of_range(acc, plain_ants):
     {"gram_tensor": 0}, {"gram_tensor": 1},
     {"gmres_cluster": 2}, {"gmres_cluster": 4}, {"gmres_cluster": 8},
     {"gmres_cluster": 8, "gram_tensor": 0, "class_shift": 2, "graph": 2},
+    {"factor_streams": 4}, {"factor_streams": 2, "class_shift": 2, "graph": 2},
+    {"unit_factor": 0}, {"unit_factor": 1, "factor_streams": 4, "graph": 2},
 ])
 def test_mixed_within_gate_under_every_schedule(acc, sched):
     ants = _ants(acc, 20, seed=32)  # few solves: clusters up to 8 CTAs fit
@@ -153,3 +156,21 @@ def test_tuner_sets_and_caches_the_fastest(acc, tmp_path):
     assert b3.schedule == rep["best"]  # applied at creation
     b3.close()
     acc.tune_cache_clear()
+
+
+def test_mixed_factor_groups_give_identical_bits(acc):
+    """Grouping units onto concurrent streams, or factoring small units whole
+    in one CTA, changes only which launches run beside which: every unit's
+    factor (the same operations in the same order), and so every solve, is
+    the same."""
+    ants = _ants(acc, 32, seed=35)
+    b = acc.HallenBatch(ants, precision=acc.PRECISION_MIXED)
+    b.schedule = {"factor_streams": 1, "unit_factor": 0, "graph": 0}
+    ref = _bits(_run(b))
+    for sched in ({"factor_streams": 2}, {"factor_streams": 4}, {"factor_streams": 4, "graph": 2},
+                  {"unit_factor": 1, "factor_streams": 1}, {"unit_factor": 1, "factor_streams": 4}):
+        b.schedule = sched
+        got = _bits(_run(b, times=2))
+        for r, g in zip(ref, got):
+            assert np.array_equal(r, g), sched
+    b.close()
