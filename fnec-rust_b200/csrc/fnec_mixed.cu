@@ -93,16 +93,21 @@ __device__ __forceinline__ cx elem_fast(const double *om, const double *od, cons
         double r_end = sqrt(half * half + a * a);
         ire += 2.0 * log((half + r_end) / a);
     } else {
+        // e^{-jkR}/R with one reciprocal square root per sample and the
+        // phase as a multiple of pi (sincospi needs no Cody-Waite argument
+        // reduction); the phase error stays a few ulp of kR
+        const double kpi = k * 0.31830988618379067;  // k / pi
 #pragma unroll
         for (int m = 0; m < 8; ++m) {
             double sc = m_gl_n8[m] * half;
             double r0 = om[0] - (sm[0] + sc * sd[0]);
             double r1 = om[1] - (sm[1] + sc * sd[1]);
             double r2 = om[2] - (sm[2] + sc * sd[2]);
-            double r = sqrt(r0 * r0 + r1 * r1 + r2 * r2 + a * a);
+            double r2s = r0 * r0 + r1 * r1 + r2 * r2 + a * a;
+            double inv = rsqrt(r2s);
             double sn, cs;
-            sincos(-k * r, &sn, &cs);
-            double wr = m_gl_w8[m] / r;
+            sincospi(-kpi * (r2s * inv), &sn, &cs);
+            double wr = m_gl_w8[m] * inv;
             ire += wr * cs;
             iim += wr * sn;
         }
@@ -716,6 +721,7 @@ struct GmresCtx {
     const float2 *lu;
     const int32_t *piv;
     const int32_t *perm = nullptr;  // the row permutation of piv, if built (then P in = in[perm])
+    const cx *binv = nullptr;       // the factor's diagonal block inverses, if built
     cx *t;  // rows
 };
 
@@ -838,6 +844,71 @@ __device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, cx *sy) {
             }
     }
     __syncthreads();
+    if (g.binv) {
+        // block products with the diagonal blocks' inverses: every warp
+        // takes rows of the 32x32 product (no serial substitution chain),
+        // then all threads update the rows outside the block
+        __shared__ cx s_blk[32];
+        for (int c0 = 0; c0 < s; c0 += 32) {
+            const int nb = min(32, s - c0);
+            const cx *Li = g.binv + (int64_t)(c0 / 32) * 2048;
+            const cx xk = lane < nb ? sy[c0 + lane] : cx{0, 0};
+            for (int i = wid; i < nb; i += (int)(blockDim.x >> 5)) {
+                cx p = warp_sum(lane < nb ? zmul(Li[i * 32 + lane], xk) : cx{0, 0});
+                if (lane == 0) s_blk[i] = p;
+            }
+            __syncthreads();
+            for (int i = tid; i < nb; i += blockDim.x) sy[c0 + i] = s_blk[i];
+            if (nb == 32) {
+                for (int r = c0 + 32 + tid; r < s; r += blockDim.x) {
+                    const float2 *lrow = g.lu + (int64_t)r * s + c0;
+                    cx acc = sy[r];
+#pragma unroll
+                    for (int c8 = 0; c8 < 32; c8 += 8) {
+                        float2 lr[8];
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) lr[c] = lrow[c8 + c];
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) acc = zsub(acc, zmul(f2z(lr[c]), s_blk[c8 + c]));
+                    }
+                    sy[r] = acc;
+                }
+            }
+            __syncthreads();
+        }
+        for (int c0 = ((s - 1) / 32) * 32; c0 >= 0; c0 -= 32) {
+            const int nb = min(32, s - c0);
+            const cx *Ui = g.binv + (int64_t)(c0 / 32) * 2048 + 1024;
+            const cx xk = lane < nb ? sy[c0 + lane] : cx{0, 0};
+            for (int i = wid; i < nb; i += (int)(blockDim.x >> 5)) {
+                cx p = warp_sum(lane < nb ? zmul(Ui[i * 32 + lane], xk) : cx{0, 0});
+                if (lane == 0) s_blk[i] = p;
+            }
+            __syncthreads();
+            for (int i = tid; i < nb; i += blockDim.x) sy[c0 + i] = s_blk[i];
+            for (int r = tid; r < c0; r += blockDim.x) {
+                const float2 *urow = g.lu + (int64_t)r * s + c0;
+                cx acc = sy[r];
+                if (nb == 32) {
+#pragma unroll
+                    for (int c8 = 0; c8 < 32; c8 += 8) {
+                        float2 ur[8];
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) ur[c] = urow[c8 + c];
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) acc = zsub(acc, zmul(f2z(ur[c]), s_blk[c8 + c]));
+                    }
+                } else {
+                    for (int c = 0; c < nb; ++c) acc = zsub(acc, zmul(f2z(urow[c]), s_blk[c]));
+                }
+                sy[r] = acc;
+            }
+            __syncthreads();
+        }
+        for (int i = tid; i < s; i += blockDim.x) out[i] = sy[i];
+        __syncthreads();
+        return;
+    }
     // forward: unit lower triangular (factor rows read 8 entries at a time
     // to keep the register footprint small enough for several CTAs per SM)
     for (int c0 = 0; c0 < s; c0 += 32) {
@@ -923,6 +994,52 @@ __device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, cx *sy) {
     __syncthreads();
 }
 
+// Inverses, in FP64, of the FP32 factor's 32x32 diagonal blocks of one
+// system: warp 0 forms L11^-1 (unit lower), warp 1 U11^-1 (upper), lane j
+// column j by substitution on its own column.  Stored row-major per block:
+// L^-1 then U^-1 (2 x 1024 complex128); entries outside an nb < 32 block
+// are zero.  The refinement applies the preconditioner with them.
+__global__ void __launch_bounds__(64) k_block_inv32(const UnitDesc *__restrict__ units,
+                                                    const MixedUnit *__restrict__ smu,
+                                                    const float2 *__restrict__ a32buf, cx *binvbuf,
+                                                    const int32_t *__restrict__ status) {
+    __shared__ float2 sB[32][33];
+    __shared__ cx sX[2][32][33];
+    const int ui = blockIdx.y;
+    const UnitDesc u = units[ui];
+    const int c0 = blockIdx.x * 32, s = u.s;
+    if (c0 >= s || status[ui] != 0) return;
+    const int nb = min(32, s - c0);
+    const float2 *A = a32buf + smu[ui].a32_off;
+    const int tid = threadIdx.x, w = tid >> 5, j = tid & 31;
+    for (int e = tid; e < 32 * 32; e += 64) {
+        const int i = e / 32, k = e % 32;
+        sB[i][k] = (i < nb && k < nb) ? A[(int64_t)(c0 + i) * s + c0 + k] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    cx(*X)[33] = sX[w];
+    if (w == 0) {  // L^-1 e_j: forward, unit diagonal
+        for (int i = 0; i < 32; ++i) {
+            cx v = {i == j ? 1.0 : 0.0, 0.0};
+            if (i < nb && j < nb)
+                for (int k = j; k < i; ++k) v = zsub(v, zmul(f2z(sB[i][k]), X[k][j]));
+            X[i][j] = (i < nb && j < nb) ? v : cx{0, 0};
+        }
+    } else {  // U^-1 e_j: backward
+        for (int i = 31; i >= 0; --i) {
+            if (i >= nb || j >= nb) {
+                X[i][j] = {0, 0};
+                continue;
+            }
+            cx v = {i == j ? 1.0 : 0.0, 0.0};
+            for (int k = i + 1; k <= j; ++k) v = zsub(v, zmul(f2z(sB[i][k]), X[k][j]));
+            X[i][j] = zdiv(v, f2z(sB[i][i]));
+        }
+    }
+    cx *out = binvbuf + smu[ui].binv_off + (int64_t)blockIdx.x * 2048 + (int64_t)w * 1024;
+    for (int i = 0; i < 32; ++i) out[i * 32 + j] = X[i][j];
+}
+
 __device__ double vnorm(const cx *v, int s, double *red) {
     double a = 0;
     for (int i = threadIdx.x; i < s; i += blockDim.x) a += v[i].re * v[i].re + v[i].im * v[i].im;
@@ -936,7 +1053,7 @@ __global__ void __launch_bounds__(256, 3) k_gmres_ir(const UnitDesc *__restrict_
                                                   const float2 *__restrict__ a32buf, const int32_t *__restrict__ pivbuf,
                                                   cx *xbuf, cx *vbuf, cx *wbuf, const int32_t *__restrict__ status,
                                                   int staged, int skip_s, int only, int min_s,
-                                                  const int32_t *__restrict__ s_order) {
+                                                  const int32_t *__restrict__ s_order, const cx *__restrict__ binvbuf) {
     extern __shared__ unsigned char s_dyn[];
     __shared__ cx sH[(GM + 1) * GM];
     __shared__ double scs[GM];
@@ -966,6 +1083,7 @@ __global__ void __launch_bounds__(256, 3) k_gmres_ir(const UnitDesc *__restrict_
     g.crows = crows + a.crow_off;
     g.lu = a32buf + mu.a32_off;
     g.piv = pivbuf + u.piv_off;
+    if (binvbuf) g.binv = binvbuf + mu.binv_off;
     int s = g.s;
     cx *W = wbuf + mu.w_off;
     cx *b = W, *x = W + s, *r = W + 2 * s, *w = W + 3 * s;
@@ -1717,17 +1835,20 @@ bool mixed_available() { return true; }
 
 cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, const std::vector<UnitDesc> &solves,
                         const std::vector<AntDesc> &ants, int max_s, const DevAlloc &dev, bool allow_grid) {
-    std::vector<int64_t> a32_of(systems.size());
-    int64_t a32 = 0, v = 0, wk = 0;
+    std::vector<int64_t> a32_of(systems.size()), binv_of(systems.size());
+    int64_t a32 = 0, v = 0, wk = 0, binv = 0;
     for (size_t i = 0; i < systems.size(); ++i) {
         a32_of[i] = a32;
         a32 += (int64_t)systems[i].s * systems[i].s;
+        binv_of[i] = binv;
+        binv += (int64_t)((systems[i].s + 31) / 32) * 2048;
     }
     std::vector<MixedUnit> mu(solves.size());
     for (size_t i = 0; i < solves.size(); ++i) {
         const UnitDesc &u = solves[i];
         int rows = u.n + ants[u.ant].n_crow;
         mu[i].a32_off = a32_of[u.sys];
+        mu[i].binv_off = binv_of[u.sys];
         mu[i].v_off = v;
         mu[i].w_off = wk;
         mu[i].rows = rows;
@@ -1739,7 +1860,10 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
     }
     // systems' descriptors index the factor through the first solve's entry
     std::vector<MixedUnit> sysmu(systems.size());
-    for (size_t i = 0; i < systems.size(); ++i) sysmu[i].a32_off = a32_of[i];
+    for (size_t i = 0; i < systems.size(); ++i) {
+        sysmu[i].a32_off = a32_of[i];
+        sysmu[i].binv_off = binv_of[i];
+    }
     size_t b_mu = sizeof(MixedUnit) * (mu.size() + 1);
     size_t b_smu = sizeof(MixedUnit) * (sysmu.size() + 1);
     size_t b_a32 = sizeof(float2) * (size_t)(a32 + 1);
@@ -1747,7 +1871,8 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
     size_t b_w = sizeof(cx) * (size_t)(wk + 1);
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
     size_t b_ord = sizeof(int32_t) * (solves.size() + 1);
-    size_t total = al(b_mu) + al(b_smu) + al(b_a32) + al(b_v) + al(b_w) + al(b_ord);
+    size_t b_binv = sizeof(cx) * (size_t)(binv + 1);
+    size_t total = al(b_mu) + al(b_smu) + al(b_a32) + al(b_v) + al(b_w) + al(b_ord) + al(b_binv);
     cudaError_t e = dev.alloc(&w.base, total);
     if (e != cudaSuccess) return e;
     unsigned char *p = (unsigned char *)w.base;
@@ -1769,6 +1894,8 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
     w.w = (cx *)p;
     p += al(b_w);
     w.s_order = (int32_t *)p;
+    p += al(b_ord);
+    w.binv = (cx *)p;
     w.bytes = total;
     w.n_units = (int)solves.size();
     w.max_s = max_s;
@@ -2071,6 +2198,11 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     if (!staged) smem = 0;
     const bool grid_refine = mw.grid_on && !mw.grid_solves.empty();
     const int skip_s = grid_refine ? GG_MIN_S : INT_MAX;
+    if (mw.use_binv && nu > 0) {  // the preconditioner's diagonal block inverses
+        k_block_inv32<<<dim3((unsigned)((max_s + 31) / 32), (unsigned)nu), 64, 0, st>>>(d_units, mw.smu, mw.a32, mw.binv,
+                                                                                      status);
+        ++L;
+    }
     int min_s = 0;  // solves below this are refined by the cluster kernel
     if (ns > 0 && mw.cluster_c > 1) {
         cudaLaunchConfig_t cfg = {};
@@ -2097,7 +2229,8 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     }
     if (ns > 0) {
         k_gmres_ir<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x, mw.v,
-                                          mw.w, status, staged, skip_s, -1, min_s, mw.s_order);
+                                          mw.w, status, staged, skip_s, -1, min_s, mw.s_order,
+                                          mw.use_binv ? mw.binv : nullptr);
         cudaError_t le = cudaPeekAtLastError();
         if (le != cudaSuccess && !marks.detail[0])
             std::snprintf(marks.detail, sizeof(marks.detail), "GMRES launch: %d solves, %zu B shared (%s), max_s %d, rows %d",
@@ -2130,7 +2263,8 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
                     cudaSuccess) {
                 (void)cudaGetLastError();  // not co-resident: refine this solve in one CTA
                 k_gmres_ir<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x,
-                                                  mw.v, mw.w, status, staged, INT_MAX, ui, 0, mw.s_order);
+                                                  mw.v, mw.w, status, staged, INT_MAX, ui, 0, mw.s_order,
+                                                  mw.use_binv ? mw.binv : nullptr);
             }
             L += 2;
         }

@@ -21,6 +21,7 @@ struct MixedUnit {
     int32_t iters;    // GMRES iterations used
     double resid;     // final preconditioned relative residual
     int64_t cs_off;   // complex128 scratch of the cluster GMRES (-1: none)
+    int64_t binv_off; // complex128 inverses of the factor's 32x32 diagonal blocks (per system)
 };
 
 struct MixedWork {
@@ -29,6 +30,7 @@ struct MixedWork {
     MixedUnit *mu = nullptr;   // per solve
     MixedUnit *smu = nullptr;  // per system (a32_off only)
     float2 *a32 = nullptr;
+    cx *binv = nullptr;          // per system: ceil(S/32) x (L11^-1, U11^-1), 32x32 each
     int32_t *s_order = nullptr;  // solves by decreasing N^2 (refinement launch order)
     cx *v = nullptr;
     cx *w = nullptr;
@@ -51,6 +53,7 @@ struct MixedWork {
     int cluster_max = 1;  // largest cluster the scratch was sized for
     bool use_tc = true;   // Gram on the tensor cores (else the FP32 SIMT kernel); the tuner picks it
     bool grid_on = true;  // grid_solves refine grid-wide (else one CTA each); the tuner picks it
+    bool use_binv = true; // the refinement applies the factor with diagonal block inverses
     // concurrent factor groups: the batch stream plus these, forked and
     // joined with events (parallel branches of a captured graph)
     static constexpr int MAX_FACTOR_STREAMS = 4;

@@ -551,7 +551,8 @@ def _antenna_struct(a, keep: list):
 class _Schedule(ctypes.Structure):
     _fields_ = [("grid_panels", ctypes.c_int32), ("class_shift", ctypes.c_int32), ("gram_tensor", ctypes.c_int32),
                 ("gmres_cluster", ctypes.c_int32), ("grid_gmres", ctypes.c_int32), ("graph", ctypes.c_int32),
-                ("factor_streams", ctypes.c_int32), ("unit_factor", ctypes.c_int32)]
+                ("factor_streams", ctypes.c_int32), ("unit_factor", ctypes.c_int32),
+                ("block_inverse", ctypes.c_int32)]
 
 
 class _TuneReport(ctypes.Structure):
@@ -633,7 +634,8 @@ class HallenBatch:
     @property
     def schedule(self) -> dict:
         """How the pipeline launches (grid_panels, class_shift, gram_tensor,
-        gmres_cluster, grid_gmres, graph, factor_streams, unit_factor)."""
+        gmres_cluster, grid_gmres, graph, factor_streams, unit_factor,
+        block_inverse)."""
         s = _Schedule()
         self.ctx.check(lib().fnec_batch_get_schedule(self._h, ctypes.byref(s)), "batch_get_schedule")
         return _sched_dict(s)

@@ -476,6 +476,9 @@ typedef struct {
     int32_t unit_factor;   /* mixed: 1 units with S <= 256 are factored whole,
                               one CTA each, in one launch beside the per-step
                               launches of the larger units                        */
+    int32_t block_inverse; /* mixed: 1 the refinement applies the factor's 32x32
+                              diagonal blocks through their FP64 inverses (block
+                              products); 0 by substitution in one warp            */
 } fnec_schedule;
 
 /* Graph state of a batch (fnec_batch_graph_state). */

@@ -98,7 +98,7 @@ def test_graph_capture_and_replay(acc, plain_ants):
 def test_schedule_rejects_out_of_range(acc, plain_ants):
     b = acc.HallenBatch(plain_ants[:2], precision=acc.PRECISION_FP64)
     for bad in ({"class_shift": 3}, {"gmres_cluster": 3}, {"graph": 5}, {"grid_panels": -1}, {"factor_streams": 3},
-                {"unit_factor": 2}):
+                {"unit_factor": 2}, {"block_inverse": 5}):
         with pytest.raises(acc.AccelError) as e:
             b.schedule = bad
         assert e.value.code == acc.ERR_BAD_ARG
@@ -111,6 +111,7 @@ def test_schedule_rejects_out_of_range(acc, plain_ants):
     {"gmres_cluster": 8, "gram_tensor": 0, "class_shift": 2, "graph": 2},
     {"factor_streams": 4}, {"factor_streams": 2, "class_shift": 2, "graph": 2},
     {"unit_factor": 0}, {"unit_factor": 1, "factor_streams": 4, "graph": 2},
+    {"block_inverse": 0}, {"block_inverse": 1, "gmres_cluster": 4},
 ])
 def test_mixed_within_gate_under_every_schedule(acc, sched):
     ants = _ants(acc, 20, seed=32)  # few solves: clusters up to 8 CTAs fit
