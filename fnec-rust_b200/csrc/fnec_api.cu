@@ -535,7 +535,7 @@ struct fnec_batch {
     cudaEvent_t ev[FNEC_N_PHASES + 1] = {};
     bool ev_made = false;
     // schedule and its CUDA graph
-    fnec_schedule sched = {1, 1, 1, 1, 1, 1, 1, 1, 1};
+    fnec_schedule sched = {1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 3};
     cudaGraphExec_t gexec = nullptr;
     int graph_state = FNEC_GRAPH_NONE;
     uint64_t graph_launches = 0;  // launches the graph replays
@@ -1447,7 +1447,7 @@ static bool schedule_valid(const fnec_schedule &s) {
            (s.gmres_cluster == 1 || s.gmres_cluster == 2 || s.gmres_cluster == 4 || s.gmres_cluster == 8) &&
            bit(s.grid_gmres) && s.graph >= 0 && s.graph <= 2 &&
            (s.factor_streams == 1 || s.factor_streams == 2 || s.factor_streams == 4) && bit(s.unit_factor) &&
-           bit(s.block_inverse);
+           bit(s.block_inverse) && bit(s.tensor_trailing) && (s.gmres_ctas_per_sm == 3 || s.gmres_ctas_per_sm == 4);
 }
 
 // Make the batch launch as s says (s valid); drops a captured graph when
@@ -1458,7 +1458,9 @@ static void apply_schedule(fnec_batch *b, const fnec_schedule &s) {
     const bool same_launches = t.grid_panels == b->sched.grid_panels && t.class_shift == b->sched.class_shift &&
                                t.gram_tensor == b->sched.gram_tensor && t.gmres_cluster == b->sched.gmres_cluster &&
                                t.grid_gmres == b->sched.grid_gmres && t.factor_streams == b->sched.factor_streams &&
-                               t.unit_factor == b->sched.unit_factor && t.block_inverse == b->sched.block_inverse;
+                               t.unit_factor == b->sched.unit_factor && t.block_inverse == b->sched.block_inverse &&
+                               t.tensor_trailing == b->sched.tensor_trailing &&
+                               t.gmres_ctas_per_sm == b->sched.gmres_ctas_per_sm;
     if (!same_launches || (t.graph == 0) != (b->sched.graph == 0)) drop_graph(b);
     b->sched = t;
     b->grid.grid_on = t.grid_panels != 0;
@@ -1469,6 +1471,8 @@ static void apply_schedule(fnec_batch *b, const fnec_schedule &s) {
     b->grid.factor_streams = t.factor_streams;
     b->grid.unit_factor = t.unit_factor != 0;
     b->mixed.use_binv = t.block_inverse != 0;
+    b->mixed.use_tc_trail = t.tensor_trailing != 0;
+    b->mixed.gmres_minb = t.gmres_ctas_per_sm;
 }
 
 static int ceil_log2(int64_t v) {
@@ -1608,6 +1612,7 @@ int fnec_batch_tune(fnec_batch *b, uint32_t reps, fnec_tune_report *out) {
     };
     std::vector<Knob> knobs;
     const bool mixed = b->precision == FNEC_PRECISION_MIXED;
+    if (mixed && b->mixed.trail) knobs.push_back({&fnec_schedule::tensor_trailing, {0, 1}});
     if (mixed && b->mixed.tc) knobs.push_back({&fnec_schedule::gram_tensor, {1, 0}});
     if (mixed && b->mixed.cluster_max > 1) {
         std::vector<int32_t> c;
@@ -1621,6 +1626,10 @@ int fnec_batch_tune(fnec_batch *b, uint32_t reps, fnec_tune_report *out) {
         knobs.push_back({&fnec_schedule::unit_factor, {1, 0}});
     if (mixed && b->mixed.fmade) knobs.push_back({&fnec_schedule::factor_streams, {1, 2, 4}});
     if (mixed) knobs.push_back({&fnec_schedule::block_inverse, {1, 0}});
+    if (mixed) knobs.push_back({&fnec_schedule::gmres_ctas_per_sm, {3, 4}});
+    // two passes of coordinate descent: a field's best value can depend on
+    // fields tuned after it
+    for (int pass = 0; pass < 2; ++pass)
     for (const Knob &k : knobs) {
         for (int32_t v : k.v) {
             if (best.*(k.f) == v) continue;
@@ -1650,14 +1659,15 @@ int fnec_batch_tune(fnec_batch *b, uint32_t reps, fnec_tune_report *out) {
     return FNEC_OK;
 }
 
-constexpr int N_SCHED_FIELDS = 9;
-static const char *const SCHED_FIELDS[N_SCHED_FIELDS] = {"grid_panels", "class_shift",    "gram_tensor",
-                                                         "gmres_cluster", "grid_gmres",   "graph",
-                                                         "factor_streams", "unit_factor", "block_inverse"};
+constexpr int N_SCHED_FIELDS = 11;
+static const char *const SCHED_FIELDS[N_SCHED_FIELDS] = {"grid_panels",    "class_shift",   "gram_tensor",
+                                                         "gmres_cluster",  "grid_gmres",    "graph",
+                                                         "factor_streams", "unit_factor",   "block_inverse",
+                                                         "tensor_trailing", "gmres_ctas_per_sm"};
 static int32_t *sched_field(fnec_schedule &s, int i) {
-    int32_t *f[N_SCHED_FIELDS] = {&s.grid_panels,    &s.class_shift, &s.gram_tensor,
-                                  &s.gmres_cluster,  &s.grid_gmres,  &s.graph,
-                                  &s.factor_streams, &s.unit_factor, &s.block_inverse};
+    int32_t *f[N_SCHED_FIELDS] = {&s.grid_panels,    &s.class_shift, &s.gram_tensor,   &s.gmres_cluster,
+                                  &s.grid_gmres,     &s.graph,       &s.factor_streams, &s.unit_factor,
+                                  &s.block_inverse,  &s.tensor_trailing, &s.gmres_ctas_per_sm};
     return f[i];
 }
 
@@ -1687,7 +1697,7 @@ int fnec_tune_cache_load(const char *path) {
         char *tok = strtok_r(line, " \t\r\n", &save);
         if (!tok || tok[0] == '#') continue;
         std::string key = tok;
-        fnec_schedule s = {1, 1, 1, 1, 1, 1, 1, 1, 1};
+        fnec_schedule s = {1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 3};
         int seen = 0;
         while ((tok = strtok_r(nullptr, " \t\r\n", &save))) {
             char *eq = std::strchr(tok, '=');
@@ -2221,6 +2231,10 @@ int64_t request_bytes(const HostAnt &h, int precision) {
         b += 16 * (25 * s + 6 * s + 2 * rows) * f * r;     // GMRES basis and work vectors
         b += (16 * (((n + 31) / 32) * n + 2 * s + 512) + 4) * f * r;  // cluster GMRES scratch, launch order
         b += 16 * 2048 * ((s + 31) / 32) * f;              // diagonal block inverses of the factor
+        if (s - 32 >= 192) {                               // tensor-core trailing stacks and step lists
+            const int64_t m0 = s - 32, pa = (m0 + 127) / 128 * 128, pb = (2 * m0 + 127) / 128 * 128;
+            b += (256 * (2 * pa + 2 * pb) + 32 * ((s + 31) / 32)) * f;
+        }
     } else {
         b += 16 * s * (s + 1) * f + 4 * s * f;             // FP64 factor, pivots
     }

@@ -392,16 +392,23 @@ __device__ bool panel32_body(float2 *A, int s, int c0, int32_t *piv, int32_t *st
             s_i[wid] = bi;
         }
         __syncthreads();
-        if (tid == 0) {
-            float v = s_v[0];
-            int p = s_i[0];
-            for (int q = 1; q < nw; ++q) piv_better32(v, p, s_v[q], s_i[q]);
-            if (p < 0 || !(v > 0.f)) {
-                *status_u = -(c + 1);
-                p = -1;
+        if (wid == 0) {  // the per-warp candidates, reduced by warp 0
+            float v = lane < nw ? s_v[lane] : -1.f;
+            int p = lane < nw ? s_i[lane] : -1;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                float ov = __shfl_down_sync(0xffffffffu, v, o);
+                int oi = __shfl_down_sync(0xffffffffu, p, o);
+                piv_better32(v, p, ov, oi);
             }
-            *s_p = p;
-            piv[c] = p;
+            if (lane == 0) {
+                if (p < 0 || !(v > 0.f)) {
+                    *status_u = -(c + 1);
+                    p = -1;
+                }
+                *s_p = p;
+                piv[c] = p;
+            }
         }
         __syncthreads();
         int p = *s_p;
@@ -465,6 +472,8 @@ __global__ void __launch_bounds__(NT) k_panel32_smem(const UnitDesc *__restrict_
 // operations in the same order -- so the factor is bit-identical -- but
 // without a kernel boundary or a global round trip between steps.
 constexpr int FU_MAX_S = 256;
+// trailing blocks of at least this many rows go to the tensor cores
+constexpr int TC_TRAIL_MIN_M = 192;
 constexpr int FU_THREADS = 256;
 constexpr size_t FU_SMEM = sizeof(float2) * (size_t)(MNB * (MNB + 1) + MNB * FU_THREADS);  // swap stage, the largest
 
@@ -1046,7 +1055,11 @@ __device__ double vnorm(const cx *v, int s, double *red) {
     return sqrt(block_sum(a, red));
 }
 
-__global__ void __launch_bounds__(256, 3) k_gmres_ir(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
+// MINB: CTAs per SM the registers are budgeted for (3: 80 registers, no
+// spills; 4: 64 registers, a few spilled) -- more resident solves against
+// cheaper ones, picked per batch by the tuner.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_gmres_ir(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
                                                   MixedUnit *mus, const int32_t *__restrict__ ibuf,
                                                   const DevConRow *__restrict__ crows, const cx *__restrict__ zbuf,
                                                   const cx *__restrict__ rhs, const double *__restrict__ cosv,
@@ -2001,6 +2014,42 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
             delete p;
         }
     }
+    {
+        // tensor-core trailing updates: units whose first trailing block has
+        // at least TC_TRAIL_MIN_M rows, while it still does
+        std::vector<int32_t> ord(systems.size());
+        for (size_t i = 0; i < ord.size(); ++i) ord[i] = (int32_t)i;
+        std::stable_sort(ord.begin(), ord.end(), [&](int32_t x, int32_t y) { return systems[x].s > systems[y].s; });
+        std::vector<int> sd(ord.size());
+        for (size_t i = 0; i < ord.size(); ++i) sd[i] = systems[ord[i]].s;
+        int n_tc = 0;
+        while (n_tc < (int)sd.size() && sd[n_tc] - 32 >= TC_TRAIL_MIN_M) ++n_tc;
+        if (n_tc > 0 && w.tc) {
+            TcTrailPlan *p = new TcTrailPlan();
+            tc_trail_plan(sd, ord, n_tc, TC_TRAIL_MIN_M, *p);
+            size_t b_st = sizeof(float) * 32 * (size_t)p->rows, b_u = sizeof(TcTrailUnit) * (p->units.size() + 1);
+            size_t tot = 2 * al(b_st) + al(b_u);
+            e = dev.alloc(&w.trail_base, tot);
+            if (e != cudaSuccess) {
+                delete p;
+                return e;
+            }
+            unsigned char *q = (unsigned char *)w.trail_base;
+            w.tr_hi = (float *)q;
+            q += al(b_st);
+            w.tr_lo = (float *)q;
+            q += al(b_st);
+            w.d_trail = q;
+            w.bytes += tot;
+            e = dev.upload(w.d_trail, p->units.data(), sizeof(TcTrailUnit) * p->units.size());
+            if (e != cudaSuccess || !tc_trail_maps(*p, w.tr_hi, w.tr_lo)) {
+                delete p;
+                return e != cudaSuccess ? e : cudaErrorNotSupported;
+            }
+            w.trail = p;
+            w.trail_n = n_tc;
+        }
+    }
     if (systems.size() >= 4 && !w.fmade) {  // concurrent factor groups
         bool ok = true;
         for (int g = 0; g + 1 < MixedWork::MAX_FACTOR_STREAMS && ok; ++g)
@@ -2027,6 +2076,11 @@ void free_mixed(MixedWork &w, const DevAlloc &dev) {
     dev.release(w.grid_base);
     dev.release(w.tc_base);
     dev.release(w.c_base);
+    dev.release(w.trail_base);
+    w.trail_base = nullptr;
+    delete w.trail;
+    w.trail = nullptr;
+    w.trail_n = 0;
     w.c_base = nullptr;
     w.c_scratch = nullptr;
     w.grid_base = nullptr;
@@ -2099,6 +2153,7 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         // panels, one exchange area) all stay in the first group
         int n_tall = 0;
         while (n_tall < i_unit && gp.s_desc[n_tall] > thr_rows) ++n_tall;
+        if (mw.trail && mw.use_tc_trail) n_tall = std::max(n_tall, std::min(mw.trail_n, i_unit));  // one stack set
         double tot = 0, acc = 0;
         for (int i = 0; i < i_unit; ++i) tot += (double)gp.s_desc[i] * gp.s_desc[i] * gp.s_desc[i];
         for (int i = 0; i < i_unit && (int)gb.size() < G; ++i) {
@@ -2172,13 +2227,26 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
             dim3 g1((m + c0 + 63) / 64, c.i1 - c.i0);  // every column outside the panel
             k_swap_u12_32<<<g1, 64, 0, fs>>>(d_units, mw.smu, c0, mw.a32, piv, status, ord, c.i0);
             ++L;
-            int rows = m - MNB;
+        }
+        // trailing updates: the largest units' on the tensor cores (a prefix
+        // of the order, in the first group), the rest as FP32 SIMT tiles
+        // (never a unit factored whole: those are the order's tail from i_unit)
+        const int k_tc =
+            (grp == 0 && mw.trail && mw.use_tc_trail) ? std::min(mw.trail->active(c0 / MNB), i_unit) : 0;
+        step_classes(gp, c0, std::max(gi0, k_tc), cls, gi1);
+        for (const StepClass &c : cls) {
+            int rows = c.m_max - MNB;
             if (rows > 0) {
                 int t = ((rows + 63) / 64) * ((rows + 63) / 64);
                 dim3 g2(t, c.i1 - c.i0);
                 k_trailing32<<<g2, 256, 0, fs>>>(d_units, mw.smu, c0, mw.a32, status, ord, c.i0);
                 ++L;
             }
+        }
+        if (k_tc > 0) {
+            tc_trail_run(*mw.trail, c0 / MNB, k_tc, static_cast<const TcTrailUnit *>(mw.d_trail), d_units, mw.smu, mw.a32,
+                         mw.tr_hi, mw.tr_lo, status, fs);
+            L += 3;
         }
     }
     }
@@ -2192,7 +2260,7 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     size_t smem = sizeof(cx) * (size_t)(2 * max_s + max_rows) + sizeof(int32_t) * (size_t)max_s;  // + perm
     int staged = smem <= 200 * 1024;
     if (staged && smem > 0) {  // static + dynamic above 48 KB needs the raised limit
-        int lim = set_smem_limit_once(k_gmres_ir, 200 * 1024);
+        int lim = std::min(set_smem_limit_once(k_gmres_ir<3>, 200 * 1024), set_smem_limit_once(k_gmres_ir<4>, 200 * 1024));
         if (lim < 0 || (size_t)lim < smem) staged = 0;
     }
     if (!staged) smem = 0;
@@ -2228,9 +2296,9 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         }
     }
     if (ns > 0) {
-        k_gmres_ir<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x, mw.v,
-                                          mw.w, status, staged, skip_s, -1, min_s, mw.s_order,
-                                          mw.use_binv ? mw.binv : nullptr);
+        auto gk = mw.gmres_minb == 4 ? k_gmres_ir<4> : k_gmres_ir<3>;
+        gk<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x, mw.v, mw.w, status,
+                                  staged, skip_s, -1, min_s, mw.s_order, mw.use_binv ? mw.binv : nullptr);
         cudaError_t le = cudaPeekAtLastError();
         if (le != cudaSuccess && !marks.detail[0])
             std::snprintf(marks.detail, sizeof(marks.detail), "GMRES launch: %d solves, %zu B shared (%s), max_s %d, rows %d",
@@ -2262,7 +2330,7 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
                 launch_cooperative((const void *)k_gmres_grid, dim3(mw.grid_ctas), dim3(256), args, 0, st) !=
                     cudaSuccess) {
                 (void)cudaGetLastError();  // not co-resident: refine this solve in one CTA
-                k_gmres_ir<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x,
+                k_gmres_ir<3><<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x,
                                                   mw.v, mw.w, status, staged, INT_MAX, ui, 0, mw.s_order,
                                                   mw.use_binv ? mw.binv : nullptr);
             }

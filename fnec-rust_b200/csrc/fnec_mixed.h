@@ -10,6 +10,7 @@
 namespace fnec {
 
 struct TcGramPlan;
+struct TcTrailPlan;
 
 // Per-unit offsets into the mixed path's work buffers, and its refinement
 // statistics (written by the GMRES kernel).
@@ -54,6 +55,7 @@ struct MixedWork {
     bool use_tc = true;   // Gram on the tensor cores (else the FP32 SIMT kernel); the tuner picks it
     bool grid_on = true;  // grid_solves refine grid-wide (else one CTA each); the tuner picks it
     bool use_binv = true; // the refinement applies the factor with diagonal block inverses
+    int gmres_minb = 3;   // refinement CTAs per SM its registers are budgeted for (3 or 4)
     // concurrent factor groups: the batch stream plus these, forked and
     // joined with events (parallel branches of a captured graph)
     static constexpr int MAX_FACTOR_STREAMS = 4;
@@ -68,6 +70,13 @@ struct MixedWork {
     float *tc_hi = nullptr, *tc_lo = nullptr;
     void *tc_gu = nullptr, *tc_tiles = nullptr;
     int tc_max_n = 0;
+    // the factor's trailing updates of the largest units on the tensor cores
+    TcTrailPlan *trail = nullptr;
+    void *trail_base = nullptr;
+    float *tr_hi = nullptr, *tr_lo = nullptr;
+    void *d_trail = nullptr;  // TcTrailUnit per (step, unit)
+    int trail_n = 0;          // units (a prefix of the s-descending order) it covers
+    bool use_tc_trail = false; // the tuner picks it
 };
 
 // Phase events the mixed path records after its fill, Gram, factor and

@@ -19,6 +19,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <mutex>
 
 #include "fnec_cuda.h"
@@ -172,6 +173,34 @@ __device__ __forceinline__ void epi_gram(const TcTile &t, const TcEpilogue &ep, 
     }
 }
 
+// A22 -= D for one factor step: rows c0 + 32 + tile row, float columns
+// 2 (c0 + 32) + tile column of the unit's interleaved complex A32.  The
+// warp's 32 x 32 block (a row per lane from TMEM) is transposed through
+// shared memory (stg: 32 x 33 floats of the warp) so that each
+// read-modify-write covers 32 consecutive floats of one row.
+__device__ __forceinline__ void epi_trail(const TcTile &t, const TcEpilogue &ep, int row0, int col, const float (&v)[32],
+                                          int lane, float *stg) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j) stg[lane * 33 + j] = v[j];
+    __syncwarp();
+    const int s = ep.units[t.unit].s;
+    float *A = reinterpret_cast<float *>(ep.a32 + ep.mus[t.unit].a32_off);
+    const int64_t F = 2 * ((int64_t)ep.c0 + 32) + (int64_t)t.tj * BN + col + lane;
+    const int64_t R0 = (int64_t)ep.c0 + 32 + (int64_t)t.ti * BM + row0;
+    // all reads (the transposed block, then A22) before any write, so no
+    // load waits behind a store it might alias
+    float d[32], a[32];
+#pragma unroll
+    for (int r = 0; r < 32; ++r) d[r] = stg[r * 33 + lane];
+    __syncwarp();
+    const bool col_ok = F < 2 * (int64_t)s;
+#pragma unroll
+    for (int r = 0; r < 32; ++r) a[r] = (col_ok && R0 + r < s) ? A[(R0 + r) * 2 * s + F] : 0.f;
+#pragma unroll
+    for (int r = 0; r < 32; ++r)
+        if (col_ok && R0 + r < s) A[(R0 + r) * 2 * s + F] = a[r] - d[r];
+}
+
 template <int EPI>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_tc_gemm(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
@@ -183,7 +212,22 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     __shared__ int s_abort;
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const TcTile t = tiles[blockIdx.x];
+    TcTile t;
+    if (EPI == TC_EPI_TRAIL) {  // the tile from (unit of the step, tile index)
+        const TcTrailUnit tu = ep.trail[blockIdx.y];
+        const int ntj = tu.n2_pad / BN, ti = (int)blockIdx.x / ntj, tj = (int)blockIdx.x % ntj;
+        if (ti >= tu.m_pad / BM) return;  // the whole CTA, before any barrier or TMEM allocation
+        t.a_row = (int32_t)(tu.a_base + (int64_t)ti * BM);
+        t.b_row = (int32_t)(tu.b_base + (int64_t)tj * BN);
+        t.a_kstride = tu.m_pad;
+        t.b_kstride = tu.n2_pad;
+        t.kblocks = 2;
+        t.unit = tu.unit;
+        t.ti = ti;
+        t.tj = tj;
+    } else {
+        t = tiles[blockIdx.x];
+    }
     const uint32_t sbase = smem_u32(smem);
     auto full = [&](int st) { return smem_u32(&s_bar[st]); };
     auto empty = [&](int st) { return smem_u32(&s_bar[STAGES + st]); };
@@ -253,12 +297,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (ok) {
             const int q = warp & 3;  // TMEM lane quarter this warp may access
             const int row = q * 32 + lane;
+            // every MMA has completed: the stage buffers are free for staging
+            float *stg = reinterpret_cast<float *>(smem) + q * 32 * 33;
 #pragma unroll 1
             for (int cc = 0; cc < BN / 32; ++cc) {
                 float v[32];
                 tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(cc * 32), v);
                 if (EPI == TC_EPI_STORE) epi_store(t, ep, row, cc * 32, v);
-                else epi_gram(t, ep, row, cc * 32, v, lane);
+                else if (EPI == TC_EPI_GRAM) epi_gram(t, ep, row, cc * 32, v, lane);
+                else epi_trail(t, ep, q * 32, cc * 32, v, lane, stg);
             }
         }
     }
@@ -325,6 +372,62 @@ __global__ void k_split_gram(const UnitDesc *__restrict__ units, const TcGramUni
         int64_t o = ((int64_t)g.base + (int64_t)blockIdx.y * g.rpad + 2 * c0 + rr) * 32 + kk;
         hi[o] = h;
         lo[o] = l;
+    }
+}
+
+// L21 of one factor step -> the trailing A operand (K-blocked hi/lo):
+// k-block 0 the real parts, k-block 1 the imaginary parts, a warp per row.
+__global__ void k_split_trail_a(const TcTrailUnit *__restrict__ tu_list, const UnitDesc *__restrict__ systems,
+                                const MixedUnit *__restrict__ smu, const float2 *__restrict__ a32buf, int c0,
+                                float *hi, float *lo) {
+    const TcTrailUnit tu = tu_list[blockIdx.y];
+    const int i = blockIdx.x * 8 + (threadIdx.x >> 5), k = threadIdx.x & 31;
+    if (i >= tu.m_pad) return;
+    const int s = systems[tu.unit].s;
+    float2 v = make_float2(0.f, 0.f);
+    if (i < tu.m) v = a32buf[smu[tu.unit].a32_off + (int64_t)(c0 + 32 + i) * s + c0 + k];
+    float h, l;
+    const int64_t o0 = (tu.a_base + i) * 32 + k, o1 = (tu.a_base + tu.m_pad + i) * 32 + k;
+    split_tf32(v.x, h, l);
+    hi[o0] = h;
+    lo[o0] = l;
+    split_tf32(v.y, h, l);
+    hi[o1] = h;
+    lo[o1] = l;
+}
+
+// U12 of one factor step -> the trailing B operand: rows 2j (Re U, -Im U)
+// and 2j+1 (Im U, Re U) over k-blocks 0 / 1.  A 32 (k) x 32 (j) block of
+// U is transposed through shared memory.
+__global__ void k_split_trail_b(const TcTrailUnit *__restrict__ tu_list, const UnitDesc *__restrict__ systems,
+                                const MixedUnit *__restrict__ smu, const float2 *__restrict__ a32buf, int c0,
+                                float *hi, float *lo) {
+    __shared__ float2 s_u[32][33];  // [j local][k]
+    const TcTrailUnit tu = tu_list[blockIdx.y];
+    const int j0 = blockIdx.x * 32;
+    if (2 * j0 >= tu.n2_pad) return;
+    const int s = systems[tu.unit].s;
+    const float2 *A = a32buf + smu[tu.unit].a32_off;
+    for (int e = threadIdx.x; e < 32 * 32; e += blockDim.x) {
+        const int k = e / 32, jj = e % 32, j = j0 + jj;
+        s_u[jj][k] = j < tu.m ? A[(int64_t)(c0 + k) * s + c0 + 32 + j] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    for (int e = threadIdx.x; e < 64 * 32; e += blockDim.x) {  // 64 B rows (2j + sgn) x 32 k
+        const int rr = e / 32, k = e % 32, jj = rr >> 1, sg = rr & 1;
+        const int64_t row = 2 * (int64_t)j0 + rr;
+        if (row >= tu.n2_pad) continue;
+        const float2 u = s_u[jj][k];
+        const float x0 = sg ? u.y : u.x;   // k-block 0
+        const float x1 = sg ? u.x : -u.y;  // k-block 1
+        float h, l;
+        const int64_t o0 = (tu.b_base + row) * 32 + k, o1 = (tu.b_base + tu.n2_pad + row) * 32 + k;
+        split_tf32(x0, h, l);
+        hi[o0] = h;
+        lo[o0] = l;
+        split_tf32(x1, h, l);
+        hi[o1] = h;
+        lo[o1] = l;
     }
 }
 
@@ -401,6 +504,83 @@ cudaError_t tc_gram_plan(const std::vector<UnitDesc> &systems, TcGramPlan &p) {
     }
     p.rows = rows;
     return cudaSuccess;
+}
+
+cudaError_t tc_trail_plan(const std::vector<int> &s_desc, const std::vector<int32_t> &order, int n, int min_m,
+                          TcTrailPlan &p) {
+    p.units.clear();
+    p.u_off.assign(1, 0);
+    p.max_tiles.clear();
+    p.max_mpad.clear();
+    p.max_n2pad.clear();
+    auto pad = [](int64_t x) { return (int32_t)((x + BM - 1) / BM * BM); };
+    std::vector<int64_t> a_base(n), b_base(n);
+    int64_t rows = 0;
+    for (int q = 0; q < n; ++q) {  // stack rows sized for the unit's first step
+        const int64_t m0 = std::max(0, s_desc[q] - 32);
+        a_base[q] = rows;
+        rows += 2 * (int64_t)pad(m0);
+        b_base[q] = rows;
+        rows += 2 * (int64_t)pad(2 * m0);
+    }
+    p.rows = rows;
+    const int max_s = n > 0 ? s_desc[0] : 0;
+    for (int c0 = 0; c0 < max_s; c0 += 32) {
+        int32_t mt = 0, mm = 0, mn = 0;
+        for (int q = 0; q < n && s_desc[q] - c0 - 32 >= min_m; ++q) {
+            TcTrailUnit t;
+            t.unit = order[q];
+            t.m = s_desc[q] - c0 - 32;
+            t.m_pad = pad(t.m);
+            t.n2_pad = pad(2 * (int64_t)t.m);
+            t.a_base = a_base[q];
+            t.b_base = b_base[q];
+            p.units.push_back(t);
+            mt = std::max(mt, (t.m_pad / BM) * (t.n2_pad / BN));
+            mm = std::max(mm, t.m_pad);
+            mn = std::max(mn, t.n2_pad);
+        }
+        p.u_off.push_back((int32_t)p.units.size());
+        p.max_tiles.push_back(mt);
+        p.max_mpad.push_back(mm);
+        p.max_n2pad.push_back(mn);
+    }
+    return cudaSuccess;
+}
+
+bool tc_trail_maps(TcTrailPlan &p, const float *hi, const float *lo) {
+    p.ready = make_map(&p.m_hi, hi, p.rows) && make_map(&p.m_lo, lo, p.rows);
+    return p.ready;
+}
+
+cudaError_t tc_trail_run(const TcTrailPlan &p, int step, int count, const TcTrailUnit *d_trail, const UnitDesc *d_systems,
+                         const MixedUnit *d_smu, float2 *a32, float *hi, float *lo, int32_t *status, cudaStream_t st) {
+    const int na = std::min(count, p.active(step));
+    if (na <= 0) return cudaSuccess;
+    const TcTrailUnit *tl = d_trail + p.u_off[step];
+    const int c0 = 32 * step;
+    k_split_trail_a<<<dim3((unsigned)(p.max_mpad[step] / 8), (unsigned)na), 256, 0, st>>>(tl, d_systems, d_smu, a32,
+                                                                                         c0, hi, lo);
+    k_split_trail_b<<<dim3((unsigned)((p.max_n2pad[step] / 2 + 31) / 32), (unsigned)na), 256, 0, st>>>(
+        tl, d_systems, d_smu, a32, c0, hi, lo);
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<TC_EPI_TRAIL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)tc_smem_bytes());
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    TcEpilogue ep{};
+    ep.units = d_systems;
+    ep.mus = d_smu;
+    ep.a32 = a32;
+    ep.status = status;
+    ep.status_of_tile = 1;
+    ep.c0 = c0;
+    ep.trail = tl;
+    k_tc_gemm<TC_EPI_TRAIL><<<dim3((unsigned)p.max_tiles[step], (unsigned)na), TC_THREADS, tc_smem_bytes(), st>>>(
+        p.m_hi, p.m_lo, p.m_hi, p.m_lo, nullptr, ep);
+    return cudaGetLastError();
 }
 
 bool tc_gram_maps(TcGramPlan &p, const float *hi, const float *lo) {

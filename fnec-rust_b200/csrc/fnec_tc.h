@@ -11,6 +11,22 @@ namespace fnec {
 
 constexpr int TC_EPI_STORE = 0;  // C[R][C] = D (row-major FP32), bounds m x n
 constexpr int TC_EPI_GRAM = 1;   // complex Gram combine into the unit's A32
+constexpr int TC_EPI_TRAIL = 2;  // A22 -= L21 U12 of one factor step, into the unit's A32
+
+// One unit's trailing update at one factor step (TC_EPI_TRAIL).  The
+// complex product L21 U12 (m x 32 times 32 x m) runs as one real GEMM of
+// K = 64 whose output columns interleave (Re, Im) like A32 itself:
+//   A[i][k] = Re L(i,k), A[i][32+k] = Im L(i,k)
+//   B[2j][k] = Re U(k,j), B[2j][32+k] = -Im U(k,j)
+//   B[2j+1][k] = Im U(k,j), B[2j+1][32+k] = Re U(k,j)
+// so D[i][2j+s] = (Re, Im) of (L U)(i,j).
+struct TcTrailUnit {
+    int32_t unit;    // system index
+    int32_t m;       // trailing rows (= columns) at this step: s - c0 - 32
+    int32_t m_pad;   // m rounded up to 128: A rows per k-block
+    int32_t n2_pad;  // 2m rounded up to 128: B rows per k-block
+    int64_t a_base, b_base;  // first rows of the unit's A and B in the stacks
+};
 
 // One 128x128 output tile.  Operand rows of k-block kb start at
 // a_row + kb * a_kstride (A) and b_row + kb * b_kstride (B) of the
@@ -34,6 +50,9 @@ struct TcEpilogue {
     // both: a CTA whose waits ran out marks status[unit] (or status[0])
     int32_t *status;
     int32_t status_of_tile;
+    // TC_EPI_TRAIL: the step and its units (blockIdx.y), tiles from blockIdx.x
+    int32_t c0;
+    const TcTrailUnit *trail;
 };
 
 // Gram operand layout of one unit: T (2N x N) as kblocks k-blocks of rpad
@@ -53,6 +72,29 @@ struct TcGramPlan {
     CUtensorMap m_hi, m_lo;
     bool ready = false;
 };
+
+// The tensor-core trailing updates of the mixed factor: the units at
+// positions [0, n) of the s-descending order, at every step where their
+// trailing block has at least min_m rows.  Each unit owns operand rows in
+// the stacks sized for its first step; later steps reuse them.
+struct TcTrailPlan {
+    std::vector<TcTrailUnit> units;  // every step's units, concatenated
+    std::vector<int32_t> u_off;      // per step: first entry (steps + 1 values)
+    std::vector<int32_t> max_tiles, max_mpad, max_n2pad;  // per step
+    int64_t rows = 0;                // rows of each stack (hi, lo)
+    CUtensorMap m_hi, m_lo;
+    bool ready = false;
+    int steps() const { return (int)u_off.size() - 1; }
+    int active(int step) const { return step < steps() ? u_off[step + 1] - u_off[step] : 0; }
+};
+cudaError_t tc_trail_plan(const std::vector<int> &s_desc, const std::vector<int32_t> &order, int n, int min_m,
+                          TcTrailPlan &p);
+bool tc_trail_maps(TcTrailPlan &p, const float *hi, const float *lo);
+// Step `step` (c0 = 32 step): split L21 / U12 of the step's first `count`
+// units (<= active(step)) into the stacks, then the GEMM subtracting
+// L21 U12 from each one's A22.
+cudaError_t tc_trail_run(const TcTrailPlan &p, int step, int count, const TcTrailUnit *d_trail, const UnitDesc *d_systems,
+                         const MixedUnit *d_smu, float2 *a32, float *hi, float *lo, int32_t *status, cudaStream_t st);
 
 cudaError_t tc_gram_plan(const std::vector<UnitDesc> &systems, TcGramPlan &p);
 // Tensor maps over the hi / lo stacks (rows x 32 floats each); false when

@@ -479,6 +479,11 @@ typedef struct {
     int32_t block_inverse; /* mixed: 1 the refinement applies the factor's 32x32
                               diagonal blocks through their FP64 inverses (block
                               products); 0 by substitution in one warp            */
+    int32_t tensor_trailing;/* mixed: 1 trailing updates of >= 192 rows run on
+                              tcgen05 (3xTF32, complex as one real GEMM of K 64);
+                              0 all as FP32 SIMT tiles                            */
+    int32_t gmres_ctas_per_sm;/* mixed: 3 or 4 refinement CTAs per SM (the
+                              register budget of the one-CTA-per-solve kernel)    */
 } fnec_schedule;
 
 /* Graph state of a batch (fnec_batch_graph_state). */
@@ -503,7 +508,7 @@ int fnec_batch_set_schedule(fnec_batch *b, const fnec_schedule *s);
 /* state: FNEC_GRAPH_*; nodes: kernel launches one replay issues. */
 int fnec_batch_graph_state(const fnec_batch *b, int32_t *state, uint64_t *nodes);
 /* Time the batch under candidate schedules (coordinate descent over the
- * fields above, reps timed runs each after one warm-up, median device time
+ * fields above, two passes; reps timed runs each after one warm-up, median device time
  * on the batch stream), set the fastest and record it in the process-wide
  * tuning cache under the batch's shape key.  Batches created later with
  * the same key start from the cached schedule.  With reps == 0 the cached

@@ -98,7 +98,7 @@ def test_graph_capture_and_replay(acc, plain_ants):
 def test_schedule_rejects_out_of_range(acc, plain_ants):
     b = acc.HallenBatch(plain_ants[:2], precision=acc.PRECISION_FP64)
     for bad in ({"class_shift": 3}, {"gmres_cluster": 3}, {"graph": 5}, {"grid_panels": -1}, {"factor_streams": 3},
-                {"unit_factor": 2}, {"block_inverse": 5}):
+                {"unit_factor": 2}, {"block_inverse": 5}, {"tensor_trailing": -1}, {"gmres_ctas_per_sm": 2}):
         with pytest.raises(acc.AccelError) as e:
             b.schedule = bad
         assert e.value.code == acc.ERR_BAD_ARG
@@ -112,6 +112,8 @@ def test_schedule_rejects_out_of_range(acc, plain_ants):
     {"factor_streams": 4}, {"factor_streams": 2, "class_shift": 2, "graph": 2},
     {"unit_factor": 0}, {"unit_factor": 1, "factor_streams": 4, "graph": 2},
     {"block_inverse": 0}, {"block_inverse": 1, "gmres_cluster": 4},
+    {"tensor_trailing": 0}, {"tensor_trailing": 1, "factor_streams": 4, "unit_factor": 0},
+    {"gmres_ctas_per_sm": 4}, {"gmres_ctas_per_sm": 4, "block_inverse": 0},
 ])
 def test_mixed_within_gate_under_every_schedule(acc, sched):
     ants = _ants(acc, 20, seed=32)  # few solves: clusters up to 8 CTAs fit
@@ -166,7 +168,9 @@ def test_mixed_factor_groups_give_identical_bits(acc):
     the same."""
     ants = _ants(acc, 32, seed=35)
     b = acc.HallenBatch(ants, precision=acc.PRECISION_MIXED)
-    b.schedule = {"factor_streams": 1, "unit_factor": 0, "graph": 0}
+    # all trailing updates as FP32 SIMT tiles: the whole-unit kernel repeats
+    # the per-step kernels' arithmetic
+    b.schedule = {"factor_streams": 1, "unit_factor": 0, "tensor_trailing": 0, "graph": 0}
     ref = _bits(_run(b))
     for sched in ({"factor_streams": 2}, {"factor_streams": 4}, {"factor_streams": 4, "graph": 2},
                   {"unit_factor": 1, "factor_streams": 1}, {"unit_factor": 1, "factor_streams": 4}):
@@ -174,4 +178,37 @@ def test_mixed_factor_groups_give_identical_bits(acc):
         got = _bits(_run(b, times=2))
         for r, g in zip(ref, got):
             assert np.array_equal(r, g), sched
+    # tensor-core trailing updates: the same units take them in every grouping
+    b.schedule = {"factor_streams": 1, "unit_factor": 1, "tensor_trailing": 1, "graph": 0}
+    ref = _bits(_run(b))
+    for sched in ({"factor_streams": 2}, {"factor_streams": 4, "graph": 2}):
+        b.schedule = sched
+        got = _bits(_run(b, times=2))
+        for r, g in zip(ref, got):
+            assert np.array_equal(r, g), sched
     b.close()
+
+
+@pytest.mark.parametrize("cells", [9, 12])
+def test_tensor_core_trailing_keeps_the_refinement(acc, cells):
+    """The factor's trailing updates on tcgen05 (3xTF32) give a preconditioner
+    as good as the FP32 SIMT one: the same answer within the gate and no more
+    than one extra refinement iteration."""
+    wl, src, f = bench.mesh_workload(cells)
+    ant = [acc.Antenna(acc.wires_array(wl), acc.sources_array(src), [f], acc.GROUND_PEC, None)]
+    plain = acc.HallenBatch(ant, precision=acc.PRECISION_FP64)
+    zp = _zin(_run(plain))[0]
+    plain.close()
+    out = {}
+    for tt in (0, 1):
+        b = acc.HallenBatch(ant, precision=acc.PRECISION_MIXED)
+        assert b.info.max_s - 32 >= 192
+        b.schedule = {"tensor_trailing": tt}
+        res = _run(b)
+        assert np.all(res.status == 0)
+        it, rs = b.refinement_stats()
+        out[tt] = (_zin(res)[0], int(it.max()))
+        b.close()
+    for tt, (zm, it) in out.items():
+        assert abs(zm - zp) <= 1e-6 * abs(zp), tt
+    assert out[1][1] <= out[0][1] + 1
