@@ -311,7 +311,9 @@ def phase_rooflines(form, o, n, s, g, d, shapes, fma, muladd, ffma, peaks, runs)
         n_s = np.array([u["n"] for u in shapes], np.float64)
         s_s = np.array([u["s"] for u in shapes], np.float64)
         its = it if it is not None and len(it) == len(n_s) else np.full(len(n_s), 5.0)
-        byt = float(np.sum((its + 2) * (32 * n_s * n_s + 8 * s_s * s_s)))
+        # per operator + preconditioner application: Z once (16 N^2), the
+        # FP32 factor (8 S^2), its diagonal block inverses (1 KB per row)
+        byt = float(np.sum((its + 2) * (16 * n_s * n_s + 8 * s_s * s_s + 1024 * s_s)))
         put("solve", byt / 1e9, peaks["hbm_gbs"], "GB/s", "hbm", peaks["source"])
     dd = np.asarray(d, np.float64)
     nr = np.asarray(runs, np.float64)
