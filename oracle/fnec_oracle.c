@@ -543,6 +543,94 @@ int or_hallen_rhs_paths(const or_seg *segs, int64_t n, double freq_hz, const or_
     return OR_OK;
 }
 
+/* loads.rs:34-57 i0_over_i1: I0(z)/I1(z) by the power series for |z| <= 15,
+ * the asymptotic expansion beyond. */
+static c64 i0_over_i1(c64 z) {
+    if (cnorm(z) > 15.0) {
+        c64 inv = cdiv(cmk(1.0, 0.0), z);
+        return cadd(cadd(cmk(1.0, 0.0), cmk(inv.re * 0.5, inv.im * 0.5)),
+                    (c64){cmul(inv, inv).re * 0.375, cmul(inv, inv).im * 0.375});
+    }
+    c64 half = cmk(z.re * 0.5, z.im * 0.5);
+    c64 half_sq = cmul(half, half);
+    c64 i0 = cmk(1.0, 0.0), term0 = cmk(1.0, 0.0);
+    c64 i1 = half, term1 = half;
+    for (int k = 1; k < 300; ++k) {
+        double kf = (double)k;
+        term0 = cmul(term0, cdivr(half_sq, kf * kf));
+        i0 = cadd(i0, term0);
+        term1 = cmul(term1, cdivr(half_sq, kf * (kf + 1.0)));
+        i1 = cadd(i1, term1);
+        if (cnorm(term0) <= 1e-17 * cnorm(i0) && cnorm(term1) <= 1e-17 * cnorm(i1)) break;
+    }
+    return cdiv(i0, i1);
+}
+
+/* loads.rs:73-81 wire_internal_impedance (skin-effect series impedance). */
+static c64 wire_internal_impedance(double sigma, double a, double dl, double omega) {
+    const double MU0 = 4.0 * OR_PI * 1e-7;
+    if (omega <= 0.0) return cmk(dl / (sigma * OR_PI * a * a), 0.0);
+    double delta = sqrt(2.0 / (omega * MU0 * sigma));
+    c64 gamma = cmk(1.0 / delta, 1.0 / delta);
+    c64 g = cdivr(gamma, 2.0 * OR_PI * a * sigma);
+    c64 r = cmul(g, i0_over_i1(crs(a, gamma)));
+    return cmk(r.re * dl, r.im * dl);
+}
+
+/* loads.rs:209-222 segment_matches. */
+static int load_matches(const or_load *ld, const or_seg *s) {
+    if (ld->tag != 0 && s->tag != ld->tag) return 0;
+    if (ld->seg_first == 0) return 1;
+    uint32_t last = ld->seg_last == 0 ? ld->seg_first : ld->seg_last;
+    return s->tag_index >= ld->seg_first && s->tag_index <= last;
+}
+
+int64_t or_build_loads(const or_seg *segs, int64_t n, double freq_hz, const or_load *ld, int64_t nl,
+                       double *out) {
+    for (int64_t i = 0; i < 2 * n; ++i) out[i] = 0.0;
+    const double omega = 2.0 * OR_PI * freq_hz;
+    int64_t ignored = 0;
+    for (int64_t q = 0; q < nl; ++q) {
+        const or_load *L = &ld[q];
+        if (L->load_type < 0 || L->load_type > 5) {  /* unsupported: warned, ignored */
+            ignored++;
+            continue;
+        }
+        for (int64_t i = 0; i < n; ++i) {
+            if (!load_matches(L, &segs[i])) continue;
+            c64 z;
+            switch (L->load_type) {
+            case 0: {
+                double x_l = omega * L->f2;
+                double x_c = L->f3 > 0.0 ? 1.0 / (omega * L->f3) : 0.0;
+                z = cmk(L->f1, x_l - x_c);
+                break;
+            }
+            case 1: {
+                c64 y = cmk(0.0, 0.0);
+                if (L->f1 > 0.0) y = cadd(y, cmk(1.0 / L->f1, 0.0));
+                if (L->f2 > 0.0) y = cadd(y, cmk(0.0, -1.0 / (omega * L->f2)));
+                if (L->f3 > 0.0) y = cadd(y, cmk(0.0, omega * L->f3));
+                z = cnorm(y) < 1e-30 ? cmk(0.0, 0.0) : cdiv(cmk(1.0, 0.0), y);
+                break;
+            }
+            case 2: z = cmk(L->f1, omega * L->f2); break;
+            case 3: z = cmk(L->f1, -(L->f3 > 0.0 ? 1.0 / (omega * L->f3) : 0.0)); break;
+            case 4: z = cmk(L->f1, L->f2); break;
+            default: /* 5 */
+                if (L->f1 <= 0.0) {
+                    ignored++;
+                    continue;
+                }
+                z = wire_internal_impedance(L->f1, segs[i].radius, segs[i].length, omega);
+                break;
+            }
+            cst(&out[2 * i], cadd(cld(&out[2 * i]), z));
+        }
+    }
+    return ignored;
+}
+
 /* ------------------------------------------------------------------------- */
 /* Z-matrix fill                                                              */
 /* ------------------------------------------------------------------------- */
@@ -1136,6 +1224,16 @@ int64_t or_rp_card_points(uint32_t n_theta, uint32_t n_phi, double theta0, doubl
 /* Whole per-frequency solve (CLI standard Hallen branch)                     */
 /* ------------------------------------------------------------------------- */
 
+/* solve_session.rs:1285-1289: the LD loads on Z's diagonal (matrix.rs:131-139
+ * add_to_diagonal), before the branch is chosen. */
+static void add_loads(const or_problem *p, const or_seg *segs, int64_t n, double *z) {
+    if (!p->loads || p->n_loads <= 0) return;
+    double *ld = (double *)malloc(sizeof(double) * 2 * (size_t)(n > 0 ? n : 1));
+    or_build_loads(segs, n, p->freq_hz, p->loads, p->n_loads, ld);
+    for (int64_t i = 0; i < n; ++i) cst(&z[2 * (i * n + i)], cadd(cld(&z[2 * (i * n + i)]), cld(&ld[2 * i])));
+    free(ld);
+}
+
 int or_solve_problem(or_problem *p) {
     int64_t cap = 0;
     for (int64_t w = 0; w < p->n_wires; ++w) cap += p->wires[w].segments;
@@ -1166,6 +1264,7 @@ int or_solve_problem(or_problem *p) {
             if (st == OR_OK) {
                 z = (double *)malloc(sizeof(double) * 2 * (size_t)(n * n));
                 or_assemble_z(segs, n, p->freq_hz, p->ground, z);
+                add_loads(p, segs, n, z);
                 st = or_solve_hallen_paths(z, n, rhs, cosv, path_of, fe, 2 * np, x, p->pivots, NULL, 0, 1);
             }
             if (st == OR_OK) {
@@ -1199,6 +1298,7 @@ int or_solve_problem(or_problem *p) {
     }
     double *z = (double *)malloc(sizeof(double) * 2 * (size_t)(n * n));
     or_assemble_z(segs, n, p->freq_hz, p->ground, z);
+    add_loads(p, segs, n, z);
     int64_t w = or_merge_collinear(segs, n, NULL, 0);
     int64_t *ep = (int64_t *)malloc(sizeof(int64_t) * 2 * (size_t)w);
     or_merge_collinear(segs, n, ep, w);

@@ -134,6 +134,24 @@ void or_radiation_pattern(const or_seg *segs, int64_t n, const double *cur, doub
 int64_t or_rp_card_points(uint32_t n_theta, uint32_t n_phi, double theta0, double phi0,
                           double d_theta, double d_phi, double *pts);
 
+/* One LD card (nec_model card.rs:265-279): load type 0-5, tag (0 = every
+ * tag), first and last segment (0 = every segment of the tag; last 0 =
+ * first), F1..F3. */
+typedef struct {
+    int32_t load_type;
+    uint32_t tag;
+    uint32_t seg_first;
+    uint32_t seg_last;
+    double f1, f2, f3;
+} or_load;
+
+/* loads.rs:103-222 build_loads: the series load impedance of every segment
+ * (2*n doubles) summed over the cards in deck order.  Returns the number of
+ * cards (or card/segment pairs for type 5 with sigma <= 0) ignored with a
+ * warning by the reference. */
+int64_t or_build_loads(const or_seg *segs, int64_t n, double freq_hz, const or_load *ld, int64_t nl,
+                       double *out);
+
 /* A whole per-frequency solve of the CLI standard Hallen branch
  * (solve_session.rs:1186-1437 + :1645): geometry -> rhs -> Z -> merged
  * endpoints + junctions -> solve_hallen -> feedpoints -> pattern.  */
@@ -153,6 +171,8 @@ typedef struct {
     double *pattern;      /* 4 * n_points */
     int32_t *pivots;      /* S, optional */
     int status;
+    const or_load *loads; /* LD cards in deck order; may be NULL */
+    int64_t n_loads;
 } or_problem;
 
 /* Solve one problem; returns its status. */

@@ -58,7 +58,21 @@ class _Problem(ctypes.Structure):
         ("pattern", _P),
         ("pivots", _P),
         ("status", ctypes.c_int),
+        ("loads", _P),
+        ("n_loads", _I64),
     ]
+
+
+LOAD_DTYPE = np.dtype([("load_type", np.int32), ("tag", np.uint32), ("seg_first", np.uint32),
+                       ("seg_last", np.uint32), ("f1", np.float64), ("f2", np.float64), ("f3", np.float64)])
+
+
+def loads_array(loads) -> np.ndarray:
+    """loads: iterable of LD cards (type, tag, seg_first, seg_last, f1, f2, f3)."""
+    arr = np.zeros(len(loads), dtype=LOAD_DTYPE)
+    for i, (t, tag, s0, s1, f1, f2, f3) in enumerate(loads):
+        arr[i] = (t, tag, s0, s1, f1, f2, f3)
+    return arr
 
 
 def build() -> str:
@@ -102,6 +116,8 @@ def lib():
         L.or_solve_hallen_paths.restype = ctypes.c_int
         L.or_solve_hallen_paths.argtypes = [_P, _I64, _P, _P, _P, _P, _I64, _P, _P, _P, ctypes.c_int,
                                             ctypes.c_int]
+        L.or_build_loads.restype = _I64
+        L.or_build_loads.argtypes = [_P, _I64, _D, _P, _I64, _P]
         L.or_solve_square.restype = ctypes.c_int
         L.or_solve_square.argtypes = [_P, _P, _I64, _P, _P, ctypes.c_int]
         L.or_feedpoints.restype = _I64
@@ -293,6 +309,15 @@ def solve_hallen_paths(z, rhs, cosv, paths: ConductorPaths, nthreads=1):
     return x, piv[:s]
 
 
+def build_loads(segs, freq_hz, loads):
+    """loads.rs build_loads: (per-segment load impedance, ignored count)."""
+    n = len(segs)
+    out = np.zeros(max(n, 1), np.complex128)
+    ld = np.ascontiguousarray(loads, LOAD_DTYPE)
+    ign = lib().or_build_loads(_ptr(segs), n, float(freq_hz), _ptr(ld), len(ld), _ptr(out))
+    return out[:n], int(ign)
+
+
 def solve_square(a, b, nthreads=1):
     s = a.shape[0]
     a = np.array(a, np.complex128, order="C")
@@ -341,7 +366,8 @@ class Problem:
     degree-2 conductor-path branch when some path is non-trivial
     (:1338-1378), else the standard branch."""
 
-    def __init__(self, wires, sources, freq_hz, ground=GROUND_FREE, points=None):
+    def __init__(self, wires, sources, freq_hz, ground=GROUND_FREE, points=None, loads=None):
+        self.loads = None if loads is None or len(loads) == 0 else np.ascontiguousarray(loads, LOAD_DTYPE)
         self.wires = np.ascontiguousarray(wires)
         self.sources = np.ascontiguousarray(sources)
         self.freq_hz = float(freq_hz)
@@ -358,7 +384,8 @@ class Problem:
         self._s = _Problem(
             _ptr(self.wires), len(self.wires), _ptr(self.sources), len(self.sources), self.ground,
             self.freq_hz, _ptr(self.points), npts, _ptr(self.currents), _ptr(self.feed),
-            _ptr(self.n_feed), _ptr(self.pattern), _ptr(self.pivots), 0)
+            _ptr(self.n_feed), _ptr(self.pattern), _ptr(self.pivots), 0, _ptr(self.loads),
+            0 if self.loads is None else len(self.loads))
 
     @property
     def status(self):

@@ -23,6 +23,14 @@ def deck_arrays(deck):
     return wires, sources, pts
 
 
+def deck_loads(deck):
+    """The deck's LD cards as the oracle's load array (None without any)."""
+    from oracle import oracle as O
+
+    ld = deck.get("loads") or []
+    return O.loads_array([tuple(x) for x in ld]) if ld else None
+
+
 def golden_zins(case):
     """Golden feedpoint impedances as {freq_hz: [z per source]}."""
     fp = case["feedpoint_impedance"]

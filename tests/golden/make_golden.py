@@ -3,9 +3,9 @@ committed fixture (tests/golden/corpus_golden.json).
 
 Source: corpus/reference-results.json and the corpus/*.nec decks of
 dc0sk/fnec-rust, read as text.  Only decks built from GW/GE/GN/EX/FR/RP
-cards (no GM/GR transforms, loads, TL/NT networks or plane waves) are kept:
+and LD cards (no GM/GR transforms, TL/NT networks or plane waves) are kept:
 those are the cases that exercise exactly the hot path (geometry, Hallen
-RHS, Z fill, normal-equation solve, feedpoint, RP pattern).
+RHS, Z fill, load stamps, normal-equation solve, feedpoint, RP pattern).
 
 Run in a checkout that has the reference mounted:
     python tests/golden/make_golden.py /path/to/fnec-rust
@@ -27,12 +27,16 @@ CASES = [
     "yagi-5elm-51seg",
     "frequency-sweep-dipole",
     "multi-source",
+    "dipole-loaded",
+    "dipole-ld-loaded-51seg",
+    "dipole-ld-series-rl-51seg",
+    "dipole-ld-series-rc-51seg",
 ]
 
 
 def parse_deck(text: str) -> dict:
-    """Minimal NEC card reader for GW/GN/GE/EX/FR/RP (columns as in NEC-2)."""
-    deck = {"wires": [], "sources": [], "ground": 0, "freqs": [], "rp": None}
+    """Minimal NEC card reader for GW/GN/GE/EX/FR/RP/LD (columns as in NEC-2)."""
+    deck = {"wires": [], "sources": [], "ground": 0, "freqs": [], "rp": None, "loads": []}
     ge_flag = 0
     gn = None
     for line in text.splitlines():
@@ -62,6 +66,12 @@ def parse_deck(text: str) -> dict:
             fi, si = (4, 5) if len(g) >= 6 else (2, 3)
             nfr, f0, df = int(g[1]), float(g[fi]), float(g[si])
             deck["freqs"] = [(f0 + i * df) * 1e6 for i in range(max(nfr, 1))]
+        elif card == "LD":
+            # nec_parser/src/lib.rs:325-355: I1 type, I2 tag, I3/I4 segments,
+            # F1-F3 defaulting to 0
+            g = f[1:]
+            fl = [float(x) for x in g[4:7]] + [0.0] * (3 - len(g[4:7]))
+            deck["loads"].append([int(g[0]), int(g[1]), int(g[2]), int(g[3])] + fl)
         elif card == "RP":
             # nec_parser/src/lib.rs:293-325: angles start at field 4 with
             # XNDA present (>= 8 fields), else at field 3.

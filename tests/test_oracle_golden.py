@@ -11,7 +11,7 @@ significant digits, phases 4 decimals.
 import numpy as np
 import pytest
 
-from _corpus import deck_arrays, golden_zins, load_cases
+from _corpus import deck_arrays, deck_loads, golden_zins, load_cases
 from oracle import oracle as O
 
 CASES = load_cases()
@@ -37,7 +37,8 @@ def test_feedpoint_impedance_matches_golden(name):
     case = CASES[name]
     wires, sources, _ = deck_arrays(case["deck"])
     for f, zs in golden_zins(case).items():
-        p = O.solve_problem(O.Problem(wires, sources, f, ground=case["deck"]["ground"]))
+        p = O.solve_problem(O.Problem(wires, sources, f, ground=case["deck"]["ground"],
+                                      loads=deck_loads(case["deck"])))
         assert p.status == 0
         assert len(p.zin) == len(zs)
         for got, want in zip(p.zin, zs):
