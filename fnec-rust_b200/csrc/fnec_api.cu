@@ -126,7 +126,94 @@ struct HostAnt {
     std::vector<double> arc;        // 2n: signed arc length of each midpoint, then its sign
     std::vector<int64_t> free_ends; // 2 per path: I = 0 rows
     int64_t cols() const { return paths ? (int64_t)free_ends.size() / 2 : (int64_t)ep.size(); }
+    std::vector<fnec_load> loads;   // LD cards, deck order
 };
+
+// num-complex 0.4.6 arithmetic on the host, each operation separately
+// rounded (this file is built without FMA contraction)
+struct HC {
+    double re, im;
+};
+inline HC hc_add(HC a, HC b) { return {a.re + b.re, a.im + b.im}; }
+inline HC hc_mul(HC a, HC b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+inline HC hc_div(HC a, HC b) {
+    const double n = b.re * b.re + b.im * b.im;
+    return {(a.re * b.re + a.im * b.im) / n, (a.im * b.re - a.re * b.im) / n};
+}
+inline HC hc_scale(HC a, double s) { return {a.re * s, a.im * s}; }
+inline HC hc_divr(HC a, double s) { return {a.re / s, a.im / s}; }
+inline double hc_norm(HC a) { return std::hypot(a.re, a.im); }
+
+// I0(z)/I1(z) (loads.rs:34-57): power series up to |z| = 15, the
+// asymptotic expansion beyond.
+HC bessel_i0_over_i1(HC z) {
+    if (hc_norm(z) > 15.0) {
+        const HC inv = hc_div({1.0, 0.0}, z);
+        return hc_add(hc_add({1.0, 0.0}, hc_scale(inv, 0.5)), hc_scale(hc_mul(inv, inv), 0.375));
+    }
+    const HC half = hc_scale(z, 0.5), half_sq = hc_mul(half, half);
+    HC i0{1.0, 0.0}, t0{1.0, 0.0}, i1 = half, t1 = half;
+    for (int k = 1; k < 300; ++k) {
+        const double kf = (double)k;
+        t0 = hc_mul(t0, hc_divr(half_sq, kf * kf));
+        i0 = hc_add(i0, t0);
+        t1 = hc_mul(t1, hc_divr(half_sq, kf * (kf + 1.0)));
+        i1 = hc_add(i1, t1);
+        if (hc_norm(t0) <= 1e-17 * hc_norm(i0) && hc_norm(t1) <= 1e-17 * hc_norm(i1)) break;
+    }
+    return hc_div(i0, i1);
+}
+
+// Series load impedance of every segment at one frequency (loads.rs:103-222,
+// the cards summed in deck order); exact zeros where no card applies.
+void segment_loads(const HostAnt &h, double freq_hz, std::vector<HC> &out) {
+    const double PI_ = 3.14159265358979323846;
+    const double TWO_PI = 2.0 * PI_, MU0 = 4.0 * PI_ * 1e-7;
+    const double omega = TWO_PI * freq_hz;
+    out.assign(h.segs.size(), HC{0.0, 0.0});
+    for (const fnec_load &L : h.loads) {
+        if (L.load_type < 0 || L.load_type > 5) continue;  // the reference warns and ignores it
+        if (L.load_type == 5 && L.f1 <= 0.0) continue;     // sigma <= 0: likewise
+        for (size_t i = 0; i < h.segs.size(); ++i) {
+            const DevSeg &s = h.segs[i];
+            if (L.tag != 0 && s.tag != L.tag) continue;  // segment_matches (loads.rs:209-222)
+            if (L.seg_first != 0) {
+                const uint32_t last = L.seg_last == 0 ? L.seg_first : L.seg_last;
+                if (s.tag_index < L.seg_first || s.tag_index > last) continue;
+            }
+            HC z{0.0, 0.0};
+            switch (L.load_type) {
+            case 0:
+                z = {L.f1, omega * L.f2 - (L.f3 > 0.0 ? 1.0 / (omega * L.f3) : 0.0)};
+                break;
+            case 1: {
+                HC y{0.0, 0.0};
+                if (L.f1 > 0.0) y = hc_add(y, {1.0 / L.f1, 0.0});
+                if (L.f2 > 0.0) y = hc_add(y, {0.0, -1.0 / (omega * L.f2)});
+                if (L.f3 > 0.0) y = hc_add(y, {0.0, omega * L.f3});
+                z = hc_norm(y) < 1e-30 ? HC{0.0, 0.0} : hc_div({1.0, 0.0}, y);
+                break;
+            }
+            case 2: z = {L.f1, omega * L.f2}; break;
+            case 3: z = {L.f1, -(L.f3 > 0.0 ? 1.0 / (omega * L.f3) : 0.0)}; break;
+            case 4: z = {L.f1, L.f2}; break;
+            default: {  // 5: round-wire skin-effect impedance (loads.rs:73-81)
+                const double sigma = L.f1, rad = s.rad, dl = s.len;
+                if (omega <= 0.0) {
+                    z = {dl / (sigma * PI_ * rad * rad), 0.0};
+                } else {
+                    const double delta = std::sqrt(2.0 / (omega * MU0 * sigma));
+                    const HC gamma{1.0 / delta, 1.0 / delta};
+                    z = hc_scale(hc_mul(hc_divr(gamma, TWO_PI * rad * sigma), bessel_i0_over_i1(hc_scale(gamma, rad))),
+                                 dl);
+                }
+                break;
+            }
+            }
+            out[i] = hc_add(out[i], z);
+        }
+    }
+}
 
 }  // namespace
 
@@ -472,6 +559,7 @@ struct fnec_batch {
     std::vector<double> cos_given;
     bool rhs_given_flag = false;
     std::vector<double> z_given;  // caller-supplied Z for every unit (fill skipped)
+    std::vector<DevStamp> stamps; // LD load stamps on the filled Z
     std::vector<fnec_unit_info> uinfo;
     int max_s = 0, max_n = 0;
     int64_t tot_seg = 0, z_el = 0, a_el = 0, x_el = 0, rhs_el = 0, pat_el = 0, feed_rows = 0, cos_el = 0,
@@ -500,6 +588,7 @@ struct fnec_batch {
     int4 *d_fill_tiles = nullptr, *d_gram_tiles = nullptr;
     int64_t *d_feed_row_off = nullptr;
     double *d_rhs_given = nullptr, *d_cos_given = nullptr, *d_z_given = nullptr;
+    DevStamp *d_stamps = nullptr;
     cx *d_z = nullptr, *d_a = nullptr, *d_x = nullptr, *d_rhs = nullptr;
     double *d_cos = nullptr;
     int32_t *d_piv = nullptr, *d_status = nullptr;
@@ -890,6 +979,13 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
             u.piv_off = b->piv_el;
             u.n_rhs = a.n_rhs;
             u.sys = (int32_t)b->units.size();
+            if (need_solve && !h.loads.empty()) {  // LD loads on this system's Z diagonal
+                std::vector<HC> lv;
+                segment_loads(h, f, lv);
+                for (int i = 0; i < n; ++i)
+                    if (lv[i].re != 0.0 || lv[i].im != 0.0)  // adding an exact zero changes nothing
+                        b->stamps.push_back(DevStamp{u.z_off + (int64_t)i * n + i, lv[i].re, lv[i].im});
+            }
             if (need_solve) {
                 b->z_el += (int64_t)n * n;
                 b->a_el += (int64_t)s * (s + 1);
@@ -959,7 +1055,8 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
            o_feeds = pk.add(b->feeds), o_cons = pk.add(b->cons), o_codes = pk.add(b->codes),
            o_runs = pk.add(b->runs), o_rps = pk.add(b->rps), o_pts = pk.add(b->pts),
            o_ft = pk.add(b->fill_tiles), o_crows = pk.add(b->crows), o_gt = pk.add(b->gram_tiles), o_fro = pk.add(b->feed_row_off),
-           o_rhs = pk.add(b->rhs_given), o_cos = pk.add(b->cos_given), o_z = pk.add(b->z_given);
+           o_rhs = pk.add(b->rhs_given), o_cos = pk.add(b->cos_given), o_z = pk.add(b->z_given),
+           o_st = pk.add(b->stamps);
     b->in_bytes = pk.total > 0 ? pk.total : 256;
     const auto ta0 = std::chrono::steady_clock::now();
     if (b->pooled) {
@@ -992,6 +1089,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
         b->d_rhs_given = (double *)(b->d_in + o_rhs);
         b->d_cos_given = (double *)(b->d_in + o_cos);
         b->d_z_given = (double *)(b->d_in + o_z);
+        b->d_stamps = (DevStamp *)(b->d_in + o_st);
     }
     // segments: uploaded with the arena for caller-provided geometry,
     // expanded on the device from the wires otherwise
@@ -1145,6 +1243,13 @@ static int antenna_from_cards(const fnec_antenna &A, HostAnt &h, std::string &wh
         h.rp.skip_integral = 1;
     }
     h.freqs.assign(A.freqs_hz, A.freqs_hz + A.n_freqs);
+    if (A.n_loads > 0) {
+        if (!A.loads) {
+            why = "n_loads > 0 without loads";
+            return FNEC_ERR_BAD_ARG;
+        }
+        h.loads.assign(A.loads, A.loads + A.n_loads);
+    }
     return FNEC_OK;
 }
 
@@ -1296,7 +1401,7 @@ static int run_pipeline(fnec_batch *b) {
         L += run_mixed(b->mixed, b->d_units, nu, b->d_solves, ns, b->d_ants, b->d_segs, b->d_fill_tiles,
                        (int)b->fill_tiles.size(), b->d_gram_tiles, (int)b->gram_tiles.size(), b->d_ibuf,
                        b->d_crows, b->d_z, b->d_rhs, b->d_cos, b->d_x, b->d_piv, b->d_status, b->max_s,
-                       b->z_given.empty(), b->max_w, b->grid, mm, st);
+                       b->z_given.empty(), b->max_w, b->grid, mm, st, b->d_stamps, (int)b->stamps.size());
         if (!failed && mm.failed_phase) failed = mm.failed_phase;
         if (mm.detail[0]) detail = mm.detail;
     } else {
@@ -1304,6 +1409,10 @@ static int run_pipeline(fnec_batch *b) {
             launch_fill_exact(b->d_units, b->d_ants, b->d_segs, b->d_fill_tiles, (int)b->fill_tiles.size(),
                               b->d_z, st);
             ++L;
+            if (!b->stamps.empty()) {
+                launch_stamps(b->d_stamps, (int)b->stamps.size(), b->d_z, st);
+                ++L;
+            }
         }
         mark(3);
         launch_gram_exact(b->d_units, nu, b->max_w, b->d_ants, b->d_gram_tiles, (int)b->gram_tiles.size(), b->d_ibuf,

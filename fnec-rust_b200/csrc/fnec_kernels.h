@@ -107,6 +107,8 @@ uint64_t launch_factor_exact(const UnitDesc *units, int nu, int max_s, const Gri
                              int32_t *piv, int32_t *status, cudaStream_t st);
 void launch_backsub(const UnitDesc *units, int nu, int max_s, const cx *A, cx *x,
                     const int32_t *status, cudaStream_t st);
+// Z[index] += (re, im) for every stamp (LD loads on the diagonal)
+void launch_stamps(const DevStamp *stamps, int n, cx *z, cudaStream_t st);
 void launch_feedpoints(const UnitDesc *solves, int ns, const AntDesc *ants, const DevSeg *segs,
                        const int32_t *ibuf, const DevFeed *feeds, const cx *x, const int32_t *status,
                        double *feed_out, const int64_t *feed_row_off, cudaStream_t st);

@@ -2095,7 +2095,8 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
                    const AntDesc *d_ants, const DevSeg *d_segs, const int4 *fill_tiles, int n_fill,
                    const int4 *gram_tiles, int n_gram, const int32_t *ibuf, const DevConRow *crows, cx *z,
                    const cx *rhs, const double *cosv, cx *x, int32_t *piv, int32_t *status, int max_s,
-                   bool do_fill, int max_w, const GridPlan &gp, MixedMarks &marks, cudaStream_t st) {
+                   bool do_fill, int max_w, const GridPlan &gp, MixedMarks &marks, cudaStream_t st,
+                   const DevStamp *stamps, int n_stamps) {
     uint64_t L = 0;
     static const char *const phase_name[4] = {"fill", "gram", "factor", "refinement"};
     auto mark = [&](int k) {
@@ -2105,6 +2106,10 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     if (do_fill && n_fill > 0) {
         k_fill_fast<<<n_fill, 256, 0, st>>>(d_units, d_ants, d_segs, fill_tiles, z);
         ++L;
+        if (n_stamps > 0) {  // LD loads on the diagonal, before Z is used
+            launch_stamps(stamps, n_stamps, z, st);
+            ++L;
+        }
     }
     mark(0);
     if (mw.tc && mw.use_tc) {

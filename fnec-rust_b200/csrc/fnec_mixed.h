@@ -99,7 +99,8 @@ uint64_t run_mixed(MixedWork &w, const UnitDesc *d_units, int nu, const UnitDesc
                    const AntDesc *d_ants, const DevSeg *d_segs, const int4 *fill_tiles, int n_fill,
                    const int4 *gram_tiles, int n_gram, const int32_t *ibuf, const DevConRow *crows, cx *z,
                    const cx *rhs, const double *cosv, cx *x, int32_t *piv, int32_t *status, int max_s,
-                   bool do_fill, int max_w, const GridPlan &gp, MixedMarks &marks, cudaStream_t st);
+                   bool do_fill, int max_w, const GridPlan &gp, MixedMarks &marks, cudaStream_t st,
+                   const DevStamp *stamps = nullptr, int n_stamps = 0);
 cudaError_t read_mixed_stats(MixedWork &w, int32_t *iters, double *resid, cudaStream_t st);
 
 }  // namespace fnec

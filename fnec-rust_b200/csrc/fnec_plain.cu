@@ -1134,6 +1134,16 @@ void launch_backsub(const UnitDesc *units, int nu, int max_s, const cx *A, cx *x
     if (!staged) smem = 0;
     if (nu > 0) k_backsub<<<nu, 32, smem, st>>>(units, A, x, status, staged);
 }
+// matrix.rs:131-139 add_to_diagonal: one separately rounded complex add
+__global__ void k_stamps(const DevStamp *__restrict__ stamps, int n, cx *z) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n) return;
+    const DevStamp d = stamps[q];
+    z[d.index] = cx_add(z[d.index], cx_make(d.re, d.im));
+}
+void launch_stamps(const DevStamp *stamps, int n, cx *z, cudaStream_t st) {
+    if (n > 0) k_stamps<<<(n + 255) / 256, 256, 0, st>>>(stamps, n, z);
+}
 void launch_feedpoints(const UnitDesc *solves, int ns, const AntDesc *ants, const DevSeg *segs,
                        const int32_t *ibuf, const DevFeed *feeds, const cx *x, const int32_t *status,
                        double *feed_out, const int64_t *feed_row_off, cudaStream_t st) {

@@ -156,6 +156,13 @@ struct DevRp {
     int32_t pad_rp;
 };
 
+// One load stamp: Z[index] += (re, im) for a diagonal entry of a system's Z
+// (matrix.rs:131-139 add_to_diagonal of the LD loads).
+struct DevStamp {
+    int64_t index;  // complex element of the batch's Z
+    double re, im;
+};
+
 // Constraint-row contribution codes: bit 1 set -> the conj side is -1,
 // bit 0 set -> the other side is -1 (values are 1 or the junction sign).
 inline int32_t con_code(double u, double v) { return (u < 0 ? 2 : 0) | (v < 0 ? 1 : 0); }

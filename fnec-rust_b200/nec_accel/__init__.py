@@ -58,6 +58,9 @@ JUNCTION_DTYPE = np.dtype([("seg_a", "<u8"), ("seg_b", "<u8"), ("sign", "<f8")])
 WIRE_DTYPE = np.dtype([("tag", "<u4"), ("segments", "<u4"), ("start", "<f8", 3), ("end", "<f8", 3),
                        ("radius", "<f8")])
 SOURCE_DTYPE = np.dtype([("tag", "<u4"), ("segment", "<u4"), ("v_re", "<f8"), ("v_im", "<f8")])
+# LD card (fnec_load): type, tag, first and last segment, F1..F3
+LOAD_DTYPE = np.dtype([("load_type", "<i4"), ("tag", "<u4"), ("seg_first", "<u4"), ("seg_last", "<u4"),
+                       ("f1", "<f8"), ("f2", "<f8"), ("f3", "<f8")])
 FEED_COLUMNS = ("seg", "v_re", "v_im", "i_re", "i_im", "z_re", "z_im")
 PATTERN_COLUMNS = ("gain_total_dbi", "gain_theta_dbi", "gain_phi_dbi", "axial_ratio", "u_theta", "u_phi")
 
@@ -83,7 +86,8 @@ class _RpCard(ctypes.Structure):
 
 class _Antenna(ctypes.Structure):
     _fields_ = [("wires", _P), ("n_wires", _U32), ("sources", _P), ("n_sources", _U32), ("ground", _I32),
-                ("n_freqs", _U32), ("freqs_hz", _P), ("rp", _P), ("separate_sources", _U32)]
+                ("n_freqs", _U32), ("freqs_hz", _P), ("rp", _P), ("separate_sources", _U32), ("loads", _P),
+                ("n_loads", _U32)]
 
 
 class _UnitInfo(ctypes.Structure):
@@ -497,8 +501,9 @@ def dispatch_frequency_point(request_kind: int, freq_hz: float) -> str:
 # --------------------------------------------------------------------------
 @dataclass
 class Antenna:
-    """One geometry: GW wires, voltage EX sources, ground, FR frequencies and
-    an optional RP card (n_theta, n_phi, theta0, phi0, d_theta, d_phi)."""
+    """One geometry: GW wires, voltage EX sources, ground, FR frequencies, an
+    optional RP card (n_theta, n_phi, theta0, phi0, d_theta, d_phi) and
+    optional LD cards (a LOAD_DTYPE array, deck order)."""
 
     wires: np.ndarray
     sources: np.ndarray
@@ -506,6 +511,7 @@ class Antenna:
     ground: int = GROUND_FREE
     rp: Optional[tuple] = None
     separate_sources: bool = False  # each source its own right-hand side on one factorisation
+    loads: Optional[np.ndarray] = None
 
 
 def wires_array(wires) -> np.ndarray:
@@ -513,6 +519,14 @@ def wires_array(wires) -> np.ndarray:
     arr = np.zeros(len(wires), dtype=WIRE_DTYPE)
     for i, (tag, nseg, s, e, r) in enumerate(wires):
         arr[i] = (tag, nseg, s, e, r)
+    return arr
+
+
+def loads_array(loads) -> np.ndarray:
+    """loads: iterable of LD cards (type, tag, seg_first, seg_last, f1, f2, f3)."""
+    arr = np.zeros(len(loads), dtype=LOAD_DTYPE)
+    for i, (t, tag, s0, s1, f1, f2, f3) in enumerate(loads):
+        arr[i] = (t, tag, s0, s1, f1, f2, f3)
     return arr
 
 
@@ -542,10 +556,13 @@ def _antenna_struct(a, keep: list):
     rp = None
     if a.rp is not None:
         rp = _RpCard(*[int(a.rp[0]), int(a.rp[1])] + [float(v) for v in a.rp[2:6]])
-    keep += [w, s, f, rp]
+    ld = None
+    if a.loads is not None and len(a.loads) > 0:
+        ld = np.ascontiguousarray(a.loads, dtype=LOAD_DTYPE)
+    keep += [w, s, f, rp, ld]
     return _Antenna(_ptr(w), len(w), _ptr(s), len(s), int(a.ground), len(f), _ptr(f),
                     ctypes.cast(ctypes.pointer(rp), _P) if rp is not None else None,
-                    int(bool(a.separate_sources)))
+                    int(bool(a.separate_sources)), _ptr(ld), 0 if ld is None else len(ld))
 
 
 class _Schedule(ctypes.Structure):

@@ -133,6 +133,19 @@ typedef struct {
     double d_phi;
 } fnec_rp_card;
 
+/* One LD card (nec_model card.rs:265-279; applied by loads.rs:103-222 and
+ * solve_session.rs:1285-1289): load type 0 series RLC, 1 parallel RLC,
+ * 2 series RL, 3 series RC, 4 series R + jX, 5 wire conductivity (other
+ * types are ignored, as the reference ignores them with a warning); tag 0
+ * = every tag; seg_first 0 = every segment of the tag; seg_last 0 = seg_first. */
+typedef struct {
+    int32_t load_type;
+    uint32_t tag;
+    uint32_t seg_first;
+    uint32_t seg_last;
+    double f1, f2, f3;
+} fnec_load;
+
 /* One antenna of a batch: its geometry, sources, ground, frequency list and
  * optional pattern request.  Each frequency is one unit (one solve). */
 typedef struct {
@@ -149,6 +162,10 @@ typedef struct {
      * single-source deck it stands for -- and all of them reuse the one
      * factorisation of each frequency. */
     uint32_t separate_sources;
+    /* LD cards in deck order (may be NULL): their series impedances are added
+     * to Z's diagonal at every frequency before the solve */
+    const fnec_load *loads;
+    uint32_t n_loads;
 } fnec_antenna;
 
 /* Per-unit shape, for sizing result buffers.  A unit is one solve: one

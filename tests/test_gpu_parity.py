@@ -15,7 +15,7 @@ must reproduce the oracle's solution bit for bit.
 import numpy as np
 import pytest
 
-from _corpus import deck_arrays, golden_zins, load_cases
+from _corpus import deck_arrays, deck_loads, golden_zins, load_cases
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -23,6 +23,12 @@ pytestmark = pytest.mark.gpu
 CASES = load_cases()
 ZIN_TOL = 1e-9
 CUR_TOL = 1e-9
+# The top-hat loaded dipole's normal equations have cond(A) = 3.7e10 (the
+# others here 3e8-5e8): the ulp-level differences between the device's
+# correctly rounded fill and the oracle's libm fill reach its small loop
+# currents at ~5e-9 of the peak.  Its solve is bit-exact given the oracle's
+# Z (test_solve_is_bit_exact_given_the_oracle_z) and its Zin meets 1e-9.
+CUR_TOL_CASE = {"dipole-loaded": 1e-7}
 GAIN_TOL_DB = 1e-6
 
 
@@ -37,12 +43,14 @@ def acc():
 def _antenna(acc, deck, freqs=None, rp=None):
     wires, sources, _ = deck_arrays(deck)
     rp = rp if rp is not None else (tuple(deck["rp"]) if deck.get("rp") else None)
+    ld = deck_loads(deck)
     return acc.Antenna(wires.view(acc.WIRE_DTYPE), sources.view(acc.SOURCE_DTYPE),
-                       freqs if freqs is not None else deck["freqs"], deck["ground"], rp)
+                       freqs if freqs is not None else deck["freqs"], deck["ground"], rp,
+                       loads=None if ld is None else ld.view(acc.LOAD_DTYPE))
 
 
-def _check_unit(acc, batch, res, u, wires, sources, ground, freq, pts):
-    p = O.Problem(wires, sources, freq, ground=ground, points=pts)
+def _check_unit(acc, batch, res, u, wires, sources, ground, freq, pts, loads=None, cur_tol=CUR_TOL):
+    p = O.Problem(wires, sources, freq, ground=ground, points=pts, loads=loads)
     O.solve_problem(p)
     assert p.status == 0
     assert res.status[u] == 0
@@ -56,7 +64,7 @@ def _check_unit(acc, batch, res, u, wires, sources, ground, freq, pts):
     if peak == 0.0:  # every segment is a constrained free end (a 1-segment wire)
         assert np.array_equal(cur, p.currents)
     else:
-        assert np.abs(cur - p.currents).max() / peak <= CUR_TOL
+        assert np.abs(cur - p.currents).max() / peak <= cur_tol
     _, piv = batch.read_unit(u)
     # the oracle's pivot buffer has room for n + (GW cards) rows; the solve
     # uses n + (columns): merged wires, or conductor paths in the path form
@@ -86,7 +94,8 @@ def test_corpus_case_matches_oracle_and_golden(acc, name):
     res = batch.solve()
     golden = golden_zins(case)
     for u, f in enumerate(deck["freqs"]):
-        _check_unit(acc, batch, res, u, wires, sources, deck["ground"], f, pts)
+        _check_unit(acc, batch, res, u, wires, sources, deck["ground"], f, pts, loads=deck_loads(deck),
+                    cur_tol=CUR_TOL_CASE.get(name, CUR_TOL))
         if f in golden:
             for row, want in zip(res.feeds[u], golden[f]):
                 got = complex(row[5], row[6])
@@ -115,7 +124,7 @@ def test_z_fill_matches_oracle(acc):
 def test_solve_is_bit_exact_given_the_oracle_z(acc):
     """Gram (linear.rs:765-785), GEPP (:1343-1370) and back substitution
     (:1372-1381) reproduce the oracle bit for bit on the same inputs."""
-    for name in ("yagi-5elm-51seg", "dipole-ground-51seg", "multi-source"):
+    for name in ("yagi-5elm-51seg", "dipole-ground-51seg", "multi-source", "dipole-loaded"):
         deck = CASES[name]["deck"]
         wires, sources, _ = deck_arrays(deck)
         segs = O.build_geometry(wires)
