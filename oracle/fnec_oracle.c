@@ -631,6 +631,102 @@ int64_t or_build_loads(const or_seg *segs, int64_t n, double freq_hz, const or_l
     return ignored;
 }
 
+/* tl.rs:186-241 find_segment_index: segment 0 is the tag's centre (the
+ * middle one of an odd count; the lower centre of an even count). */
+static int64_t tl_find_segment(const or_seg *segs, int64_t n, uint32_t tag, uint32_t seg) {
+    if (seg != 0) return find_seg(segs, n, tag, seg);
+    int64_t cnt = 0;
+    for (int64_t i = 0; i < n; ++i)
+        if (segs[i].tag == tag) cnt++;
+    if (cnt == 0) return -1;
+    int64_t pick;
+    if (cnt % 2 == 1) {
+        pick = cnt / 2;
+    } else {
+        uint32_t lower = (uint32_t)(cnt / 2);
+        pick = -1;
+        int64_t q = 0;
+        for (int64_t i = 0; i < n && pick < 0; ++i)
+            if (segs[i].tag == tag) {
+                if (segs[i].tag_index == lower) pick = q;
+                q++;
+            }
+        if (pick < 0) pick = cnt / 2 >= 1 ? cnt / 2 - 1 : 0;
+    }
+    int64_t q = 0;
+    for (int64_t i = 0; i < n; ++i)
+        if (segs[i].tag == tag) {
+            if (q == pick) return i;
+            q++;
+        }
+    return -1;
+}
+
+static int64_t put4(int64_t c, int64_t cap, int64_t *rows, int64_t *cols, double *vals, int64_t i1, int64_t i2,
+                    c64 zd1, c64 zd2, c64 z12, c64 z21) {
+    int64_t r[4] = {i1, i2, i1, i2}, cc[4] = {i1, i2, i2, i1};
+    c64 v[4] = {zd1, zd2, z12, z21};
+    for (int q = 0; q < 4; ++q, ++c)
+        if (c < cap) {
+            rows[c] = r[q];
+            cols[c] = cc[q];
+            cst(&vals[2 * c], v[q]);
+        }
+    return c;
+}
+
+int64_t or_tl_stamps(const or_seg *segs, int64_t n, double freq_hz, const or_tl *tl, int64_t ntl, int64_t *rows,
+                     int64_t *cols, double *vals, int64_t cap) {
+    const double k = 2.0 * OR_PI * freq_hz / C0;
+    int64_t c = 0;
+    for (int64_t q = 0; q < ntl; ++q) {
+        const or_tl *T = &tl[q];
+        int64_t i1 = tl_find_segment(segs, n, T->tag1, T->seg1);
+        if (i1 < 0) continue;
+        int64_t i2 = tl_find_segment(segs, n, T->tag2, T->seg2);
+        if (i2 < 0 || i1 == i2 || T->z0 <= 0.0 || T->length <= 0.0) continue;
+        if (T->tl_type != 0) {  /* lossy: Z0 coth(gl), Z0 csch(gl), velocity factor 1 */
+            double beta_l = k * T->length;
+            double alpha_l = T->f3 * M_LN10 / 20.0;
+            /* num-complex sinh / cosh of (alpha_l + j beta_l) */
+            c64 sh = cmk(sinh(alpha_l) * cos(beta_l), cosh(alpha_l) * sin(beta_l));
+            c64 ch = cmk(cosh(alpha_l) * cos(beta_l), sinh(alpha_l) * sin(beta_l));
+            if (cnorm(sh) < 1e-9) continue;
+            c64 z0c = cmk(T->z0, 0.0);
+            c64 zd = cdiv(cmul(z0c, ch), sh), zo = cdiv(z0c, sh);
+            c = put4(c, cap, rows, cols, vals, i1, i2, zd, zd, zo, zo);
+            continue;
+        }
+        double vf = (T->f3 >= 0.0 && T->f3 <= 1.0 && T->f3 > 0.0) ? T->f3 : 1.0;
+        double theta = k * T->length / vf;
+        double sin_t = sin(theta);
+        if (fabs(sin_t) < 1e-9) continue;
+        double cot = cos(theta) / sin_t, csc = 1.0 / sin_t;
+        c64 zd = cmk(0.0, -T->z0 * cot), zo = cmk(0.0, -T->z0 * csc);
+        c = put4(c, cap, rows, cols, vals, i1, i2, zd, zd, zo, zo);
+    }
+    return c;
+}
+
+int64_t or_nt_stamps(const or_seg *segs, int64_t n, const or_nt *nt, int64_t nnt, int64_t *rows, int64_t *cols,
+                     double *vals, int64_t cap) {
+    int64_t c = 0;
+    for (int64_t q = 0; q < nnt; ++q) {
+        const or_nt *N = &nt[q];
+        c64 y11 = cmk(N->y11r, N->y11i), y12 = cmk(N->y12r, N->y12i), y21 = y12, y22 = cmk(N->y22r, N->y22i);
+        int64_t i1 = tl_find_segment(segs, n, N->tag1, N->seg1);
+        if (i1 < 0) continue;
+        int64_t i2 = tl_find_segment(segs, n, N->tag2, N->seg2);
+        if (i2 < 0 || i1 == i2) continue;
+        c64 det = csub(cmul(y11, y22), cmul(y12, y21));
+        if (cnorm(det) < 1e-30) continue;
+        c64 z11 = cdiv(y22, det), z22 = cdiv(y11, det);
+        c64 z12 = cdiv(cmk(-y12.re, -y12.im), det), z21 = cdiv(cmk(-y21.re, -y21.im), det);
+        c = put4(c, cap, rows, cols, vals, i1, i2, z11, z22, z12, z21);
+    }
+    return c;
+}
+
 /* ------------------------------------------------------------------------- */
 /* Z-matrix fill                                                              */
 /* ------------------------------------------------------------------------- */
@@ -1226,12 +1322,29 @@ int64_t or_rp_card_points(uint32_t n_theta, uint32_t n_phi, double theta0, doubl
 
 /* solve_session.rs:1285-1289: the LD loads on Z's diagonal (matrix.rs:131-139
  * add_to_diagonal), before the branch is chosen. */
+static void add_stamps(double *z, int64_t n, const int64_t *r, const int64_t *c, const double *v, int64_t cnt) {
+    for (int64_t q = 0; q < cnt; ++q) {
+        double *e = &z[2 * (r[q] * n + c[q])];
+        cst(e, cadd(cld(e), cld(&v[2 * q])));  /* matrix.rs add_to_entry */
+    }
+}
+
 static void add_loads(const or_problem *p, const or_seg *segs, int64_t n, double *z) {
-    if (!p->loads || p->n_loads <= 0) return;
-    double *ld = (double *)malloc(sizeof(double) * 2 * (size_t)(n > 0 ? n : 1));
-    or_build_loads(segs, n, p->freq_hz, p->loads, p->n_loads, ld);
-    for (int64_t i = 0; i < n; ++i) cst(&z[2 * (i * n + i)], cadd(cld(&z[2 * (i * n + i)]), cld(&ld[2 * i])));
-    free(ld);
+    if (p->loads && p->n_loads > 0) {
+        double *ld = (double *)malloc(sizeof(double) * 2 * (size_t)(n > 0 ? n : 1));
+        or_build_loads(segs, n, p->freq_hz, p->loads, p->n_loads, ld);
+        for (int64_t i = 0; i < n; ++i) cst(&z[2 * (i * n + i)], cadd(cld(&z[2 * (i * n + i)]), cld(&ld[2 * i])));
+        free(ld);
+    }
+    /* then the TL stamps, then the NT stamps (solve_session.rs:1290-1309) */
+    int64_t cap = 4 * ((p->tls ? p->n_tls : 0) + (p->nts ? p->n_nts : 0)) + 1;
+    int64_t *r = (int64_t *)malloc(sizeof(int64_t) * (size_t)cap), *cc = (int64_t *)malloc(sizeof(int64_t) * (size_t)cap);
+    double *v = (double *)malloc(sizeof(double) * 2 * (size_t)cap);
+    if (p->tls && p->n_tls > 0) add_stamps(z, n, r, cc, v, or_tl_stamps(segs, n, p->freq_hz, p->tls, p->n_tls, r, cc, v, cap));
+    if (p->nts && p->n_nts > 0) add_stamps(z, n, r, cc, v, or_nt_stamps(segs, n, p->nts, p->n_nts, r, cc, v, cap));
+    free(r);
+    free(cc);
+    free(v);
 }
 
 int or_solve_problem(or_problem *p) {

@@ -152,6 +152,28 @@ typedef struct {
 int64_t or_build_loads(const or_seg *segs, int64_t n, double freq_hz, const or_load *ld, int64_t nl,
                        double *out);
 
+/* One TL card (card.rs TlCard; tl.rs:47-183): ends (tag, segment; segment 0
+ * = the tag's centre segment), sections, type (0 lossless; else lossy with
+ * F3 the matched-line loss in dB), Z0, length, F3 (velocity factor of a
+ * lossless line; parsed default 1). */
+typedef struct {
+    uint32_t tag1, seg1, tag2, seg2, num_segments, tl_type;
+    double z0, length, f3;
+} or_tl;
+/* One NT card with its 10 fields parsed (network.rs:55-142): ends and the
+ * reciprocal two-port's short-circuit admittances Y11, Y12 (= Y21), Y22. */
+typedef struct {
+    uint32_t tag1, seg1, tag2, seg2;
+    double y11r, y11i, y12r, y12i, y22r, y22i;
+} or_nt;
+/* tl.rs:47-183 build_tl_stamps / network.rs:55-142 build_nt_stamps: the
+ * (row, col, delta) stamps in order (4 per applied card; cap entries).
+ * Returns the stamp count. */
+int64_t or_tl_stamps(const or_seg *segs, int64_t n, double freq_hz, const or_tl *tl, int64_t ntl, int64_t *rows,
+                     int64_t *cols, double *vals, int64_t cap);
+int64_t or_nt_stamps(const or_seg *segs, int64_t n, const or_nt *nt, int64_t nnt, int64_t *rows, int64_t *cols,
+                     double *vals, int64_t cap);
+
 /* A whole per-frequency solve of the CLI standard Hallen branch
  * (solve_session.rs:1186-1437 + :1645): geometry -> rhs -> Z -> merged
  * endpoints + junctions -> solve_hallen -> feedpoints -> pattern.  */
@@ -173,6 +195,10 @@ typedef struct {
     int status;
     const or_load *loads; /* LD cards in deck order; may be NULL */
     int64_t n_loads;
+    const or_tl *tls;     /* TL cards in deck order; may be NULL */
+    int64_t n_tls;
+    const or_nt *nts;     /* NT cards in deck order; may be NULL */
+    int64_t n_nts;
 } or_problem;
 
 /* Solve one problem; returns its status. */

@@ -60,7 +60,35 @@ class _Problem(ctypes.Structure):
         ("status", ctypes.c_int),
         ("loads", _P),
         ("n_loads", _I64),
+        ("tls", _P),
+        ("n_tls", _I64),
+        ("nts", _P),
+        ("n_nts", _I64),
     ]
+
+
+TL_DTYPE = np.dtype([("tag1", np.uint32), ("seg1", np.uint32), ("tag2", np.uint32), ("seg2", np.uint32),
+                     ("num_segments", np.uint32), ("tl_type", np.uint32), ("z0", np.float64),
+                     ("length", np.float64), ("f3", np.float64)])
+NT_DTYPE = np.dtype([("tag1", np.uint32), ("seg1", np.uint32), ("tag2", np.uint32), ("seg2", np.uint32),
+                     ("y11r", np.float64), ("y11i", np.float64), ("y12r", np.float64), ("y12i", np.float64),
+                     ("y22r", np.float64), ("y22i", np.float64)])
+
+
+def tls_array(tls) -> np.ndarray:
+    """TL cards (tag1, seg1, tag2, seg2, num_segments, tl_type, z0, length, f3)."""
+    arr = np.zeros(len(tls), dtype=TL_DTYPE)
+    for i, t in enumerate(tls):
+        arr[i] = tuple(t)
+    return arr
+
+
+def nts_array(nts) -> np.ndarray:
+    """NT cards (tag1, seg1, tag2, seg2, y11r, y11i, y12r, y12i, y22r, y22i)."""
+    arr = np.zeros(len(nts), dtype=NT_DTYPE)
+    for i, t in enumerate(nts):
+        arr[i] = tuple(t)
+    return arr
 
 
 LOAD_DTYPE = np.dtype([("load_type", np.int32), ("tag", np.uint32), ("seg_first", np.uint32),
@@ -118,6 +146,10 @@ def lib():
                                             ctypes.c_int]
         L.or_build_loads.restype = _I64
         L.or_build_loads.argtypes = [_P, _I64, _D, _P, _I64, _P]
+        L.or_tl_stamps.restype = _I64
+        L.or_tl_stamps.argtypes = [_P, _I64, _D, _P, _I64, _P, _P, _P, _I64]
+        L.or_nt_stamps.restype = _I64
+        L.or_nt_stamps.argtypes = [_P, _I64, _P, _I64, _P, _P, _P, _I64]
         L.or_solve_square.restype = ctypes.c_int
         L.or_solve_square.argtypes = [_P, _P, _I64, _P, _P, ctypes.c_int]
         L.or_feedpoints.restype = _I64
@@ -318,6 +350,24 @@ def build_loads(segs, freq_hz, loads):
     return out[:n], int(ign)
 
 
+def tl_stamps(segs, freq_hz, tls):
+    """tl.rs build_tl_stamps: [(row, col, delta)] in order."""
+    t = np.ascontiguousarray(tls, TL_DTYPE)
+    cap = 4 * len(t) + 1
+    r, c, v = np.zeros(cap, np.int64), np.zeros(cap, np.int64), np.zeros(cap, np.complex128)
+    k = lib().or_tl_stamps(_ptr(segs), len(segs), float(freq_hz), _ptr(t), len(t), _ptr(r), _ptr(c), _ptr(v), cap)
+    return list(zip(r[:k].tolist(), c[:k].tolist(), v[:k].tolist()))
+
+
+def nt_stamps(segs, nts):
+    """network.rs build_nt_stamps: [(row, col, delta)] in order."""
+    t = np.ascontiguousarray(nts, NT_DTYPE)
+    cap = 4 * len(t) + 1
+    r, c, v = np.zeros(cap, np.int64), np.zeros(cap, np.int64), np.zeros(cap, np.complex128)
+    k = lib().or_nt_stamps(_ptr(segs), len(segs), _ptr(t), len(t), _ptr(r), _ptr(c), _ptr(v), cap)
+    return list(zip(r[:k].tolist(), c[:k].tolist(), v[:k].tolist()))
+
+
 def solve_square(a, b, nthreads=1):
     s = a.shape[0]
     a = np.array(a, np.complex128, order="C")
@@ -366,8 +416,10 @@ class Problem:
     degree-2 conductor-path branch when some path is non-trivial
     (:1338-1378), else the standard branch."""
 
-    def __init__(self, wires, sources, freq_hz, ground=GROUND_FREE, points=None, loads=None):
+    def __init__(self, wires, sources, freq_hz, ground=GROUND_FREE, points=None, loads=None, tls=None, nts=None):
         self.loads = None if loads is None or len(loads) == 0 else np.ascontiguousarray(loads, LOAD_DTYPE)
+        self.tls = None if tls is None or len(tls) == 0 else np.ascontiguousarray(tls, TL_DTYPE)
+        self.nts = None if nts is None or len(nts) == 0 else np.ascontiguousarray(nts, NT_DTYPE)
         self.wires = np.ascontiguousarray(wires)
         self.sources = np.ascontiguousarray(sources)
         self.freq_hz = float(freq_hz)
@@ -385,7 +437,8 @@ class Problem:
             _ptr(self.wires), len(self.wires), _ptr(self.sources), len(self.sources), self.ground,
             self.freq_hz, _ptr(self.points), npts, _ptr(self.currents), _ptr(self.feed),
             _ptr(self.n_feed), _ptr(self.pattern), _ptr(self.pivots), 0, _ptr(self.loads),
-            0 if self.loads is None else len(self.loads))
+            0 if self.loads is None else len(self.loads), _ptr(self.tls), 0 if self.tls is None else len(self.tls),
+            _ptr(self.nts), 0 if self.nts is None else len(self.nts))
 
     @property
     def status(self):

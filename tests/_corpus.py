@@ -31,6 +31,14 @@ def deck_loads(deck):
     return O.loads_array([tuple(x) for x in ld]) if ld else None
 
 
+def deck_networks(deck):
+    """The deck's TL and NT cards as the oracle's arrays (None without any)."""
+    from oracle import oracle as O
+
+    tl, nt = deck.get("tls") or [], deck.get("nts") or []
+    return (O.tls_array([tuple(x) for x in tl]) if tl else None, O.nts_array([tuple(x) for x in nt]) if nt else None)
+
+
 def golden_zins(case):
     """Golden feedpoint impedances as {freq_hz: [z per source]}."""
     fp = case["feedpoint_impedance"]

@@ -3,7 +3,7 @@ committed fixture (tests/golden/corpus_golden.json).
 
 Source: corpus/reference-results.json and the corpus/*.nec decks of
 dc0sk/fnec-rust, read as text.  Only decks built from GW/GE/GN/EX/FR/RP
-and LD cards (no GM/GR transforms, TL/NT networks or plane waves) are kept:
+LD/TL/NT cards (no GM/GR transforms or plane waves) are kept:
 those are the cases that exercise exactly the hot path (geometry, Hallen
 RHS, Z fill, load stamps, normal-equation solve, feedpoint, RP pattern).
 
@@ -31,12 +31,18 @@ CASES = [
     "dipole-ld-loaded-51seg",
     "dipole-ld-series-rl-51seg",
     "dipole-ld-series-rc-51seg",
+    "tl-two-dipoles-linked",
+    "tl-two-dipoles-linked-seg0",
+    "tl-two-dipoles-linked-nseg0",
+    "tl-two-dipoles-linked-seg0-even52",
+    "dipole-nt-freesp-51seg",
+    "dipole-nt-tl-equiv-freesp-51seg",
 ]
 
 
 def parse_deck(text: str) -> dict:
     """Minimal NEC card reader for GW/GN/GE/EX/FR/RP/LD (columns as in NEC-2)."""
-    deck = {"wires": [], "sources": [], "ground": 0, "freqs": [], "rp": None, "loads": []}
+    deck = {"wires": [], "sources": [], "ground": 0, "freqs": [], "rp": None, "loads": [], "tls": [], "nts": []}
     ge_flag = 0
     gn = None
     for line in text.splitlines():
@@ -72,6 +78,17 @@ def parse_deck(text: str) -> dict:
             g = f[1:]
             fl = [float(x) for x in g[4:7]] + [0.0] * (3 - len(g[4:7]))
             deck["loads"].append([int(g[0]), int(g[1]), int(g[2]), int(g[3])] + fl)
+        elif card == "TL":
+            # nec_parser/src/lib.rs:356-377: 6 integers, Z0, length, F3 (default 1)
+            g = f[1:]
+            deck["tls"].append([int(x) for x in g[:6]] + [float(g[6]), float(g[7]),
+                                                           float(g[8]) if len(g) > 8 else 1.0])
+        elif card == "NT":
+            # network.rs:60-93: only a card with all 10 fields is stamped;
+            # the reference warns and ignores any other
+            g = f[1:]
+            if len(g) >= 10:
+                deck["nts"].append([int(x) for x in g[:4]] + [float(x) for x in g[4:10]])
         elif card == "RP":
             # nec_parser/src/lib.rs:293-325: angles start at field 4 with
             # XNDA present (>= 8 fields), else at field 3.

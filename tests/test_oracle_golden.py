@@ -11,7 +11,7 @@ significant digits, phases 4 decimals.
 import numpy as np
 import pytest
 
-from _corpus import deck_arrays, deck_loads, golden_zins, load_cases
+from _corpus import deck_arrays, deck_loads, deck_networks, golden_zins, load_cases
 from oracle import oracle as O
 
 CASES = load_cases()
@@ -37,8 +37,9 @@ def test_feedpoint_impedance_matches_golden(name):
     case = CASES[name]
     wires, sources, _ = deck_arrays(case["deck"])
     for f, zs in golden_zins(case).items():
+        tls, nts = deck_networks(case["deck"])
         p = O.solve_problem(O.Problem(wires, sources, f, ground=case["deck"]["ground"],
-                                      loads=deck_loads(case["deck"])))
+                                      loads=deck_loads(case["deck"]), tls=tls, nts=nts))
         assert p.status == 0
         assert len(p.zin) == len(zs)
         for got, want in zip(p.zin, zs):
