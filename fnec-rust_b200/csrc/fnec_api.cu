@@ -127,6 +127,9 @@ struct HostAnt {
     std::vector<int64_t> free_ends; // 2 per path: I = 0 rows
     int64_t cols() const { return paths ? (int64_t)free_ends.size() / 2 : (int64_t)ep.size(); }
     std::vector<fnec_load> loads;   // LD cards, deck order
+    std::vector<fnec_tl> tls;       // TL cards, deck order
+    std::vector<fnec_nt> nts;       // NT cards, deck order
+    bool stamped() const { return !loads.empty() || !tls.empty() || !nts.empty(); }
 };
 
 // num-complex 0.4.6 arithmetic on the host, each operation separately
@@ -162,6 +165,83 @@ HC bessel_i0_over_i1(HC z) {
         if (hc_norm(t0) <= 1e-17 * hc_norm(i0) && hc_norm(t1) <= 1e-17 * hc_norm(i1)) break;
     }
     return hc_div(i0, i1);
+}
+
+// tl.rs:186-241 find_segment_index: segment 0 is the tag's centre segment
+// (the middle one of an odd count, the lower centre of an even count).
+int64_t tl_segment(const std::vector<DevSeg> &s, uint32_t tag, uint32_t seg) {
+    if (seg != 0) {
+        for (size_t i = 0; i < s.size(); ++i)
+            if (s[i].tag == tag && s[i].tag_index == seg) return (int64_t)i;
+        return -1;
+    }
+    std::vector<size_t> tagged;
+    for (size_t i = 0; i < s.size(); ++i)
+        if (s[i].tag == tag) tagged.push_back(i);
+    if (tagged.empty()) return -1;
+    size_t pick = tagged.size() / 2;
+    if (tagged.size() % 2 == 0) {
+        const uint32_t lower = (uint32_t)(tagged.size() / 2);
+        pick = tagged.size() / 2 - 1;
+        for (size_t q = 0; q < tagged.size(); ++q)
+            if (s[tagged[q]].tag_index == lower) {
+                pick = q;
+                break;
+            }
+    }
+    return (int64_t)tagged[pick];
+}
+
+struct Stamp {
+    int64_t row, col;
+    HC v;
+};
+
+// The two-port stamps of the TL cards (tl.rs:47-183) then the NT cards
+// (network.rs:55-142) at one frequency, in order, 4 per applied card.
+void network_stamps(const HostAnt &h, double freq_hz, std::vector<Stamp> &out) {
+    const double PI_ = 3.14159265358979323846, C0_ = 299792458.0;
+    const double k = 2.0 * PI_ * freq_hz / C0_;
+    auto put4 = [&](int64_t i1, int64_t i2, HC d1, HC d2, HC o12, HC o21) {
+        out.push_back({i1, i1, d1});
+        out.push_back({i2, i2, d2});
+        out.push_back({i1, i2, o12});
+        out.push_back({i2, i1, o21});
+    };
+    for (const fnec_tl &T : h.tls) {
+        const int64_t i1 = tl_segment(h.segs, T.tag1, T.seg1);
+        if (i1 < 0) continue;
+        const int64_t i2 = tl_segment(h.segs, T.tag2, T.seg2);
+        if (i2 < 0 || i1 == i2 || T.z0 <= 0.0 || T.length <= 0.0) continue;
+        if (T.tl_type != 0) {  // lossy: Z0 coth(gl), Z0 csch(gl)
+            const double beta_l = k * T.length, alpha_l = T.f3 * 2.302585092994046 / 20.0;  // ln 10
+            const HC sh{std::sinh(alpha_l) * std::cos(beta_l), std::cosh(alpha_l) * std::sin(beta_l)};
+            const HC ch{std::cosh(alpha_l) * std::cos(beta_l), std::sinh(alpha_l) * std::sin(beta_l)};
+            if (hc_norm(sh) < 1e-9) continue;
+            const HC z0c{T.z0, 0.0};
+            const HC zd = hc_div(hc_mul(z0c, ch), sh), zo = hc_div(z0c, sh);
+            put4(i1, i2, zd, zd, zo, zo);
+            continue;
+        }
+        const double vf = (T.f3 >= 0.0 && T.f3 <= 1.0 && T.f3 > 0.0) ? T.f3 : 1.0;
+        const double theta = k * T.length / vf, sin_t = std::sin(theta);
+        if (std::fabs(sin_t) < 1e-9) continue;
+        const double cot = std::cos(theta) / sin_t, csc = 1.0 / sin_t;
+        const HC zd{0.0, -T.z0 * cot}, zo{0.0, -T.z0 * csc};
+        put4(i1, i2, zd, zd, zo, zo);
+    }
+    for (const fnec_nt &N : h.nts) {
+        const HC y11{N.y11_re, N.y11_im}, y12{N.y12_re, N.y12_im}, y21 = y12, y22{N.y22_re, N.y22_im};
+        const int64_t i1 = tl_segment(h.segs, N.tag1, N.seg1);
+        if (i1 < 0) continue;
+        const int64_t i2 = tl_segment(h.segs, N.tag2, N.seg2);
+        if (i2 < 0 || i1 == i2) continue;
+        const HC p = hc_mul(y11, y22), q = hc_mul(y12, y21);
+        const HC det{p.re - q.re, p.im - q.im};
+        if (hc_norm(det) < 1e-30) continue;
+        put4(i1, i2, hc_div(y22, det), hc_div(y11, det), hc_div({-y12.re, -y12.im}, det),
+             hc_div({-y21.re, -y21.im}, det));
+    }
 }
 
 // Series load impedance of every segment at one frequency (loads.rs:103-222,
@@ -979,12 +1059,29 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
             u.piv_off = b->piv_el;
             u.n_rhs = a.n_rhs;
             u.sys = (int32_t)b->units.size();
-            if (need_solve && !h.loads.empty()) {  // LD loads on this system's Z diagonal
-                std::vector<HC> lv;
-                segment_loads(h, f, lv);
-                for (int i = 0; i < n; ++i)
-                    if (lv[i].re != 0.0 || lv[i].im != 0.0)  // adding an exact zero changes nothing
-                        b->stamps.push_back(DevStamp{u.z_off + (int64_t)i * n + i, lv[i].re, lv[i].im});
+            if (need_solve && h.stamped()) {
+                // this system's stamps in the reference's order: the LD loads on
+                // the diagonal, then the TL and NT two-ports; runs per entry
+                std::vector<Stamp> sv;
+                if (!h.loads.empty()) {
+                    std::vector<HC> lv;
+                    segment_loads(h, f, lv);
+                    for (int i = 0; i < n; ++i)
+                        if (lv[i].re != 0.0 || lv[i].im != 0.0)  // adding an exact zero changes nothing
+                            sv.push_back({i, i, lv[i]});
+                }
+                network_stamps(h, f, sv);
+                std::stable_sort(sv.begin(), sv.end(), [](const Stamp &x, const Stamp &y) {
+                    return x.row != y.row ? x.row < y.row : x.col < y.col;
+                });
+                for (size_t q = 0; q < sv.size();) {
+                    size_t e = q;
+                    while (e < sv.size() && sv[e].row == sv[q].row && sv[e].col == sv[q].col) ++e;
+                    for (size_t t = q; t < e; ++t)
+                        b->stamps.push_back(DevStamp{u.z_off + sv[t].row * n + sv[t].col, sv[t].v.re, sv[t].v.im,
+                                                     t == q ? 1 : 0, t == q ? (int32_t)(e - q) : 0});
+                    q = e;
+                }
             }
             if (need_solve) {
                 b->z_el += (int64_t)n * n;
@@ -1250,6 +1347,12 @@ static int antenna_from_cards(const fnec_antenna &A, HostAnt &h, std::string &wh
         }
         h.loads.assign(A.loads, A.loads + A.n_loads);
     }
+    if ((A.n_tls > 0 && !A.tls) || (A.n_nts > 0 && !A.nts)) {
+        why = "n_tls / n_nts > 0 without their cards";
+        return FNEC_ERR_BAD_ARG;
+    }
+    if (A.n_tls > 0) h.tls.assign(A.tls, A.tls + A.n_tls);
+    if (A.n_nts > 0) h.nts.assign(A.nts, A.nts + A.n_nts);
     return FNEC_OK;
 }
 

@@ -1134,12 +1134,16 @@ void launch_backsub(const UnitDesc *units, int nu, int max_s, const cx *A, cx *x
     if (!staged) smem = 0;
     if (nu > 0) k_backsub<<<nu, 32, smem, st>>>(units, A, x, status, staged);
 }
-// matrix.rs:131-139 add_to_diagonal: one separately rounded complex add
+// matrix.rs:131-139 add_to_diagonal / add_to_entry: each stamp one
+// separately rounded complex add, an entry's stamps in their order (the
+// thread at the first stamp of each run applies the run).
 __global__ void k_stamps(const DevStamp *__restrict__ stamps, int n, cx *z) {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= n) return;
+    if (q >= n || !stamps[q].first) return;
     const DevStamp d = stamps[q];
-    z[d.index] = cx_add(z[d.index], cx_make(d.re, d.im));
+    cx v = z[d.index];
+    for (int t = 0; t < d.count; ++t) v = cx_add(v, cx_make(stamps[q + t].re, stamps[q + t].im));
+    z[d.index] = v;
 }
 void launch_stamps(const DevStamp *stamps, int n, cx *z, cudaStream_t st) {
     if (n > 0) k_stamps<<<(n + 255) / 256, 256, 0, st>>>(stamps, n, z);

@@ -156,11 +156,16 @@ struct DevRp {
     int32_t pad_rp;
 };
 
-// One load stamp: Z[index] += (re, im) for a diagonal entry of a system's Z
-// (matrix.rs:131-139 add_to_diagonal of the LD loads).
+// One stamp: Z[index] += (re, im) on a system's Z (matrix.rs:131-139
+// add_to_diagonal of the LD loads, matrix.rs add_to_entry of the TL / NT
+// two-ports).  Stamps on one entry are consecutive, in the reference's
+// order (loads, then TL cards, then NT cards); `first` marks the first of
+// each entry's run.
 struct DevStamp {
     int64_t index;  // complex element of the batch's Z
     double re, im;
+    int32_t first;  // 1 on the first stamp of an entry
+    int32_t count;  // on the first: the run's length
 };
 
 // Constraint-row contribution codes: bit 1 set -> the conj side is -1,

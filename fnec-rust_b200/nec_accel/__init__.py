@@ -61,6 +61,11 @@ SOURCE_DTYPE = np.dtype([("tag", "<u4"), ("segment", "<u4"), ("v_re", "<f8"), ("
 # LD card (fnec_load): type, tag, first and last segment, F1..F3
 LOAD_DTYPE = np.dtype([("load_type", "<i4"), ("tag", "<u4"), ("seg_first", "<u4"), ("seg_last", "<u4"),
                        ("f1", "<f8"), ("f2", "<f8"), ("f3", "<f8")])
+# TL card (fnec_tl) and NT card with its ten fields parsed (fnec_nt)
+TL_DTYPE = np.dtype([("tag1", "<u4"), ("seg1", "<u4"), ("tag2", "<u4"), ("seg2", "<u4"), ("num_segments", "<u4"),
+                     ("tl_type", "<u4"), ("z0", "<f8"), ("length", "<f8"), ("f3", "<f8")])
+NT_DTYPE = np.dtype([("tag1", "<u4"), ("seg1", "<u4"), ("tag2", "<u4"), ("seg2", "<u4"), ("y11_re", "<f8"),
+                     ("y11_im", "<f8"), ("y12_re", "<f8"), ("y12_im", "<f8"), ("y22_re", "<f8"), ("y22_im", "<f8")])
 FEED_COLUMNS = ("seg", "v_re", "v_im", "i_re", "i_im", "z_re", "z_im")
 PATTERN_COLUMNS = ("gain_total_dbi", "gain_theta_dbi", "gain_phi_dbi", "axial_ratio", "u_theta", "u_phi")
 
@@ -87,7 +92,7 @@ class _RpCard(ctypes.Structure):
 class _Antenna(ctypes.Structure):
     _fields_ = [("wires", _P), ("n_wires", _U32), ("sources", _P), ("n_sources", _U32), ("ground", _I32),
                 ("n_freqs", _U32), ("freqs_hz", _P), ("rp", _P), ("separate_sources", _U32), ("loads", _P),
-                ("n_loads", _U32)]
+                ("n_loads", _U32), ("tls", _P), ("n_tls", _U32), ("nts", _P), ("n_nts", _U32)]
 
 
 class _UnitInfo(ctypes.Structure):
@@ -503,7 +508,8 @@ def dispatch_frequency_point(request_kind: int, freq_hz: float) -> str:
 class Antenna:
     """One geometry: GW wires, voltage EX sources, ground, FR frequencies, an
     optional RP card (n_theta, n_phi, theta0, phi0, d_theta, d_phi) and
-    optional LD cards (a LOAD_DTYPE array, deck order)."""
+    optional LD, TL and NT cards (LOAD_DTYPE / TL_DTYPE / NT_DTYPE arrays,
+    deck order)."""
 
     wires: np.ndarray
     sources: np.ndarray
@@ -512,6 +518,8 @@ class Antenna:
     rp: Optional[tuple] = None
     separate_sources: bool = False  # each source its own right-hand side on one factorisation
     loads: Optional[np.ndarray] = None
+    tls: Optional[np.ndarray] = None
+    nts: Optional[np.ndarray] = None
 
 
 def wires_array(wires) -> np.ndarray:
@@ -527,6 +535,22 @@ def loads_array(loads) -> np.ndarray:
     arr = np.zeros(len(loads), dtype=LOAD_DTYPE)
     for i, (t, tag, s0, s1, f1, f2, f3) in enumerate(loads):
         arr[i] = (t, tag, s0, s1, f1, f2, f3)
+    return arr
+
+
+def tls_array(tls) -> np.ndarray:
+    """tls: iterable of TL cards (tag1, seg1, tag2, seg2, num_segments, tl_type, z0, length, f3)."""
+    arr = np.zeros(len(tls), dtype=TL_DTYPE)
+    for i, t in enumerate(tls):
+        arr[i] = tuple(t)
+    return arr
+
+
+def nts_array(nts) -> np.ndarray:
+    """nts: iterable of NT cards (tag1, seg1, tag2, seg2, y11_re, y11_im, y12_re, y12_im, y22_re, y22_im)."""
+    arr = np.zeros(len(nts), dtype=NT_DTYPE)
+    for i, t in enumerate(nts):
+        arr[i] = tuple(t)
     return arr
 
 
@@ -556,13 +580,15 @@ def _antenna_struct(a, keep: list):
     rp = None
     if a.rp is not None:
         rp = _RpCard(*[int(a.rp[0]), int(a.rp[1])] + [float(v) for v in a.rp[2:6]])
-    ld = None
-    if a.loads is not None and len(a.loads) > 0:
-        ld = np.ascontiguousarray(a.loads, dtype=LOAD_DTYPE)
-    keep += [w, s, f, rp, ld]
+    def opt(x, dt):
+        return None if x is None or len(x) == 0 else np.ascontiguousarray(x, dtype=dt)
+
+    ld, tl, nt = opt(a.loads, LOAD_DTYPE), opt(a.tls, TL_DTYPE), opt(a.nts, NT_DTYPE)
+    keep += [w, s, f, rp, ld, tl, nt]
     return _Antenna(_ptr(w), len(w), _ptr(s), len(s), int(a.ground), len(f), _ptr(f),
                     ctypes.cast(ctypes.pointer(rp), _P) if rp is not None else None,
-                    int(bool(a.separate_sources)), _ptr(ld), 0 if ld is None else len(ld))
+                    int(bool(a.separate_sources)), _ptr(ld), 0 if ld is None else len(ld),
+                    _ptr(tl), 0 if tl is None else len(tl), _ptr(nt), 0 if nt is None else len(nt))
 
 
 class _Schedule(ctypes.Structure):

@@ -146,6 +146,27 @@ typedef struct {
     double f1, f2, f3;
 } fnec_load;
 
+/* One TL card (card.rs TlCard; stamped by tl.rs:47-183 as in
+ * solve_session.rs:1290-1296): the line's ends (tag, segment; segment 0 =
+ * the tag's centre segment, the lower one of an even count), sections
+ * (stamped as one section), type (0 lossless with velocity factor f3 when
+ * 0 < f3 <= 1, else 1; any other type lossy with f3 the matched-line loss in
+ * dB), z0 (> 0) and length (> 0).  Cards that cannot stamp are ignored, as
+ * the reference ignores them with a warning. */
+typedef struct {
+    uint32_t tag1, seg1, tag2, seg2;
+    uint32_t num_segments, tl_type;
+    double z0, length, f3;
+} fnec_tl;
+
+/* One NT card with its ten fields parsed (network.rs:55-142): the ends and
+ * the reciprocal two-port's short-circuit admittances Y11, Y12 = Y21, Y22;
+ * stamped as [Z] = [Y]^-1.  A singular [Y] or coincident ends are ignored. */
+typedef struct {
+    uint32_t tag1, seg1, tag2, seg2;
+    double y11_re, y11_im, y12_re, y12_im, y22_re, y22_im;
+} fnec_nt;
+
 /* One antenna of a batch: its geometry, sources, ground, frequency list and
  * optional pattern request.  Each frequency is one unit (one solve). */
 typedef struct {
@@ -166,6 +187,12 @@ typedef struct {
      * to Z's diagonal at every frequency before the solve */
     const fnec_load *loads;
     uint32_t n_loads;
+    /* TL and NT cards in deck order (may be NULL): their two-port stamps are
+     * added to Z after the loads, TL first (solve_session.rs:1290-1309) */
+    const fnec_tl *tls;
+    uint32_t n_tls;
+    const fnec_nt *nts;
+    uint32_t n_nts;
 } fnec_antenna;
 
 /* Per-unit shape, for sizing result buffers.  A unit is one solve: one

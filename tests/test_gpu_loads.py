@@ -1,6 +1,7 @@
-"""LD loads on the device (loads.rs:103-222 applied as in
-solve_session.rs:1285-1289): every type's series impedance added to Z's
-diagonal at each frequency, before the Hallen solve.
+"""LD loads and TL / NT two-ports on the device (loads.rs:103-222,
+tl.rs:47-183, network.rs:55-142, applied as in solve_session.rs:1285-1309):
+every load type's series impedance added to Z's diagonal, then the TL and
+NT Z-parameter stamps, at each frequency before the Hallen solve.
 
 Plain FP64 form vs the CPU oracle: the stamped diagonal bit for bit (the
 host builds the same load values with the same num-complex operations),
@@ -116,3 +117,71 @@ def test_loads_with_separate_sources_and_a_path_deck(acc):
     p = O.Problem(O.wires_array(split), O.sources_array([(1, 1, 1.0)]), 14.2e6, loads=O.loads_array(ld))
     O.solve_problem(p)
     assert abs(complex(*res.feeds[0][0, 5:7]) - p.zin[0]) <= 1e-9 * abs(p.zin[0])
+
+
+# a lossless line (velocity factor 0.66) from wire 1 to wire 2's centre,
+# a lossy line (2 dB), a line sharing the first one's end on wire 2 (a
+# loaded segment), two ignored cards (coincident ends, z0 <= 0), and an NT
+# two-port; stamps on one entry add in card order
+TLS = [(1, 8, 2, 0, 1, 0, 75.0, 3.1, 0.66), (1, 24, 3, 6, 3, 1, 300.0, 7.5, 2.0), (2, 11, 3, 2, 0, 0, 450.0, 1.2, 1.0),
+       (1, 5, 1, 5, 1, 0, 50.0, 1.0, 1.0), (1, 3, 2, 3, 1, 0, -50.0, 1.0, 1.0)]
+NTS = [(1, 20, 2, 11, 0.002, -0.01, 0.0, 0.004, 0.001, -0.012)]
+
+
+def _net_ant(acc, ground, freqs=FREQS):
+    return acc.Antenna(acc.wires_array(WIRES), acc.sources_array(SOURCES), freqs, ground, None,
+                       loads=acc.loads_array(LOADS), tls=acc.tls_array(TLS), nts=acc.nts_array(NTS))
+
+
+def _oracle_net(f, ground):
+    p = O.Problem(O.wires_array(WIRES), O.sources_array(SOURCES), f, ground=ground, loads=O.loads_array(LOADS),
+                  tls=O.tls_array(TLS), nts=O.nts_array(NTS))
+    return O.solve_problem(p)
+
+
+def test_network_stamps_are_the_oracle_stamps_bit_for_bit(acc):
+    segs = O.build_geometry(O.wires_array(WIRES))
+    plain = acc.HallenBatch([_ant(acc, 0, loads=None)])
+    plain.solve()
+    stamped = acc.HallenBatch([_net_ant(acc, 0)])
+    stamped.solve()
+    for u, f in enumerate(FREQS):
+        z = plain.read_z(u).copy()
+        lv, _ = O.build_loads(segs, f, O.loads_array(LOADS))
+        seq = [(i, i, lv[i]) for i in range(len(segs)) if lv[i] != 0]
+        seq += O.tl_stamps(segs, f, O.tls_array(TLS)) + O.nt_stamps(segs, O.nts_array(NTS))
+        assert len(O.tl_stamps(segs, f, O.tls_array(TLS))) == 12  # the two ignored cards stamp nothing
+        for r, c, d in seq:  # separately rounded adds, in the reference's order
+            v = z[r, c]
+            z[r, c] = complex(v.real + d.real, v.imag + d.imag)
+        got = stamped.read_z(u)
+        assert np.array_equal(np.ascontiguousarray(got).view(np.uint64), z.view(np.uint64))
+    plain.close()
+    stamped.close()
+
+
+@pytest.mark.parametrize("ground", [0, 1])
+def test_plain_matches_oracle_with_networks(acc, ground):
+    b = acc.HallenBatch([_net_ant(acc, ground)])
+    res = b.solve()
+    for u, f in enumerate(FREQS):
+        p = _oracle_net(f, ground)
+        assert p.status == 0 and res.status[u] == 0
+        zg, zo = complex(*res.feeds[u][0, 5:7]), p.zin[0]
+        assert abs(zg - zo) <= 1e-9 * abs(zo), (f, zg, zo)
+        assert np.abs(res.currents[u] - p.currents).max() <= 1e-9 * np.abs(p.currents).max()
+        _, piv = b.read_unit(u)
+        assert np.array_equal(piv, p.pivots[: len(piv)])
+    b.close()
+
+
+def test_mixed_within_gate_with_networks(acc):
+    ants = [_net_ant(acc, g) for g in (0, 1)]
+    plain = acc.HallenBatch(ants, precision=acc.PRECISION_FP64).solve()
+    b = acc.HallenBatch(ants, precision=acc.PRECISION_MIXED)
+    mixed = b.solve()
+    assert np.all(mixed.status == 0)
+    for fm, fp in zip(mixed.feeds, plain.feeds):
+        zm, zp = complex(*fm[0, 5:7]), complex(*fp[0, 5:7])
+        assert abs(zm - zp) <= 1e-6 * abs(zp)
+    b.close()
