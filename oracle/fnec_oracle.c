@@ -727,6 +727,83 @@ int64_t or_nt_stamps(const or_seg *segs, int64_t n, const or_nt *nt, int64_t nnt
     return c;
 }
 
+void or_near_field(const or_seg *segs, int64_t n, const double *cur, double freq_hz, const double *pts, int64_t p,
+                   double *e_out, double *h_out) {
+    const double C = 299792458.0;
+    const double k = 2.0 * OR_PI * freq_hz / C;
+    const double ETA0 = 4.0 * OR_PI * 1e-7 * C;
+    const double coeff_e = ETA0 / (4.0 * OR_PI), coeff_h = 1.0 / (4.0 * OR_PI);
+    for (int64_t q = 0; q < p; ++q) {
+        const double *P = &pts[3 * q];
+        c64 e[3] = {{0, 0}, {0, 0}, {0, 0}}, h[3] = {{0, 0}, {0, 0}, {0, 0}};
+        for (int64_t m = 0; m < n; ++m) {
+            const or_seg *s = &segs[m];
+            double d[3] = {P[0] - s->mid[0], P[1] - s->mid[1], P[2] - s->mid[2]};
+            double r = sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            if (r < 1e-9) continue; /* on the segment itself */
+            double rh[3] = {d[0] / r, d[1] / r, d[2] / r};
+            const double *u = s->dir;
+            double kr_c = cos(k * r), kr_s = sin(k * r);
+            c64 phase = cmk(kr_c, -kr_s);
+            c64 jkr = cmk(0.0, k * r);
+            c64 inv_jkr = cdiv(cmk(1.0, 0.0), jkr);
+            c64 I = cld(&cur[2 * m]);
+            if (e_out) {
+                double c = u[0] * rh[0] + u[1] * rh[1] + u[2] * rh[2];
+                c64 pref = cmul(crs(s->length * coeff_e, I), phase);
+                double inv_kr2 = 1.0 / (k * r * k * r);
+                c64 rad = crs(2.0 * c / (r * r), cadd(cmk(1.0, 0.0), inv_jkr));
+                c64 th = cmul(cdivr(jkr, r * r), csub(cadd(cmk(1.0, 0.0), inv_jkr), cmk(inv_kr2, 0.0)));
+                for (int a = 0; a < 3; ++a) {
+                    double tan_a = c * rh[a] - u[a];
+                    e[a] = cadd(e[a], cmul(pref, cadd(crs(rh[a], rad), crs(tan_a, th))));
+                }
+            }
+            if (h_out) {
+                double cr[3] = {u[1] * rh[2] - u[2] * rh[1], u[2] * rh[0] - u[0] * rh[2], u[0] * rh[1] - u[1] * rh[0]};
+                c64 factor = cmul(cdivr(jkr, r * r), cadd(cmk(1.0, 0.0), inv_jkr));
+                c64 pref = cmul(cmul(crs(s->length * coeff_h, I), phase), factor);
+                for (int a = 0; a < 3; ++a) h[a] = cadd(h[a], crs(cr[a], pref));
+            }
+        }
+        for (int a = 0; a < 3; ++a) {
+            if (e_out) cst(&e_out[6 * q + 2 * a], e[a]);
+            if (h_out) cst(&h_out[6 * q + 2 * a], h[a]);
+        }
+    }
+}
+
+int64_t or_near_field_points(uint32_t coord_type, uint32_t nx, uint32_t ny, uint32_t nz, double x0, double y0,
+                             double z0, double dx, double dy, double dz, double *pts) {
+    uint32_t mx = nx ? nx : 1, my = ny ? ny : 1, mz = nz ? nz : 1;
+    int64_t c = 0;
+    if (coord_type == 0) {
+        for (uint32_t ix = 0; ix < mx; ++ix)
+            for (uint32_t iy = 0; iy < my; ++iy)
+                for (uint32_t iz = 0; iz < mz; ++iz, ++c)
+                    if (pts) {
+                        pts[3 * c] = x0 + (double)ix * dx;
+                        pts[3 * c + 1] = y0 + (double)iy * dy;
+                        pts[3 * c + 2] = z0 + (double)iz * dz;
+                    }
+    } else { /* theta outer, phi, then R inner */
+        for (uint32_t it = 0; it < mz; ++it) {
+            double th = (z0 + (double)it * dz) * RADS_PER_DEG;
+            for (uint32_t ip = 0; ip < my; ++ip) {
+                double ph = (y0 + (double)ip * dy) * RADS_PER_DEG;
+                for (uint32_t ir = 0; ir < mx; ++ir, ++c)
+                    if (pts) {
+                        double r = x0 + (double)ir * dx;
+                        pts[3 * c] = r * sin(th) * cos(ph);
+                        pts[3 * c + 1] = r * sin(th) * sin(ph);
+                        pts[3 * c + 2] = r * cos(th);
+                    }
+            }
+        }
+    }
+    return c;
+}
+
 /* ------------------------------------------------------------------------- */
 /* Z-matrix fill                                                              */
 /* ------------------------------------------------------------------------- */

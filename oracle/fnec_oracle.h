@@ -174,6 +174,17 @@ int64_t or_tl_stamps(const or_seg *segs, int64_t n, double freq_hz, const or_tl 
 int64_t or_nt_stamps(const or_seg *segs, int64_t n, const or_nt *nt, int64_t nnt, int64_t *rows, int64_t *cols,
                      double *vals, int64_t cap);
 
+/* farfield.rs:154-261 near_e_field / near_h_field: the Hertzian-element sum
+ * of the segment currents (2n doubles) at p points (3p doubles, metres);
+ * e_out / h_out (6p doubles: x, y, z complex components) may be NULL. */
+void or_near_field(const or_seg *segs, int64_t n, const double *cur, double freq_hz, const double *pts, int64_t p,
+                   double *e_out, double *h_out);
+/* solve_session.rs:645-688 near_field_grid_points of one NE/NH card
+ * (coord_type 0 rectangular x/y/z, else spherical R/phi/theta); returns the
+ * point count, writes 3 doubles per point when pts != NULL. */
+int64_t or_near_field_points(uint32_t coord_type, uint32_t nx, uint32_t ny, uint32_t nz, double x0, double y0,
+                             double z0, double dx, double dy, double dz, double *pts);
+
 /* A whole per-frequency solve of the CLI standard Hallen branch
  * (solve_session.rs:1186-1437 + :1645): geometry -> rhs -> Z -> merged
  * endpoints + junctions -> solve_hallen -> feedpoints -> pattern.  */

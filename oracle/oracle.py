@@ -150,6 +150,10 @@ def lib():
         L.or_tl_stamps.argtypes = [_P, _I64, _D, _P, _I64, _P, _P, _P, _I64]
         L.or_nt_stamps.restype = _I64
         L.or_nt_stamps.argtypes = [_P, _I64, _P, _I64, _P, _P, _P, _I64]
+        L.or_near_field.restype = None
+        L.or_near_field.argtypes = [_P, _I64, _P, _D, _P, _I64, _P, _P]
+        L.or_near_field_points.restype = _I64
+        L.or_near_field_points.argtypes = [ctypes.c_uint32] * 4 + [_D] * 6 + [_P]
         L.or_solve_square.restype = ctypes.c_int
         L.or_solve_square.argtypes = [_P, _P, _I64, _P, _P, ctypes.c_int]
         L.or_feedpoints.restype = _I64
@@ -366,6 +370,25 @@ def nt_stamps(segs, nts):
     r, c, v = np.zeros(cap, np.int64), np.zeros(cap, np.int64), np.zeros(cap, np.complex128)
     k = lib().or_nt_stamps(_ptr(segs), len(segs), _ptr(t), len(t), _ptr(r), _ptr(c), _ptr(v), cap)
     return list(zip(r[:k].tolist(), c[:k].tolist(), v[:k].tolist()))
+
+
+def near_field(segs, currents, freq_hz, points):
+    """farfield.rs near_e_field / near_h_field: (E, H), each (p, 3) complex."""
+    pts = np.ascontiguousarray(points, np.float64).reshape(-1, 3)
+    cur = np.ascontiguousarray(currents, np.complex128)
+    e = np.zeros((max(len(pts), 1), 3), np.complex128)
+    h = np.zeros((max(len(pts), 1), 3), np.complex128)
+    lib().or_near_field(_ptr(segs), len(segs), _ptr(cur), float(freq_hz), _ptr(pts), len(pts), _ptr(e), _ptr(h))
+    return e[: len(pts)], h[: len(pts)]
+
+
+def near_field_points(coord_type, nx, ny, nz, x0, y0, z0, dx, dy, dz):
+    """The observation points of one NE/NH card, (p, 3)."""
+    args = [int(coord_type), int(nx), int(ny), int(nz)] + [float(v) for v in (x0, y0, z0, dx, dy, dz)]
+    cnt = lib().or_near_field_points(*args, None)
+    out = np.zeros((max(cnt, 1), 3), np.float64)
+    lib().or_near_field_points(*args, _ptr(out))
+    return out[:cnt]
 
 
 def solve_square(a, b, nthreads=1):
