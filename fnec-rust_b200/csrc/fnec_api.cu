@@ -2304,6 +2304,47 @@ int fnec_integrate_radiated_power(fnec_ctx *ctx, const fnec_gpu_segment *segment
     return FNEC_OK;
 }
 
+static_assert(sizeof(fnec_gpu_segment) == 7 * sizeof(double), "fnec_gpu_segment is 7 packed doubles");
+
+int fnec_near_field(fnec_ctx *ctx, const fnec_gpu_segment *segments, uint64_t n, const double *currents,
+                    double freq_hz, const double *points, uint64_t p, double *e_out, double *h_out) {
+    if (!ctx) return FNEC_ERR_BAD_ARG;
+    if (p == 0) return FNEC_OK;
+    if (!points || (!e_out && !h_out) || (n && (!segments || !currents)))
+        return fail(ctx, FNEC_ERR_BAD_ARG, "near field: null argument");
+    if (!(freq_hz > 0.0) || !std::isfinite(freq_hz)) return fail(ctx, FNEC_ERR_BAD_ARG, "near field: bad frequency");
+    if (p > (uint64_t)INT32_MAX * 128 || n > (uint64_t)INT32_MAX)
+        return fail(ctx, FNEC_ERR_BAD_ARG, "near field: too many points or segments");
+    // farfield.rs:160-161, :224-225 (host code built without contraction)
+    const double k = 2.0 * PI * freq_hz / C0;
+    const double eta0 = 4.0 * PI * 1e-7 * C0;
+    const double coeff_e = eta0 / (4.0 * PI), coeff_h = 1.0 / (4.0 * PI);
+    cudaSetDevice(ctx->device);
+    const size_t n_seg = 7 * n, n_cur = 2 * n, n_pts = 3 * p, n_fld = 6 * p;
+    const size_t total = n_seg + n_cur + n_pts + (e_out ? n_fld : 0) + (h_out ? n_fld : 0);
+    double *d = nullptr;
+    CUDA_TRY(ctx, cudaMalloc(&d, sizeof(double) * total));
+    double *d_seg = d, *d_cur = d_seg + n_seg, *d_pts = d_cur + n_cur, *d_e = d_pts + n_pts;
+    double *d_h = d_e + (e_out ? n_fld : 0);
+    cudaStream_t s = ctx->stream;
+    cudaError_t e = cudaSuccess;
+    if (n) e = cudaMemcpyAsync(d_seg, segments, sizeof(double) * n_seg, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess && n) e = cudaMemcpyAsync(d_cur, currents, sizeof(double) * n_cur, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_pts, points, sizeof(double) * n_pts, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        launch_near_field(d_seg, (int64_t)n, reinterpret_cast<const cx *>(d_cur), k, coeff_e, coeff_h, d_pts,
+                          (int64_t)p, e_out ? reinterpret_cast<cx *>(d_e) : nullptr,
+                          h_out ? reinterpret_cast<cx *>(d_h) : nullptr, s);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess && e_out) e = cudaMemcpyAsync(e_out, d_e, sizeof(double) * n_fld, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess && h_out) e = cudaMemcpyAsync(h_out, d_h, sizeof(double) * n_fld, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(ctx, FNEC_ERR_CUDA, cudaGetErrorString(e));
+    return FNEC_OK;
+}
+
 int fnec_microbench_zmatrix_dispatch(int device, uint64_t n_segments, uint32_t n_dispatches,
                                      uint64_t *device_init_us, uint64_t *dispatch_min_us,
                                      uint64_t *dispatch_median_us) {

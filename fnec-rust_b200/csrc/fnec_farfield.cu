@@ -324,4 +324,98 @@ void launch_farfield(const UnitDesc *units, int nu, const AntDesc *ants, const D
                                 total_out);
 }
 
+// ---------------------------------------------------------------------------
+// Near fields (farfield.rs:154-261 near_e_field / near_h_field): each
+// segment is a Hertzian element of moment I_n L_n at its midpoint, and the
+// field at P is the sum over segments in index order of
+//   E += eta/(4 pi) I L e^{-jkr} [ rh 2c/r^2 (1 + 1/jkr)
+//                                  + (c rh - u) jk/r^2 (1 + 1/jkr - 1/(kr)^2) ]
+//   H += 1/(4 pi) I L e^{-jkr} jk/r^2 (1 + 1/jkr) (u x rh),
+// c = u.rh, skipping segments whose midpoint is within 1e-9 m of P.  Every
+// operation is a separately rounded FP64 op in the reference's order and
+// sin/cos(kr) are correctly rounded, so a point's field is the CPU sum bit
+// for bit.  One thread per point; the segment list is staged through shared
+// memory in tiles that every thread of the block reads by broadcast.
+// ---------------------------------------------------------------------------
+constexpr int NF_THREADS = 128;
+constexpr int NF_TILE = 128;
+constexpr int NF_SEG_DOUBLES = 9;  // midpoint, direction, length, current (re, im)
+
+__device__ __forceinline__ cx nf_scale(double s, cx a) { return cx_make(D_MUL(a.re, s), D_MUL(a.im, s)); }
+
+__global__ void __launch_bounds__(NF_THREADS) k_near_field(const double *__restrict__ segs, int64_t n,
+                                                           const cx *__restrict__ cur, double k, double coeff_e,
+                                                           double coeff_h, const double *__restrict__ pts,
+                                                           int64_t p, cx *e_out, cx *h_out) {
+    __shared__ double tile[NF_TILE * NF_SEG_DOUBLES];
+    const int64_t q = (int64_t)blockIdx.x * NF_THREADS + threadIdx.x;
+    const bool live = q < p;
+    double P[3] = {0.0, 0.0, 0.0};
+    if (live)
+        for (int c = 0; c < 3; ++c) P[c] = pts[3 * q + c];
+    cx e[3], h[3];
+    for (int a = 0; a < 3; ++a) e[a] = h[a] = cx_make(0.0, 0.0);
+    const cx one = cx_make(1.0, 0.0);
+    for (int64_t base = 0; base < n; base += NF_TILE) {
+        const int cnt = (int)min((int64_t)NF_TILE, n - base);
+        __syncthreads();
+        for (int t = threadIdx.x; t < cnt * NF_SEG_DOUBLES; t += NF_THREADS) {
+            const int m = t / NF_SEG_DOUBLES, f = t % NF_SEG_DOUBLES;
+            const int64_t g = base + m;
+            tile[t] = f < 7 ? segs[7 * g + f] : (f == 7 ? cur[g].re : cur[g].im);
+        }
+        __syncthreads();
+        if (!live) continue;
+        for (int m = 0; m < cnt; ++m) {
+            const double *s = &tile[m * NF_SEG_DOUBLES];
+            const double d[3] = {D_SUB(P[0], s[0]), D_SUB(P[1], s[1]), D_SUB(P[2], s[2])};
+            const double r = D_SQRT(D_ADD(D_ADD(D_MUL(d[0], d[0]), D_MUL(d[1], d[1])), D_MUL(d[2], d[2])));
+            if (r < 1e-9) continue;
+            const double rh[3] = {D_DIV(d[0], r), D_DIV(d[1], r), D_DIV(d[2], r)};
+            const double *u = &s[3];
+            const double len = s[6];
+            const cx I = cx_make(s[7], s[8]);
+            const double kr = D_MUL(k, r);
+            double sn, cs;
+            cr_sincos(kr, &sn, &cs);
+            const cx phase = cx_make(cs, -sn);
+            const cx jkr = cx_make(0.0, kr);
+            const cx one_p = cx_add(one, cx_div(one, jkr));
+            const double rr = D_MUL(r, r);
+            const cx jk_rr = cx_make(D_DIV(jkr.re, rr), D_DIV(jkr.im, rr));
+            if (e_out) {
+                const double c = D_ADD(D_ADD(D_MUL(u[0], rh[0]), D_MUL(u[1], rh[1])), D_MUL(u[2], rh[2]));
+                const cx pref = cx_mul(nf_scale(D_MUL(len, coeff_e), I), phase);
+                const double inv_kr2 = D_DIV(1.0, D_MUL(D_MUL(D_MUL(k, r), k), r));
+                const cx rad = nf_scale(D_DIV(D_MUL(2.0, c), rr), one_p);
+                const cx th = cx_mul(jk_rr, cx_sub(one_p, cx_make(inv_kr2, 0.0)));
+                for (int a = 0; a < 3; ++a) {
+                    const double tan_a = D_SUB(D_MUL(c, rh[a]), u[a]);
+                    e[a] = cx_add(e[a], cx_mul(pref, cx_add(nf_scale(rh[a], rad), nf_scale(tan_a, th))));
+                }
+            }
+            if (h_out) {
+                const double cr[3] = {D_SUB(D_MUL(u[1], rh[2]), D_MUL(u[2], rh[1])),
+                                      D_SUB(D_MUL(u[2], rh[0]), D_MUL(u[0], rh[2])),
+                                      D_SUB(D_MUL(u[0], rh[1]), D_MUL(u[1], rh[0]))};
+                const cx factor = cx_mul(jk_rr, one_p);
+                const cx pref = cx_mul(cx_mul(nf_scale(D_MUL(len, coeff_h), I), phase), factor);
+                for (int a = 0; a < 3; ++a) h[a] = cx_add(h[a], nf_scale(cr[a], pref));
+            }
+        }
+    }
+    if (!live) return;
+    for (int a = 0; a < 3; ++a) {
+        if (e_out) e_out[3 * q + a] = e[a];
+        if (h_out) h_out[3 * q + a] = h[a];
+    }
+}
+
+void launch_near_field(const double *segs, int64_t n, const cx *cur, double k, double coeff_e, double coeff_h,
+                       const double *pts, int64_t p, cx *e_out, cx *h_out, cudaStream_t st) {
+    if (p <= 0) return;
+    const int64_t blocks = (p + NF_THREADS - 1) / NF_THREADS;
+    k_near_field<<<(unsigned)blocks, NF_THREADS, 0, st>>>(segs, n, cur, k, coeff_e, coeff_h, pts, p, e_out, h_out);
+}
+
 }  // namespace fnec

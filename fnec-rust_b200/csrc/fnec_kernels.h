@@ -124,5 +124,9 @@ void launch_farfield(const UnitDesc *units, int nu, const AntDesc *ants, const D
                      const DevRp *rps, const double *pts, const int32_t *ibuf, const cx *x, const int32_t *status,
                      double *fld, double *partials, int max_blocks, size_t smem, double *pat_out,
                      double *total_out, cudaStream_t st);
+// near E and H (either may be null) at p points from n segments given as
+// fnec_gpu_segment records (7 doubles each) and their currents
+void launch_near_field(const double *segs, int64_t n, const cx *cur, double k, double coeff_e, double coeff_h,
+                       const double *pts, int64_t p, cx *e_out, cx *h_out, cudaStream_t st);
 
 }  // namespace fnec

@@ -148,6 +148,7 @@ SIGNATURES = {
     "fnec_rp_farfield_batch": (ctypes.c_int, [_P, _P, _U64, _P, _D, _D, _P, _U64, _P]),
     "fnec_radiation_pattern": (ctypes.c_int, [_P, _P, _U64, _P, _D, _I32, _P, _U64, _P, _P]),
     "fnec_integrate_radiated_power": (ctypes.c_int, [_P, _P, _U64, _P, _D, _I32, _P]),
+    "fnec_near_field": (ctypes.c_int, [_P, _P, _U64, _P, _D, _P, _U64, _P, _P]),
     "fnec_microbench_zmatrix_dispatch": (ctypes.c_int, [ctypes.c_int, _U64, _U32, _P, _P, _P]),
     "fnec_enumerate_devices": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_char_p, _U64]),
     "fnec_dispatch_frequency_point": (ctypes.c_int, [ctypes.c_int, _D]),
@@ -423,6 +424,25 @@ def integrate_radiated_power(segments, currents, freq_hz: float, pec_ground: boo
                                                   int(bool(pec_ground)), _ptr(tot)),
               "integrate_radiated_power")
     return float(tot[0])
+
+
+def near_field(segments, currents, freq_hz: float, points, electric: bool = True, magnetic: bool = True,
+               ctx: Optional[Context] = None):
+    """near_e_field / near_h_field (farfield.rs:154-261): the fields of the
+    segment currents at (p, 3) points in metres.  Returns (E, H), each (p, 3)
+    complex, or None for the one not asked for."""
+    if not (electric or magnetic):
+        raise ValueError("near_field: ask for E, H or both")
+    ctx = ctx or default_context()
+    segs = np.ascontiguousarray(segments, dtype=GPU_SEGMENT_DTYPE)
+    cur = np.ascontiguousarray(currents, np.complex128)
+    pts = np.ascontiguousarray(points, np.float64).reshape(-1, 3)
+    e = np.zeros((len(pts), 3), np.complex128) if electric else None
+    h = np.zeros((len(pts), 3), np.complex128) if magnetic else None
+    ctx.check(lib().fnec_near_field(ctx.handle, _ptr(segs), len(segs), _ptr(cur), float(freq_hz), _ptr(pts),
+                                    len(pts), None if e is None else _ptr(e), None if h is None else _ptr(h)),
+              "near_field")
+    return e, h
 
 
 @dataclass

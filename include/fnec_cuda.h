@@ -17,6 +17,7 @@
  *   fnec_rp_farfield_batch       <- run_rp_farfield_batch_wgpu   crates/nec_accel/src/wgpu_device.rs:461
  *   fnec_radiation_pattern       <- compute_radiation_pattern    crates/nec_solver/src/farfield.rs:563
  *   fnec_integrate_radiated_power<- integrate_radiated_power     crates/nec_solver/src/farfield.rs:409
+ *   fnec_near_field              <- near_e_field / near_h_field  crates/nec_solver/src/farfield.rs:154, :218
  *   fnec_microbench_zmatrix_dispatch <- microbench_zmatrix_dispatch crates/nec_accel/src/wgpu_device.rs:1087
  *   fnec_enumerate_devices       <- enumerate_compute_adapters   crates/nec_accel/src/wgpu_device.rs:24
  *   fnec_dispatch_frequency_point<- dispatch_frequency_point     crates/nec_accel/src/lib.rs:92
@@ -282,6 +283,14 @@ int fnec_radiation_pattern(fnec_ctx *ctx, const fnec_gpu_segment *segments, uint
 int fnec_integrate_radiated_power(fnec_ctx *ctx, const fnec_gpu_segment *segments, uint64_t n,
                                   const double *currents, double freq_hz, int32_t pec_ground,
                                   double *out);
+
+/* near_e_field / near_h_field: the near electric and magnetic fields at p
+ * points (3p doubles, metres) as the sum over the n segments of Hertzian
+ * elements I_n L_n at their midpoints, free space, segments within 1e-9 m of
+ * a point skipped.  currents: 2n doubles.  e_out / h_out: 6p doubles each
+ * (Ex, Ey, Ez complex), either may be null but not both. */
+int fnec_near_field(fnec_ctx *ctx, const fnec_gpu_segment *segments, uint64_t n, const double *currents,
+                    double freq_hz, const double *points, uint64_t p, double *e_out, double *h_out);
 
 /* microbench_zmatrix_dispatch: device-init vs dispatch split (microseconds). */
 int fnec_microbench_zmatrix_dispatch(int device, uint64_t n_segments, uint32_t n_dispatches,
