@@ -545,6 +545,103 @@ int or_hallen_rhs_paths(const or_seg *segs, int64_t n, double freq_hz, const or_
 
 /* loads.rs:34-57 i0_over_i1: I0(z)/I1(z) by the power series for |z| <= 15,
  * the asymptotic expansion beyond. */
+/* planewave.rs:86-105 r_hat / pol_hat: the arrival direction and the
+ * complex polarisation vector e = u_maj + j sense AR u_min. */
+static void pw_vectors(const or_wave *w, double *r_hat, c64 *pol) {
+    double t = w->theta_deg * RADS_PER_DEG, p = w->phi_deg * RADS_PER_DEG;
+    r_hat[0] = sin(t) * cos(p);
+    r_hat[1] = sin(t) * sin(p);
+    r_hat[2] = cos(t);
+    double eta = w->eta_deg * RADS_PER_DEG;
+    double th[3] = {cos(t) * cos(p), cos(t) * sin(p), -sin(t)};
+    double ph[3] = {-sin(p), cos(p), 0.0};
+    double ce = cos(eta), se = sin(eta);
+    double ar = 0.0, sense = 0.0; /* planewave.rs:62-67 */
+    if (w->ex_type == 2) {
+        ar = w->axial_ratio;
+        sense = 1.0;
+    } else if (w->ex_type == 3) {
+        ar = w->axial_ratio;
+        sense = -1.0;
+    }
+    c64 jminor = cmk(0.0, sense * ar);
+    for (int i = 0; i < 3; ++i) {
+        double major = ce * th[i] + se * ph[i];
+        double minor = -se * th[i] + ce * ph[i];
+        pol[i] = cadd(cmk(major, 0.0), crs(minor, jminor));
+    }
+}
+
+int or_planewave_rhs(const or_seg *segs, int64_t n, double freq_hz, const or_wave *wave, const int64_t *path_of,
+                     const double *sign, const double *s_mid, double *rhs, double *cosv, double *sinv) {
+    const double C0 = 299792458.0;
+    const double ETA0 = 4.0 * OR_PI * 1e-7 * C0;
+    double k = 2.0 * OR_PI * freq_hz / C0;
+    double scale = 2.0 * OR_PI / ETA0;
+    double r_hat[3];
+    c64 pol[3];
+    pw_vectors(wave, r_hat, pol);
+    int64_t *grp = (int64_t *)malloc(sizeof(int64_t) * (size_t)(n > 0 ? n : 1));
+    double *sc = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+    double *sg = (double *)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+    c64 *e = (c64 *)malloc(sizeof(c64) * (size_t)(n > 0 ? n : 1));
+    int st = OR_OK;
+    if (!path_of) {
+        /* :176-209 per-tag wires, rejected when junctioned; s from the wire's
+         * geometric midpoint along the direction of its first segment */
+        int64_t w = or_wire_endpoints(segs, n, NULL, 0);
+        int64_t *ep = (int64_t *)malloc(sizeof(int64_t) * 2 * (size_t)(w > 0 ? w : 1));
+        or_wire_endpoints(segs, n, ep, w);
+        if (or_detect_junctions(segs, ep, w, 1e-6, NULL, NULL, NULL, 0) > 0) st = OR_ERR_JUNCTION;
+        for (int64_t q = 0; q < w && st == OR_OK; ++q) {
+            const double *a = segs[ep[2 * q]].mid, *b = segs[ep[2 * q + 1]].mid;
+            const double *dir = segs[ep[2 * q]].dir;
+            double wm[3] = {(a[0] + b[0]) / 2.0, (a[1] + b[1]) / 2.0, (a[2] + b[2]) / 2.0};
+            for (int64_t i = ep[2 * q]; i <= ep[2 * q + 1]; ++i) {
+                double d[3] = {segs[i].mid[0] - wm[0], segs[i].mid[1] - wm[1], segs[i].mid[2] - wm[2]};
+                grp[i] = q;
+                sc[i] = dot3(d, dir);
+                sg[i] = 1.0;
+                c64 coup = cmk(0.0, 0.0);
+                for (int c = 0; c < 3; ++c) coup = cadd(coup, crs(dir[c], pol[c]));
+                double phase = k * dot3(r_hat, segs[i].mid);
+                e[i] = cmul(coup, cmk(1.0 * cos(phase), 1.0 * sin(phase))); /* from_polar(1, phase) */
+            }
+        }
+        free(ep);
+    } else {
+        /* :291-315 the path's signed arc length and traversal sign */
+        for (int64_t i = 0; i < n; ++i) {
+            grp[i] = path_of[i];
+            sc[i] = s_mid[i];
+            sg[i] = sign[i];
+            c64 coup = cmk(0.0, 0.0);
+            for (int c = 0; c < 3; ++c) coup = cadd(coup, crs(segs[i].dir[c], pol[c]));
+            double phase = k * dot3(r_hat, segs[i].mid);
+            e[i] = crs(sg[i], cmul(coup, cmk(1.0 * cos(phase), 1.0 * sin(phase))));
+        }
+    }
+    if (st == OR_OK)
+        for (int64_t m = 0; m < n; ++m) {
+            c64 acc = cmk(0.0, 0.0);
+            for (int64_t p = 0; p < n; ++p) {
+                if (grp[p] != grp[m]) continue;
+                double kern = sin(k * fabs(sc[m] - sc[p]));
+                acc = cadd(acc, crs(segs[p].length, crs(kern, e[p])));
+            }
+            c64 r = cmul(cmk(0.0, -scale), acc);
+            if (path_of) r = crs(sg[m], r);
+            cst(&rhs[2 * m], r);
+            cosv[m] = sg[m] * cos(k * sc[m]);
+            sinv[m] = sg[m] * sin(k * sc[m]);
+        }
+    free(grp);
+    free(sc);
+    free(sg);
+    free(e);
+    return st;
+}
+
 static c64 i0_over_i1(c64 z) {
     if (cnorm(z) > 15.0) {
         c64 inv = cdiv(cmk(1.0, 0.0), z);
@@ -1034,7 +1131,7 @@ int or_solve_square(double *a, double *b, int64_t s, double *x, int32_t *pivots,
  * started at +0 never changes its value or its sign under round-to-nearest,
  * so the skipped form is value-identical (checked bit-for-bit by the tests).
  * Per element, the surviving terms are still added in ascending r. */
-static int solve_core(const double *z, int64_t n, const double *rhs, const double *cosv,
+static int solve_core(const double *z, int64_t n, const double *rhs, const double *cosv, const double *sinv,
                       const int64_t *row_wire, int64_t w, const int64_t *cc0, const int64_t *cc1,
                       const double *cv1, int64_t nc, double *x, int32_t *pivots, double *gram, int naive,
                       int nthreads);
@@ -1099,7 +1196,7 @@ int or_solve_hallen(const double *z, int64_t n, const double *rhs, const double 
         crow++;
     }
     (void)rows;
-    int st = solve_core(z, n, rhs, cosv, row_wire, w, cc0, cc1, cv1, nc, x, pivots, gram, naive, nthreads);
+    int st = solve_core(z, n, rhs, cosv, NULL, row_wire, w, cc0, cc1, cv1, nc, x, pivots, gram, naive, nthreads);
     free(cc0);
     free(cc1);
     free(cv1);
@@ -1123,7 +1220,41 @@ int or_solve_hallen_paths(const double *z, int64_t n, const double *rhs, const d
         cc1[q] = -1;
         cv1[q] = 0.0;
     }
-    int st = solve_core(z, n, rhs, cosv, path_of, w, free_ends, cc1, cv1, n_free, x, pivots, gram, naive, nthreads);
+    int st = solve_core(z, n, rhs, cosv, NULL, path_of, w, free_ends, cc1, cv1, n_free, x, pivots, gram, naive,
+                        nthreads);
+    free(cc1);
+    free(cv1);
+    return st;
+}
+
+int or_solve_hallen_planewave(const double *z, int64_t n, const double *rhs, const double *cosv,
+                              const double *sinv, const int64_t *row_wire, int64_t w, const int64_t *free_ends,
+                              int64_t n_free, double *x, int32_t *pivots, double *gram, int naive) {
+    /* per-tag wires: rows I = 0 at (first, last) of each wire in order */
+    int64_t nc = free_ends ? n_free : 2 * w;
+    int64_t *cc0 = (int64_t *)malloc(sizeof(int64_t) * (size_t)(nc + 1));
+    int64_t *cc1 = (int64_t *)malloc(sizeof(int64_t) * (size_t)(nc + 1));
+    double *cv1 = (double *)malloc(sizeof(double) * (size_t)(nc + 1));
+    if (free_ends) {
+        for (int64_t q = 0; q < nc; ++q) cc0[q] = free_ends[q];
+    } else {
+        for (int64_t q = 0; q < w; ++q) {
+            int64_t first = -1, last = -1;
+            for (int64_t r = 0; r < n; ++r)
+                if (row_wire[r] == q) {
+                    if (first < 0) first = r;
+                    last = r;
+                }
+            cc0[2 * q] = first;
+            cc0[2 * q + 1] = last;
+        }
+    }
+    for (int64_t q = 0; q < nc; ++q) {
+        cc1[q] = -1;
+        cv1[q] = 0.0;
+    }
+    int st = solve_core(z, n, rhs, cosv, sinv, row_wire, w, cc0, cc1, cv1, nc, x, pivots, gram, naive, 1);
+    free(cc0);
     free(cc1);
     free(cv1);
     return st;
@@ -1131,12 +1262,15 @@ int or_solve_hallen_paths(const double *z, int64_t n, const double *rhs, const d
 
 /* The normal equations (MᴴM + 1e-8 I) x = Mᴴy of M = [Z | -cos columns]
  * over constraint rows (cc0, cc1, cv1), then GEPP. */
-static int solve_core(const double *z, int64_t n, const double *rhs, const double *cosv,
+static int solve_core(const double *z, int64_t n, const double *rhs, const double *cosv, const double *sinv,
                       const int64_t *row_wire, int64_t w, const int64_t *cc0, const int64_t *cc1,
                       const double *cv1, int64_t nc, double *x, int32_t *pivots, double *gram, int naive,
                       int nthreads) {
+    /* sinv != NULL: two homogeneous columns (cos, sin) per wire, the
+     * plane-wave form (linear.rs:955-961) */
+    const int64_t hw = sinv ? 2 : 1;
     int64_t rows = n + nc;
-    int64_t cols = n + w;
+    int64_t cols = n + hw * w;
     int64_t aw = cols + 1;
     c64 *aug = (c64 *)calloc((size_t)(cols * aw + 1), sizeof(c64));
 
@@ -1145,7 +1279,8 @@ static int solve_core(const double *z, int64_t n, const double *rhs, const doubl
         c64 *y = (c64 *)calloc((size_t)(rows + 1), sizeof(c64));
         for (int64_t r = 0; r < n; ++r) {
             for (int64_t c = 0; c < n; ++c) m[r * cols + c] = cld(&z[2 * (r * n + c)]);
-            m[r * cols + n + row_wire[r]] = cmk(-cosv[r], 0.0);
+            m[r * cols + n + hw * row_wire[r]] = cmk(-cosv[r], 0.0);
+            if (sinv) m[r * cols + n + hw * row_wire[r] + 1] = cmk(-sinv[r], 0.0);
             y[r] = cld(&rhs[2 * r]);
         }
         for (int64_t q = 0; q < nc; ++q) {
@@ -1170,21 +1305,26 @@ static int solve_core(const double *z, int64_t n, const double *rhs, const doubl
          * ascending r, and structurally-zero products are skipped. */
         for (int64_t r = 0; r < n; ++r) {
             const double *zr = &z[2 * r * n];
-            int64_t cw = n + row_wire[r];
+            int64_t cw = n + hw * row_wire[r];
             c64 cval = cmk(-cosv[r], 0.0);
+            c64 sval = cmk(sinv ? -sinv[r] : 0.0, 0.0);
             c64 yr = cld(&rhs[2 * r]);
             for (int64_t i = 0; i < n; ++i) {
                 c64 ci = cconj(cld(&zr[2 * i]));
                 c64 *arow = &aug[i * aw];
                 for (int64_t j = 0; j < n; ++j) arow[j] = cadd(arow[j], cmul(ci, cld(&zr[2 * j])));
                 arow[cw] = cadd(arow[cw], cmul(ci, cval));
+                if (sinv) arow[cw + 1] = cadd(arow[cw + 1], cmul(ci, sval));
                 arow[cols] = cadd(arow[cols], cmul(ci, yr));
             }
-            c64 cc = cconj(cval);
-            c64 *crw = &aug[cw * aw];
-            for (int64_t j = 0; j < n; ++j) crw[j] = cadd(crw[j], cmul(cc, cld(&zr[2 * j])));
-            crw[cw] = cadd(crw[cw], cmul(cc, cval));
-            crw[cols] = cadd(crw[cols], cmul(cc, yr));
+            for (int64_t h = 0; h < hw; ++h) { /* the cos row, then the sin row */
+                c64 cc = cconj(h ? sval : cval);
+                c64 *crw = &aug[(cw + h) * aw];
+                for (int64_t j = 0; j < n; ++j) crw[j] = cadd(crw[j], cmul(cc, cld(&zr[2 * j])));
+                crw[cw] = cadd(crw[cw], cmul(cc, cval));
+                if (sinv) crw[cw + 1] = cadd(crw[cw + 1], cmul(cc, sval));
+                crw[cols] = cadd(crw[cols], cmul(cc, yr));
+            }
         }
         /* constraint rows r = n .. rows-1 in order; y = 0 there, so their
          * aty products are structurally zero. */
@@ -1424,6 +1564,61 @@ static void add_loads(const or_problem *p, const or_seg *segs, int64_t n, double
     free(v);
 }
 
+/* solve_session.rs:262-301 solve_plane_wave_hallen: a non-trivial
+ * degree-2 path deck takes the path form, any other deck the per-tag wire
+ * form (junctioned decks fail there); no feed rows. */
+static int planewave_problem(or_problem *p, const or_seg *segs, int64_t n) {
+    size_t nn = (size_t)(n > 0 ? n : 1);
+    int64_t *path_of = (int64_t *)malloc(sizeof(int64_t) * nn);
+    int64_t *fe = (int64_t *)malloc(sizeof(int64_t) * 2 * nn);
+    int64_t *row_wire = (int64_t *)malloc(sizeof(int64_t) * nn);
+    double *sgn = (double *)malloc(sizeof(double) * nn), *smid = (double *)malloc(sizeof(double) * nn);
+    double *rhs = (double *)malloc(sizeof(double) * 2 * nn);
+    double *cosv = (double *)malloc(sizeof(double) * nn), *sinv = (double *)malloc(sizeof(double) * nn);
+    int nontrivial = 0;
+    int64_t np = or_conductor_paths(segs, n, path_of, sgn, smid, fe, &nontrivial);
+    int paths = np >= 0 && nontrivial;
+    int st = or_planewave_rhs(segs, n, p->freq_hz, p->wave, paths ? path_of : NULL, sgn, smid, rhs, cosv, sinv);
+    int64_t w = 0;
+    if (paths) {
+        w = np;
+        memcpy(row_wire, path_of, sizeof(int64_t) * (size_t)n);
+    } else {
+        w = or_wire_endpoints(segs, n, NULL, 0);
+        int64_t *ep = (int64_t *)malloc(sizeof(int64_t) * 2 * (size_t)(w > 0 ? w : 1));
+        or_wire_endpoints(segs, n, ep, w);
+        for (int64_t q = 0; q < w; ++q)
+            for (int64_t r = ep[2 * q]; r <= ep[2 * q + 1]; ++r) row_wire[r] = q;
+        free(ep);
+    }
+    double *z = NULL, *x = NULL;
+    if (st == OR_OK) {
+        z = (double *)malloc(sizeof(double) * 2 * nn * nn);
+        or_assemble_z(segs, n, p->freq_hz, p->ground, z);
+        add_loads(p, segs, n, z);
+        x = (double *)malloc(sizeof(double) * 2 * (size_t)(n + 2 * w));
+        st = or_solve_hallen_planewave(z, n, rhs, cosv, sinv, row_wire, w, paths ? fe : NULL, 2 * np, x, p->pivots,
+                                       NULL, 0);
+    }
+    if (st == OR_OK) {
+        memcpy(p->currents, x, sizeof(double) * 2 * (size_t)n);
+        if (p->n_feed) *p->n_feed = 0;
+        if (p->n_points > 0 && p->points && p->pattern)
+            or_radiation_pattern(segs, n, x, p->freq_hz, p->ground, p->points, p->n_points, p->pattern, NULL, NULL);
+    }
+    free(path_of);
+    free(fe);
+    free(row_wire);
+    free(sgn);
+    free(smid);
+    free(rhs);
+    free(cosv);
+    free(sinv);
+    free(z);
+    free(x);
+    return st;
+}
+
 int or_solve_problem(or_problem *p) {
     int64_t cap = 0;
     for (int64_t w = 0; w < p->n_wires; ++w) cap += p->wires[w].segments;
@@ -1432,6 +1627,11 @@ int or_solve_problem(or_problem *p) {
     if (n < 0) {
         free(segs);
         return p->status = (int)n;
+    }
+    if (p->wave) {
+        int st = planewave_problem(p, segs, n);
+        free(segs);
+        return p->status = st;
     }
     double *rhs = (double *)malloc(sizeof(double) * 2 * (size_t)n);
     double *cosv = (double *)malloc(sizeof(double) * (size_t)n);

@@ -65,7 +65,8 @@ enum {
     OR_ERR_NO_WIRES = -4,
     OR_ERR_SEGMENT_NOT_FOUND = -5,
     OR_ERR_CAPACITY = -6,
-    OR_ERR_DIM = -7
+    OR_ERR_DIM = -7,
+    OR_ERR_JUNCTION = -8 /* planewave.rs:131-133 JunctionedGeometryNotSupported */
 };
 
 /* geometry.rs:676-754 (GW only). Returns N, or a negative error. */
@@ -185,6 +186,29 @@ void or_near_field(const or_seg *segs, int64_t n, const double *cur, double freq
 int64_t or_near_field_points(uint32_t coord_type, uint32_t nx, uint32_t ny, uint32_t nz, double x0, double y0,
                              double z0, double dx, double dy, double dz, double *pts);
 
+/* An incident plane wave (planewave.rs:37-105, EX types 1/2/3): it arrives
+ * from (theta, phi) degrees with polarisation angle eta; types 2 / 3 are
+ * right / left elliptic with the given axial ratio, type 1 linear. */
+typedef struct {
+    int32_t ex_type;
+    double theta_deg, phi_deg, eta_deg, axial_ratio;
+} or_wave;
+
+/* planewave.rs:162-254 build_planewave_hallen (path_of == NULL: per-tag
+ * wires; returns OR_ERR_JUNCTION when any two wire ends touch) and
+ * :278-348 build_planewave_hallen_paths (path_of, sign, s_mid from
+ * or_conductor_paths): the forcing (2n doubles) and the cos / sin
+ * homogeneous columns (n doubles each). */
+int or_planewave_rhs(const or_seg *segs, int64_t n, double freq_hz, const or_wave *wave, const int64_t *path_of,
+                     const double *sign, const double *s_mid, double *rhs, double *cosv, double *sinv);
+/* linear.rs:910-993 solve_hallen_planewave (free_ends == NULL: I = 0 at
+ * both ends of each per-tag wire) and :1024-1090 solve_hallen_planewave_paths
+ * (the listed free-end rows): two homogeneous columns (cos, sin) per wire or
+ * path, the same regularised normal equations and GEPP; x: 2(n + 2w). */
+int or_solve_hallen_planewave(const double *z, int64_t n, const double *rhs, const double *cosv,
+                              const double *sinv, const int64_t *row_wire, int64_t w, const int64_t *free_ends,
+                              int64_t n_free, double *x, int32_t *pivots, double *gram, int naive);
+
 /* A whole per-frequency solve of the CLI standard Hallen branch
  * (solve_session.rs:1186-1437 + :1645): geometry -> rhs -> Z -> merged
  * endpoints + junctions -> solve_hallen -> feedpoints -> pattern.  */
@@ -210,6 +234,10 @@ typedef struct {
     int64_t n_tls;
     const or_nt *nts;     /* NT cards in deck order; may be NULL */
     int64_t n_nts;
+    /* the first plane-wave EX card, or NULL: with it the problem is the CLI's
+     * receive solve (solve_session.rs:262-301); voltage sources are then not
+     * used and no feed rows are produced */
+    const or_wave *wave;
 } or_problem;
 
 /* Solve one problem; returns its status. */

@@ -9,6 +9,7 @@ import this module.  It is the checker, never the measured product.
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 import subprocess
 
@@ -64,7 +65,13 @@ class _Problem(ctypes.Structure):
         ("n_tls", _I64),
         ("nts", _P),
         ("n_nts", _I64),
+        ("wave", _P),
     ]
+
+
+class _Wave(ctypes.Structure):
+    _fields_ = [("ex_type", ctypes.c_int32), ("theta_deg", _D), ("phi_deg", _D), ("eta_deg", _D),
+                ("axial_ratio", _D)]
 
 
 TL_DTYPE = np.dtype([("tag1", np.uint32), ("seg1", np.uint32), ("tag2", np.uint32), ("seg2", np.uint32),
@@ -146,6 +153,10 @@ def lib():
                                             ctypes.c_int]
         L.or_build_loads.restype = _I64
         L.or_build_loads.argtypes = [_P, _I64, _D, _P, _I64, _P]
+        L.or_planewave_rhs.restype = ctypes.c_int
+        L.or_planewave_rhs.argtypes = [_P, _I64, _D, _P, _P, _P, _P, _P, _P, _P]
+        L.or_solve_hallen_planewave.restype = ctypes.c_int
+        L.or_solve_hallen_planewave.argtypes = [_P, _I64, _P, _P, _P, _P, _I64, _P, _I64, _P, _P, _P, ctypes.c_int]
         L.or_tl_stamps.restype = _I64
         L.or_tl_stamps.argtypes = [_P, _I64, _D, _P, _I64, _P, _P, _P, _I64]
         L.or_nt_stamps.restype = _I64
@@ -345,6 +356,77 @@ def solve_hallen_paths(z, rhs, cosv, paths: ConductorPaths, nthreads=1):
     return x, piv[:s]
 
 
+def wave(ex_type=1, theta_deg=0.0, phi_deg=0.0, eta_deg=0.0, axial_ratio=0.0):
+    """One incident plane wave (planewave.rs IncidentPlaneWave): EX type
+    1 linear, 2 right / 3 left elliptic."""
+    return _Wave(int(ex_type), float(theta_deg), float(phi_deg), float(eta_deg), float(axial_ratio))
+
+
+def planewave_rhs(segs, freq_hz, w, paths=None):
+    """planewave.rs build_planewave_hallen (paths None) or
+    build_planewave_hallen_paths: (rhs, cos_vec, sin_vec)."""
+    n = len(segs)
+    rhs = np.zeros(n, np.complex128)
+    cosv = np.zeros(n, np.float64)
+    sinv = np.zeros(n, np.float64)
+    args = (None, None, None) if paths is None else (_ptr(paths.path_of), _ptr(paths.sign), _ptr(paths.s_mid))
+    st = lib().or_planewave_rhs(_ptr(segs), n, float(freq_hz), ctypes.byref(w), *args, _ptr(rhs), _ptr(cosv),
+                                _ptr(sinv))
+    if st != 0:
+        raise OracleError(f"planewave_rhs: status {st}")
+    return rhs, cosv, sinv
+
+
+def solve_hallen_planewave(z, rhs, cosv, sinv, row_wire, n_cols, free_ends=None, naive=False):
+    """linear.rs solve_hallen_planewave (free_ends None: both ends of every
+    per-tag wire) / solve_hallen_planewave_paths: (x, pivots, gram)."""
+    n = z.shape[0]
+    z = np.ascontiguousarray(z, np.complex128)
+    s = n + 2 * n_cols
+    x = np.zeros(s, np.complex128)
+    piv = np.zeros(max(s, 1), np.int32)
+    gram = np.zeros((s, s + 1), np.complex128)
+    rw = np.ascontiguousarray(row_wire, np.int64)
+    fe = None if free_ends is None else np.ascontiguousarray(free_ends, np.int64).reshape(-1)
+    st = lib().or_solve_hallen_planewave(_ptr(z), n, _ptr(np.ascontiguousarray(rhs, np.complex128)),
+                                         _ptr(np.ascontiguousarray(cosv, np.float64)),
+                                         _ptr(np.ascontiguousarray(sinv, np.float64)), _ptr(rw), int(n_cols),
+                                         _ptr(fe), 0 if fe is None else len(fe), _ptr(x), _ptr(piv), _ptr(gram),
+                                         int(bool(naive)))
+    if st != 0:
+        raise OracleError(f"solve_hallen_planewave: status {st}")
+    return x, piv[:s], gram
+
+
+def wave_directions(ex_type, n_theta, n_phi, theta0, phi0, d_theta, d_phi, eta_deg=0.0, axial_ratio=0.0):
+    """solve_session.rs:313-355: the incidence grid of one plane-wave EX card,
+    theta outer, phi inner; the first is the deck's own direction."""
+    out = []
+    for it in range(max(int(n_theta), 1)):
+        for ip in range(max(int(n_phi), 1)):
+            out.append(wave(ex_type, theta0 + it * float(d_theta), phi0 + ip * float(d_phi), eta_deg, axial_ratio))
+    return out
+
+
+def receive_sweep(wires, freq_hz, waves, ground=GROUND_FREE, loads=None, tls=None, nts=None):
+    """solve_session.rs:313-375 plane_wave_receive_sweep: one full receive
+    solve per incidence direction, the peak |I| of each, and the response
+    20 log10(peak / max peak) dB (-999.99 for a zero peak).  Returns
+    (peaks, response_db, currents of every direction)."""
+    peaks, cur = [], []
+    for w in waves:
+        p = solve_problem(Problem(wires, sources_array([]), freq_hz, ground=ground, loads=loads, tls=tls, nts=nts,
+                                  wave=w))
+        if p.status != 0:
+            raise OracleError(f"receive solve: status {p.status}")
+        mags = [math.hypot(c.real, c.imag) for c in p.currents]
+        peaks.append(max([0.0] + mags))
+        cur.append(p.currents.copy())
+    top = max([0.0] + peaks)
+    db = [20.0 * math.log10(pk / top) if pk > 0.0 and top > 0.0 else -999.99 for pk in peaks]
+    return np.array(peaks), np.array(db), cur
+
+
 def build_loads(segs, freq_hz, loads):
     """loads.rs build_loads: (per-segment load impedance, ignored count)."""
     n = len(segs)
@@ -439,7 +521,9 @@ class Problem:
     degree-2 conductor-path branch when some path is non-trivial
     (:1338-1378), else the standard branch."""
 
-    def __init__(self, wires, sources, freq_hz, ground=GROUND_FREE, points=None, loads=None, tls=None, nts=None):
+    def __init__(self, wires, sources, freq_hz, ground=GROUND_FREE, points=None, loads=None, tls=None, nts=None,
+                 wave=None):
+        self.wave = wave
         self.loads = None if loads is None or len(loads) == 0 else np.ascontiguousarray(loads, LOAD_DTYPE)
         self.tls = None if tls is None or len(tls) == 0 else np.ascontiguousarray(tls, TL_DTYPE)
         self.nts = None if nts is None or len(nts) == 0 else np.ascontiguousarray(nts, NT_DTYPE)
@@ -455,13 +539,14 @@ class Problem:
         self.n_feed = np.zeros(1, np.int64)
         npts = 0 if self.points is None else len(self.points)
         self.pattern = np.zeros((max(npts, 1), 4), np.float64)
-        self.pivots = np.zeros(n + w, np.int32)
+        self.pivots = np.zeros(n + 2 * w, np.int32)
         self._s = _Problem(
             _ptr(self.wires), len(self.wires), _ptr(self.sources), len(self.sources), self.ground,
             self.freq_hz, _ptr(self.points), npts, _ptr(self.currents), _ptr(self.feed),
             _ptr(self.n_feed), _ptr(self.pattern), _ptr(self.pivots), 0, _ptr(self.loads),
             0 if self.loads is None else len(self.loads), _ptr(self.tls), 0 if self.tls is None else len(self.tls),
-            _ptr(self.nts), 0 if self.nts is None else len(self.nts))
+            _ptr(self.nts), 0 if self.nts is None else len(self.nts),
+            None if wave is None else ctypes.addressof(wave))
 
     @property
     def status(self):
