@@ -125,7 +125,16 @@ struct HostAnt {
     std::vector<int32_t> path_of;   // column (path) of each row
     std::vector<double> arc;        // 2n: signed arc length of each midpoint, then its sign
     std::vector<int64_t> free_ends; // 2 per path: I = 0 rows
-    int64_t cols() const { return paths ? (int64_t)free_ends.size() / 2 : (int64_t)ep.size(); }
+    // plane-wave receive form: two homogeneous columns per wire or path, one
+    // right-hand side per incidence direction (theta, phi) with its r_hat and
+    // polarisation vector (10 doubles)
+    bool planewave = false;
+    std::vector<double> dirs;       // 2 per right-hand side
+    std::vector<double> waves;      // 10 per right-hand side
+    int64_t cols() const {
+        const int64_t c = paths ? (int64_t)free_ends.size() / 2 : (int64_t)ep.size();
+        return planewave ? 2 * c : c;
+    }
     std::vector<fnec_load> loads;   // LD cards, deck order
     std::vector<fnec_tl> tls;       // TL cards, deck order
     std::vector<fnec_nt> nts;       // NT cards, deck order
@@ -676,6 +685,11 @@ struct fnec_batch {
            *d_total = nullptr;
     cx *d_cur = nullptr;           // compact currents (read into pinned memory)
     int64_t *d_cur_off = nullptr;  // per solve: its first entry in d_cur
+    // plane-wave antennas: per solve its incidence (theta, phi) or NaNs, and
+    // the device's peak |I| of each solve
+    bool has_wave = false;
+    std::vector<double> recv_dirs;
+    double *d_peak = nullptr;
     MixedWork mixed;
     GridPlan grid;
     // execution: the stream every operation of the batch is enqueued on;
@@ -853,6 +867,13 @@ struct BatchPlace {
 
 static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, fnec_batch **out,
                        bool need_solve = true, const BatchPlace &place = BatchPlace()) {
+    int64_t n_solves = 0;
+    for (const HostAnt &h : hs) {
+        if (h.planewave && precision == FNEC_PRECISION_MIXED)
+            return fail(ctx, FNEC_ERR_UNSUPPORTED, "plane-wave antennas solve in the FP64 form");
+        n_solves += (int64_t)h.freqs.size() * (int64_t)std::max<size_t>(h.rhs_srcs.size(), 1);
+    }
+    if (n_solves > 65535) return fail(ctx, FNEC_ERR_TOO_LARGE, "a batch holds at most 65535 solves");
     fnec_batch *b = new fnec_batch();
     b->ctx = ctx;
     b->st = place.st ? place.st : ctx->stream;
@@ -886,10 +907,16 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
         for (size_t q = 0; q < h.ep.size(); ++q)
             for (int64_t r = h.ep[q].first; r <= h.ep[q].second; ++r) row_wire[r] = (int32_t)q;
         if (h.paths) row_wire = h.path_of;  // linear.rs:851-856: one column per path
+        if (h.planewave)  // linear.rs:955-961: the cos column 2q, the sin column 2q + 1
+            for (auto &c : row_wire) c *= 2;
+        a.hom2 = h.planewave ? 1 : 0;
         a.rowwire_off = (int64_t)b->ibuf.size();
         b->ibuf.insert(b->ibuf.end(), row_wire.begin(), row_wire.end());
         std::vector<std::vector<int32_t>> rows_of(a.w);
-        for (int r = 0; r < n; ++r) rows_of[row_wire[r]].push_back(r);
+        for (int r = 0; r < n; ++r) {
+            rows_of[row_wire[r]].push_back(r);
+            if (h.planewave) rows_of[row_wire[r] + 1].push_back(r);
+        }
         a.wptr_off = (int64_t)b->ibuf.size();
         int32_t acc = 0;
         b->ibuf.push_back(0);
@@ -1034,10 +1061,15 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
         ff_req_max = std::max(ff_req_max, n_req);
         ff_int_max = std::max(ff_int_max, n_int);
         smem_max = std::max(smem_max, sizeof(DevRun) * h.runs.size() + sizeof(cx) * (size_t)n);
-        if (h.paths) {
-            a.paths = 1;
+        if (h.paths) a.paths = 1;
+        if (!h.arc.empty()) {
             a.arc_off = (int64_t)b->pts.size();  // 2n doubles (n arc lengths, n signs): pairs stay aligned
             b->pts.insert(b->pts.end(), h.arc.begin(), h.arc.end());
+        }
+        if (h.planewave) {
+            a.wave_off = (int64_t)b->pts.size();  // 10 doubles per direction: pairs stay aligned
+            b->pts.insert(b->pts.end(), h.waves.begin(), h.waves.end());
+            b->has_wave = true;
         }
         b->ants.push_back(a);
         b->max_w = std::max(b->max_w, (int)a.w);
@@ -1087,7 +1119,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
                 b->z_el += (int64_t)n * n;
                 b->a_el += (int64_t)s * (s + 1);
             }
-            b->cos_el += n;
+            b->cos_el += h.planewave ? 2 * (int64_t)n : n;
             b->piv_el += s;
             b->max_s = std::max(b->max_s, s);
             b->max_n = std::max(b->max_n, n);
@@ -1124,6 +1156,8 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
                 b->feed_row_off.push_back(b->feed_rows);
                 b->feed_rows += nf;
                 b->uinfo.push_back(ui);
+                b->recv_dirs.push_back(h.planewave ? h.dirs[2 * r] : std::nan(""));
+                b->recv_dirs.push_back(h.planewave ? h.dirs[2 * r + 1] : std::nan(""));
                 b->solves.push_back(v);
             }
             b->units.push_back(u);
@@ -1206,6 +1240,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
     DA(d_partials, (int64_t)b->ff_blocks * (int64_t)b->solves.size());
     DA(d_pat, PAT_STRIDE * b->pat_el);
     DA(d_total, b->solves.size());
+    DA(d_peak, b->has_wave ? b->solves.size() : 1);
     {
         int64_t tc = b->uinfo.empty() ? 0 : b->uinfo.back().cur_off + b->uinfo.back().n;
         std::vector<int64_t> co(b->uinfo.size());
@@ -1276,6 +1311,107 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
     return FNEC_OK;
 }
 
+// planewave.rs:86-105 r_hat and pol_hat of one incidence direction, with the
+// platform sin/cos as the reference calls them (this file is built without
+// contraction): 10 doubles, r_hat[3], pol re[3], pol im[3], 0.
+static void wave_vectors(uint32_t ex_type, double theta_deg, double phi_deg, double eta_deg, double ar_card,
+                         double *out) {
+    const double rad = PI / 180.0;  // f64::to_radians
+    const double t = theta_deg * rad, p = phi_deg * rad, eta = eta_deg * rad;
+    out[0] = std::sin(t) * std::cos(p);
+    out[1] = std::sin(t) * std::sin(p);
+    out[2] = std::cos(t);
+    const double th[3] = {std::cos(t) * std::cos(p), std::cos(t) * std::sin(p), -std::sin(t)};
+    const double ph[3] = {-std::sin(p), std::cos(p), 0.0};
+    const double ce = std::cos(eta), se = std::sin(eta);
+    double ar = 0.0, sense = 0.0;  // planewave.rs:62-67
+    if (ex_type == 2) {
+        ar = ar_card;
+        sense = 1.0;
+    } else if (ex_type == 3) {
+        ar = ar_card;
+        sense = -1.0;
+    }
+    const HC jminor{0.0, sense * ar};
+    for (int i = 0; i < 3; ++i) {
+        const double major = ce * th[i] + se * ph[i];
+        const double minor = -se * th[i] + ce * ph[i];
+        const HC v = hc_add({major, 0.0}, hc_scale(jminor, minor));
+        out[3 + i] = v.re;
+        out[6 + i] = v.im;
+    }
+    out[9] = 0.0;
+}
+
+// solve_session.rs:262-301 and :313-355: the receive form of a deck with a
+// plane-wave EX card.  A non-trivial degree-2 conductor path takes the path
+// form (build_planewave_hallen_paths); otherwise the per-tag wires, which
+// must not touch (planewave.rs:176-180, detect_wire_junctions within 1e-6 m
+// between ends of different segments).  The arc table carries the
+// along-wire coordinate from each wire's geometric midpoint (sign 1).
+static int plane_wave_form(const fnec_antenna &A, HostAnt &h, std::string &why) {
+    const fnec_plane_wave &pw = *A.plane_wave;
+    if (pw.ex_type < 1 || pw.ex_type > 3) {
+        why = "plane wave: EX type must be 1, 2 or 3";
+        return FNEC_ERR_BAD_ARG;
+    }
+    if (A.n_sources != 0) {
+        why = "a plane-wave antenna takes no voltage sources";
+        return FNEC_ERR_BAD_ARG;
+    }
+    h.planewave = true;
+    if (!conductor_paths(h)) {
+        const auto wires = wire_endpoints(h.segs);
+        for (size_t i = 0; i < 2 * wires.size(); ++i) {
+            const int64_t si = i % 2 == 0 ? wires[i / 2].first : wires[i / 2].second;
+            const double *pi = i % 2 == 0 ? h.segs[si].start : h.segs[si].end;
+            for (size_t j = i + 1; j < 2 * wires.size(); ++j) {
+                const int64_t sj = j % 2 == 0 ? wires[j / 2].first : wires[j / 2].second;
+                if (si == sj) continue;
+                const double *pj = j % 2 == 0 ? h.segs[sj].start : h.segs[sj].end;
+                const double dx = pi[0] - pj[0], dy = pi[1] - pj[1], dz = pi[2] - pj[2];
+                if (std::sqrt(dx * dx + dy * dy + dz * dz) <= 1e-6) {
+                    why = "EX: incident plane wave is supported on straight, non-junctioned wires; junctioned "
+                          "geometry is not yet supported";
+                    return FNEC_ERR_UNSUPPORTED;
+                }
+            }
+        }
+        h.ep = wires;
+        set_comp(h, wires);
+        const int64_t n = (int64_t)h.segs.size();
+        h.arc.assign(2 * n, 1.0);
+        for (const auto &w : wires) {
+            const double *a = h.segs[w.first].mid, *b = h.segs[w.second].mid, *dir = h.segs[w.first].dir;
+            const double wm[3] = {(a[0] + b[0]) / 2.0, (a[1] + b[1]) / 2.0, (a[2] + b[2]) / 2.0};
+            for (int64_t i = w.first; i <= w.second; ++i) {
+                const double d[3] = {h.segs[i].mid[0] - wm[0], h.segs[i].mid[1] - wm[1], h.segs[i].mid[2] - wm[2]};
+                h.arc[i] = d[0] * dir[0] + d[1] * dir[1] + d[2] * dir[2];
+            }
+        }
+    }
+    const uint32_t nt = std::max<uint32_t>(pw.n_theta, 1), np = std::max<uint32_t>(pw.n_phi, 1);
+    const uint64_t nd = (uint64_t)nt * np;
+    if (nd > 65535) {
+        why = "plane wave: at most 65535 incidence directions";
+        return FNEC_ERR_TOO_LARGE;
+    }
+    for (uint32_t it = 0; it < nt; ++it)
+        for (uint32_t ip = 0; ip < np; ++ip) {
+            // the first direction is the deck's own (theta0, phi0) as given
+            const double th = it == 0 ? pw.theta0 : pw.theta0 + (double)it * pw.d_theta;
+            const double ph = ip == 0 ? pw.phi0 : pw.phi0 + (double)ip * pw.d_phi;
+            h.dirs.push_back(th);
+            h.dirs.push_back(ph);
+            double v[10];
+            wave_vectors(pw.ex_type, th, ph, pw.eta, pw.axial_ratio, v);
+            h.waves.insert(h.waves.end(), v, v + 10);
+        }
+    h.rhs_srcs.assign(nd, {});
+    h.rhs_feeds.assign(nd, {});
+    return FNEC_OK;
+}
+
 // HostAnt from GW/EX/RP cards: the CLI standard Hallen branch topology
 // (solve_session.rs:1379-1400).
 static int antenna_from_cards(const fnec_antenna &A, HostAnt &h, std::string &why) {
@@ -1319,11 +1455,14 @@ static int antenna_from_cards(const fnec_antenna &A, HostAnt &h, std::string &wh
     }
     auto merged = merge_collinear(h.segs);
     set_comp(h, merged);
-    if (!conductor_paths(h)) {  // the standard branch (solve_session.rs:1379-1400)
+    if (A.plane_wave) {
+        int st = plane_wave_form(A, h, why);
+        if (st != FNEC_OK) return st;
+    } else if (!conductor_paths(h)) {  // the standard branch (solve_session.rs:1379-1400)
         h.ep = merged;
         cli_junctions(h.segs, merged, h);
     }
-    int st = resolve_sources(h, A.sources, A.n_sources, A.separate_sources != 0, why);
+    int st = A.plane_wave ? FNEC_OK : resolve_sources(h, A.sources, A.n_sources, A.separate_sources != 0, why);
     if (st != FNEC_OK) return st;
     build_runs(h);
     h.rp.pts_off = -1;
@@ -1496,6 +1635,11 @@ static int run_pipeline(fnec_batch *b) {
         launch_hallen_rhs(b->d_solves, ns, b->d_ants, b->d_segs, b->d_ibuf, b->d_srcs, b->d_pts, b->d_rhs, b->d_cos,
                           2.0 * PI / ETA0, st);
         ++L;
+        if (b->has_wave) {
+            launch_planewave_rhs(b->d_solves, ns, b->max_n, b->d_ants, b->d_segs, b->d_ibuf, b->d_pts, b->d_x,
+                                 b->d_rhs, b->d_cos, 2.0 * PI / ETA0, st);
+            L += 2;
+        }
     }
     mark(2);
     if (b->precision == FNEC_PRECISION_MIXED) {
@@ -1536,6 +1680,10 @@ static int run_pipeline(fnec_batch *b) {
     launch_feedpoints(b->d_solves, ns, b->d_ants, b->d_segs, b->d_ibuf, b->d_feeds, b->d_x, b->d_status,
                       b->d_feed_out, b->d_feed_row_off, st);
     ++L;
+    if (b->has_wave) {
+        launch_receive_peaks(b->d_solves, ns, b->d_ants, b->d_x, b->d_status, b->d_peak, st);
+        ++L;
+    }
     check("feedpoints");
     mark(7);
     if (b->ff_blocks > 0) {
@@ -2038,6 +2186,30 @@ int fnec_batch_read(fnec_batch *b, double *currents, double *feeds, double *patt
     return FNEC_OK;
 }
 
+int fnec_batch_read_receive(fnec_batch *b, double *out) {
+    if (!b || !out) return FNEC_ERR_BAD_ARG;
+    const size_t ns = b->solves.size();
+    std::vector<double> peak(ns, std::nan(""));
+    if (b->has_wave && ns > 0) {
+        cudaError_t e = cudaMemcpyAsync(peak.data(), b->d_peak, sizeof(double) * ns, cudaMemcpyDeviceToHost, b->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->st);
+        if (e != cudaSuccess) return fail(b->ctx, FNEC_ERR_CUDA, cudaGetErrorString(e));
+    }
+    // solve_session.rs:356-374: each system's responses relative to its
+    // largest peak (f64::max folds from 0 and passes over NaN)
+    std::vector<double> top(b->units.size(), 0.0);
+    for (size_t q = 0; q < ns; ++q)
+        if (!std::isnan(peak[q])) top[b->solves[q].sys] = std::max(top[b->solves[q].sys], peak[q]);
+    for (size_t q = 0; q < ns; ++q) {
+        out[3 * q] = b->recv_dirs[2 * q];
+        out[3 * q + 1] = b->recv_dirs[2 * q + 1];
+        const double pk = peak[q], mx = top[b->solves[q].sys];
+        if (std::isnan(b->recv_dirs[2 * q]) || std::isnan(pk)) out[3 * q + 2] = std::nan("");
+        else out[3 * q + 2] = (pk > 0.0 && mx > 0.0) ? 20.0 * std::log10(pk / mx) : -999.99;
+    }
+    return FNEC_OK;
+}
+
 int fnec_batch_read_unit(fnec_batch *b, uint32_t unit, double *x, int32_t *pivots) {
     if (!b || unit >= b->solves.size()) return FNEC_ERR_BAD_ARG;
     fnec_ctx *ctx = b->ctx;
@@ -2476,6 +2648,7 @@ int64_t request_bytes(const HostAnt &h, int precision) {
     b += n * n / 16 + 64 * ((n + 63) / 64) * ((n + 64) / 64);  // fill and Gram tile lists
     b += 16 * n * f * r;                                   // compact currents for pinned reads
     b += (16 * s + 16 * n + 8 * n + 64) * f * r;           // x, rhs, cos, feeds
+    if (h.planewave) b += 8 * n * f + 8 * f * r + 80 * r + 16 * n;  // sin column, peaks, waves, arc
     b += (48 + 32) * pts * f * r + 8 * 1024 * f * r;      // pattern, fields, partials
     if (precision == FNEC_PRECISION_MIXED) {
         int64_t kb = (n + 31) / 32, rp = ((2 * n + 127) / 128) * 128;

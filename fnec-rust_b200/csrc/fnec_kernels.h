@@ -107,6 +107,14 @@ uint64_t launch_factor_exact(const UnitDesc *units, int nu, int max_s, const Gri
                              int32_t *piv, int32_t *status, cudaStream_t st);
 void launch_backsub(const UnitDesc *units, int nu, int max_s, const cx *A, cx *x,
                     const int32_t *status, cudaStream_t st);
+// plane-wave forcing and homogeneous columns of the hom2 solves (x holds
+// the incident field until the solve overwrites it)
+void launch_planewave_rhs(const UnitDesc *solves, int ns, int max_n, const AntDesc *ants, const DevSeg *segs,
+                          const int32_t *ibuf, const double *dtab, cx *x, cx *rhs, double *cosv, double scale,
+                          cudaStream_t st);
+// peak |I| per plane-wave solve (NaN for a failed system)
+void launch_receive_peaks(const UnitDesc *solves, int ns, const AntDesc *ants, const cx *x, const int32_t *status,
+                          double *peak, cudaStream_t st);
 // Z[index] += (re, im) for every stamp (LD loads on the diagonal)
 void launch_stamps(const DevStamp *stamps, int n, cx *z, cudaStream_t st);
 void launch_feedpoints(const UnitDesc *solves, int ns, const AntDesc *ants, const DevSeg *segs,

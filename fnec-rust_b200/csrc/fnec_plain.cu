@@ -95,6 +95,7 @@ __global__ void k_hallen_rhs(const UnitDesc *__restrict__ solves, const AntDesc 
                              cx *rhs_buf, double *cos_buf, double scale) {
     UnitDesc u = solves[blockIdx.x];  // one right-hand side
     AntDesc a = ants[u.ant];
+    if (a.hom2) return;  // a receiving antenna: k_planewave_field / k_planewave_rhs
     const DevSeg *sg = segs + a.seg_off;
     const int32_t *comp = ibuf + a.comp_off;
     const int32_t *sptr = ibuf + a.sptr_off;
@@ -159,6 +160,90 @@ __global__ void k_hallen_rhs(const UnitDesc *__restrict__ solves, const AntDesc 
         }
         rhs_buf[u.rhs_off + m] = r;
     }
+}
+
+// ---------------------------------------------------------------------------
+// Plane-wave forcing (planewave.rs:162-254 per wire, :278-348 per path).
+// k_planewave_field: the tangential incident field of every segment for
+// every incidence direction, E_p = sign_p (e . d_p) exp(+j k r_hat . r_p)
+// with d_p the direction of the wire's first segment (per-wire form) or of
+// the segment itself (path form); the solve's x vector holds it until the
+// solve overwrites x.  Solve 0 of each system also writes cos(k s) and
+// sin(k s), times the sign, as the two homogeneous columns.
+// k_planewave_rhs: rhs_m = sign_m (-j 2 pi / eta0) sum_p E_p sin(k |s_m -
+// s_p|) dl_p over the rows p of m's wire or path in ascending order.
+// Every operation is the reference's, in its order; sign = 1 in the
+// per-wire form, where multiplying by it is exact.
+// ---------------------------------------------------------------------------
+__global__ void k_planewave_field(const UnitDesc *__restrict__ solves, int ns, const AntDesc *__restrict__ ants,
+                                  const DevSeg *__restrict__ segs, const int32_t *__restrict__ ibuf,
+                                  const double *__restrict__ dtab, cx *xbuf, double *cos_buf) {
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int si = blockIdx.y; si < ns; si += gridDim.y) {  // solves beyond the grid's y limit
+        UnitDesc u = solves[si];
+        AntDesc a = ants[u.ant];
+        if (!a.hom2 || p >= a.n) continue;
+        const DevSeg *sg = segs + a.seg_off;
+        const double *wv = dtab + a.wave_off + 10 * (int64_t)u.rhs;  // r_hat[3], pol re[3], pol im[3]
+        const double *dir = a.paths ? sg[p].dir : sg[ibuf[a.comp_off + 2 * p]].dir;
+        const double s = dtab[a.arc_off + p], sgn = dtab[a.arc_off + a.n + p];
+        const double k = u.k_fill;
+        cx coup = cx_make(0.0, 0.0);
+        for (int c = 0; c < 3; ++c) coup = cx_add(coup, cx_make(D_MUL(wv[3 + c], dir[c]), D_MUL(wv[6 + c], dir[c])));
+        const double phase = D_MUL(
+            k, D_ADD(D_ADD(D_MUL(wv[0], sg[p].mid[0]), D_MUL(wv[1], sg[p].mid[1])), D_MUL(wv[2], sg[p].mid[2])));
+        double sn, cs;
+        cr_sincos(phase, &sn, &cs);
+        const cx e = cx_mul(coup, cx_make(D_MUL(1.0, cs), D_MUL(1.0, sn)));  // from_polar(1, phase)
+        xbuf[u.x_off + p] = cx_make(D_MUL(e.re, sgn), D_MUL(e.im, sgn));
+        if (u.rhs == 0) {
+            double ss, sc;
+            cr_sincos(D_MUL(k, s), &ss, &sc);
+            cos_buf[u.cos_off + p] = D_MUL(sgn, sc);
+            cos_buf[u.cos_off + a.n + p] = D_MUL(sgn, ss);
+        }
+    }
+}
+
+__global__ void k_planewave_rhs(const UnitDesc *__restrict__ solves, int ns, const AntDesc *__restrict__ ants,
+                                const DevSeg *__restrict__ segs, const int32_t *__restrict__ ibuf,
+                                const double *__restrict__ dtab, const cx *__restrict__ xbuf, cx *rhs_buf,
+                                double scale) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    for (int si = blockIdx.y; si < ns; si += gridDim.y) {
+        UnitDesc u = solves[si];
+        AntDesc a = ants[u.ant];
+        if (!a.hom2 || m >= a.n) continue;
+        const DevSeg *sg = segs + a.seg_off;
+        const double *s_mid = dtab + a.arc_off, *sgn = s_mid + a.n;
+        const int32_t col = ibuf[a.rowwire_off + m];  // the wire's cos column
+        const int32_t *wptr = ibuf + a.wptr_off, *wrow = ibuf + a.wrow_off;
+        const cx *e = xbuf + u.x_off;
+        const double k = u.k_fill, sm = s_mid[m];
+        cx acc = cx_make(0.0, 0.0);
+        for (int q = wptr[col]; q < wptr[col + 1]; ++q) {
+            const int p = wrow[q];
+            double ks, kc;
+            cr_sincos(D_MUL(k, fabs(D_SUB(sm, s_mid[p]))), &ks, &kc);
+            const cx ep = e[p];
+            const double len = sg[p].len;
+            acc = cx_add(acc, cx_make(D_MUL(D_MUL(ep.re, ks), len), D_MUL(D_MUL(ep.im, ks), len)));
+        }
+        const cx r = cx_mul(cx_make(0.0, -scale), acc);
+        rhs_buf[u.rhs_off + m] = cx_make(D_MUL(r.re, sgn[m]), D_MUL(r.im, sgn[m]));
+    }
+}
+
+// Peak |I| of each plane-wave solve (solve_session.rs:354): the largest
+// hypot over the segment currents, NaN when the solve failed.
+__global__ void k_receive_peaks(const UnitDesc *__restrict__ solves, const AntDesc *__restrict__ ants,
+                                const cx *__restrict__ xbuf, const int32_t *__restrict__ status, double *peak) {
+    UnitDesc u = solves[blockIdx.x];
+    if (!ants[u.ant].hom2) return;
+    double v = 0.0;
+    for (int m = threadIdx.x; m < u.n; m += 32) v = fmax(v, cx_norm(xbuf[u.x_off + m]));
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0) peak[blockIdx.x] = status[u.sys] != 0 ? __longlong_as_double(0x7ff8000000000000ll) : v;
 }
 
 // ---------------------------------------------------------------------------
@@ -347,7 +432,8 @@ __global__ void k_gram_ccols(const UnitDesc *__restrict__ units, const AntDesc *
     int n = u.n, s = u.s, w1 = s + 1;
     const cx *z = zbuf + u.z_off;
     const cx *y = rhs_buf + u.rhs_off;
-    const double *cv = cos_buf + u.cos_off;
+    // the plane-wave form's odd columns hold -sin(k s): the second half
+    const double *cv = cos_buf + u.cos_off + ((a.hom2 && (w & 1)) ? n : 0);
     const int32_t *wptr = ibuf + a.wptr_off;
     const int32_t *wrow = ibuf + a.wrow_off;
     cx *A = abuf + u.a_off;
@@ -369,13 +455,17 @@ __global__ void k_gram_ccols(const UnitDesc *__restrict__ units, const AntDesc *
             A[(int64_t)(n + w) * w1 + s] = row;
         }
     }
-    // the W x W block row of this wire: cos^2 sum on the diagonal, exact zeros elsewhere
+    // the W x W block row of this column: the sum of squares on the
+    // diagonal, and in the plane-wave form the cos-sin cross sum of the same
+    // wire (its rows ascending, as the reference's sum over all rows); exact
+    // zeros elsewhere
     for (int v = threadIdx.x; v < a.w; v += blockDim.x) {
         cx d = cx_make(0.0, 0.0);
-        if (v == w) {
+        if (v == w || (a.hom2 && v == (w ^ 1))) {
+            const double *cw = cos_buf + u.cos_off + ((a.hom2 && (v & 1)) ? n : 0);
             for (int q = b; q < e; ++q) {
-                cx c = cx_make(-cv[wrow[q]], 0.0);
-                d = cx_add(d, cx_conj_mul(c, c));
+                const int r = wrow[q];
+                d = cx_add(d, cx_conj_mul(cx_make(-cv[r], 0.0), cx_make(-cw[r], 0.0)));
             }
         }
         A[(int64_t)(n + w) * w1 + n + v] = d;
@@ -896,7 +986,7 @@ __global__ void k_extra_rhs_b(const UnitDesc *__restrict__ solves, const AntDesc
     } else if (i < n + a.w) {
         int w = i - n;
         const int32_t *wptr = ibuf + a.wptr_off, *wrow = ibuf + a.wrow_off;
-        const double *cv = cos_buf + u.cos_off;
+        const double *cv = cos_buf + u.cos_off + ((a.hom2 && (w & 1)) ? n : 0);
         cx acc = cx_make(0.0, 0.0);
         for (int q = wptr[w]; q < wptr[w + 1]; ++q) {
             int r = wrow[q];
@@ -953,6 +1043,18 @@ void launch_hallen_rhs(const UnitDesc *solves, int ns, const AntDesc *ants, cons
                        const int32_t *ibuf, const DevSource *srcs, const double *dtab, cx *rhs, double *cosv,
                        double scale, cudaStream_t st) {
     if (ns > 0) k_hallen_rhs<<<ns, 128, 0, st>>>(solves, ants, segs, ibuf, srcs, dtab, rhs, cosv, scale);
+}
+void launch_planewave_rhs(const UnitDesc *solves, int ns, int max_n, const AntDesc *ants, const DevSeg *segs,
+                          const int32_t *ibuf, const double *dtab, cx *x, cx *rhs, double *cosv, double scale,
+                          cudaStream_t st) {
+    if (ns <= 0 || max_n <= 0) return;
+    dim3 g((max_n + 127) / 128, ns < 65535 ? ns : 65535);
+    k_planewave_field<<<g, 128, 0, st>>>(solves, ns, ants, segs, ibuf, dtab, x, cosv);
+    k_planewave_rhs<<<g, 128, 0, st>>>(solves, ns, ants, segs, ibuf, dtab, x, rhs, scale);
+}
+void launch_receive_peaks(const UnitDesc *solves, int ns, const AntDesc *ants, const cx *x, const int32_t *status,
+                          double *peak, cudaStream_t st) {
+    if (ns > 0) k_receive_peaks<<<ns, 32, 0, st>>>(solves, ants, x, status, peak);
 }
 void launch_fill_exact(const UnitDesc *units, const AntDesc *ants, const DevSeg *segs,
                        const int4 *tiles, int ntiles, cx *z, cudaStream_t st) {

@@ -78,8 +78,12 @@ struct AntDesc {
     // path (rowwire), I = 0 rows at the two free ends of each path, and
     // cos / source terms along the signed arc length of each path
     int32_t paths;       // 1: the path form; 0: merged straight wires
-    int32_t pad_a;
+    // plane-wave form (linear.rs:910-1090): two homogeneous columns per wire
+    // or path, cos (2q) then sin (2q + 1); cos(k s) then sin(k s) per system
+    // (2n doubles); the arc table holds s and sign for both layouts
+    int32_t hom2;
     int64_t arc_off;     // doubles: s_mid[n] (signed arc length), then sign[n]
+    int64_t wave_off;    // doubles: 10 per right-hand side (r_hat, pol re, pol im, pad)
 };
 
 // One constraint row of M (linear.rs:744-762): M[N+q][c0] = 1 and, for a

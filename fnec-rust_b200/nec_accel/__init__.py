@@ -89,10 +89,16 @@ class _RpCard(ctypes.Structure):
                 ("d_phi", _D)]
 
 
+class _PlaneWave(ctypes.Structure):
+    _fields_ = [("ex_type", _U32), ("n_theta", _U32), ("n_phi", _U32), ("reserved", _U32), ("theta0", _D),
+                ("phi0", _D), ("eta", _D), ("d_theta", _D), ("d_phi", _D), ("axial_ratio", _D)]
+
+
 class _Antenna(ctypes.Structure):
     _fields_ = [("wires", _P), ("n_wires", _U32), ("sources", _P), ("n_sources", _U32), ("ground", _I32),
                 ("n_freqs", _U32), ("freqs_hz", _P), ("rp", _P), ("separate_sources", _U32), ("loads", _P),
-                ("n_loads", _U32), ("tls", _P), ("n_tls", _U32), ("nts", _P), ("n_nts", _U32)]
+                ("n_loads", _U32), ("tls", _P), ("n_tls", _U32), ("nts", _P), ("n_nts", _U32),
+                ("plane_wave", _P)]
 
 
 class _UnitInfo(ctypes.Structure):
@@ -181,6 +187,7 @@ SIGNATURES = {
     "fnec_batch_set_profiling": (ctypes.c_int, [_P, ctypes.c_int]),
     "fnec_batch_phase_ms": (ctypes.c_int, [_P, _P]),
     "fnec_batch_read_unit": (ctypes.c_int, [_P, _U32, _P, _P]),
+    "fnec_batch_read_receive": (ctypes.c_int, [_P, _P]),
     "fnec_batch_read_z": (ctypes.c_int, [_P, _U32, _P]),
     "fnec_batch_read_refinement": (ctypes.c_int, [_P, _P, _P]),
     "fnec_batch_get_schedule": (ctypes.c_int, [_P, _P]),
@@ -527,9 +534,10 @@ def dispatch_frequency_point(request_kind: int, freq_hz: float) -> str:
 @dataclass
 class Antenna:
     """One geometry: GW wires, voltage EX sources, ground, FR frequencies, an
-    optional RP card (n_theta, n_phi, theta0, phi0, d_theta, d_phi) and
+    optional RP card (n_theta, n_phi, theta0, phi0, d_theta, d_phi),
     optional LD, TL and NT cards (LOAD_DTYPE / TL_DTYPE / NT_DTYPE arrays,
-    deck order)."""
+    deck order) and an optional plane-wave EX card (plane_wave(...); the
+    sources must then be empty)."""
 
     wires: np.ndarray
     sources: np.ndarray
@@ -540,6 +548,16 @@ class Antenna:
     loads: Optional[np.ndarray] = None
     tls: Optional[np.ndarray] = None
     nts: Optional[np.ndarray] = None
+    plane_wave: Optional[tuple] = None
+
+
+def plane_wave(ex_type=1, theta0=0.0, phi0=0.0, eta=0.0, n_theta=1, n_phi=1, d_theta=0.0, d_phi=0.0,
+               axial_ratio=0.0) -> tuple:
+    """A plane-wave EX card (type 1 linear, 2 right / 3 left elliptic): I2 =
+    n_theta, I3 = n_phi, F1..F6 = theta0, phi0, eta, d_theta, d_phi, axial
+    ratio.  Its directions are the receive sweep (theta outer, phi inner)."""
+    return (int(ex_type), int(n_theta), int(n_phi), float(theta0), float(phi0), float(eta), float(d_theta),
+            float(d_phi), float(axial_ratio))
 
 
 def wires_array(wires) -> np.ndarray:
@@ -604,11 +622,16 @@ def _antenna_struct(a, keep: list):
         return None if x is None or len(x) == 0 else np.ascontiguousarray(x, dtype=dt)
 
     ld, tl, nt = opt(a.loads, LOAD_DTYPE), opt(a.tls, TL_DTYPE), opt(a.nts, NT_DTYPE)
-    keep += [w, s, f, rp, ld, tl, nt]
+    pw = None
+    if a.plane_wave is not None:
+        t, nth, nph, th0, ph0, eta, dth, dph, ar = a.plane_wave
+        pw = _PlaneWave(t, nth, nph, 0, th0, ph0, eta, dth, dph, ar)
+    keep += [w, s, f, rp, ld, tl, nt, pw]
     return _Antenna(_ptr(w), len(w), _ptr(s), len(s), int(a.ground), len(f), _ptr(f),
                     ctypes.cast(ctypes.pointer(rp), _P) if rp is not None else None,
                     int(bool(a.separate_sources)), _ptr(ld), 0 if ld is None else len(ld),
-                    _ptr(tl), 0 if tl is None else len(tl), _ptr(nt), 0 if nt is None else len(nt))
+                    _ptr(tl), 0 if tl is None else len(tl), _ptr(nt), 0 if nt is None else len(nt),
+                    ctypes.cast(ctypes.pointer(pw), _P) if pw is not None else None)
 
 
 class _Schedule(ctypes.Structure):
@@ -786,6 +809,13 @@ class HallenBatch:
         piv = np.zeros(u["s"], np.int32)
         self.ctx.check(lib().fnec_batch_read_unit(self._h, unit, _ptr(x), _ptr(piv)), "batch_read_unit")
         return x, piv
+
+    def read_receive(self) -> np.ndarray:
+        """(n_units, 3): theta, phi and the receive response in dB of every
+        plane-wave unit (solve_session.rs:313-375); NaN rows for the others."""
+        out = np.zeros((len(self.units), 3), np.float64)
+        self.ctx.check(lib().fnec_batch_read_receive(self._h, _ptr(out)), "batch_read_receive")
+        return out
 
     def refinement_stats(self):
         """(GMRES iterations, final preconditioned relative residual) per unit

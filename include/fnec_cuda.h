@@ -134,6 +134,22 @@ typedef struct {
     double d_phi;
 } fnec_rp_card;
 
+/* The first plane-wave EX card of a deck (EX types 1, 2, 3; card.rs ExCard
+ * via planewave.rs:60-80 and solve_session.rs:313-355): the wave arrives
+ * from (theta0, phi0) degrees with polarisation angle eta (F3); types 2 / 3
+ * are right / left elliptic with axial ratio F6, type 1 linear.  I2 x I3 =
+ * n_theta x n_phi incidence directions stepped by (d_theta, d_phi) (F4, F5)
+ * form the receive sweep, theta outer, phi inner; the first direction is
+ * the deck's own solve. */
+typedef struct {
+    uint32_t ex_type;
+    uint32_t n_theta, n_phi;
+    uint32_t reserved;
+    double theta0, phi0, eta;
+    double d_theta, d_phi;
+    double axial_ratio;
+} fnec_plane_wave;
+
 /* One LD card (nec_model card.rs:265-279; applied by loads.rs:103-222 and
  * solve_session.rs:1285-1289): load type 0 series RLC, 1 parallel RLC,
  * 2 series RL, 3 series RC, 4 series R + jX, 5 wire conductivity (other
@@ -194,6 +210,14 @@ typedef struct {
     uint32_t n_tls;
     const fnec_nt *nts;
     uint32_t n_nts;
+    /* NULL: the voltage sources drive the antenna.  Otherwise the antenna is
+     * a receiving one (solve_session.rs:262-301, linear.rs:910-1090): each
+     * incidence direction of the card is one right-hand side of the
+     * frequency's factorisation, with two homogeneous columns (cos, sin) per
+     * wire -- or per conductor path when some degree-2 path is non-trivial;
+     * other junctioned decks are FNEC_ERR_UNSUPPORTED, as the reference
+     * rejects them.  n_sources must be 0; FP64 form only. */
+    const fnec_plane_wave *plane_wave;
 } fnec_antenna;
 
 /* Per-unit shape, for sizing result buffers.  A unit is one solve: one
@@ -495,6 +519,12 @@ int fnec_batch_phase_ms(fnec_batch *b, double *ms);
 /* Per-unit solution vector x (currents then homogeneous constants), 2*s
  * doubles, and the pivot rows (s int32), for parity checks. */
 int fnec_batch_read_unit(fnec_batch *b, uint32_t unit, double *x, int32_t *pivots);
+/* Receive pattern of plane-wave units (solve_session.rs:313-375
+ * plane_wave_receive_sweep): 3 doubles per unit -- theta, phi (degrees)
+ * and 20 log10(peak |I| / the largest peak of the unit's system) dB,
+ * -999.99 for a zero peak; units without a plane wave get NaNs.  The peak
+ * is formed on the device. */
+int fnec_batch_read_receive(fnec_batch *b, double *out);
 /* Mixed-precision batches: per-unit GMRES iterations (n_units int32) and
  * final preconditioned relative residual (n_units doubles) of the last run. */
 int fnec_batch_read_refinement(fnec_batch *b, int32_t *iters, double *resid);
