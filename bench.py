@@ -60,6 +60,29 @@ def sweep_workload(seed: int = 11, n_freqs: int = 201):
     return wires, sources, freqs, rp
 
 
+def receive_workload(n_theta: int = 37, n_phi: int = 72):
+    """The 5-element array of the sweep as a receiving antenna: an EX 2 card
+    (right elliptic, axial ratio 0.5, eta 20 degrees) whose n_theta x n_phi
+    incidence directions in 5 degree steps are the receive sweep, at 13.0,
+    14.2 and 15.5 MHz; no RP card."""
+    wires, _, _, _ = sweep_workload()
+    freqs = [13.0e6, 14.2e6, 15.5e6]
+    card = (2, n_theta, n_phi, 0.0, 0.0, 20.0, 5.0, 5.0, 0.5)
+    return wires, freqs, card
+
+
+def receive_units(wires, freqs, card):
+    """The receive sweep as (wires, sources, ground, freq, rp, wave) units:
+    one per (frequency, direction), theta outer, phi inner."""
+    t, nth, nph, th0, ph0, eta, dth, dph, ar = card
+    out = []
+    for f in freqs:
+        for it in range(nth):
+            for ip in range(nph):
+                out.append((wires, [], 0, f, None, (t, th0 + it * dth, ph0 + ip * dph, eta, ar)))
+    return out
+
+
 def _seg_closest(p1, q1, p2, q2):
     """Closest distance and parameters between segments p1-q1 and p2-q2."""
     d1, d2, r = q1 - p1, q2 - p2, p1 - p2
@@ -377,9 +400,10 @@ def cpu_oracle_units(ref_units, n_units: int, threads: int):
     idx = np.linspace(0, len(ref_units) - 1, n_units).round().astype(int)
     probs = []
     for i in idx:
-        w, src, g, f, rp = ref_units[i]
+        w, src, g, f, rp = ref_units[i][:5]
+        wave = O.wave(*ref_units[i][5]) if len(ref_units[i]) > 5 else None
         pts = O.rp_card_points(*rp) if rp is not None else None
-        probs.append(O.Problem(O.wires_array(w), O.sources_array(src), f, ground=g, points=pts))
+        probs.append(O.Problem(O.wires_array(w), O.sources_array(src), f, ground=g, points=pts, wave=wave))
     t0 = time.perf_counter()
     O.solve_problems(probs, threads)
     dt = time.perf_counter() - t0
@@ -396,6 +420,9 @@ def reference_units(args):
     if args.workload == "mesh":
         wl, src, f = mesh_workload(args.cells)
         return [(wl, src, 1, f, None)], f"mesh: {args.cells}x{args.cells} cells over PEC ground"
+    if args.workload == "receive":
+        wires, freqs, card = receive_workload(args.n_theta, args.n_phi)
+        return receive_units(wires, freqs, card), RECEIVE_DESC(args.n_theta, args.n_phi)
     if args.workload == "serve":
         reqs = serve_requests(512, seed=13)
         return ([(w, [s], g, f, rp) for w, srcs, g, f, rp in reqs for s in srcs],
@@ -420,8 +447,10 @@ def run_reference(args):
         _, dt, _, _ = cpu_oracle_units(ref_units, n, threads)
         times.append(dt)
     rate = n * len(times) / sum(times)
+    metric = "receive solves/s (plane-wave incidence directions x frequencies)" if args.workload == "receive" \
+        else METRIC
     line = {
-        "impl": "reference", "metric": METRIC, "value": rate, "unit": "solves/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": metric, "value": rate, "unit": "solves/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * float(np.mean(times)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded)",
@@ -433,6 +462,121 @@ def run_reference(args):
         "e2e": {"value": rate, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def RECEIVE_DESC(nth, nph):
+    return (f"receive: 5-wire parallel array (N=255, S=265), EX 2 plane wave, {nth}x{nph} incidence directions "
+            f"x 3 freqs, each direction one right-hand side of its frequency's factorisation")
+
+
+def run_receive(args, acc, ctx, rank, local, dist):
+    """The plane-wave receive sweep (solve_session.rs:313-375): all
+    incidence directions of all frequencies in one FP64 batch; a unit is one
+    (frequency, direction) receive solve.  e2e uploads the batch tables,
+    runs, and reads the receive pattern (3 doubles per unit)."""
+    import torch
+
+    wires, freqs, card = receive_workload(args.n_theta, args.n_phi)
+    ant = acc.Antenna(acc.wires_array(wires), acc.sources_array([]), freqs, acc.GROUND_FREE, None, plane_wave=card)
+    batch = acc.HallenBatch([ant], precision=acc.PRECISION_FP64, ctx=ctx)
+    units = len(batch.units)
+    stream = torch.cuda.ExternalStream(acc.lib().fnec_ctx_stream(ctx.handle), device=local)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+
+    for _ in range(args.warmup):
+        batch.run()
+    batch.sync()
+    sampler = clock_sampler(local) if rank == 0 else None
+    barrier()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    evs[0].record(stream)
+    for k in range(args.steps):
+        batch.run()
+        evs[k + 1].record(stream)
+    batch.sync()
+    barrier()
+    step_ms = np.array([evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)])
+    clocks = clock_summary(sampler) if sampler is not None else None
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(args.steps):
+        batch.upload()
+        batch.run()
+        rec = batch.read_receive()  # synchronises: device peaks -> host, dB per unit
+    e1.record(stream)
+    batch.sync()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    batch.set_profiling(True)
+    phase = {k: 0.0 for k in batch.PHASES}
+    for _ in range(3):
+        batch.run()
+        for k, v in batch.phase_ms().items():
+            phase[k] += v / 3
+    batch.set_profiling(False)
+    vals = torch.tensor([float(step_ms.sum()), e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+    total_ms, e2e_ms = vals.tolist()
+    res = batch.read()
+    launches = batch.kernel_launches * args.steps
+    if rank == 0:
+        _, muladd_tf = acc.measure_fp64_peak(local)
+        n = 255.0
+        s = n + 2 * len(wires)
+        nsys = len(freqs)
+        lw = [w[1] for w in wires]
+        pairs = float(sum(L * L for L in lw))
+        # work per phase (real FP64 ops): rhs 6 per (direction, same-wire
+        # segment pair) + the per-system sin table; solve: Z^H y (8 N^2) and
+        # the cos/sin columns (16 N) per extra direction, forward + back
+        # substitution 8 S^2 per direction
+        work = {"rhs": units * (6.0 * pairs + n * (8 + 2 * SINCOS_FLOPS)) + nsys * pairs * SINCOS_FLOPS,
+                "gram": nsys * 8.0 * n * n * (n + 1), "factor": nsys * 8.0 * s ** 3 / 3,
+                "solve": (units - nsys) * (8.0 * n * n + 16.0 * n) + units * 8.0 * s * s}
+        dom = max(("rhs", "fill", "gram", "factor", "solve"), key=lambda k: phase[k])
+        rr = {k: {"achieved": w / 1e12 / (phase[k] * 1e-3), "unit": "TFLOP/s", "bound": "fp64",
+                  "peak": muladd_tf, "frac": w / 1e12 / (phase[k] * 1e-3) / muladd_tf}
+              for k, w in work.items() if phase[k] > 0}
+        roof = dict(rr.get(dom, {"bound": "fp64", "achieved": None, "peak": muladd_tf, "unit": "TFLOP/s",
+                                 "frac": None}))
+        roof.update({"kernel": dom, "traffic": None,
+                     "peak_source": "DMUL+DADD measured by fnec_measure_fp64_peak (the exact path issues no FMA)"})
+        line = {
+            "metric": "receive solves/s (plane-wave incidence directions x frequencies)", "workload": "receive",
+            "value": args.gpus * units * args.steps / (total_ms * 1e-3), "unit": "solves/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded 5-element array, seed 11)",
+            "config": {"workload": RECEIVE_DESC(args.n_theta, args.n_phi), "units_per_step": units,
+                       "precision": "fp64", "l2": "per-step working set ~60 MB (Z, factors, right-hand sides "
+                                                  "of 3 systems): L2-resident, no flush",
+                       "parallelism": f"replicas x{args.gpus} (no collective)"},
+            "e2e": {"value": args.gpus * units * args.steps / (e2e_ms * 1e-3), "unit": "solves/s",
+                    "h2d_bytes_per_step": int(batch.h2d_bytes), "d2h_bytes_per_step": 8 * units},
+            "gpu_launches": int(launches), "roofline": roof, "phase_rooflines": rr,
+            "phase_ms": {k: round(v, 4) for k, v in phase.items()}, "clocks": clocks,
+            "receive_db_range": [float(np.min(rec[:, 2])), float(np.max(rec[:, 2]))],
+        }
+        if not args.no_cpu_baseline:
+            ref = receive_units(wires, freqs, card)
+            threads = os.cpu_count() or 1
+            n_units = max(threads, 8)
+            rate, dt, probs, idx = cpu_oracle_units(ref, n_units, threads)
+            line["cpu_baseline"] = {"value": rate, "unit": "solves/s", "cores": threads, "kind": "port",
+                                    "sample": f"{n_units} evenly spaced (frequency, direction) receive solves, one "
+                                              f"per thread, each a full solve as the reference re-solves every "
+                                              f"direction, {dt:.1f} s wall"}
+            dev = max(float(np.abs(res.currents[i] - p.currents).max() / max(np.abs(p.currents).max(), 1e-300))
+                      for p, i in zip(probs, idx))
+            line["parity"] = {"units_checked": n_units, "max_rel_current_vs_oracle": dev}
+        print(json.dumps(line), flush=True)
+    batch.close()
 
 
 def run_serve(args, acc, ctx, rank, local, dist):
@@ -582,7 +726,7 @@ def main():
                          "mixed-only: the chosen form alone, no accuracy gate (for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--freqs", type=int, default=201, help="sweep points (201 = the workload; fewer = profiling)")
-    ap.add_argument("--workload", default="sweep5", choices=["sweep5", "uneven", "mesh", "serve"],
+    ap.add_argument("--workload", default="sweep5", choices=["sweep5", "uneven", "mesh", "serve", "receive"],
                     help="sweep5: the 5-wire frequency sweep (headline); uneven: 4096 random antennas; "
                          "mesh: the junctioned wire mesh over ground (one large solve); serve: a Poisson "
                          "request stream through the continuous-batching server")
@@ -591,6 +735,8 @@ def main():
     ap.add_argument("--lanes", type=int, default=4, help="serve: concurrent batches")
     ap.add_argument("--budget-gb", type=float, default=64.0, help="serve: HBM budget of the batches in flight")
     ap.add_argument("--cells", type=int, default=46, help="mesh workload size (cells per side)")
+    ap.add_argument("--n-theta", type=int, default=37, help="receive: incidence directions in theta")
+    ap.add_argument("--n-phi", type=int, default=72, help="receive: incidence directions in phi")
     ap.add_argument("--antennas", type=int, default=4096, help="uneven workload size")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner (default schedule; the pipeline is still graph-captured)")
@@ -616,8 +762,8 @@ def main():
     import nec_accel as acc
 
     ctx = acc.Context(local)
-    if args.workload == "serve":
-        run_serve(args, acc, ctx, rank, local, dist)
+    if args.workload in ("serve", "receive"):
+        (run_serve if args.workload == "serve" else run_receive)(args, acc, ctx, rank, local, dist)
         ctx.close()
         if dist is not None:
             dist.barrier()

@@ -690,6 +690,10 @@ struct fnec_batch {
     bool has_wave = false;
     std::vector<double> recv_dirs;
     double *d_peak = nullptr;
+    // right-hand sides beyond each system's first, in groups of up to 32
+    // solves: (system, first solve, count, 0)
+    std::vector<int4> rhs_groups;
+    int4 *d_rhs_groups = nullptr;
     MixedWork mixed;
     GridPlan grid;
     // execution: the stream every operation of the batch is enqueued on;
@@ -917,6 +921,14 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
             rows_of[row_wire[r]].push_back(r);
             if (h.planewave) rows_of[row_wire[r] + 1].push_back(r);
         }
+        int64_t ktab = 0;  // plane-wave form: each row's sin(k |s_m - s_p|) entries over its wire's rows
+        if (h.planewave) {
+            a.koff_off = (int64_t)b->ibuf.size();
+            for (int r = 0; r < n; ++r) {
+                b->ibuf.push_back((int32_t)ktab);
+                ktab += (int64_t)rows_of[row_wire[r]].size();
+            }
+        }
         a.wptr_off = (int64_t)b->ibuf.size();
         int32_t acc = 0;
         b->ibuf.push_back(0);
@@ -1119,12 +1131,15 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
                 b->z_el += (int64_t)n * n;
                 b->a_el += (int64_t)s * (s + 1);
             }
-            b->cos_el += h.planewave ? 2 * (int64_t)n : n;
+            b->cos_el += h.planewave ? 2 * (int64_t)n + ktab : n;
             b->piv_el += s;
             b->max_s = std::max(b->max_s, s);
             b->max_n = std::max(b->max_n, n);
             b->max_rhs = std::max(b->max_rhs, (int)a.n_rhs);
             int32_t uidx = u.sys;
+            const int32_t first_solve = (int32_t)b->solves.size();
+            for (int r0 = 1; r0 < a.n_rhs; r0 += 32)
+                b->rhs_groups.push_back(make_int4(uidx, first_solve + r0, std::min(32, a.n_rhs - r0), 0));
             const int32_t *fptr = &b->ibuf[a.fptr_off];
             for (int r = 0; r < a.n_rhs; ++r) {
                 UnitDesc v = u;
@@ -1187,7 +1202,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
            o_runs = pk.add(b->runs), o_rps = pk.add(b->rps), o_pts = pk.add(b->pts),
            o_ft = pk.add(b->fill_tiles), o_crows = pk.add(b->crows), o_gt = pk.add(b->gram_tiles), o_fro = pk.add(b->feed_row_off),
            o_rhs = pk.add(b->rhs_given), o_cos = pk.add(b->cos_given), o_z = pk.add(b->z_given),
-           o_st = pk.add(b->stamps);
+           o_st = pk.add(b->stamps), o_rg = pk.add(b->rhs_groups);
     b->in_bytes = pk.total > 0 ? pk.total : 256;
     const auto ta0 = std::chrono::steady_clock::now();
     if (b->pooled) {
@@ -1221,6 +1236,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
         b->d_cos_given = (double *)(b->d_in + o_cos);
         b->d_z_given = (double *)(b->d_in + o_z);
         b->d_stamps = (DevStamp *)(b->d_in + o_st);
+        b->d_rhs_groups = (int4 *)(b->d_in + o_rg);
     }
     // segments: uploaded with the arena for caller-provided geometry,
     // expanded on the device from the wires otherwise
@@ -1358,6 +1374,10 @@ static int plane_wave_form(const fnec_antenna &A, HostAnt &h, std::string &why) 
     if (A.n_sources != 0) {
         why = "a plane-wave antenna takes no voltage sources";
         return FNEC_ERR_BAD_ARG;
+    }
+    if (h.segs.size() > 46340) {  // the sin(k |s_m - s_p|) table is indexed in int32
+        why = "plane wave: at most 46340 segments";
+        return FNEC_ERR_TOO_LARGE;
     }
     h.planewave = true;
     if (!conductor_paths(h)) {
@@ -1669,8 +1689,11 @@ static int run_pipeline(fnec_batch *b) {
         mark(5);
         launch_backsub(b->d_units, nu, b->max_s, b->d_a, b->d_x, b->d_status, st);
         if (b->max_rhs > 1) {
+            // many right-hand sides per factorisation (receive sweeps): the grouped kernels
+            const bool grouped = b->max_rhs >= 8;
             launch_extra_rhs_exact(b->d_solves, ns, b->max_s, b->d_ants, b->d_ibuf, b->d_z, b->d_rhs, b->d_cos,
-                                   b->d_a, b->d_piv, b->d_x, b->d_status, st);
+                                   b->d_a, b->d_piv, b->d_x, b->d_status, st, grouped ? b->d_rhs_groups : nullptr,
+                                   grouped ? (int)b->rhs_groups.size() : 0);
             L += 2;
         }
         mark(6);
@@ -2648,7 +2671,8 @@ int64_t request_bytes(const HostAnt &h, int precision) {
     b += n * n / 16 + 64 * ((n + 63) / 64) * ((n + 64) / 64);  // fill and Gram tile lists
     b += 16 * n * f * r;                                   // compact currents for pinned reads
     b += (16 * s + 16 * n + 8 * n + 64) * f * r;           // x, rhs, cos, feeds
-    if (h.planewave) b += 8 * n * f + 8 * f * r + 80 * r + 16 * n;  // sin column, peaks, waves, arc
+    if (h.planewave) b += 8 * n * f + 8 * f * r + 80 * r + 16 * n + 8 * n * n * f;  // sin column, peaks,
+                                                                                   // waves, arc, sin(k|ds|) table
     b += (48 + 32) * pts * f * r + 8 * 1024 * f * r;      // pattern, fields, partials
     if (precision == FNEC_PRECISION_MIXED) {
         int64_t kb = (n + 31) / 32, rp = ((2 * n + 127) / 128) * 128;

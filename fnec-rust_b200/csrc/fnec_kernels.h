@@ -120,9 +120,11 @@ void launch_stamps(const DevStamp *stamps, int n, cx *z, cudaStream_t st);
 void launch_feedpoints(const UnitDesc *solves, int ns, const AntDesc *ants, const DevSeg *segs,
                        const int32_t *ibuf, const DevFeed *feeds, const cx *x, const int32_t *status,
                        double *feed_out, const int64_t *feed_row_off, cudaStream_t st);
+// groups (system, first solve, count <= 32): grouped kernels for many right-hand sides
 void launch_extra_rhs_exact(const UnitDesc *solves, int ns, int max_s, const AntDesc *ants, const int32_t *ibuf,
                             const cx *z, const cx *rhs, const double *cosv, const cx *A, const int32_t *piv,
-                            cx *x, const int32_t *status, cudaStream_t st);
+                            cx *x, const int32_t *status, cudaStream_t st, const int4 *groups = nullptr,
+                            int n_groups = 0);
 
 // fnec_farfield.cu
 int farfield_max_blocks(int n_int_max, int n_req_max);

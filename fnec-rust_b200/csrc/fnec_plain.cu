@@ -170,8 +170,10 @@ __global__ void k_hallen_rhs(const UnitDesc *__restrict__ solves, const AntDesc 
 // the segment itself (path form); the solve's x vector holds it until the
 // solve overwrites x.  Solve 0 of each system also writes cos(k s) and
 // sin(k s), times the sign, as the two homogeneous columns.
+// It also tabulates sin(k |s_m - s_p|) for the rows p of m's wire or path
+// (ascending), which no incidence direction changes, after the two columns.
 // k_planewave_rhs: rhs_m = sign_m (-j 2 pi / eta0) sum_p E_p sin(k |s_m -
-// s_p|) dl_p over the rows p of m's wire or path in ascending order.
+// s_p|) dl_p over those rows in ascending order, reading the table.
 // Every operation is the reference's, in its order; sign = 1 in the
 // per-wire form, where multiplying by it is exact.
 // ---------------------------------------------------------------------------
@@ -201,14 +203,22 @@ __global__ void k_planewave_field(const UnitDesc *__restrict__ solves, int ns, c
             cr_sincos(D_MUL(k, s), &ss, &sc);
             cos_buf[u.cos_off + p] = D_MUL(sgn, sc);
             cos_buf[u.cos_off + a.n + p] = D_MUL(sgn, ss);
+            const int32_t col = ibuf[a.rowwire_off + p];
+            const int32_t *wptr = ibuf + a.wptr_off, *wrow = ibuf + a.wrow_off;
+            double *kt = cos_buf + u.cos_off + 2 * (int64_t)a.n + ibuf[a.koff_off + p];
+            for (int q = wptr[col]; q < wptr[col + 1]; ++q) {
+                double ks, kc;
+                cr_sincos(D_MUL(k, fabs(D_SUB(s, dtab[a.arc_off + wrow[q]]))), &ks, &kc);
+                kt[q - wptr[col]] = ks;
+            }
         }
     }
 }
 
 __global__ void k_planewave_rhs(const UnitDesc *__restrict__ solves, int ns, const AntDesc *__restrict__ ants,
                                 const DevSeg *__restrict__ segs, const int32_t *__restrict__ ibuf,
-                                const double *__restrict__ dtab, const cx *__restrict__ xbuf, cx *rhs_buf,
-                                double scale) {
+                                const double *__restrict__ dtab, const double *__restrict__ cos_buf,
+                                const cx *__restrict__ xbuf, cx *rhs_buf, double scale) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     for (int si = blockIdx.y; si < ns; si += gridDim.y) {
         UnitDesc u = solves[si];
@@ -219,12 +229,11 @@ __global__ void k_planewave_rhs(const UnitDesc *__restrict__ solves, int ns, con
         const int32_t col = ibuf[a.rowwire_off + m];  // the wire's cos column
         const int32_t *wptr = ibuf + a.wptr_off, *wrow = ibuf + a.wrow_off;
         const cx *e = xbuf + u.x_off;
-        const double k = u.k_fill, sm = s_mid[m];
+        const double *kt = cos_buf + u.cos_off + 2 * (int64_t)a.n + ibuf[a.koff_off + m];
         cx acc = cx_make(0.0, 0.0);
         for (int q = wptr[col]; q < wptr[col + 1]; ++q) {
             const int p = wrow[q];
-            double ks, kc;
-            cr_sincos(D_MUL(k, fabs(D_SUB(sm, s_mid[p]))), &ks, &kc);
+            const double ks = kt[q - wptr[col]];
             const cx ep = e[p];
             const double len = sg[p].len;
             acc = cx_add(acc, cx_make(D_MUL(D_MUL(ep.re, ks), len), D_MUL(D_MUL(ep.im, ks), len)));
@@ -1034,6 +1043,208 @@ __global__ void k_extra_rhs_solve(const UnitDesc *__restrict__ solves, const cx 
 }
 
 // ---------------------------------------------------------------------------
+// Many right-hand sides on one factorisation (a receive sweep's incidence
+// directions), in groups of up to 32 solves of one system: group g =
+// (system, first solve, count).  k_extra_rhs_b_group forms M^H y of every
+// solve of the group with Z read once per group: thread i keeps the 32
+// accumulators of row i, each summed over r ascending exactly as
+// k_extra_rhs_b sums it.  k_extra_rhs_solve_group gives each solve one lane
+// (16 per block): its right-hand side lives in a shared [s][16] tile, the row swaps, the
+// forward elimination (b[r] -= f[r][c] b[c], c ascending) and the back
+// substitution (j ascending, then the division) are k_extra_rhs_solve's
+// operations in its order, with the factor read warp-uniformly.
+// ---------------------------------------------------------------------------
+constexpr int RG = 32;  // solves per group
+constexpr int SG = 16;  // solves per substitution block: a [s][16] tile, several blocks per SM
+
+__global__ void __launch_bounds__(64) k_extra_rhs_b_group(const UnitDesc *__restrict__ solves,
+                                                          const int4 *__restrict__ groups,
+                                                          const AntDesc *__restrict__ ants,
+                                                          const int32_t *__restrict__ ibuf,
+                                                          const cx *__restrict__ zbuf,
+                                                          const cx *__restrict__ rhs_buf,
+                                                          const double *__restrict__ cos_buf, cx *xbuf) {
+    __shared__ cx Y[RG][RG];  // [row in chunk][solve]
+    const int4 g = groups[blockIdx.y];
+    const UnitDesc u0 = solves[g.y];
+    const int n = u0.n, s = u0.s;
+    if ((int)(blockIdx.x * blockDim.x) >= s) return;  // the whole block: no barrier is skipped
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const cx *z = zbuf + u0.z_off;
+    cx acc[RG];
+#pragma unroll
+    for (int d = 0; d < RG; ++d) acc[d] = cx_make(0.0, 0.0);
+    for (int r0 = 0; r0 < n; r0 += RG) {
+        __syncthreads();
+        for (int t = threadIdx.x; t < RG * RG; t += blockDim.x) {
+            const int d = t / RG, rr = t % RG;
+            Y[rr][d] = (d < g.z && r0 + rr < n) ? rhs_buf[solves[g.y + d].rhs_off + r0 + rr] : cx_make(0.0, 0.0);
+        }
+        __syncthreads();
+        if (i < n) {
+            const int rmax = min(RG, n - r0);
+            for (int rr = 0; rr < rmax; ++rr) {
+                const cx zz = z[(int64_t)(r0 + rr) * n + i];
+#pragma unroll
+                for (int d = 0; d < RG; ++d) acc[d] = cx_add(acc[d], cx_conj_mul(zz, Y[rr][d]));
+            }
+        }
+    }
+    if (i < n) {
+#pragma unroll
+        for (int d = 0; d < RG; ++d)  // static indices keep acc in registers
+            if (d < g.z) xbuf[solves[g.y + d].x_off + i] = acc[d];
+    } else if (i < s) {  // a homogeneous column: its rows' -cos (or -sin) values
+        const AntDesc a = ants[u0.ant];
+        const int w = i - n;
+        const int32_t *wptr = ibuf + a.wptr_off, *wrow = ibuf + a.wrow_off;
+        const double *cv = cos_buf + u0.cos_off + ((a.hom2 && (w & 1)) ? n : 0);
+        for (int d = 0; d < g.z; ++d) {
+            const cx *y = rhs_buf + solves[g.y + d].rhs_off;
+            cx b = cx_make(0.0, 0.0);
+            for (int q = wptr[w]; q < wptr[w + 1]; ++q) {
+                const int r = wrow[q];
+                b = cx_add(b, cx_conj_mul(cx_make(-cv[r], 0.0), y[r]));
+            }
+            xbuf[solves[g.y + d].x_off + i] = b;
+        }
+    }
+}
+
+// The factor streams through the lanes in 16-wide row chunks, PD chunks
+// ahead of the arithmetic: lane k loads entry c0 + k of a chunk (one
+// coalesced access), and the chain receives the entries in column order
+// by shuffles.  Forward chunks: rows 1 .. s-1, columns 0 .. r-1; back
+// chunks: rows s-1 .. 0, columns i+1 .. s-1 (rows without any skipped).
+constexpr int PD = 8;
+struct FwdChunks {
+    int r, c0;
+    __device__ void next(int s) {
+        c0 += SG;
+        if (c0 >= r) {
+            ++r;
+            c0 = 0;
+        }
+        (void)s;
+    }
+    __device__ bool valid(int s) const { return r < s; }
+    __device__ int end(int s) const { return r; }
+};
+struct BackChunks {
+    int r, c0;
+    __device__ void norm(int s) {
+        while (r >= 0 && c0 >= s) {
+            --r;
+            c0 = r + 1;
+        }
+    }
+    __device__ void next(int s) {
+        c0 += SG;
+        norm(s);
+    }
+    __device__ bool valid(int s) const { return r >= 0; }
+    __device__ int end(int s) const { return s; }
+};
+
+template <typename Cur>
+__device__ __forceinline__ cx chunk_entry(const cx *A, int w1, int s, const Cur &pf, int l) {
+    const int c = pf.c0 + l;
+    return (pf.valid(s) && c < pf.end(s)) ? A[(int64_t)pf.r * w1 + c] : cx_make(0.0, 0.0);
+}
+
+__global__ void __launch_bounds__(SG) k_extra_rhs_solve_group(const UnitDesc *__restrict__ solves,
+                                                             const int4 *__restrict__ groups,
+                                                             const cx *__restrict__ abuf,
+                                                             const int32_t *__restrict__ piv_buf, cx *xbuf,
+                                                             const int32_t *__restrict__ status) {
+    extern __shared__ cx B[];  // [s][SG], then the diagonal [s], then the pivots (int32 [s])
+    const int4 g = groups[blockIdx.x];
+    const UnitDesc u0 = solves[g.y];
+    if (status[u0.sys] != 0 || (int)(blockIdx.y * SG) >= g.z) return;
+    const int s = u0.s, w1 = s + 1, d = blockIdx.y * SG + threadIdx.x, l = threadIdx.x;
+    const unsigned mask = (1u << SG) - 1u;
+    cx *diag = B + (size_t)s * SG;
+    int32_t *pv = reinterpret_cast<int32_t *>(diag + s);
+    const cx *A = abuf + u0.a_off;
+    const int32_t *piv = piv_buf + u0.piv_off;
+    for (int i = l; i < s; i += SG) {
+        diag[i] = A[(int64_t)i * w1 + i];
+        pv[i] = piv[i];
+    }
+    const bool live = d < g.z;
+    cx *x = xbuf + solves[g.y + (live ? d : 0)].x_off;
+    for (int j = 0; j < s; ++j) B[j * SG + l] = live ? x[j] : cx_make(0.0, 0.0);
+    __syncwarp(mask);
+    for (int c = 0; c < s; ++c) {
+        const int p = pv[c];
+        if (p != c) {
+            const cx t = B[c * SG + l];
+            B[c * SG + l] = B[p * SG + l];
+            B[p * SG + l] = t;
+        }
+    }
+    // forward elimination row by row: row r receives b[r] -= f[r][c] b[c]
+    // for c ascending -- the operations and order of the column sweep, as
+    // every b[c] with c < r is final when row r starts
+    {
+        FwdChunks pf{1, 0};
+        cx u[PD];
+#pragma unroll
+        for (int q = 0; q < PD; ++q) {
+            u[q] = chunk_entry(A, w1, s, pf, l);
+            if (pf.valid(s)) pf.next(s);
+        }
+        for (int r = 1; r < s; ++r) {
+            cx sum = B[r * SG + l];
+            for (int c0 = 0; c0 < r; c0 += SG) {
+                const cx uv = u[0];
+#pragma unroll
+                for (int q = 0; q < PD - 1; ++q) u[q] = u[q + 1];
+                u[PD - 1] = chunk_entry(A, w1, s, pf, l);
+                if (pf.valid(s)) pf.next(s);
+                const int cnt = min(SG, r - c0);
+#pragma unroll
+                for (int q = 0; q < SG; ++q) {
+                    const cx a = cx_make(__shfl_sync(mask, uv.re, q, SG), __shfl_sync(mask, uv.im, q, SG));
+                    if (q < cnt) sum = cx_sub(sum, cx_mul(a, B[(c0 + q) * SG + l]));
+                }
+            }
+            B[r * SG + l] = sum;
+        }
+    }
+    // back substitution: j ascending, then the division by the diagonal
+    {
+        BackChunks pf{s - 1, s};
+        pf.norm(s);
+        cx u[PD];
+#pragma unroll
+        for (int q = 0; q < PD; ++q) {
+            u[q] = chunk_entry(A, w1, s, pf, l);
+            if (pf.valid(s)) pf.next(s);
+        }
+        for (int i = s - 1; i >= 0; --i) {
+            cx sum = B[i * SG + l];
+            for (int j0 = i + 1; j0 < s; j0 += SG) {
+                const cx uv = u[0];
+#pragma unroll
+                for (int q = 0; q < PD - 1; ++q) u[q] = u[q + 1];
+                u[PD - 1] = chunk_entry(A, w1, s, pf, l);
+                if (pf.valid(s)) pf.next(s);
+                const int cnt = min(SG, s - j0);
+#pragma unroll
+                for (int q = 0; q < SG; ++q) {
+                    const cx a = cx_make(__shfl_sync(mask, uv.re, q, SG), __shfl_sync(mask, uv.im, q, SG));
+                    if (q < cnt) sum = cx_sub(sum, cx_mul(a, B[(j0 + q) * SG + l]));
+                }
+            }
+            B[i * SG + l] = cx_div(sum, diag[i]);
+        }
+    }
+    if (live)
+        for (int j = 0; j < s; ++j) x[j] = B[j * SG + l];
+}
+
+// ---------------------------------------------------------------------------
 // launch wrappers (host)
 // ---------------------------------------------------------------------------
 void launch_expand_segments(const DevWire *wires, int nw, DevSeg *segs, cudaStream_t st) {
@@ -1050,7 +1261,7 @@ void launch_planewave_rhs(const UnitDesc *solves, int ns, int max_n, const AntDe
     if (ns <= 0 || max_n <= 0) return;
     dim3 g((max_n + 127) / 128, ns < 65535 ? ns : 65535);
     k_planewave_field<<<g, 128, 0, st>>>(solves, ns, ants, segs, ibuf, dtab, x, cosv);
-    k_planewave_rhs<<<g, 128, 0, st>>>(solves, ns, ants, segs, ibuf, dtab, x, rhs, scale);
+    k_planewave_rhs<<<g, 128, 0, st>>>(solves, ns, ants, segs, ibuf, dtab, cosv, x, rhs, scale);
 }
 void launch_receive_peaks(const UnitDesc *solves, int ns, const AntDesc *ants, const cx *x, const int32_t *status,
                           double *peak, cudaStream_t st) {
@@ -1258,8 +1469,21 @@ void launch_feedpoints(const UnitDesc *solves, int ns, const AntDesc *ants, cons
 }
 void launch_extra_rhs_exact(const UnitDesc *solves, int ns, int max_s, const AntDesc *ants, const int32_t *ibuf,
                             const cx *z, const cx *rhs, const double *cosv, const cx *A, const int32_t *piv,
-                            cx *x, const int32_t *status, cudaStream_t st) {
+                            cx *x, const int32_t *status, cudaStream_t st, const int4 *groups, int n_groups) {
     if (ns <= 0) return;
+    if (groups && n_groups > 0) {
+        dim3 gb((max_s + 63) / 64, n_groups);
+        k_extra_rhs_b_group<<<gb, 64, 0, st>>>(solves, groups, ants, ibuf, z, rhs, cosv, x);
+        const size_t smem = (sizeof(cx) * (SG + 1) + sizeof(int32_t)) * (size_t)max_s;
+        int lim = smem <= BS_SMEM_MAX ? set_smem_limit_once(k_extra_rhs_solve_group, (int)BS_SMEM_MAX) : -1;
+        if (lim >= 0 && (size_t)lim >= smem) {
+            k_extra_rhs_solve_group<<<dim3(n_groups, RG / SG), SG, smem, st>>>(solves, groups, A, piv, x, status);
+            return;
+        }
+        // a factor too tall for the shared tile: one warp per solve on the b vectors formed above
+        k_extra_rhs_solve<<<ns, 32, 0, st>>>(solves, A, piv, x, status, 0);
+        return;
+    }
     dim3 g((max_s + 127) / 128, ns);
     k_extra_rhs_b<<<g, 128, 0, st>>>(solves, ants, ibuf, z, rhs, cosv, x);
     size_t smem = sizeof(cx) * (size_t)max_s;

@@ -84,6 +84,7 @@ struct AntDesc {
     int32_t hom2;
     int64_t arc_off;     // doubles: s_mid[n] (signed arc length), then sign[n]
     int64_t wave_off;    // doubles: 10 per right-hand side (r_hat, pol re, pol im, pad)
+    int64_t koff_off;    // int32[n]: row m's entry of the system's sin(k |s_m - s_p|) table
 };
 
 // One constraint row of M (linear.rs:744-762): M[N+q][c0] = 1 and, for a

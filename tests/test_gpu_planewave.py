@@ -94,15 +94,16 @@ def test_currents_bit_level_on_the_dipole(acc):
 
 def test_receive_sweep_matches_the_oracle(acc):
     """An EX card with I2 x I3 directions: every direction one right-hand
-    side of one factorisation per frequency; the response relative to the
-    largest peak of its frequency."""
-    card = acc.plane_wave(1, 10.0, 0.0, 0.0, n_theta=5, n_phi=3, d_theta=20.0, d_phi=45.0)
+    side of one factorisation per frequency (45 directions: the grouped
+    kernels, two groups per frequency, the second partial); the response
+    relative to the largest peak of its frequency."""
+    card = acc.plane_wave(1, 10.0, 0.0, 0.0, n_theta=5, n_phi=9, d_theta=20.0, d_phi=40.0)
     freqs = [F14, 16.0e6]
     b = acc.HallenBatch([_ant(acc, DIPOLE, freqs, card)])
     res = b.solve()
     assert np.all(res.status == 0)
     rec = b.read_receive()
-    waves = O.wave_directions(1, 5, 3, 10.0, 0.0, 20.0, 45.0)
+    waves = O.wave_directions(1, 5, 9, 10.0, 0.0, 20.0, 40.0)
     assert len(rec) == len(freqs) * len(waves)
     for fi, f in enumerate(freqs):
         peaks, db, cur = O.receive_sweep(O.wires_array(DIPOLE), f, waves)
@@ -166,3 +167,19 @@ def test_mixed_form_and_sources_are_refused(acc):
                       plane_wave=acc.plane_wave(1, 30.0))
     with pytest.raises(Exception, match="voltage sources"):
         acc.HallenBatch([ant])
+
+
+def test_grouped_right_hand_sides_equal_single_direction_solves(acc):
+    """The grouped many-right-hand-side kernels against the first-solve path
+    (the right-hand side carried through the Gram and the elimination):
+    the same directions, one antenna each, give the same currents to the
+    last bit."""
+    card = acc.plane_wave(2, 15.0, 10.0, 25.0, n_theta=4, n_phi=9, d_theta=25.0, d_phi=35.0, axial_ratio=0.3)
+    b = acc.HallenBatch([_ant(acc, MIXED, [F14], card)])
+    res = b.solve()
+    singles = [_ant(acc, MIXED, [F14], acc.plane_wave(2, 15.0 + it * 25.0, 10.0 + ip * 35.0, 25.0, axial_ratio=0.3))
+               for it in range(4) for ip in range(9)]
+    one = acc.HallenBatch(singles).solve()
+    for u in range(36):
+        assert np.array_equal(res.currents[u].view(np.uint64), one.currents[u].view(np.uint64)), u
+    b.close()
