@@ -1486,7 +1486,13 @@ static int antenna_from_cards(const fnec_antenna &A, HostAnt &h, std::string &wh
     if (st != FNEC_OK) return st;
     build_runs(h);
     h.rp.pts_off = -1;
-    if (A.rp) {
+    if (A.rp_points && A.n_rp_points > 0) {
+        if (A.rp) {
+            why = "rp and rp_points are exclusive";
+            return FNEC_ERR_BAD_ARG;
+        }
+        h.pts.assign(A.rp_points, A.rp_points + 2 * (size_t)A.n_rp_points);
+    } else if (A.rp) {
         h.rp.n_theta = (int32_t)std::max<uint32_t>(A.rp->n_theta, 1);
         h.rp.n_phi = (int32_t)std::max<uint32_t>(A.rp->n_phi, 1);
         h.rp.theta0 = A.rp->theta0;
@@ -2496,6 +2502,32 @@ int fnec_integrate_radiated_power(fnec_ctx *ctx, const fnec_gpu_segment *segment
                             pec_ground ? FNEC_GROUND_PEC : FNEC_GROUND_FREE, nullptr, 0, false, 0.0, pat, total);
     if (st != FNEC_OK) return st;
     *out = total;
+    return FNEC_OK;
+}
+
+int fnec_build_geometry(const fnec_wire *wires, uint32_t n_wires, fnec_zsegment *out, uint64_t cap,
+                        uint64_t *n_out) {
+    if (!n_out || (n_wires && !wires)) return FNEC_ERR_BAD_ARG;
+    uint64_t n = 0;
+    for (uint32_t w = 0; w < n_wires; ++w) {
+        const fnec_wire &gw = wires[w];
+        const double dx = gw.end[0] - gw.start[0], dy = gw.end[1] - gw.start[1], dz = gw.end[2] - gw.start[2];
+        if (gw.segments == 0 || std::sqrt(dx * dx + dy * dy + dz * dz) == 0.0) return FNEC_ERR_BAD_ARG;
+        n += gw.segments;
+    }
+    *n_out = n;
+    if (!out || cap < n) return FNEC_OK;
+    uint64_t q = 0;
+    for (uint32_t w = 0; w < n_wires; ++w)
+        for (uint32_t i = 0; i < wires[w].segments; ++i, ++q) {
+            const DevSeg d = host_seg(wires[w], i);
+            for (int c = 0; c < 3; ++c) {
+                out[q].midpoint[c] = d.mid[c];
+                out[q].direction[c] = d.dir[c];
+            }
+            out[q].length = d.len;
+            out[q].radius = d.rad;
+        }
     return FNEC_OK;
 }
 

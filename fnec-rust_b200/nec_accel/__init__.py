@@ -98,7 +98,14 @@ class _Antenna(ctypes.Structure):
     _fields_ = [("wires", _P), ("n_wires", _U32), ("sources", _P), ("n_sources", _U32), ("ground", _I32),
                 ("n_freqs", _U32), ("freqs_hz", _P), ("rp", _P), ("separate_sources", _U32), ("loads", _P),
                 ("n_loads", _U32), ("tls", _P), ("n_tls", _U32), ("nts", _P), ("n_nts", _U32),
-                ("plane_wave", _P)]
+                ("plane_wave", _P), ("rp_points", _P), ("n_rp_points", _U32)]
+
+
+class _DeckInfo(ctypes.Structure):
+    _fields_ = [("n_wires", _U32), ("n_sources", _U32), ("n_ex", _U32), ("n_loads", _U32), ("n_tls", _U32),
+                ("n_nts", _U32), ("n_freqs", _U32), ("n_rp_cards", _U32), ("n_points", _U32), ("n_ne_cards", _U32),
+                ("ground", _I32), ("plane_wave", _U32), ("warnings", _U32), ("runnable", _U32),
+                ("why", ctypes.c_char * 200)]
 
 
 class _UnitInfo(ctypes.Structure):
@@ -154,6 +161,12 @@ SIGNATURES = {
     "fnec_rp_farfield_batch": (ctypes.c_int, [_P, _P, _U64, _P, _D, _D, _P, _U64, _P]),
     "fnec_radiation_pattern": (ctypes.c_int, [_P, _P, _U64, _P, _D, _I32, _P, _U64, _P, _P]),
     "fnec_integrate_radiated_power": (ctypes.c_int, [_P, _P, _U64, _P, _D, _I32, _P]),
+    "fnec_build_geometry": (ctypes.c_int, [_P, _U32, _P, _U64, _P]),
+    "fnec_deck_parse": (ctypes.c_int, [ctypes.c_char_p, _P, ctypes.c_char_p, _U64]),
+    "fnec_deck_destroy": (ctypes.c_int, [_P]),
+    "fnec_deck_get_info": (ctypes.c_int, [_P, _P]),
+    "fnec_deck_get_antenna": (ctypes.c_int, [_P, _P, _P]),
+    "fnec_deck_solve": (ctypes.c_int, [_P, _P, _I32, _P, _P]),
     "fnec_near_field": (ctypes.c_int, [_P, _P, _U64, _P, _D, _P, _U64, _P, _P]),
     "fnec_microbench_zmatrix_dispatch": (ctypes.c_int, [ctypes.c_int, _U64, _U32, _P, _P, _P]),
     "fnec_enumerate_devices": (ctypes.c_int, [_P, ctypes.c_int, ctypes.c_char_p, _U64]),
@@ -323,6 +336,66 @@ def gpu_segments_from(segs) -> np.ndarray:
 # --------------------------------------------------------------------------
 # reference nec_accel entry points
 # --------------------------------------------------------------------------
+def build_geometry(wires) -> np.ndarray:
+    """build_geometry (geometry.rs:676-754) on the host: ZSEGMENT_DTYPE records
+    of the GW cards' segments in card order."""
+    w = np.ascontiguousarray(wires, dtype=WIRE_DTYPE)
+    n = ctypes.c_uint64(0)
+    st = lib().fnec_build_geometry(_ptr(w), len(w), None, 0, ctypes.byref(n))
+    if st != OK:
+        raise AccelError(st, "build_geometry: invalid GW card")
+    out = np.zeros(n.value, dtype=ZSEGMENT_DTYPE)
+    lib().fnec_build_geometry(_ptr(w), len(w), _ptr(out), n.value, ctypes.byref(n))
+    return out
+
+
+class Deck:
+    """A NEC deck read by the library (nec_parser::parse): its cards as one
+    antenna, and fnec_deck_solve's per-frequency report contract v1 text."""
+
+    def __init__(self, text: str):
+        h = ctypes.c_void_p()
+        err = ctypes.create_string_buffer(512)
+        st = lib().fnec_deck_parse(text.encode(), ctypes.byref(h), err, len(err))
+        if st != OK:
+            raise AccelError(st, f"deck_parse: {err.value.decode()}")
+        self._h = h
+
+    def info(self) -> dict:
+        i = _DeckInfo()
+        lib().fnec_deck_get_info(self._h, ctypes.byref(i))
+        d = {k: getattr(i, k) for k, _ in _DeckInfo._fields_}
+        d["why"] = i.why.decode()
+        return d
+
+    def antenna(self):
+        """(the C fnec_antenna view, the FR frequencies in Hz)."""
+        a = _Antenna()
+        n = self.info()["n_freqs"]
+        f = np.zeros(max(n, 1), np.float64)
+        lib().fnec_deck_get_antenna(self._h, ctypes.byref(a), _ptr(f))
+        return a, f[:n]
+
+    def solve(self, precision: int = PRECISION_FP64, ctx: Optional[Context] = None) -> str:
+        ctx = ctx or default_context()
+        p = ctypes.c_char_p()
+        n = ctypes.c_uint64(0)
+        ctx.check(lib().fnec_deck_solve(ctx.handle, self._h, int(precision), ctypes.byref(p), ctypes.byref(n)),
+                  "deck_solve")
+        return ctypes.string_at(p, n.value).decode()
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().fnec_deck_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def fill_zmatrix(segments, freq_hz: float, ground: int = GROUND_FREE, ctx: Optional[Context] = None):
     """fill_zmatrix_wgpu (wgpu_device.rs:832): the N x N Hallen matrix,
     complex128, row-major; FP64 and with the PEC image when ground == 1."""
@@ -631,7 +704,7 @@ def _antenna_struct(a, keep: list):
                     ctypes.cast(ctypes.pointer(rp), _P) if rp is not None else None,
                     int(bool(a.separate_sources)), _ptr(ld), 0 if ld is None else len(ld),
                     _ptr(tl), 0 if tl is None else len(tl), _ptr(nt), 0 if nt is None else len(nt),
-                    ctypes.cast(ctypes.pointer(pw), _P) if pw is not None else None)
+                    ctypes.cast(ctypes.pointer(pw), _P) if pw is not None else None, None, 0)
 
 
 class _Schedule(ctypes.Structure):

@@ -218,6 +218,11 @@ typedef struct {
      * other junctioned decks are FNEC_ERR_UNSUPPORTED, as the reference
      * rejects them.  n_sources must be 0; FP64 form only. */
     const fnec_plane_wave *plane_wave;
+    /* Several RP cards (main.rs:292-304 concatenates their grids): the
+     * (theta, phi) degree pairs of every requested direction, in the place of
+     * rp (which must then be NULL); the power integral is formed as for rp. */
+    const double *rp_points;
+    uint32_t n_rp_points;
 } fnec_antenna;
 
 /* Per-unit shape, for sizing result buffers.  A unit is one solve: one
@@ -307,6 +312,43 @@ int fnec_radiation_pattern(fnec_ctx *ctx, const fnec_gpu_segment *segments, uint
 int fnec_integrate_radiated_power(fnec_ctx *ctx, const fnec_gpu_segment *segments, uint64_t n,
                                   const double *currents, double freq_hz, int32_t pec_ground,
                                   double *out);
+
+/* ---- decks and reports ------------------------------------------------ *
+ * The deck reader (nec_parser::parse, crates/nec_parser/src/lib.rs:78-418)
+ * and the report contract v1 writer (nec_report::render_text_report,
+ * crates/nec_report/src/lib.rs:307-484) around the batch interface: a deck's
+ * text in, the CLI's text report for every FR frequency out. */
+typedef struct fnec_deck fnec_deck;
+typedef struct {
+    uint32_t n_wires, n_sources, n_ex, n_loads, n_tls, n_nts, n_freqs, n_rp_cards, n_points, n_ne_cards;
+    int32_t ground;      /* FNEC_GROUND_FREE / FNEC_GROUND_PEC as the deck's GN / GE cards select */
+    uint32_t plane_wave; /* the deck's first plane-wave EX card drives it */
+    uint32_t warnings;   /* unknown cards skipped by the parser */
+    uint32_t runnable;   /* 0: the device path does not build this deck (why says what) */
+    char why[200];       /* the reason, or the first parser warning */
+} fnec_deck_info;
+/* Parse a deck.  A bad or missing field is fatal (FNEC_ERR_BAD_ARG; err
+ * receives "line N: ..."); unknown cards are counted and skipped. */
+int fnec_deck_parse(const char *text, fnec_deck **out, char *err, uint64_t err_cap);
+int fnec_deck_destroy(fnec_deck *d);
+int fnec_deck_get_info(const fnec_deck *d, fnec_deck_info *out);
+/* The deck as one fnec_antenna (pointers into the deck, valid while it
+ * lives); freqs (optional, n_freqs doubles) receives the FR frequencies. */
+int fnec_deck_get_antenna(const fnec_deck *d, fnec_antenna *out, double *freqs);
+/* Solve every FR frequency in one batch and render the report of each
+ * (FEEDPOINTS, SOURCES, LOADS, CURRENTS with the last PT card's filter,
+ * RADIATION_PATTERN, RECEIVE_PATTERN, NEAR_FIELD, NEAR_H_FIELD,
+ * NORMALIZED_PATTERN, AVERAGE_POWER_GAIN), separated by blank lines as the
+ * CLI prints them.  *report is owned by the deck (until the next solve or
+ * destroy).  FNEC_ERR_UNSUPPORTED for decks the device path does not build,
+ * FNEC_ERR_SINGULAR when a solve fails. */
+int fnec_deck_solve(fnec_ctx *ctx, fnec_deck *d, int32_t precision, const char **report, uint64_t *len);
+
+/* build_geometry (geometry.rs:676-754): the segments of GW cards in card
+ * order, on the host, as the device expands them.  out may be NULL (count
+ * only); *n_out receives the segment count; cap < count writes nothing. */
+int fnec_build_geometry(const fnec_wire *wires, uint32_t n_wires, fnec_zsegment *out, uint64_t cap,
+                        uint64_t *n_out);
 
 /* near_e_field / near_h_field: the near electric and magnetic fields at p
  * points (3p doubles, metres) as the sum over the n segments of Hertzian

@@ -7,6 +7,9 @@ LD/TL/NT cards (no GM/GR transforms or plane waves) are kept:
 those are the cases that exercise exactly the hot path (geometry, Hallen
 RHS, Z fill, load stamps, normal-equation solve, feedpoint, RP pattern).
 
+It also writes tests/golden/corpus_decks.json: the text of every corpus deck,
+for the deck reader's tests.
+
 Run in a checkout that has the reference mounted:
     python tests/golden/make_golden.py /path/to/fnec-rust
 The GPU test host never runs this script; it only reads the JSON output.
@@ -118,8 +121,9 @@ def main(ref_root: str) -> None:
     for name in CASES:
         case = results[name]
         with open(os.path.join(corpus, case["deck_file"])) as fh:
-            deck = parse_deck(fh.read())
-        entry = {"deck_file": case["deck_file"], "deck": deck,
+            text = fh.read()
+        deck = parse_deck(text)
+        entry = {"deck_file": case["deck_file"], "deck": deck, "text": text,
                  "feedpoint_impedance": case.get("feedpoint_impedance", {}),
                  "tolerance_gates": case.get("tolerance_gates", {})}
         if "current_samples" in case:
@@ -131,6 +135,16 @@ def main(ref_root: str) -> None:
     with open(dst, "w") as fh:
         json.dump(out, fh, indent=1)
     print(f"wrote {dst} ({len(out['cases'])} cases)")
+    # every corpus deck's text, for the deck reader's tests
+    decks = {}
+    for fn in sorted(os.listdir(corpus)):
+        if fn.endswith(".nec"):
+            with open(os.path.join(corpus, fn)) as fh:
+                decks[fn[:-4]] = fh.read()
+    dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), "corpus_decks.json")
+    with open(dst, "w") as fh:
+        json.dump({"source": "dc0sk/fnec-rust corpus/*.nec", "decks": decks}, fh, indent=1)
+    print(f"wrote {dst} ({len(decks)} decks)")
 
 
 if __name__ == "__main__":
