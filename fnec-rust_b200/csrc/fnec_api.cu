@@ -694,6 +694,10 @@ struct fnec_batch {
     // solves: (system, first solve, count, 0)
     std::vector<int4> rhs_groups;
     int4 *d_rhs_groups = nullptr;
+    // a second stream for the first right-hand sides' back substitution,
+    // which runs beside the grouped kernels of the others
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     MixedWork mixed;
     GridPlan grid;
     // execution: the stream every operation of the batch is enqueued on;
@@ -772,6 +776,11 @@ static void free_batch(fnec_batch *b) {
     if (b->ev_made)
         for (auto &e : b->ev) cudaEventDestroy(e);
     b->ev_made = false;
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
+    if (b->side) cudaStreamDestroy(b->side);
+    b->ev_fork = b->ev_join = nullptr;
+    b->side = nullptr;
     free_mixed(b->mixed, DevAlloc{b->st, b->pooled});
 }
 
@@ -1693,14 +1702,30 @@ static int run_pipeline(fnec_batch *b) {
         mark(4);
         L += launch_factor_exact(b->d_units, nu, b->max_s, b->grid, b->d_a, b->d_piv, b->d_status, st);
         mark(5);
-        launch_backsub(b->d_units, nu, b->max_s, b->d_a, b->d_x, b->d_status, st);
+        // many right-hand sides per factorisation (receive sweeps): the grouped
+        // kernels, with the first right-hand sides' back substitution beside
+        // them on the side stream (they read the same factor, write other x)
+        const bool grouped = b->max_rhs >= 8;
+        bool forked = false;
+        if (grouped) {
+            if (!b->side && (cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+                             cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+                             cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess)) {
+                (void)cudaGetLastError();  // no side stream: both run on st
+            }
+            forked = b->side && b->ev_fork && b->ev_join && cudaEventRecord(b->ev_fork, st) == cudaSuccess &&
+                     cudaStreamWaitEvent(b->side, b->ev_fork, 0) == cudaSuccess;
+        }
+        launch_backsub(b->d_units, nu, b->max_s, b->d_a, b->d_x, b->d_status, forked ? b->side : st);
         if (b->max_rhs > 1) {
-            // many right-hand sides per factorisation (receive sweeps): the grouped kernels
-            const bool grouped = b->max_rhs >= 8;
             launch_extra_rhs_exact(b->d_solves, ns, b->max_s, b->d_ants, b->d_ibuf, b->d_z, b->d_rhs, b->d_cos,
                                    b->d_a, b->d_piv, b->d_x, b->d_status, st, grouped ? b->d_rhs_groups : nullptr,
                                    grouped ? (int)b->rhs_groups.size() : 0);
             L += 2;
+        }
+        if (forked) {
+            cudaEventRecord(b->ev_join, b->side);
+            cudaStreamWaitEvent(st, b->ev_join, 0);
         }
         mark(6);
         L += 3 + 1;  // Gram (3 kernels) and the back substitution

@@ -1244,6 +1244,107 @@ __global__ void __launch_bounds__(SG) k_extra_rhs_solve_group(const UnitDesc *__
         for (int j = 0; j < s; ++j) x[j] = B[j * SG + l];
 }
 
+// Four warps per group of 32 solves (lane = solve): the forward elimination
+// as the column sweep (every row r > c receives b[r] -= f[r][c] b[c] at step
+// c, rows spread over the warps, the factor staged PC columns at a time in
+// shared memory, a barrier per column), the back substitution with each
+// 32-column chunk's products formed by all warps and subtracted in ascending
+// j by warp 0.  Same operations in the same order per element as
+// k_extra_rhs_solve; used while [s][32] + the panel + one product chunk fit.
+constexpr int PC = 8;   // factor columns per staged panel
+constexpr int CH = 32;  // back-substitution product chunk
+constexpr int GW4 = 4;  // warps per block
+constexpr int RB = 3;   // row-buffer loads per thread: S <= 3 * 128
+
+size_t solve_group4_smem(int s) { return sizeof(cx) * ((size_t)s * (RG + PC + 2) + (size_t)CH * RG); }
+
+__global__ void __launch_bounds__(GW4 * 32) k_extra_rhs_solve_group4(const UnitDesc *__restrict__ solves,
+                                                                    const int4 *__restrict__ groups,
+                                                                    const cx *__restrict__ abuf,
+                                                                    const int32_t *__restrict__ piv_buf, cx *xbuf,
+                                                                    const int32_t *__restrict__ status) {
+    extern __shared__ cx sm[];
+    const int4 g = groups[blockIdx.x];
+    const UnitDesc u0 = solves[g.y];
+    if (status[u0.sys] != 0) return;  // uniform over the block
+    const int s = u0.s, w1 = s + 1;
+    const int d = threadIdx.x & 31, w = threadIdx.x >> 5;
+    cx *B = sm;                        // [s][RG]
+    cx *Ap = B + (size_t)s * RG;       // [s][PC]: rows of the staged columns
+    cx *P = Ap + (size_t)s * PC;       // [CH][RG]
+    const cx *A = abuf + u0.a_off;
+    const int32_t *piv = piv_buf + u0.piv_off;
+    const bool live = d < g.z;
+    cx *x = xbuf + solves[g.y + (live ? d : 0)].x_off;
+    for (int j = w; j < s; j += GW4) B[j * RG + d] = live ? x[j] : cx_make(0.0, 0.0);
+    __syncthreads();
+    if (w == 0)
+        for (int c = 0; c < s; ++c) {
+            const int p = piv[c];
+            if (p != c) {
+                const cx t = B[c * RG + d];
+                B[c * RG + d] = B[p * RG + d];
+                B[p * RG + d] = t;
+            }
+        }
+    // forward elimination, column by column
+    for (int c0 = 0; c0 < s; c0 += PC) {
+        const int pc_n = min(PC, s - c0);
+        __syncthreads();  // the previous panel is no longer read
+        for (int t = threadIdx.x; t < (s - c0 - 1) * PC; t += blockDim.x) {
+            const int r = c0 + 1 + t / PC, q = t % PC;
+            if (q < pc_n) Ap[r * PC + q] = A[(int64_t)r * w1 + c0 + q];
+        }
+        __syncthreads();
+        for (int q = 0; q < pc_n; ++q) {
+            const int c = c0 + q;
+            const cx bc = B[c * RG + d];
+            int r = c + 1;
+            r += (w - r % GW4 + GW4) % GW4;  // this warp's first row after c
+            for (; r < s; r += GW4) B[r * RG + d] = cx_sub(B[r * RG + d], cx_mul(Ap[r * PC + q], bc));
+            __syncthreads();
+        }
+    }
+    // back substitution; the factor rows pass through two shared row
+    // buffers, row i-1 loaded while row i is processed
+    cx *Ar = P + (size_t)CH * RG;  // [2][s]
+    for (int t = threadIdx.x; t < s; t += blockDim.x)
+        if (t >= s - 1) Ar[t] = A[(int64_t)(s - 1) * w1 + t];
+    __syncthreads();
+    cx sum = cx_make(0.0, 0.0);
+    int cur = 0;
+    for (int i = s - 1; i >= 0; --i) {
+        cx nxt[RB];
+#pragma unroll
+        for (int k = 0; k < RB; ++k) {
+            const int t = threadIdx.x + k * GW4 * 32;
+            nxt[k] = (i > 0 && t >= i - 1 && t < s) ? A[(int64_t)(i - 1) * w1 + t] : cx_make(0.0, 0.0);
+        }
+        const cx *ar = Ar + (size_t)cur * s;
+        if (w == 0) sum = B[i * RG + d];
+        for (int j0 = i + 1; j0 < s; j0 += CH) {
+            const int cnt = min(CH, s - j0);
+            __syncthreads();  // P is free; x[j] for j > i is final
+            for (int q = w; q < cnt; q += GW4) P[q * RG + d] = cx_mul(ar[j0 + q], B[(j0 + q) * RG + d]);
+            __syncthreads();
+            if (w == 0)
+                for (int q = 0; q < cnt; ++q) sum = cx_sub(sum, P[q * RG + d]);
+        }
+        if (w == 0) B[i * RG + d] = cx_div(sum, ar[i]);
+        // row i+1's buffer was last read before this row's barriers
+#pragma unroll
+        for (int k = 0; k < RB; ++k) {
+            const int t = threadIdx.x + k * GW4 * 32;
+            if (i > 0 && t >= i - 1 && t < s) Ar[(size_t)(cur ^ 1) * s + t] = nxt[k];
+        }
+        cur ^= 1;
+        if (i == s - 1) __syncthreads();  // row s-1 has no chunk barrier before row s-2 reads its buffer
+    }
+    __syncthreads();
+    if (live)
+        for (int j = w; j < s; j += GW4) x[j] = B[j * RG + d];
+}
+
 // ---------------------------------------------------------------------------
 // launch wrappers (host)
 // ---------------------------------------------------------------------------
@@ -1474,6 +1575,14 @@ void launch_extra_rhs_exact(const UnitDesc *solves, int ns, int max_s, const Ant
     if (groups && n_groups > 0) {
         dim3 gb((max_s + 63) / 64, n_groups);
         k_extra_rhs_b_group<<<gb, 64, 0, st>>>(solves, groups, ants, ibuf, z, rhs, cosv, x);
+        const size_t smem4 = solve_group4_smem(max_s);
+        int lim4 = (smem4 <= BS_SMEM_MAX && max_s <= RB * GW4 * 32)
+                       ? set_smem_limit_once(k_extra_rhs_solve_group4, (int)BS_SMEM_MAX)
+                       : -1;
+        if (lim4 >= 0 && (size_t)lim4 >= smem4) {
+            k_extra_rhs_solve_group4<<<n_groups, GW4 * 32, smem4, st>>>(solves, groups, A, piv, x, status);
+            return;
+        }
         const size_t smem = (sizeof(cx) * (SG + 1) + sizeof(int32_t)) * (size_t)max_s;
         int lim = smem <= BS_SMEM_MAX ? set_smem_limit_once(k_extra_rhs_solve_group, (int)BS_SMEM_MAX) : -1;
         if (lim >= 0 && (size_t)lim >= smem) {
