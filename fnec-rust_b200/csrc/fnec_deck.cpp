@@ -507,6 +507,20 @@ void ne_points(const NeCard &n, std::vector<double> &out) {
 
 extern "C" {
 
+uint32_t fnec_abi_struct_sizes(uint64_t *out, uint32_t cap) {
+    const uint64_t sz[] = {sizeof(fnec_wire),          sizeof(fnec_source),         sizeof(fnec_rp_card),
+                           sizeof(fnec_plane_wave),    sizeof(fnec_load),           sizeof(fnec_tl),
+                           sizeof(fnec_nt),            sizeof(fnec_antenna),        sizeof(fnec_unit_info),
+                           sizeof(fnec_batch_info),    sizeof(fnec_deck_info),      sizeof(fnec_server_config),
+                           sizeof(fnec_request_out),   sizeof(fnec_request_info),   sizeof(fnec_request_result),
+                           sizeof(fnec_server_stats_t), sizeof(fnec_schedule),      sizeof(fnec_tune_report),
+                           sizeof(fnec_zsegment),      sizeof(fnec_gpu_segment),    sizeof(fnec_rp_result),
+                           sizeof(fnec_junction)};
+    const uint32_t n = (uint32_t)(sizeof sz / sizeof sz[0]);
+    for (uint32_t i = 0; i < n && i < cap && out; ++i) out[i] = sz[i];
+    return n;
+}
+
 int fnec_deck_parse(const char *text, fnec_deck **out, char *err, uint64_t err_cap) {
     if (!text || !out) return FNEC_ERR_BAD_ARG;
     *out = nullptr;

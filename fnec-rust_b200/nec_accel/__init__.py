@@ -162,6 +162,7 @@ SIGNATURES = {
     "fnec_radiation_pattern": (ctypes.c_int, [_P, _P, _U64, _P, _D, _I32, _P, _U64, _P, _P]),
     "fnec_integrate_radiated_power": (ctypes.c_int, [_P, _P, _U64, _P, _D, _I32, _P]),
     "fnec_build_geometry": (ctypes.c_int, [_P, _U32, _P, _U64, _P]),
+    "fnec_abi_struct_sizes": (_U32, [_P, _U32]),
     "fnec_deck_parse": (ctypes.c_int, [ctypes.c_char_p, _P, ctypes.c_char_p, _U64]),
     "fnec_deck_destroy": (ctypes.c_int, [_P]),
     "fnec_deck_get_info": (ctypes.c_int, [_P, _P]),

@@ -344,6 +344,16 @@ int fnec_deck_get_antenna(const fnec_deck *d, fnec_antenna *out, double *freqs);
  * FNEC_ERR_SINGULAR when a solve fails. */
 int fnec_deck_solve(fnec_ctx *ctx, fnec_deck *d, int32_t precision, const char **report, uint64_t *len);
 
+/* sizeof of the public structs, in this order, for bindings to check their
+ * layouts against: fnec_wire, fnec_source, fnec_rp_card, fnec_plane_wave,
+ * fnec_load, fnec_tl, fnec_nt, fnec_antenna, fnec_unit_info,
+ * fnec_batch_info, fnec_deck_info, fnec_server_config, fnec_request_out,
+ * fnec_request_info, fnec_request_result, fnec_server_stats_t,
+ * fnec_schedule, fnec_tune_report, fnec_zsegment, fnec_gpu_segment,
+ * fnec_rp_result, fnec_junction.  Returns how many there are; writes at
+ * most cap. */
+uint32_t fnec_abi_struct_sizes(uint64_t *out, uint32_t cap);
+
 /* build_geometry (geometry.rs:676-754): the segments of GW cards in card
  * order, on the host, as the device expands them.  out may be NULL (count
  * only); *n_out receives the segment count; cap < count writes nothing. */

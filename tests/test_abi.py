@@ -87,3 +87,27 @@ def test_tune_cache_file_round_trip(tmp_path):
         acc.tune_cache_load(tmp_path / "absent.txt")
     acc.tune_cache_clear()
     assert acc.tune_cache_size() == 0
+
+
+def test_struct_layouts_match_the_library():
+    """Every public struct's size as compiled into the library equals its
+    mirror's (numpy dtypes for the card arrays, ctypes for the rest), so a
+    field added on one side only is caught without a GPU."""
+    import ctypes
+
+    import numpy as np
+
+    import nec_accel as acc
+
+    n = acc.lib().fnec_abi_struct_sizes(None, 0)
+    sizes = (ctypes.c_uint64 * n)()
+    acc.lib().fnec_abi_struct_sizes(sizes, n)
+    mirror = [acc.WIRE_DTYPE.itemsize, acc.SOURCE_DTYPE.itemsize, ctypes.sizeof(acc._RpCard),
+              ctypes.sizeof(acc._PlaneWave), acc.LOAD_DTYPE.itemsize, acc.TL_DTYPE.itemsize, acc.NT_DTYPE.itemsize,
+              ctypes.sizeof(acc._Antenna), ctypes.sizeof(acc._UnitInfo), ctypes.sizeof(acc._BatchInfo),
+              ctypes.sizeof(acc._DeckInfo), ctypes.sizeof(acc._ServerConfig), ctypes.sizeof(acc._RequestOut),
+              ctypes.sizeof(acc._RequestInfo), ctypes.sizeof(acc._RequestResult), ctypes.sizeof(acc._ServerStats),
+              ctypes.sizeof(acc._Schedule), ctypes.sizeof(acc._TuneReport), acc.ZSEGMENT_DTYPE.itemsize,
+              acc.GPU_SEGMENT_DTYPE.itemsize, acc.RP_RESULT_DTYPE.itemsize, acc.JUNCTION_DTYPE.itemsize]
+    assert list(sizes) == mirror
+    assert np.dtype(acc.WIRE_DTYPE).itemsize == 64
