@@ -13,7 +13,8 @@ feedpoint + pattern with its power integral).
             stream, max over ranks (weak scaling: every rank solves its own
             201-frequency sweep)
   e2e       the same through the C ABI with host buffers: pinned H2D of the
-            batch tables, the run, D2H of currents/feeds/pattern per step
+            batch tables, the run, D2H of what the report prints per step
+            (currents, feeds, the 4 pattern columns; fnec_batch_read_report)
   roofline  the dominant phase, FP64-pipe bound, against the FP64 peak this
             script measures on the same GPU
   cpu_baseline  the CPU oracle (C restatement of the reference CPU path),
@@ -825,7 +826,7 @@ def main():
         for _ in range(args.steps):
             batch.upload()
             batch.run()
-            batch.read_raw()  # synchronises: device -> pinned -> host arrays
+            batch.read_report()  # synchronises: the report's results, device -> page-locked host arrays
         e1.record(stream)
         batch.sync()
         barrier()
@@ -843,7 +844,7 @@ def main():
             dist.all_reduce(vals, op=dist.ReduceOp.MAX)
         total_ms, e2e_ms = vals.tolist()
         return {"step_ms": step_ms, "total_ms": total_ms, "e2e_ms": e2e_ms, "clocks": clocks,
-                "launches": int(launches), "h2d": batch.h2d_bytes, "d2h": batch.d2h_bytes(), "phase": phase,
+                "launches": int(launches), "h2d": batch.h2d_bytes, "d2h": batch.d2h_report_bytes(), "phase": phase,
                 "res": batch.read()}
 
     forms = {"mixed": ["mixed", "fp64"], "fp64": ["fp64"], "mixed-only": ["mixed"]}[args.precision]

@@ -2240,6 +2240,34 @@ int fnec_batch_read(fnec_batch *b, double *currents, double *feeds, double *patt
     return FNEC_OK;
 }
 
+}  // extern "C"
+
+// The report's pattern columns (gain_total, gain_theta, gain_phi, axial
+// ratio) of every point, packed from the 6-column rows into 4.
+__global__ void k_pack_report(const double *__restrict__ pat, int64_t n_points, double *__restrict__ out) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < 4 * n_points;
+         t += (int64_t)gridDim.x * blockDim.x)
+        out[t] = pat[PAT_STRIDE * (t / 4) + t % 4];
+}
+
+extern "C" {
+
+int fnec_batch_read_report(fnec_batch *b, double *currents, double *feeds, double *pattern4, int32_t *status) {
+    if (!b) return FNEC_ERR_BAD_ARG;
+    fnec_ctx *ctx = b->ctx;
+    cudaSetDevice(ctx->device);
+    cudaStream_t st = b->st;
+    const int64_t np = b->pat_el;
+    if (pattern4 && np > 0) {
+        if (!is_pinned(pattern4)) return fail(ctx, FNEC_ERR_BAD_ARG, "read_report: pattern4 must be page-locked");
+        // the far-field field buffer (4 doubles per point) is free after the run
+        const int blocks = (int)std::min<int64_t>((4 * np + 255) / 256, 148 * 16);
+        k_pack_report<<<blocks, 256, 0, st>>>(b->d_pat, np, b->d_fld);
+        CUDA_TRY(ctx, cudaMemcpyAsync(pattern4, b->d_fld, sizeof(double) * 4 * np, cudaMemcpyDeviceToHost, st));
+    }
+    return fnec_batch_read(b, currents, feeds, nullptr, status, nullptr);
+}
+
 int fnec_batch_read_receive(fnec_batch *b, double *out) {
     if (!b || !out) return FNEC_ERR_BAD_ARG;
     const size_t ns = b->solves.size();

@@ -202,6 +202,7 @@ SIGNATURES = {
     "fnec_batch_phase_ms": (ctypes.c_int, [_P, _P]),
     "fnec_batch_read_unit": (ctypes.c_int, [_P, _U32, _P, _P]),
     "fnec_batch_read_receive": (ctypes.c_int, [_P, _P]),
+    "fnec_batch_read_report": (ctypes.c_int, [_P, _P, _P, _P, _P]),
     "fnec_batch_read_z": (ctypes.c_int, [_P, _U32, _P]),
     "fnec_batch_read_refinement": (ctypes.c_int, [_P, _P, _P]),
     "fnec_batch_get_schedule": (ctypes.c_int, [_P, _P]),
@@ -780,6 +781,7 @@ class HallenBatch:
         self._cur = self._pinned((max(info.total_currents, 1),), np.complex128)
         self._feed = self._pinned((max(info.total_feeds, 1), 7), np.float64)
         self._pat = self._pinned((max(info.total_points, 1), 6), np.float64)
+        self._pat4 = self._pinned((max(info.total_points, 1), 4), np.float64)
         self._status = self._pinned((max(info.n_units, 1),), np.int32)
         self._total = self._pinned((max(info.n_units, 1),), np.float64)
 
@@ -843,6 +845,18 @@ class HallenBatch:
                                              _ptr(self._pat) if pattern else None, _ptr(self._status),
                                              _ptr(self._total)), "batch_read")
         return self._cur, self._feed, self._pat, self._status, self._total
+
+    def read_report(self):
+        """The report's results (fnec_batch_read_report): currents, feeds,
+        the 4 report columns of every pattern point, status; views of the
+        batch's page-locked buffers."""
+        self.ctx.check(lib().fnec_batch_read_report(self._h, _ptr(self._cur), _ptr(self._feed), _ptr(self._pat4),
+                                                    _ptr(self._status)), "batch_read_report")
+        return self._cur, self._feed, self._pat4, self._status
+
+    def d2h_report_bytes(self) -> int:
+        i = self.info
+        return int(4 * i.n_systems + 16 * i.total_currents + 56 * i.total_feeds + 32 * i.total_points)
 
     def d2h_bytes(self, currents=True, feeds=True, pattern=True) -> int:
         i = self.info

@@ -571,6 +571,12 @@ int fnec_batch_phase_ms(fnec_batch *b, double *ms);
 /* Per-unit solution vector x (currents then homogeneous constants), 2*s
  * doubles, and the pivot rows (s int32), for parity checks. */
 int fnec_batch_read_unit(fnec_batch *b, uint32_t unit, double *x, int32_t *pivots);
+/* The report's results only (what render_text_report prints): currents,
+ * feeds and status as fnec_batch_read; pattern4 receives 4 doubles per point
+ * (gain_total, gain_theta, gain_phi, axial_ratio), packed on the device, so
+ * the copy is two thirds of the 6-column rows.  pattern4 must be page-locked
+ * (fnec_host_alloc). */
+int fnec_batch_read_report(fnec_batch *b, double *currents, double *feeds, double *pattern4, int32_t *status);
 /* Receive pattern of plane-wave units (solve_session.rs:313-375
  * plane_wave_receive_sweep): 3 doubles per unit -- theta, phi (degrees)
  * and 20 log10(peak |I| / the largest peak of the unit's system) dB,

@@ -212,3 +212,23 @@ def test_tensor_core_trailing_keeps_the_refinement(acc, cells):
     for tt, (zm, it) in out.items():
         assert abs(zm - zp) <= 1e-6 * abs(zp), tt
     assert out[1][1] <= out[0][1] + 1
+
+
+def test_read_report_equals_the_full_read():
+    """fnec_batch_read_report: the packed 4 pattern columns, currents, feeds
+    and status are the full read's, bit for bit."""
+    import nec_accel as acc
+
+    nec = acc
+    wires = [(1, 21, (0, 0, -2.5), (0, 0, 2.5), 0.001), (2, 15, (1.0, 0, -2.0), (1.0, 0, 2.0), 0.001)]
+    ant = nec.Antenna(nec.wires_array(wires), nec.sources_array([(1, 11, 1.0)]), [14.2e6, 21.0e6], 0,
+                      (10, 7, 0.0, 0.0, 20.0, 60.0))
+    b = nec.HallenBatch([ant])
+    b.run()
+    b.sync()
+    cur, feed, pat, st, _ = [x.copy() for x in b.read_raw()]
+    cur4, feed4, pat4, st4 = [x.copy() for x in b.read_report()]
+    assert np.array_equal(pat4.view(np.uint64), np.ascontiguousarray(pat[:, :4]).view(np.uint64))
+    assert np.array_equal(cur4.view(np.uint64), cur.view(np.uint64))
+    assert np.array_equal(feed4.view(np.uint64), feed.view(np.uint64)) and np.array_equal(st4, st)
+    b.close()
