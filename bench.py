@@ -14,7 +14,8 @@ feedpoint + pattern with its power integral).
             201-frequency sweep)
   e2e       the same through the C ABI with host buffers: pinned H2D of the
             batch tables, the run, D2H of what the report prints per step
-            (currents, feeds, the 4 pattern columns; fnec_batch_read_report)
+            (currents, feeds, the 4 pattern columns; the columns stream out
+            behind the far field: fnec_batch_run_report + _read_report)
   roofline  the dominant phase, FP64-pipe bound, against the FP64 peak this
             script measures on the same GPU
   cpu_baseline  the CPU oracle (C restatement of the reference CPU path),
@@ -825,8 +826,8 @@ def main():
         e0.record(stream)
         for _ in range(args.steps):
             batch.upload()
-            batch.run()
-            batch.read_report()  # synchronises: the report's results, device -> page-locked host arrays
+            batch.run_report()  # the pattern columns stream out chunk by chunk behind the far field
+            batch.read_report(pattern=False)  # synchronises; currents, feeds, status
         e1.record(stream)
         batch.sync()
         barrier()

@@ -698,6 +698,12 @@ struct fnec_batch {
     // which runs beside the grouped kernels of the others
     cudaStream_t side = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // fnec_batch_run_report: the page-locked destination of the report's
+    // pattern columns, copied chunk by chunk behind the far field
+    double *sink = nullptr;
+    cudaStream_t copy_st = nullptr;
+    std::vector<cudaEvent_t> ev_chunk;
+    cudaEvent_t ev_copy = nullptr;
     MixedWork mixed;
     GridPlan grid;
     // execution: the stream every operation of the batch is enqueued on;
@@ -776,6 +782,12 @@ static void free_batch(fnec_batch *b) {
     if (b->ev_made)
         for (auto &e : b->ev) cudaEventDestroy(e);
     b->ev_made = false;
+    for (auto e : b->ev_chunk) cudaEventDestroy(e);
+    b->ev_chunk.clear();
+    if (b->ev_copy) cudaEventDestroy(b->ev_copy);
+    if (b->copy_st) cudaStreamDestroy(b->copy_st);
+    b->ev_copy = nullptr;
+    b->copy_st = nullptr;
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     if (b->ev_join) cudaEventDestroy(b->ev_join);
     if (b->side) cudaStreamDestroy(b->side);
@@ -1636,6 +1648,15 @@ int fnec_batch_upload(fnec_batch *b) {
 
 // Enqueue the pipeline's launches on the batch stream (eagerly, or into
 // the graph being captured on it).
+// The report's pattern columns (gain_total, gain_theta, gain_phi, axial
+// ratio) of every point, packed from the 6-column rows into 4.
+__global__ void k_pack_report(const double *__restrict__ pat, int64_t n_points, double *__restrict__ out) {
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < 4 * n_points;
+         t += (int64_t)gridDim.x * blockDim.x)
+        out[t] = pat[PAT_STRIDE * (t / 4) + t % 4];
+}
+
+
 static int run_pipeline(fnec_batch *b) {
     fnec_ctx *ctx = b->ctx;
     cudaStream_t st = b->st;
@@ -1741,9 +1762,51 @@ static int run_pipeline(fnec_batch *b) {
     check("feedpoints");
     mark(7);
     if (b->ff_blocks > 0) {
-        launch_farfield(b->d_solves, ns, b->d_ants, b->d_runs, b->d_rps, b->d_pts, b->d_ibuf, b->d_x, b->d_status, b->d_fld,
-                        b->d_partials, b->ff_blocks, b->ff_smem, b->d_pat, b->d_total, st);
-        L += 2;
+        // with a report sink the far field runs in chunks of solves, each
+        // chunk's report columns packed and copied on the copy stream while
+        // the next chunk computes (the kernels index solves, partials and
+        // totals by the launch's own solve index)
+        constexpr int K_CHUNKS = 8;
+        bool chunked = false;
+        if (b->sink) {
+            if (!b->copy_st) {
+                bool ok = cudaStreamCreateWithFlags(&b->copy_st, cudaStreamNonBlocking) == cudaSuccess &&
+                          cudaEventCreateWithFlags(&b->ev_copy, cudaEventDisableTiming) == cudaSuccess;
+                for (int k = 0; ok && k < K_CHUNKS; ++k) {
+                    cudaEvent_t e = nullptr;
+                    ok = cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
+                    if (ok) b->ev_chunk.push_back(e);
+                }
+                if (!ok) (void)cudaGetLastError();
+            }
+            chunked = b->copy_st && b->ev_copy && (int)b->ev_chunk.size() == K_CHUNKS;
+        }
+        const int k_n = chunked ? std::min(ns, K_CHUNKS) : 1, cs = (ns + k_n - 1) / k_n;
+        for (int s0 = 0, k = 0; s0 < ns; s0 += cs, ++k) {
+            const int s1 = std::min(ns, s0 + cs);
+            launch_farfield(b->d_solves + s0, s1 - s0, b->d_ants, b->d_runs, b->d_rps, b->d_pts, b->d_ibuf, b->d_x,
+                            b->d_status, b->d_fld, b->d_partials + (int64_t)s0 * b->ff_blocks, b->ff_blocks, b->ff_smem,
+                            b->d_pat, b->d_total + s0, st);
+            L += 2;
+            if (chunked) {
+                const int64_t p0 = (int64_t)b->uinfo[s0].pat_off;
+                const int64_t p1 = (int64_t)b->uinfo[s1 - 1].pat_off + b->uinfo[s1 - 1].n_points;
+                if (p1 > p0) {
+                    cudaEventRecord(b->ev_chunk[k], st);
+                    cudaStreamWaitEvent(b->copy_st, b->ev_chunk[k], 0);
+                    // the chunk's field scratch is dead after its gains: the packed rows go there
+                    k_pack_report<<<(int)std::min<int64_t>((4 * (p1 - p0) + 255) / 256, 148 * 16), 256, 0,
+                                    b->copy_st>>>(b->d_pat + PAT_STRIDE * p0, p1 - p0, b->d_fld + 4 * p0);
+                    cudaMemcpyAsync(b->sink + 4 * p0, b->d_fld + 4 * p0, sizeof(double) * 4 * (p1 - p0),
+                                    cudaMemcpyDeviceToHost, b->copy_st);
+                    ++L;
+                }
+            }
+        }
+        if (chunked) {
+            cudaEventRecord(b->ev_copy, b->copy_st);
+            cudaStreamWaitEvent(st, b->ev_copy, 0);
+        }
     }
     mark(8);
     check("far field");
@@ -2240,17 +2303,16 @@ int fnec_batch_read(fnec_batch *b, double *currents, double *feeds, double *patt
     return FNEC_OK;
 }
 
-}  // extern "C"
-
-// The report's pattern columns (gain_total, gain_theta, gain_phi, axial
-// ratio) of every point, packed from the 6-column rows into 4.
-__global__ void k_pack_report(const double *__restrict__ pat, int64_t n_points, double *__restrict__ out) {
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < 4 * n_points;
-         t += (int64_t)gridDim.x * blockDim.x)
-        out[t] = pat[PAT_STRIDE * (t / 4) + t % 4];
+int fnec_batch_run_report(fnec_batch *b, double *pattern4) {
+    if (!b || !pattern4) return FNEC_ERR_BAD_ARG;
+    if (!is_pinned(pattern4)) return fail(b->ctx, FNEC_ERR_BAD_ARG, "run_report: pattern4 must be page-locked");
+    cudaSetDevice(b->ctx->device);
+    b->sink = pattern4;
+    const int st = run_pipeline(b);  // eager: the sink's copies are not part of the batch's graph
+    b->sink = nullptr;
+    ++b->n_runs;
+    return st;
 }
-
-extern "C" {
 
 int fnec_batch_read_report(fnec_batch *b, double *currents, double *feeds, double *pattern4, int32_t *status) {
     if (!b) return FNEC_ERR_BAD_ARG;

@@ -203,6 +203,7 @@ SIGNATURES = {
     "fnec_batch_read_unit": (ctypes.c_int, [_P, _U32, _P, _P]),
     "fnec_batch_read_receive": (ctypes.c_int, [_P, _P]),
     "fnec_batch_read_report": (ctypes.c_int, [_P, _P, _P, _P, _P]),
+    "fnec_batch_run_report": (ctypes.c_int, [_P, _P]),
     "fnec_batch_read_z": (ctypes.c_int, [_P, _U32, _P]),
     "fnec_batch_read_refinement": (ctypes.c_int, [_P, _P, _P]),
     "fnec_batch_get_schedule": (ctypes.c_int, [_P, _P]),
@@ -846,13 +847,21 @@ class HallenBatch:
                                              _ptr(self._total)), "batch_read")
         return self._cur, self._feed, self._pat, self._status, self._total
 
-    def read_report(self):
+    def read_report(self, pattern: bool = True):
         """The report's results (fnec_batch_read_report): currents, feeds,
         the 4 report columns of every pattern point, status; views of the
-        batch's page-locked buffers."""
-        self.ctx.check(lib().fnec_batch_read_report(self._h, _ptr(self._cur), _ptr(self._feed), _ptr(self._pat4),
-                                                    _ptr(self._status)), "batch_read_report")
+        batch's page-locked buffers.  pattern=False after run_report, which
+        has streamed the columns already."""
+        self.ctx.check(lib().fnec_batch_read_report(self._h, _ptr(self._cur), _ptr(self._feed),
+                                                    _ptr(self._pat4) if pattern else None, _ptr(self._status)),
+                       "batch_read_report")
         return self._cur, self._feed, self._pat4, self._status
+
+    def run_report(self):
+        """fnec_batch_run_report: a run whose report pattern columns are
+        copied into the batch's page-locked buffer chunk by chunk behind the
+        far field; read_report(pattern=False) then completes the step."""
+        self.ctx.check(lib().fnec_batch_run_report(self._h, _ptr(self._pat4)), "batch_run_report")
 
     def d2h_report_bytes(self) -> int:
         i = self.info

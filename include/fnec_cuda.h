@@ -577,6 +577,13 @@ int fnec_batch_read_unit(fnec_batch *b, uint32_t unit, double *x, int32_t *pivot
  * the copy is two thirds of the 6-column rows.  pattern4 must be page-locked
  * (fnec_host_alloc). */
 int fnec_batch_read_report(fnec_batch *b, double *currents, double *feeds, double *pattern4, int32_t *status);
+/* Run the batch with the report's pattern columns streamed out: the far
+ * field runs in chunks of solves and each chunk's 4 columns are copied to
+ * pattern4 (page-locked, 4 doubles per point) while the next chunk
+ * computes.  Launched eagerly (not from the batch's graph).  Follow with
+ * fnec_batch_read_report(b, currents, feeds, NULL, status), which waits for
+ * the copies too. */
+int fnec_batch_run_report(fnec_batch *b, double *pattern4);
 /* Receive pattern of plane-wave units (solve_session.rs:313-375
  * plane_wave_receive_sweep): 3 doubles per unit -- theta, phi (degrees)
  * and 20 log10(peak |I| / the largest peak of the unit's system) dB,

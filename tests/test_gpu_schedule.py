@@ -231,4 +231,10 @@ def test_read_report_equals_the_full_read():
     assert np.array_equal(pat4.view(np.uint64), np.ascontiguousarray(pat[:, :4]).view(np.uint64))
     assert np.array_equal(cur4.view(np.uint64), cur.view(np.uint64))
     assert np.array_equal(feed4.view(np.uint64), feed.view(np.uint64)) and np.array_equal(st4, st)
+    # the streamed run: the same columns, copied chunk by chunk behind the far field
+    b._pat4[:] = 0.0
+    b.run_report()
+    cur5, feed5, pat5, st5 = [x.copy() for x in b.read_report(pattern=False)]
+    assert np.array_equal(pat5.view(np.uint64), pat4.view(np.uint64))
+    assert np.array_equal(cur5.view(np.uint64), cur.view(np.uint64)) and np.array_equal(st5, st)
     b.close()
