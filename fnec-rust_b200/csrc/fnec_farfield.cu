@@ -174,7 +174,7 @@ __device__ __forceinline__ void ff_store(double *fld_out, const UnitDesc &u, con
 // the requested points not already covered by an integration direction.
 // Requested fields go to fld_out (4 doubles per point); each block writes
 // one partial integral.
-__global__ void __launch_bounds__(FF_THREADS) k_farfield(
+__global__ void __launch_bounds__(FF_THREADS, 5) k_farfield(
     const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
     const DevRun *__restrict__ runs_all, const DevRp *__restrict__ rps, const double *__restrict__ pts,
     const int32_t *__restrict__ ibuf, const cx *__restrict__ xbuf, const int32_t *__restrict__ status,
