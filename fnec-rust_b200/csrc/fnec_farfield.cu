@@ -241,15 +241,17 @@ __global__ void __launch_bounds__(FF_THREADS, 5) k_farfield(
     }
 }
 
-// Per unit: total radiated power (fixed-order sum of block partials), then
-// gains in dBi and the Stokes axial ratio for each requested point.
+// Per unit (blockIdx.y): total radiated power (fixed-order sum of block
+// partials, formed by every block of the unit), then gains in dBi and the
+// Stokes axial ratio for the requested points of this block's slice
+// (blockIdx.x of gridDim.x).
 __global__ void k_gains(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
                         const DevRp *__restrict__ rps, const double *__restrict__ pts,
                         const int32_t *__restrict__ status,
                         const double *__restrict__ fld, const double *__restrict__ partials,
                         int max_blocks, double *pat_out, double *total_out) {
     __shared__ double s_total;
-    int ui = blockIdx.x;
+    int ui = blockIdx.y;
     UnitDesc u = units[ui];
     AntDesc a = ants[u.ant];
     DevRp rp = rps[u.ant];
@@ -264,12 +266,12 @@ __global__ void k_gains(const UnitDesc *__restrict__ units, const AntDesc *__res
         else
             for (int b = 0; b < nblocks; ++b) t += partials[(int64_t)ui * max_blocks + b];
         s_total = t;
-        total_out[ui] = status[u.sys] == 0 ? t : 0.0;
+        if (blockIdx.x == 0) total_out[ui] = status[u.sys] == 0 ? t : 0.0;
     }
     __syncthreads();
     double total = s_total;
     double norm = total > 0.0 ? 4.0 * 3.14159265358979323846 / total : 0.0;
-    for (int p = threadIdx.x; p < n_req; p += blockDim.x) {
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < n_req; p += gridDim.x * blockDim.x) {
         double *o = pat_out + PAT_STRIDE * (u.pat_off + p);
         double th_deg, ph_deg;
         req_point(rp, pts, p, th_deg, ph_deg);
@@ -320,8 +322,10 @@ void launch_farfield(const UnitDesc *units, int nu, const AntDesc *ants, const D
     dim3 g(max_blocks, nu);
     k_farfield<<<g, FF_THREADS, smem, st>>>(units, ants, runs, rps, pts, ibuf, x, status, fld, partials,
                                             max_blocks, staged);
-    k_gains<<<nu, 256, 0, st>>>(units, ants, rps, pts, status, fld, partials, max_blocks, pat_out,
-                                total_out);
+    // slices per unit: about one per 8 far-field blocks, at most 16
+    const int gx = max_blocks / 8 < 1 ? 1 : (max_blocks / 8 > 16 ? 16 : max_blocks / 8);
+    k_gains<<<dim3(gx, nu), 256, 0, st>>>(units, ants, rps, pts, status, fld, partials, max_blocks, pat_out,
+                                          total_out);
 }
 
 // ---------------------------------------------------------------------------
