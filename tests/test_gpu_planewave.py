@@ -183,3 +183,19 @@ def test_grouped_right_hand_sides_equal_single_direction_solves(acc):
     for u in range(36):
         assert np.array_equal(res.currents[u].view(np.uint64), one.currents[u].view(np.uint64)), u
     b.close()
+
+
+def test_grouped_right_hand_sides_on_a_tall_factor(acc):
+    """S = 393: beyond the four-warp kernel's shared tile, the grouped
+    directions take the 16-lane kernel; still the single-direction solves
+    to the last bit."""
+    wire = [(1, 391, (0, 0, -15.0), (0, 0, 15.0), 0.001)]
+    card = acc.plane_wave(1, 20.0, 0.0, 0.0, n_theta=9, d_theta=15.0)
+    b = acc.HallenBatch([_ant(acc, wire, [F14], card)])
+    res = b.solve()
+    assert b.units[0]["s"] == 393
+    one = acc.HallenBatch([_ant(acc, wire, [F14], acc.plane_wave(1, 20.0 + it * 15.0, 0.0, 0.0))
+                           for it in range(9)]).solve()
+    for u in range(9):
+        assert np.array_equal(res.currents[u].view(np.uint64), one.currents[u].view(np.uint64)), u
+    b.close()
