@@ -153,3 +153,15 @@ def test_restated_formats_match_the_reference_strings():
     assert R.rfix(-0.0, 6) == "-0.000000" and R.rfix(-1e-9, 6) == "-0.000000"
     assert R.rexp(1234.5, 6) == "1.234500e3" and R.rexp(-0.00123, 6) == "-1.230000e-3"
     assert R.rexp(0.0, 6) == "0.000000e0" and R.rfix(float("nan"), 4) == "NaN" and R.rexp(float("-inf"), 6) == "-inf"
+
+
+def test_restated_ne_points_are_the_oracle_points():
+    """The test-side NE/NH grid (which the library's deck path must equal,
+    tests/test_gpu_deck.py) against the oracle's near_field_grid_points."""
+    from oracle import oracle as O
+
+    for card in ((0, 3, 2, 4, -1.0, 0.5, 2.0, 0.7, 1.1, 0.25), (1, 2, 5, 3, 4.0, 10.0, 20.0, 1.5, 30.0, 25.0),
+                 (1, 0, 0, 0, 2.0, 0.0, 90.0, 0.0, 0.0, 0.0)):
+        want = O.near_field_points(*card)
+        got = np.array(R.ne_points(card))
+        assert got.shape == want.shape and np.array_equal(got, want), card

@@ -161,3 +161,25 @@ def test_unsupported_and_singular_decks_are_errors(acc):
     deck = acc.Deck("GW 1 11 0 0 -1 0 0 1 0.001\nGN 2\nEX 0 1 6 0 1\nFR 0 1 0 0 28 0\n")
     with pytest.raises(acc.AccelError):
         deck.solve()
+
+
+@pytest.mark.parametrize("name", ["dipole-ex1-freesp-51seg", "dipole-ex2-freesp-51seg", "dipole-ex3-freesp-51seg"])
+def test_corpus_plane_wave_decks_print_the_oracle_currents(acc, name):
+    """The corpus's receive decks end to end: the CURRENTS the report prints
+    (6 significant digits) are the oracle's receive solve of the deck's
+    first direction."""
+    from oracle import oracle as O
+
+    with open(os.path.join(HERE, "golden", "corpus_decks.json")) as f:
+        text = json.load(f)["decks"][name]
+    ref = R.parse(text)
+    rep = acc.Deck(text).solve()
+    e = [x for x in ref["ex"] if x[0] in (1, 2, 3)][0]
+    p = O.Problem(O.wires_array(ref["wires"]), O.sources_array([]), R.frequencies(ref)[0],
+                  wave=O.wave(e[0], e[4], e[5], e[6], e[9]))
+    O.solve_problem(p)
+    assert p.status == 0
+    rows = rep.split("CURRENTS\n")[1].split("\n\n")[0].splitlines()[1:]
+    got = np.array([complex(float(r.split()[2]), float(r.split()[3])) for r in rows])
+    peak = np.abs(p.currents).max()
+    assert len(got) == len(p.currents) and np.abs(got - p.currents).max() <= 1e-6 * peak
