@@ -483,6 +483,8 @@ def run_receive(args, acc, ctx, rank, local, dist):
     batch = acc.HallenBatch([ant], precision=acc.PRECISION_FP64, ctx=ctx)
     units = len(batch.units)
     stream = torch.cuda.ExternalStream(acc.lib().fnec_ctx_stream(ctx.handle), device=local)
+    # schedule: the autotuner's pick, timed before and outside the timed region
+    tune = None if args.no_tune else batch.tune(reps=args.tune_reps)
 
     def barrier():
         if dist is not None:
@@ -564,6 +566,8 @@ def run_receive(args, acc, ctx, rank, local, dist):
             "gpu_launches": int(launches), "roofline": roof, "phase_rooflines": rr,
             "phase_ms": {k: round(v, 4) for k, v in phase.items()}, "clocks": clocks,
             "receive_db_range": [float(np.min(rec[:, 2])), float(np.max(rec[:, 2]))],
+            "schedule": {"schedule": batch.schedule,
+                         "tune": None if tune is None else {k: tune[k] for k in ("candidates", "default_ms", "best_ms")}},
         }
         if not args.no_cpu_baseline:
             ref = receive_units(wires, freqs, card)
