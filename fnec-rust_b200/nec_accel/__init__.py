@@ -625,6 +625,7 @@ class Antenna:
     tls: Optional[np.ndarray] = None
     nts: Optional[np.ndarray] = None
     plane_wave: Optional[tuple] = None
+    rp_points: Optional[np.ndarray] = None  # (p, 2) theta, phi degrees: several RP cards' points (rp None)
 
 
 def plane_wave(ex_type=1, theta0=0.0, phi0=0.0, eta=0.0, n_theta=1, n_phi=1, d_theta=0.0, d_phi=0.0,
@@ -702,12 +703,14 @@ def _antenna_struct(a, keep: list):
     if a.plane_wave is not None:
         t, nth, nph, th0, ph0, eta, dth, dph, ar = a.plane_wave
         pw = _PlaneWave(t, nth, nph, 0, th0, ph0, eta, dth, dph, ar)
-    keep += [w, s, f, rp, ld, tl, nt, pw]
+    rpp = None if a.rp_points is None else np.ascontiguousarray(a.rp_points, np.float64).reshape(-1, 2)
+    keep += [w, s, f, rp, ld, tl, nt, pw, rpp]
     return _Antenna(_ptr(w), len(w), _ptr(s), len(s), int(a.ground), len(f), _ptr(f),
                     ctypes.cast(ctypes.pointer(rp), _P) if rp is not None else None,
                     int(bool(a.separate_sources)), _ptr(ld), 0 if ld is None else len(ld),
                     _ptr(tl), 0 if tl is None else len(tl), _ptr(nt), 0 if nt is None else len(nt),
-                    ctypes.cast(ctypes.pointer(pw), _P) if pw is not None else None, None, 0)
+                    ctypes.cast(ctypes.pointer(pw), _P) if pw is not None else None, _ptr(rpp),
+                    0 if rpp is None else len(rpp))
 
 
 class _Schedule(ctypes.Structure):

@@ -43,15 +43,16 @@ def _expected_report(acc, text):
         t, tag, seg, _, vr, vi, f3, f4, f5, f6 = pw[0]
         card = acc.plane_wave(t, vr, vi, f3, n_theta=max(tag, 1), n_phi=max(seg, 1), d_theta=f4, d_phi=f5,
                               axial_ratio=f6)
-    rp = None
-    if ref["rp"]:
-        assert len(ref["rp"]) == 1
+    rp, rp_points = None, None
+    if len(ref["rp"]) == 1:
         rp = tuple(ref["rp"][0][:6])
+    elif ref["rp"]:
+        rp_points = np.array(R.rp_points(ref))
     freqs = R.frequencies(ref)
     ant = acc.Antenna(acc.wires_array(ref["wires"]), acc.sources_array([(e[1], e[2], complex(e[4], e[5])) for e in ex_v]),
                       freqs, R.ground(ref), rp, loads=acc.loads_array(ref["ld"]) if ref["ld"] else None,
                       tls=acc.tls_array(ref["tl"]) if ref["tl"] else None,
-                      nts=acc.nts_array(R.nts(ref)) if R.nts(ref) else None, plane_wave=card)
+                      nts=acc.nts_array(R.nts(ref)) if R.nts(ref) else None, plane_wave=card, rp_points=rp_points)
     b = acc.HallenBatch([ant])
     res = b.solve()
     assert np.all(res.status == 0)
@@ -145,6 +146,17 @@ def test_synthetic_deck_with_every_section(acc):
     assert got.count("FNEC FEEDPOINT REPORT") == 2
     cur = got.split("CURRENTS\n")[1].split("\n\n")[0].splitlines()[1:]
     assert [tuple(map(int, c.split()[:2])) for c in cur] == [(1, s) for s in range(5, 10)]
+
+
+def test_several_rp_cards_concatenate_their_grids(acc):
+    """main.rs:292-304: two RP cards' points in card order, one pattern (the
+    explicit point list of fnec_antenna), normalised over both."""
+    text = ("GW 1 21 0 0 -2.5 0 0 2.5 0.001\nEX 0 1 11 0 1 0\nFR 0 1 0 0 28 0\n"
+            "RP 0 5 1 1000 0 0 45 0\nRP 0 3 4 10 90 30 45 0\nEN\n")
+    deck = acc.Deck(text)
+    got = deck.solve()
+    assert got == _expected_report(acc, text)
+    assert "RADIATION_PATTERN\nN_POINTS 17" in got and "NORMALIZED_PATTERN\nN_POINTS 17" in got
 
 
 def test_plane_wave_deck_reports_the_receive_pattern(acc):
