@@ -1,27 +1,35 @@
 """Benchmark of the Hallen MoM hot path on B200.
 
-Workload (one "step" = one pass of the hot path over one batch): the
-frequency sweep of a 5-element parallel-wire array in free space -- five
-z-parallel wires of 51 segments (N = 255, S = 260) with seeded lengths
-U(0.9, 1.1) * lambda/2 and gaps U(0.15, 0.25) * lambda at 14.2 MHz, radius
-1 mm, a 1 V source on the centre segment of element 2, 201 linear
-frequencies 13.0-15.5 MHz, and the 91 x 361 (1 degree) RP gain grid per
-frequency.  Each frequency is one solve (fill + normal equations + GEPP +
-feedpoint + pattern with its power integral).
+Headline workload (one "step" = one pass of the hot path over one batch):
+the uneven batch of 4096 random wire antennas -- 1-8 straight wires each
+(count uniform), endpoints uniform in a 20 m cube, 11-101 segments per wire
+(odd, uniform), radius log-uniform 0.5-5 mm, one 1 V source on the centre
+segment of wire 1, one frequency log-uniform 3-30 MHz, free space or GN 1
+with probability 1/2 -- filled, normal-equation formed, factored and solved
+in one captured pipeline, in both forms: the mixed form (3xTF32 Gram, FP32
+factor, FP64 GMRES refinement) and the plain FP64 form.
 
-  value     solves/s, inputs resident in HBM, CUDA events on the library's
-            stream, max over ranks (weak scaling: every rank solves its own
-            201-frequency sweep)
+  value     solves/s of the chosen (mixed) form, inputs resident in HBM,
+            CUDA events on the library's stream, max over ranks.  With N
+            GPUs the job is N x 4096 antennas split across the ranks by the
+            work model (nec_accel.shard), no collective on the data path
+            (weak scaling); the feedpoint rows are gathered on rank 0 after
+            the timed region.
   e2e       the same through the C ABI with host buffers: pinned H2D of the
             batch tables, the run, D2H of what the report prints per step
-            (currents, feeds, the 4 pattern columns; the columns stream out
-            behind the far field: fnec_batch_run_report + _read_report)
-  roofline  the dominant phase, FP64-pipe bound, against the FP64 peak this
-            script measures on the same GPU
+            (currents, feeds, status); e2e_with_planning also plans a new
+            batch (topology, junctions, packing, device allocation) every
+            step, as a call that brings new geometries must
+  roofline  the dominant phase of the chosen form against the measured peak
+            of the pipe that bounds it
   cpu_baseline  the CPU oracle (C restatement of the reference CPU path),
-            one solve per host thread, on a bounded sample of the sweep
+            one solve per host thread, on a bounded sample of the units;
+            the same sample checks both forms' Zin and currents
 
---impl reference times that CPU implementation alone on the same workload.
+The 5-wire frequency sweep (201 frequencies, 91 x 361 pattern each) is
+measured after the headline and reported under the key "sweep5".
+--workload selects another workload as the headline (sweep5, mesh, serve,
+receive).  --impl reference times the CPU implementation alone.
 """
 from __future__ import annotations
 
@@ -135,6 +143,11 @@ def uneven_workload(n_ant: int = 4096, seed: int = 7):
             continue
         out.append((wires, [(1, (wires[0][1] + 1) // 2, 1.0)], ground, f))
     return out
+
+
+def uneven_desc(n):
+    return (f"uneven: {n} random antennas of 1-8 wires, 11-101 segments per wire (N 11-808), "
+            f"one frequency each (3-30 MHz), free space / GN 1, no pattern")
 
 
 SERVE_RP = (91, 361, 0.0, 0.0, 1.0, 1.0)  # theta 0-90 x phi 0-360, 1 degree steps
@@ -303,7 +316,7 @@ def phase_rooflines(form, o, n, s, g, d, shapes, fma, muladd, ffma, peaks, runs)
     (mixed); factor (8/3) S^3 flops; solve: plain back substitution 8 S^2
     flops on a serial chain, mixed GMRES HBM bytes (iterations + 2) x
     (32 N^2 + 8 S^2) (FP64 Z read twice, FP32 factor once per apply); far
-    field 8 N flops per direction plus 2 sincos per (direction, wire run)."""
+    field 8 N flops per direction (its sincos per wire run is not counted)."""
     ph = o["phase"]
     exact = form == "fp64"
     samples = float(np.sum((8 * n * n - 4 * n) * (1 + g)))
@@ -342,7 +355,9 @@ def phase_rooflines(form, o, n, s, g, d, shapes, fma, muladd, ffma, peaks, runs)
         put("solve", byt / 1e9, peaks["hbm_gbs"], "GB/s", "hbm", peaks["source"])
     dd = np.asarray(d, np.float64)
     nr = np.asarray(runs, np.float64)
-    put("farfield", float(np.sum(dd * (8 * n + 2 * SINCOS_FLOPS * nr))) / 1e12, fma, "TFLOP/s", "fp64",
+    # 8 flops (one complex multiply-add) per (direction, segment); the
+    # per-(direction, wire run) sincos pairs are not counted as flops
+    put("farfield", float(np.sum(dd * 8 * n)) / 1e12, fma, "TFLOP/s", "fp64",
         "DFMA measured by fnec_measure_fp64_peak")
     return res
 
@@ -430,7 +445,7 @@ def reference_units(args):
         return ([(w, [s], g, f, rp) for w, srcs, g, f, rp in reqs for s in srcs],
                 "serve: random antennas, N lognormal (median 150), 1-4 source positions, half with 91x361 RP")
     wl = uneven_workload(args.antennas)
-    return [(w, src, g, f, None) for w, src, g, f in wl], f"uneven: {len(wl)} random antennas, one frequency each"
+    return [(w, src, g, f, None) for w, src, g, f in wl], uneven_desc(len(wl))
 
 
 def run_reference(args):
@@ -441,7 +456,7 @@ def run_reference(args):
         return
     ref_units, desc = reference_units(args)
     threads = os.cpu_count() or 1
-    n = min(len(ref_units), max(threads, 1))
+    n = min(len(ref_units), 2 * max(threads, 1))
     for _ in range(args.warmup):
         cpu_oracle_units(ref_units, min(n, 8), threads)
     times = []
@@ -721,10 +736,314 @@ def run_serve(args, acc, ctx, rank, local, dist):
     print(json.dumps(line), flush=True)
 
 
+def rank_workload(args, acc, world, rank):
+    """This rank's antennas of a batch workload.  The uneven batch is a job
+    of world x `antennas` random antennas split across ranks by the work
+    model (nec_accel.shard.partition_antennas: largest first onto the least
+    loaded rank); sweep5 and the mesh run as replicas (one sweep or one mesh
+    per rank).  Returns (antennas, reference units, job indices of this
+    rank's units, job size, description, data)."""
+    from nec_accel import shard
+
+    if args.workload == "sweep5":
+        wires, sources, freqs, rp = sweep_workload(n_freqs=args.freqs)
+        ants = [acc.Antenna(acc.wires_array(wires), acc.sources_array(sources), freqs, acc.GROUND_FREE, rp)]
+        desc = (f"sweep5: 5-wire parallel array, N=255 (S=260), {len(freqs)} freqs 13.0-15.5 MHz, "
+                f"RP 91x361 per freq")
+        ref = [(wires, sources, acc.GROUND_FREE, f, rp) for f in freqs]
+        return ants, ref, list(range(len(ref))), len(ref) * world, desc, \
+            "synthetic (seeded 5-element array, seed 11)", f"replicas x{world} (no collective)"
+    if args.workload == "mesh":
+        wl, src, f = mesh_workload(args.cells)
+        ants = [acc.Antenna(acc.wires_array(wl), acc.sources_array(src), [f], acc.GROUND_PEC, None)]
+        desc = (f"mesh: {args.cells}x{args.cells} cells of 2-segment wires over PEC ground (GN 1), N={2 * len(wl)}, "
+                f"W={len(wl)}, one frequency 14.2 MHz, no pattern")
+        return ants, [(wl, src, acc.GROUND_PEC, f, None)], [0], world, desc, \
+            "synthetic (seeded jittered mesh, seed 5)", f"replicas x{world} (one solve; no distributed LU)"
+    wl = uneven_workload(args.antennas * world)
+    all_ants = [acc.Antenna(acc.wires_array(w), acc.sources_array(src), [f], g, None) for w, src, g, f in wl]
+    parts = shard.partition_antennas(all_ants, world, mixed=args.precision != "fp64")
+    mine = parts[rank]
+    desc = uneven_desc(len(wl))
+    if world > 1:
+        desc += f"; {len(mine)} on this rank (work-balanced shard {rank}/{world})"
+    ref = [(wl[i][0], wl[i][1], wl[i][2], wl[i][3], None) for i in mine]
+    par = "1 GPU" if world == 1 else f"sharded x{world}: work-balanced partition of the antennas, no collective"
+    return [all_ants[i] for i in mine], ref, mine, len(wl), desc, "synthetic (seeded random antennas, seed 7)", par
+
+
+def current_err(a, b):
+    """Normwise relative difference of two current vectors (2-norm)."""
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def gain_err(pa, pb):
+    """Largest |difference| in dB of the three gain columns over the points
+    where the reference value is printed (above -999.99 dB)."""
+    g = pb[:, :3]
+    ok = g > -900
+    if not np.any(ok):
+        return 0.0
+    return float(np.max(np.abs(pa[:, :3][ok] - g[ok])))
+
+
+def measure_batch(args, acc, batch, stream, rank, local, dist, steps, warmup, with_clocks):
+    """Device-timed steps with inputs resident, then the same steps end to
+    end through the C ABI with host buffers, then per-phase times."""
+    import torch
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+
+    for _ in range(warmup):
+        batch.run()
+    batch.sync()
+    sampler = clock_sampler(local) if (rank == 0 and with_clocks) else None
+    barrier()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    evs[0].record(stream)
+    for k in range(steps):
+        batch.run()
+        evs[k + 1].record(stream)
+    batch.sync()
+    barrier()
+    step_ms = np.array([evs[k].elapsed_time(evs[k + 1]) for k in range(steps)])
+    clocks = clock_summary(sampler) if sampler is not None else None
+    launches = batch.kernel_launches * steps
+    # end to end through the C ABI with host buffers
+    batch.read_raw()
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        batch.upload()
+        batch.run_report()  # the pattern columns stream out chunk by chunk behind the far field
+        batch.read_report(pattern=False)  # synchronises; currents, feeds, status
+    e1.record(stream)
+    batch.sync()
+    barrier()
+    e2e_ms = e0.elapsed_time(e1)
+    # per-phase times (profiled runs, outside the timed regions)
+    batch.set_profiling(True)
+    phase = {k: 0.0 for k in batch.PHASES}
+    for _ in range(3):
+        batch.run()
+        for k, v in batch.phase_ms().items():
+            phase[k] += v / 3
+    batch.set_profiling(False)
+    vals = torch.tensor([float(step_ms.sum()), e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+    total_ms, e2e_ms = vals.tolist()
+    return {"step_ms": step_ms, "total_ms": total_ms, "e2e_ms": e2e_ms, "clocks": clocks,
+            "launches": int(launches), "h2d": batch.h2d_bytes, "d2h": batch.d2h_report_bytes(), "phase": phase,
+            "res": batch.read()}
+
+
+def measure_with_planning(acc, ants, prec, ctx, stream, local, dist, steps):
+    """End to end per call when every call brings new geometries: the C
+    ABI's batch planning (topology, junctions, constraint rows, packing,
+    device allocation), upload, run, the report's results to host memory and
+    the batch's release, timed by the host clock between device
+    synchronisations (max over ranks)."""
+    import torch
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(local)
+
+    b = acc.HallenBatch(ants, precision=prec, ctx=ctx)  # warm-up: caches, allocator
+    b.upload()
+    b.run()
+    b.read_report()
+    b.close()
+    barrier()
+    t0 = time.perf_counter()
+    plan = 0.0
+    for _ in range(steps):
+        p0 = time.perf_counter()
+        b = acc.HallenBatch(ants, precision=prec, ctx=ctx)
+        plan += time.perf_counter() - p0
+        b.upload()
+        b.run()
+        b.read_report()
+        b.close()
+    barrier()
+    ms = 1e3 * (time.perf_counter() - t0)
+    vals = torch.tensor([ms, 1e3 * plan], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+    return vals.tolist()
+
+
+def run_batch_workload(args, acc, ctx, rank, local, dist, world, steps, warmup, oracle_units=0,
+                       with_planning=False):
+    """Both forms of one batch workload; rank 0 returns the JSON line."""
+    import torch
+
+    ants, ref_units, job_index, job_units, desc, data, parallelism = rank_workload(args, acc, world, rank)
+    units_local = len(ref_units)
+    stream = torch.cuda.ExternalStream(acc.lib().fnec_ctx_stream(ctx.handle), device=local)
+    forms = {"mixed": ["mixed", "fp64"], "fp64": ["fp64"], "mixed-only": ["mixed"]}[args.precision]
+    out = {}
+    for form in forms:
+        prec = acc.PRECISION_MIXED if form == "mixed" else acc.PRECISION_FP64
+        batch = acc.HallenBatch(ants, precision=prec, ctx=ctx)
+        shapes = batch.units
+        # schedule: the autotuner's pick (timed before, outside the timed region)
+        tune = None if args.no_tune else batch.tune(reps=args.tune_reps)
+        out[form] = measure_batch(args, acc, batch, stream, rank, local, dist, steps, warmup,
+                                  with_clocks=(form == forms[0]))
+        st, nodes = batch.graph_state()
+        out[form]["schedule"] = {"schedule": batch.schedule,
+                                 "graph": {1: "replayed", 0: "eager", -1: "capture refused"}[st],
+                                 "graph_kernels": nodes}
+        if tune is not None:
+            out[form]["schedule"]["tune"] = {k: tune[k] for k in ("candidates", "default_ms", "best_ms", "key")}
+        if form == "mixed":
+            it, rs = batch.refinement_stats()
+            out[form]["gmres"] = {"iters_mean": float(it.mean()), "iters_max": int(it.max()),
+                                  "resid_max": float(rs.max())}
+            out[form]["gmres_iters"] = it.astype(np.float64)
+        batch.close()
+        if with_planning:
+            ms, plan_ms = measure_with_planning(acc, ants, prec, ctx, stream, local, dist, max(1, min(steps, 3)))
+            out[form]["planning"] = {"ms": ms / max(1, min(steps, 3)), "plan_ms": plan_ms / max(1, min(steps, 3)),
+                                     "steps": max(1, min(steps, 3))}
+
+    # results of this rank's units gathered on rank 0 in job order (feedpoint
+    # rows: 7 doubles per row)
+    gathered = None
+    if dist is not None and args.workload == "uneven":
+        from nec_accel import shard
+
+        got = shard.gather_units([f.copy() for f in out[forms[0]]["res"].feeds], job_index, job_units, dst=0)
+        if rank == 0:
+            gathered = {"units": len(got), "all_present": bool(all(g is not None for g in got))}
+    if rank != 0:
+        return None
+    fma_tf, muladd_tf = acc.measure_fp64_peak(local)
+    ffma_tf = acc.measure_fp32_peak(local)
+    peaks = measured_peaks()
+    n_u = np.array([u["n"] for u in shapes], np.float64)
+    s_u = np.array([u["s"] for u in shapes], np.float64)
+    g_u = np.array([ref_units[i][2] if i < len(ref_units) else 0 for i in range(len(shapes))], np.float64)
+    d_u = [ff_directions(ref_units[i][2], ref_units[i][4]) if u["n_points"] else 0 for i, u in enumerate(shapes)]
+    flops = algorithmic_flops(n_u, s_u, d_u)
+    w_u = [len(ref_units[i][0]) if i < len(ref_units) else 1 for i in range(len(shapes))]
+    rr = {form: phase_rooflines(form, out[form], n_u, s_u, g_u, d_u, shapes, fma_tf, muladd_tf, ffma_tf, peaks,
+                                w_u) for form in forms}
+    # accuracy of the chosen form against the plain FP64 GPU path (all units)
+    gate = None
+    if "mixed" in out and "fp64" in out:
+        rm, rp_ = out["mixed"]["res"], out["fp64"]["res"]
+        dz = max(abs(complex(*a[0, 5:7]) - complex(*b[0, 5:7])) / abs(complex(*b[0, 5:7]))
+                 for a, b in zip(rm.feeds, rp_.feeds))
+        di = max(current_err(a, b) for a, b in zip(rm.currents, rp_.currents))
+        gate = {"max_rel_dzin_mixed_vs_fp64_gpu": dz, "gate": 1e-6, "passed": bool(dz <= 1e-6),
+                "max_rel_current_mixed_vs_fp64_gpu": di, "units": len(rm.feeds)}
+        if any(len(p) for p in rm.pattern):
+            gate["max_abs_gain_db_mixed_vs_fp64_gpu"] = max(gain_err(a, b) for a, b in zip(rm.pattern, rp_.pattern)
+                                                            if len(b))
+    headline = forms[0] if (gate is None or gate["passed"]) else "fp64"
+    H = out[headline]
+    phase = H["phase"]
+    dom = max(("fill", "gram", "factor", "solve", "farfield"), key=lambda k: phase[k])
+    roof = dict(rr[headline][dom])
+    roof["kernel"] = dom
+    roof["traffic"], roof["traffic_source"] = dram_traffic(dom, headline, units_local)
+    samples = flops["fill_samples"]
+    per_step_units = job_units
+    line = {
+        "metric": METRIC,
+        "value": per_step_units * steps / (H["total_ms"] * 1e-3),
+        "unit": "solves/s",
+        "n_gpus": args.gpus,
+        "steps": steps,
+        "warmup": warmup,
+        "ms_per_step": H["total_ms"] / steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64" if headline == "fp64" else "f32+f64",
+        "data": data,
+        "config": {"workload": desc, "precision": headline, "units_per_step": per_step_units,
+                   "units_this_rank": units_local,
+                   "l2": "working set > 0.9 GB per step > 126 MB L2 (no flush needed)",
+                   "parallelism": parallelism},
+        "latency_ms": {"p50": float(np.percentile(H["step_ms"], 50)),
+                       "p99": float(np.percentile(H["step_ms"], 99)),
+                       "what": f"batch ({units_local}-solve step) latency"},
+        "e2e": {"value": per_step_units * steps / (H["e2e_ms"] * 1e-3), "unit": "solves/s",
+                "h2d_bytes_per_step": int(H["h2d"]), "d2h_bytes_per_step": int(H["d2h"])},
+        "gpu_launches": int(sum(o["launches"] for o in out.values())),
+        "roofline": roof,
+        "phase_ms": {k: round(v, 4) for k, v in phase.items()},
+        "phase_detail": {"fill_gsamples_per_s": samples / (phase["fill"] * 1e-3) / 1e9
+                         if phase["fill"] else None,
+                         "measured_peaks": {"fp64_dfma_tflops": fma_tf, "fp64_dmul_dadd_tflops": muladd_tf,
+                                            "fp32_ffma_tflops": ffma_tf, **peaks}},
+        "phase_rooflines": rr,
+        "clocks": out[forms[0]]["clocks"],
+    }
+    if gathered is not None:
+        line["gathered_on_rank0"] = gathered
+    for form in forms:
+        o = out[form]
+        line[f"form_{form}"] = {"value": per_step_units * steps / (o["total_ms"] * 1e-3),
+                                "ms_per_step": o["total_ms"] / steps,
+                                "e2e_value": per_step_units * steps / (o["e2e_ms"] * 1e-3),
+                                "phase_ms": {k: round(v, 4) for k, v in o["phase"].items()}}
+        if "gmres" in o:
+            line[f"form_{form}"]["gmres"] = o["gmres"]
+        if "planning" in o:
+            pl = o["planning"]
+            line[f"form_{form}"]["e2e_with_planning"] = {
+                "value": per_step_units / (pl["ms"] * 1e-3), "unit": "solves/s", "ms_per_step": pl["ms"],
+                "planning_ms_per_step": pl["plan_ms"], "steps": pl["steps"],
+                "what": "every step plans a new batch through the C ABI (topology, junctions, constraint rows, "
+                        "packing, device allocation), uploads, runs, reads the results and frees the batch; "
+                        "host clock between device synchronisations"}
+        line[f"form_{form}"]["schedule"] = o["schedule"]
+    if "planning" in H:
+        line["e2e_with_planning"] = line[f"form_{headline}"]["e2e_with_planning"]
+    if gate is not None:
+        line["mixed_gate"] = gate
+        line["mixed_vs_fp64"] = line["form_mixed"]["value"] / line["form_fp64"]["value"]
+        line["mixed_vs_fp64_e2e"] = line["form_mixed"]["e2e_value"] / line["form_fp64"]["e2e_value"]
+    if args.workload == "mesh" and args.cells > 12:
+        line["cpu_baseline"] = {"value": None, "unit": "solves/s", "cores": os.cpu_count() or 1, "kind": "port",
+                                "sample": "not run: the faithful single-threaded CPU solve of this mesh takes "
+                                          "hours (2.9e13 flops of naive Gram + 5.8e12 of GEPP)"}
+    elif oracle_units:
+        threads = os.cpu_count() or 1
+        n_units = min(units_local, oracle_units)
+        rate, dt, probs, idx = cpu_oracle_units(ref_units, n_units, threads)
+        line["cpu_baseline"] = {"value": rate, "unit": "solves/s", "cores": threads, "kind": "port",
+                                "sample": f"{n_units} evenly spaced units of the workload, one per thread, "
+                                          f"{dt:.1f} s wall"}
+        par = {"units_checked": n_units, "unit_index": [int(i) for i in idx]}
+        for form in forms:
+            rr_ = out[form]["res"]
+            par[f"max_rel_dzin_{form}_vs_oracle"] = float(max(
+                abs(complex(*rr_.feeds[i][0, 5:7]) - p.zin[0]) / abs(p.zin[0]) for p, i in zip(probs, idx)))
+            par[f"max_rel_current_{form}_vs_oracle"] = float(max(
+                current_err(rr_.currents[i], p.currents) for p, i in zip(probs, idx)))
+            if any(len(rr_.pattern[i]) for i in idx):
+                par[f"max_abs_gain_db_{form}_vs_oracle"] = float(max(
+                    gain_err(rr_.pattern[i], p.pattern) for p, i in zip(probs, idx) if len(rr_.pattern[i])))
+        line["parity"] = par
+    return line
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=60)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="mixed", choices=["fp64", "mixed", "mixed-only"],
@@ -732,10 +1051,14 @@ def main():
                          "mixed-only: the chosen form alone, no accuracy gate (for profiling)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--freqs", type=int, default=201, help="sweep points (201 = the workload; fewer = profiling)")
-    ap.add_argument("--workload", default="sweep5", choices=["sweep5", "uneven", "mesh", "serve", "receive"],
-                    help="sweep5: the 5-wire frequency sweep (headline); uneven: 4096 random antennas; "
-                         "mesh: the junctioned wire mesh over ground (one large solve); serve: a Poisson "
-                         "request stream through the continuous-batching server")
+    ap.add_argument("--workload", default="uneven", choices=["sweep5", "uneven", "mesh", "serve", "receive"],
+                    help="uneven: 4096 random antennas of uneven N in one batch (headline); sweep5: the 5-wire "
+                         "frequency sweep; mesh: the junctioned wire mesh over ground (one large solve); serve: "
+                         "a Poisson request stream through the continuous-batching server; receive: the "
+                         "plane-wave receive sweep")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="uneven: skip the extra sweep5 measurement reported under the key 'sweep5'")
+    ap.add_argument("--extra-steps", type=int, default=10, help="timed steps of the extra sweep5 measurement")
     ap.add_argument("--rates", default="100,1000,5000,20000", help="serve: offered request rates (req/s)")
     ap.add_argument("--serve-seconds", type=float, default=2.0, help="serve: arrival window per rate")
     ap.add_argument("--lanes", type=int, default=4, help="serve: concurrent batches")
@@ -743,7 +1066,7 @@ def main():
     ap.add_argument("--cells", type=int, default=46, help="mesh workload size (cells per side)")
     ap.add_argument("--n-theta", type=int, default=37, help="receive: incidence directions in theta")
     ap.add_argument("--n-phi", type=int, default=72, help="receive: incidence directions in phi")
-    ap.add_argument("--antennas", type=int, default=4096, help="uneven workload size")
+    ap.add_argument("--antennas", type=int, default=4096, help="uneven workload size (per GPU)")
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner (default schedule; the pipeline is still graph-captured)")
     ap.add_argument("--tune-reps", type=int, default=2, help="timed runs per candidate schedule")
@@ -770,200 +1093,27 @@ def main():
     ctx = acc.Context(local)
     if args.workload in ("serve", "receive"):
         (run_serve if args.workload == "serve" else run_receive)(args, acc, ctx, rank, local, dist)
-        ctx.close()
-        if dist is not None:
-            dist.barrier()
-            dist.destroy_process_group()
-        return
-    if args.workload == "sweep5":
-        wires, sources, freqs, rp = sweep_workload(n_freqs=args.freqs)
-        ants = [acc.Antenna(acc.wires_array(wires), acc.sources_array(sources), freqs, acc.GROUND_FREE, rp)]
-        desc = (f"sweep5: 5-wire parallel array, N=255 (S=260), {len(freqs)} freqs 13.0-15.5 MHz, "
-                f"RP 91x361 per freq")
-        ref_units = [(wires, sources, acc.GROUND_FREE, f, rp) for f in freqs]
-        data = "synthetic (seeded 5-element array, seed 11)"
-    elif args.workload == "mesh":
-        wl, src, f = mesh_workload(args.cells)
-        ants = [acc.Antenna(acc.wires_array(wl), acc.sources_array(src), [f], acc.GROUND_PEC, None)]
-        n_seg = 2 * len(wl)
-        desc = (f"mesh: {args.cells}x{args.cells} cells of 2-segment wires over PEC ground (GN 1), N={n_seg}, "
-                f"W={len(wl)}, one frequency 14.2 MHz, no pattern")
-        ref_units = [(wl, src, acc.GROUND_PEC, f, None)]
-        data = "synthetic (seeded jittered mesh, seed 5)"
     else:
-        wl = uneven_workload(args.antennas)
-        ants = [acc.Antenna(acc.wires_array(w), acc.sources_array(src), [f], g, None) for w, src, g, f in wl]
-        desc = (f"uneven: {len(wl)} random antennas of 1-8 wires, 11-101 segments per wire (N 11-808), "
-                f"one frequency each (3-30 MHz), free space / GN 1, no pattern")
-        ref_units = [(w, src, g, f, None) for w, src, g, f in wl]
-        data = "synthetic (seeded random antennas, seed 7)"
-    units = len(ref_units)
-    stream = torch.cuda.ExternalStream(acc.lib().fnec_ctx_stream(ctx.handle), device=local)
-
-    def barrier():
-        if dist is not None:
-            dist.barrier()
-        torch.cuda.synchronize(local)
-
-    def measure(batch, with_clocks):
-        # device-resident timing
-        for _ in range(args.warmup):
-            batch.run()
-        batch.sync()
-        sampler = clock_sampler(local) if (rank == 0 and with_clocks) else None
-        barrier()
-        evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
-        evs[0].record(stream)
-        for k in range(args.steps):
-            batch.run()
-            evs[k + 1].record(stream)
-        batch.sync()
-        barrier()
-        step_ms = np.array([evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)])
-        clocks = clock_summary(sampler) if sampler is not None else None
-        launches = batch.kernel_launches * args.steps
-        # end to end through the C ABI with host buffers
-        batch.read_raw()
-        barrier()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
-            batch.upload()
-            batch.run_report()  # the pattern columns stream out chunk by chunk behind the far field
-            batch.read_report(pattern=False)  # synchronises; currents, feeds, status
-        e1.record(stream)
-        batch.sync()
-        barrier()
-        e2e_ms = e0.elapsed_time(e1)
-        # per-phase times (profiled runs, outside the timed regions)
-        batch.set_profiling(True)
-        phase = {k: 0.0 for k in batch.PHASES}
-        for _ in range(3):
-            batch.run()
-            for k, v in batch.phase_ms().items():
-                phase[k] += v / 3
-        batch.set_profiling(False)
-        vals = torch.tensor([float(step_ms.sum()), e2e_ms], dtype=torch.float64, device=f"cuda:{local}")
-        if dist is not None:
-            dist.all_reduce(vals, op=dist.ReduceOp.MAX)
-        total_ms, e2e_ms = vals.tolist()
-        return {"step_ms": step_ms, "total_ms": total_ms, "e2e_ms": e2e_ms, "clocks": clocks,
-                "launches": int(launches), "h2d": batch.h2d_bytes, "d2h": batch.d2h_report_bytes(), "phase": phase,
-                "res": batch.read()}
-
-    forms = {"mixed": ["mixed", "fp64"], "fp64": ["fp64"], "mixed-only": ["mixed"]}[args.precision]
-    out = {}
-    for form in forms:
-        prec = acc.PRECISION_MIXED if form == "mixed" else acc.PRECISION_FP64
-        batch = acc.HallenBatch(ants, precision=prec, ctx=ctx)
-        shapes = batch.units
-        # schedule: the autotuner's pick (timed before, outside the timed region)
-        tune = None if args.no_tune else batch.tune(reps=args.tune_reps)
-        out[form] = measure(batch, with_clocks=(form == forms[0]))
-        st, nodes = batch.graph_state()
-        out[form]["schedule"] = {"schedule": batch.schedule,
-                                 "graph": {1: "replayed", 0: "eager", -1: "capture refused"}[st],
-                                 "graph_kernels": nodes}
-        if tune is not None:
-            out[form]["schedule"]["tune"] = {k: tune[k] for k in ("candidates", "default_ms", "best_ms", "key")}
-        if form == "mixed":
-            it, rs = batch.refinement_stats()
-            out[form]["gmres"] = {"iters_mean": float(it.mean()), "iters_max": int(it.max()),
-                                  "resid_max": float(rs.max())}
-            out[form]["gmres_iters"] = it.astype(np.float64)
-        batch.close()
-
-    if rank == 0:
-        fma_tf, muladd_tf = acc.measure_fp64_peak(local)
-        ffma_tf = acc.measure_fp32_peak(local)
-        peaks = measured_peaks()
-        n_u = np.array([u["n"] for u in shapes], np.float64)
-        s_u = np.array([u["s"] for u in shapes], np.float64)
-        g_u = np.array([ref_units[i][2] if i < len(ref_units) else 0 for i in range(len(shapes))], np.float64)
-        d_u = [ff_directions(ref_units[i][2], ref_units[i][4]) if u["n_points"] else 0 for i, u in enumerate(shapes)]
-        flops = algorithmic_flops(n_u, s_u, d_u)
-        w_u = [len(ref_units[i][0]) if i < len(ref_units) else 1 for i in range(len(shapes))]
-        rr = {form: phase_rooflines(form, out[form], n_u, s_u, g_u, d_u, shapes, fma_tf, muladd_tf, ffma_tf, peaks,
-                                    w_u) for form in forms}
-        head = out[forms[0]]
-        phase = head["phase"]
-        dom = max(("fill", "gram", "factor", "solve", "farfield"), key=lambda k: phase[k])
-        roof = dict(rr[forms[0]][dom])
-        roof["kernel"] = dom
-        roof["traffic"], roof["traffic_source"] = dram_traffic(dom, forms[0], units)
-        samples = flops["fill_samples"]
-        # accuracy of the chosen form against the plain FP64 GPU path (all units)
-        gate = None
-        if "mixed" in out and "fp64" in out:
-            fm, fp = out["mixed"]["res"].feeds, out["fp64"]["res"].feeds
-            dz = max(abs(complex(*a[0, 5:7]) - complex(*b[0, 5:7])) / abs(complex(*b[0, 5:7]))
-                     for a, b in zip(fm, fp))
-            gate = {"max_rel_dzin_mixed_vs_fp64_gpu": dz, "gate": 1e-6, "passed": bool(dz <= 1e-6)}
-        headline = forms[0] if (gate is None or gate["passed"]) else "fp64"
-        H = out[headline]
-        line = {
-            "metric": METRIC,
-            "value": args.gpus * units * args.steps / (H["total_ms"] * 1e-3),
-            "unit": "solves/s",
-            "n_gpus": args.gpus,
-            "steps": args.steps,
-            "warmup": args.warmup,
-            "ms_per_step": H["total_ms"] / args.steps,
-            "higher_is_better": True,
-            "scaling": "weak",
-            "vs_baseline": None,
-            "dtype": "f64" if headline == "fp64" else "f32+f64",
-            "data": data,
-            "config": {"workload": desc, "precision": headline, "units_per_step": units,
-                       "l2": "working set > 0.9 GB per step > 126 MB L2 (no flush needed)",
-                       "parallelism": f"replicas x{args.gpus} (no collective)"},
-            "latency_ms": {"p50": float(np.percentile(H["step_ms"], 50)),
-                           "p99": float(np.percentile(H["step_ms"], 99)),
-                           "what": f"batch ({units}-solve step) latency"},
-            "e2e": {"value": args.gpus * units * args.steps / (H["e2e_ms"] * 1e-3), "unit": "solves/s",
-                    "h2d_bytes_per_step": int(H["h2d"]), "d2h_bytes_per_step": int(H["d2h"])},
-            "gpu_launches": int(sum(o["launches"] for o in out.values())),
-            "roofline": roof,
-            "phase_ms": {k: round(v, 4) for k, v in phase.items()},
-            "phase_detail": {"fill_gsamples_per_s": samples / (phase["fill"] * 1e-3) / 1e9
-                             if phase["fill"] else None,
-                             "measured_peaks": {"fp64_dfma_tflops": fma_tf, "fp64_dmul_dadd_tflops": muladd_tf,
-                                                "fp32_ffma_tflops": ffma_tf, **peaks}},
-            "phase_rooflines": rr,
-            "clocks": head["clocks"],
-        }
-        for form in forms:
-            o = out[form]
-            line[f"form_{form}"] = {"value": args.gpus * units * args.steps / (o["total_ms"] * 1e-3),
-                                    "ms_per_step": o["total_ms"] / args.steps,
-                                    "e2e_value": args.gpus * units * args.steps / (o["e2e_ms"] * 1e-3),
-                                    "phase_ms": {k: round(v, 4) for k, v in o["phase"].items()}}
-            if "gmres" in o:
-                line[f"form_{form}"]["gmres"] = o["gmres"]
-            line[f"form_{form}"]["schedule"] = o["schedule"]
-        if gate is not None:
-            line["mixed_gate"] = gate
-            line["mixed_vs_fp64"] = line["form_mixed"]["value"] / line["form_fp64"]["value"]
-        res = H["res"]
-        if args.workload == "mesh" and args.cells > 12:
-            line["cpu_baseline"] = {"value": None, "unit": "solves/s", "cores": os.cpu_count() or 1, "kind": "port",
-                                    "sample": "not run: the faithful single-threaded CPU solve of this mesh takes "
-                                              "hours (2.9e13 flops of naive Gram + 5.8e12 of GEPP)"}
-        elif not args.no_cpu_baseline:
-            threads = os.cpu_count() or 1
-            n_units = min(units, max(threads, 4))
-            rate, dt, probs, idx = cpu_oracle_units(ref_units, n_units, threads)
-            line["cpu_baseline"] = {"value": rate, "unit": "solves/s", "cores": threads, "kind": "port",
-                                    "sample": f"{n_units} evenly spaced units of the workload, one per thread, "
-                                              f"{dt:.1f} s wall"}
-            par = {"units_checked": n_units}
-            for form in forms:
-                rr = out[form]["res"]
-                dz = [abs(complex(*rr.feeds[i][0, 5:7]) - p.zin[0]) / abs(p.zin[0]) for p, i in zip(probs, idx)]
-                par[f"max_rel_dzin_{form}_vs_oracle"] = float(max(dz))
-            line["parity"] = par
-        print(json.dumps(line), flush=True)
+        threads = os.cpu_count() or 1
+        line = run_batch_workload(args, acc, ctx, rank, local, dist, world, args.steps, args.warmup,
+                                  oracle_units=0 if args.no_cpu_baseline else max(threads, 4),
+                                  with_planning=args.workload == "uneven")
+        if args.workload == "uneven" and not args.no_extra:
+            # the 5-wire sweep (201 frequencies, 91 x 361 pattern each), kept
+            # beside the headline: its far field is the dominant kernel there;
+            # the oracle checks 4 of its frequencies (Zin, currents, gains)
+            sub = argparse.Namespace(**vars(args))
+            sub.workload, sub.freqs = "sweep5", 201
+            extra = run_batch_workload(sub, acc, ctx, rank, local, dist, world, args.extra_steps,
+                                       max(3, args.warmup), oracle_units=0 if args.no_cpu_baseline else 4)
+            if rank == 0:
+                keep = ("value", "ms_per_step", "e2e", "roofline", "phase_ms", "mixed_gate", "mixed_vs_fp64",
+                        "mixed_vs_fp64_e2e", "parity", "form_mixed", "form_fp64", "config", "steps", "warmup",
+                        "gpu_launches")
+                line["sweep5"] = {k: extra[k] for k in keep if k in extra}
+                line["gpu_launches"] += extra["gpu_launches"]
+        if rank == 0:
+            print(json.dumps(line), flush=True)
     ctx.close()
     if dist is not None:
         dist.barrier()
