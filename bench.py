@@ -316,7 +316,9 @@ def phase_rooflines(form, o, n, s, g, d, shapes, fma, muladd, ffma, peaks, runs)
     (mixed); factor (8/3) S^3 flops; solve: plain back substitution 8 S^2
     flops on a serial chain, mixed GMRES HBM bytes (iterations + 2) x
     (32 N^2 + 8 S^2) (FP64 Z read twice, FP32 factor once per apply); far
-    field 8 N flops per direction (its sincos per wire run is not counted)."""
+    field 8 N flops per direction (its sincos per wire run is not counted);
+    antennas of z-parallel wires: 8 flops per (block row, segment) plus 8
+    per (direction, run), the per-row path of the kernel."""
     ph = o["phase"]
     exact = form == "fp64"
     samples = float(np.sum((8 * n * n - 4 * n) * (1 + g)))
@@ -357,7 +359,16 @@ def phase_rooflines(form, o, n, s, g, d, shapes, fma, muladd, ffma, peaks, runs)
     nr = np.asarray(runs, np.float64)
     # 8 flops (one complex multiply-add) per (direction, segment); the
     # per-(direction, wire run) sincos pairs are not counted as flops
-    put("farfield", float(np.sum(dd * 8 * n)) / 1e12, fma, "TFLOP/s", "fp64",
+    # antennas whose wires all run along z (runs[i] < 0 marks them, -runs[i]
+    # wire runs) evaluate each run's Horner polynomial once per (block,
+    # integration row): 8 flops per (row, segment), plus one complex
+    # multiply-add per (direction, run) -- the far-field kernel's work for them
+    vert = nr < 0
+    nrun = np.abs(nr)
+    pec = np.asarray(g, np.float64) > 0
+    blocks = np.ceil(dd / 256.0)
+    ff = np.where(vert, blocks * 2 * (1 + pec) * 8 * n + dd * (1 + pec) * 8 * nrun, dd * 8 * n)
+    put("farfield", float(np.sum(ff)) / 1e12, fma, "TFLOP/s", "fp64",
         "DFMA measured by fnec_measure_fp64_peak")
     return res
 
@@ -934,7 +945,15 @@ def run_batch_workload(args, acc, ctx, rank, local, dist, world, steps, warmup, 
     g_u = np.array([ref_units[i][2] if i < len(ref_units) else 0 for i in range(len(shapes))], np.float64)
     d_u = [ff_directions(ref_units[i][2], ref_units[i][4]) if u["n_points"] else 0 for i, u in enumerate(shapes)]
     flops = algorithmic_flops(n_u, s_u, d_u)
-    w_u = [len(ref_units[i][0]) if i < len(ref_units) else 1 for i in range(len(shapes))]
+    def wire_runs(u):
+        # -W for antennas whose wires all run along z (the far field's per-row path), else W
+        wl = ref_units[u][0] if u < len(ref_units) else []
+        if not wl:
+            return 1
+        z_par = all(w[2][0] == w[3][0] and w[2][1] == w[3][1] for w in wl)
+        return -len(wl) if z_par else len(wl)
+
+    w_u = [wire_runs(i) for i in range(len(shapes))]
     rr = {form: phase_rooflines(form, out[form], n_u, s_u, g_u, d_u, shapes, fma_tf, muladd_tf, ffma_tf, peaks,
                                 w_u) for form in forms}
     # accuracy of the chosen form against the plain FP64 GPU path (all units)

@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -61,6 +62,15 @@ static int fail(fnec_ctx *c, int code, const std::string &msg) {
 // ---------------------------------------------------------------------------
 // host restatements needed for topology (same arithmetic as k_expand_segments)
 // ---------------------------------------------------------------------------
+// The analytic part of the self term, 2 ln((h + sqrt(h^2 + a^2)) / a) with
+// h = len / 2 (matrix.rs:297-331), in the reference's operation order and
+// with the host libm's ln -- the library the reference's f64::ln calls.
+static double self_log_term(double len, double rad) {
+    double half = len * 0.5;
+    double r_end = std::sqrt(half * half + rad * rad);
+    return 2.0 * std::log((half + r_end) / rad);
+}
+
 static DevSeg host_seg(const fnec_wire &gw, uint32_t i) {
     double dx = gw.end[0] - gw.start[0], dy = gw.end[1] - gw.start[1], dz = gw.end[2] - gw.start[2];
     double wl = std::sqrt(dx * dx + dy * dy + dz * dz);
@@ -83,7 +93,7 @@ static DevSeg host_seg(const fnec_wire &gw, uint32_t i) {
     s.rad = gw.radius;
     s.tag = gw.tag;
     s.tag_index = i + 1;
-    s.pad = 0.0;
+    s.self_log = self_log_term(s.len, s.rad);
     return s;
 }
 
@@ -740,10 +750,23 @@ struct fnec_batch {
     std::string graph_why;        // why capture was refused
 };
 
+// Test hook for the allocation-failure path (fnec_test_fail_device_allocation):
+// the n-th batch device allocation from now on fails as if the device were
+// out of memory (once); -1 = off.
+static std::atomic<int> g_fail_alloc_after{-1};
+static bool take_injected_alloc_failure() {
+    int v = g_fail_alloc_after.load();
+    while (v >= 0) {
+        if (g_fail_alloc_after.compare_exchange_weak(v, v - 1)) return v == 0;
+    }
+    return false;
+}
+
 template <typename T>
 static cudaError_t dalloc(fnec_batch *b, T **p, size_t count) {
     *p = nullptr;
     if (count == 0) count = 1;
+    if (take_injected_alloc_failure()) return cudaErrorMemoryAllocation;
     const auto t0 = std::chrono::steady_clock::now();
     cudaError_t e = b->pooled ? cudaMallocAsync((void **)p, sizeof(T) * count, b->st)
                               : cudaMalloc((void **)p, sizeof(T) * count);
@@ -1468,12 +1491,25 @@ static int antenna_from_cards(const fnec_antenna &A, HostAnt &h, std::string &wh
         why = "no frequencies";
         return FNEC_ERR_BAD_ARG;
     }
+    for (uint32_t f = 0; f < A.n_freqs; ++f)
+        if (!std::isfinite(A.freqs_hz[f]) || !(A.freqs_hz[f] > 0.0)) {
+            why = "frequency " + std::to_string(f) + " is not a finite positive number";
+            return FNEC_ERR_BAD_ARG;
+        }
     h.ground = A.ground;
     int64_t off = 0;
     for (uint32_t w = 0; w < A.n_wires; ++w) {
         const fnec_wire &gw = A.wires[w];
         if (gw.segments == 0) {
             why = "GW tag " + std::to_string(gw.tag) + ": segment count must be >= 1";
+            return FNEC_ERR_BAD_ARG;
+        }
+        // a NaN or infinite coordinate or radius is refused here, at the
+        // boundary, so that no kernel sees it
+        bool finite = std::isfinite(gw.radius);
+        for (int c = 0; c < 3; ++c) finite = finite && std::isfinite(gw.start[c]) && std::isfinite(gw.end[c]);
+        if (!finite) {
+            why = "GW tag " + std::to_string(gw.tag) + ": non-finite coordinate or radius";
             return FNEC_ERR_BAD_ARG;
         }
         double dx = gw.end[0] - gw.start[0], dy = gw.end[1] - gw.start[1], dz = gw.end[2] - gw.start[2];
@@ -1490,8 +1526,9 @@ static int antenna_from_cards(const fnec_antenna &A, HostAnt &h, std::string &wh
         d.tag = gw.tag;
         d.nseg = gw.segments;
         d.seg_off = off;
-        h.wires.push_back(d);
         for (uint32_t i = 0; i < gw.segments; ++i) h.segs.push_back(host_seg(gw, i));
+        d.self_log = h.segs.back().self_log;
+        h.wires.push_back(d);
         off += gw.segments;
     }
     auto merged = merge_collinear(h.segs);
@@ -1880,6 +1917,131 @@ int fnec_batch_run(fnec_batch *b) {
     }
     CUDA_TRY(ctx, cudaGraphLaunch(b->gexec, b->st));
     b->launches = b->graph_launches;
+    return FNEC_OK;
+}
+
+// ---- resident systems: new voltage sources on the stored factorisation ----
+
+// The voltage sources of one antenna of a batch that has run: resolved on
+// the host against the antenna's own segments (excitation.rs:119-187, the
+// same resolution as at planning) and written into the batch's source and
+// feed tables, host and device.  The new cards must give every right-hand
+// side the planned numbers of resolved sources and feed rows.
+int fnec_batch_set_sources(fnec_batch *b, uint32_t antenna, const fnec_source *sources, uint32_t n_sources) {
+    if (!b || (!sources && n_sources)) return FNEC_ERR_BAD_ARG;
+    fnec_ctx *ctx = b->ctx;
+    if (antenna >= b->ants.size()) return fail(ctx, FNEC_ERR_BAD_ARG, "set_sources: no such antenna");
+    const AntDesc &a = b->ants[antenna];
+    if (a.hom2) return fail(ctx, FNEC_ERR_BAD_ARG, "set_sources: a receiving (plane-wave) antenna has no sources");
+    if (b->rhs_given_flag || !b->from_wires)
+        return fail(ctx, FNEC_ERR_BAD_ARG, "set_sources: the batch was planned from segments and given right-hand sides");
+    // the antenna's GW cards, as planned
+    std::vector<fnec_wire> wires;
+    for (const DevWire &d : b->wires)
+        if (d.seg_off >= a.seg_off && d.seg_off < a.seg_off + a.n) {
+            fnec_wire w{};
+            w.tag = d.tag;
+            w.segments = d.nseg;
+            for (int c = 0; c < 3; ++c) {
+                w.start[c] = d.start[c];
+                w.end[c] = d.end[c];
+            }
+            w.radius = d.radius;
+            wires.push_back(w);
+        }
+    const double f1 = 1.0e6;
+    fnec_antenna A{};
+    A.wires = wires.data();
+    A.n_wires = (uint32_t)wires.size();
+    A.sources = sources;
+    A.n_sources = n_sources;
+    A.ground = a.ground;
+    A.n_freqs = 1;
+    A.freqs_hz = &f1;
+    A.separate_sources = a.n_rhs > 1 ? 1u : 0u;
+    HostAnt h;
+    std::string why;
+    int st = antenna_from_cards(A, h, why);
+    if (st != FNEC_OK) return fail(ctx, st, "set_sources: " + why);
+    if (h.rhs_srcs.empty()) {
+        h.rhs_srcs.assign(1, {});
+        h.rhs_feeds.assign(1, {});
+    }
+    if ((int)h.rhs_srcs.size() != a.n_rhs)
+        return fail(ctx, FNEC_ERR_BAD_ARG, "set_sources: the planned antenna has " + std::to_string(a.n_rhs) +
+                                                " right-hand sides, the new sources give " +
+                                                std::to_string(h.rhs_srcs.size()));
+    const int32_t *sptr = b->ibuf.data() + a.sptr_off, *fptr = b->ibuf.data() + a.fptr_off;
+    for (int r = 0; r < a.n_rhs; ++r)
+        if ((int)h.rhs_srcs[r].size() != sptr[r + 1] - sptr[r] || (int)h.rhs_feeds[r].size() != fptr[r + 1] - fptr[r])
+            return fail(ctx, FNEC_ERR_BAD_ARG,
+                        "set_sources: right-hand side " + std::to_string(r) +
+                            " needs the planned numbers of resolved sources and feed rows (EX cards)");
+    for (int r = 0; r < a.n_rhs; ++r) {
+        std::copy(h.rhs_srcs[r].begin(), h.rhs_srcs[r].end(), b->srcs.begin() + a.src_off + sptr[r]);
+        std::copy(h.rhs_feeds[r].begin(), h.rhs_feeds[r].end(), b->feeds.begin() + a.feed_off + fptr[r]);
+    }
+    // the packed input arena mirrors the tables: keep both copies current
+    cudaSetDevice(ctx->device);
+    const size_t so = (size_t)((unsigned char *)(b->d_srcs + a.src_off) - b->d_in);
+    const size_t fo = (size_t)((unsigned char *)(b->d_feeds + a.feed_off) - b->d_in);
+    const size_t sb = sizeof(DevSource) * (size_t)a.n_src, fb = sizeof(DevFeed) * (size_t)a.n_feed;
+    if (sb) std::memcpy(b->h_in + so, b->srcs.data() + a.src_off, sb);
+    if (fb) std::memcpy(b->h_in + fo, b->feeds.data() + a.feed_off, fb);
+    if (sb) CUDA_TRY(ctx, cudaMemcpyAsync(b->d_in + so, b->h_in + so, sb, cudaMemcpyHostToDevice, b->st));
+    if (fb) CUDA_TRY(ctx, cudaMemcpyAsync(b->d_in + fo, b->h_in + fo, fb, cudaMemcpyHostToDevice, b->st));
+    return FNEC_OK;
+}
+
+// Every solve of the batch again on the factorisations of its last run:
+// the right-hand sides of the current sources, then the plain form's
+// substitution on the stored factor (the elimination replayed for each
+// right-hand side, bit-identical to a fresh solve) or the mixed form's
+// refinement on the stored preconditioner, the feedpoints and the pattern.
+// Fill, normal equations and factorisation do not run.
+int fnec_batch_resolve(fnec_batch *b) {
+    if (!b) return FNEC_ERR_BAD_ARG;
+    fnec_ctx *ctx = b->ctx;
+    cudaSetDevice(ctx->device);
+    if (b->units.empty()) return FNEC_OK;
+    if (b->n_runs == 0) return fail(ctx, FNEC_ERR_BAD_ARG, "resolve: the batch has not run (no factorisation yet)");
+    if (b->has_wave || b->rhs_given_flag)
+        return fail(ctx, FNEC_ERR_BAD_ARG, "resolve: receiving antennas and given right-hand sides are not re-solved");
+    {
+        cudaError_t pre = cudaGetLastError();
+        if (pre != cudaSuccess)
+            return fail(ctx, FNEC_ERR_CUDA, std::string("an earlier call left an error: ") + cudaGetErrorString(pre));
+    }
+    cudaStream_t st = b->st;
+    const int nu = (int)b->units.size(), ns = (int)b->solves.size();
+    uint64_t L = 0;
+    const double MU0 = 4.0 * PI * 1e-7;
+    const double ETA0 = MU0 * C0;
+    // the factor's status words stay: a singular system stays flagged
+    CUDA_TRY(ctx, cudaMemsetAsync(b->d_total, 0, sizeof(double) * ns, st));
+    launch_hallen_rhs(b->d_solves, ns, b->d_ants, b->d_segs, b->d_ibuf, b->d_srcs, b->d_pts, b->d_rhs, b->d_cos,
+                      2.0 * PI / ETA0, st);
+    ++L;
+    if (b->precision == FNEC_PRECISION_MIXED) {
+        MixedMarks mm{nullptr};
+        L += refine_mixed(b->mixed, b->d_units, nu, b->d_solves, ns, b->d_ants, b->d_ibuf, b->d_crows, b->d_z,
+                          b->d_rhs, b->d_cos, b->d_x, b->d_piv, b->d_status, b->max_s, mm, st, false);
+    } else {
+        launch_extra_rhs_exact(b->d_solves, ns, b->max_s, b->d_ants, b->d_ibuf, b->d_z, b->d_rhs, b->d_cos, b->d_a,
+                               b->d_piv, b->d_x, b->d_status, st, nullptr, 0, 0);
+        L += 2;
+    }
+    launch_feedpoints(b->d_solves, ns, b->d_ants, b->d_segs, b->d_ibuf, b->d_feeds, b->d_x, b->d_status,
+                      b->d_feed_out, b->d_feed_row_off, st);
+    ++L;
+    if (b->ff_blocks > 0) {
+        launch_farfield(b->d_solves, ns, b->d_ants, b->d_runs, b->d_rps, b->d_pts, b->d_ibuf, b->d_x, b->d_status,
+                        b->d_fld, b->d_partials, b->ff_blocks, b->ff_smem, b->d_pat, b->d_total, st);
+        L += 2;
+    }
+    b->launches = L;
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(ctx, FNEC_ERR_CUDA, std::string("resolve: ") + cudaGetErrorString(e));
     return FNEC_OK;
 }
 
@@ -2405,6 +2567,7 @@ int fnec_fill_zmatrix(fnec_ctx *ctx, const fnec_zsegment *segments, uint64_t n, 
         }
         s.len = segments[i].length;
         s.rad = segments[i].radius;
+        s.self_log = self_log_term(s.len, s.rad);
         hs[i] = s;
     }
     DevSeg *d_s = nullptr;
@@ -2453,6 +2616,7 @@ static int solve_common(fnec_ctx *ctx, const fnec_zsegment *segments, const doub
             }
             s.len = segments[i].length;
             s.rad = segments[i].radius;
+            s.self_log = self_log_term(s.len, s.rad);
         }
         h.segs.push_back(s);
     }
@@ -3358,4 +3522,32 @@ const char *fnec_server_last_error(fnec_server *S) {
     std::lock_guard<std::mutex> lk(S->mu);
     S->err_copy = S->last_err;
     return S->err_copy.c_str();
+}
+
+// ---- self-tests of the failure paths (no counterpart in the reference) -----
+
+extern "C" int fnec_selftest_wait_timeout(int32_t device, int32_t which, uint64_t wait_ns, int32_t *unit_status,
+                                          double *elapsed_ms) {
+    if (!unit_status || wait_ns == 0 || wait_ns > 2000000000ull) return FNEC_ERR_BAD_ARG;
+    *unit_status = 0;
+    if (elapsed_ms) *elapsed_ms = 0.0;
+    switch (which) {
+    case 0: return fnec::selftest_grid_timeout(device, 8, 3, wait_ns, unit_status, elapsed_ms);
+    case 1: return fnec::selftest_grid_timeout(device, 8, -1, wait_ns, unit_status, elapsed_ms);
+    case 2: {
+        if (cudaSetDevice(device) != cudaSuccess) return FNEC_ERR_NO_DEVICE;
+        const auto t0 = std::chrono::steady_clock::now();
+        int rc = fnec::selftest_tc_timeout(device, wait_ns, unit_status);
+        if (elapsed_ms)
+            *elapsed_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        return rc;
+    }
+    default: return FNEC_ERR_BAD_ARG;
+    }
+}
+
+extern "C" int fnec_test_fail_device_allocation(int32_t after) {
+    if (after < -1) return FNEC_ERR_BAD_ARG;
+    g_fail_alloc_after.store(after);
+    return FNEC_OK;
 }

@@ -27,6 +27,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <new>
+#include <stdexcept>
 #include <string>
 #include <vector>
 
@@ -209,6 +211,11 @@ std::string upper(std::string s) {
 
 // fatal field errors, in the reference's wording
 struct Fatal {
+    std::string msg;
+};
+
+// A deck whose expanded grids exceed the built maxima (FNEC_DECK_MAX_*).
+struct TooLarge {
     std::string msg;
 };
 
@@ -412,6 +419,9 @@ void build_view(fnec_deck &d) {
     if (!d.fr.empty()) {
         const FrCard &r = d.fr[0];
         const uint32_t steps = std::max<uint32_t>(r.steps, 1);
+        if (steps > FNEC_DECK_MAX_FREQS && r.step_type <= 1)
+            throw TooLarge{"FR card asks for " + std::to_string(steps) + " frequencies; at most " +
+                           std::to_string(FNEC_DECK_MAX_FREQS) + " are built"};
         for (uint32_t i = 0; i < steps; ++i) {
             if (r.step_type == 0) d.freqs.push_back((r.f_mhz + (double)i * r.step_mhz) * 1e6);
             else if (r.step_type == 1) d.freqs.push_back(r.f_mhz * powi(r.step_mhz, (int)i) * 1e6);
@@ -424,6 +434,18 @@ void build_view(fnec_deck &d) {
     if (d.freqs.empty()) refuse("deck has no FR card");
     // main.rs:292-304: every RP card's grid, phi outer, theta inner (farfield.rs:677-699)
     d.rp_pts.clear();
+    uint64_t rp_total = 0;
+    for (const RpCard &r : d.rp)
+        rp_total += (uint64_t)std::max<uint32_t>(r.n_theta, 1) * std::max<uint32_t>(r.n_phi, 1);
+    if (rp_total > FNEC_DECK_MAX_POINTS)
+        throw TooLarge{"RP cards ask for " + std::to_string(rp_total) + " pattern points; at most " +
+                       std::to_string(FNEC_DECK_MAX_POINTS) + " are built"};
+    uint64_t ne_total = 0;
+    for (const NeCard &c : d.ne)
+        ne_total += (uint64_t)std::max<uint32_t>(c.nx, 1) * std::max<uint32_t>(c.ny, 1) * std::max<uint32_t>(c.nz, 1);
+    if (ne_total > FNEC_DECK_MAX_POINTS)
+        throw TooLarge{"NE/NH cards ask for " + std::to_string(ne_total) + " field points; at most " +
+                       std::to_string(FNEC_DECK_MAX_POINTS) + " are built"};
     for (const RpCard &r : d.rp) {
         const uint32_t nt = std::max<uint32_t>(r.n_theta, 1), np = std::max<uint32_t>(r.n_phi, 1);
         for (uint32_t ip = 0; ip < np; ++ip) {
@@ -524,18 +546,29 @@ uint32_t fnec_abi_struct_sizes(uint64_t *out, uint32_t cap) {
 int fnec_deck_parse(const char *text, fnec_deck **out, char *err, uint64_t err_cap) {
     if (!text || !out) return FNEC_ERR_BAD_ARG;
     *out = nullptr;
-    fnec_deck *d = new fnec_deck();
-    try {
-        parse_text(*d, text);
-    } catch (const Fatal &e) {
+    fnec_deck *d = new (std::nothrow) fnec_deck();
+    if (!d) return FNEC_ERR_OUT_OF_MEMORY;
+    auto fail = [&](int code, const std::string &msg) {
         if (err && err_cap) {
-            std::strncpy(err, e.msg.c_str(), err_cap - 1);
+            std::strncpy(err, msg.c_str(), err_cap - 1);
             err[err_cap - 1] = '\0';
         }
         delete d;
-        return FNEC_ERR_BAD_ARG;
+        return code;
+    };
+    // no C++ exception crosses the C boundary
+    try {
+        parse_text(*d, text);
+        build_view(*d);
+    } catch (const Fatal &e) {
+        return fail(FNEC_ERR_BAD_ARG, e.msg);
+    } catch (const TooLarge &e) {
+        return fail(FNEC_ERR_TOO_LARGE, e.msg);
+    } catch (const std::bad_alloc &) {
+        return fail(FNEC_ERR_OUT_OF_MEMORY, "host memory exhausted while expanding the deck");
+    } catch (const std::exception &e) {
+        return fail(FNEC_ERR_BAD_ARG, e.what());
     }
-    build_view(*d);
     *out = d;
     return FNEC_OK;
 }
@@ -575,7 +608,20 @@ int fnec_deck_get_antenna(const fnec_deck *d, fnec_antenna *out, double *freqs) 
     return FNEC_OK;
 }
 
+static int deck_solve(fnec_ctx *ctx, fnec_deck *d, int32_t precision, const char **report, uint64_t *len);
+
 int fnec_deck_solve(fnec_ctx *ctx, fnec_deck *d, int32_t precision, const char **report, uint64_t *len) {
+    // no C++ exception crosses the C boundary
+    try {
+        return deck_solve(ctx, d, precision, report, len);
+    } catch (const std::bad_alloc &) {
+        return FNEC_ERR_OUT_OF_MEMORY;
+    } catch (const std::exception &) {
+        return FNEC_ERR_BAD_ARG;
+    }
+}
+
+static int deck_solve(fnec_ctx *ctx, fnec_deck *d, int32_t precision, const char **report, uint64_t *len) {
     if (!ctx || !d || !report) return FNEC_ERR_BAD_ARG;
     *report = nullptr;
     if (!d->unsupported.empty()) return FNEC_ERR_UNSUPPORTED;

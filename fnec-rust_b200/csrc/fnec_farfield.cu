@@ -17,6 +17,7 @@
 // reduction (deterministic), and the gains, the Stokes axial ratio and the
 // -999.99 clamps are formed on the device.
 #include "fnec_kernels.h"
+#include "fnec_libm.cuh"
 #include "fnec_math.cuh"
 
 namespace fnec {
@@ -114,6 +115,67 @@ __device__ __forceinline__ void field_dir2(const DevRun *runs, int n_run, const 
     fp0 = cx_make(a_pr, a_pi);
     ft1 = cx_make(b_tr, b_ti);
     fp1 = cx_make(b_pr, b_pi);
+}
+
+// Runs along z (every run of the antenna with zero x and y direction and
+// step -- z-parallel wires): their Horner polynomial P(z) depends on the
+// direction only through cos(theta), so along a theta row of the
+// integration grid it is the same for all 360 phi.  A block evaluates it
+// once per (row, run, image) into a shared table and each direction only
+// forms exp(j k r.m0) P L and its projections -- the operations of
+// field_dir2 on the same values (contraction choices aside), with one
+// sincos per (direction, run) instead of two and no per-direction Horner.
+constexpr int FF_VMAX = 32;  // largest run count of the per-row table
+
+__device__ __forceinline__ bool run_is_vertical(const DevRun &R) {
+    return R.dir[0] == 0.0 && R.dir[1] == 0.0 && R.step[0] == 0.0 && R.step[1] == 0.0;
+}
+
+// P of run R (image if img) for the direction of unit vector rh: Horner
+// over its currents, as in field_dir2
+__device__ __forceinline__ cx run_poly(const DevRun &R, const cx *cur, double k, int img, const double *rh) {
+    double s0 = R.step[0], s1 = R.step[1], s2 = img ? -R.step[2] : R.step[2];
+    double da = k * (s0 * rh[0] + s1 * rh[1] + s2 * rh[2]);
+    double zas, zac;
+    sincos(da, &zas, &zac);
+    const cx *I = cur + R.first;
+    int c = R.count;
+    cx last = I[c - 1];
+    double ar = last.re, ai = last.im;
+    for (int n = c - 2; n >= 0; --n) {
+        cx v = I[n];
+        double nar = fma(ar, zac, fma(-ai, zas, v.re));
+        double nai = fma(ar, zas, fma(ai, zac, v.im));
+        ar = nar;
+        ai = nai;
+    }
+    return cx_make(ar, ai);
+}
+
+// The field of one direction from the per-row table P[run * 2 + img].
+__device__ __forceinline__ void field_vert(const DevRun *runs, int n_run, const cx *P, double k, bool pec,
+                                           const double *rh, const double *th, const double *ph, cx &ft, cx &fp) {
+    double a_tr = 0, a_ti = 0, a_pr = 0, a_pi = 0;
+    for (int q = 0; q < n_run; ++q) {
+        const DevRun &R = runs[q];
+        for (int img = 0; img < (pec ? 2 : 1); ++img) {
+            double m0 = R.mid0[0], m1 = R.mid0[1], m2 = img ? -R.mid0[2] : R.mid0[2];
+            double d0 = img ? -R.dir[0] : R.dir[0], d1 = img ? -R.dir[1] : R.dir[1], d2 = R.dir[2];
+            double pa = k * (m0 * rh[0] + m1 * rh[1] + m2 * rh[2]);
+            double eas, eac;
+            sincos(pa, &eas, &eac);
+            const cx acc = P[q * 2 + img];
+            double fr = (eac * acc.re - eas * acc.im) * R.len, fi = (eac * acc.im + eas * acc.re) * R.len;
+            double pta = d0 * th[0] + d1 * th[1] + d2 * th[2];
+            double ppa = d0 * ph[0] + d1 * ph[1] + d2 * ph[2];
+            a_tr = fma(fr, pta, a_tr);
+            a_ti = fma(fi, pta, a_ti);
+            a_pr = fma(fr, ppa, a_pr);
+            a_pi = fma(fi, ppa, a_pi);
+        }
+    }
+    ft = cx_make(a_tr, a_ti);
+    fp = cx_make(a_pr, a_pi);
 }
 
 // One direction's role: an integration direction (weight, and possibly the
@@ -214,13 +276,42 @@ __global__ void __launch_bounds__(FF_THREADS, 5) k_farfield(
     const int d0 = blockIdx.x * 2 * FF_THREADS + threadIdx.x, d1 = d0 + FF_THREADS;
     FfDir r0 = ff_dir(d0, n_int, n_xr, n_th, th_max, pec, rp, pts, ibuf);
     FfDir r1 = ff_dir(d1, n_int, n_xr, n_th, th_max, pec, rp, pts, ibuf);
+    // z-parallel antennas: the run polynomials of the block's (at most two)
+    // integration rows, once per block
+    __shared__ cx s_rowp[2][FF_VMAX * 2];
+    __shared__ int s_vert;
+    const int row_lo = (int)(blockIdx.x * 2 * FF_THREADS) / 360;
+    if (threadIdx.x == 0) {
+        int v = a.n_run <= FF_VMAX && n_int > 0;
+        for (int q = 0; v && q < a.n_run; ++q) v = run_is_vertical(s_runs[q]);
+        s_vert = v;
+    }
+    __syncthreads();
+    const bool vert = s_vert != 0;
+    if (vert) {
+        const int nimg = pec ? 2 : 1;
+        for (int t = threadIdx.x; t < 2 * a.n_run * nimg; t += blockDim.x) {
+            const int rr = t / (a.n_run * nimg), q = (t / nimg) % a.n_run, img = t % nimg;
+            const int row = row_lo + rr;
+            if (row >= n_th) continue;
+            double rh[3], th[3], ph[3];
+            unit_vectors_dev((double)row * th_max / ((double)n_th - 1.0), 0.0, rh, th, ph);
+            s_rowp[rr][q * 2 + img] = run_poly(s_runs[q], s_cur, u.k_rp, img, rh);
+        }
+        __syncthreads();
+    }
     double contrib = 0.0;
     if (r0.live || r1.live) {
         double rh0[3], th0[3], ph0[3], rh1[3], th1[3], ph1[3];
         unit_vectors_dev(r0.th, r0.ph, rh0, th0, ph0);
         unit_vectors_dev(r1.th, r1.ph, rh1, th1, ph1);
         cx ft0, fp0, ft1, fp1;
-        field_dir2(s_runs, a.n_run, s_cur, u.k_rp, pec, rh0, th0, ph0, rh1, th1, ph1, ft0, fp0, ft1, fp1);
+        if (vert && d0 < n_int && d1 < n_int) {
+            field_vert(s_runs, a.n_run, s_rowp[d0 / 360 - row_lo], u.k_rp, pec, rh0, th0, ph0, ft0, fp0);
+            field_vert(s_runs, a.n_run, s_rowp[d1 / 360 - row_lo], u.k_rp, pec, rh1, th1, ph1, ft1, fp1);
+        } else {
+            field_dir2(s_runs, a.n_run, s_cur, u.k_rp, pec, rh0, th0, ph0, rh1, th1, ph1, ft0, fp0, ft1, fp1);
+        }
         if (r0.integ) contrib += (ft0.re * ft0.re + ft0.im * ft0.im + fp0.re * fp0.re + fp0.im * fp0.im) * r0.wgt;
         if (r1.integ) contrib += (ft1.re * ft1.re + ft1.im * ft1.im + fp1.re * fp1.re + fp1.im * fp1.im) * r1.wgt;
         ff_store(fld_out, u, r0, ft0, fp0);
@@ -337,8 +428,8 @@ void launch_farfield(const UnitDesc *units, int nu, const AntDesc *ants, const D
 //   H += 1/(4 pi) I L e^{-jkr} jk/r^2 (1 + 1/jkr) (u x rh),
 // c = u.rh, skipping segments whose midpoint is within 1e-9 m of P.  Every
 // operation is a separately rounded FP64 op in the reference's order and
-// sin/cos(kr) are correctly rounded, so a point's field is the CPU sum bit
-// for bit.  One thread per point; the segment list is staged through shared
+// sin/cos(kr) are the platform libm's values (fnec_libm.cuh), so a point's
+// field is the CPU sum bit for bit.  One thread per point; the segment list is staged through shared
 // memory in tiles that every thread of the block reads by broadcast.
 // ---------------------------------------------------------------------------
 constexpr int NF_THREADS = 128;
@@ -381,7 +472,7 @@ __global__ void __launch_bounds__(NF_THREADS) k_near_field(const double *__restr
             const cx I = cx_make(s[7], s[8]);
             const double kr = D_MUL(k, r);
             double sn, cs;
-            cr_sincos(kr, &sn, &cs);
+            fnec_libm::libm_sincos(kr, &sn, &cs);
             const cx phase = cx_make(cs, -sn);
             const cx jkr = cx_make(0.0, kr);
             const cx one_p = cx_add(one, cx_div(one, jkr));

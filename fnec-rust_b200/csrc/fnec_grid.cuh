@@ -41,9 +41,11 @@ __device__ __forceinline__ unsigned long long gtimer_ns() {
 }
 
 // Barrier number `epoch` (1, 2, ...) of a launch whose GridSync was zeroed
-// before the launch; nblocks CTAs take part.  Returns false (in every thread
-// of the CTA) when the barrier failed: the caller returns at once.
-__device__ __forceinline__ bool grid_barrier(GridSync *gs, unsigned int nblocks, unsigned int epoch) {
+// before the launch; nblocks CTAs take part; each CTA waits at most wait_ns.
+// Returns false (in every thread of the CTA) when the barrier failed: the
+// caller returns at once.
+__device__ __forceinline__ bool grid_barrier(GridSync *gs, unsigned int nblocks, unsigned int epoch,
+                                             unsigned long long wait_ns = GRID_WAIT_NS) {
     __shared__ int s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -59,7 +61,7 @@ __device__ __forceinline__ bool grid_barrier(GridSync *gs, unsigned int nblocks,
                 ok = 0;
                 break;
             }
-            if (gtimer_ns() - t0 > GRID_WAIT_NS) {
+            if (gtimer_ns() - t0 > wait_ns) {
                 atomicExch(&gs->err, 1);
                 ok = 0;
                 break;

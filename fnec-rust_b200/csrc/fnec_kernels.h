@@ -13,11 +13,16 @@ namespace fnec {
 constexpr int PAT_STRIDE = 6;  // gain_total, gain_theta, gain_phi, axial_ratio, u_theta, u_phi
 
 // Raise a kernel's dynamic shared-memory limit to its largest use, once per
-// process.  The limit is a per-function attribute shared by every thread
-// and stream: setting it to each launch's own size would let a concurrent
-// launch (another server lane) lower it under a larger one.
+// device.  The limit is a per-function attribute of the device's context,
+// shared by every thread and stream there: setting it to each launch's own
+// size would let a concurrent launch (another server lane) lower it under a
+// larger one.
 // Returns the kernel's resulting limit (bytes), or -1 if it could not be raised.
 int set_smem_limit_once(const void *kernel, int bytes);  // fnec_plain.cu
+// self-tests of the bounded waits (fnec_selftest_wait_timeout)
+int selftest_grid_timeout(int32_t device, int32_t ctas, int32_t absent, uint64_t wait_ns, int32_t *unit_status,
+                          double *elapsed_ms);                   // fnec_plain.cu
+int selftest_tc_timeout(int32_t device, uint64_t wait_ns, int32_t *unit_status);  // fnec_tc.cu
 template <class K>
 inline int set_smem_limit_once(K kernel, int bytes) {
     return set_smem_limit_once(reinterpret_cast<const void *>(kernel), bytes);
@@ -124,7 +129,8 @@ void launch_feedpoints(const UnitDesc *solves, int ns, const AntDesc *ants, cons
 void launch_extra_rhs_exact(const UnitDesc *solves, int ns, int max_s, const AntDesc *ants, const int32_t *ibuf,
                             const cx *z, const cx *rhs, const double *cosv, const cx *A, const int32_t *piv,
                             cx *x, const int32_t *status, cudaStream_t st, const int4 *groups = nullptr,
-                            int n_groups = 0);
+                            int n_groups = 0, int first_rhs = 1);  // first_rhs 0: every right-hand side
+                                                                   // (a resident system's re-solve)
 
 // fnec_farfield.cu
 int farfield_max_blocks(int n_int_max, int n_req_max);

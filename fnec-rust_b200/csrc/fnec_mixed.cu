@@ -1139,17 +1139,24 @@ __global__ void __launch_bounds__(256, MINB) k_gmres_ir(const UnitDesc *__restri
         for (int k = g.wptr[q]; k < g.wptr[q + 1]; ++k) acc = zadd(acc, zscale(g.t[g.wrow[k]], -g.cv[g.wrow[k]]));
         b[g.n + q] = acc;
     }
+    // x0 = 0: the first cycle's residual is b itself (no operator pass), and
+    // its first Krylov vector P^-1 b is the classical first guess
+    for (int i = tid; i < s; i += blockDim.x) x[i] = {0, 0};
     __syncthreads();
-    apply_prec(g, b, x, sy);
-    double bnorm = vnorm(x, s, red);  // |P^-1 b|, the scale of the preconditioned residual
+    double bnorm = 0.0;  // |P^-1 b|, the scale of the preconditioned residual
     int iters = 0;
     double rel = 1.0;
     for (int outer = 0; outer < MAX_OUTER; ++outer) {
-        apply_A(g, x, w, sv, stv, sy);
-        for (int i = tid; i < s; i += blockDim.x) r[i] = zsub(b[i], w[i]);
-        __syncthreads();
-        apply_prec(g, r, V, sy);
+        if (outer == 0) {
+            apply_prec(g, b, V, sy);
+        } else {
+            apply_A(g, x, w, sv, stv, sy);
+            for (int i = tid; i < s; i += blockDim.x) r[i] = zsub(b[i], w[i]);
+            __syncthreads();
+            apply_prec(g, r, V, sy);
+        }
         double beta = vnorm(V, s, red);
+        if (outer == 0) bnorm = beta;
         rel = bnorm > 0 ? beta / bnorm : 0.0;
         if (rel <= GMRES_TOL || beta == 0.0) break;
         for (int i = tid; i < s; i += blockDim.x) V[i] = zscale(V[i], 1.0 / beta);
@@ -1246,6 +1253,15 @@ __global__ void __launch_bounds__(256, MINB) k_gmres_ir(const UnitDesc *__restri
             x[k] = v;
         }
         __syncthreads();
+        // a cycle that met the tolerance ends the refinement on GMRES's own
+        // residual estimate (|g_{j+1}|, the preconditioned residual of x in
+        // FP64 with twice-orthogonalised Krylov vectors); a cycle that ran
+        // out of vectors restarts from the explicit residual b - A x
+        if (s_stop) {
+            const cx gl = sg[jend + 1];
+            rel = bnorm > 0 ? sqrt(gl.re * gl.re + gl.im * gl.im) / bnorm : 0.0;
+            break;
+        }
     }
     for (int i = tid; i < s; i += blockDim.x) xbuf[u.x_off + i] = x[i];
     if (tid == 0) {
@@ -2091,6 +2107,100 @@ void free_mixed(MixedWork &w, const DevAlloc &dev) {
     w.bytes = 0;
 }
 
+// The FP64 GMRES refinement of every solve on the stored FP32 factor (the
+// last part of run_mixed; also a resident system's re-solve with new
+// right-hand sides, where the factor and its block inverses are reused:
+// fresh_factor false).
+uint64_t refine_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDesc *d_solves, int ns,
+                      const AntDesc *d_ants, const int32_t *ibuf, const DevConRow *crows, const cx *z, const cx *rhs,
+                      const double *cosv, cx *x, int32_t *piv, int32_t *status, int max_s, MixedMarks &marks,
+                      cudaStream_t st, bool fresh_factor) {
+    uint64_t L = 0;
+    int max_rows = 0;
+    for (size_t i = 0; i < mw.host.size(); ++i) max_rows = max_rows > mw.host[i].rows ? max_rows : mw.host[i].rows;
+    size_t smem = sizeof(cx) * (size_t)(2 * max_s + max_rows) + sizeof(int32_t) * (size_t)max_s;  // + perm
+    int staged = smem <= 200 * 1024;
+    if (staged && smem > 0) {  // static + dynamic above 48 KB needs the raised limit
+        int lim = std::min(set_smem_limit_once(k_gmres_ir<3>, 200 * 1024), set_smem_limit_once(k_gmres_ir<4>, 200 * 1024));
+        if (lim < 0 || (size_t)lim < smem) staged = 0;
+    }
+    if (!staged) smem = 0;
+    const bool grid_refine = mw.grid_on && !mw.grid_solves.empty();
+    const int skip_s = grid_refine ? GG_MIN_S : INT_MAX;
+    if (fresh_factor && mw.use_binv && nu > 0) {  // the preconditioner's diagonal block inverses
+        k_block_inv32<<<dim3((unsigned)((max_s + 31) / 32), (unsigned)nu), 64, 0, st>>>(d_units, mw.smu, mw.a32, mw.binv,
+                                                                                      status);
+        ++L;
+    }
+    int min_s = 0;  // solves below this are refined by the cluster kernel
+    if (ns > 0 && mw.cluster_c > 1) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(ns * mw.cluster_c));
+        cfg.blockDim = dim3(256);
+        cfg.dynamicSmemBytes = sizeof(int32_t) * (size_t)std::min(max_s, GC_MAX_S);
+        cfg.stream = st;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = (unsigned)mw.cluster_c;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        set_smem_limit_once(k_gmres_cluster, (int)(sizeof(int32_t) * GC_MAX_S));
+        if (cudaLaunchKernelEx(&cfg, k_gmres_cluster, d_solves, d_ants, mw.mu, ibuf, crows, (const cx *)z, rhs, cosv,
+                               (const float2 *)mw.a32, (const int32_t *)piv, x, mw.v, mw.w, status, mw.c_scratch,
+                               mw.cluster_c, skip_s) == cudaSuccess) {
+            min_s = GC_MAX_S + 1;
+            ++L;
+        } else {
+            (void)cudaGetLastError();  // clusters not schedulable: one CTA per solve
+        }
+    }
+    if (ns > 0) {
+        auto gk = mw.gmres_minb == 4 ? k_gmres_ir<4> : k_gmres_ir<3>;
+        gk<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x, mw.v, mw.w, status,
+                                  staged, skip_s, -1, min_s, mw.s_order, mw.use_binv ? mw.binv : nullptr);
+        cudaError_t le = cudaPeekAtLastError();
+        if (le != cudaSuccess && !marks.detail[0])
+            std::snprintf(marks.detail, sizeof(marks.detail), "GMRES launch: %d solves, %zu B shared (%s), max_s %d, rows %d",
+                          ns, smem, staged ? "staged" : "unstaged", max_s, max_rows);
+    }
+    ++L;
+    if (grid_refine) {
+        cudaMemsetAsync(mw.g_sync, 0, sizeof(GridSync) * mw.grid_solves.size(), st);
+        for (size_t k = 0; k < mw.grid_solves.size(); ++k) {
+            int ui = mw.grid_solves[k];
+            size_t psm = sizeof(int32_t) * (size_t)mw.grid_s[k];
+            int pst = psm <= 200 * 1024;
+            if (pst && psm > 0) {
+                int lim = set_smem_limit_once(k_perm_from_piv, 200 * 1024);
+                if (lim < 0 || (size_t)lim < psm) pst = 0;
+            }
+            if (!pst) psm = 0;
+            k_perm_from_piv<<<1, 256, psm, st>>>(d_solves, ui, piv, mw.g_perm, pst);
+            GridSync *gs = static_cast<GridSync *>(mw.g_sync) + k;
+            MixedUnit *mus = mw.mu;
+            float2 *a32 = mw.a32;
+            cx *vb = mw.v, *wb = mw.w;
+            const int32_t *perm = mw.g_perm;
+            void *args[] = {(void *)&d_solves, (void *)&d_ants, (void *)&mus, (void *)&ui, (void *)&ibuf,
+                            (void *)&crows, (void *)&z, (void *)&rhs, (void *)&cosv, (void *)&a32,
+                            (void *)&piv, (void *)&x, (void *)&vb, (void *)&wb, (void *)&status,
+                            (void *)&perm, (void *)&mw.g_part, (void *)&mw.g_y, (void *)&mw.g_red, (void *)&gs};
+            if (mw.grid_ctas <= 0 ||
+                launch_cooperative((const void *)k_gmres_grid, dim3(mw.grid_ctas), dim3(256), args, 0, st) !=
+                    cudaSuccess) {
+                (void)cudaGetLastError();  // not co-resident: refine this solve in one CTA
+                k_gmres_ir<3><<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x,
+                                                  mw.v, mw.w, status, staged, INT_MAX, ui, 0, mw.s_order,
+                                                  mw.use_binv ? mw.binv : nullptr);
+            }
+            L += 2;
+        }
+    }
+    return L;
+}
+
 uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDesc *d_solves, int ns,
                    const AntDesc *d_ants, const DevSeg *d_segs, const int4 *fill_tiles, int n_fill,
                    const int4 *gram_tiles, int n_gram, const int32_t *ibuf, const DevConRow *crows, cx *z,
@@ -2126,16 +2236,10 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     k_gram32_rest<<<nu, 256, 0, st>>>(d_units, d_ants, mw.smu, ibuf, crows, mw.a32);
     L += 3;
     mark(1);
-    static bool attr = false, attr_grid = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_panel32_smem<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, PANEL32_SMEM_MAX);
-        cudaFuncSetAttribute(k_panel32_smem<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, PANEL32_SMEM_MAX);
-        attr = true;
-    }
-    if (!attr_grid) {
-        cudaFuncSetAttribute(k_panel32_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-        attr_grid = true;
-    }
+    // raised once per device (set_smem_limit_once)
+    set_smem_limit_once((const void *)k_panel32_smem<256>, PANEL32_SMEM_MAX);
+    set_smem_limit_once((const void *)k_panel32_smem<1024>, PANEL32_SMEM_MAX);
+    set_smem_limit_once((const void *)k_panel32_grid, 96 * 1024);
     const int thr_rows = PANEL32_SMEM_MAX / (int)((MNB + 1) * sizeof(float2));
     const int32_t *ord = gp.d_order;
     if (gp.d_sync) cudaMemsetAsync(gp.d_sync, 0, grid_sync_bytes(gp.steps), st);
@@ -2177,11 +2281,7 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         for (int g = 0; g < n_side; ++g) cudaStreamWaitEvent(mw.fstream[g], mw.fevent[0], 0);
     }
     if (unit_launch) {
-        static bool fu_attr = false;
-        if (!fu_attr) {
-            cudaFuncSetAttribute(k_factor32_unit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FU_SMEM);
-            fu_attr = true;
-        }
+        set_smem_limit_once((const void *)k_factor32_unit, (int)FU_SMEM);
         cudaStream_t us = unit_own ? mw.fstream[G - 1] : st;
         k_factor32_unit<<<nu_all - i_unit, FU_THREADS, FU_SMEM, us>>>(d_units, mw.smu, mw.a32, piv, status, ord, i_unit);
         ++L;
@@ -2260,88 +2360,8 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         cudaStreamWaitEvent(st, mw.fevent[g + 1], 0);
     }
     mark(2);
-    int max_rows = 0;
-    for (size_t i = 0; i < mw.host.size(); ++i) max_rows = max_rows > mw.host[i].rows ? max_rows : mw.host[i].rows;
-    size_t smem = sizeof(cx) * (size_t)(2 * max_s + max_rows) + sizeof(int32_t) * (size_t)max_s;  // + perm
-    int staged = smem <= 200 * 1024;
-    if (staged && smem > 0) {  // static + dynamic above 48 KB needs the raised limit
-        int lim = std::min(set_smem_limit_once(k_gmres_ir<3>, 200 * 1024), set_smem_limit_once(k_gmres_ir<4>, 200 * 1024));
-        if (lim < 0 || (size_t)lim < smem) staged = 0;
-    }
-    if (!staged) smem = 0;
-    const bool grid_refine = mw.grid_on && !mw.grid_solves.empty();
-    const int skip_s = grid_refine ? GG_MIN_S : INT_MAX;
-    if (mw.use_binv && nu > 0) {  // the preconditioner's diagonal block inverses
-        k_block_inv32<<<dim3((unsigned)((max_s + 31) / 32), (unsigned)nu), 64, 0, st>>>(d_units, mw.smu, mw.a32, mw.binv,
-                                                                                      status);
-        ++L;
-    }
-    int min_s = 0;  // solves below this are refined by the cluster kernel
-    if (ns > 0 && mw.cluster_c > 1) {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3((unsigned)(ns * mw.cluster_c));
-        cfg.blockDim = dim3(256);
-        cfg.dynamicSmemBytes = sizeof(int32_t) * (size_t)std::min(max_s, GC_MAX_S);
-        cfg.stream = st;
-        cudaLaunchAttribute at[1];
-        at[0].id = cudaLaunchAttributeClusterDimension;
-        at[0].val.clusterDim.x = (unsigned)mw.cluster_c;
-        at[0].val.clusterDim.y = 1;
-        at[0].val.clusterDim.z = 1;
-        cfg.attrs = at;
-        cfg.numAttrs = 1;
-        set_smem_limit_once(k_gmres_cluster, (int)(sizeof(int32_t) * GC_MAX_S));
-        if (cudaLaunchKernelEx(&cfg, k_gmres_cluster, d_solves, d_ants, mw.mu, ibuf, crows, (const cx *)z, rhs, cosv,
-                               (const float2 *)mw.a32, (const int32_t *)piv, x, mw.v, mw.w, status, mw.c_scratch,
-                               mw.cluster_c, skip_s) == cudaSuccess) {
-            min_s = GC_MAX_S + 1;
-            ++L;
-        } else {
-            (void)cudaGetLastError();  // clusters not schedulable: one CTA per solve
-        }
-    }
-    if (ns > 0) {
-        auto gk = mw.gmres_minb == 4 ? k_gmres_ir<4> : k_gmres_ir<3>;
-        gk<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x, mw.v, mw.w, status,
-                                  staged, skip_s, -1, min_s, mw.s_order, mw.use_binv ? mw.binv : nullptr);
-        cudaError_t le = cudaPeekAtLastError();
-        if (le != cudaSuccess && !marks.detail[0])
-            std::snprintf(marks.detail, sizeof(marks.detail), "GMRES launch: %d solves, %zu B shared (%s), max_s %d, rows %d",
-                          ns, smem, staged ? "staged" : "unstaged", max_s, max_rows);
-    }
-    ++L;
-    if (grid_refine) {
-        cudaMemsetAsync(mw.g_sync, 0, sizeof(GridSync) * mw.grid_solves.size(), st);
-        for (size_t k = 0; k < mw.grid_solves.size(); ++k) {
-            int ui = mw.grid_solves[k];
-            size_t psm = sizeof(int32_t) * (size_t)mw.grid_s[k];
-            int pst = psm <= 200 * 1024;
-            if (pst && psm > 0) {
-                int lim = set_smem_limit_once(k_perm_from_piv, 200 * 1024);
-                if (lim < 0 || (size_t)lim < psm) pst = 0;
-            }
-            if (!pst) psm = 0;
-            k_perm_from_piv<<<1, 256, psm, st>>>(d_solves, ui, piv, mw.g_perm, pst);
-            GridSync *gs = static_cast<GridSync *>(mw.g_sync) + k;
-            MixedUnit *mus = mw.mu;
-            float2 *a32 = mw.a32;
-            cx *vb = mw.v, *wb = mw.w;
-            const int32_t *perm = mw.g_perm;
-            void *args[] = {(void *)&d_solves, (void *)&d_ants, (void *)&mus, (void *)&ui, (void *)&ibuf,
-                            (void *)&crows, (void *)&z, (void *)&rhs, (void *)&cosv, (void *)&a32,
-                            (void *)&piv, (void *)&x, (void *)&vb, (void *)&wb, (void *)&status,
-                            (void *)&perm, (void *)&mw.g_part, (void *)&mw.g_y, (void *)&mw.g_red, (void *)&gs};
-            if (mw.grid_ctas <= 0 ||
-                launch_cooperative((const void *)k_gmres_grid, dim3(mw.grid_ctas), dim3(256), args, 0, st) !=
-                    cudaSuccess) {
-                (void)cudaGetLastError();  // not co-resident: refine this solve in one CTA
-                k_gmres_ir<3><<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x,
-                                                  mw.v, mw.w, status, staged, INT_MAX, ui, 0, mw.s_order,
-                                                  mw.use_binv ? mw.binv : nullptr);
-            }
-            L += 2;
-        }
-    }
+    L += refine_mixed(mw, d_units, nu, d_solves, ns, d_ants, ibuf, crows, z, rhs, cosv, x, piv, status, max_s, marks,
+                      st, true);
     mark(3);
     return L;
 }

@@ -9,6 +9,9 @@
 
 namespace fnec {
 
+// defined in fnec_plain.cu (declared with its template wrapper in fnec_kernels.h)
+int set_smem_limit_once(const void *kernel, int bytes);
+
 struct TcGramPlan;
 struct TcTrailPlan;
 
@@ -101,6 +104,12 @@ uint64_t run_mixed(MixedWork &w, const UnitDesc *d_units, int nu, const UnitDesc
                    const cx *rhs, const double *cosv, cx *x, int32_t *piv, int32_t *status, int max_s,
                    bool do_fill, int max_w, const GridPlan &gp, MixedMarks &marks, cudaStream_t st,
                    const DevStamp *stamps = nullptr, int n_stamps = 0);
+// The refinement alone on the stored factor (run_mixed's last phase; a
+// resident system's re-solve passes fresh_factor = false).
+uint64_t refine_mixed(MixedWork &w, const UnitDesc *d_units, int nu, const UnitDesc *d_solves, int ns,
+                      const AntDesc *d_ants, const int32_t *ibuf, const DevConRow *crows, const cx *z, const cx *rhs,
+                      const double *cosv, cx *x, int32_t *piv, int32_t *status, int max_s, MixedMarks &marks,
+                      cudaStream_t st, bool fresh_factor);
 cudaError_t read_mixed_stats(MixedWork &w, int32_t *iters, double *resid, cudaStream_t st);
 
 }  // namespace fnec

@@ -35,7 +35,7 @@ struct NoallocScratch {
     UnitDesc unit;
     AntDesc ant;
     DevRp rp;
-    int32_t status;
+    int32_t status;  // the solve status the far-field kernels read: 0, the caller's currents are a solution
     int32_t pad;
     double total;
     DevRun runs[NA_MAX_SEGMENTS];
@@ -153,6 +153,10 @@ extern "C" int fnec_radiation_pattern_noalloc(const fnec_gpu_segment *d_segments
     if (ground != FNEC_GROUND_FREE && ground != FNEC_GROUND_PEC) return FNEC_ERR_BAD_ARG;
     if (!(freq_hz > 0.0)) return FNEC_ERR_BAD_ARG;
     if (n > (uint64_t)NA_MAX_SEGMENTS || p > (uint64_t)NA_MAX_POINTS) return FNEC_ERR_TOO_LARGE;
+    // A CUDA error still pending on this thread belongs to earlier work: it
+    // is reported and left in place (not cleared), and nothing is launched,
+    // so the launch check below sees this call's launches only.
+    if (cudaPeekAtLastError() != cudaSuccess) return FNEC_ERR_CUDA;
     NoallocScratch *S = nullptr;
     int st = scratch_for_current_device(&S);
     if (st != FNEC_OK) return st;

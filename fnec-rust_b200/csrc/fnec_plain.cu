@@ -2,8 +2,10 @@
 //
 // Every arithmetic operation below is one separately rounded IEEE
 // operation (explicit _rn intrinsics; the file is also built with
-// -fmad=false), issued in the order the reference issues it, and the
-// transcendental calls are correctly rounded (fnec_math.cuh).  Given the
+// -fmad=false), issued in the order the reference issues it, and sin, cos
+// and hypot return the platform libm's values (fnec_libm.cuh restates
+// glibc's algorithms; the self term's ln comes from the host libm, see
+// DevSeg::self_log).  Given the
 // same inputs the Gram matrix, the elimination and the back substitution
 // therefore reproduce the reference CPU path bit for bit; pivot order is
 // chosen with the reference's "last maximum by hypot" rule.
@@ -24,11 +26,14 @@
 #include <algorithm>
 #include <cstdio>
 #include <climits>
+#include <map>
 #include <mutex>
 #include <unordered_map>
+#include <utility>
 
 #include "fnec_grid.cuh"
 #include "fnec_kernels.h"
+#include "fnec_libm.cuh"
 #include "fnec_math.cuh"
 
 namespace fnec {
@@ -80,7 +85,7 @@ __global__ void k_expand_segments(const DevWire *__restrict__ wires, int nw, Dev
         s.rad = gw.radius;
         s.tag = gw.tag;
         s.tag_index = i + 1;
-        s.pad = 0.0;
+        s.self_log = gw.self_log;
         segs[gw.seg_off + i] = s;
     }
 }
@@ -111,7 +116,7 @@ __global__ void k_hallen_rhs(const UnitDesc *__restrict__ solves, const AntDesc 
         for (int m = threadIdx.x; m < a.n; m += blockDim.x) {
             if (u.rhs == 0) {
                 double sn, cs;
-                cr_sincos(D_MUL(k, s_mid[m]), &sn, &cs);
+                fnec_libm::libm_sincos(D_MUL(k, s_mid[m]), &sn, &cs);
                 cos_buf[u.cos_off + m] = D_MUL(sgn[m], cs);
             }
             cx r = cx_make(0.0, 0.0);
@@ -120,7 +125,7 @@ __global__ void k_hallen_rhs(const UnitDesc *__restrict__ solves, const AntDesc 
                 if (col[m] != col[s.feed]) continue;
                 double ds = fabs(D_SUB(s_mid[m], s_mid[s.feed]));
                 double ss, sc;
-                cr_sincos(D_MUL(k, ds), &ss, &sc);
+                fnec_libm::libm_sincos(D_MUL(k, ds), &ss, &sc);
                 cx t = cx_mul(cx_make(0.0, D_MUL(-scale, ss)), cx_make(s.v_re, s.v_im));
                 double f = D_MUL(sgn[m], sgn[s.feed]);
                 r = cx_add(r, cx_make(D_MUL(t.re, f), D_MUL(t.im, f)));
@@ -141,7 +146,7 @@ __global__ void k_hallen_rhs(const UnitDesc *__restrict__ solves, const AntDesc 
         double s_local = D_ADD(D_ADD(D_MUL(dl0, wd[0]), D_MUL(dl1, wd[1])), D_MUL(dl2, wd[2]));
         if (u.rhs == 0) {  // cos(k s) belongs to the system: written once
             double sn, cs;
-            cr_sincos(D_MUL(k, s_local), &sn, &cs);
+            fnec_libm::libm_sincos(D_MUL(k, s_local), &sn, &cs);
             cos_buf[u.cos_off + m] = cs;
         }
         cx r = cx_make(0.0, 0.0);
@@ -154,7 +159,7 @@ __global__ void k_hallen_rhs(const UnitDesc *__restrict__ solves, const AntDesc 
             double d2 = D_SUB(sg[m].mid[2], f.mid[2]);
             double sd = D_ADD(D_ADD(D_MUL(d0, f.dir[0]), D_MUL(d1, f.dir[1])), D_MUL(d2, f.dir[2]));
             double ss, sc;
-            cr_sincos(D_MUL(k, fabs(sd)), &ss, &sc);
+            fnec_libm::libm_sincos(D_MUL(k, fabs(sd)), &ss, &sc);
             cx t = cx_mul(cx_make(0.0, D_MUL(-scale, ss)), cx_make(s.v_re, s.v_im));
             r = cx_add(r, t);
         }
@@ -195,12 +200,12 @@ __global__ void k_planewave_field(const UnitDesc *__restrict__ solves, int ns, c
         const double phase = D_MUL(
             k, D_ADD(D_ADD(D_MUL(wv[0], sg[p].mid[0]), D_MUL(wv[1], sg[p].mid[1])), D_MUL(wv[2], sg[p].mid[2])));
         double sn, cs;
-        cr_sincos(phase, &sn, &cs);
+        fnec_libm::libm_sincos(phase, &sn, &cs);
         const cx e = cx_mul(coup, cx_make(D_MUL(1.0, cs), D_MUL(1.0, sn)));  // from_polar(1, phase)
         xbuf[u.x_off + p] = cx_make(D_MUL(e.re, sgn), D_MUL(e.im, sgn));
         if (u.rhs == 0) {
             double ss, sc;
-            cr_sincos(D_MUL(k, s), &ss, &sc);
+            fnec_libm::libm_sincos(D_MUL(k, s), &ss, &sc);
             cos_buf[u.cos_off + p] = D_MUL(sgn, sc);
             cos_buf[u.cos_off + a.n + p] = D_MUL(sgn, ss);
             const int32_t col = ibuf[a.rowwire_off + p];
@@ -208,7 +213,7 @@ __global__ void k_planewave_field(const UnitDesc *__restrict__ solves, int ns, c
             double *kt = cos_buf + u.cos_off + 2 * (int64_t)a.n + ibuf[a.koff_off + p];
             for (int q = wptr[col]; q < wptr[col + 1]; ++q) {
                 double ks, kc;
-                cr_sincos(D_MUL(k, fabs(D_SUB(s, dtab[a.arc_off + wrow[q]]))), &ks, &kc);
+                fnec_libm::libm_sincos(D_MUL(k, fabs(D_SUB(s, dtab[a.arc_off + wrow[q]]))), &ks, &kc);
                 kt[q - wptr[col]] = ks;
             }
         }
@@ -261,13 +266,14 @@ __global__ void k_receive_peaks(const UnitDesc *__restrict__ solves, const AntDe
 // G(R) = exp(-jkR)/R with exp(0 + jt) = (cos t, sin t) (num-complex exp)
 __device__ __forceinline__ cx green_k_exact(double r, double k) {
     double sn, cs;
-    cr_sincos(D_MUL(-k, r), &sn, &cs);
+    fnec_libm::libm_sincos(D_MUL(-k, r), &sn, &cs);
     return cx_make(D_DIV(cs, r), D_DIV(sn, r));
 }
 
-// matrix.rs:297-331 elem(obs, src, k, is_self)
+// matrix.rs:297-331 elem(obs, src, k, is_self); self_log is the source
+// segment's 2 ln((h + sqrt(h^2 + a^2)) / a), evaluated on the host
 __device__ __forceinline__ cx elem_exact(const double *om, const double *od, const double *sm,
-                                         const double *sd, double slen, double srad, double k,
+                                         const double *sd, double slen, double srad, double self_log, double k,
                                          bool is_self) {
     double cos_alpha = D_ADD(D_ADD(D_MUL(od[0], sd[0]), D_MUL(od[1], sd[1])), D_MUL(od[2], sd[2]));
     double half = D_MUL(slen, 0.5);
@@ -286,9 +292,7 @@ __device__ __forceinline__ cx elem_exact(const double *om, const double *od, con
         }
         sre = D_MUL(sre, half);
         sim = D_MUL(sim, half);
-        double r_end = D_SQRT(D_ADD(D_MUL(half, half), D_MUL(a, a)));
-        double analytic = D_MUL(2.0, cr_log(D_DIV(D_ADD(half, r_end), a)));
-        ire = D_ADD(sre, analytic);
+        ire = D_ADD(sre, self_log);
         iim = sim;
     } else {
         double sre = 0.0, sim = 0.0;
@@ -313,13 +317,13 @@ __device__ __forceinline__ cx elem_exact(const double *om, const double *od, con
 
 __device__ __forceinline__ cx z_entry_exact(const DevSeg &o, const DevSeg &s, double k, int ground,
                                             bool is_self) {
-    cx direct = elem_exact(o.mid, o.dir, s.mid, s.dir, s.len, s.rad, k, is_self);
+    cx direct = elem_exact(o.mid, o.dir, s.mid, s.dir, s.len, s.rad, s.self_log, k, is_self);
     cx img = cx_make(0.0, 0.0);
     if (ground == 1) {
         // matrix.rs:265-279 image: position (x, y, -z), current (-Jx, -Jy, +Jz)
         double im_mid[3] = {s.mid[0], s.mid[1], -s.mid[2]};
         double im_dir[3] = {-s.dir[0], -s.dir[1], s.dir[2]};
-        img = elem_exact(o.mid, o.dir, im_mid, im_dir, s.len, s.rad, k, false);
+        img = elem_exact(o.mid, o.dir, im_mid, im_dir, s.len, s.rad, 0.0, k, false);
     }
     return cx_add(direct, img);
 }
@@ -979,9 +983,10 @@ __global__ void k_feedpoints(const UnitDesc *__restrict__ solves, const AntDesc 
 // ---------------------------------------------------------------------------
 __global__ void k_extra_rhs_b(const UnitDesc *__restrict__ solves, const AntDesc *__restrict__ ants,
                               const int32_t *__restrict__ ibuf, const cx *__restrict__ zbuf,
-                              const cx *__restrict__ rhs_buf, const double *__restrict__ cos_buf, cx *xbuf) {
+                              const cx *__restrict__ rhs_buf, const double *__restrict__ cos_buf, cx *xbuf,
+                              int first_rhs) {
     UnitDesc u = solves[blockIdx.y];
-    if (u.rhs == 0) return;
+    if (u.rhs < first_rhs) return;
     AntDesc a = ants[u.ant];
     int n = u.n;
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1007,10 +1012,10 @@ __global__ void k_extra_rhs_b(const UnitDesc *__restrict__ solves, const AntDesc
 
 __global__ void k_extra_rhs_solve(const UnitDesc *__restrict__ solves, const cx *__restrict__ abuf,
                                   const int32_t *__restrict__ piv_buf, cx *xbuf,
-                                  const int32_t *__restrict__ status, int staged) {
+                                  const int32_t *__restrict__ status, int staged, int first_rhs) {
     extern __shared__ cx s_bs[];
     UnitDesc u = solves[blockIdx.x];
-    if (u.rhs == 0 || status[u.sys] != 0) return;
+    if (u.rhs < first_rhs || status[u.sys] != 0) return;
     int s = u.s, w1 = s + 1;
     const cx *A = abuf + u.a_off;
     const int32_t *piv = piv_buf + u.piv_off;
@@ -1389,11 +1394,20 @@ void launch_gram_exact(const UnitDesc *units, int nu, int max_w, const AntDesc *
 }
 constexpr size_t TRAILING_SMEM = sizeof(cx) * (64 * (NB + 1) + NB * 64);
 
+// Raises a kernel's dynamic shared-memory limit once per device: the
+// attribute belongs to the kernel in the current device's context, so a
+// second GPU needs its own call.  Returns the limit in effect.
 int set_smem_limit_once(const void *kernel, int bytes) {
     static std::mutex mu;
-    static std::unordered_map<const void *, int> done;
+    static std::map<std::pair<int, const void *>, int> done;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return -1;
+    }
     std::lock_guard<std::mutex> lk(mu);
-    auto it = done.find(kernel);
+    const auto key = std::make_pair(dev, kernel);
+    auto it = done.find(key);
     if (it != done.end()) return it->second;
     int got = -1;
     cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -1407,7 +1421,7 @@ int set_smem_limit_once(const void *kernel, int bytes) {
         if (cudaFuncGetAttributes(&fa, kernel) == cudaSuccess) got = fa.maxDynamicSharedSizeBytes;
         else (void)cudaGetLastError();
     }
-    done[kernel] = got;
+    done[key] = got;
     return got;
 }
 
@@ -1476,14 +1490,9 @@ void step_classes(const GridPlan &gp, int c0, int i_begin, std::vector<StepClass
 uint64_t launch_factor_exact(const UnitDesc *units, int nu, int max_s, const GridPlan &gp, cx *A,
                              int32_t *piv, int32_t *status, cudaStream_t st) {
     uint64_t L = 0;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_trailing, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)TRAILING_SMEM);
-        cudaFuncSetAttribute(k_panel_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, PANEL_SMEM_MAX);
-        cudaFuncSetAttribute(k_panel_grid, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024);
-        attr = true;
-    }
+    set_smem_limit_once(k_trailing, (int)TRAILING_SMEM);  // once per device
+    set_smem_limit_once(k_panel_smem, PANEL_SMEM_MAX);
+    set_smem_limit_once(k_panel_grid, 96 * 1024);
     (void)nu;
     const int thr_rows = PANEL_SMEM_MAX / (int)((NB + 1) * sizeof(cx));
     const int32_t *ord = gp.d_order;
@@ -1570,9 +1579,10 @@ void launch_feedpoints(const UnitDesc *solves, int ns, const AntDesc *ants, cons
 }
 void launch_extra_rhs_exact(const UnitDesc *solves, int ns, int max_s, const AntDesc *ants, const int32_t *ibuf,
                             const cx *z, const cx *rhs, const double *cosv, const cx *A, const int32_t *piv,
-                            cx *x, const int32_t *status, cudaStream_t st, const int4 *groups, int n_groups) {
+                            cx *x, const int32_t *status, cudaStream_t st, const int4 *groups, int n_groups,
+                            int first_rhs) {
     if (ns <= 0) return;
-    if (groups && n_groups > 0) {
+    if (groups && n_groups > 0 && first_rhs == 1) {
         dim3 gb((max_s + 63) / 64, n_groups);
         k_extra_rhs_b_group<<<gb, 64, 0, st>>>(solves, groups, ants, ibuf, z, rhs, cosv, x);
         const size_t smem4 = solve_group4_smem(max_s);
@@ -1590,11 +1600,11 @@ void launch_extra_rhs_exact(const UnitDesc *solves, int ns, int max_s, const Ant
             return;
         }
         // a factor too tall for the shared tile: one warp per solve on the b vectors formed above
-        k_extra_rhs_solve<<<ns, 32, 0, st>>>(solves, A, piv, x, status, 0);
+        k_extra_rhs_solve<<<ns, 32, 0, st>>>(solves, A, piv, x, status, 0, 1);
         return;
     }
     dim3 g((max_s + 127) / 128, ns);
-    k_extra_rhs_b<<<g, 128, 0, st>>>(solves, ants, ibuf, z, rhs, cosv, x);
+    k_extra_rhs_b<<<g, 128, 0, st>>>(solves, ants, ibuf, z, rhs, cosv, x, first_rhs);
     size_t smem = sizeof(cx) * (size_t)max_s;
     int staged = smem <= BS_SMEM_MAX;
     if (staged && smem > 0) {  // static + dynamic above 48 KB needs the raised limit
@@ -1602,7 +1612,68 @@ void launch_extra_rhs_exact(const UnitDesc *solves, int ns, int max_s, const Ant
         if (lim < 0 || (size_t)lim < smem) staged = 0;
     }
     if (!staged) smem = 0;
-    k_extra_rhs_solve<<<ns, 32, smem, st>>>(solves, A, piv, x, status, staged);
+    k_extra_rhs_solve<<<ns, 32, smem, st>>>(solves, A, piv, x, status, staged, first_rhs);
 }
 
+}  // namespace fnec
+
+// ---------------------------------------------------------------------------
+// Self-test of the bounded grid barrier's timeout path
+// (fnec_selftest_wait_timeout): every CTA but `absent` takes the barrier;
+// the absent CTA returns without arriving, so the others' waits run out
+// after wait_ns and each marks the status word FNEC_UNIT_TIMEOUT.  With
+// absent < 0 every CTA arrives and the status stays 0.
+// ---------------------------------------------------------------------------
+namespace fnec {
+__global__ void k_grid_barrier_probe(GridSync *gs, int32_t *status, int absent, unsigned long long wait_ns) {
+    if ((int)blockIdx.x == absent) return;
+    if (!grid_barrier(gs, gridDim.x, 1, wait_ns)) {
+        if (threadIdx.x == 0) atomicExch(status, FNEC_UNIT_TIMEOUT);
+        return;
+    }
+}
+
+int selftest_grid_timeout(int32_t device, int32_t ctas, int32_t absent, uint64_t wait_ns, int32_t *unit_status,
+                          double *elapsed_ms) {
+    if (cudaSetDevice(device) != cudaSuccess) return FNEC_ERR_NO_DEVICE;
+    if (ctas < 2 || ctas > 148 || absent >= ctas) return FNEC_ERR_BAD_ARG;
+    GridSync *gs = nullptr;
+    int32_t *st = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int rc = FNEC_OK;
+    do {
+        if (cudaMalloc(&gs, sizeof(GridSync)) != cudaSuccess || cudaMalloc(&st, sizeof(int32_t)) != cudaSuccess) {
+            rc = FNEC_ERR_OUT_OF_MEMORY;
+            break;
+        }
+        if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+            rc = FNEC_ERR_CUDA;
+            break;
+        }
+        cudaMemset(gs, 0, sizeof(GridSync));
+        cudaMemset(st, 0, sizeof(int32_t));
+        unsigned long long w = wait_ns;
+        void *args[] = {(void *)&gs, (void *)&st, (void *)&absent, (void *)&w};
+        cudaEventRecord(e0, 0);
+        if (launch_cooperative((const void *)k_grid_barrier_probe, dim3(ctas), dim3(64), args, 0, 0) != cudaSuccess) {
+            (void)cudaGetLastError();
+            rc = FNEC_ERR_UNSUPPORTED;
+            break;
+        }
+        cudaEventRecord(e1, 0);
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            rc = FNEC_ERR_CUDA;
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (elapsed_ms) *elapsed_ms = ms;
+        if (unit_status) cudaMemcpy(unit_status, st, sizeof(int32_t), cudaMemcpyDeviceToHost);
+    } while (0);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(gs);
+    cudaFree(st);
+    return rc;
+}
 }  // namespace fnec

@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <mutex>
 
 #include "fnec_cuda.h"
@@ -56,23 +57,24 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
 }
 // Bounded wait.  false: the CTA is aborting (abort word set by another role)
 // or this wait ran out of time (it then sets the abort word).
-__device__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_word) {
+__device__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_word,
+                          unsigned long long limit_ns = TC_WAIT_NS) {
     unsigned long long t0 = gtimer_ns();
     for (uint32_t it = 1;; ++it) {
         if (mbar_try(bar, parity)) return true;
         if (*abort_word) return false;
-        if ((it & 63) == 0 && gtimer_ns() - t0 > TC_WAIT_NS) {
+        if ((it & 63) == 0 && gtimer_ns() - t0 > limit_ns) {
             *abort_word = 1;
             return false;
         }
     }
 }
 // Bounded wait that ignores the abort word (draining after an abort).
-__device__ void mbar_drain(uint32_t bar, uint32_t parity) {
+__device__ void mbar_drain(uint32_t bar, uint32_t parity, unsigned long long limit_ns = TC_WAIT_NS) {
     unsigned long long t0 = gtimer_ns();
     for (uint32_t it = 1;; ++it) {
         if (mbar_try(bar, parity)) return;
-        if ((it & 63) == 0 && gtimer_ns() - t0 > TC_WAIT_NS) return;
+        if ((it & 63) == 0 && gtimer_ns() - t0 > limit_ns) return;
     }
 }
 
@@ -247,14 +249,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = s_tmem;
+    const unsigned long long wlim = ep.wait_ns ? (unsigned long long)ep.wait_ns : TC_WAIT_NS;
+    const int stop_kb = ep.test_stop_on ? ep.test_stop_kb : INT_MAX;
 
     if (warp == 0) {
         if (lane == 0) {
             int issued = 0;
-            for (int kb = 0; kb < t.kblocks; ++kb) {
+            for (int kb = 0; kb < t.kblocks && kb < stop_kb; ++kb) {
                 const int st = kb % STAGES;
                 const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
-                if (kb >= STAGES && !mbar_wait(empty(st), ph ^ 1u, abort_word)) break;
+                if (kb >= STAGES && !mbar_wait(empty(st), ph ^ 1u, abort_word, wlim)) break;
                 const uint32_t dst = sbase + st * STAGE_BYTES;
                 mbar_expect_tx(full(st), STAGE_BYTES);
                 const int ya = t.a_row + kb * t.a_kstride, yb = t.b_row + kb * t.b_kstride;
@@ -264,16 +268,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 tma_load_2d(dst + 3 * BOX_BYTES, &mBl, 0, yb, full(st));
                 issued = kb + 1;
             }
-            if (*abort_word)  // let the copies already issued land before the CTA exits
+            if (*abort_word || issued < t.kblocks)  // let the copies already issued land before the CTA exits
                 for (int kb = issued - 1; kb >= 0 && kb >= issued - STAGES; --kb)
-                    mbar_drain(full(kb % STAGES), (uint32_t)(kb / STAGES) & 1u);
+                    mbar_drain(full(kb % STAGES), (uint32_t)(kb / STAGES) & 1u, wlim);
         }
     } else if (warp == 1) {
         if (lane == 0) {
             for (int kb = 0; kb < t.kblocks; ++kb) {
                 const int st = kb % STAGES;
                 const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
-                if (!mbar_wait(full(st), ph, abort_word)) break;
+                if (!mbar_wait(full(st), ph, abort_word, wlim)) break;
                 tc_fence_after();
                 const uint32_t a_hi = sbase + st * STAGE_BYTES, a_lo = a_hi + BOX_BYTES;
                 const uint32_t b_hi = a_hi + 2 * BOX_BYTES, b_lo = a_hi + 3 * BOX_BYTES;
@@ -289,10 +293,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 mma_commit(empty(st));
             }
             mma_commit(tfull);  // arrives once every MMA issued above has completed
-            if (*abort_word) mbar_drain(tfull, 0);
+            if (*abort_word) mbar_drain(tfull, 0, wlim);
         }
     } else {
-        const bool ok = mbar_wait(tfull, 0, abort_word);
+        const bool ok = mbar_wait(tfull, 0, abort_word, wlim);
         tc_fence_after();
         if (ok) {
             const int q = warp & 3;  // TMEM lane quarter this warp may access
@@ -458,13 +462,8 @@ size_t tc_smem_bytes() { return (size_t)STAGES * STAGE_BYTES + 1024; }
 template <int EPI>
 cudaError_t launch_tc(const CUtensorMap &ah, const CUtensorMap &al, const CUtensorMap &bh, const CUtensorMap &bl,
                       const TcTile *tiles, int ntiles, const TcEpilogue &ep, cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)tc_smem_bytes());
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    if (set_smem_limit_once((const void *)k_tc_gemm<EPI>, (int)tc_smem_bytes()) < (int)tc_smem_bytes())
+        return cudaErrorInvalidConfiguration;
     if (ntiles <= 0) return cudaSuccess;
     k_tc_gemm<EPI><<<ntiles, TC_THREADS, tc_smem_bytes(), st>>>(ah, al, bh, bl, tiles, ep);
     return cudaGetLastError();
@@ -563,13 +562,8 @@ cudaError_t tc_trail_run(const TcTrailPlan &p, int step, int count, const TcTrai
                                                                                          c0, hi, lo);
     k_split_trail_b<<<dim3((unsigned)((p.max_n2pad[step] / 2 + 31) / 32), (unsigned)na), 256, 0, st>>>(
         tl, d_systems, d_smu, a32, c0, hi, lo);
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(k_tc_gemm<TC_EPI_TRAIL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)tc_smem_bytes());
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    if (set_smem_limit_once((const void *)k_tc_gemm<TC_EPI_TRAIL>, (int)tc_smem_bytes()) < (int)tc_smem_bytes())
+        return cudaErrorInvalidConfiguration;
     TcEpilogue ep{};
     ep.units = d_systems;
     ep.mus = d_smu;
@@ -608,8 +602,12 @@ cudaError_t tc_gram_run(const TcGramPlan &p, const UnitDesc *d_units, const TcGr
 
 using namespace fnec;
 
-extern "C" int fnec_selftest_tf32x3_gemm(int32_t device, uint64_t m, uint64_t n, uint64_t k, const float *a,
-                                         const float *b, float *c) {
+// The GEMM self-test; stop_kb >= 0 makes the producer stop issuing loads
+// at that k-block, so the MMA warp's wait on the next one runs out after
+// wait_ns and the CTAs take the timeout path (drain, free TMEM, mark the
+// status word), which *unit_status reports.
+static int tc_selftest(int32_t device, uint64_t m, uint64_t n, uint64_t k, const float *a, const float *b, float *c,
+                       int32_t stop_kb, uint64_t wait_ns, int32_t *unit_status) {
     if (!a || !b || !c || m == 0 || n == 0 || k == 0) return FNEC_ERR_BAD_ARG;
     if (m > (1u << 16) || n > (1u << 16) || k > (1u << 16)) return FNEC_ERR_TOO_LARGE;
     if (cudaSetDevice(device) != cudaSuccess) return FNEC_ERR_NO_DEVICE;
@@ -662,6 +660,9 @@ extern "C" int fnec_selftest_tf32x3_gemm(int32_t device, uint64_t m, uint64_t n,
         ep.n = (int64_t)n;
         ep.status = dst;
         ep.status_of_tile = 0;
+        ep.wait_ns = wait_ns;
+        ep.test_stop_on = stop_kb >= 0 ? 1 : 0;
+        ep.test_stop_kb = stop_kb;
         if (launch_tc<TC_EPI_STORE>(mah, mal, mbh, mbl, dt, (int)tiles.size(), ep, 0) != cudaSuccess) {
             rc = FNEC_ERR_CUDA;
             break;
@@ -672,6 +673,7 @@ extern "C" int fnec_selftest_tf32x3_gemm(int32_t device, uint64_t m, uint64_t n,
         }
         int32_t stv = 0;
         cudaMemcpy(&stv, dst, sizeof(int32_t), cudaMemcpyDeviceToHost);
+        if (unit_status) *unit_status = stv;
         if (stv != 0) {
             rc = FNEC_ERR_TIMEOUT;
             break;
@@ -686,3 +688,20 @@ extern "C" int fnec_selftest_tf32x3_gemm(int32_t device, uint64_t m, uint64_t n,
     cudaFree(dst);
     return rc;
 }
+
+extern "C" int fnec_selftest_tf32x3_gemm(int32_t device, uint64_t m, uint64_t n, uint64_t k, const float *a,
+                                         const float *b, float *c) {
+    return tc_selftest(device, m, n, k, a, b, c, -1, 0, nullptr);
+}
+
+namespace fnec {
+// The timeout path of the tensor-core GEMM (fnec_selftest_wait_timeout):
+// a 128 x 128 x 256 product whose loads stop after two of its eight
+// k-blocks.  FNEC_OK when the CTA gave up within its limit and marked the
+// status word; *unit_status is that word.
+int selftest_tc_timeout(int32_t device, uint64_t wait_ns, int32_t *unit_status) {
+    std::vector<float> a(128 * 256, 0.5f), b(128 * 256, 0.25f), c(128 * 128);
+    int rc = tc_selftest(device, 128, 128, 256, a.data(), b.data(), c.data(), 2, wait_ns, unit_status);
+    return rc == FNEC_ERR_TIMEOUT ? FNEC_OK : (rc == FNEC_OK ? FNEC_ERR_CUDA : rc);
+}
+}  // namespace fnec

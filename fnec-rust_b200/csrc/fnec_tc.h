@@ -53,6 +53,13 @@ struct TcEpilogue {
     // TC_EPI_TRAIL: the step and its units (blockIdx.y), tiles from blockIdx.x
     int32_t c0;
     const TcTrailUnit *trail;
+    // limit of every mbarrier wait (0: TC_WAIT_NS, 2 s)
+    uint64_t wait_ns;
+    // self-test of the timeout path only: the producer stops issuing loads
+    // at this k-block (-1 or 0 fields of a zeroed struct: never; see
+    // fnec_selftest_wait_timeout)
+    int32_t test_stop_kb;
+    int32_t test_stop_on;
 };
 
 // Gram operand layout of one unit: T (2N x N) as kblocks k-blocks of rpad

@@ -25,7 +25,10 @@ struct DevSeg {          // nec_solver::geometry::Segment (geometry.rs:115-134)
     double end[3];
     uint32_t tag;
     uint32_t tag_index;
-    double pad;
+    // 2 ln((len/2 + sqrt((len/2)^2 + rad^2)) / rad): the analytic part of
+    // the self term (matrix.rs:297-331), evaluated on the host with the
+    // platform libm so that the exact fill uses the reference's value
+    double self_log;
 };
 static_assert(sizeof(DevSeg) == 128, "DevSeg is one 128-byte line");
 
@@ -36,6 +39,7 @@ struct DevWire {         // one GW card, expanded by k_expand_segments
     uint32_t tag;
     uint32_t nseg;
     int64_t seg_off;     // global index of its first segment
+    double self_log;     // DevSeg::self_log of its segments (all equal)
 };
 
 // A straight run of segments whose midpoints advance by a constant step

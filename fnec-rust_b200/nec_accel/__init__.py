@@ -41,6 +41,7 @@ ERR_TIMEOUT = -8
 ERR_BUSY = -9
 ERR_TOO_LARGE = -10
 NOALLOC_MAX_SEGMENTS = 4096
+UNIT_TIMEOUT = 0x40000000  # per-unit status: a bounded device wait gave up
 NOALLOC_MAX_POINTS = 65536
 
 GROUND_FREE = 0
@@ -190,6 +191,10 @@ SIGNATURES = {
     "fnec_selftest_tf32x3_gemm": (ctypes.c_int, [ctypes.c_int32, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
                                                  _P, _P, _P]),
     "fnec_radiation_pattern_noalloc": (ctypes.c_int, [_P, _U64, _P, _D, _I32, _P, _U64, _P, _P, _P]),
+    "fnec_selftest_wait_timeout": (ctypes.c_int, [_I32, _I32, _U64, _P, _P]),
+    "fnec_batch_set_sources": (ctypes.c_int, [_P, _U32, _P, _U32]),
+    "fnec_batch_resolve": (ctypes.c_int, [_P]),
+    "fnec_test_fail_device_allocation": (ctypes.c_int, [_I32]),
     "fnec_batch_create": (ctypes.c_int, [_P, _P, _U32, _I32, _P]),
     "fnec_batch_destroy": (ctypes.c_int, [_P]),
     "fnec_batch_get_info": (ctypes.c_int, [_P, _P]),
@@ -576,6 +581,28 @@ def selftest_tf32x3_gemm(a: np.ndarray, b: np.ndarray, device: int = 0) -> np.nd
     return c
 
 
+WAIT_GRID_ABSENT_CTA, WAIT_GRID_ALL_ARRIVE, WAIT_GEMM_LOADS_STOPPED = 0, 1, 2
+
+
+def selftest_wait_timeout(which: int, wait_ns: int = 1_000_000, device: int = 0):
+    """Make one bounded device wait run out on purpose (fnec_selftest_wait_timeout):
+    returns (the status word the kernel left, the launch's milliseconds)."""
+    st = ctypes.c_int32()
+    ms = ctypes.c_double()
+    rc = lib().fnec_selftest_wait_timeout(int(device), int(which), int(wait_ns), ctypes.byref(st), ctypes.byref(ms))
+    if rc != OK:
+        raise AccelError(rc, f"selftest_wait_timeout({which})")
+    return int(st.value), float(ms.value)
+
+
+def test_fail_device_allocation(after: int):
+    """Test hook: the after-th batch device allocation from now on fails
+    with OUT_OF_MEMORY (once); -1 disarms."""
+    rc = lib().fnec_test_fail_device_allocation(int(after))
+    if rc != OK:
+        raise AccelError(rc, "test_fail_device_allocation")
+
+
 def measure_fp32_peak(device: int = 0) -> float:
     """FP32 FFMA throughput of the GPU in TFLOP/s."""
     a = ctypes.c_double()
@@ -933,6 +960,23 @@ class HallenBatch:
 
     def solve(self) -> BatchResult:
         self.run()
+        self.sync()
+        return self.read()
+
+    def set_sources(self, antenna: int, sources):
+        """New voltage sources for one antenna of a batch that has run
+        (fnec_batch_set_sources); sources: a SOURCE_DTYPE array or
+        (tag, segment, voltage) tuples, giving every right-hand side its
+        planned numbers of resolved sources and feed rows."""
+        arr = sources if isinstance(sources, np.ndarray) else sources_array(sources)
+        arr = np.ascontiguousarray(arr, dtype=SOURCE_DTYPE)
+        self.ctx.check(lib().fnec_batch_set_sources(self._h, int(antenna), _ptr(arr) if len(arr) else None, len(arr)),
+                       "batch_set_sources")
+
+    def resolve(self) -> BatchResult:
+        """Solve every unit again on the resident factorisations with the
+        current sources (fnec_batch_resolve) and read the results."""
+        self.ctx.check(lib().fnec_batch_resolve(self._h), "batch_resolve")
         self.sync()
         return self.read()
 

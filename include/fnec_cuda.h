@@ -328,7 +328,11 @@ typedef struct {
     char why[200];       /* the reason, or the first parser warning */
 } fnec_deck_info;
 /* Parse a deck.  A bad or missing field is fatal (FNEC_ERR_BAD_ARG; err
- * receives "line N: ..."); unknown cards are counted and skipped. */
+ * receives "line N: ..."); unknown cards are counted and skipped.  Grids
+ * beyond the maxima below are refused with FNEC_ERR_TOO_LARGE (err says
+ * which card); host memory exhaustion gives FNEC_ERR_OUT_OF_MEMORY. */
+#define FNEC_DECK_MAX_FREQS (1u << 20)  /* FR steps                          */
+#define FNEC_DECK_MAX_POINTS (1u << 22) /* RP points over all RP cards; NE/NH */
 int fnec_deck_parse(const char *text, fnec_deck **out, char *err, uint64_t err_cap);
 int fnec_deck_destroy(fnec_deck *d);
 int fnec_deck_get_info(const fnec_deck *d, fnec_deck_info *out);
@@ -508,6 +512,24 @@ int fnec_host_free(void *p);
 int fnec_selftest_tf32x3_gemm(int32_t device, uint64_t m, uint64_t n, uint64_t k, const float *a,
                               const float *b, float *c);
 
+/* Self-tests of the failure paths (no counterpart in the reference; test
+ * use).  fnec_selftest_wait_timeout makes one bounded device wait run out
+ * on purpose and reports the status word the kernel left:
+ *   which 0  a cooperative launch of 8 CTAs whose CTA 3 never reaches the
+ *            grid barrier: the others give up after wait_ns and mark
+ *            FNEC_UNIT_TIMEOUT;
+ *   which 1  the same launch with every CTA arriving: status 0;
+ *   which 2  the tcgen05 GEMM with its loads stopped after 2 of 8 k-blocks:
+ *            the MMA warp's wait runs out, the CTA drains its copies and
+ *            MMAs, frees TMEM and marks FNEC_UNIT_TIMEOUT.
+ * wait_ns is 1 .. 2e9.  Returns FNEC_OK when the kernel ran to its end;
+ * *elapsed_ms is the launch's duration.  The context stays usable.
+ * fnec_test_fail_device_allocation(n): the n-th batch device allocation
+ * from now on fails as if the device were full (once); -1 disarms. */
+int fnec_selftest_wait_timeout(int32_t device, int32_t which, uint64_t wait_ns, int32_t *unit_status,
+                               double *elapsed_ms);
+int fnec_test_fail_device_allocation(int32_t after);
+
 /* Radiation pattern that allocates no device memory.  No counterpart in
  * the reference: it serves callers that cannot call cudaMalloc -- a host
  * framework that owns all device memory through its own pool, a plugin held
@@ -521,10 +543,15 @@ int fnec_selftest_tf32x3_gemm(int32_t device, uint64_t m, uint64_t n, uint64_t k
  * work is enqueued on `stream` (a cudaStream_t; NULL = legacy default) of
  * the current device; the caller synchronises.
  * Scratch lives in a fixed static device array of about 5.6 MB held by
- * every GPU that loads the library until exit.  The first call on each
- * device looks its address up (cudaGetSymbolAddress); make that first call
- * before any stream capture.  Calls that overlap on the GPU (other streams,
- * other threads) race on the shared scratch and must be serialised.
+ * every GPU that loads the library until exit.  With CUDA's lazy module
+ * loading the array (and the kernels) are committed on a device at the
+ * first call there, which also looks the array's address up
+ * (cudaGetSymbolAddress): make that first call before the host framework
+ * reserves its memory pool and before any stream capture.  Calls that
+ * overlap on the GPU (other streams, other threads) race on the shared
+ * scratch and must be serialised.  A CUDA error already pending on the
+ * calling thread is returned as FNEC_ERR_CUDA (and left pending) with
+ * nothing launched.
  * Limits: n <= FNEC_NOALLOC_MAX_SEGMENTS, p <= FNEC_NOALLOC_MAX_POINTS;
  * larger sizes return FNEC_ERR_TOO_LARGE without touching the device. */
 #define FNEC_NOALLOC_MAX_SEGMENTS 4096
@@ -596,6 +623,19 @@ int fnec_batch_read_refinement(fnec_batch *b, int32_t *iters, double *resid);
 /* Z matrix (2*n*n doubles) and the augmented normal-equation matrix before
  * elimination is not kept; the Z of a unit can be read after a run. */
 int fnec_batch_read_z(fnec_batch *b, uint32_t unit, double *z);
+/* Resident systems (no counterpart in the reference, whose accelerator
+ * keeps no device state between calls): after a run, a batch keeps every
+ * system's Z and factorisation on the device.  fnec_batch_set_sources
+ * replaces the voltage sources of one antenna (resolved against its
+ * segments as at planning); every right-hand side must keep its planned
+ * numbers of resolved sources and feed rows.  fnec_batch_resolve then
+ * solves every unit again on the stored factorisations -- right-hand
+ * sides, substitution (plain: bit-identical to a fresh batch with those
+ * sources) or refinement (mixed), feedpoints and pattern -- without the
+ * fill, the normal equations or the factorisation.  Results are read as
+ * after fnec_batch_run. */
+int fnec_batch_set_sources(fnec_batch *b, uint32_t antenna, const fnec_source *sources, uint32_t n_sources);
+int fnec_batch_resolve(fnec_batch *b);
 
 /* ---- schedules, CUDA graphs and the autotuner --------------------------
  *

@@ -78,4 +78,7 @@ def main(root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FNEC_REFERENCE")
+    if not ref:
+        sys.exit("usage: %s REFERENCE_CHECKOUT (or set FNEC_REFERENCE)" % os.path.basename(sys.argv[0]))
+    main(ref)

@@ -165,3 +165,27 @@ def test_restated_ne_points_are_the_oracle_points():
         want = O.near_field_points(*card)
         got = np.array(R.ne_points(card))
         assert got.shape == want.shape and np.array_equal(got, want), card
+
+
+@pytest.mark.parametrize("card,what", [("RP 0 100000 100000 0 0 1 1", "RP cards ask for 10000000000 pattern points"),
+                                       ("RP 0 2049 2048 0 0 1 1", "RP cards ask for 4196352 pattern points"),
+                                       ("NE 0 2000 2000 2 0 0 0 1 1 1", "NE/NH cards ask for 8000000 field points"),
+                                       ("FR 0 2000000 0 0 14.2 0.001", "FR card asks for 2000000 frequencies")])
+def test_oversize_grids_are_refused_with_too_large(acc, card, what):
+    """Grids the deck expands on the host are bounded: a card that asks for
+    more than FNEC_DECK_MAX_POINTS points or FNEC_DECK_MAX_FREQS
+    frequencies is refused with TOO_LARGE and a message, instead of an
+    allocation failure escaping the C boundary."""
+    base = ["CM big", "CE", "GW 1 11 0 0 -1 0 0 1 0.001", "GE 0", "EX 0 1 6 0 1 0", "FR 0 1 0 0 14.2 0"]
+    lines = base[:-1] + [card] if card.startswith("FR") else base + [card]
+    with pytest.raises(acc.AccelError) as ei:
+        acc.Deck("\n".join(lines + ["EN"]) + "\n")
+    assert ei.value.code == acc.ERR_TOO_LARGE
+    assert what in str(ei.value)
+
+
+def test_grid_at_the_limit_is_accepted(acc):
+    d = acc.Deck("CM ok\nCE\nGW 1 11 0 0 -1 0 0 1 0.001\nGE 0\nEX 0 1 6 0 1 0\nFR 0 1 0 0 14.2 0\n"
+                 "RP 0 2048 2048 0 0 0.05 0.1\nEN\n")
+    assert d.info()["n_points"] == 2048 * 2048
+    d.close()

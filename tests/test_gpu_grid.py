@@ -78,3 +78,23 @@ def test_grid_panel_and_gmres_mixed(acc):
         xm, _ = mixed.read_unit(u)
         xp, _ = plain.read_unit(0)
         assert np.linalg.norm(xm - xp) / np.linalg.norm(xp) <= 1e-7
+
+
+def test_mesh_20x20_plain_end_to_end_bit_exact(acc):
+    """Mesh of 20x20 cells over PEC ground (N = 1680 segments, W = 840
+    wires, S = 2520, 2,398 pairwise junction rows): the plain form end to
+    end -- fill with image terms, Gram with the constraint rows, grid-wide
+    panels, back substitution, feedpoint -- against the oracle (its
+    row-parallel GEPP is the reference's elimination bit for bit): pivots,
+    currents and Zin identical."""
+    w, s, f = _mesh(20)
+    ant = acc.Antenna(w.view(acc.WIRE_DTYPE), s.view(acc.SOURCE_DTYPE), [f], 1, None)
+    batch = acc.HallenBatch([ant])
+    res = batch.solve()
+    assert res.status[0] == 0
+    assert batch.units[0]["s"] == 2520
+    p = O.Problem(w, s, f, ground=1)
+    O.solve_problems([p], 8)
+    assert p.status == 0
+    _check_unit(acc, batch, res, 0, w, s, 1, f, None, bit_exact=True, solved=p)
+    batch.close()

@@ -23,22 +23,6 @@ pytestmark = pytest.mark.gpu
 CASES = load_cases()
 ZIN_TOL = 1e-9
 CUR_TOL = 1e-9
-# The top-hat loaded dipole's normal equations have cond(A) = 3.7e10 (the
-# others here 3e8-5e8): the ulp-level differences between the device's
-# correctly rounded fill and the oracle's libm fill reach its small loop
-# currents at ~5e-9 of the peak.  Its solve is bit-exact given the oracle's
-# Z (test_solve_is_bit_exact_given_the_oracle_z) and its Zin meets 1e-9.
-CUR_TOL_CASE = {"dipole-loaded": 1e-7}
-# The four TL corpus decks (two dipoles joined by a line) have cond(A) =
-# 1.2e13-1.3e13: there the same ulp-level fill differences move Zin by
-# 2e-8 (51 segments per wire) to 7e-7 (52) relative, against the oracle and
-# against the golden values alike.  Their stamps are bit-identical to the
-# oracle's (test_gpu_loads.py) and their solve is bit-exact given the
-# oracle's stamped Z (test_solve_is_bit_exact_given_the_oracle_z).
-for _name in ("tl-two-dipoles-linked", "tl-two-dipoles-linked-seg0", "tl-two-dipoles-linked-nseg0",
-              "tl-two-dipoles-linked-seg0-even52"):
-    CUR_TOL_CASE[_name] = 1e-5
-ZIN_TOL_CASE = {n: 2e-6 for n in CUR_TOL_CASE if n.startswith("tl-")}
 GAIN_TOL_DB = 1e-6
 
 
@@ -63,9 +47,11 @@ def _antenna(acc, deck, freqs=None, rp=None):
 
 
 def _check_unit(acc, batch, res, u, wires, sources, ground, freq, pts, loads=None, cur_tol=CUR_TOL, tls=None,
-                nts=None, zin_tol=ZIN_TOL):
-    p = O.Problem(wires, sources, freq, ground=ground, points=pts, loads=loads, tls=tls, nts=nts)
-    O.solve_problem(p)
+                nts=None, zin_tol=ZIN_TOL, bit_exact=False, solved=None):
+    p = solved
+    if p is None:
+        p = O.Problem(wires, sources, freq, ground=ground, points=pts, loads=loads, tls=tls, nts=nts)
+        O.solve_problem(p)
     assert p.status == 0
     assert res.status[u] == 0
     feeds = res.feeds[u]
@@ -79,6 +65,13 @@ def _check_unit(acc, batch, res, u, wires, sources, ground, freq, pts, loads=Non
         assert np.array_equal(cur, p.currents)
     else:
         assert np.abs(cur - p.currents).max() / peak <= cur_tol
+    if bit_exact:
+        # the fill's sin/cos/hypot are the platform libm's and its ln is the
+        # host's, so the whole solve reproduces the oracle bit for bit
+        assert np.array_equal(cur.view(np.uint64), p.currents.view(np.uint64)), \
+            np.abs(cur - p.currents).max() / max(peak, 1e-300)
+        zg = np.array([complex(r[5], r[6]) for r in feeds])
+        assert np.array_equal(zg.view(np.uint64), np.asarray(p.zin, np.complex128).view(np.uint64))
     _, piv = batch.read_unit(u)
     # the oracle's pivot buffer has room for n + (GW cards) rows; the solve
     # uses n + (columns): merged wires, or conductor paths in the path form
@@ -110,32 +103,51 @@ def test_corpus_case_matches_oracle_and_golden(acc, name):
     for u, f in enumerate(deck["freqs"]):
         tl, nt = deck_networks(deck)
         _check_unit(acc, batch, res, u, wires, sources, deck["ground"], f, pts, loads=deck_loads(deck),
-                    cur_tol=CUR_TOL_CASE.get(name, CUR_TOL), tls=tl, nts=nt,
-                    zin_tol=ZIN_TOL_CASE.get(name, ZIN_TOL))
+                    tls=tl, nts=nt, bit_exact=True)
         if f in golden:
             for row, want in zip(res.feeds[u], golden[f]):
                 got = complex(row[5], row[6])
                 tol = 2e-6 if len(repr(want.real).split(".")[-1]) >= 6 else 0.05
-                tol = max(tol, ZIN_TOL_CASE.get(name, 0.0) * abs(want))
                 assert abs(got.real - want.real) <= tol and abs(got.imag - want.imag) <= tol
 
 
-def test_z_fill_matches_oracle(acc):
-    """matrix.rs fill with correctly rounded sin/cos/ln: almost every element
-    is bit-identical to the glibc-based oracle; the rest differ by ulps."""
-    deck = CASES["yagi-5elm-51seg"]["deck"]
+def _oracle_stamped_z(segs, f, ground, deck):
+    """The oracle's Z with the deck's LD loads on the diagonal, then its TL
+    and NT stamps in card order (solve_session.rs:1285-1309), each stamp one
+    separately rounded add per part."""
+    z = O.assemble_z(segs, f, ground)
+    ld = deck_loads(deck)
+    if ld is not None:
+        lv, _ = O.build_loads(segs, f, ld)
+        for i in range(len(segs)):
+            z[i, i] = complex(z[i, i].real + lv[i].real, z[i, i].imag + lv[i].imag)
+    tl, nt = deck_networks(deck)
+    for r, c, d in (O.tl_stamps(segs, f, tl) if tl is not None else []) + \
+            (O.nt_stamps(segs, nt) if nt is not None else []):
+        z[r, c] = complex(z[r, c].real + d.real, z[r, c].imag + d.imag)
+    return z
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_z_fill_bit_identical_to_oracle(acc, name):
+    """matrix.rs fill (elem + green_k + image terms, matrix.rs:186-331,
+    :397) and the LD/TL/NT stamps: with glibc's sin/cos restated on the
+    device and the self term's ln taken from the host libm, every element of
+    Z equals the oracle's bit for bit, in free space and over PEC ground."""
+    deck = CASES[name]["deck"]
     wires, sources, _ = deck_arrays(deck)
-    for ground in (0, 1):
-        d = dict(deck, ground=ground)
+    segs = O.build_geometry(wires)
+    grounds = (0, 1) if name == "yagi-5elm-51seg" else (deck["ground"],)
+    for ground in grounds:
+        d = dict(deck, ground=ground, rp=None)
         batch = acc.HallenBatch([_antenna(acc, d)])
         batch.solve()
-        zg = batch.read_z(0)
-        segs = O.build_geometry(wires)
-        zr = O.assemble_z(segs, deck["freqs"][0], ground)
-        same = np.mean(zg.view(np.uint64) == zr.view(np.uint64))
-        rel = np.abs(zg - zr).max() / np.abs(zr).max()
-        assert same > 0.98, same
-        assert rel < 1e-14, rel
+        for u, f in enumerate(deck["freqs"]):
+            zg = batch.read_z(u)
+            zr = _oracle_stamped_z(segs, f, ground, deck)
+            assert np.array_equal(zg.view(np.uint64), zr.view(np.uint64)), \
+                (f, np.mean(zg.view(np.uint64) == zr.view(np.uint64)), np.abs(zg - zr).max())
+        batch.close()
 
 
 def test_solve_is_bit_exact_given_the_oracle_z(acc):

@@ -75,6 +75,70 @@ def test_noalloc_pattern_matches_allocating_entry_point_twice():
         assert np.abs(out[:, 3] - ref[:, 3]).max() <= 1e-9
 
 
+def _run_noalloc(acc, torch, dev, gseg, cur, f, ground, pts):
+    d_seg = torch.from_numpy(gseg.view(np.uint8).copy()).to(dev)
+    d_cur = torch.from_numpy(np.ascontiguousarray(cur).view(np.float64).copy()).to(dev)
+    d_pts = torch.from_numpy(np.ascontiguousarray(pts, np.float64).ravel().copy()).to(dev)
+    d_out = torch.full((len(pts) * 4,), np.nan, dtype=torch.float64, device=dev)
+    d_tot = torch.zeros(1, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def call():
+        return acc.radiation_pattern_noalloc(d_seg.data_ptr(), len(gseg), d_cur.data_ptr(), f, ground,
+                                             d_pts.data_ptr(), len(pts), d_out.data_ptr(), d_tot.data_ptr(),
+                                             stream.cuda_stream)
+
+    return call, d_out, d_tot
+
+
+@pytest.mark.parametrize("n_wires,seg_per_wire,n_theta,n_phi,ground", [
+    (4, 250, 64, 32, 1),      # 1000 segments: runs + currents staged above the default 48 KB
+    (8, 512, 256, 256, 0),    # the maxima: 4096 segments (unstaged branch), 65,536 points
+])
+def test_noalloc_large_cases_allocate_nothing(n_wires, seg_per_wire, n_theta, n_phi, ground):
+    """Sizes that take the far field's other shared-memory branches, up to
+    the entry point's maxima (4096 segments, 65,536 points), against the
+    allocating entry point; after a first call, a call changes the device's
+    free memory by nothing (cudaMemGetInfo)."""
+    import torch
+
+    import nec_accel as acc
+
+    dev = torch.device("cuda", 0)
+    rng = np.random.default_rng(n_wires)
+    wl = []
+    for t in range(n_wires):
+        p0 = rng.uniform([-10, -10, 1], [10, 10, 20])
+        p1 = rng.uniform([-10, -10, 1], [10, 10, 20])
+        wl.append((t + 1, seg_per_wire, tuple(p0), tuple(p1), 1e-3))
+    segs = O.build_geometry(O.wires_array(wl))
+    n = len(segs)
+    assert n == n_wires * seg_per_wire <= acc.NOALLOC_MAX_SEGMENTS
+    cur = rng.normal(size=n) + 1j * rng.normal(size=n)
+    pts = O.rp_card_points(n_theta, n_phi, 0.0, 0.0, 90.0 / n_theta if ground else 180.0 / n_theta,
+                           360.0 / n_phi)
+    assert len(pts) <= acc.NOALLOC_MAX_POINTS
+    f = 7.1e6
+    gseg = acc.gpu_segments_from(segs)
+    ref, tot_ref = acc.compute_radiation_pattern(gseg, cur, f, pts, ground)
+    call, d_out, d_tot = _run_noalloc(acc, torch, dev, gseg, cur, f, ground, pts)
+    assert call() == acc.OK
+    torch.cuda.synchronize(dev)
+    free0, _ = torch.cuda.mem_get_info(dev)
+    assert call() == acc.OK
+    torch.cuda.synchronize(dev)
+    free1, _ = torch.cuda.mem_get_info(dev)
+    assert free1 == free0
+    out = d_out.cpu().numpy().reshape(-1, 4)
+    tot = float(d_tot.cpu().numpy()[0])
+    assert abs(tot - tot_ref) <= 1e-12 * tot_ref
+    for col in (0, 1, 2):
+        live = ref[:, col] > -999.0
+        assert np.abs(out[live, col] - ref[live, col]).max(initial=0.0) <= GAIN_TOL_DB
+        assert np.array_equal(out[~live, col], ref[~live, col])
+    assert np.abs(out[:, 3] - ref[:, 3]).max() <= 1e-9
+
+
 def test_noalloc_rejects_sizes_beyond_its_static_maximum():
     import nec_accel as acc
 
