@@ -2085,7 +2085,8 @@ static bool schedule_valid(const fnec_schedule &s) {
     return bit(s.grid_panels) && (s.class_shift == 1 || s.class_shift == 2) && bit(s.gram_tensor) &&
            (s.gmres_cluster == 1 || s.gmres_cluster == 2 || s.gmres_cluster == 4 || s.gmres_cluster == 8) &&
            bit(s.grid_gmres) && s.graph >= 0 && s.graph <= 2 &&
-           (s.factor_streams == 1 || s.factor_streams == 2 || s.factor_streams == 4) && bit(s.unit_factor) &&
+           (s.factor_streams == 1 || s.factor_streams == 2 || s.factor_streams == 4) && s.unit_factor >= 0 &&
+           s.unit_factor <= 3 &&
            bit(s.block_inverse) && bit(s.tensor_trailing) && (s.gmres_ctas_per_sm == 3 || s.gmres_ctas_per_sm == 4);
 }
 
@@ -2108,7 +2109,7 @@ static void apply_schedule(fnec_batch *b, const fnec_schedule &s) {
     b->mixed.cluster_c = t.gmres_cluster < 1 ? 1 : t.gmres_cluster;
     b->mixed.grid_on = t.grid_gmres != 0;
     b->grid.factor_streams = t.factor_streams;
-    b->grid.unit_factor = t.unit_factor != 0;
+    b->grid.unit_factor = t.unit_factor;
     b->mixed.use_binv = t.block_inverse != 0;
     b->mixed.use_tc_trail = t.tensor_trailing != 0;
     b->mixed.gmres_minb = t.gmres_ctas_per_sm;
@@ -2261,8 +2262,8 @@ int fnec_batch_tune(fnec_batch *b, uint32_t reps, fnec_tune_report *out) {
     if (mixed && !b->mixed.grid_solves.empty()) knobs.push_back({&fnec_schedule::grid_gmres, {1, 0}});
     if (b->grid.d_xchg) knobs.push_back({&fnec_schedule::grid_panels, {1, 0}});
     if (b->units.size() > 1) knobs.push_back({&fnec_schedule::class_shift, {1, 2}});
-    if (mixed && !b->grid.s_desc.empty() && b->grid.s_desc.back() <= 256)
-        knobs.push_back({&fnec_schedule::unit_factor, {1, 0}});
+    if (mixed && !b->grid.s_desc.empty() && b->grid.s_desc.back() <= 512)
+        knobs.push_back({&fnec_schedule::unit_factor, {1, 0, 2, 3}});
     if (mixed && b->mixed.fmade) knobs.push_back({&fnec_schedule::factor_streams, {1, 2, 4}});
     if (mixed) knobs.push_back({&fnec_schedule::block_inverse, {1, 0}});
     if (mixed) knobs.push_back({&fnec_schedule::gmres_ctas_per_sm, {3, 4}});

@@ -71,7 +71,8 @@ struct GridPlan {
     bool grid_on = true;         // tall panels grid-wide (else one CTA from global memory)
     int class_shift = 1;         // size classes of panel heights: (2^k x lo, hi]
     int factor_streams = 1;      // mixed factor: groups of units factored on concurrent streams
-    bool unit_factor = true;     // mixed factor: small units factored whole, one CTA each
+    int unit_factor = 1;         // mixed factor: units with S <= 256 / 384 / 512 (1 / 2 / 3) factored
+                                 // whole, one CTA each; 0: none
 };
 size_t grid_xchg_bytes();        // bytes of d_xchg
 size_t grid_sync_bytes(int steps);

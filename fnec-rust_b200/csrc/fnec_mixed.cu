@@ -466,16 +466,23 @@ __global__ void __launch_bounds__(NT) k_panel32_smem(const UnitDesc *__restrict_
     panel32_body<NT>(a32buf + mus[ui].a32_off, s, c0, piv_buf + u.piv_off, &status[ui], s_pan32, s_v, s_i, &s_p);
 }
 
-// The whole FP32 blocked GEPP of one small unit (S <= FU_MAX_S) per CTA:
+// The whole FP32 blocked GEPP of one small unit (S <= fu_max_s(level)) per CTA:
 // the panel, swap/U12 and trailing steps of the per-step kernels
 // (k_panel32_smem, k_swap_u12_32, k_trailing32) with the same per-element
 // operations in the same order -- so the factor is bit-identical -- but
 // without a kernel boundary or a global round trip between steps.
-constexpr int FU_MAX_S = 256;
+// unit_factor level 1, 2, 3: units with S <= 256, 384, 512 (0: none)
+__host__ __device__ constexpr int fu_max_s(int level) { return level <= 0 ? 0 : 128 + 128 * level; }
+constexpr int FU_MAX_S_ALL = 512;
 // trailing blocks of at least this many rows go to the tensor cores
 constexpr int TC_TRAIL_MIN_M = 192;
 constexpr int FU_THREADS = 256;
-constexpr size_t FU_SMEM = sizeof(float2) * (size_t)(MNB * (MNB + 1) + MNB * FU_THREADS);  // swap stage, the largest
+constexpr size_t FU_SMEM = sizeof(float2) * (size_t)(MNB * (MNB + 1) + MNB * FU_THREADS);  // the swap stage
+// dynamic shared memory of a launch whose largest unit has S = smax: the
+// swap stage, or the panel (S rows of MNB + 1 entries) when taller
+__host__ __device__ constexpr size_t fu_smem(int smax) {
+    return FU_SMEM > sizeof(float2) * (size_t)smax * (MNB + 1) ? FU_SMEM : sizeof(float2) * (size_t)smax * (MNB + 1);
+}
 
 __global__ void __launch_bounds__(FU_THREADS, 3) k_factor32_unit(const UnitDesc *__restrict__ units,
                                                                 const MixedUnit *__restrict__ mus, float2 *a32buf,
@@ -2251,8 +2258,8 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     // units with S <= FU_MAX_S (the tail of the order) are factored whole,
     // one CTA each, in one launch on a stream of their own
     int i_unit = nu_all;
-    if (gp.unit_factor)
-        while (i_unit > 0 && gp.s_desc[i_unit - 1] <= FU_MAX_S) --i_unit;
+    if (gp.unit_factor > 0)
+        while (i_unit > 0 && gp.s_desc[i_unit - 1] <= fu_max_s(gp.unit_factor)) --i_unit;
     const bool unit_launch = i_unit < nu_all;
     int G = std::max(1, std::min(gp.factor_streams, MixedWork::MAX_FACTOR_STREAMS) - (unit_launch ? 1 : 0));
     if (!mw.fmade || i_unit < 2 * G) G = 1;
@@ -2281,9 +2288,10 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         for (int g = 0; g < n_side; ++g) cudaStreamWaitEvent(mw.fstream[g], mw.fevent[0], 0);
     }
     if (unit_launch) {
-        set_smem_limit_once((const void *)k_factor32_unit, (int)FU_SMEM);
+        set_smem_limit_once((const void *)k_factor32_unit, (int)fu_smem(FU_MAX_S_ALL));
         cudaStream_t us = unit_own ? mw.fstream[G - 1] : st;
-        k_factor32_unit<<<nu_all - i_unit, FU_THREADS, FU_SMEM, us>>>(d_units, mw.smu, mw.a32, piv, status, ord, i_unit);
+        const size_t fsm = fu_smem(gp.s_desc[i_unit]);  // the launch's largest unit
+        k_factor32_unit<<<nu_all - i_unit, FU_THREADS, fsm, us>>>(d_units, mw.smu, mw.a32, piv, status, ord, i_unit);
         ++L;
     }
     std::vector<StepClass> cls;

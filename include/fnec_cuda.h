@@ -661,9 +661,10 @@ typedef struct {
     int32_t factor_streams;/* mixed: the factor's units in 1, 2 or 4 groups of
                               about equal work, each on its own stream (parallel
                               branches of the graph)                              */
-    int32_t unit_factor;   /* mixed: 1 units with S <= 256 are factored whole,
-                              one CTA each, in one launch beside the per-step
-                              launches of the larger units                        */
+    int32_t unit_factor;   /* mixed: units with S <= 256 (1), 384 (2) or 512 (3)
+                              are factored whole, one CTA each, in one launch
+                              beside the per-step launches of the larger units;
+                              0 none                                              */
     int32_t block_inverse; /* mixed: 1 the refinement applies the factor's 32x32
                               diagonal blocks through their FP64 inverses (block
                               products); 0 by substitution in one warp            */
