@@ -854,6 +854,36 @@ def measure_batch(args, acc, batch, stream, rank, local, dist, steps, warmup, wi
             "res": batch.read()}
 
 
+def measure_followup(acc, batch, stream, local, dist, steps):
+    """Follow-up requests on the resident factorisations: new voltage
+    sources for the sweep (the source moved along element 2, alternating
+    between two positions), then every frequency solved again on the stored
+    factor (fnec_batch_set_sources + fnec_batch_resolve: right-hand sides,
+    substitution or refinement, feedpoints, pattern; no fill, Gram or
+    factorisation).  CUDA events on the batch's stream; max over ranks."""
+    import torch
+
+    srcs = [[(2, 20, 1.0)], [(2, 32, 1.0)]]
+    batch.set_sources(0, srcs[0])
+    batch.resolve(read=False)
+    batch.sync()
+    if dist is not None:
+        dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for k in range(steps):
+        batch.set_sources(0, srcs[k % 2])
+        batch.resolve(read=False)
+    e1.record(stream)
+    batch.sync()
+    ms = e0.elapsed_time(e1)
+    vals = torch.tensor([ms], dtype=torch.float64, device=f"cuda:{local}")
+    if dist is not None:
+        dist.all_reduce(vals, op=dist.ReduceOp.MAX)
+    batch.set_sources(0, [(2, 26, 1.0)])  # the workload's own source again
+    return {"ms_per_step": vals.item() / steps, "steps": steps}
+
+
 def measure_with_planning(acc, ants, prec, ctx, stream, local, dist, steps):
     """End to end per call when every call brings new geometries: the C
     ABI's batch planning (topology, junctions, constraint rows, packing,
@@ -915,6 +945,8 @@ def run_batch_workload(args, acc, ctx, rank, local, dist, world, steps, warmup, 
                                  "graph_kernels": nodes}
         if tune is not None:
             out[form]["schedule"]["tune"] = {k: tune[k] for k in ("candidates", "default_ms", "best_ms", "key")}
+        if args.workload == "sweep5":
+            out[form]["followup"] = measure_followup(acc, batch, stream, local, dist, steps)
         if form == "mixed":
             it, rs = batch.refinement_stats()
             out[form]["gmres"] = {"iters_mean": float(it.mean()), "iters_max": int(it.max()),
@@ -1019,6 +1051,14 @@ def run_batch_workload(args, acc, ctx, rank, local, dist, world, steps, warmup, 
                                 "phase_ms": {k: round(v, 4) for k, v in o["phase"].items()}}
         if "gmres" in o:
             line[f"form_{form}"]["gmres"] = o["gmres"]
+        if "followup" in o:
+            fu = o["followup"]
+            line[f"form_{form}"]["followup_resident"] = {
+                "value": per_step_units / (fu["ms_per_step"] * 1e-3), "unit": "solves/s",
+                "ms_per_step": fu["ms_per_step"],
+                "what": "new source position on every frequency, solved on the resident factorisations "
+                        "(fnec_batch_set_sources + fnec_batch_resolve): right-hand sides, substitution or "
+                        "refinement, feedpoints, the 91x361 pattern; device time"}
         if "planning" in o:
             pl = o["planning"]
             line[f"form_{form}"]["e2e_with_planning"] = {

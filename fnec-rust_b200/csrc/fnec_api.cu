@@ -18,6 +18,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <tuple>
 #include <vector>
 
@@ -1627,11 +1628,25 @@ int fnec_batch_create(fnec_ctx *ctx, const fnec_antenna *antennas, uint32_t n_an
         return fail(ctx, FNEC_ERR_UNSUPPORTED, "mixed precision path not built");
     cudaSetDevice(ctx->device);
     std::vector<HostAnt> hs(n_antennas);
-    for (uint32_t a = 0; a < n_antennas; ++a) {
-        std::string why;
-        int st = antenna_from_cards(antennas[a], hs[a], why);
-        if (st != FNEC_OK) return fail(ctx, st, "antenna " + std::to_string(a) + ": " + why);
+    // each antenna's host planning (segments, topology, junctions, sources)
+    // is independent: spread over host threads for large batches
+    std::vector<int> st_of(n_antennas, FNEC_OK);
+    std::vector<std::string> why_of(n_antennas);
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned nt = n_antennas >= 256 ? std::min(hw, 16u) : 1u;
+    auto work = [&](unsigned k) {
+        for (uint32_t a = k; a < n_antennas; a += nt) st_of[a] = antenna_from_cards(antennas[a], hs[a], why_of[a]);
+    };
+    if (nt > 1) {
+        std::vector<std::thread> pool;
+        for (unsigned k = 1; k < nt; ++k) pool.emplace_back(work, k);
+        work(0);
+        for (auto &t : pool) t.join();
+    } else {
+        work(0);
     }
+    for (uint32_t a = 0; a < n_antennas; ++a)
+        if (st_of[a] != FNEC_OK) return fail(ctx, st_of[a], "antenna " + std::to_string(a) + ": " + why_of[a]);
     return build_batch(ctx, hs, precision, out);
 }
 
@@ -2087,7 +2102,8 @@ static bool schedule_valid(const fnec_schedule &s) {
            bit(s.grid_gmres) && s.graph >= 0 && s.graph <= 2 &&
            (s.factor_streams == 1 || s.factor_streams == 2 || s.factor_streams == 4) && s.unit_factor >= 0 &&
            s.unit_factor <= 3 &&
-           bit(s.block_inverse) && bit(s.tensor_trailing) && (s.gmres_ctas_per_sm == 3 || s.gmres_ctas_per_sm == 4);
+           bit(s.block_inverse) && s.tensor_trailing >= 0 && s.tensor_trailing <= 2 &&
+           (s.gmres_ctas_per_sm == 3 || s.gmres_ctas_per_sm == 4);
 }
 
 // Make the batch launch as s says (s valid); drops a captured graph when
@@ -2111,7 +2127,8 @@ static void apply_schedule(fnec_batch *b, const fnec_schedule &s) {
     b->grid.factor_streams = t.factor_streams;
     b->grid.unit_factor = t.unit_factor;
     b->mixed.use_binv = t.block_inverse != 0;
-    b->mixed.use_tc_trail = t.tensor_trailing != 0;
+    b->mixed.use_tc_trail = t.tensor_trailing == 1;
+    b->mixed.two_step = t.tensor_trailing == 2;
     b->mixed.gmres_minb = t.gmres_ctas_per_sm;
 }
 
@@ -2252,7 +2269,8 @@ int fnec_batch_tune(fnec_batch *b, uint32_t reps, fnec_tune_report *out) {
     };
     std::vector<Knob> knobs;
     const bool mixed = b->precision == FNEC_PRECISION_MIXED;
-    if (mixed && b->mixed.trail) knobs.push_back({&fnec_schedule::tensor_trailing, {0, 1}});
+    if (mixed) knobs.push_back(b->mixed.trail ? Knob{&fnec_schedule::tensor_trailing, {0, 1, 2}}
+                                              : Knob{&fnec_schedule::tensor_trailing, {0, 2}});
     if (mixed && b->mixed.tc) knobs.push_back({&fnec_schedule::gram_tensor, {1, 0}});
     if (mixed && b->mixed.cluster_max > 1) {
         std::vector<int32_t> c;

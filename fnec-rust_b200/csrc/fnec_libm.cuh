@@ -58,9 +58,12 @@
 
 namespace fnec_libm {
 
-// sin(i/128) hi, lo, cos(i/128) hi, lo for i = 0..109
+// sin(i/128) hi, lo, cos(i/128) hi, lo for i = 0..109.  The device copy
+// lives in global memory and is read through the read-only cache: the lanes
+// of a warp index it with different points, which the constant cache would
+// serialise.
 #ifdef __CUDACC__
-static __device__ __constant__ const double libm_sincos_tab_dev[440] = {
+static __device__ const double libm_sincos_tab_dev[440] = {
 #include "libm_tables.inc"
 };
 #endif
@@ -73,7 +76,7 @@ static const double libm_sincos_tab_host[440] = {
 #define LM_MUL(a, b) __dmul_rn((a), (b))
 #define LM_ADD(a, b) __dadd_rn((a), (b))
 #define LM_SUB(a, b) __dsub_rn((a), (b))
-#define LM_TAB(i) libm_sincos_tab_dev[i]
+#define LM_TAB(i) __ldg(&libm_sincos_tab_dev[i])
 #else
 #define LM_FMA(a, b, c) fma((a), (b), (c))
 #define LM_MUL(a, b) ((a) * (b))
@@ -231,27 +234,46 @@ FNEC_LIBM_FN double libm_cos(double x) {
 }
 
 // (libm_sin(x), libm_cos(x)) with the branch and the reduction shared:
-// glibc's sincos returns the same two values as sin and cos.
+// glibc's sincos returns the same two values as sin and cos.  Every branch
+// evaluates one do_sin and one do_cos; only their arguments differ, so the
+// branch picks arguments and the two evaluations run once for all lanes of
+// a warp whose arguments fall in different branches.
 FNEC_LIBM_FN void libm_sincos(double x, double *s, double *c) {
     uint32_t k = (uint32_t)(lm_bits(x) >> 32) & 0x7fffffffu;
-    if (k < 0x3feb6000u) {
-        *s = k < 0x3e500000u ? x : lm_do_sin(x, 0.0);
-        *c = k < 0x3e400000u ? 1.0 : lm_do_cos(x, 0.0);
-    } else if (k < 0x400368fdu) {
+    double as, das, ac, dac;
+    int mode, n = 0;
+    if (k < 0x3feb6000u) {  // |x| < 0.855469: the table around x itself
+        as = ac = x;
+        das = dac = 0.0;
+        mode = 0;
+    } else if (k < 0x400368fdu) {  // |x| < 2.426265: taken from pi/2
         double y = LM_SUB(LM_HP0, fabs(x));
-        *s = lm_copysign(lm_do_cos(y, LM_HP1), x);
-        double a = LM_ADD(y, LM_HP1);
-        double da = LM_ADD(LM_SUB(y, a), LM_HP1);
-        *c = lm_do_sin(a, da);
-    } else if (k < 0x419921fbu) {
+        ac = y;  // sin x = copysign(cos(y + hp1), x)
+        dac = LM_HP1;
+        as = LM_ADD(y, LM_HP1);  // cos x = sin(a + da)
+        das = LM_ADD(LM_SUB(y, as), LM_HP1);
+        mode = 1;
+    } else if (k < 0x419921fbu) {  // x - n pi/2
         double a, da;
-        int n = lm_reduce(x, &a, &da);
-        double ds = lm_do_sin(a, da), dc = lm_do_cos(a, da);
-        double sv = (n & 1) ? dc : ds, cv = (n & 1) ? ds : dc;
-        *s = (n & 2) ? -sv : sv;
-        *c = ((n + 1) & 2) ? -cv : cv;
+        n = lm_reduce(x, &a, &da);
+        as = ac = a;
+        das = dac = da;
+        mode = 2;
     } else {
         *s = *c = x - x + NAN;
+        return;
+    }
+    const double sp = lm_do_sin(as, das), cp = lm_do_cos(ac, dac);
+    if (mode == 0) {
+        *s = k < 0x3e500000u ? x : sp;
+        *c = k < 0x3e400000u ? 1.0 : cp;
+    } else if (mode == 1) {
+        *s = lm_copysign(cp, x);
+        *c = sp;
+    } else {
+        double sv = (n & 1) ? cp : sp, cv = (n & 1) ? sp : cp;
+        *s = (n & 2) ? -sv : sv;
+        *c = ((n + 1) & 2) ? -cv : cv;
     }
 }
 

@@ -117,11 +117,19 @@ __device__ __forceinline__ cx elem_fast(const double *om, const double *od, cons
     return {ire * cos_alpha, iim * cos_alpha};
 }
 
-__global__ void __launch_bounds__(256) k_fill_fast(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
+// One CTA of 256 threads fills a 16x16 tile of one unit's Z.  With gu set
+// it also writes the tile into the tensor-core Gram's operand stacks --
+// T[2c+s][k] = (Re, Im) Z[k][c] as tf32 hi/lo pairs, K-blocked (k_split_gram's
+// layout and rounding) -- through a shared-memory transpose, so the Gram
+// does not read Z back for them.  The stacks' padding is zero from their
+// allocation and never written.
+__global__ void __launch_bounds__(256, 4) k_fill_fast(const UnitDesc *__restrict__ units, const AntDesc *__restrict__ ants,
                                                    const DevSeg *__restrict__ segs, const int4 *__restrict__ tiles,
-                                                   cx *zbuf) {
+                                                   cx *zbuf, const TcGramUnit *__restrict__ gu, float *ghi,
+                                                   float *glo) {
     __shared__ DevSeg s_obs[16];
     __shared__ DevSeg s_src[16];
+    __shared__ cx s_z[16][17];
     int4 t = tiles[blockIdx.x];
     UnitDesc u = units[t.x];
     AntDesc a = ants[u.ant];
@@ -133,16 +141,34 @@ __global__ void __launch_bounds__(256) k_fill_fast(const UnitDesc *__restrict__ 
     __syncthreads();
     int ii = tid / 16, jj = tid % 16;
     int i = t.y + ii, j = t.z + jj;
-    if (i >= n || j >= n) return;
-    const DevSeg &o = s_obs[ii], &s = s_src[jj];
-    cx z = elem_fast(o.mid, o.dir, s.mid, s.dir, s.len, s.rad, u.k_fill, i == j);
-    if (a.ground == 1) {
-        double im_mid[3] = {s.mid[0], s.mid[1], -s.mid[2]};
-        double im_dir[3] = {-s.dir[0], -s.dir[1], s.dir[2]};
-        cx g = elem_fast(o.mid, o.dir, im_mid, im_dir, s.len, s.rad, u.k_fill, false);
-        z = zadd(z, g);
+    if (i < n && j < n) {
+        const DevSeg &o = s_obs[ii], &s = s_src[jj];
+        cx z = elem_fast(o.mid, o.dir, s.mid, s.dir, s.len, s.rad, u.k_fill, i == j);
+        if (a.ground == 1) {
+            double im_mid[3] = {s.mid[0], s.mid[1], -s.mid[2]};
+            double im_dir[3] = {-s.dir[0], -s.dir[1], s.dir[2]};
+            cx g = elem_fast(o.mid, o.dir, im_mid, im_dir, s.len, s.rad, u.k_fill, false);
+            z = zadd(z, g);
+        }
+        zbuf[u.z_off + (int64_t)i * n + j] = z;
+        s_z[ii][jj] = z;
     }
-    zbuf[u.z_off + (int64_t)i * n + j] = z;
+    if (!gu) return;  // block-uniform
+    __syncthreads();
+    const TcGramUnit g = gu[t.x];
+    // 32 stack rows (2 jj + s) of 16 consecutive k = t.y + kk each
+#pragma unroll
+    for (int e = tid; e < 32 * 16; e += 256) {
+        const int rr = e / 16, kk = e % 16;
+        const int jc = t.z + rr / 2, ik = t.y + kk;
+        if (ik >= n || jc >= n) continue;
+        const cx v = s_z[kk][rr / 2];
+        float h, l;
+        split_tf32((float)((rr & 1) ? v.im : v.re), h, l);
+        const int64_t o = ((int64_t)g.base + (int64_t)(ik / 32) * g.rpad + 2 * jc + (rr & 1)) * 32 + (ik % 32);
+        ghi[o] = h;
+        glo[o] = l;
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -419,22 +445,25 @@ __device__ bool panel32_body(float2 *A, int s, int c0, int32_t *piv, int32_t *st
             s_pan32[(p - c0) * PS + tid] = t0;
         }
         __syncthreads();
-        const float2 pj = lane < nb ? s_pan32[lc * PS + lane] : cf(0.f, 0.f);
-        const float2 diag = s_pan32[lc * PS + lc];
+        const float2 *prow = s_pan32 + lc * PS;  // the pivot row, read by broadcast
+        const float2 diag = prow[lc];
         const float dn = 1.0f / (diag.x * diag.x + diag.y * diag.y);
         const float2 dinv = cf(diag.x * dn, -diag.y * dn);
         const int nx = lc + 1;
         bv = -1.f;
         bi = -1;
-#pragma unroll 4
-        for (int r = c + 1 + wid; r < s; r += nw) {
+        // a thread per row: its multiplier, then its remaining panel entries
+        // in column order (the row's entries sit 33 float2 apart from the
+        // next row's, an odd stride: a warp's accesses are conflict-free)
+        for (int r = c + 1 + tid; r < s; r += NT) {
             float2 *row = s_pan32 + (r - c0) * PS;
-            float2 x = lane < nb ? row[lane] : cf(0.f, 0.f);
-            float2 f = cf_mul(make_float2(__shfl_sync(0xffffffffu, x.x, lc), __shfl_sync(0xffffffffu, x.y, lc)), dinv);
-            float2 y = cf_sub(x, cf_mul(f, pj));
-            if (lane == lc) row[lc] = f;
-            else if (lane > lc && lane < nb) row[lane] = y;
-            if (nx < nb) piv_better32(bv, bi, __shfl_sync(0xffffffffu, y.x * y.x + y.y * y.y, nx), r);
+            const float2 f = cf_mul(row[lc], dinv);
+            row[lc] = f;
+            for (int k = lc + 1; k < nb; ++k) row[k] = cf_sub(row[k], cf_mul(f, prow[k]));
+            if (nx < nb) {
+                const float2 y = row[nx];
+                piv_better32(bv, bi, y.x * y.x + y.y * y.y, r);
+            }
         }
         // no barrier here: the next column's first barrier orders these
         // writes before its swap, and s_v is rewritten only after this
@@ -622,10 +651,17 @@ __global__ void __launch_bounds__(256) k_panel32_grid(const UnitDesc *__restrict
                                              (int)blockIdx.x, s_gpan32);
 }
 
+// defer: the previous step's update (columns c0 - 32 .. c0 of L, rows of
+// U) is still owed by the trailing columns of this panel's rows (the
+// second step of a two-step pair): it is applied to them after the swaps,
+// before U12 is solved.
+// Columns idx in [lo, hi) of the columns outside the panel (idx < c0: the
+// column idx; else idx + nb), 64 per CTA: hi < 0 means all of them.
 __global__ void __launch_bounds__(64) k_swap_u12_32(const UnitDesc *__restrict__ units,
                                                     const MixedUnit *__restrict__ mus, int c0, float2 *a32buf,
                                                     const int32_t *__restrict__ piv_buf,
-                                                    const int32_t *__restrict__ status, const int32_t *__restrict__ order, int base) {
+                                                    const int32_t *__restrict__ status, const int32_t *__restrict__ order, int base,
+                                                    int defer, int lo, int hi) {
     __shared__ float2 s_c[MNB][64];
     __shared__ float2 s_L[MNB][MNB + 1];
     int ui = order[base + blockIdx.y];
@@ -634,10 +670,11 @@ __global__ void __launch_bounds__(64) k_swap_u12_32(const UnitDesc *__restrict__
     if (c0 >= s || status[ui] != 0) return;
     int nb = min(MNB, s - c0);
     int t = threadIdx.x;
-    int idx = blockIdx.x * 64 + t;
-    if (blockIdx.x * 64 >= s - nb) return;
+    const int end = hi < 0 ? s - nb : min(hi, s - nb);
+    int idx = lo + blockIdx.x * 64 + t;
+    if (lo + (int)blockIdx.x * 64 >= end) return;
     int K = idx < c0 ? idx : idx + nb;  // skip the panel columns
-    bool live = K < s;
+    bool live = idx < end;
     bool trailing = K >= c0 + nb;
     float2 *A = a32buf + mus[ui].a32_off;
     const int32_t *piv = piv_buf + u.piv_off;
@@ -658,6 +695,20 @@ __global__ void __launch_bounds__(64) k_swap_u12_32(const UnitDesc *__restrict__
             A[(int64_t)p * s + K] = t0;
         }
     }
+    if (trailing && defer) {
+        // the deferred update, on the swapped rows: L rows from columns
+        // c0 - 32 .. c0 of this panel's rows, U from rows c0 - 32 .. c0
+        for (int q = 0; q < nb; ++q) {
+            float2 v = s_c[q][t];
+            for (int c = 0; c < MNB; ++c) {
+                const float2 l = A[(int64_t)(c0 + q) * s + c0 - MNB + c];
+                const float2 uu = A[(int64_t)(c0 - MNB + c) * s + K];
+                v.x = fmaf(-l.x, uu.x, fmaf(l.y, uu.y, v.x));
+                v.y = fmaf(-l.x, uu.y, fmaf(-l.y, uu.x, v.y));
+            }
+            s_c[q][t] = v;
+        }
+    }
     if (trailing)
         for (int q = 1; q < nb; ++q) {
             float2 v = s_c[q][t];
@@ -667,30 +718,34 @@ __global__ void __launch_bounds__(64) k_swap_u12_32(const UnitDesc *__restrict__
     for (int q = 0; q < nb; ++q) A[(int64_t)(c0 + q) * s + K] = s_c[q][t];
 }
 
+// A22 -= L21 U12 over kparts consecutive 32-column steps starting at c0
+// (L21: columns c0 .. c0 + 32 kparts, U12: the same rows), on rows and
+// columns from r0 = c0 + 32 kparts up to col_end (columns) and s (rows);
+// 64x64 tiles, a 4x4 complex block per thread, the parts' products
+// accumulated in registers so A22 is read and written once.  kparts 1,
+// col_end s: the one-step update; kparts 1, col_end c0 + 64: the next
+// panel's columns only (the look-ahead of a two-step pair); kparts 2: the
+// pair's deferred update of everything to the right and below.
 __global__ void __launch_bounds__(256) k_trailing32(const UnitDesc *__restrict__ units, const MixedUnit *__restrict__ mus,
-                                                    int c0, float2 *a32buf, const int32_t *__restrict__ status, const int32_t *__restrict__ order, int base) {
+                                                    int c0, float2 *a32buf, const int32_t *__restrict__ status,
+                                                    const int32_t *__restrict__ order, int base, int kparts,
+                                                    int col_end) {
     __shared__ float2 s_l[64][MNB + 1];
     __shared__ float2 s_u[MNB][64];
     int ui = order[base + blockIdx.y];
     UnitDesc u = units[ui];
     int s = u.s;
-    if (c0 + MNB >= s || status[ui] != 0) return;
-    int r0 = c0 + MNB, rows = s - r0, cols = s - r0;
+    int r0 = c0 + MNB * kparts;
+    if (r0 >= s || status[ui] != 0) return;
+    const int ce = min(s, col_end);
+    if (ce <= r0) return;
+    int rows = s - r0, cols = ce - r0;
     int tiles_c = (cols + 63) / 64, tiles_r = (rows + 63) / 64;
     int tile = blockIdx.x;
     if (tile >= tiles_r * tiles_c) return;
     int R0 = r0 + (tile / tiles_c) * 64, K0 = r0 + (tile % tiles_c) * 64;
     float2 *A = a32buf + mus[ui].a32_off;
     int tid = threadIdx.x;
-    for (int e = tid; e < 64 * MNB; e += 256) {
-        int rr = e / MNB, q = e % MNB, R = R0 + rr;
-        s_l[rr][q] = (R < s) ? A[(int64_t)R * s + c0 + q] : cf(0.f, 0.f);
-    }
-    for (int e = tid; e < MNB * 64; e += 256) {
-        int q = e / 64, cc = e % 64, K = K0 + cc;
-        s_u[q][cc] = (K < s) ? A[(int64_t)(c0 + q) * s + K] : cf(0.f, 0.f);
-    }
-    __syncthreads();
     int ty = tid / 16, tx = tid % 16;
     float2 acc[4][4];
 #pragma unroll
@@ -698,29 +753,42 @@ __global__ void __launch_bounds__(256) k_trailing32(const UnitDesc *__restrict__
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             int R = R0 + ty + 16 * a, K = K0 + tx + 16 * b;
-            acc[a][b] = (R < s && K < s) ? A[(int64_t)R * s + K] : cf(0.f, 0.f);
+            acc[a][b] = (R < s && K < ce) ? A[(int64_t)R * s + K] : cf(0.f, 0.f);
         }
+    for (int part = 0; part < kparts; ++part) {
+        const int cp = c0 + MNB * part;
+        if (part) __syncthreads();  // the previous part's reads of s_l / s_u are done
+        for (int e = tid; e < 64 * MNB; e += 256) {
+            int rr = e / MNB, q = e % MNB, R = R0 + rr;
+            s_l[rr][q] = (R < s) ? A[(int64_t)R * s + cp + q] : cf(0.f, 0.f);
+        }
+        for (int e = tid; e < MNB * 64; e += 256) {
+            int q = e / 64, cc = e % 64, K = K0 + cc;
+            s_u[q][cc] = (K < ce) ? A[(int64_t)(cp + q) * s + K] : cf(0.f, 0.f);
+        }
+        __syncthreads();
 #pragma unroll 4
-    for (int q = 0; q < MNB; ++q) {
-        float2 lv[4], uv[4];
+        for (int q = 0; q < MNB; ++q) {
+            float2 lv[4], uv[4];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) lv[a] = s_l[ty + 16 * a][q];
+            for (int a = 0; a < 4; ++a) lv[a] = s_l[ty + 16 * a][q];
 #pragma unroll
-        for (int b = 0; b < 4; ++b) uv[b] = s_u[q][tx + 16 * b];
+            for (int b = 0; b < 4; ++b) uv[b] = s_u[q][tx + 16 * b];
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+            for (int a = 0; a < 4; ++a)
 #pragma unroll
-            for (int b = 0; b < 4; ++b) {
-                acc[a][b].x = fmaf(-lv[a].x, uv[b].x, fmaf(lv[a].y, uv[b].y, acc[a][b].x));
-                acc[a][b].y = fmaf(-lv[a].x, uv[b].y, fmaf(-lv[a].y, uv[b].x, acc[a][b].y));
-            }
+                for (int b = 0; b < 4; ++b) {
+                    acc[a][b].x = fmaf(-lv[a].x, uv[b].x, fmaf(lv[a].y, uv[b].y, acc[a][b].x));
+                    acc[a][b].y = fmaf(-lv[a].x, uv[b].y, fmaf(-lv[a].y, uv[b].x, acc[a][b].y));
+                }
+        }
     }
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             int R = R0 + ty + 16 * a, K = K0 + tx + 16 * b;
-            if (R < s && K < s) A[(int64_t)R * s + K] = acc[a][b];
+            if (R < s && K < ce) A[(int64_t)R * s + K] = acc[a][b];
         }
 }
 
@@ -769,6 +837,7 @@ __device__ double block_sum(double v, double *red) {
 // the column sums M^H t (a thread per column), so the second use of every
 // row costs no HBM traffic.
 constexpr int ARB = 16;  // rows per block (2 per warp)
+
 __device__ void apply_A(const GmresCtx &g, const cx *v, cx *out, cx *sv, cx *st, cx *so) {
     int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int n = g.n;
@@ -2032,6 +2101,15 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
                 return cudaErrorNotSupported;  // no tensor-map encoder in this driver
             }
             for (const UnitDesc &u : systems) w.tc_max_n = std::max(w.tc_max_n, u.n);
+            // the fill may write the stacks (one gram entry per system, same
+            // index); their padding must then be zero once and for all
+            w.tc_fusable = p->units.size() == systems.size();
+            for (size_t q = 0; w.tc_fusable && q < p->units.size(); ++q) w.tc_fusable = p->units[q].unit == (int)q;
+            if (w.tc_fusable) e = cudaMemsetAsync(w.tc_hi, 0, 2 * al(b_st), dev.st);
+            if (e != cudaSuccess) {
+                delete p;
+                return e;
+            }
             w.tc = p;
         } else {
             delete p;
@@ -2220,8 +2298,13 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         if (!marks.failed_phase && cudaPeekAtLastError() != cudaSuccess) marks.failed_phase = phase_name[k];
         if (marks.ev) cudaEventRecord(marks.ev[k], st);
     };
+    // the fill writes the Gram's tf32 operand stacks itself when the Gram
+    // runs on the tensor cores and no stamp changes Z after the fill
+    const bool fused_split = do_fill && n_fill > 0 && mw.tc && mw.use_tc && mw.tc_fusable && n_stamps == 0;
     if (do_fill && n_fill > 0) {
-        k_fill_fast<<<n_fill, 256, 0, st>>>(d_units, d_ants, d_segs, fill_tiles, z);
+        k_fill_fast<<<n_fill, 256, 0, st>>>(d_units, d_ants, d_segs, fill_tiles, z,
+                                            fused_split ? static_cast<const TcGramUnit *>(mw.tc_gu) : nullptr,
+                                            mw.tc_hi, mw.tc_lo);
         ++L;
         if (n_stamps > 0) {  // LD loads on the diagonal, before Z is used
             launch_stamps(stamps, n_stamps, z, st);
@@ -2231,7 +2314,7 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     mark(0);
     if (mw.tc && mw.use_tc) {
         tc_gram_run(*mw.tc, d_units, static_cast<const TcGramUnit *>(mw.tc_gu), static_cast<const TcTile *>(mw.tc_tiles),
-                    mw.smu, z, mw.tc_hi, mw.tc_lo, mw.a32, status, mw.tc_max_n, st);
+                    mw.smu, z, mw.tc_hi, mw.tc_lo, mw.a32, status, mw.tc_max_n, st, !fused_split);
         ++L;
     } else if (n_gram > 0) {
         k_gram32_zz<<<n_gram, 256, 0, st>>>(d_units, mw.smu, gram_tiles, z, mw.a32);
@@ -2295,6 +2378,7 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         ++L;
     }
     std::vector<StepClass> cls;
+    const bool two_step = mw.two_step && !(mw.trail && mw.use_tc_trail);
     for (int grp = 0; grp < G && i_unit > 0; ++grp) {
     const int gi0 = gb[grp], gi1 = gb[grp + 1];
     cudaStream_t fs = grp == 0 ? st : mw.fstream[grp - 1];
@@ -2334,12 +2418,30 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
                                                                  ord, c.i0);
             ++L;
         }
+        // Two-step pairs (two_step): the first step of a pair updates only
+        // the next panel's 32 columns (look-ahead); the second step's swaps
+        // run first on the L columns, then its trailing columns take the
+        // owed update of the first step before U12 is solved, and one
+        // trailing pass applies both steps (K = 64), reading and writing
+        // A22 once per pair instead of once per step.
+        const bool pair_first = two_step && (c0 / MNB) % 2 == 0;
+        const bool pair_second = two_step && (c0 / MNB) % 2 == 1;
         step_classes(gp, c0, gi0, cls, gi1);
         for (const StepClass &c : cls) {
             int m = c.m_max;
-            dim3 g1((m + c0 + 63) / 64, c.i1 - c.i0);  // every column outside the panel
-            k_swap_u12_32<<<g1, 64, 0, fs>>>(d_units, mw.smu, c0, mw.a32, piv, status, ord, c.i0);
-            ++L;
+            if (pair_second) {
+                // the L columns first (the owed update reads them swapped) ...
+                dim3 ga((c0 + 63) / 64, c.i1 - c.i0);
+                k_swap_u12_32<<<ga, 64, 0, fs>>>(d_units, mw.smu, c0, mw.a32, piv, status, ord, c.i0, 0, 0, c0);
+                // ... then the trailing columns with the owed update and U12
+                dim3 gt((m + 63) / 64, c.i1 - c.i0);
+                k_swap_u12_32<<<gt, 64, 0, fs>>>(d_units, mw.smu, c0, mw.a32, piv, status, ord, c.i0, 1, c0, -1);
+                L += 2;
+            } else {
+                dim3 g1((m + c0 + 63) / 64, c.i1 - c.i0);  // every column outside the panel
+                k_swap_u12_32<<<g1, 64, 0, fs>>>(d_units, mw.smu, c0, mw.a32, piv, status, ord, c.i0, 0, 0, -1);
+                ++L;
+            }
         }
         // trailing updates: the largest units' on the tensor cores (a prefix
         // of the order, in the first group), the rest as FP32 SIMT tiles
@@ -2349,12 +2451,20 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         step_classes(gp, c0, std::max(gi0, k_tc), cls, gi1);
         for (const StepClass &c : cls) {
             int rows = c.m_max - MNB;
-            if (rows > 0) {
+            if (rows <= 0) continue;
+            if (pair_first) {  // the next panel's columns only
+                dim3 g2((rows + 63) / 64, c.i1 - c.i0);
+                k_trailing32<<<g2, 256, 0, fs>>>(d_units, mw.smu, c0, mw.a32, status, ord, c.i0, 1, c0 + 2 * MNB);
+            } else if (pair_second) {  // both steps of the pair, from the pair's first column
                 int t = ((rows + 63) / 64) * ((rows + 63) / 64);
                 dim3 g2(t, c.i1 - c.i0);
-                k_trailing32<<<g2, 256, 0, fs>>>(d_units, mw.smu, c0, mw.a32, status, ord, c.i0);
-                ++L;
+                k_trailing32<<<g2, 256, 0, fs>>>(d_units, mw.smu, c0 - MNB, mw.a32, status, ord, c.i0, 2, INT_MAX);
+            } else {
+                int t = ((rows + 63) / 64) * ((rows + 63) / 64);
+                dim3 g2(t, c.i1 - c.i0);
+                k_trailing32<<<g2, 256, 0, fs>>>(d_units, mw.smu, c0, mw.a32, status, ord, c.i0, 1, INT_MAX);
             }
+            ++L;
         }
         if (k_tc > 0) {
             tc_trail_run(*mw.trail, c0 / MNB, k_tc, static_cast<const TcTrailUnit *>(mw.d_trail), d_units, mw.smu, mw.a32,

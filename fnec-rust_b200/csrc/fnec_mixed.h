@@ -73,6 +73,7 @@ struct MixedWork {
     float *tc_hi = nullptr, *tc_lo = nullptr;
     void *tc_gu = nullptr, *tc_tiles = nullptr;
     int tc_max_n = 0;
+    bool tc_fusable = false;  // the fill can write the Gram's operand stacks (k_fill_fast)
     // the factor's trailing updates of the largest units on the tensor cores
     TcTrailPlan *trail = nullptr;
     void *trail_base = nullptr;
@@ -80,6 +81,7 @@ struct MixedWork {
     void *d_trail = nullptr;  // TcTrailUnit per (step, unit)
     int trail_n = 0;          // units (a prefix of the s-descending order) it covers
     bool use_tc_trail = false; // the tuner picks it
+    bool two_step = false;     // SIMT trailing updates once per two steps (look-ahead of the next panel)
 };
 
 // Phase events the mixed path records after its fill, Gram, factor and

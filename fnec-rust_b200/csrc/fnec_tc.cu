@@ -322,17 +322,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                                                                  FNEC_UNIT_TIMEOUT);
 }
 
-// -- operand preparation -----------------------------------------------------
-// x = hi + lo with both parts tf32 values, each rounded to nearest: the
-// tensor core then uses lo as given (it would otherwise drop lo's low 13
-// bits), so x is carried to ~2^-23 relative instead of ~2^-22.
-__device__ __forceinline__ void split_tf32(float x, float &hi, float &lo) {
-    uint32_t h, l;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
-    hi = __uint_as_float(h);
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(x - hi));
-    lo = __uint_as_float(l);
-}
+// -- operand preparation (split_tf32: fnec_tc.h) -----------------------------
 
 // Row-major FP32 [rows][k] -> K-blocked hi/lo stacks (zero padded to
 // kblocks * 32 columns and rpad rows per k-block).
@@ -584,11 +574,13 @@ bool tc_gram_maps(TcGramPlan &p, const float *hi, const float *lo) {
 
 cudaError_t tc_gram_run(const TcGramPlan &p, const UnitDesc *d_units, const TcGramUnit *d_gu, const TcTile *d_tiles,
                         const MixedUnit *d_mus, const cx *z, float *hi, float *lo, float2 *a32, int32_t *status,
-                        int max_n, cudaStream_t st) {
+                        int max_n, cudaStream_t st, bool split) {
     if (p.units.empty()) return cudaSuccess;
-    int max_kb = (max_n + 31) / 32, max_cb = (max_n + 15) / 16;
-    dim3 g(max_cb, max_kb, (unsigned)p.units.size());
-    k_split_gram<<<g, 256, 0, st>>>(d_units, d_gu, z, hi, lo);
+    if (split) {  // else the fill has written the stacks
+        int max_kb = (max_n + 31) / 32, max_cb = (max_n + 15) / 16;
+        dim3 g(max_cb, max_kb, (unsigned)p.units.size());
+        k_split_gram<<<g, 256, 0, st>>>(d_units, d_gu, z, hi, lo);
+    }
     TcEpilogue ep{};
     ep.units = d_units;
     ep.mus = d_mus;

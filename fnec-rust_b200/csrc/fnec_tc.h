@@ -9,6 +9,17 @@
 
 namespace fnec {
 
+// x = hi + lo with both parts tf32 values, each rounded to nearest: the
+// tensor core then uses lo as given (it would otherwise drop lo's low 13
+// bits), so x is carried to ~2^-23 relative instead of ~2^-22.
+__device__ __forceinline__ void split_tf32(float x, float &hi, float &lo) {
+    uint32_t h, l;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(x));
+    hi = __uint_as_float(h);
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(x - hi));
+    lo = __uint_as_float(l);
+}
+
 constexpr int TC_EPI_STORE = 0;  // C[R][C] = D (row-major FP32), bounds m x n
 constexpr int TC_EPI_GRAM = 1;   // complex Gram combine into the unit's A32
 constexpr int TC_EPI_TRAIL = 2;  // A22 -= L21 U12 of one factor step, into the unit's A32
@@ -111,6 +122,6 @@ bool tc_gram_maps(TcGramPlan &p, const float *hi, const float *lo);
 // (its N x N block).
 cudaError_t tc_gram_run(const TcGramPlan &p, const UnitDesc *d_units, const TcGramUnit *d_gu, const TcTile *d_tiles,
                         const MixedUnit *d_mus, const cx *z, float *hi, float *lo, float2 *a32, int32_t *status,
-                        int max_n, cudaStream_t st);
+                        int max_n, cudaStream_t st, bool split = true);  // split false: the fill wrote the stacks
 
 }  // namespace fnec

@@ -973,10 +973,13 @@ class HallenBatch:
         self.ctx.check(lib().fnec_batch_set_sources(self._h, int(antenna), _ptr(arr) if len(arr) else None, len(arr)),
                        "batch_set_sources")
 
-    def resolve(self) -> BatchResult:
+    def resolve(self, read: bool = True):
         """Solve every unit again on the resident factorisations with the
-        current sources (fnec_batch_resolve) and read the results."""
+        current sources (fnec_batch_resolve); read=True waits and returns the
+        results, read=False only enqueues the work on the batch's stream."""
         self.ctx.check(lib().fnec_batch_resolve(self._h), "batch_resolve")
+        if not read:
+            return None
         self.sync()
         return self.read()
 

@@ -670,7 +670,9 @@ typedef struct {
                               products); 0 by substitution in one warp            */
     int32_t tensor_trailing;/* mixed: 1 trailing updates of >= 192 rows run on
                               tcgen05 (3xTF32, complex as one real GEMM of K 64);
-                              0 all as FP32 SIMT tiles                            */
+                              0 all as FP32 SIMT tiles, one pass per step; 2
+                              SIMT tiles once per two steps (the first step
+                              updates only the next panel's columns)            */
     int32_t gmres_ctas_per_sm;/* mixed: 3 or 4 refinement CTAs per SM (the
                               register budget of the one-CTA-per-solve kernel)    */
 } fnec_schedule;

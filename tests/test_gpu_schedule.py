@@ -98,7 +98,7 @@ def test_graph_capture_and_replay(acc, plain_ants):
 def test_schedule_rejects_out_of_range(acc, plain_ants):
     b = acc.HallenBatch(plain_ants[:2], precision=acc.PRECISION_FP64)
     for bad in ({"class_shift": 3}, {"gmres_cluster": 3}, {"graph": 5}, {"grid_panels": -1}, {"factor_streams": 3},
-                {"unit_factor": 4}, {"unit_factor": -1}, {"block_inverse": 5}, {"tensor_trailing": -1},
+                {"unit_factor": 4}, {"unit_factor": -1}, {"block_inverse": 5}, {"tensor_trailing": -1}, {"tensor_trailing": 3},
                 {"gmres_ctas_per_sm": 2}):
         with pytest.raises(acc.AccelError) as e:
             b.schedule = bad
@@ -115,6 +115,7 @@ def test_schedule_rejects_out_of_range(acc, plain_ants):
     {"unit_factor": 2}, {"unit_factor": 3, "factor_streams": 2},
     {"block_inverse": 0}, {"block_inverse": 1, "gmres_cluster": 4},
     {"tensor_trailing": 0}, {"tensor_trailing": 1, "factor_streams": 4, "unit_factor": 0},
+    {"tensor_trailing": 2}, {"tensor_trailing": 2, "factor_streams": 4, "unit_factor": 0},
     {"gmres_ctas_per_sm": 4}, {"gmres_ctas_per_sm": 4, "block_inverse": 0},
 ])
 def test_mixed_within_gate_under_every_schedule(acc, sched):
