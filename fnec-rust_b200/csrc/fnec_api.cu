@@ -743,7 +743,7 @@ struct fnec_batch {
     cudaEvent_t ev[FNEC_N_PHASES + 1] = {};
     bool ev_made = false;
     // schedule and its CUDA graph
-    fnec_schedule sched = {1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 3};
+    fnec_schedule sched = {1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 3, 0};
     cudaGraphExec_t gexec = nullptr;
     int graph_state = FNEC_GRAPH_NONE;
     uint64_t graph_launches = 0;  // launches the graph replays
@@ -2103,7 +2103,7 @@ static bool schedule_valid(const fnec_schedule &s) {
            (s.factor_streams == 1 || s.factor_streams == 2 || s.factor_streams == 4) && s.unit_factor >= 0 &&
            s.unit_factor <= 3 &&
            bit(s.block_inverse) && s.tensor_trailing >= 0 && s.tensor_trailing <= 2 &&
-           (s.gmres_ctas_per_sm == 3 || s.gmres_ctas_per_sm == 4);
+           (s.gmres_ctas_per_sm == 3 || s.gmres_ctas_per_sm == 4) && bit(s.factor_pivoting);
 }
 
 // Make the batch launch as s says (s valid); drops a captured graph when
@@ -2116,7 +2116,8 @@ static void apply_schedule(fnec_batch *b, const fnec_schedule &s) {
                                t.grid_gmres == b->sched.grid_gmres && t.factor_streams == b->sched.factor_streams &&
                                t.unit_factor == b->sched.unit_factor && t.block_inverse == b->sched.block_inverse &&
                                t.tensor_trailing == b->sched.tensor_trailing &&
-                               t.gmres_ctas_per_sm == b->sched.gmres_ctas_per_sm;
+                               t.gmres_ctas_per_sm == b->sched.gmres_ctas_per_sm &&
+                               t.factor_pivoting == b->sched.factor_pivoting;
     if (!same_launches || (t.graph == 0) != (b->sched.graph == 0)) drop_graph(b);
     b->sched = t;
     b->grid.grid_on = t.grid_panels != 0;
@@ -2130,6 +2131,7 @@ static void apply_schedule(fnec_batch *b, const fnec_schedule &s) {
     b->mixed.use_tc_trail = t.tensor_trailing == 1;
     b->mixed.two_step = t.tensor_trailing == 2;
     b->mixed.gmres_minb = t.gmres_ctas_per_sm;
+    b->mixed.pivoting = t.factor_pivoting != 0;
 }
 
 static int ceil_log2(int64_t v) {
@@ -2285,6 +2287,7 @@ int fnec_batch_tune(fnec_batch *b, uint32_t reps, fnec_tune_report *out) {
     if (mixed && b->mixed.fmade) knobs.push_back({&fnec_schedule::factor_streams, {1, 2, 4}});
     if (mixed) knobs.push_back({&fnec_schedule::block_inverse, {1, 0}});
     if (mixed) knobs.push_back({&fnec_schedule::gmres_ctas_per_sm, {3, 4}});
+    if (mixed) knobs.push_back({&fnec_schedule::factor_pivoting, {0, 1}});
     // two passes of coordinate descent: a field's best value can depend on
     // fields tuned after it
     for (int pass = 0; pass < 2; ++pass)
@@ -2317,15 +2320,15 @@ int fnec_batch_tune(fnec_batch *b, uint32_t reps, fnec_tune_report *out) {
     return FNEC_OK;
 }
 
-constexpr int N_SCHED_FIELDS = 11;
+constexpr int N_SCHED_FIELDS = 12;
 static const char *const SCHED_FIELDS[N_SCHED_FIELDS] = {"grid_panels",    "class_shift",   "gram_tensor",
                                                          "gmres_cluster",  "grid_gmres",    "graph",
                                                          "factor_streams", "unit_factor",   "block_inverse",
-                                                         "tensor_trailing", "gmres_ctas_per_sm"};
+                                                         "tensor_trailing", "gmres_ctas_per_sm", "factor_pivoting"};
 static int32_t *sched_field(fnec_schedule &s, int i) {
     int32_t *f[N_SCHED_FIELDS] = {&s.grid_panels,    &s.class_shift, &s.gram_tensor,   &s.gmres_cluster,
                                   &s.grid_gmres,     &s.graph,       &s.factor_streams, &s.unit_factor,
-                                  &s.block_inverse,  &s.tensor_trailing, &s.gmres_ctas_per_sm};
+                                  &s.block_inverse,  &s.tensor_trailing, &s.gmres_ctas_per_sm, &s.factor_pivoting};
     return f[i];
 }
 
@@ -2355,7 +2358,7 @@ int fnec_tune_cache_load(const char *path) {
         char *tok = strtok_r(line, " \t\r\n", &save);
         if (!tok || tok[0] == '#') continue;
         std::string key = tok;
-        fnec_schedule s = {1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 3};
+        fnec_schedule s = {1, 1, 1, 1, 1, 1, 1, 1, 1, 0, 3, 0};
         int seen = 0;
         while ((tok = strtok_r(nullptr, " \t\r\n", &save))) {
             char *eq = std::strchr(tok, '=');

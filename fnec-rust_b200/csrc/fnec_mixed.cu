@@ -664,6 +664,7 @@ __global__ void __launch_bounds__(64) k_swap_u12_32(const UnitDesc *__restrict__
                                                     int defer, int lo, int hi) {
     __shared__ float2 s_c[MNB][64];
     __shared__ float2 s_L[MNB][MNB + 1];
+    __shared__ float2 s_D[MNB][MNB + 1];  // defer: the owed step's L rows of this panel (swapped)
     int ui = order[base + blockIdx.y];
     UnitDesc u = units[ui];
     int s = u.s;
@@ -679,6 +680,8 @@ __global__ void __launch_bounds__(64) k_swap_u12_32(const UnitDesc *__restrict__
     float2 *A = a32buf + mus[ui].a32_off;
     const int32_t *piv = piv_buf + u.piv_off;
     for (int e = t; e < nb * nb; e += 64) s_L[e / nb][e % nb] = A[(int64_t)(c0 + e / nb) * s + c0 + e % nb];
+    if (defer)  // its L columns were swapped by the launch before this one
+        for (int e = t; e < nb * MNB; e += 64) s_D[e / MNB][e % MNB] = A[(int64_t)(c0 + e / MNB) * s + c0 - MNB + e % MNB];
     for (int q = 0; q < nb; ++q) s_c[q][t] = live ? A[(int64_t)(c0 + q) * s + K] : cf(0.f, 0.f);
     __syncthreads();
     if (!live) return;
@@ -697,14 +700,17 @@ __global__ void __launch_bounds__(64) k_swap_u12_32(const UnitDesc *__restrict__
     }
     if (trailing && defer) {
         // the deferred update, on the swapped rows: L rows from columns
-        // c0 - 32 .. c0 of this panel's rows, U from rows c0 - 32 .. c0
+        // c0 - 32 .. c0 of this panel's rows (s_D), U from rows c0 - 32 .. c0
+        float2 uc[MNB];
+#pragma unroll
+        for (int c = 0; c < MNB; ++c) uc[c] = A[(int64_t)(c0 - MNB + c) * s + K];
         for (int q = 0; q < nb; ++q) {
             float2 v = s_c[q][t];
+#pragma unroll
             for (int c = 0; c < MNB; ++c) {
-                const float2 l = A[(int64_t)(c0 + q) * s + c0 - MNB + c];
-                const float2 uu = A[(int64_t)(c0 - MNB + c) * s + K];
-                v.x = fmaf(-l.x, uu.x, fmaf(l.y, uu.y, v.x));
-                v.y = fmaf(-l.x, uu.y, fmaf(-l.y, uu.x, v.y));
+                const float2 l = s_D[q][c];
+                v.x = fmaf(-l.x, uc[c].x, fmaf(l.y, uc[c].y, v.x));
+                v.y = fmaf(-l.x, uc[c].y, fmaf(-l.y, uc[c].x, v.y));
             }
             s_c[q][t] = v;
         }
@@ -725,11 +731,21 @@ __global__ void __launch_bounds__(64) k_swap_u12_32(const UnitDesc *__restrict__
 // accumulated in registers so A22 is read and written once.  kparts 1,
 // col_end s: the one-step update; kparts 1, col_end c0 + 64: the next
 // panel's columns only (the look-ahead of a two-step pair); kparts 2: the
-// pair's deferred update of everything to the right and below.
+// pair's deferred update of everything to the right and below.  lower:
+// only the tiles on and below the diagonal (the Hermitian factor; kparts
+// 1, col_end s), T (T + 1) / 2 of them, row-major.
+__device__ __forceinline__ void lower_tile(int i, int &tr, int &tc) {
+    int r = (int)((sqrtf(8.f * (float)i + 1.f) - 1.f) * 0.5f);
+    while (r * (r + 1) / 2 > i) --r;
+    while ((r + 1) * (r + 2) / 2 <= i) ++r;
+    tr = r;
+    tc = i - r * (r + 1) / 2;
+}
+
 __global__ void __launch_bounds__(256) k_trailing32(const UnitDesc *__restrict__ units, const MixedUnit *__restrict__ mus,
                                                     int c0, float2 *a32buf, const int32_t *__restrict__ status,
                                                     const int32_t *__restrict__ order, int base, int kparts,
-                                                    int col_end) {
+                                                    int col_end, int lower) {
     __shared__ float2 s_l[64][MNB + 1];
     __shared__ float2 s_u[MNB][64];
     int ui = order[base + blockIdx.y];
@@ -742,8 +758,18 @@ __global__ void __launch_bounds__(256) k_trailing32(const UnitDesc *__restrict__
     int rows = s - r0, cols = ce - r0;
     int tiles_c = (cols + 63) / 64, tiles_r = (rows + 63) / 64;
     int tile = blockIdx.x;
-    if (tile >= tiles_r * tiles_c) return;
-    int R0 = r0 + (tile / tiles_c) * 64, K0 = r0 + (tile % tiles_c) * 64;
+    int R0, K0;
+    if (lower) {
+        if (tile >= tiles_r * (tiles_r + 1) / 2) return;
+        int tr, tc;
+        lower_tile(tile, tr, tc);
+        R0 = r0 + tr * 64;
+        K0 = r0 + tc * 64;
+    } else {
+        if (tile >= tiles_r * tiles_c) return;
+        R0 = r0 + (tile / tiles_c) * 64;
+        K0 = r0 + (tile % tiles_c) * 64;
+    }
     float2 *A = a32buf + mus[ui].a32_off;
     int tid = threadIdx.x;
     int ty = tid / 16, tx = tid % 16;
@@ -790,6 +816,204 @@ __global__ void __launch_bounds__(256) k_trailing32(const UnitDesc *__restrict__
             int R = R0 + ty + 16 * a, K = K0 + tx + 16 * b;
             if (R < s && K < ce) A[(int64_t)R * s + K] = acc[a][b];
         }
+}
+
+// ---------------------------------------------------------------------------
+// Hermitian factor without row exchanges (schedule factor_pivoting 0)
+// ---------------------------------------------------------------------------
+// A32 = M^H M + lambda I is Hermitian positive definite, so Gaussian
+// elimination needs no row exchanges, and its factor A = L U has
+// U = D L^H (D: the pivots).  Two consequences: the trailing update
+// A22 -= L21 U12 stays Hermitian, so only the tiles on and below the
+// diagonal are computed (the 32x32 diagonal blocks always lie inside
+// diagonal tiles, and nothing reads the stale entries above them); and
+// each step's U12 is its L21 mirrored, U12[q][K] = d_q conj(L21[K][q]),
+// written by the panel instead of a triangular solve.  The factor is
+// stored in the GEPP layout (unit-lower L below the diagonal, U on and
+// above it, identity pivots), so the refinement applies it unchanged.
+// A zero or non-finite pivot fails the unit as a singular GEPP panel does.
+
+// The nb x nb diagonal block at c0, factored in shared memory by all NT
+// threads (sD[r][k]; one barrier per column).  On return sD holds L11
+// (unit lower, below the diagonal) and U11, sDinv the pivots' reciprocals;
+// *s_bad the first failing column + 1, or 0.
+template <int NT>
+__device__ void herm_diag_block(const float2 *A, int s, int c0, int nb, float2 (*sD)[MNB + 1], float2 *sDinv,
+                                int *s_bad) {
+    const int tid = threadIdx.x;
+    for (int e = tid; e < nb * nb; e += NT) sD[e / nb][e % nb] = A[(int64_t)(c0 + e / nb) * s + c0 + e % nb];
+    if (tid == 0) *s_bad = 0;
+    for (int c = 0; c < nb; ++c) {
+        __syncthreads();  // column c - 1's update is complete
+        const float2 d = sD[c][c];
+        const float dn = d.x * d.x + d.y * d.y;
+        const float2 dinv = cf(d.x / dn, -d.y / dn);
+        if (tid == 0) {
+            sDinv[c] = dinv;
+            if ((!(dn > 0.f) || !(dn < INFINITY)) && *s_bad == 0) *s_bad = c + 1;
+        }
+        // column c - 1's multipliers (nobody reads that column in this pass)
+        if (c > 0 && tid >= c && tid < nb) sD[tid][c - 1] = cf_mul(sD[tid][c - 1], sDinv[c - 1]);
+        const int m = nb - 1 - c;
+        for (int e = tid; e < m * m; e += NT) {
+            const int r = c + 1 + e / m, k = c + 1 + e % m;
+            const float2 f = cf_mul(sD[r][c], dinv);
+            sD[r][k] = cf_sub(sD[r][k], cf_mul(f, sD[c][k]));
+        }
+    }
+    __syncthreads();
+}
+
+// Rows [r_begin, r_end) below a full (32-column) diagonal block: L21 row r
+// solves l U11 = A[r][c0 .. c0 + 32) (a thread per row, U11 read by
+// broadcast), then U12's column r is its mirror.  Two halves of 16
+// columns keep the live row in 16 complex registers: the second half
+// takes the first's contribution from its stored entries.
+template <int NT>
+__device__ void herm_rows(float2 *A, int s, int c0, int r_begin, int r_end, const float2 (*sD)[MNB + 1],
+                          const float2 *sDinv) {
+    constexpr int H = MNB / 2;
+    for (int r = r_begin + (int)threadIdx.x; r < r_end; r += NT) {
+        float2 *row = A + (int64_t)r * s + c0;
+#pragma unroll 1
+        for (int h = 0; h < 2; ++h) {
+            const int o = h * H;
+            float2 a[H];
+#pragma unroll
+            for (int q = 0; q < H; ++q) a[q] = row[o + q];
+            if (h) {
+#pragma unroll 4
+                for (int c = 0; c < H; ++c) {
+                    const float2 l = row[c];
+#pragma unroll
+                    for (int k = 0; k < H; ++k) a[k] = cf_sub(a[k], cf_mul(l, sD[c][o + k]));
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < H; ++c) {
+                a[c] = cf_mul(a[c], sDinv[o + c]);
+#pragma unroll
+                for (int k = c + 1; k < H; ++k) a[k] = cf_sub(a[k], cf_mul(a[c], sD[o + c][o + k]));
+            }
+#pragma unroll
+            for (int q = 0; q < H; ++q) {
+                row[o + q] = a[q];
+                const float2 d = sD[o + q][o + q];
+                A[(int64_t)(c0 + o + q) * s + r] = cf(d.x * a[q].x + d.y * a[q].y, d.y * a[q].x - d.x * a[q].y);
+            }
+        }
+    }
+}
+
+// The panel step at c0 of every unit of a size class, one CTA of NT
+// threads per unit (1024 for panels of more than 256 rows below the
+// diagonal block): the diagonal block, then every row below it.
+template <int NT>
+__global__ void __launch_bounds__(NT) k_panel32_herm(const UnitDesc *__restrict__ units,
+                                                    const MixedUnit *__restrict__ mus, int c0, float2 *a32buf,
+                                                    int32_t *piv_buf, int32_t *status,
+                                                    const int32_t *__restrict__ order, int base) {
+    __shared__ float2 sD[MNB][MNB + 1];
+    __shared__ float2 sDinv[MNB];
+    __shared__ int s_bad;
+    const int ui = order[base + blockIdx.x];
+    const UnitDesc u = units[ui];
+    const int s = u.s;
+    if (c0 >= s || status[ui] != 0) return;
+    const int nb = min(MNB, s - c0);
+    float2 *A = a32buf + mus[ui].a32_off;
+    herm_diag_block<NT>(A, s, c0, nb, sD, sDinv, &s_bad);
+    const int tid = threadIdx.x;
+    if (s_bad) {
+        if (tid == 0) status[ui] = -(c0 + s_bad);
+        return;
+    }
+    for (int e = tid; e < nb * nb; e += NT) A[(int64_t)(c0 + e / nb) * s + c0 + e % nb] = sD[e / nb][e % nb];
+    if (tid < nb) piv_buf[u.piv_off + c0 + tid] = c0 + tid;
+    if (nb == MNB) herm_rows<NT>(A, s, c0, c0 + MNB, s, sD, sDinv);
+}
+
+// The whole Hermitian factor of one small unit (S <= fu_max_s(level)) per
+// CTA: the per-step kernels' operations without a launch between steps.
+__global__ void __launch_bounds__(FU_THREADS, 3) k_factor32_unit_herm(const UnitDesc *__restrict__ units,
+                                                                     const MixedUnit *__restrict__ mus,
+                                                                     float2 *a32buf, int32_t *piv_buf,
+                                                                     int32_t *status,
+                                                                     const int32_t *__restrict__ order, int base) {
+    __shared__ float2 sD[MNB][MNB + 1];
+    __shared__ float2 sDinv[MNB];
+    __shared__ float2 s_l[64][MNB + 1];
+    __shared__ float2 s_u[MNB][64];
+    __shared__ int s_bad;
+    const int ui = order[base + blockIdx.x];
+    const UnitDesc u = units[ui];
+    const int s = u.s;
+    if (status[ui] != 0) return;
+    float2 *A = a32buf + mus[ui].a32_off;
+    const int tid = threadIdx.x;
+    for (int c0 = 0; c0 < s; c0 += MNB) {
+        const int nb = min(MNB, s - c0);
+        herm_diag_block<FU_THREADS>(A, s, c0, nb, sD, sDinv, &s_bad);
+        if (s_bad) {
+            if (tid == 0) status[ui] = -(c0 + s_bad);
+            return;
+        }
+        for (int e = tid; e < nb * nb; e += FU_THREADS) A[(int64_t)(c0 + e / nb) * s + c0 + e % nb] = sD[e / nb][e % nb];
+        if (tid < nb) piv_buf[u.piv_off + c0 + tid] = c0 + tid;
+        if (nb < MNB) break;  // the last block: nothing below it
+        herm_rows<FU_THREADS>(A, s, c0, c0 + MNB, s, sD, sDinv);
+        __syncthreads();  // L21 and U12 written (global, this CTA)
+        // A22 -= L21 U12 on the tiles on and below the diagonal
+        const int r0 = c0 + MNB, rows = s - r0;
+        if (rows <= 0) continue;
+        const int T = (rows + 63) / 64;
+        const int ty = tid / 16, tx = tid % 16;
+        for (int tile = 0; tile < T * (T + 1) / 2; ++tile) {
+            int tr, tc;
+            lower_tile(tile, tr, tc);
+            const int R0 = r0 + tr * 64, K0 = r0 + tc * 64;
+            for (int e = tid; e < 64 * MNB; e += FU_THREADS) {
+                int rr = e / MNB, q = e % MNB, R = R0 + rr;
+                s_l[rr][q] = (R < s) ? A[(int64_t)R * s + c0 + q] : cf(0.f, 0.f);
+            }
+            for (int e = tid; e < MNB * 64; e += FU_THREADS) {
+                int q = e / 64, cc = e % 64, K = K0 + cc;
+                s_u[q][cc] = (K < s) ? A[(int64_t)(c0 + q) * s + K] : cf(0.f, 0.f);
+            }
+            __syncthreads();
+            float2 acc[4][4];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    int R = R0 + ty + 16 * a, K = K0 + tx + 16 * b;
+                    acc[a][b] = (R < s && K < s) ? A[(int64_t)R * s + K] : cf(0.f, 0.f);
+                }
+#pragma unroll 4
+            for (int q = 0; q < MNB; ++q) {
+                float2 lv[4], uv[4];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) lv[a] = s_l[ty + 16 * a][q];
+#pragma unroll
+                for (int b = 0; b < 4; ++b) uv[b] = s_u[q][tx + 16 * b];
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) {
+                        acc[a][b].x = fmaf(-lv[a].x, uv[b].x, fmaf(lv[a].y, uv[b].y, acc[a][b].x));
+                        acc[a][b].y = fmaf(-lv[a].x, uv[b].y, fmaf(-lv[a].y, uv[b].x, acc[a][b].y));
+                    }
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    int R = R0 + ty + 16 * a, K = K0 + tx + 16 * b;
+                    if (R < s && K < s) A[(int64_t)R * s + K] = acc[a][b];
+                }
+            __syncthreads();
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -2338,6 +2562,8 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     // column-serial panel chain of the tallest units then overlaps the
     // many short units' work instead of leaving the GPU idle.
     const int nu_all = (int)gp.s_desc.size();
+    // no row exchanges on the Hermitian normal equations (k_panel32_herm)
+    const bool herm = !mw.pivoting;
     // units with S <= FU_MAX_S (the tail of the order) are factored whole,
     // one CTA each, in one launch on a stream of their own
     int i_unit = nu_all;
@@ -2351,8 +2577,8 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         // units whose panels outgrow one CTA (grid-wide or global-memory
         // panels, one exchange area) all stay in the first group
         int n_tall = 0;
-        while (n_tall < i_unit && gp.s_desc[n_tall] > thr_rows) ++n_tall;
-        if (mw.trail && mw.use_tc_trail) n_tall = std::max(n_tall, std::min(mw.trail_n, i_unit));  // one stack set
+        while (!herm && n_tall < i_unit && gp.s_desc[n_tall] > thr_rows) ++n_tall;
+        if (!herm && mw.trail && mw.use_tc_trail) n_tall = std::max(n_tall, std::min(mw.trail_n, i_unit));  // one stack set
         double tot = 0, acc = 0;
         for (int i = 0; i < i_unit; ++i) tot += (double)gp.s_desc[i] * gp.s_desc[i] * gp.s_desc[i];
         for (int i = 0; i < i_unit && (int)gb.size() < G; ++i) {
@@ -2371,10 +2597,16 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         for (int g = 0; g < n_side; ++g) cudaStreamWaitEvent(mw.fstream[g], mw.fevent[0], 0);
     }
     if (unit_launch) {
-        set_smem_limit_once((const void *)k_factor32_unit, (int)fu_smem(FU_MAX_S_ALL));
         cudaStream_t us = unit_own ? mw.fstream[G - 1] : st;
-        const size_t fsm = fu_smem(gp.s_desc[i_unit]);  // the launch's largest unit
-        k_factor32_unit<<<nu_all - i_unit, FU_THREADS, fsm, us>>>(d_units, mw.smu, mw.a32, piv, status, ord, i_unit);
+        if (herm) {
+            k_factor32_unit_herm<<<nu_all - i_unit, FU_THREADS, 0, us>>>(d_units, mw.smu, mw.a32, piv, status, ord,
+                                                                         i_unit);
+        } else {
+            set_smem_limit_once((const void *)k_factor32_unit, (int)fu_smem(FU_MAX_S_ALL));
+            const size_t fsm = fu_smem(gp.s_desc[i_unit]);  // the launch's largest unit
+            k_factor32_unit<<<nu_all - i_unit, FU_THREADS, fsm, us>>>(d_units, mw.smu, mw.a32, piv, status, ord,
+                                                                      i_unit);
+        }
         ++L;
     }
     std::vector<StepClass> cls;
@@ -2382,7 +2614,27 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     for (int grp = 0; grp < G && i_unit > 0; ++grp) {
     const int gi0 = gb[grp], gi1 = gb[grp + 1];
     cudaStream_t fs = grp == 0 ? st : mw.fstream[grp - 1];
-    for (int c0 = 0; gi0 < gi1 && c0 < gp.s_desc[gi0]; c0 += MNB) {
+    for (int c0 = 0; herm && gi0 < gi1 && c0 < gp.s_desc[gi0]; c0 += MNB) {
+        // Hermitian factor: panel (diagonal block, L21, mirrored U12), then
+        // the trailing tiles on and below the diagonal, per size class
+        step_classes(gp, c0, gi0, cls, gi1);
+        for (const StepClass &c : cls) {
+            if (c.m_max - MNB > 256)
+                k_panel32_herm<1024><<<c.i1 - c.i0, 1024, 0, fs>>>(d_units, mw.smu, c0, mw.a32, piv, status, ord, c.i0);
+            else
+                k_panel32_herm<256><<<c.i1 - c.i0, 256, 0, fs>>>(d_units, mw.smu, c0, mw.a32, piv, status, ord, c.i0);
+            ++L;
+        }
+        for (const StepClass &c : cls) {
+            const int rows = c.m_max - MNB;
+            if (rows <= 0) continue;
+            const int T = (rows + 63) / 64;
+            dim3 g2(T * (T + 1) / 2, c.i1 - c.i0);
+            k_trailing32<<<g2, 256, 0, fs>>>(d_units, mw.smu, c0, mw.a32, status, ord, c.i0, 1, INT_MAX, 1);
+            ++L;
+        }
+    }
+    for (int c0 = 0; !herm && gi0 < gi1 && c0 < gp.s_desc[gi0]; c0 += MNB) {
         // panels as in the plain path: tallest grid-wide (or one CTA from
         // global memory), the rest one CTA from shared memory per size class
         int n_thr = gi0;
@@ -2454,15 +2706,15 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
             if (rows <= 0) continue;
             if (pair_first) {  // the next panel's columns only
                 dim3 g2((rows + 63) / 64, c.i1 - c.i0);
-                k_trailing32<<<g2, 256, 0, fs>>>(d_units, mw.smu, c0, mw.a32, status, ord, c.i0, 1, c0 + 2 * MNB);
+                k_trailing32<<<g2, 256, 0, fs>>>(d_units, mw.smu, c0, mw.a32, status, ord, c.i0, 1, c0 + 2 * MNB, 0);
             } else if (pair_second) {  // both steps of the pair, from the pair's first column
                 int t = ((rows + 63) / 64) * ((rows + 63) / 64);
                 dim3 g2(t, c.i1 - c.i0);
-                k_trailing32<<<g2, 256, 0, fs>>>(d_units, mw.smu, c0 - MNB, mw.a32, status, ord, c.i0, 2, INT_MAX);
+                k_trailing32<<<g2, 256, 0, fs>>>(d_units, mw.smu, c0 - MNB, mw.a32, status, ord, c.i0, 2, INT_MAX, 0);
             } else {
                 int t = ((rows + 63) / 64) * ((rows + 63) / 64);
                 dim3 g2(t, c.i1 - c.i0);
-                k_trailing32<<<g2, 256, 0, fs>>>(d_units, mw.smu, c0, mw.a32, status, ord, c.i0, 1, INT_MAX);
+                k_trailing32<<<g2, 256, 0, fs>>>(d_units, mw.smu, c0, mw.a32, status, ord, c.i0, 1, INT_MAX, 0);
             }
             ++L;
         }

@@ -82,6 +82,7 @@ struct MixedWork {
     int trail_n = 0;          // units (a prefix of the s-descending order) it covers
     bool use_tc_trail = false; // the tuner picks it
     bool two_step = false;     // SIMT trailing updates once per two steps (look-ahead of the next panel)
+    bool pivoting = false;     // GEPP with row exchanges; else the Hermitian factor without them
 };
 
 // Phase events the mixed path records after its fill, Gram, factor and

@@ -745,7 +745,7 @@ class _Schedule(ctypes.Structure):
                 ("gmres_cluster", ctypes.c_int32), ("grid_gmres", ctypes.c_int32), ("graph", ctypes.c_int32),
                 ("factor_streams", ctypes.c_int32), ("unit_factor", ctypes.c_int32),
                 ("block_inverse", ctypes.c_int32), ("tensor_trailing", ctypes.c_int32),
-                ("gmres_ctas_per_sm", ctypes.c_int32)]
+                ("gmres_ctas_per_sm", ctypes.c_int32), ("factor_pivoting", ctypes.c_int32)]
 
 
 class _TuneReport(ctypes.Structure):
@@ -829,7 +829,7 @@ class HallenBatch:
     def schedule(self) -> dict:
         """How the pipeline launches (grid_panels, class_shift, gram_tensor,
         gmres_cluster, grid_gmres, graph, factor_streams, unit_factor,
-        block_inverse, tensor_trailing, gmres_ctas_per_sm)."""
+        block_inverse, tensor_trailing, gmres_ctas_per_sm, factor_pivoting)."""
         s = _Schedule()
         self.ctx.check(lib().fnec_batch_get_schedule(self._h, ctypes.byref(s)), "batch_get_schedule")
         return _sched_dict(s)

@@ -675,6 +675,11 @@ typedef struct {
                               updates only the next panel's columns)            */
     int32_t gmres_ctas_per_sm;/* mixed: 3 or 4 refinement CTAs per SM (the
                               register budget of the one-CTA-per-solve kernel)    */
+    int32_t factor_pivoting;/* mixed: 0 the FP32 factor of the Hermitian normal
+                              equations without row exchanges (lower-triangle
+                              trailing updates, U12 mirrored from L21); 1 GEPP
+                              with partial pivoting (tensor_trailing applies
+                              only here)                                          */
 } fnec_schedule;
 
 /* Graph state of a batch (fnec_batch_graph_state). */

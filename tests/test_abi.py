@@ -64,9 +64,9 @@ def test_tune_cache_file_round_trip(tmp_path):
     good = tmp_path / "tune.txt"
     good.write_text("# shape key, then every schedule field\n"
                     "p1.sm148.ns8.nu8.smax9.smean8.gp0.gg0.tc1.cm1 grid_panels=1 class_shift=2 gram_tensor=0 "
-                    "gmres_cluster=1 grid_gmres=1 graph=1 factor_streams=4 unit_factor=0 block_inverse=1 tensor_trailing=1 gmres_ctas_per_sm=4\n"
+                    "gmres_cluster=1 grid_gmres=1 graph=1 factor_streams=4 unit_factor=0 block_inverse=1 tensor_trailing=1 gmres_ctas_per_sm=4 factor_pivoting=1\n"
                     "p0.sm148.ns12.nu12.smax10.smean8.gp1.gg0.tc0.cm1 grid_panels=0 class_shift=1 gram_tensor=1 "
-                    "gmres_cluster=1 grid_gmres=1 graph=0 factor_streams=1 unit_factor=1 block_inverse=0 tensor_trailing=0 gmres_ctas_per_sm=3\n")
+                    "gmres_cluster=1 grid_gmres=1 graph=0 factor_streams=1 unit_factor=1 block_inverse=0 tensor_trailing=0 gmres_ctas_per_sm=3 factor_pivoting=0\n")
     acc.tune_cache_load(good)
     assert acc.tune_cache_size() == 2
     out = tmp_path / "saved.txt"
@@ -74,11 +74,11 @@ def test_tune_cache_file_round_trip(tmp_path):
     lines = sorted(out.read_text().split("\n")[:-1])
     assert lines == sorted(l for l in good.read_text().split("\n")[1:] if l)
     bad = tmp_path / "bad.txt"
-    for text in ("k grid_panels=1 class_shift=3 gram_tensor=1 gmres_cluster=1 grid_gmres=1 graph=1 factor_streams=1 unit_factor=1 block_inverse=0 tensor_trailing=0 gmres_ctas_per_sm=3\n",  # range
-                 "k grid_panels=1 class_shift=1 gram_tensor=1 gmres_cluster=3 grid_gmres=1 graph=1 factor_streams=1 unit_factor=1 block_inverse=0 tensor_trailing=0 gmres_ctas_per_sm=3\n",  # cluster
+    for text in ("k grid_panels=1 class_shift=3 gram_tensor=1 gmres_cluster=1 grid_gmres=1 graph=1 factor_streams=1 unit_factor=1 block_inverse=0 tensor_trailing=0 gmres_ctas_per_sm=3 factor_pivoting=0\n",  # range
+                 "k grid_panels=1 class_shift=1 gram_tensor=1 gmres_cluster=3 grid_gmres=1 graph=1 factor_streams=1 unit_factor=1 block_inverse=0 tensor_trailing=0 gmres_ctas_per_sm=3 factor_pivoting=0\n",  # cluster
                  "k grid_panels=1 class_shift=1\n",  # fields missing
-                 "k grid_panels=1 class_shift=1 gram_tensor=1 gmres_cluster=1 grid_gmres=1 graph=1 factor_streams=3 unit_factor=1 block_inverse=0 tensor_trailing=0 gmres_ctas_per_sm=3\n",
-                 "k grid_panels=1 tile=7 class_shift=1 gram_tensor=1 gmres_cluster=1 grid_gmres=1 graph=1 factor_streams=1 unit_factor=1 block_inverse=0 tensor_trailing=0 gmres_ctas_per_sm=3\n"):
+                 "k grid_panels=1 class_shift=1 gram_tensor=1 gmres_cluster=1 grid_gmres=1 graph=1 factor_streams=3 unit_factor=1 block_inverse=0 tensor_trailing=0 gmres_ctas_per_sm=3 factor_pivoting=0\n",
+                 "k grid_panels=1 tile=7 class_shift=1 gram_tensor=1 gmres_cluster=1 grid_gmres=1 graph=1 factor_streams=1 unit_factor=1 block_inverse=0 tensor_trailing=0 gmres_ctas_per_sm=3 factor_pivoting=0\n"):
         bad.write_text(text)
         with pytest.raises(acc.AccelError):
             acc.tune_cache_load(bad)

@@ -99,7 +99,7 @@ def test_schedule_rejects_out_of_range(acc, plain_ants):
     b = acc.HallenBatch(plain_ants[:2], precision=acc.PRECISION_FP64)
     for bad in ({"class_shift": 3}, {"gmres_cluster": 3}, {"graph": 5}, {"grid_panels": -1}, {"factor_streams": 3},
                 {"unit_factor": 4}, {"unit_factor": -1}, {"block_inverse": 5}, {"tensor_trailing": -1}, {"tensor_trailing": 3},
-                {"gmres_ctas_per_sm": 2}):
+                {"gmres_ctas_per_sm": 2}, {"factor_pivoting": 2}, {"factor_pivoting": -1}):
         with pytest.raises(acc.AccelError) as e:
             b.schedule = bad
         assert e.value.code == acc.ERR_BAD_ARG
@@ -114,9 +114,13 @@ def test_schedule_rejects_out_of_range(acc, plain_ants):
     {"unit_factor": 0}, {"unit_factor": 1, "factor_streams": 4, "graph": 2},
     {"unit_factor": 2}, {"unit_factor": 3, "factor_streams": 2},
     {"block_inverse": 0}, {"block_inverse": 1, "gmres_cluster": 4},
-    {"tensor_trailing": 0}, {"tensor_trailing": 1, "factor_streams": 4, "unit_factor": 0},
-    {"tensor_trailing": 2}, {"tensor_trailing": 2, "factor_streams": 4, "unit_factor": 0},
+    {"tensor_trailing": 0}, {"tensor_trailing": 1, "factor_streams": 4, "unit_factor": 0, "factor_pivoting": 1},
+    {"tensor_trailing": 2, "factor_pivoting": 1},
+    {"tensor_trailing": 2, "factor_streams": 4, "unit_factor": 0, "factor_pivoting": 1},
     {"gmres_ctas_per_sm": 4}, {"gmres_ctas_per_sm": 4, "block_inverse": 0},
+    {"factor_pivoting": 1}, {"factor_pivoting": 1, "unit_factor": 3, "factor_streams": 2},
+    {"factor_pivoting": 0, "unit_factor": 0, "factor_streams": 4, "class_shift": 2},
+    {"factor_pivoting": 0, "unit_factor": 3, "block_inverse": 0},
 ])
 def test_mixed_within_gate_under_every_schedule(acc, sched):
     ants = _ants(acc, 20, seed=32)  # few solves: clusters up to 8 CTAs fit
@@ -164,23 +168,29 @@ def test_tuner_sets_and_caches_the_fastest(acc, tmp_path):
     acc.tune_cache_clear()
 
 
-def test_mixed_factor_groups_give_identical_bits(acc):
+@pytest.mark.parametrize("pivoting", [0, 1])
+def test_mixed_factor_groups_give_identical_bits(acc, pivoting):
     """Grouping units onto concurrent streams, or factoring small units whole
     in one CTA, changes only which launches run beside which: every unit's
     factor (the same operations in the same order), and so every solve, is
-    the same."""
+    the same -- for the Hermitian factor and for GEPP."""
     ants = _ants(acc, 32, seed=35)
     b = acc.HallenBatch(ants, precision=acc.PRECISION_MIXED)
     # all trailing updates as FP32 SIMT tiles: the whole-unit kernel repeats
     # the per-step kernels' arithmetic
-    b.schedule = {"factor_streams": 1, "unit_factor": 0, "tensor_trailing": 0, "graph": 0}
+    b.schedule = {"factor_streams": 1, "unit_factor": 0, "tensor_trailing": 0, "graph": 0,
+                  "factor_pivoting": pivoting}
     ref = _bits(_run(b))
     for sched in ({"factor_streams": 2}, {"factor_streams": 4}, {"factor_streams": 4, "graph": 2},
-                  {"unit_factor": 1, "factor_streams": 1}, {"unit_factor": 1, "factor_streams": 4}):
+                  {"unit_factor": 1, "factor_streams": 1}, {"unit_factor": 1, "factor_streams": 4},
+                  {"unit_factor": 3, "factor_streams": 2}):
         b.schedule = sched
         got = _bits(_run(b, times=2))
         for r, g in zip(ref, got):
             assert np.array_equal(r, g), sched
+    if pivoting == 0:
+        b.close()
+        return
     # tensor-core trailing updates: the same units take them in every grouping
     b.schedule = {"factor_streams": 1, "unit_factor": 1, "tensor_trailing": 1, "graph": 0}
     ref = _bits(_run(b))
@@ -206,7 +216,7 @@ def test_tensor_core_trailing_keeps_the_refinement(acc, cells):
     for tt in (0, 1):
         b = acc.HallenBatch(ant, precision=acc.PRECISION_MIXED)
         assert b.info.max_s - 32 >= 192
-        b.schedule = {"tensor_trailing": tt}
+        b.schedule = {"tensor_trailing": tt, "factor_pivoting": 1}  # GEPP's trailing updates
         res = _run(b)
         assert np.all(res.status == 0)
         it, rs = b.refinement_stats()
