@@ -904,6 +904,7 @@ struct PinnedArena {
 };
 extern "C" {
 static void schedule_from_cache(fnec_batch *b);  // defined with the C API below
+static void apply_schedule(fnec_batch *b, const fnec_schedule &s);
 }
 
 struct BatchPlace {
@@ -1361,6 +1362,13 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
                     std::string("batch allocation: ") + cudaGetErrorString(e));
     }
     *out = b;
+    // the default for many systems: every unit up to S 512 factored whole,
+    // one CTA each (enough of them to fill the GPU)
+    if (precision == FNEC_PRECISION_MIXED && (int64_t)b->units.size() >= 2 * (int64_t)b->grid.sms) {
+        fnec_schedule s = b->sched;
+        s.unit_factor = 3;
+        apply_schedule(b, s);
+    }
     schedule_from_cache(b);
     int st = fnec_batch_upload(b);
     if (st != FNEC_OK) {

@@ -20,6 +20,7 @@
 // few directions.  The error against the FP64 oracle is reported per unit
 // (iterations and final residual are kept for inspection).
 #include <algorithm>
+#include <cstring>
 #include <climits>
 #include <vector>
 
@@ -72,6 +73,55 @@ __constant__ double m_gl_w8[8] = {0.101228536290376, 0.222381034453374, 0.313706
 // ---------------------------------------------------------------------------
 // fast FP64 fill (matrix.rs:297-331 with hardware sincos/log and FMA)
 // ---------------------------------------------------------------------------
+// sin(pi x) and cos(pi x) for 0 <= x < 2^50, the phase of the fill's
+// samples.  Quadrant reduction in half-turns: adding 1.5 * 2^52 rounds 2x
+// to the integer n (its low bits are n), and f = x - n / 2 is exact with
+// |f| <= 1/4; then the Taylor series of sin and cos at theta = pi f
+// (|theta| <= pi/4) to theta^15 and theta^16, whose truncation error is
+// below 5e-17, in Horner form in theta^2, and the quadrant n mod 4 swaps
+// and signs the pair.  About 22 FP64 operations and no table.
+__host__ __device__ __forceinline__ void fill_sincospi(double x, double &sn, double &cs) {
+    const double big = 6755399441055744.0;  // 1.5 * 2^52
+    const double t = fma(x, 2.0, big);
+    const double nd = t - big;
+#ifdef __CUDA_ARCH__
+    const int q = __double2loint(t) & 3;
+#else
+    long long bits;
+    memcpy(&bits, &t, sizeof(bits));
+    const int q = (int)(bits & 3);
+#endif
+    const double th = fma(nd, -0.5, x) * 3.141592653589793;
+    const double t2 = th * th;
+    // sin: theta (1 + t2 (-1/3! + t2 (1/5! - ... - t2 / 15!)))
+    double ps = -7.647163731819816e-13;  // -1/15!
+    ps = fma(ps, t2, 1.6059043836821613e-10);   // 1/13!
+    ps = fma(ps, t2, -2.505210838544172e-08);   // -1/11!
+    ps = fma(ps, t2, 2.7557319223985893e-06);   // 1/9!
+    ps = fma(ps, t2, -0.0001984126984126984);   // -1/7!
+    ps = fma(ps, t2, 0.008333333333333333);    // 1/5!
+    ps = fma(ps, t2, -0.16666666666666666);  // -1/3!
+    const double s0 = fma(th * t2, ps, th);
+    // cos: 1 + t2 (-1/2! + t2 (1/4! - ... + t2 / 16!))
+    double pc = 4.779477332387385e-14;  // 1/16!
+    pc = fma(pc, t2, -1.1470745597729725e-11);  // -1/14!
+    pc = fma(pc, t2, 2.08767569878681e-09);     // 1/12!
+    pc = fma(pc, t2, -2.755731922398589e-07);   // -1/10!
+    pc = fma(pc, t2, 2.48015873015873e-05);     // 1/8!
+    pc = fma(pc, t2, -0.001388888888888889);  // -1/6!
+    pc = fma(pc, t2, 0.041666666666666664);   // 1/4!
+    pc = fma(pc, t2, -0.5);                     // -1/2!
+    const double c0 = fma(t2, pc, 1.0);
+    const double a = (q & 1) ? c0 : s0, b = (q & 1) ? s0 : c0;
+    sn = (q & 2) ? -a : a;
+    cs = ((q + 1) & 2) ? -b : b;
+}
+
+// Z element (obs midpoint om, source segment mid sm / unit direction sd /
+// length slen / radius srad); the far form takes the midpoint difference
+// d = om - sm and the half-length step hs = sd slen / 2 once per element,
+// then per Gauss-Legendre sample r = d - x_m hs, R^2 = |r|^2 + a^2, one
+// reciprocal square root for R and 1/R and fill_sincospi(k R / pi).
 __device__ __forceinline__ cx elem_fast(const double *om, const double *od, const double *sm, const double *sd,
                                         double slen, double srad, double k, bool is_self) {
     double cos_alpha = od[0] * sd[0] + od[1] * sd[1] + od[2] * sd[2];
@@ -93,23 +143,21 @@ __device__ __forceinline__ cx elem_fast(const double *om, const double *od, cons
         double r_end = sqrt(half * half + a * a);
         ire += 2.0 * log((half + r_end) / a);
     } else {
-        // e^{-jkR}/R with one reciprocal square root per sample and the
-        // phase as a multiple of pi (sincospi needs no Cody-Waite argument
-        // reduction); the phase error stays a few ulp of kR
         const double kpi = k * 0.31830988618379067;  // k / pi
+        const double d0 = om[0] - sm[0], d1 = om[1] - sm[1], d2 = om[2] - sm[2];
+        const double h0 = sd[0] * half, h1 = sd[1] * half, h2 = sd[2] * half;
+        const double a2 = a * a;
 #pragma unroll
         for (int m = 0; m < 8; ++m) {
-            double sc = m_gl_n8[m] * half;
-            double r0 = om[0] - (sm[0] + sc * sd[0]);
-            double r1 = om[1] - (sm[1] + sc * sd[1]);
-            double r2 = om[2] - (sm[2] + sc * sd[2]);
-            double r2s = r0 * r0 + r1 * r1 + r2 * r2 + a * a;
-            double inv = rsqrt(r2s);
+            const double xm = m_gl_n8[m];
+            const double r0 = fma(-xm, h0, d0), r1 = fma(-xm, h1, d1), r2 = fma(-xm, h2, d2);
+            const double r2s = fma(r0, r0, fma(r1, r1, fma(r2, r2, a2)));
+            const double inv = rsqrt(r2s);
             double sn, cs;
-            sincospi(-kpi * (r2s * inv), &sn, &cs);
-            double wr = m_gl_w8[m] * inv;
-            ire += wr * cs;
-            iim += wr * sn;
+            fill_sincospi(kpi * (r2s * inv), sn, cs);
+            const double wr = m_gl_w8[m] * inv;
+            ire = fma(wr, cs, ire);
+            iim = fma(-wr, sn, iim);  // e^{-jkR}
         }
         ire *= half;
         iim *= half;
@@ -127,8 +175,10 @@ __global__ void __launch_bounds__(256, 4) k_fill_fast(const UnitDesc *__restrict
                                                    const DevSeg *__restrict__ segs, const int4 *__restrict__ tiles,
                                                    cx *zbuf, const TcGramUnit *__restrict__ gu, float *ghi,
                                                    float *glo) {
-    __shared__ DevSeg s_obs[16];
-    __shared__ DevSeg s_src[16];
+    // the tile's segments field by field (structure of arrays): a warp's 16
+    // source lanes read 16 consecutive doubles, one conflict-free wavefront
+    __shared__ double s_o[6][16];  // observation midpoint, direction
+    __shared__ double s_s[8][16];  // source midpoint, direction, length, radius
     __shared__ cx s_z[16][17];
     int4 t = tiles[blockIdx.x];
     UnitDesc u = units[t.x];
@@ -136,18 +186,27 @@ __global__ void __launch_bounds__(256, 4) k_fill_fast(const UnitDesc *__restrict
     int n = a.n;
     const DevSeg *sg = segs + a.seg_off;
     int tid = threadIdx.x;
-    if (tid < 16 && t.y + tid < n) s_obs[tid] = sg[t.y + tid];
-    if (tid >= 32 && tid < 48 && t.z + tid - 32 < n) s_src[tid - 32] = sg[t.z + tid - 32];
+    if (tid < 6 * 16) {
+        const int q = tid / 6, f = tid % 6;
+        const DevSeg *g = sg + min(t.y + q, n - 1);
+        s_o[f][q] = f < 3 ? g->mid[f] : g->dir[f - 3];
+    } else if (tid < 6 * 16 + 8 * 16) {
+        const int q = (tid - 96) / 8, f = (tid - 96) % 8;
+        const DevSeg *g = sg + min(t.z + q, n - 1);
+        s_s[f][q] = f < 3 ? g->mid[f] : (f < 6 ? g->dir[f - 3] : (f == 6 ? g->len : g->rad));
+    }
     __syncthreads();
     int ii = tid / 16, jj = tid % 16;
     int i = t.y + ii, j = t.z + jj;
     if (i < n && j < n) {
-        const DevSeg &o = s_obs[ii], &s = s_src[jj];
-        cx z = elem_fast(o.mid, o.dir, s.mid, s.dir, s.len, s.rad, u.k_fill, i == j);
+        const double om[3] = {s_o[0][ii], s_o[1][ii], s_o[2][ii]}, od[3] = {s_o[3][ii], s_o[4][ii], s_o[5][ii]};
+        const double sm[3] = {s_s[0][jj], s_s[1][jj], s_s[2][jj]}, sd[3] = {s_s[3][jj], s_s[4][jj], s_s[5][jj]};
+        const double slen = s_s[6][jj], srad = s_s[7][jj];
+        cx z = elem_fast(om, od, sm, sd, slen, srad, u.k_fill, i == j);
         if (a.ground == 1) {
-            double im_mid[3] = {s.mid[0], s.mid[1], -s.mid[2]};
-            double im_dir[3] = {-s.dir[0], -s.dir[1], s.dir[2]};
-            cx g = elem_fast(o.mid, o.dir, im_mid, im_dir, s.len, s.rad, u.k_fill, false);
+            const double im_mid[3] = {sm[0], sm[1], -sm[2]};
+            const double im_dir[3] = {-sd[0], -sd[1], sd[2]};
+            cx g = elem_fast(om, od, im_mid, im_dir, slen, srad, u.k_fill, false);
             z = zadd(z, g);
         }
         zbuf[u.z_off + (int64_t)i * n + j] = z;
@@ -2750,3 +2809,12 @@ cudaError_t read_mixed_stats(MixedWork &mw, int32_t *iters, double *resid, cudaS
 }
 
 }  // namespace fnec
+
+extern "C" int fnec_test_fill_sincospi(const double *x, uint64_t n, double *sin_out, double *cos_out) {
+    if ((n && (!x || !sin_out || !cos_out))) return FNEC_ERR_BAD_ARG;
+    for (uint64_t i = 0; i < n; ++i) {
+        if (!(x[i] >= 0.0 && x[i] < 1125899906842624.0)) return FNEC_ERR_BAD_ARG;  // [0, 2^50)
+        fnec::fill_sincospi(x[i], sin_out[i], cos_out[i]);
+    }
+    return FNEC_OK;
+}

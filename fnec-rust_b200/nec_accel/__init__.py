@@ -195,6 +195,7 @@ SIGNATURES = {
     "fnec_batch_set_sources": (ctypes.c_int, [_P, _U32, _P, _U32]),
     "fnec_batch_resolve": (ctypes.c_int, [_P]),
     "fnec_test_fail_device_allocation": (ctypes.c_int, [_I32]),
+    "fnec_test_fill_sincospi": (ctypes.c_int, [_P, _U64, _P, _P]),
     "fnec_batch_create": (ctypes.c_int, [_P, _P, _U32, _I32, _P]),
     "fnec_batch_destroy": (ctypes.c_int, [_P]),
     "fnec_batch_get_info": (ctypes.c_int, [_P, _P]),
@@ -601,6 +602,17 @@ def test_fail_device_allocation(after: int):
     rc = lib().fnec_test_fail_device_allocation(int(after))
     if rc != OK:
         raise AccelError(rc, "test_fail_device_allocation")
+
+
+def test_fill_sincospi(x):
+    """Test hook: the mixed fill's own sin(pi x), cos(pi x), run on the host
+    (0 <= x < 2^50)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    s, c = np.empty_like(x), np.empty_like(x)
+    rc = lib().fnec_test_fill_sincospi(_ptr(x), len(x), _ptr(s), _ptr(c))
+    if rc != OK:
+        raise AccelError(rc, "test_fill_sincospi")
+    return s, c
 
 
 def measure_fp32_peak(device: int = 0) -> float:

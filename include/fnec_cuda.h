@@ -529,6 +529,11 @@ int fnec_selftest_tf32x3_gemm(int32_t device, uint64_t m, uint64_t n, uint64_t k
 int fnec_selftest_wait_timeout(int32_t device, int32_t which, uint64_t wait_ns, int32_t *unit_status,
                                double *elapsed_ms);
 int fnec_test_fail_device_allocation(int32_t after);
+/* The mixed form's fill evaluates its samples' phase with its own
+ * sin(pi x), cos(pi x) (quadrant reduction, Taylor series; the same source
+ * is compiled for the host): fnec_test_fill_sincospi runs it on the host
+ * for n arguments 0 <= x < 2^50 (test use). */
+int fnec_test_fill_sincospi(const double *x, uint64_t n, double *sin_out, double *cos_out);
 
 /* Radiation pattern that allocates no device memory.  No counterpart in
  * the reference: it serves callers that cannot call cudaMalloc -- a host
