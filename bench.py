@@ -313,7 +313,8 @@ def phase_rooflines(form, o, n, s, g, d, shapes, fma, muladd, ffma, peaks, runs)
     Work models (per unit): fill 60 FP64 ops per G(R) sample (8 N^2 - 4 N
     samples, doubled over GN 1); Gram 8 N^2 (N+1) flops (plain) or the
     3xTF32 tensor-core flops issued on the upper-triangle 128x128 tiles
-    (mixed); factor (8/3) S^3 flops; solve: plain back substitution 8 S^2
+    (mixed); factor (8/3) S^3 flops (GEPP) or (4/3) S^3 (the mixed form's
+    Hermitian factor, lower triangle only); solve: plain back substitution 8 S^2
     flops on a serial chain, mixed GMRES HBM bytes (iterations + 2) x
     (32 N^2 + 8 S^2) (FP64 Z read twice, FP32 factor once per apply); far
     field 8 N flops per direction (its sincos per wire run is not counted);
@@ -345,7 +346,11 @@ def phase_rooflines(form, o, n, s, g, d, shapes, fma, muladd, ffma, peaks, runs)
         tc = float(np.sum(nt * (nt + 1) / 2 * 128 * 128 * kb * 32 * 2 * 3))
         put("gram", tc / 1e12, peaks["tf32_tflops"], "TFLOP/s", "tensor (tf32)",
             "half the BF16 rate of " + peaks["source"])
-        put("factor", float(np.sum(8 * s ** 3 / 3)) / 1e12, ffma, "TFLOP/s", "fp32",
+        # the Hermitian factor (schedule factor_pivoting 0) updates only the
+        # lower triangle: half of GEPP's (8/3) S^3
+        sched = (o.get("schedule") or {}).get("schedule") or {}
+        herm = int(sched.get("factor_pivoting", 0)) == 0
+        put("factor", float(np.sum((4 if herm else 8) * s ** 3 / 3)) / 1e12, ffma, "TFLOP/s", "fp32",
             "FFMA measured by fnec_measure_fp32_peak")
         it = o.get("gmres_iters")
         n_s = np.array([u["n"] for u in shapes], np.float64)

@@ -44,6 +44,7 @@ __device__ __forceinline__ float2 cf_mul(float2 a, float2 b) {
     return cf(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 __device__ __forceinline__ float2 cf_sub(float2 a, float2 b) { return cf(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cf_add(float2 a, float2 b) { return cf(a.x + b.x, a.y + b.y); }
 __device__ __forceinline__ float2 cf_div(float2 a, float2 b) {
     float inv = 1.0f / (b.x * b.x + b.y * b.y);
     return cf((a.x * b.x + a.y * b.y) * inv, (a.y * b.x - a.x * b.y) * inv);
@@ -964,6 +965,61 @@ __device__ void herm_rows(float2 *A, int s, int c0, int r_begin, int r_end, cons
     }
 }
 
+// The inverses of a factored diagonal block for the refinement's
+// preconditioner (sD: unit-lower L11 below the diagonal, U11 on and above
+// it; sDinv: 1 / U11[i][i]), in FP32, by threads 0 .. 255: threads
+// 0 .. 127 form L11^-1, 128 .. 255 U11^-1, four consecutive lanes per
+// column j, each summing the terms k = q (mod 4) of the substitution; the
+// quarter sums are added by two shuffles (a column's lanes share a warp)
+// and the column lives in X (a 32 x 33 scratch per triangle in shared
+// memory).  Stored row-major, L^-1 then U^-1 (2 x 1024 entries), zero
+// outside an nb < 32 block.
+__device__ void herm_block_inverse(const float2 (*sD)[MNB + 1], const float2 *sDinv, int nb, float2 (*X)[MNB + 1],
+                                   float2 *out) {
+    const int t = threadIdx.x, w = t >> 7, j = (t & 127) >> 2, q = t & 3;
+    X += w * 32;
+    const bool live = j < nb;
+    if (w == 0) {  // L^-1 e_j: forward, unit diagonal
+        for (int i = 0; i < 32; ++i) {
+            float2 p = cf(0.f, 0.f);
+#pragma unroll
+            for (int m = 0; m < 8; ++m) {
+                const int k = q + 4 * m;
+                if (k < i && k < nb) p = cf_add(p, cf_mul(sD[i][k], X[k][j]));  // X[k][j] = 0 for k < j
+            }
+            p.x += __shfl_xor_sync(0xffffffffu, p.x, 1);
+            p.y += __shfl_xor_sync(0xffffffffu, p.y, 1);
+            p.x += __shfl_xor_sync(0xffffffffu, p.x, 2);
+            p.y += __shfl_xor_sync(0xffffffffu, p.y, 2);
+            if (q == 0) X[i][j] = (live && i >= j && i < nb) ? cf((i == j ? 1.f : 0.f) - p.x, -p.y) : cf(0.f, 0.f);
+            __syncwarp();
+        }
+    } else {  // U^-1 e_j: backward
+        for (int i = 31; i >= 0; --i) {
+            float2 p = cf(0.f, 0.f);
+#pragma unroll
+            for (int m = 0; m < 8; ++m) {
+                const int k = q + 4 * m;
+                if (k > i && k < nb) p = cf_add(p, cf_mul(sD[i][k], X[k][j]));  // X[k][j] = 0 for k > j
+            }
+            p.x += __shfl_xor_sync(0xffffffffu, p.x, 1);
+            p.y += __shfl_xor_sync(0xffffffffu, p.y, 1);
+            p.x += __shfl_xor_sync(0xffffffffu, p.x, 2);
+            p.y += __shfl_xor_sync(0xffffffffu, p.y, 2);
+            if (q == 0)
+                X[i][j] = (live && i <= j && i < nb) ? cf_mul(cf((i == j ? 1.f : 0.f) - p.x, -p.y), sDinv[i])
+                                                     : cf(0.f, 0.f);
+            __syncwarp();
+        }
+    }
+    out += w * 1024;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        const int i = q + 4 * m;
+        out[i * 32 + j] = X[i][j];
+    }
+}
+
 // The panel step at c0 of every unit of a size class, one CTA of NT
 // threads per unit (1024 for panels of more than 256 rows below the
 // diagonal block): the diagonal block, then every row below it.
@@ -994,7 +1050,7 @@ __global__ void __launch_bounds__(NT) k_panel32_herm(const UnitDesc *__restrict_
 
 // The whole Hermitian factor of one small unit (S <= fu_max_s(level)) per
 // CTA: the per-step kernels' operations without a launch between steps.
-__global__ void __launch_bounds__(FU_THREADS, 3) k_factor32_unit_herm(const UnitDesc *__restrict__ units,
+__global__ void __launch_bounds__(FU_THREADS, 4) k_factor32_unit_herm(const UnitDesc *__restrict__ units,
                                                                      const MixedUnit *__restrict__ mus,
                                                                      float2 *a32buf, int32_t *piv_buf,
                                                                      int32_t *status,
@@ -1088,7 +1144,7 @@ struct GmresCtx {
     const float2 *lu;
     const int32_t *piv;
     const int32_t *perm = nullptr;  // the row permutation of piv, if built (then P in = in[perm])
-    const cx *binv = nullptr;       // the factor's diagonal block inverses, if built
+    const float2 *binv = nullptr;   // the factor's diagonal block inverses (FP32), if built
     cx *t;  // rows
 };
 
@@ -1219,10 +1275,10 @@ __device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, cx *sy) {
         __shared__ cx s_blk[32];
         for (int c0 = 0; c0 < s; c0 += 32) {
             const int nb = min(32, s - c0);
-            const cx *Li = g.binv + (int64_t)(c0 / 32) * 2048;
+            const float2 *Li = g.binv + (int64_t)(c0 / 32) * 2048;
             const cx xk = lane < nb ? sy[c0 + lane] : cx{0, 0};
             for (int i = wid; i < nb; i += (int)(blockDim.x >> 5)) {
-                cx p = warp_sum(lane < nb ? zmul(Li[i * 32 + lane], xk) : cx{0, 0});
+                cx p = warp_sum(lane < nb ? zmul(f2z(Li[i * 32 + lane]), xk) : cx{0, 0});
                 if (lane == 0) s_blk[i] = p;
             }
             __syncthreads();
@@ -1246,10 +1302,10 @@ __device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, cx *sy) {
         }
         for (int c0 = ((s - 1) / 32) * 32; c0 >= 0; c0 -= 32) {
             const int nb = min(32, s - c0);
-            const cx *Ui = g.binv + (int64_t)(c0 / 32) * 2048 + 1024;
+            const float2 *Ui = g.binv + (int64_t)(c0 / 32) * 2048 + 1024;
             const cx xk = lane < nb ? sy[c0 + lane] : cx{0, 0};
             for (int i = wid; i < nb; i += (int)(blockDim.x >> 5)) {
-                cx p = warp_sum(lane < nb ? zmul(Ui[i * 32 + lane], xk) : cx{0, 0});
+                cx p = warp_sum(lane < nb ? zmul(f2z(Ui[i * 32 + lane]), xk) : cx{0, 0});
                 if (lane == 0) s_blk[i] = p;
             }
             __syncthreads();
@@ -1367,45 +1423,35 @@ __device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, cx *sy) {
 // column j by substitution on its own column.  Stored row-major per block:
 // L^-1 then U^-1 (2 x 1024 complex128); entries outside an nb < 32 block
 // are zero.  The refinement applies the preconditioner with them.
-__global__ void __launch_bounds__(64) k_block_inv32(const UnitDesc *__restrict__ units,
-                                                    const MixedUnit *__restrict__ smu,
-                                                    const float2 *__restrict__ a32buf, cx *binvbuf,
-                                                    const int32_t *__restrict__ status) {
-    __shared__ float2 sB[32][33];
-    __shared__ cx sX[2][32][33];
+// The inverses of every system's 32x32 diagonal blocks of the factor (any
+// factor: unit-lower L11, U11 on and above the diagonal), one CTA of 256
+// threads per block (herm_block_inverse).
+__global__ void __launch_bounds__(256) k_block_inv32(const UnitDesc *__restrict__ units,
+                                                     const MixedUnit *__restrict__ smu,
+                                                     const float2 *__restrict__ a32buf, float2 *binvbuf,
+                                                     const int32_t *__restrict__ status) {
+    __shared__ float2 sB[MNB][MNB + 1];
+    __shared__ float2 sDinv[MNB];
+    __shared__ float2 sX[2 * MNB][MNB + 1];
     const int ui = blockIdx.y;
     const UnitDesc u = units[ui];
     const int c0 = blockIdx.x * 32, s = u.s;
     if (c0 >= s || status[ui] != 0) return;
     const int nb = min(32, s - c0);
     const float2 *A = a32buf + smu[ui].a32_off;
-    const int tid = threadIdx.x, w = tid >> 5, j = tid & 31;
-    for (int e = tid; e < 32 * 32; e += 64) {
+    const int tid = threadIdx.x;
+    for (int e = tid; e < 32 * 32; e += 256) {
         const int i = e / 32, k = e % 32;
         sB[i][k] = (i < nb && k < nb) ? A[(int64_t)(c0 + i) * s + c0 + k] : make_float2(0.f, 0.f);
     }
     __syncthreads();
-    cx(*X)[33] = sX[w];
-    if (w == 0) {  // L^-1 e_j: forward, unit diagonal
-        for (int i = 0; i < 32; ++i) {
-            cx v = {i == j ? 1.0 : 0.0, 0.0};
-            if (i < nb && j < nb)
-                for (int k = j; k < i; ++k) v = zsub(v, zmul(f2z(sB[i][k]), X[k][j]));
-            X[i][j] = (i < nb && j < nb) ? v : cx{0, 0};
-        }
-    } else {  // U^-1 e_j: backward
-        for (int i = 31; i >= 0; --i) {
-            if (i >= nb || j >= nb) {
-                X[i][j] = {0, 0};
-                continue;
-            }
-            cx v = {i == j ? 1.0 : 0.0, 0.0};
-            for (int k = i + 1; k <= j; ++k) v = zsub(v, zmul(f2z(sB[i][k]), X[k][j]));
-            X[i][j] = zdiv(v, f2z(sB[i][i]));
-        }
+    if (tid < 32) {
+        const float2 d = sB[tid][tid];
+        const float dn = d.x * d.x + d.y * d.y;
+        sDinv[tid] = tid < nb ? cf(d.x / dn, -d.y / dn) : cf(0.f, 0.f);
     }
-    cx *out = binvbuf + smu[ui].binv_off + (int64_t)blockIdx.x * 2048 + (int64_t)w * 1024;
-    for (int i = 0; i < 32; ++i) out[i * 32 + j] = X[i][j];
+    __syncthreads();
+    herm_block_inverse(sB, sDinv, nb, sX, binvbuf + smu[ui].binv_off + (int64_t)blockIdx.x * 2048);
 }
 
 __device__ double vnorm(const cx *v, int s, double *red) {
@@ -1425,7 +1471,7 @@ __global__ void __launch_bounds__(256, MINB) k_gmres_ir(const UnitDesc *__restri
                                                   const float2 *__restrict__ a32buf, const int32_t *__restrict__ pivbuf,
                                                   cx *xbuf, cx *vbuf, cx *wbuf, const int32_t *__restrict__ status,
                                                   int staged, int skip_s, int only, int min_s,
-                                                  const int32_t *__restrict__ s_order, const cx *__restrict__ binvbuf) {
+                                                  const int32_t *__restrict__ s_order, const float2 *__restrict__ binvbuf) {
     extern __shared__ unsigned char s_dyn[];
     __shared__ cx sH[(GM + 1) * GM];
     __shared__ double scs[GM];
@@ -2259,7 +2305,7 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
     size_t b_w = sizeof(cx) * (size_t)(wk + 1);
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
     size_t b_ord = sizeof(int32_t) * (solves.size() + 1);
-    size_t b_binv = sizeof(cx) * (size_t)(binv + 1);
+    size_t b_binv = sizeof(float2) * (size_t)(binv + 1);
     size_t total = al(b_mu) + al(b_smu) + al(b_a32) + al(b_v) + al(b_w) + al(b_ord) + al(b_binv);
     cudaError_t e = dev.alloc(&w.base, total);
     if (e != cudaSuccess) return e;
@@ -2283,7 +2329,7 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
     p += al(b_w);
     w.s_order = (int32_t *)p;
     p += al(b_ord);
-    w.binv = (cx *)p;
+    w.binv = (float2 *)p;
     w.bytes = total;
     w.n_units = (int)solves.size();
     w.max_s = max_s;
@@ -2496,7 +2542,7 @@ uint64_t refine_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const Unit
     const bool grid_refine = mw.grid_on && !mw.grid_solves.empty();
     const int skip_s = grid_refine ? GG_MIN_S : INT_MAX;
     if (fresh_factor && mw.use_binv && nu > 0) {  // the preconditioner's diagonal block inverses
-        k_block_inv32<<<dim3((unsigned)((max_s + 31) / 32), (unsigned)nu), 64, 0, st>>>(d_units, mw.smu, mw.a32, mw.binv,
+        k_block_inv32<<<dim3((unsigned)((max_s + 31) / 32), (unsigned)nu), 256, 0, st>>>(d_units, mw.smu, mw.a32, mw.binv,
                                                                                       status);
         ++L;
     }
@@ -2597,7 +2643,7 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     mark(0);
     if (mw.tc && mw.use_tc) {
         tc_gram_run(*mw.tc, d_units, static_cast<const TcGramUnit *>(mw.tc_gu), static_cast<const TcTile *>(mw.tc_tiles),
-                    mw.smu, z, mw.tc_hi, mw.tc_lo, mw.a32, status, mw.tc_max_n, st, !fused_split);
+                    mw.smu, z, mw.tc_hi, mw.tc_lo, mw.a32, status, mw.tc_max_n, st, !fused_split, !mw.pivoting);
         ++L;
     } else if (n_gram > 0) {
         k_gram32_zz<<<n_gram, 256, 0, st>>>(d_units, mw.smu, gram_tiles, z, mw.a32);

@@ -25,7 +25,7 @@ struct MixedUnit {
     int32_t iters;    // GMRES iterations used
     double resid;     // final preconditioned relative residual
     int64_t cs_off;   // complex128 scratch of the cluster GMRES (-1: none)
-    int64_t binv_off; // complex128 inverses of the factor's 32x32 diagonal blocks (per system)
+    int64_t binv_off; // complex64 inverses of the factor's 32x32 diagonal blocks (per system)
 };
 
 struct MixedWork {
@@ -34,7 +34,7 @@ struct MixedWork {
     MixedUnit *mu = nullptr;   // per solve
     MixedUnit *smu = nullptr;  // per system (a32_off only)
     float2 *a32 = nullptr;
-    cx *binv = nullptr;          // per system: ceil(S/32) x (L11^-1, U11^-1), 32x32 each
+    float2 *binv = nullptr;      // per system: ceil(S/32) x (L11^-1, U11^-1), 32x32 each
     int32_t *s_order = nullptr;  // solves by decreasing N^2 (refinement launch order)
     cx *v = nullptr;
     cx *w = nullptr;

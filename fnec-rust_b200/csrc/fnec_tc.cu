@@ -165,9 +165,13 @@ __device__ __forceinline__ void epi_gram(const TcTile &t, const TcEpilogue &ep, 
         float o1 = odd ? v[17 + 2 * q] : p[2 * q + 1];
         out[q] = make_float2(e0 + o1, e1 - o0);
     }
+    // tiles lie on and above the diagonal (ti <= tj): the entry at (c, c1 + q)
+    // is the upper one; lower_only keeps diagonal tiles whole
+    if (!ep.lower_only || t.ti == t.tj) {
 #pragma unroll
-    for (int q = 0; q < 8; ++q)
-        if (c1 + q < n) A[(int64_t)c * s + c1 + q] = out[q];
+        for (int q = 0; q < 8; ++q)
+            if (c1 + q < n) A[(int64_t)c * s + c1 + q] = out[q];
+    }
     if (t.ti != t.tj) {
 #pragma unroll
         for (int q = 0; q < 8; ++q)
@@ -574,7 +578,7 @@ bool tc_gram_maps(TcGramPlan &p, const float *hi, const float *lo) {
 
 cudaError_t tc_gram_run(const TcGramPlan &p, const UnitDesc *d_units, const TcGramUnit *d_gu, const TcTile *d_tiles,
                         const MixedUnit *d_mus, const cx *z, float *hi, float *lo, float2 *a32, int32_t *status,
-                        int max_n, cudaStream_t st, bool split) {
+                        int max_n, cudaStream_t st, bool split, bool lower_only) {
     if (p.units.empty()) return cudaSuccess;
     if (split) {  // else the fill has written the stacks
         int max_kb = (max_n + 31) / 32, max_cb = (max_n + 15) / 16;
@@ -587,6 +591,7 @@ cudaError_t tc_gram_run(const TcGramPlan &p, const UnitDesc *d_units, const TcGr
     ep.a32 = a32;
     ep.status = status;
     ep.status_of_tile = 1;
+    ep.lower_only = lower_only ? 1 : 0;
     return launch_tc<TC_EPI_GRAM>(p.m_hi, p.m_lo, p.m_hi, p.m_lo, d_tiles, (int)p.tiles.size(), ep, st);
 }
 

@@ -58,6 +58,7 @@ struct TcEpilogue {
     const UnitDesc *units;
     const MixedUnit *mus;
     float2 *a32;
+    int32_t lower_only;  // off-diagonal tiles write only their mirrored (lower) entries
     // both: a CTA whose waits ran out marks status[unit] (or status[0])
     int32_t *status;
     int32_t status_of_tile;
@@ -120,8 +121,11 @@ cudaError_t tc_gram_plan(const std::vector<UnitDesc> &systems, TcGramPlan &p);
 bool tc_gram_maps(TcGramPlan &p, const float *hi, const float *lo);
 // Z -> hi/lo stacks, then the tile GEMM writing Z^H Z into each unit's A32
 // (its N x N block).
+// lower_only: write only the tiles' lower-triangle entries (and the
+// diagonal tiles whole), enough for the Hermitian factor
 cudaError_t tc_gram_run(const TcGramPlan &p, const UnitDesc *d_units, const TcGramUnit *d_gu, const TcTile *d_tiles,
                         const MixedUnit *d_mus, const cx *z, float *hi, float *lo, float2 *a32, int32_t *status,
-                        int max_n, cudaStream_t st, bool split = true);  // split false: the fill wrote the stacks
+                        int max_n, cudaStream_t st, bool split = true,  // split false: the fill wrote the stacks
+                        bool lower_only = false);
 
 }  // namespace fnec
