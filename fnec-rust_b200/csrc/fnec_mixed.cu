@@ -970,14 +970,16 @@ __device__ void herm_rows(float2 *A, int s, int c0, int r_begin, int r_end, cons
 // it; sDinv: 1 / U11[i][i]), in FP32, by threads 0 .. 255: threads
 // 0 .. 127 form L11^-1, 128 .. 255 U11^-1, four consecutive lanes per
 // column j, each summing the terms k = q (mod 4) of the substitution; the
-// quarter sums are added by two shuffles (a column's lanes share a warp)
-// and the column lives in X (a 32 x 33 scratch per triangle in shared
-// memory).  Stored row-major, L^-1 then U^-1 (2 x 1024 entries), zero
-// outside an nb < 32 block.
-__device__ void herm_block_inverse(const float2 (*sD)[MNB + 1], const float2 *sDinv, int nb, float2 (*X)[MNB + 1],
+// quarter sums are added by two shuffles (a column's lanes share a warp).
+// The columns live in X, column-major with a pitch of 36 entries per
+// column (a warp's 8 columns x 4 quarters then read 2-way-spread banks:
+// two wavefronts per 64-bit load, the minimum).  Stored row-major, L^-1
+// then U^-1 (2 x 1024 entries), zero outside an nb < 32 block.
+constexpr int BI_PITCH = 36;
+__device__ void herm_block_inverse(const float2 (*sD)[MNB + 1], const float2 *sDinv, int nb, float2 *X,
                                    float2 *out) {
     const int t = threadIdx.x, w = t >> 7, j = (t & 127) >> 2, q = t & 3;
-    X += w * 32;
+    float2 *Xj = X + (w * 32 + j) * BI_PITCH;  // column j of this triangle's inverse
     const bool live = j < nb;
     if (w == 0) {  // L^-1 e_j: forward, unit diagonal
         for (int i = 0; i < 32; ++i) {
@@ -985,13 +987,13 @@ __device__ void herm_block_inverse(const float2 (*sD)[MNB + 1], const float2 *sD
 #pragma unroll
             for (int m = 0; m < 8; ++m) {
                 const int k = q + 4 * m;
-                if (k < i && k < nb) p = cf_add(p, cf_mul(sD[i][k], X[k][j]));  // X[k][j] = 0 for k < j
+                if (k < i && k < nb) p = cf_add(p, cf_mul(sD[i][k], Xj[k]));  // Xj[k] = 0 for k < j
             }
             p.x += __shfl_xor_sync(0xffffffffu, p.x, 1);
             p.y += __shfl_xor_sync(0xffffffffu, p.y, 1);
             p.x += __shfl_xor_sync(0xffffffffu, p.x, 2);
             p.y += __shfl_xor_sync(0xffffffffu, p.y, 2);
-            if (q == 0) X[i][j] = (live && i >= j && i < nb) ? cf((i == j ? 1.f : 0.f) - p.x, -p.y) : cf(0.f, 0.f);
+            if (q == 0) Xj[i] = (live && i >= j && i < nb) ? cf((i == j ? 1.f : 0.f) - p.x, -p.y) : cf(0.f, 0.f);
             __syncwarp();
         }
     } else {  // U^-1 e_j: backward
@@ -1000,15 +1002,15 @@ __device__ void herm_block_inverse(const float2 (*sD)[MNB + 1], const float2 *sD
 #pragma unroll
             for (int m = 0; m < 8; ++m) {
                 const int k = q + 4 * m;
-                if (k > i && k < nb) p = cf_add(p, cf_mul(sD[i][k], X[k][j]));  // X[k][j] = 0 for k > j
+                if (k > i && k < nb) p = cf_add(p, cf_mul(sD[i][k], Xj[k]));  // Xj[k] = 0 for k > j
             }
             p.x += __shfl_xor_sync(0xffffffffu, p.x, 1);
             p.y += __shfl_xor_sync(0xffffffffu, p.y, 1);
             p.x += __shfl_xor_sync(0xffffffffu, p.x, 2);
             p.y += __shfl_xor_sync(0xffffffffu, p.y, 2);
             if (q == 0)
-                X[i][j] = (live && i <= j && i < nb) ? cf_mul(cf((i == j ? 1.f : 0.f) - p.x, -p.y), sDinv[i])
-                                                     : cf(0.f, 0.f);
+                Xj[i] = (live && i <= j && i < nb) ? cf_mul(cf((i == j ? 1.f : 0.f) - p.x, -p.y), sDinv[i])
+                                                   : cf(0.f, 0.f);
             __syncwarp();
         }
     }
@@ -1016,7 +1018,7 @@ __device__ void herm_block_inverse(const float2 (*sD)[MNB + 1], const float2 *sD
 #pragma unroll
     for (int m = 0; m < 8; ++m) {
         const int i = q + 4 * m;
-        out[i * 32 + j] = X[i][j];
+        out[i * 32 + j] = Xj[i];
     }
 }
 
@@ -1184,15 +1186,33 @@ __device__ void apply_A(const GmresCtx &g, const cx *v, cx *out, cx *sv, cx *st,
     for (int c = tid; c < n; c += blockDim.x) so[c] = {0, 0};
     __syncthreads();
     for (int rb = 0; rb < n; rb += ARB) {
-        for (int r = rb + wid; r < rb + ARB && r < n; r += 8) {
-            cx acc = {0, 0};
-            const cx *zr = g.z + (int64_t)r * n;
+        // a warp's ARB / 8 rows of the block together: their loads are in
+        // flight at once (each row's sum in the same order as alone)
+        constexpr int RPW = ARB / 8;
+        cx acc[RPW];
+        const cx *zr[RPW];
+        bool has[RPW];
+#pragma unroll
+        for (int q = 0; q < RPW; ++q) {
+            const int r = rb + wid + 8 * q;
+            acc[q] = {0, 0};
+            has[q] = r < n;
+            zr[q] = g.z + (int64_t)(has[q] ? r : 0) * n;
+        }
 #pragma unroll 4
-            for (int c = lane; c < n; c += 32) acc = zadd(acc, zmul(zr[c], sv[c]));
-            acc = warp_sum(acc);
-            if (lane == 0) {
+        for (int c = lane; c < n; c += 32) {
+            const cx x = sv[c];
+#pragma unroll
+            for (int q = 0; q < RPW; ++q)
+                if (has[q]) acc[q] = zadd(acc[q], zmul(zr[q][c], x));
+        }
+#pragma unroll
+        for (int q = 0; q < RPW; ++q) {
+            const int r = rb + wid + 8 * q;
+            const cx a = warp_sum(acc[q]);
+            if (lane == 0 && has[q]) {
                 cx cvv = sv[n + g.rowwire[r]];
-                st[r] = {acc.re - g.cv[r] * cvv.re, acc.im - g.cv[r] * cvv.im};
+                st[r] = {a.re - g.cv[r] * cvv.re, a.im - g.cv[r] * cvv.im};
             }
         }
         __syncthreads();
@@ -1432,7 +1452,7 @@ __global__ void __launch_bounds__(256) k_block_inv32(const UnitDesc *__restrict_
                                                      const int32_t *__restrict__ status) {
     __shared__ float2 sB[MNB][MNB + 1];
     __shared__ float2 sDinv[MNB];
-    __shared__ float2 sX[2 * MNB][MNB + 1];
+    __shared__ float2 sX[2 * MNB * BI_PITCH];
     const int ui = blockIdx.y;
     const UnitDesc u = units[ui];
     const int c0 = blockIdx.x * 32, s = u.s;
