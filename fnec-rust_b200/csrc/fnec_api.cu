@@ -1363,10 +1363,12 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
     }
     *out = b;
     // the default for many systems: every unit up to S 512 factored whole,
-    // one CTA each (enough of them to fill the GPU)
+    // one CTA each (enough of them to fill the GPU), and 4 refinement CTAs
+    // per SM (more solves in flight)
     if (precision == FNEC_PRECISION_MIXED && (int64_t)b->units.size() >= 2 * (int64_t)b->grid.sms) {
         fnec_schedule s = b->sched;
         s.unit_factor = 3;
+        if ((int64_t)b->solves.size() >= 8 * (int64_t)b->grid.sms) s.gmres_ctas_per_sm = 4;
         apply_schedule(b, s);
     }
     schedule_from_cache(b);

@@ -10,8 +10,8 @@
 // and their midpoints advance by a constant step, so along a wire
 //   sum_n I_n exp(jk r.(m0 + n d)) = exp(jk r.m0) * P(z),  z = exp(jk r.d),
 // with P(z) = sum_n I_n z^n evaluated by Horner's rule.  Each direction
-// costs two sincos per wire run and 4 FP64 FMAs per segment instead of one
-// sincos per segment; the rounding difference to the reference's direct sum
+// costs two sincos per wire run (sincospi_taylor on the phase in half-turns)
+// and 4 FP64 FMAs per segment instead of one sincos per segment; the rounding difference to the reference's direct sum
 // is O(n eps), i.e. ~1e-14 relative for runs of 100 segments (the parity
 // bar for gains is 1e-6 dB).  The integral is a fixed-order block tree
 // reduction (deterministic), and the gains, the Stokes axial ratio and the
@@ -19,6 +19,7 @@
 #include "fnec_kernels.h"
 #include "fnec_libm.cuh"
 #include "fnec_math.cuh"
+#include "fnec_sincospi.cuh"
 
 namespace fnec {
 
@@ -64,21 +65,23 @@ __device__ __forceinline__ void field_dir2(const DevRun *runs, int n_run, const 
                                            cx &fp0, cx &ft1, cx &fp1) {
     double a_tr = 0, a_ti = 0, a_pr = 0, a_pi = 0;
     double b_tr = 0, b_ti = 0, b_pr = 0, b_pi = 0;
+    const double kpi = k * 0.31830988618379067;  // k / pi
     for (int q = 0; q < n_run; ++q) {
         const DevRun &R = runs[q];
         for (int img = 0; img < (pec ? 2 : 1); ++img) {
             double m0 = R.mid0[0], m1 = R.mid0[1], m2 = img ? -R.mid0[2] : R.mid0[2];
             double s0 = R.step[0], s1 = R.step[1], s2 = img ? -R.step[2] : R.step[2];
             double d0 = img ? -R.dir[0] : R.dir[0], d1 = img ? -R.dir[1] : R.dir[1], d2 = R.dir[2];
-            double pa = k * (m0 * rh0[0] + m1 * rh0[1] + m2 * rh0[2]);
-            double da = k * (s0 * rh0[0] + s1 * rh0[1] + s2 * rh0[2]);
-            double pb = k * (m0 * rh1[0] + m1 * rh1[1] + m2 * rh1[2]);
-            double db = k * (s0 * rh1[0] + s1 * rh1[1] + s2 * rh1[2]);
+            // phases in half-turns (k / pi): sincospi_taylor needs no Cody-Waite reduction
+            double pa = kpi * (m0 * rh0[0] + m1 * rh0[1] + m2 * rh0[2]);
+            double da = kpi * (s0 * rh0[0] + s1 * rh0[1] + s2 * rh0[2]);
+            double pb = kpi * (m0 * rh1[0] + m1 * rh1[1] + m2 * rh1[2]);
+            double db = kpi * (s0 * rh1[0] + s1 * rh1[1] + s2 * rh1[2]);
             double eas, eac, zas, zac, ebs, ebc, zbs, zbc;
-            sincos(pa, &eas, &eac);
-            sincos(da, &zas, &zac);
-            sincos(pb, &ebs, &ebc);
-            sincos(db, &zbs, &zbc);
+            sincospi_taylor_signed(pa, eas, eac);
+            sincospi_taylor_signed(da, zas, zac);
+            sincospi_taylor_signed(pb, ebs, ebc);
+            sincospi_taylor_signed(db, zbs, zbc);
             const cx *I = cur + R.first;
             int c = R.count;
             cx last = I[c - 1];
@@ -135,9 +138,9 @@ __device__ __forceinline__ bool run_is_vertical(const DevRun &R) {
 // over its currents, as in field_dir2
 __device__ __forceinline__ cx run_poly(const DevRun &R, const cx *cur, double k, int img, const double *rh) {
     double s0 = R.step[0], s1 = R.step[1], s2 = img ? -R.step[2] : R.step[2];
-    double da = k * (s0 * rh[0] + s1 * rh[1] + s2 * rh[2]);
+    double da = k * 0.31830988618379067 * (s0 * rh[0] + s1 * rh[1] + s2 * rh[2]);  // half-turns
     double zas, zac;
-    sincos(da, &zas, &zac);
+    sincospi_taylor_signed(da, zas, zac);
     const cx *I = cur + R.first;
     int c = R.count;
     cx last = I[c - 1];
@@ -161,9 +164,9 @@ __device__ __forceinline__ void field_vert(const DevRun *runs, int n_run, const 
         for (int img = 0; img < (pec ? 2 : 1); ++img) {
             double m0 = R.mid0[0], m1 = R.mid0[1], m2 = img ? -R.mid0[2] : R.mid0[2];
             double d0 = img ? -R.dir[0] : R.dir[0], d1 = img ? -R.dir[1] : R.dir[1], d2 = R.dir[2];
-            double pa = k * (m0 * rh[0] + m1 * rh[1] + m2 * rh[2]);
+            double pa = k * 0.31830988618379067 * (m0 * rh[0] + m1 * rh[1] + m2 * rh[2]);  // half-turns
             double eas, eac;
-            sincos(pa, &eas, &eac);
+            sincospi_taylor_signed(pa, eas, eac);
             const cx acc = P[q * 2 + img];
             double fr = (eac * acc.re - eas * acc.im) * R.len, fi = (eac * acc.im + eas * acc.re) * R.len;
             double pta = d0 * th[0] + d1 * th[1] + d2 * th[2];

@@ -26,6 +26,7 @@
 
 #include "fnec_grid.cuh"
 #include "fnec_mixed.h"
+#include "fnec_sincospi.cuh"
 #include "fnec_tc.h"
 
 namespace fnec {
@@ -74,55 +75,11 @@ __constant__ double m_gl_w8[8] = {0.101228536290376, 0.222381034453374, 0.313706
 // ---------------------------------------------------------------------------
 // fast FP64 fill (matrix.rs:297-331 with hardware sincos/log and FMA)
 // ---------------------------------------------------------------------------
-// sin(pi x) and cos(pi x) for 0 <= x < 2^50, the phase of the fill's
-// samples.  Quadrant reduction in half-turns: adding 1.5 * 2^52 rounds 2x
-// to the integer n (its low bits are n), and f = x - n / 2 is exact with
-// |f| <= 1/4; then the Taylor series of sin and cos at theta = pi f
-// (|theta| <= pi/4) to theta^15 and theta^16, whose truncation error is
-// below 5e-17, in Horner form in theta^2, and the quadrant n mod 4 swaps
-// and signs the pair.  About 22 FP64 operations and no table.
-__host__ __device__ __forceinline__ void fill_sincospi(double x, double &sn, double &cs) {
-    const double big = 6755399441055744.0;  // 1.5 * 2^52
-    const double t = fma(x, 2.0, big);
-    const double nd = t - big;
-#ifdef __CUDA_ARCH__
-    const int q = __double2loint(t) & 3;
-#else
-    long long bits;
-    memcpy(&bits, &t, sizeof(bits));
-    const int q = (int)(bits & 3);
-#endif
-    const double th = fma(nd, -0.5, x) * 3.141592653589793;
-    const double t2 = th * th;
-    // sin: theta (1 + t2 (-1/3! + t2 (1/5! - ... - t2 / 15!)))
-    double ps = -7.647163731819816e-13;  // -1/15!
-    ps = fma(ps, t2, 1.6059043836821613e-10);   // 1/13!
-    ps = fma(ps, t2, -2.505210838544172e-08);   // -1/11!
-    ps = fma(ps, t2, 2.7557319223985893e-06);   // 1/9!
-    ps = fma(ps, t2, -0.0001984126984126984);   // -1/7!
-    ps = fma(ps, t2, 0.008333333333333333);    // 1/5!
-    ps = fma(ps, t2, -0.16666666666666666);  // -1/3!
-    const double s0 = fma(th * t2, ps, th);
-    // cos: 1 + t2 (-1/2! + t2 (1/4! - ... + t2 / 16!))
-    double pc = 4.779477332387385e-14;  // 1/16!
-    pc = fma(pc, t2, -1.1470745597729725e-11);  // -1/14!
-    pc = fma(pc, t2, 2.08767569878681e-09);     // 1/12!
-    pc = fma(pc, t2, -2.755731922398589e-07);   // -1/10!
-    pc = fma(pc, t2, 2.48015873015873e-05);     // 1/8!
-    pc = fma(pc, t2, -0.001388888888888889);  // -1/6!
-    pc = fma(pc, t2, 0.041666666666666664);   // 1/4!
-    pc = fma(pc, t2, -0.5);                     // -1/2!
-    const double c0 = fma(t2, pc, 1.0);
-    const double a = (q & 1) ? c0 : s0, b = (q & 1) ? s0 : c0;
-    sn = (q & 2) ? -a : a;
-    cs = ((q + 1) & 2) ? -b : b;
-}
-
 // Z element (obs midpoint om, source segment mid sm / unit direction sd /
 // length slen / radius srad); the far form takes the midpoint difference
 // d = om - sm and the half-length step hs = sd slen / 2 once per element,
 // then per Gauss-Legendre sample r = d - x_m hs, R^2 = |r|^2 + a^2, one
-// reciprocal square root for R and 1/R and fill_sincospi(k R / pi).
+// reciprocal square root for R and 1/R and sincospi_taylor(k R / pi).
 __device__ __forceinline__ cx elem_fast(const double *om, const double *od, const double *sm, const double *sd,
                                         double slen, double srad, double k, bool is_self) {
     double cos_alpha = od[0] * sd[0] + od[1] * sd[1] + od[2] * sd[2];
@@ -155,7 +112,7 @@ __device__ __forceinline__ cx elem_fast(const double *om, const double *od, cons
             const double r2s = fma(r0, r0, fma(r1, r1, fma(r2, r2, a2)));
             const double inv = rsqrt(r2s);
             double sn, cs;
-            fill_sincospi(kpi * (r2s * inv), sn, cs);
+            sincospi_taylor(kpi * (r2s * inv), sn, cs);
             const double wr = m_gl_w8[m] * inv;
             ire = fma(wr, cs, ire);
             iim = fma(-wr, sn, iim);  // e^{-jkR}
@@ -1269,6 +1226,59 @@ __device__ void apply_A(const GmresCtx &g, const cx *v, cx *out, cx *sv, cx *st,
 // in/out are FP64, sy is shared memory (S).
 __device__ __forceinline__ cx f2z(float2 a) { return {(double)a.x, (double)a.y}; }
 
+// y = B x for a 32x32 diagonal-block inverse B (FP32, row-major) and x the
+// block's entries of sy: every warp takes 4 rows, their 4 products' warp
+// sums interleaved (each row's sum in the same order as alone), into s_blk.
+__device__ __forceinline__ void block_product(const float2 *B, const cx *sy, int c0, int nb, cx *s_blk) {
+    const int lane = threadIdx.x & 31, i0 = (threadIdx.x >> 5) * 4;
+    const cx xk = lane < nb ? sy[c0 + lane] : cx{0, 0};
+    cx p[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) p[q] = (lane < nb && i0 + q < nb) ? zmul(f2z(B[(i0 + q) * 32 + lane]), xk) : cx{0, 0};
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            p[q].re += __shfl_down_sync(0xffffffffu, p[q].re, o);
+            p[q].im += __shfl_down_sync(0xffffffffu, p[q].im, o);
+        }
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (i0 + q < nb) s_blk[i0 + q] = p[q];
+}
+
+// sy[r] -= F[r][c0 .. c0 + 32) s_blk for rows r in [r_lo, r_hi) (F the FP32
+// factor, full 32-column blocks), two rows per thread at once so that both
+// rows' loads are in flight together (each row's sum in column order).
+__device__ __forceinline__ void block_update(const float2 *lu, int s, int c0, int r_lo, int r_hi, cx *sy,
+                                             const cx *s_blk) {
+    const int nt = blockDim.x;
+    for (int r = r_lo + threadIdx.x; r < r_hi; r += 2 * nt) {
+        const int r2 = r + nt;
+        const bool two = r2 < r_hi;
+        const float2 *f0 = lu + (int64_t)r * s + c0;
+        const float2 *f1 = lu + (int64_t)(two ? r2 : r) * s + c0;
+        cx a0 = sy[r], a1 = two ? sy[r2] : cx{0, 0};
+#pragma unroll
+        for (int c8 = 0; c8 < 32; c8 += 8) {
+            float2 l0[8], l1[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                l0[c] = f0[c8 + c];
+                l1[c] = f1[c8 + c];
+            }
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                a0 = zsub(a0, zmul(f2z(l0[c]), s_blk[c8 + c]));
+                a1 = zsub(a1, zmul(f2z(l1[c]), s_blk[c8 + c]));
+            }
+        }
+        sy[r] = a0;
+        if (two) sy[r2] = a1;
+    }
+}
+
 __device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, cx *sy) {
     int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     int s = g.s;
@@ -1295,41 +1305,22 @@ __device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, cx *sy) {
         __shared__ cx s_blk[32];
         for (int c0 = 0; c0 < s; c0 += 32) {
             const int nb = min(32, s - c0);
-            const float2 *Li = g.binv + (int64_t)(c0 / 32) * 2048;
-            const cx xk = lane < nb ? sy[c0 + lane] : cx{0, 0};
-            for (int i = wid; i < nb; i += (int)(blockDim.x >> 5)) {
-                cx p = warp_sum(lane < nb ? zmul(f2z(Li[i * 32 + lane]), xk) : cx{0, 0});
-                if (lane == 0) s_blk[i] = p;
-            }
+            block_product(g.binv + (int64_t)(c0 / 32) * 2048, sy, c0, nb, s_blk);
             __syncthreads();
             for (int i = tid; i < nb; i += blockDim.x) sy[c0 + i] = s_blk[i];
-            if (nb == 32) {
-                for (int r = c0 + 32 + tid; r < s; r += blockDim.x) {
-                    const float2 *lrow = g.lu + (int64_t)r * s + c0;
-                    cx acc = sy[r];
-#pragma unroll
-                    for (int c8 = 0; c8 < 32; c8 += 8) {
-                        float2 lr[8];
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) lr[c] = lrow[c8 + c];
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) acc = zsub(acc, zmul(f2z(lr[c]), s_blk[c8 + c]));
-                    }
-                    sy[r] = acc;
-                }
-            }
+            if (nb == 32) block_update(g.lu, s, c0, c0 + 32, s, sy, s_blk);
             __syncthreads();
         }
         for (int c0 = ((s - 1) / 32) * 32; c0 >= 0; c0 -= 32) {
             const int nb = min(32, s - c0);
-            const float2 *Ui = g.binv + (int64_t)(c0 / 32) * 2048 + 1024;
-            const cx xk = lane < nb ? sy[c0 + lane] : cx{0, 0};
-            for (int i = wid; i < nb; i += (int)(blockDim.x >> 5)) {
-                cx p = warp_sum(lane < nb ? zmul(f2z(Ui[i * 32 + lane]), xk) : cx{0, 0});
-                if (lane == 0) s_blk[i] = p;
-            }
+            block_product(g.binv + (int64_t)(c0 / 32) * 2048 + 1024, sy, c0, nb, s_blk);
             __syncthreads();
             for (int i = tid; i < nb; i += blockDim.x) sy[c0 + i] = s_blk[i];
+            if (nb == 32) {
+                block_update(g.lu, s, c0, 0, c0, sy, s_blk);
+                __syncthreads();
+                continue;
+            }
             for (int r = tid; r < c0; r += blockDim.x) {
                 const float2 *urow = g.lu + (int64_t)r * s + c0;
                 cx acc = sy[r];
@@ -2880,7 +2871,7 @@ extern "C" int fnec_test_fill_sincospi(const double *x, uint64_t n, double *sin_
     if ((n && (!x || !sin_out || !cos_out))) return FNEC_ERR_BAD_ARG;
     for (uint64_t i = 0; i < n; ++i) {
         if (!(x[i] >= 0.0 && x[i] < 1125899906842624.0)) return FNEC_ERR_BAD_ARG;  // [0, 2^50)
-        fnec::fill_sincospi(x[i], sin_out[i], cos_out[i]);
+        fnec::sincospi_taylor(x[i], sin_out[i], cos_out[i]);
     }
     return FNEC_OK;
 }
