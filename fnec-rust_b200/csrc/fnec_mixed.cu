@@ -1226,59 +1226,6 @@ __device__ void apply_A(const GmresCtx &g, const cx *v, cx *out, cx *sv, cx *st,
 // in/out are FP64, sy is shared memory (S).
 __device__ __forceinline__ cx f2z(float2 a) { return {(double)a.x, (double)a.y}; }
 
-// y = B x for a 32x32 diagonal-block inverse B (FP32, row-major) and x the
-// block's entries of sy: every warp takes 4 rows, their 4 products' warp
-// sums interleaved (each row's sum in the same order as alone), into s_blk.
-__device__ __forceinline__ void block_product(const float2 *B, const cx *sy, int c0, int nb, cx *s_blk) {
-    const int lane = threadIdx.x & 31, i0 = (threadIdx.x >> 5) * 4;
-    const cx xk = lane < nb ? sy[c0 + lane] : cx{0, 0};
-    cx p[4];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) p[q] = (lane < nb && i0 + q < nb) ? zmul(f2z(B[(i0 + q) * 32 + lane]), xk) : cx{0, 0};
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            p[q].re += __shfl_down_sync(0xffffffffu, p[q].re, o);
-            p[q].im += __shfl_down_sync(0xffffffffu, p[q].im, o);
-        }
-    if (lane == 0)
-#pragma unroll
-        for (int q = 0; q < 4; ++q)
-            if (i0 + q < nb) s_blk[i0 + q] = p[q];
-}
-
-// sy[r] -= F[r][c0 .. c0 + 32) s_blk for rows r in [r_lo, r_hi) (F the FP32
-// factor, full 32-column blocks), two rows per thread at once so that both
-// rows' loads are in flight together (each row's sum in column order).
-__device__ __forceinline__ void block_update(const float2 *lu, int s, int c0, int r_lo, int r_hi, cx *sy,
-                                             const cx *s_blk) {
-    const int nt = blockDim.x;
-    for (int r = r_lo + threadIdx.x; r < r_hi; r += 2 * nt) {
-        const int r2 = r + nt;
-        const bool two = r2 < r_hi;
-        const float2 *f0 = lu + (int64_t)r * s + c0;
-        const float2 *f1 = lu + (int64_t)(two ? r2 : r) * s + c0;
-        cx a0 = sy[r], a1 = two ? sy[r2] : cx{0, 0};
-#pragma unroll
-        for (int c8 = 0; c8 < 32; c8 += 8) {
-            float2 l0[8], l1[8];
-#pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                l0[c] = f0[c8 + c];
-                l1[c] = f1[c8 + c];
-            }
-#pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                a0 = zsub(a0, zmul(f2z(l0[c]), s_blk[c8 + c]));
-                a1 = zsub(a1, zmul(f2z(l1[c]), s_blk[c8 + c]));
-            }
-        }
-        sy[r] = a0;
-        if (two) sy[r2] = a1;
-    }
-}
-
 __device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, cx *sy) {
     int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     int s = g.s;
@@ -1305,22 +1252,41 @@ __device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, cx *sy) {
         __shared__ cx s_blk[32];
         for (int c0 = 0; c0 < s; c0 += 32) {
             const int nb = min(32, s - c0);
-            block_product(g.binv + (int64_t)(c0 / 32) * 2048, sy, c0, nb, s_blk);
+            const float2 *Li = g.binv + (int64_t)(c0 / 32) * 2048;
+            const cx xk = lane < nb ? sy[c0 + lane] : cx{0, 0};
+            for (int i = wid; i < nb; i += (int)(blockDim.x >> 5)) {
+                cx p = warp_sum(lane < nb ? zmul(f2z(Li[i * 32 + lane]), xk) : cx{0, 0});
+                if (lane == 0) s_blk[i] = p;
+            }
             __syncthreads();
             for (int i = tid; i < nb; i += blockDim.x) sy[c0 + i] = s_blk[i];
-            if (nb == 32) block_update(g.lu, s, c0, c0 + 32, s, sy, s_blk);
+            if (nb == 32) {
+                for (int r = c0 + 32 + tid; r < s; r += blockDim.x) {
+                    const float2 *lrow = g.lu + (int64_t)r * s + c0;
+                    cx acc = sy[r];
+#pragma unroll
+                    for (int c8 = 0; c8 < 32; c8 += 8) {
+                        float2 lr[8];
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) lr[c] = lrow[c8 + c];
+#pragma unroll
+                        for (int c = 0; c < 8; ++c) acc = zsub(acc, zmul(f2z(lr[c]), s_blk[c8 + c]));
+                    }
+                    sy[r] = acc;
+                }
+            }
             __syncthreads();
         }
         for (int c0 = ((s - 1) / 32) * 32; c0 >= 0; c0 -= 32) {
             const int nb = min(32, s - c0);
-            block_product(g.binv + (int64_t)(c0 / 32) * 2048 + 1024, sy, c0, nb, s_blk);
+            const float2 *Ui = g.binv + (int64_t)(c0 / 32) * 2048 + 1024;
+            const cx xk = lane < nb ? sy[c0 + lane] : cx{0, 0};
+            for (int i = wid; i < nb; i += (int)(blockDim.x >> 5)) {
+                cx p = warp_sum(lane < nb ? zmul(f2z(Ui[i * 32 + lane]), xk) : cx{0, 0});
+                if (lane == 0) s_blk[i] = p;
+            }
             __syncthreads();
             for (int i = tid; i < nb; i += blockDim.x) sy[c0 + i] = s_blk[i];
-            if (nb == 32) {
-                block_update(g.lu, s, c0, 0, c0, sy, s_blk);
-                __syncthreads();
-                continue;
-            }
             for (int r = tid; r < c0; r += blockDim.x) {
                 const float2 *urow = g.lu + (int64_t)r * s + c0;
                 cx acc = sy[r];
