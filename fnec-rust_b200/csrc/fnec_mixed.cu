@@ -2660,7 +2660,7 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         // panels, one exchange area) all stay in the first group
         int n_tall = 0;
         while (!herm && n_tall < i_unit && gp.s_desc[n_tall] > thr_rows) ++n_tall;
-        if (!herm && mw.trail && mw.use_tc_trail) n_tall = std::max(n_tall, std::min(mw.trail_n, i_unit));  // one stack set
+        if (mw.trail && mw.use_tc_trail) n_tall = std::max(n_tall, std::min(mw.trail_n, i_unit));  // one stack set
         double tot = 0, acc = 0;
         for (int i = 0; i < i_unit; ++i) tot += (double)gp.s_desc[i] * gp.s_desc[i] * gp.s_desc[i];
         for (int i = 0; i < i_unit && (int)gb.size() < G; ++i) {
@@ -2698,7 +2698,9 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     cudaStream_t fs = grp == 0 ? st : mw.fstream[grp - 1];
     for (int c0 = 0; herm && gi0 < gi1 && c0 < gp.s_desc[gi0]; c0 += MNB) {
         // Hermitian factor: panel (diagonal block, L21, mirrored U12), then
-        // the trailing tiles on and below the diagonal, per size class
+        // the trailing tiles on and below the diagonal, per size class: the
+        // largest units' on the tensor cores when tensor_trailing is on (a
+        // prefix of the order, in the first group), the rest as SIMT tiles
         step_classes(gp, c0, gi0, cls, gi1);
         for (const StepClass &c : cls) {
             if (c.m_max - MNB > 256)
@@ -2707,6 +2709,9 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
                 k_panel32_herm<256><<<c.i1 - c.i0, 256, 0, fs>>>(d_units, mw.smu, c0, mw.a32, piv, status, ord, c.i0);
             ++L;
         }
+        const int k_tc =
+            (grp == 0 && mw.trail && mw.use_tc_trail) ? std::min(mw.trail->active(c0 / MNB), i_unit) : 0;
+        step_classes(gp, c0, std::max(gi0, k_tc), cls, gi1);
         for (const StepClass &c : cls) {
             const int rows = c.m_max - MNB;
             if (rows <= 0) continue;
@@ -2714,6 +2719,11 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
             dim3 g2(T * (T + 1) / 2, c.i1 - c.i0);
             k_trailing32<<<g2, 256, 0, fs>>>(d_units, mw.smu, c0, mw.a32, status, ord, c.i0, 1, INT_MAX, 1);
             ++L;
+        }
+        if (k_tc > 0) {
+            tc_trail_run(*mw.trail, c0 / MNB, k_tc, static_cast<const TcTrailUnit *>(mw.d_trail), d_units, mw.smu, mw.a32,
+                         mw.tr_hi, mw.tr_lo, status, fs, true);
+            L += 3;
         }
     }
     for (int c0 = 0; !herm && gi0 < gi1 && c0 < gp.s_desc[gi0]; c0 += MNB) {

@@ -223,6 +223,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const TcTrailUnit tu = ep.trail[blockIdx.y];
         const int ntj = tu.n2_pad / BN, ti = (int)blockIdx.x / ntj, tj = (int)blockIdx.x % ntj;
         if (ti >= tu.m_pad / BM) return;  // the whole CTA, before any barrier or TMEM allocation
+        // complex columns [64 tj, 64 tj + 64) against rows [128 ti, 128 ti + 128):
+        // wholly above the diagonal when 64 tj > 128 ti + 127
+        if (ep.trail_lower && tj > 2 * ti + 1) return;
         t.a_row = (int32_t)(tu.a_base + (int64_t)ti * BM);
         t.b_row = (int32_t)(tu.b_base + (int64_t)tj * BN);
         t.a_kstride = tu.m_pad;
@@ -547,7 +550,8 @@ bool tc_trail_maps(TcTrailPlan &p, const float *hi, const float *lo) {
 }
 
 cudaError_t tc_trail_run(const TcTrailPlan &p, int step, int count, const TcTrailUnit *d_trail, const UnitDesc *d_systems,
-                         const MixedUnit *d_smu, float2 *a32, float *hi, float *lo, int32_t *status, cudaStream_t st) {
+                         const MixedUnit *d_smu, float2 *a32, float *hi, float *lo, int32_t *status, cudaStream_t st,
+                         bool lower) {
     const int na = std::min(count, p.active(step));
     if (na <= 0) return cudaSuccess;
     const TcTrailUnit *tl = d_trail + p.u_off[step];
@@ -566,6 +570,7 @@ cudaError_t tc_trail_run(const TcTrailPlan &p, int step, int count, const TcTrai
     ep.status_of_tile = 1;
     ep.c0 = c0;
     ep.trail = tl;
+    ep.trail_lower = lower ? 1 : 0;
     k_tc_gemm<TC_EPI_TRAIL><<<dim3((unsigned)p.max_tiles[step], (unsigned)na), TC_THREADS, tc_smem_bytes(), st>>>(
         p.m_hi, p.m_lo, p.m_hi, p.m_lo, nullptr, ep);
     return cudaGetLastError();

@@ -62,9 +62,12 @@ struct TcEpilogue {
     // both: a CTA whose waits ran out marks status[unit] (or status[0])
     int32_t *status;
     int32_t status_of_tile;
-    // TC_EPI_TRAIL: the step and its units (blockIdx.y), tiles from blockIdx.x
+    // TC_EPI_TRAIL: the step and its units (blockIdx.y), tiles from blockIdx.x;
+    // trail_lower: only tiles reaching the diagonal or below it (the
+    // Hermitian factor), the others leave at once
     int32_t c0;
     const TcTrailUnit *trail;
+    int32_t trail_lower;
     // limit of every mbarrier wait (0: TC_WAIT_NS, 2 s)
     uint64_t wait_ns;
     // self-test of the timeout path only: the producer stops issuing loads
@@ -112,8 +115,10 @@ bool tc_trail_maps(TcTrailPlan &p, const float *hi, const float *lo);
 // Step `step` (c0 = 32 step): split L21 / U12 of the step's first `count`
 // units (<= active(step)) into the stacks, then the GEMM subtracting
 // L21 U12 from each one's A22.
+// lower: the Hermitian factor's update, tiles on and below the diagonal only
 cudaError_t tc_trail_run(const TcTrailPlan &p, int step, int count, const TcTrailUnit *d_trail, const UnitDesc *d_systems,
-                         const MixedUnit *d_smu, float2 *a32, float *hi, float *lo, int32_t *status, cudaStream_t st);
+                         const MixedUnit *d_smu, float2 *a32, float *hi, float *lo, int32_t *status, cudaStream_t st,
+                         bool lower = false);
 
 cudaError_t tc_gram_plan(const std::vector<UnitDesc> &systems, TcGramPlan &p);
 // Tensor maps over the hi / lo stacks (rows x 32 floats each); false when

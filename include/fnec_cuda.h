@@ -674,17 +674,19 @@ typedef struct {
                               diagonal blocks through their FP64 inverses (block
                               products); 0 by substitution in one warp            */
     int32_t tensor_trailing;/* mixed: 1 trailing updates of >= 192 rows run on
-                              tcgen05 (3xTF32, complex as one real GEMM of K 64);
-                              0 all as FP32 SIMT tiles, one pass per step; 2
-                              SIMT tiles once per two steps (the first step
-                              updates only the next panel's columns)            */
+                              tcgen05 (3xTF32, complex as one real GEMM of K 64;
+                              for the Hermitian factor only the tiles on and
+                              below the diagonal); 0 all as FP32 SIMT tiles, one
+                              pass per step; 2 (GEPP only) SIMT tiles once per
+                              two steps (the first step updates only the next
+                              panel's columns)                                   */
     int32_t gmres_ctas_per_sm;/* mixed: 3 or 4 refinement CTAs per SM (the
                               register budget of the one-CTA-per-solve kernel)    */
     int32_t factor_pivoting;/* mixed: 0 the FP32 factor of the Hermitian normal
                               equations without row exchanges (lower-triangle
                               trailing updates, U12 mirrored from L21); 1 GEPP
-                              with partial pivoting (tensor_trailing applies
-                              only here)                                          */
+                              with partial pivoting (row exchanges and U12
+                              solves; tensor_trailing 2 applies to it only)     */
 } fnec_schedule;
 
 /* Graph state of a batch (fnec_batch_graph_state). */

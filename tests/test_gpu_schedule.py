@@ -202,11 +202,13 @@ def test_mixed_factor_groups_give_identical_bits(acc, pivoting):
     b.close()
 
 
+@pytest.mark.parametrize("pivoting", [1, 0])
 @pytest.mark.parametrize("cells", [9, 12])
-def test_tensor_core_trailing_keeps_the_refinement(acc, cells):
+def test_tensor_core_trailing_keeps_the_refinement(acc, cells, pivoting):
     """The factor's trailing updates on tcgen05 (3xTF32) give a preconditioner
     as good as the FP32 SIMT one: the same answer within the gate and no more
-    than one extra refinement iteration."""
+    than one extra refinement iteration -- for GEPP and for the Hermitian
+    factor (tiles on and below the diagonal only)."""
     wl, src, f = bench.mesh_workload(cells)
     ant = [acc.Antenna(acc.wires_array(wl), acc.sources_array(src), [f], acc.GROUND_PEC, None)]
     plain = acc.HallenBatch(ant, precision=acc.PRECISION_FP64)
@@ -216,7 +218,7 @@ def test_tensor_core_trailing_keeps_the_refinement(acc, cells):
     for tt in (0, 1):
         b = acc.HallenBatch(ant, precision=acc.PRECISION_MIXED)
         assert b.info.max_s - 32 >= 192
-        b.schedule = {"tensor_trailing": tt, "factor_pivoting": 1}  # GEPP's trailing updates
+        b.schedule = {"tensor_trailing": tt, "factor_pivoting": pivoting}
         res = _run(b)
         assert np.all(res.status == 0)
         it, rs = b.refinement_stats()
