@@ -1007,6 +1007,63 @@ __global__ void __launch_bounds__(NT) k_panel32_herm(const UnitDesc *__restrict_
     if (nb == MNB) herm_rows<NT>(A, s, c0, c0 + MNB, s, sD, sDinv);
 }
 
+// Tall panels (more than HERM_SPLIT_ROWS rows below the diagonal block)
+// in two launches, so that their rows spread over many CTAs: the diagonal
+// block first (one CTA per unit, stored in place with its pivots), then
+// the rows in chunks of HERM_ROWS_CHUNK, each CTA loading the stored block
+// and recomputing the pivots' reciprocals with the same operations -- every
+// stored entry is the one-CTA panel's.
+constexpr int HERM_SPLIT_ROWS = 1024;
+constexpr int HERM_ROWS_CHUNK = 256;
+
+__global__ void __launch_bounds__(256) k_herm_diag(const UnitDesc *__restrict__ units,
+                                                   const MixedUnit *__restrict__ mus, int c0, float2 *a32buf,
+                                                   int32_t *piv_buf, int32_t *status,
+                                                   const int32_t *__restrict__ order, int base) {
+    __shared__ float2 sD[MNB][MNB + 1];
+    __shared__ float2 sDinv[MNB];
+    __shared__ int s_bad;
+    const int ui = order[base + blockIdx.x];
+    const UnitDesc u = units[ui];
+    const int s = u.s;
+    if (c0 >= s || status[ui] != 0) return;
+    const int nb = min(MNB, s - c0);
+    float2 *A = a32buf + mus[ui].a32_off;
+    herm_diag_block<256>(A, s, c0, nb, sD, sDinv, &s_bad);
+    const int tid = threadIdx.x;
+    if (s_bad) {
+        if (tid == 0) status[ui] = -(c0 + s_bad);
+        return;
+    }
+    for (int e = tid; e < nb * nb; e += 256) A[(int64_t)(c0 + e / nb) * s + c0 + e % nb] = sD[e / nb][e % nb];
+    if (tid < nb) piv_buf[u.piv_off + c0 + tid] = c0 + tid;
+}
+
+__global__ void __launch_bounds__(HERM_ROWS_CHUNK) k_herm_rows(const UnitDesc *__restrict__ units,
+                                                               const MixedUnit *__restrict__ mus, int c0,
+                                                               float2 *a32buf, const int32_t *__restrict__ status,
+                                                               const int32_t *__restrict__ order, int base) {
+    __shared__ float2 sD[MNB][MNB + 1];
+    __shared__ float2 sDinv[MNB];
+    const int ui = order[base + blockIdx.y];
+    const UnitDesc u = units[ui];
+    const int s = u.s;
+    if (c0 + MNB >= s || status[ui] != 0) return;  // no rows below a full block (status: set before this launch)
+    const int r_begin = c0 + MNB + (int)blockIdx.x * HERM_ROWS_CHUNK;
+    if (r_begin >= s) return;
+    float2 *A = a32buf + mus[ui].a32_off;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < MNB * MNB; e += HERM_ROWS_CHUNK) sD[e / MNB][e % MNB] = A[(int64_t)(c0 + e / MNB) * s + c0 + e % MNB];
+    __syncthreads();
+    if (tid < MNB) {  // as herm_diag_block forms them from the same pivots
+        const float2 d = sD[tid][tid];
+        const float dn = d.x * d.x + d.y * d.y;
+        sDinv[tid] = cf(d.x / dn, -d.y / dn);
+    }
+    __syncthreads();
+    herm_rows<HERM_ROWS_CHUNK>(A, s, c0, r_begin, min(s, r_begin + HERM_ROWS_CHUNK), sD, sDinv);
+}
+
 // The whole Hermitian factor of one small unit (S <= fu_max_s(level)) per
 // CTA: the per-step kernels' operations without a launch between steps.
 __global__ void __launch_bounds__(FU_THREADS, 4) k_factor32_unit_herm(const UnitDesc *__restrict__ units,
@@ -2703,11 +2760,19 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
         // prefix of the order, in the first group), the rest as SIMT tiles
         step_classes(gp, c0, gi0, cls, gi1);
         for (const StepClass &c : cls) {
-            if (c.m_max - MNB > 256)
+            const int rows = c.m_max - MNB;
+            if (rows > HERM_SPLIT_ROWS) {  // tall: the diagonal block, then the rows over many CTAs
+                k_herm_diag<<<c.i1 - c.i0, 256, 0, fs>>>(d_units, mw.smu, c0, mw.a32, piv, status, ord, c.i0);
+                dim3 gr((unsigned)((rows + HERM_ROWS_CHUNK - 1) / HERM_ROWS_CHUNK), (unsigned)(c.i1 - c.i0));
+                k_herm_rows<<<gr, HERM_ROWS_CHUNK, 0, fs>>>(d_units, mw.smu, c0, mw.a32, status, ord, c.i0);
+                L += 2;
+            } else if (rows > 256) {
                 k_panel32_herm<1024><<<c.i1 - c.i0, 1024, 0, fs>>>(d_units, mw.smu, c0, mw.a32, piv, status, ord, c.i0);
-            else
+                ++L;
+            } else {
                 k_panel32_herm<256><<<c.i1 - c.i0, 256, 0, fs>>>(d_units, mw.smu, c0, mw.a32, piv, status, ord, c.i0);
-            ++L;
+                ++L;
+            }
         }
         const int k_tc =
             (grp == 0 && mw.trail && mw.use_tc_trail) ? std::min(mw.trail->active(c0 / MNB), i_unit) : 0;

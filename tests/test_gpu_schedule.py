@@ -203,7 +203,7 @@ def test_mixed_factor_groups_give_identical_bits(acc, pivoting):
 
 
 @pytest.mark.parametrize("pivoting", [1, 0])
-@pytest.mark.parametrize("cells", [9, 12])
+@pytest.mark.parametrize("cells", [9, 12, 16])
 def test_tensor_core_trailing_keeps_the_refinement(acc, cells, pivoting):
     """The factor's trailing updates on tcgen05 (3xTF32) give a preconditioner
     as good as the FP32 SIMT one: the same answer within the gate and no more
