@@ -34,7 +34,7 @@ constexpr int BM = 128, BN = 128, BK = 32;
 constexpr int STAGES = 3;
 constexpr int BOX_BYTES = BM * BK * 4;         // 16 KB
 constexpr int STAGE_BYTES = 4 * BOX_BYTES;    // A_hi, A_lo, B_hi, B_lo
-constexpr int TMEM_COLS = 128;
+constexpr int TRAIL_NT = 64;  // output tile width of the trailing update
 constexpr int TC_THREADS = 192;
 constexpr unsigned long long TC_WAIT_NS = 2000000000ull;
 
@@ -100,15 +100,18 @@ __device__ __forceinline__ uint64_t sw128_kmajor_desc(uint32_t saddr) {
     return d;
 }
 
-// Instruction descriptor: D f32, A and B tf32, both K-major, M=128, N=128.
-constexpr uint32_t IDESC_TF32_128x128 =
-    (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+// Instruction descriptor: D f32, A and B tf32, both K-major, M=128, N=NT.
+template <int NT>
+__host__ __device__ constexpr uint32_t idesc_tf32() {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(NT >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+}
 
+template <int NT>
 __device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t acc) {
     asm volatile(
         "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}" ::"r"(tmem_d),
-        "l"(da), "l"(db), "r"(IDESC_TF32_128x128), "r"(acc));
+        "l"(da), "l"(db), "r"(idesc_tf32<NT>()), "r"(acc));
 }
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
@@ -184,6 +187,7 @@ __device__ __forceinline__ void epi_gram(const TcTile &t, const TcEpilogue &ep, 
 // warp's 32 x 32 block (a row per lane from TMEM) is transposed through
 // shared memory (stg: 32 x 33 floats of the warp) so that each
 // read-modify-write covers 32 consecutive floats of one row.
+template <int NT>
 __device__ __forceinline__ void epi_trail(const TcTile &t, const TcEpilogue &ep, int row0, int col, const float (&v)[32],
                                           int lane, float *stg) {
 #pragma unroll
@@ -191,7 +195,7 @@ __device__ __forceinline__ void epi_trail(const TcTile &t, const TcEpilogue &ep,
     __syncwarp();
     const int s = ep.units[t.unit].s;
     float *A = reinterpret_cast<float *>(ep.a32 + ep.mus[t.unit].a32_off);
-    const int64_t F = 2 * ((int64_t)ep.c0 + 32) + (int64_t)t.tj * BN + col + lane;
+    const int64_t F = 2 * ((int64_t)ep.c0 + 32) + (int64_t)t.tj * NT + col + lane;
     const int64_t R0 = (int64_t)ep.c0 + 32 + (int64_t)t.ti * BM + row0;
     // all reads (the transposed block, then A22) before any write, so no
     // load waits behind a store it might alias
@@ -207,13 +211,19 @@ __device__ __forceinline__ void epi_trail(const TcTile &t, const TcEpilogue &ep,
         if (col_ok && R0 + r < s) A[(R0 + r) * 2 * s + F] = a[r] - d[r];
 }
 
-template <int EPI>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+// NT: output tile width (B rows) -- 128, or 64 for the trailing update,
+// whose smaller stages (ST of them) let two CTAs share an SM so that one
+// CTA's read-modify-write epilogue overlaps the other's loads and MMAs.
+template <int EPI, int NT = BN, int ST = STAGES>
+__global__ void __launch_bounds__(TC_THREADS, (NT == BN ? 1 : 2))
     k_tc_gemm(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
               const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
               const TcTile *__restrict__ tiles, TcEpilogue ep) {
+    constexpr int B_BOX = NT * BK * 4;
+    constexpr int STG = 2 * BOX_BYTES + 2 * B_BOX;  // A_hi, A_lo, B_hi, B_lo
+    constexpr int TCOLS = NT;                       // TMEM columns (power of 2, >= 32)
     extern __shared__ uint8_t smem_raw[];
-    __shared__ __align__(8) uint64_t s_bar[2 * STAGES + 1];
+    __shared__ __align__(8) uint64_t s_bar[2 * ST + 1];
     __shared__ uint32_t s_tmem;
     __shared__ int s_abort;
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
@@ -221,13 +231,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     TcTile t;
     if (EPI == TC_EPI_TRAIL) {  // the tile from (unit of the step, tile index)
         const TcTrailUnit tu = ep.trail[blockIdx.y];
-        const int ntj = tu.n2_pad / BN, ti = (int)blockIdx.x / ntj, tj = (int)blockIdx.x % ntj;
+        const int ntj = tu.n2_pad / NT, ti = (int)blockIdx.x / ntj, tj = (int)blockIdx.x % ntj;
         if (ti >= tu.m_pad / BM) return;  // the whole CTA, before any barrier or TMEM allocation
-        // complex columns [64 tj, 64 tj + 64) against rows [128 ti, 128 ti + 128):
-        // wholly above the diagonal when 64 tj > 128 ti + 127
-        if (ep.trail_lower && tj > 2 * ti + 1) return;
+        // complex columns [NT/2 tj, NT/2 (tj + 1)) against rows [128 ti, 128 ti + 128):
+        // wholly above the diagonal when (NT/2) tj > 128 ti + 127
+        if (ep.trail_lower && (NT / 2) * tj > BM * ti + BM - 1) return;
         t.a_row = (int32_t)(tu.a_base + (int64_t)ti * BM);
-        t.b_row = (int32_t)(tu.b_base + (int64_t)tj * BN);
+        t.b_row = (int32_t)(tu.b_base + (int64_t)tj * NT);
         t.a_kstride = tu.m_pad;
         t.b_kstride = tu.n2_pad;
         t.kblocks = 2;
@@ -239,17 +249,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
     const uint32_t sbase = smem_u32(smem);
     auto full = [&](int st) { return smem_u32(&s_bar[st]); };
-    auto empty = [&](int st) { return smem_u32(&s_bar[STAGES + st]); };
-    const uint32_t tfull = smem_u32(&s_bar[2 * STAGES]);
+    auto empty = [&](int st) { return smem_u32(&s_bar[ST + st]); };
+    const uint32_t tfull = smem_u32(&s_bar[2 * ST]);
     volatile int *abort_word = &s_abort;
     if (threadIdx.x == 0) {
-        for (int i = 0; i < 2 * STAGES + 1; ++i) mbar_init(smem_u32(&s_bar[i]), 1);
+        for (int i = 0; i < 2 * ST + 1; ++i) mbar_init(smem_u32(&s_bar[i]), 1);
         s_abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                     "r"(TMEM_COLS));
+                     "r"(TCOLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     tc_fence_before();
@@ -263,39 +273,39 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (lane == 0) {
             int issued = 0;
             for (int kb = 0; kb < t.kblocks && kb < stop_kb; ++kb) {
-                const int st = kb % STAGES;
-                const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
-                if (kb >= STAGES && !mbar_wait(empty(st), ph ^ 1u, abort_word, wlim)) break;
-                const uint32_t dst = sbase + st * STAGE_BYTES;
-                mbar_expect_tx(full(st), STAGE_BYTES);
+                const int st = kb % ST;
+                const uint32_t ph = (uint32_t)(kb / ST) & 1u;
+                if (kb >= ST && !mbar_wait(empty(st), ph ^ 1u, abort_word, wlim)) break;
+                const uint32_t dst = sbase + st * STG;
+                mbar_expect_tx(full(st), STG);
                 const int ya = t.a_row + kb * t.a_kstride, yb = t.b_row + kb * t.b_kstride;
                 tma_load_2d(dst, &mAh, 0, ya, full(st));
                 tma_load_2d(dst + BOX_BYTES, &mAl, 0, ya, full(st));
                 tma_load_2d(dst + 2 * BOX_BYTES, &mBh, 0, yb, full(st));
-                tma_load_2d(dst + 3 * BOX_BYTES, &mBl, 0, yb, full(st));
+                tma_load_2d(dst + 2 * BOX_BYTES + B_BOX, &mBl, 0, yb, full(st));
                 issued = kb + 1;
             }
             if (*abort_word || issued < t.kblocks)  // let the copies already issued land before the CTA exits
-                for (int kb = issued - 1; kb >= 0 && kb >= issued - STAGES; --kb)
-                    mbar_drain(full(kb % STAGES), (uint32_t)(kb / STAGES) & 1u, wlim);
+                for (int kb = issued - 1; kb >= 0 && kb >= issued - ST; --kb)
+                    mbar_drain(full(kb % ST), (uint32_t)(kb / ST) & 1u, wlim);
         }
     } else if (warp == 1) {
         if (lane == 0) {
             for (int kb = 0; kb < t.kblocks; ++kb) {
-                const int st = kb % STAGES;
-                const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+                const int st = kb % ST;
+                const uint32_t ph = (uint32_t)(kb / ST) & 1u;
                 if (!mbar_wait(full(st), ph, abort_word, wlim)) break;
                 tc_fence_after();
-                const uint32_t a_hi = sbase + st * STAGE_BYTES, a_lo = a_hi + BOX_BYTES;
-                const uint32_t b_hi = a_hi + 2 * BOX_BYTES, b_lo = a_hi + 3 * BOX_BYTES;
+                const uint32_t a_hi = sbase + st * STG, a_lo = a_hi + BOX_BYTES;
+                const uint32_t b_hi = a_hi + 2 * BOX_BYTES, b_lo = b_hi + B_BOX;
 #pragma unroll
                 for (int kk = 0; kk < BK / 8; ++kk) {
                     const uint32_t off = kk * 32;  // 8 tf32 = 32 B along the swizzled row
                     const uint64_t dah = sw128_kmajor_desc(a_hi + off), dal = sw128_kmajor_desc(a_lo + off);
                     const uint64_t dbh = sw128_kmajor_desc(b_hi + off), dbl = sw128_kmajor_desc(b_lo + off);
-                    mma_tf32(tmem, dah, dbh, (kb | kk) != 0);
-                    mma_tf32(tmem, dah, dbl, 1u);
-                    mma_tf32(tmem, dal, dbh, 1u);
+                    mma_tf32<NT>(tmem, dah, dbh, (kb | kk) != 0);
+                    mma_tf32<NT>(tmem, dah, dbl, 1u);
+                    mma_tf32<NT>(tmem, dal, dbh, 1u);
                 }
                 mma_commit(empty(st));
             }
@@ -311,12 +321,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             // every MMA has completed: the stage buffers are free for staging
             float *stg = reinterpret_cast<float *>(smem) + q * 32 * 33;
 #pragma unroll 1
-            for (int cc = 0; cc < BN / 32; ++cc) {
+            for (int cc = 0; cc < NT / 32; ++cc) {
                 float v[32];
                 tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(cc * 32), v);
                 if (EPI == TC_EPI_STORE) epi_store(t, ep, row, cc * 32, v);
                 else if (EPI == TC_EPI_GRAM) epi_gram(t, ep, row, cc * 32, v, lane);
-                else epi_trail(t, ep, q * 32, cc * 32, v, lane, stg);
+                else epi_trail<NT>(t, ep, q * 32, cc * 32, v, lane, stg);
             }
         }
     }
@@ -324,7 +334,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     __syncthreads();
     tc_fence_after();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TCOLS));
     if (threadIdx.x == 0 && *abort_word && ep.status) atomicExch(&ep.status[ep.status_of_tile ? t.unit : 0],
                                                                  FNEC_UNIT_TIMEOUT);
 }
@@ -436,7 +446,7 @@ __global__ void k_split_trail_b(const TcTrailUnit *__restrict__ tu_list, const U
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 std::once_flag g_encode_once;
 
-bool make_map(CUtensorMap *m, const float *base, int64_t rows) {
+bool make_map(CUtensorMap *m, const float *base, int64_t rows, int box_rows = BM) {
     std::call_once(g_encode_once, [] {
         void *fn = nullptr;
         cudaDriverEntryPointQueryResult q;
@@ -447,7 +457,7 @@ bool make_map(CUtensorMap *m, const float *base, int64_t rows) {
     if (!g_encode || rows <= 0) return false;
     cuuint64_t dims[2] = {32, (cuuint64_t)rows};
     cuuint64_t strides[1] = {32 * sizeof(float)};
-    cuuint32_t box[2] = {32, (cuuint32_t)BM};
+    cuuint32_t box[2] = {32, (cuuint32_t)box_rows};
     cuuint32_t es[2] = {1, 1};
     return g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float *>(base), dims, strides, box, es,
                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -545,7 +555,8 @@ cudaError_t tc_trail_plan(const std::vector<int> &s_desc, const std::vector<int3
 }
 
 bool tc_trail_maps(TcTrailPlan &p, const float *hi, const float *lo) {
-    p.ready = make_map(&p.m_hi, hi, p.rows) && make_map(&p.m_lo, lo, p.rows);
+    p.ready = make_map(&p.m_hi, hi, p.rows) && make_map(&p.m_lo, lo, p.rows) &&
+              make_map(&p.m_hi_b, hi, p.rows, TRAIL_NT) && make_map(&p.m_lo_b, lo, p.rows, TRAIL_NT);
     return p.ready;
 }
 
@@ -560,8 +571,10 @@ cudaError_t tc_trail_run(const TcTrailPlan &p, int step, int count, const TcTrai
                                                                                          c0, hi, lo);
     k_split_trail_b<<<dim3((unsigned)((p.max_n2pad[step] / 2 + 31) / 32), (unsigned)na), 256, 0, st>>>(
         tl, d_systems, d_smu, a32, c0, hi, lo);
-    if (set_smem_limit_once((const void *)k_tc_gemm<TC_EPI_TRAIL>, (int)tc_smem_bytes()) < (int)tc_smem_bytes())
-        return cudaErrorInvalidConfiguration;
+    // 128 x 64 output tiles in two 48 KB stages: two CTAs per SM
+    constexpr size_t smem = (size_t)2 * (2 * BOX_BYTES + 2 * TRAIL_NT * BK * 4) + 1024;
+    auto kern = k_tc_gemm<TC_EPI_TRAIL, TRAIL_NT, 2>;
+    if (set_smem_limit_once((const void *)kern, (int)smem) < (int)smem) return cudaErrorInvalidConfiguration;
     TcEpilogue ep{};
     ep.units = d_systems;
     ep.mus = d_smu;
@@ -571,8 +584,8 @@ cudaError_t tc_trail_run(const TcTrailPlan &p, int step, int count, const TcTrai
     ep.c0 = c0;
     ep.trail = tl;
     ep.trail_lower = lower ? 1 : 0;
-    k_tc_gemm<TC_EPI_TRAIL><<<dim3((unsigned)p.max_tiles[step], (unsigned)na), TC_THREADS, tc_smem_bytes(), st>>>(
-        p.m_hi, p.m_lo, p.m_hi, p.m_lo, nullptr, ep);
+    kern<<<dim3((unsigned)(p.max_tiles[step] * (BN / TRAIL_NT)), (unsigned)na), TC_THREADS, smem, st>>>(
+        p.m_hi, p.m_lo, p.m_hi_b, p.m_lo_b, nullptr, ep);
     return cudaGetLastError();
 }
 

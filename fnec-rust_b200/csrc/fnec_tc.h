@@ -104,7 +104,8 @@ struct TcTrailPlan {
     std::vector<int32_t> u_off;      // per step: first entry (steps + 1 values)
     std::vector<int32_t> max_tiles, max_mpad, max_n2pad;  // per step
     int64_t rows = 0;                // rows of each stack (hi, lo)
-    CUtensorMap m_hi, m_lo;
+    CUtensorMap m_hi, m_lo;          // 128-row boxes (the A operand)
+    CUtensorMap m_hi_b, m_lo_b;      // 64-row boxes (the B operand of 128 x 64 output tiles)
     bool ready = false;
     int steps() const { return (int)u_off.size() - 1; }
     int active(int step) const { return step < steps() ? u_off[step + 1] - u_off[step] : 0; }
