@@ -339,6 +339,205 @@ __global__ void __launch_bounds__(TC_THREADS, (NT == BN ? 1 : 2))
                                                                  FNEC_UNIT_TIMEOUT);
 }
 
+// -- the trailing update as a persistent kernel --------------------------------
+//
+// One CTA per SM walks the step's 128 x 64 output tiles (every unit of the
+// step; with lower, the tiles wholly above the diagonal are skipped by all
+// roles alike), so that nothing is set up per tile, and the accumulator is
+// double-buffered in TMEM (2 x 64 columns): the MMA warp fills one buffer
+// while the four epilogue warps read-modify-write A22 from the other, and
+// the TMA producer runs PT_ST stages ahead across tile boundaries.  Barriers:
+// full / empty per stage (k-blocks counted over the CTA's whole sequence),
+// tfull per buffer (the MMA warp's commit) and tempty per buffer (one
+// arrival from each epilogue warp after its TMEM reads).  Every wait is
+// bounded; a CTA that gives up drains its copies and MMAs, frees TMEM and
+// marks the unit of the tile it was on.
+constexpr int PT_ST = 3;
+constexpr int PT_EPI_WARPS = 8;  // two per TMEM lane quarter, one per 32-column chunk
+constexpr int PT_THREADS = 32 * (2 + PT_EPI_WARPS);
+constexpr int PT_STG = 2 * BOX_BYTES + 2 * TRAIL_NT * BK * 4;  // 48 KB
+constexpr int PT_MAX_UNITS = 1024;                           // units per step it takes
+constexpr size_t PT_SMEM = (size_t)PT_ST * PT_STG + PT_EPI_WARPS * 32 * 33 * sizeof(float) + 1024;
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Tile g of the step's sequence: its unit entry and grid position (false:
+// g is past the end or, with lower, the tile lies wholly above the diagonal)
+__device__ __forceinline__ bool pt_tile(const TcTrailUnit *tl, const int32_t *pre, int na, int g, bool lower,
+                                        TcTile &t) {
+    if (g >= pre[na]) return false;
+    int lo = 0, hi = na;  // pre[lo] <= g < pre[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (pre[mid] <= g) lo = mid;
+        else hi = mid;
+    }
+    const TcTrailUnit tu = tl[lo];
+    const int ntj = tu.n2_pad / TRAIL_NT, x = g - pre[lo], ti = x / ntj, tj = x % ntj;
+    if (lower && (TRAIL_NT / 2) * tj > BM * ti + BM - 1) return false;
+    t.a_row = (int32_t)(tu.a_base + (int64_t)ti * BM);
+    t.b_row = (int32_t)(tu.b_base + (int64_t)tj * TRAIL_NT);
+    t.a_kstride = tu.m_pad;
+    t.b_kstride = tu.n2_pad;
+    t.kblocks = 2;
+    t.unit = tu.unit;
+    t.ti = ti;
+    t.tj = tj;
+    return true;
+}
+
+__global__ void __launch_bounds__(PT_THREADS, 1)
+    k_tc_trail_persist(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+                       const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl, int na,
+                       TcEpilogue ep) {
+    constexpr int B_BOX = TRAIL_NT * BK * 4;
+    extern __shared__ uint8_t smem_raw[];
+    __shared__ __align__(8) uint64_t s_bar[2 * PT_ST + 5];
+    __shared__ int32_t s_pre[PT_MAX_UNITS + 1];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_abort, s_abort_unit;
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
+    float *stage_out = reinterpret_cast<float *>(smem + PT_ST * PT_STG);  // epilogue warps x 32 x 33
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const TcTrailUnit *tl = ep.trail;
+    const bool lower = ep.trail_lower != 0;
+    if (threadIdx.x == 0) {
+        int acc = 0;
+        for (int q = 0; q < na; ++q) {
+            s_pre[q] = acc;
+            acc += (tl[q].m_pad / BM) * (tl[q].n2_pad / TRAIL_NT);
+        }
+        s_pre[na] = acc;
+        for (int i = 0; i < 2 * PT_ST; ++i) mbar_init(smem_u32(&s_bar[i]), 1);
+        mbar_init(smem_u32(&s_bar[2 * PT_ST + 0]), 1);  // tfull 0
+        mbar_init(smem_u32(&s_bar[2 * PT_ST + 1]), 1);  // tfull 1
+        mbar_init(smem_u32(&s_bar[2 * PT_ST + 2]), PT_EPI_WARPS);  // tempty 0: one arrival per epilogue warp
+        mbar_init(smem_u32(&s_bar[2 * PT_ST + 3]), PT_EPI_WARPS);  // tempty 1
+        mbar_init(smem_u32(&s_bar[2 * PT_ST + 4]), 1);  // tdone: every MMA the issuer started
+        s_abort = 0;
+        s_abort_unit = -1;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                     "r"(2 * TRAIL_NT));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const uint32_t sbase = smem_u32(smem);
+    auto full = [&](int st) { return smem_u32(&s_bar[st]); };
+    auto empty = [&](int st) { return smem_u32(&s_bar[PT_ST + st]); };
+    auto tfull = [&](int b) { return smem_u32(&s_bar[2 * PT_ST + b]); };
+    auto tempty = [&](int b) { return smem_u32(&s_bar[2 * PT_ST + 2 + b]); };
+    volatile int *abort_word = &s_abort;
+    const unsigned long long wlim = ep.wait_ns ? (unsigned long long)ep.wait_ns : TC_WAIT_NS;
+    const int total = s_pre[na];
+    TcTile t;
+
+    if (warp == 0) {
+        if (lane == 0) {  // TMA producer
+            int kq = 0;   // k-blocks issued over the sequence
+            for (int g = blockIdx.x; g < total && !*abort_word; g += gridDim.x) {
+                if (!pt_tile(tl, s_pre, na, g, lower, t)) continue;
+                for (int kb = 0; kb < 2; ++kb, ++kq) {
+                    const int st = kq % PT_ST;
+                    const uint32_t ph = (uint32_t)(kq / PT_ST) & 1u;
+                    if (kq >= PT_ST && !mbar_wait(empty(st), ph ^ 1u, abort_word, wlim)) {
+                        s_abort_unit = t.unit;
+                        break;
+                    }
+                    const uint32_t dst = sbase + st * PT_STG;
+                    mbar_expect_tx(full(st), PT_STG);
+                    const int ya = t.a_row + kb * t.a_kstride, yb = t.b_row + kb * t.b_kstride;
+                    tma_load_2d(dst, &mAh, 0, ya, full(st));
+                    tma_load_2d(dst + BOX_BYTES, &mAl, 0, ya, full(st));
+                    tma_load_2d(dst + 2 * BOX_BYTES, &mBh, 0, yb, full(st));
+                    tma_load_2d(dst + 2 * BOX_BYTES + B_BOX, &mBl, 0, yb, full(st));
+                }
+            }
+            if (*abort_word)  // let the copies already issued land before the CTA exits
+                for (int q = kq - 1; q >= 0 && q >= kq - PT_ST; --q) mbar_drain(full(q % PT_ST), (uint32_t)(q / PT_ST) & 1u, wlim);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {  // MMA issuer
+            int kq = 0, i = 0;
+            bool ok = true;
+            for (int g = blockIdx.x; ok && g < total; g += gridDim.x) {
+                if (!pt_tile(tl, s_pre, na, g, lower, t)) continue;
+                const int b = i & 1;
+                if (i >= 2 && !mbar_wait(tempty(b), (uint32_t)((i >> 1) - 1) & 1u, abort_word, wlim)) {
+                    s_abort_unit = t.unit;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t acc = tmem + (uint32_t)(b * TRAIL_NT);
+                for (int kb = 0; kb < 2; ++kb, ++kq) {
+                    const int st = kq % PT_ST;
+                    if (!mbar_wait(full(st), (uint32_t)(kq / PT_ST) & 1u, abort_word, wlim)) {
+                        s_abort_unit = t.unit;
+                        ok = false;
+                        break;
+                    }
+                    tc_fence_after();
+                    const uint32_t a_hi = sbase + st * PT_STG, a_lo = a_hi + BOX_BYTES;
+                    const uint32_t b_hi = a_hi + 2 * BOX_BYTES, b_lo = b_hi + B_BOX;
+#pragma unroll
+                    for (int kk = 0; kk < BK / 8; ++kk) {
+                        const uint32_t off = kk * 32;
+                        const uint64_t dah = sw128_kmajor_desc(a_hi + off), dal = sw128_kmajor_desc(a_lo + off);
+                        const uint64_t dbh = sw128_kmajor_desc(b_hi + off), dbl = sw128_kmajor_desc(b_lo + off);
+                        mma_tf32<TRAIL_NT>(acc, dah, dbh, (kb | kk) != 0);
+                        mma_tf32<TRAIL_NT>(acc, dah, dbl, 1u);
+                        mma_tf32<TRAIL_NT>(acc, dal, dbh, 1u);
+                    }
+                    mma_commit(empty(st));
+                }
+                if (!ok) break;
+                mma_commit(tfull(b));  // arrives once this tile's MMAs have completed
+                ++i;
+            }
+            // a last commit tracks every MMA issued above (a tile cut short by an
+            // abort included): TMEM is freed only after they complete
+            mma_commit(smem_u32(&s_bar[2 * PT_ST + 4]));
+            mbar_drain(smem_u32(&s_bar[2 * PT_ST + 4]), 0, wlim);
+        }
+    } else {  // epilogue warps 2..9: TMEM lane quarter q, column chunk cc
+        const int q = warp & 3, cc = (warp - 2) >> 2;  // lane quarter, 32-column chunk
+        float *stg = stage_out + (warp - 2) * 32 * 33;
+        int i = 0;
+        for (int g = blockIdx.x; g < total; g += gridDim.x) {
+            if (!pt_tile(tl, s_pre, na, g, lower, t)) continue;
+            const int b = i & 1;
+            if (!mbar_wait(tfull(b), (uint32_t)(i >> 1) & 1u, abort_word, wlim)) {
+                if (lane == 0) s_abort_unit = t.unit;
+                break;
+            }
+            tc_fence_after();
+            {
+                float v[32];
+                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TRAIL_NT + cc * 32), v);
+                epi_trail<TRAIL_NT>(t, ep, q * 32, cc * 32, v, lane, stg);
+            }
+            tc_fence_before();
+            __syncwarp();
+            if (lane == 0) mbar_arrive(tempty(b));
+            ++i;
+        }
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TRAIL_NT));
+    if (threadIdx.x == 0 && *abort_word && ep.status)
+        atomicExch(&ep.status[s_abort_unit >= 0 ? s_abort_unit : 0], FNEC_UNIT_TIMEOUT);
+}
+
 // -- operand preparation (split_tf32: fnec_tc.h) -----------------------------
 
 // Row-major FP32 [rows][k] -> K-blocked hi/lo stacks (zero padded to
@@ -562,7 +761,7 @@ bool tc_trail_maps(TcTrailPlan &p, const float *hi, const float *lo) {
 
 cudaError_t tc_trail_run(const TcTrailPlan &p, int step, int count, const TcTrailUnit *d_trail, const UnitDesc *d_systems,
                          const MixedUnit *d_smu, float2 *a32, float *hi, float *lo, int32_t *status, cudaStream_t st,
-                         bool lower) {
+                         bool lower, bool persistent) {
     const int na = std::min(count, p.active(step));
     if (na <= 0) return cudaSuccess;
     const TcTrailUnit *tl = d_trail + p.u_off[step];
@@ -571,10 +770,6 @@ cudaError_t tc_trail_run(const TcTrailPlan &p, int step, int count, const TcTrai
                                                                                          c0, hi, lo);
     k_split_trail_b<<<dim3((unsigned)((p.max_n2pad[step] / 2 + 31) / 32), (unsigned)na), 256, 0, st>>>(
         tl, d_systems, d_smu, a32, c0, hi, lo);
-    // 128 x 64 output tiles in two 48 KB stages: two CTAs per SM
-    constexpr size_t smem = (size_t)2 * (2 * BOX_BYTES + 2 * TRAIL_NT * BK * 4) + 1024;
-    auto kern = k_tc_gemm<TC_EPI_TRAIL, TRAIL_NT, 2>;
-    if (set_smem_limit_once((const void *)kern, (int)smem) < (int)smem) return cudaErrorInvalidConfiguration;
     TcEpilogue ep{};
     ep.units = d_systems;
     ep.mus = d_smu;
@@ -584,6 +779,20 @@ cudaError_t tc_trail_run(const TcTrailPlan &p, int step, int count, const TcTrai
     ep.c0 = c0;
     ep.trail = tl;
     ep.trail_lower = lower ? 1 : 0;
+    if (persistent && na <= PT_MAX_UNITS &&
+        set_smem_limit_once((const void *)k_tc_trail_persist, (int)PT_SMEM) >= (int)PT_SMEM) {
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const int64_t tiles = (int64_t)p.max_tiles[step] * (BN / TRAIL_NT) * na;  // bound on the sequence
+        const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(sms, tiles));
+        k_tc_trail_persist<<<grid, PT_THREADS, PT_SMEM, st>>>(p.m_hi, p.m_lo, p.m_hi_b, p.m_lo_b, na, ep);
+        return cudaGetLastError();
+    }
+    // 128 x 64 output tiles in two 48 KB stages: two CTAs per SM
+    constexpr size_t smem = (size_t)2 * (2 * BOX_BYTES + 2 * TRAIL_NT * BK * 4) + 1024;
+    auto kern = k_tc_gemm<TC_EPI_TRAIL, TRAIL_NT, 2>;
+    if (set_smem_limit_once((const void *)kern, (int)smem) < (int)smem) return cudaErrorInvalidConfiguration;
     kern<<<dim3((unsigned)(p.max_tiles[step] * (BN / TRAIL_NT)), (unsigned)na), TC_THREADS, smem, st>>>(
         p.m_hi, p.m_lo, p.m_hi_b, p.m_lo_b, nullptr, ep);
     return cudaGetLastError();

@@ -116,10 +116,12 @@ bool tc_trail_maps(TcTrailPlan &p, const float *hi, const float *lo);
 // Step `step` (c0 = 32 step): split L21 / U12 of the step's first `count`
 // units (<= active(step)) into the stacks, then the GEMM subtracting
 // L21 U12 from each one's A22.
-// lower: the Hermitian factor's update, tiles on and below the diagonal only
+// lower: the Hermitian factor's update, tiles on and below the diagonal
+// only; persistent: one CTA per SM over the step's tiles with the
+// accumulator double-buffered in TMEM (else one 128 x 64 tile per CTA)
 cudaError_t tc_trail_run(const TcTrailPlan &p, int step, int count, const TcTrailUnit *d_trail, const UnitDesc *d_systems,
                          const MixedUnit *d_smu, float2 *a32, float *hi, float *lo, int32_t *status, cudaStream_t st,
-                         bool lower = false);
+                         bool lower = false, bool persistent = true);
 
 cudaError_t tc_gram_plan(const std::vector<UnitDesc> &systems, TcGramPlan &p);
 // Tensor maps over the hi / lo stacks (rows x 32 floats each); false when
