@@ -516,6 +516,8 @@ def run_receive(args, acc, ctx, rank, local, dist):
     stream = torch.cuda.ExternalStream(acc.lib().fnec_ctx_stream(ctx.handle), device=local)
     # schedule: the autotuner's pick, timed before and outside the timed region
     tune = None if args.no_tune else batch.tune(reps=args.tune_reps)
+    if args.schedule:
+        batch.schedule = json.loads(args.schedule)
 
     def barrier():
         if dist is not None:
@@ -942,6 +944,8 @@ def run_batch_workload(args, acc, ctx, rank, local, dist, world, steps, warmup, 
         shapes = batch.units
         # schedule: the autotuner's pick (timed before, outside the timed region)
         tune = None if args.no_tune else batch.tune(reps=args.tune_reps)
+        if args.schedule and form == "mixed":
+            batch.schedule = json.loads(args.schedule)
         out[form] = measure_batch(args, acc, batch, stream, rank, local, dist, steps, warmup,
                                   with_clocks=(form == forms[0]))
         st, nodes = batch.graph_state()
@@ -1134,6 +1138,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true",
                     help="skip the autotuner (default schedule; the pipeline is still graph-captured)")
     ap.add_argument("--tune-reps", type=int, default=2, help="timed runs per candidate schedule")
+    ap.add_argument("--schedule", default="",
+                    help='schedule fields set on the (mixed) batch after tuning, JSON, e.g. \'{"tensor_trailing": 1}\'')
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

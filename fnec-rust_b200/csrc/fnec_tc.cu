@@ -355,9 +355,14 @@ __global__ void __launch_bounds__(TC_THREADS, (NT == BN ? 1 : 2))
 constexpr int PT_ST = 3;
 constexpr int PT_EPI_WARPS = 8;  // two per TMEM lane quarter, one per 32-column chunk
 constexpr int PT_THREADS = 32 * (2 + PT_EPI_WARPS);
-constexpr int PT_STG = 2 * BOX_BYTES + 2 * TRAIL_NT * BK * 4;  // 48 KB
-constexpr int PT_MAX_UNITS = 1024;                           // units per step it takes
-constexpr size_t PT_SMEM = (size_t)PT_ST * PT_STG + PT_EPI_WARPS * 32 * 33 * sizeof(float) + 1024;
+constexpr int PT_MAX_UNITS = 1024;  // units per step it takes
+// shared memory of a launch: PT_ST stages of A_hi, A_lo, B_hi, B_lo (+ the
+// trailing update's epilogue staging, a 32 x 33 block per epilogue warp)
+template <int EPI, int NT>
+constexpr size_t pt_smem() {
+    return (size_t)PT_ST * (2 * BOX_BYTES + 2 * NT * BK * 4) +
+           (EPI == TC_EPI_TRAIL ? PT_EPI_WARPS * 32 * 33 * sizeof(float) : 0) + 1024;
+}
 
 __device__ __forceinline__ void mbar_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
@@ -388,28 +393,46 @@ __device__ __forceinline__ bool pt_tile(const TcTrailUnit *tl, const int32_t *pr
     return true;
 }
 
+// The next tile of the sequence: the trailing update's tile g (decoded from
+// the step's units), or entry g of the Gram's tile list.
+template <int EPI>
+__device__ __forceinline__ bool pt_next(const TcTrailUnit *tl, const TcTile *tiles, const int32_t *pre, int na,
+                                        int g, bool lower, TcTile &t) {
+    if (EPI == TC_EPI_TRAIL) return pt_tile(tl, pre, na, g, lower, t);
+    t = tiles[g];
+    return true;
+}
+
+// EPI TC_EPI_TRAIL (NT 64, na units of the step) or TC_EPI_GRAM (NT 128, na
+// tiles in `tiles`)
+template <int EPI, int NT>
 __global__ void __launch_bounds__(PT_THREADS, 1)
-    k_tc_trail_persist(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
-                       const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl, int na,
-                       TcEpilogue ep) {
-    constexpr int B_BOX = TRAIL_NT * BK * 4;
+    k_tc_persist(const __grid_constant__ CUtensorMap mAh, const __grid_constant__ CUtensorMap mAl,
+                 const __grid_constant__ CUtensorMap mBh, const __grid_constant__ CUtensorMap mBl,
+                 const TcTile *__restrict__ tiles, int na, TcEpilogue ep) {
+    constexpr int B_BOX = NT * BK * 4;
+    constexpr int PT_STG = 2 * BOX_BYTES + 2 * B_BOX;
     extern __shared__ uint8_t smem_raw[];
     __shared__ __align__(8) uint64_t s_bar[2 * PT_ST + 5];
     __shared__ int32_t s_pre[PT_MAX_UNITS + 1];
     __shared__ uint32_t s_tmem;
     __shared__ int s_abort, s_abort_unit;
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~(uintptr_t)1023);
-    float *stage_out = reinterpret_cast<float *>(smem + PT_ST * PT_STG);  // epilogue warps x 32 x 33
+    float *stage_out = reinterpret_cast<float *>(smem + PT_ST * PT_STG);  // TRAIL: epilogue warps x 32 x 33
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const TcTrailUnit *tl = ep.trail;
     const bool lower = ep.trail_lower != 0;
     if (threadIdx.x == 0) {
-        int acc = 0;
-        for (int q = 0; q < na; ++q) {
-            s_pre[q] = acc;
-            acc += (tl[q].m_pad / BM) * (tl[q].n2_pad / TRAIL_NT);
+        if (EPI == TC_EPI_TRAIL) {
+            int acc = 0;
+            for (int q = 0; q < na; ++q) {
+                s_pre[q] = acc;
+                acc += (tl[q].m_pad / BM) * (tl[q].n2_pad / NT);
+            }
+            s_pre[na] = acc;
+        } else {
+            s_pre[0] = na;
         }
-        s_pre[na] = acc;
         for (int i = 0; i < 2 * PT_ST; ++i) mbar_init(smem_u32(&s_bar[i]), 1);
         mbar_init(smem_u32(&s_bar[2 * PT_ST + 0]), 1);  // tfull 0
         mbar_init(smem_u32(&s_bar[2 * PT_ST + 1]), 1);  // tfull 1
@@ -422,7 +445,7 @@ __global__ void __launch_bounds__(PT_THREADS, 1)
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                     "r"(2 * TRAIL_NT));
+                     "r"(2 * NT));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     tc_fence_before();
@@ -436,15 +459,15 @@ __global__ void __launch_bounds__(PT_THREADS, 1)
     auto tempty = [&](int b) { return smem_u32(&s_bar[2 * PT_ST + 2 + b]); };
     volatile int *abort_word = &s_abort;
     const unsigned long long wlim = ep.wait_ns ? (unsigned long long)ep.wait_ns : TC_WAIT_NS;
-    const int total = s_pre[na];
+    const int total = EPI == TC_EPI_TRAIL ? s_pre[na] : s_pre[0];
     TcTile t;
 
     if (warp == 0) {
         if (lane == 0) {  // TMA producer
             int kq = 0;   // k-blocks issued over the sequence
             for (int g = blockIdx.x; g < total && !*abort_word; g += gridDim.x) {
-                if (!pt_tile(tl, s_pre, na, g, lower, t)) continue;
-                for (int kb = 0; kb < 2; ++kb, ++kq) {
+                if (!pt_next<EPI>(tl, tiles, s_pre, na, g, lower, t)) continue;
+                for (int kb = 0; kb < t.kblocks; ++kb, ++kq) {
                     const int st = kq % PT_ST;
                     const uint32_t ph = (uint32_t)(kq / PT_ST) & 1u;
                     if (kq >= PT_ST && !mbar_wait(empty(st), ph ^ 1u, abort_word, wlim)) {
@@ -468,15 +491,15 @@ __global__ void __launch_bounds__(PT_THREADS, 1)
             int kq = 0, i = 0;
             bool ok = true;
             for (int g = blockIdx.x; ok && g < total; g += gridDim.x) {
-                if (!pt_tile(tl, s_pre, na, g, lower, t)) continue;
+                if (!pt_next<EPI>(tl, tiles, s_pre, na, g, lower, t)) continue;
                 const int b = i & 1;
                 if (i >= 2 && !mbar_wait(tempty(b), (uint32_t)((i >> 1) - 1) & 1u, abort_word, wlim)) {
                     s_abort_unit = t.unit;
                     break;
                 }
                 tc_fence_after();
-                const uint32_t acc = tmem + (uint32_t)(b * TRAIL_NT);
-                for (int kb = 0; kb < 2; ++kb, ++kq) {
+                const uint32_t acc = tmem + (uint32_t)(b * NT);
+                for (int kb = 0; kb < t.kblocks; ++kb, ++kq) {
                     const int st = kq % PT_ST;
                     if (!mbar_wait(full(st), (uint32_t)(kq / PT_ST) & 1u, abort_word, wlim)) {
                         s_abort_unit = t.unit;
@@ -491,9 +514,9 @@ __global__ void __launch_bounds__(PT_THREADS, 1)
                         const uint32_t off = kk * 32;
                         const uint64_t dah = sw128_kmajor_desc(a_hi + off), dal = sw128_kmajor_desc(a_lo + off);
                         const uint64_t dbh = sw128_kmajor_desc(b_hi + off), dbl = sw128_kmajor_desc(b_lo + off);
-                        mma_tf32<TRAIL_NT>(acc, dah, dbh, (kb | kk) != 0);
-                        mma_tf32<TRAIL_NT>(acc, dah, dbl, 1u);
-                        mma_tf32<TRAIL_NT>(acc, dal, dbh, 1u);
+                        mma_tf32<NT>(acc, dah, dbh, (kb | kk) != 0);
+                        mma_tf32<NT>(acc, dah, dbl, 1u);
+                        mma_tf32<NT>(acc, dal, dbh, 1u);
                     }
                     mma_commit(empty(st));
                 }
@@ -506,22 +529,24 @@ __global__ void __launch_bounds__(PT_THREADS, 1)
             mma_commit(smem_u32(&s_bar[2 * PT_ST + 4]));
             mbar_drain(smem_u32(&s_bar[2 * PT_ST + 4]), 0, wlim);
         }
-    } else {  // epilogue warps 2..9: TMEM lane quarter q, column chunk cc
-        const int q = warp & 3, cc = (warp - 2) >> 2;  // lane quarter, 32-column chunk
+    } else {  // epilogue warps 2..9: TMEM lane quarter q, every other 32-column chunk from c0
+        const int q = warp & 3, c0 = (warp - 2) >> 2;
         float *stg = stage_out + (warp - 2) * 32 * 33;
         int i = 0;
         for (int g = blockIdx.x; g < total; g += gridDim.x) {
-            if (!pt_tile(tl, s_pre, na, g, lower, t)) continue;
+            if (!pt_next<EPI>(tl, tiles, s_pre, na, g, lower, t)) continue;
             const int b = i & 1;
             if (!mbar_wait(tfull(b), (uint32_t)(i >> 1) & 1u, abort_word, wlim)) {
                 if (lane == 0) s_abort_unit = t.unit;
                 break;
             }
             tc_fence_after();
-            {
+#pragma unroll 1
+            for (int cc = c0; cc < NT / 32; cc += 2) {
                 float v[32];
-                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * TRAIL_NT + cc * 32), v);
-                epi_trail<TRAIL_NT>(t, ep, q * 32, cc * 32, v, lane, stg);
+                tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * NT + cc * 32), v);
+                if (EPI == TC_EPI_TRAIL) epi_trail<NT>(t, ep, q * 32, cc * 32, v, lane, stg);
+                else epi_gram(t, ep, q * 32 + lane, cc * 32, v, lane);
             }
             tc_fence_before();
             __syncwarp();
@@ -533,7 +558,7 @@ __global__ void __launch_bounds__(PT_THREADS, 1)
     __syncthreads();
     tc_fence_after();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * TRAIL_NT));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * NT));
     if (threadIdx.x == 0 && *abort_word && ep.status)
         atomicExch(&ep.status[s_abort_unit >= 0 ? s_abort_unit : 0], FNEC_UNIT_TIMEOUT);
 }
@@ -779,14 +804,16 @@ cudaError_t tc_trail_run(const TcTrailPlan &p, int step, int count, const TcTrai
     ep.c0 = c0;
     ep.trail = tl;
     ep.trail_lower = lower ? 1 : 0;
+    constexpr size_t psm = pt_smem<TC_EPI_TRAIL, TRAIL_NT>();
     if (persistent && na <= PT_MAX_UNITS &&
-        set_smem_limit_once((const void *)k_tc_trail_persist, (int)PT_SMEM) >= (int)PT_SMEM) {
+        set_smem_limit_once((const void *)k_tc_persist<TC_EPI_TRAIL, TRAIL_NT>, (int)psm) >= (int)psm) {
         int dev = 0, sms = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const int64_t tiles = (int64_t)p.max_tiles[step] * (BN / TRAIL_NT) * na;  // bound on the sequence
         const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(sms, tiles));
-        k_tc_trail_persist<<<grid, PT_THREADS, PT_SMEM, st>>>(p.m_hi, p.m_lo, p.m_hi_b, p.m_lo_b, na, ep);
+        k_tc_persist<TC_EPI_TRAIL, TRAIL_NT><<<grid, PT_THREADS, psm, st>>>(p.m_hi, p.m_lo, p.m_hi_b, p.m_lo_b,
+                                                                          nullptr, na, ep);
         return cudaGetLastError();
     }
     // 128 x 64 output tiles in two 48 KB stages: two CTAs per SM
@@ -819,7 +846,18 @@ cudaError_t tc_gram_run(const TcGramPlan &p, const UnitDesc *d_units, const TcGr
     ep.status = status;
     ep.status_of_tile = 1;
     ep.lower_only = lower_only ? 1 : 0;
-    return launch_tc<TC_EPI_GRAM>(p.m_hi, p.m_lo, p.m_hi, p.m_lo, d_tiles, (int)p.tiles.size(), ep, st);
+    const int nt = (int)p.tiles.size();
+    constexpr size_t psm = pt_smem<TC_EPI_GRAM, BN>();
+    if (nt > 0 && set_smem_limit_once((const void *)k_tc_persist<TC_EPI_GRAM, BN>, (int)psm) >= (int)psm) {
+        // persistent: one CTA per SM over the tile list, epilogue overlapping the next tile's MMAs
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        k_tc_persist<TC_EPI_GRAM, BN><<<std::max(1, std::min(sms, nt)), PT_THREADS, psm, st>>>(
+            p.m_hi, p.m_lo, p.m_hi, p.m_lo, d_tiles, nt, ep);
+        return cudaGetLastError();
+    }
+    return launch_tc<TC_EPI_GRAM>(p.m_hi, p.m_lo, p.m_hi, p.m_lo, d_tiles, nt, ep, st);
 }
 
 }  // namespace fnec
