@@ -56,6 +56,23 @@ __device__ __forceinline__ void unit_vectors_dev(double th_deg, double ph_deg, d
     phh[2] = 0.0;
 }
 
+// The same vectors with sin / cos of theta given (sincos(th * RADS_PER_DEG)
+// of the direction's integration row, shared by the block).
+__device__ __forceinline__ void unit_vectors_row(double st, double ct, double ph_deg, double *rh, double *thh,
+                                                 double *phh) {
+    double sp, cp;
+    sincos(ph_deg * RADS_PER_DEG, &sp, &cp);
+    rh[0] = st * cp;
+    rh[1] = st * sp;
+    rh[2] = ct;
+    thh[0] = ct * cp;
+    thh[1] = ct * sp;
+    thh[2] = -st;
+    phh[0] = -sp;
+    phh[1] = cp;
+    phh[2] = 0.0;
+}
+
 // Fields of two directions at once: Horner sums over the antenna's runs
 // (+ images).  The two recurrences are independent, so each current load
 // from shared memory feeds 8 FMAs on two dependency chains.
@@ -192,14 +209,17 @@ struct FfDir {
     double th, ph;   // degrees
 };
 
+// sin_t_row: sin(theta) of the integration rows row_lo and row_lo + 1, as
+// sin(th * RADS_PER_DEG) gives it (null: computed here)
 __device__ __forceinline__ FfDir ff_dir(int d, int n_int, int n_xr, int n_th, double th_max, bool pec,
-                                        const DevRp &rp, const double *pts, const int32_t *ibuf) {
+                                        const DevRp &rp, const double *pts, const int32_t *ibuf,
+                                        const double *sin_t_row = nullptr, int row_lo = 0) {
     FfDir r{false, false, 0.0, -1, false, 0.0, 0.0};
     if (d < n_int) {
         int it = d / 360, ip = d % 360;
         r.th = (double)it * th_max / ((double)n_th - 1.0);
         r.ph = (double)ip;
-        double sin_t = sin(r.th * RADS_PER_DEG);
+        double sin_t = sin_t_row ? sin_t_row[it - row_lo] : sin(r.th * RADS_PER_DEG);
         double d_theta = (th_max * RADS_PER_DEG) / ((double)n_th - 1.0);
         double d_phi = 2.0 * 3.14159265358979323846 / 360.0;
         double w_t = (it == 0 || it == n_th - 1) ? 0.5 * d_theta : d_theta;
@@ -274,22 +294,37 @@ __global__ void __launch_bounds__(FF_THREADS, 5) k_farfield(
         s_runs = sr;
         s_cur = sc;
     }
-    __syncthreads();
-
-    const int d0 = blockIdx.x * 2 * FF_THREADS + threadIdx.x, d1 = d0 + FF_THREADS;
-    FfDir r0 = ff_dir(d0, n_int, n_xr, n_th, th_max, pec, rp, pts, ibuf);
-    FfDir r1 = ff_dir(d1, n_int, n_xr, n_th, th_max, pec, rp, pts, ibuf);
-    // z-parallel antennas: the run polynomials of the block's (at most two)
-    // integration rows, once per block
-    __shared__ cx s_rowp[2][FF_VMAX * 2];
-    __shared__ int s_vert;
+    // the block's (at most two) integration rows: sin / cos of theta once per
+    // block, as each direction would form them
+    __shared__ double s_row_st[2], s_row_ct[2], s_row_sin[2];
     const int row_lo = (int)(blockIdx.x * 2 * FF_THREADS) / 360;
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 2) {
+        const double th = (double)(row_lo + threadIdx.x) * th_max / ((double)n_th - 1.0);
+        double st, ct;
+        sincos(th * RADS_PER_DEG, &st, &ct);
+        s_row_st[threadIdx.x] = st;
+        s_row_ct[threadIdx.x] = ct;
+        s_row_sin[threadIdx.x] = sin(th * RADS_PER_DEG);
+    }
+    __shared__ int s_vert;
+    if (threadIdx.x == 32) {
         int v = a.n_run <= FF_VMAX && n_int > 0;
-        for (int q = 0; v && q < a.n_run; ++q) v = run_is_vertical(s_runs[q]);
+        for (int q = 0; v && q < a.n_run; ++q) v = run_is_vertical(runs_all[a.run_off + q]);
         s_vert = v;
     }
     __syncthreads();
+
+    const int d0 = blockIdx.x * 2 * FF_THREADS + threadIdx.x, d1 = d0 + FF_THREADS;
+    FfDir r0 = ff_dir(d0, n_int, n_xr, n_th, th_max, pec, rp, pts, ibuf, s_row_sin, row_lo);
+    FfDir r1 = ff_dir(d1, n_int, n_xr, n_th, th_max, pec, rp, pts, ibuf, s_row_sin, row_lo);
+    double rh0[3], th0[3], ph0[3], rh1[3], th1[3], ph1[3];
+    if (d0 < n_int) unit_vectors_row(s_row_st[d0 / 360 - row_lo], s_row_ct[d0 / 360 - row_lo], r0.ph, rh0, th0, ph0);
+    else unit_vectors_dev(r0.th, r0.ph, rh0, th0, ph0);
+    if (d1 < n_int) unit_vectors_row(s_row_st[d1 / 360 - row_lo], s_row_ct[d1 / 360 - row_lo], r1.ph, rh1, th1, ph1);
+    else unit_vectors_dev(r1.th, r1.ph, rh1, th1, ph1);
+    // z-parallel antennas: the run polynomials of the block's (at most two)
+    // integration rows, once per block
+    __shared__ cx s_rowp[2][FF_VMAX * 2];
     const bool vert = s_vert != 0;
     if (vert) {
         const int nimg = pec ? 2 : 1;
@@ -298,16 +333,13 @@ __global__ void __launch_bounds__(FF_THREADS, 5) k_farfield(
             const int row = row_lo + rr;
             if (row >= n_th) continue;
             double rh[3], th[3], ph[3];
-            unit_vectors_dev((double)row * th_max / ((double)n_th - 1.0), 0.0, rh, th, ph);
+            unit_vectors_row(s_row_st[rr], s_row_ct[rr], 0.0, rh, th, ph);
             s_rowp[rr][q * 2 + img] = run_poly(s_runs[q], s_cur, u.k_rp, img, rh);
         }
         __syncthreads();
     }
     double contrib = 0.0;
     if (r0.live || r1.live) {
-        double rh0[3], th0[3], ph0[3], rh1[3], th1[3], ph1[3];
-        unit_vectors_dev(r0.th, r0.ph, rh0, th0, ph0);
-        unit_vectors_dev(r1.th, r1.ph, rh1, th1, ph1);
         cx ft0, fp0, ft1, fp1;
         if (vert && d0 < n_int && d1 < n_int) {
             field_vert(s_runs, a.n_run, s_rowp[d0 / 360 - row_lo], u.k_rp, pec, rh0, th0, ph0, ft0, fp0);
