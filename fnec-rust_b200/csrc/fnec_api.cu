@@ -653,7 +653,8 @@ struct fnec_batch {
     std::vector<DevRun> runs;
     std::vector<DevRp> rps;
     std::vector<double> pts;
-    std::vector<int4> fill_tiles, gram_tiles;
+    std::vector<int4> fill_units, gram_tiles;  // fill_units: (unit, tiles per side, first tile, 0)
+    int64_t n_fill = 0;                         // 16x16 fill tiles, listed on the device (k_fill_tile_list)
     std::vector<int64_t> feed_row_off;
     std::vector<double> rhs_given;   // 2 * total rhs
     std::vector<double> cos_given;
@@ -685,7 +686,7 @@ struct fnec_batch {
     DevRun *d_runs = nullptr;
     DevRp *d_rps = nullptr;
     double *d_pts = nullptr;
-    int4 *d_fill_tiles = nullptr, *d_gram_tiles = nullptr;
+    int4 *d_fill_tiles = nullptr, *d_gram_tiles = nullptr, *d_fill_units = nullptr;
     int64_t *d_feed_row_off = nullptr;
     double *d_rhs_given = nullptr, *d_cos_given = nullptr, *d_z_given = nullptr;
     DevStamp *d_stamps = nullptr;
@@ -1223,8 +1224,9 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
             }
             b->units.push_back(u);
             if (need_solve) {
-                for (int i0 = 0; i0 < n; i0 += 16)
-                    for (int j0 = 0; j0 < n; j0 += 16) b->fill_tiles.push_back(make_int4(uidx, i0, j0, 0));
+                const int nt = (n + 15) / 16;
+                b->fill_units.push_back(make_int4(uidx, nt, (int)b->n_fill, 0));
+                b->n_fill += (int64_t)nt * nt;
                 for (int i0 = 0; i0 < n; i0 += 64)
                     for (int j0 = 0; j0 <= n; j0 += 64) b->gram_tiles.push_back(make_int4(uidx, i0, j0, 0));
             }
@@ -1246,7 +1248,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
            o_units = pk.add(b->units), o_solves = pk.add(b->solves), o_ibuf = pk.add(b->ibuf), o_srcs = pk.add(b->srcs),
            o_feeds = pk.add(b->feeds), o_cons = pk.add(b->cons), o_codes = pk.add(b->codes),
            o_runs = pk.add(b->runs), o_rps = pk.add(b->rps), o_pts = pk.add(b->pts),
-           o_ft = pk.add(b->fill_tiles), o_crows = pk.add(b->crows), o_gt = pk.add(b->gram_tiles), o_fro = pk.add(b->feed_row_off),
+           o_ft = pk.add(b->fill_units), o_crows = pk.add(b->crows), o_gt = pk.add(b->gram_tiles), o_fro = pk.add(b->feed_row_off),
            o_rhs = pk.add(b->rhs_given), o_cos = pk.add(b->cos_given), o_z = pk.add(b->z_given),
            o_st = pk.add(b->stamps), o_rg = pk.add(b->rhs_groups);
     b->in_bytes = pk.total > 0 ? pk.total : 256;
@@ -1274,7 +1276,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
         b->d_runs = (DevRun *)(b->d_in + o_runs);
         b->d_rps = (DevRp *)(b->d_in + o_rps);
         b->d_pts = (double *)(b->d_in + o_pts);
-        b->d_fill_tiles = (int4 *)(b->d_in + o_ft);
+        b->d_fill_units = (int4 *)(b->d_in + o_ft);
         b->d_crows = (DevConRow *)(b->d_in + o_crows);
         b->d_gram_tiles = (int4 *)(b->d_in + o_gt);
         b->d_feed_row_off = (int64_t *)(b->d_in + o_fro);
@@ -1290,6 +1292,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
 #define DA(p, n)                                             \
     if (e == cudaSuccess) e = dalloc(b, &b->p, (size_t)(n));
     if (b->from_wires) DA(d_segs, b->tot_seg);
+    DA(d_fill_tiles, b->n_fill);
     DA(d_z, b->z_el);
     DA(d_a, precision == FNEC_PRECISION_MIXED ? 1 : b->a_el);  // the mixed form factors in FP32
     DA(d_x, b->x_el);
@@ -1689,6 +1692,16 @@ int fnec_batch_get_unit_info(const fnec_batch *b, uint32_t unit, fnec_unit_info 
     return FNEC_OK;
 }
 
+// Entry q of the fill list covers unit fu.x with fu.y tiles per side from
+// tile fu.z on: tile fu.z + i fu.y + j is (unit, 16 i, 16 j) -- the list the
+// host would otherwise upload, formed in place.
+__global__ void k_fill_tile_list(const int4 *__restrict__ fill_units, int4 *tiles) {
+    const int4 fu = fill_units[blockIdx.y];
+    const int64_t cnt = (int64_t)fu.y * fu.y;
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < cnt; k += (int64_t)gridDim.x * blockDim.x)
+        tiles[fu.z + k] = make_int4(fu.x, (int)(k / fu.y) * 16, (int)(k % fu.y) * 16, 0);
+}
+
 int fnec_batch_upload(fnec_batch *b) {
     if (!b) return FNEC_ERR_BAD_ARG;
     fnec_ctx *ctx = b->ctx;
@@ -1696,6 +1709,10 @@ int fnec_batch_upload(fnec_batch *b) {
     // one pinned host -> device copy of every input table
     b->h2d = b->in_bytes;
     CUDA_TRY(ctx, cudaMemcpyAsync(b->d_in, b->h_in, b->in_bytes, cudaMemcpyHostToDevice, b->st));
+    if (!b->fill_units.empty()) {  // the 16x16 fill tiles, from each unit's tiles per side
+        k_fill_tile_list<<<dim3(64, (unsigned)b->fill_units.size()), 256, 0, b->st>>>(b->d_fill_units, b->d_fill_tiles);
+        CUDA_TRY(ctx, cudaPeekAtLastError());
+    }
     if (!b->z_given.empty())
         CUDA_TRY(ctx, cudaMemcpyAsync(b->d_z, b->d_z_given, sizeof(double) * b->z_given.size(),
                                       cudaMemcpyDeviceToDevice, b->st));
@@ -1764,14 +1781,14 @@ static int run_pipeline(fnec_batch *b) {
         check("segments and right-hand sides");
         MixedMarks mm{b->profile ? &b->ev[3] : nullptr};
         L += run_mixed(b->mixed, b->d_units, nu, b->d_solves, ns, b->d_ants, b->d_segs, b->d_fill_tiles,
-                       (int)b->fill_tiles.size(), b->d_gram_tiles, (int)b->gram_tiles.size(), b->d_ibuf,
+                       (int)b->n_fill, b->d_gram_tiles, (int)b->gram_tiles.size(), b->d_ibuf,
                        b->d_crows, b->d_z, b->d_rhs, b->d_cos, b->d_x, b->d_piv, b->d_status, b->max_s,
                        b->z_given.empty(), b->max_w, b->grid, mm, st, b->d_stamps, (int)b->stamps.size());
         if (!failed && mm.failed_phase) failed = mm.failed_phase;
         if (mm.detail[0]) detail = mm.detail;
     } else {
         if (b->z_given.empty()) {
-            launch_fill_exact(b->d_units, b->d_ants, b->d_segs, b->d_fill_tiles, (int)b->fill_tiles.size(),
+            launch_fill_exact(b->d_units, b->d_ants, b->d_segs, b->d_fill_tiles, (int)b->n_fill,
                               b->d_z, st);
             ++L;
             if (!b->stamps.empty()) {
