@@ -727,6 +727,7 @@ struct fnec_batch {
     unsigned char *stage = nullptr;  // page-locked staging of uploads (pooled batches)
     size_t stage_cap = 0, stage_used = 0;
     double alloc_ms = 0;  // host time spent allocating (device pool, pinned arenas, mixed work)
+    double create_ms = 0, antennas_ms = 0;  // fnec_batch_create in all, and its per-antenna planning
     double t_dev = 0, t_copy = 0, t_pinned = 0, t_mixed = 0;  // its parts: device allocations,
                                                              // table uploads, pinned arenas, mixed work
     std::vector<int32_t> grid_order;
@@ -791,6 +792,62 @@ static cudaError_t up(fnec_batch *b, T *d, const std::vector<T> &h) {
     return e;
 }
 
+// Page-locked host blocks kept for reuse: pinning pages is the slowest part
+// of planning a batch (tens of milliseconds for its input arena), and a
+// caller that plans a new batch per request frees and asks again for
+// blocks of the same sizes.  A request takes the smallest cached block of
+// at least its size and at most twice it (plus 4 MB); freed blocks are kept
+// while the cache holds at most PIN_CACHE_MAX bytes.  Blocks are rounded up
+// to 1 MB.  fnec_host_cache_release frees what is cached.
+constexpr size_t PIN_CACHE_MAX = (size_t)1 << 30;
+static std::mutex g_pin_mu;
+static std::multimap<size_t, void *> g_pin_free;   // capacity -> block
+static std::map<void *, size_t> g_pin_cap;          // every block handed out -> capacity
+static size_t g_pin_cached = 0;
+
+static cudaError_t pin_alloc(void **p, size_t bytes) {
+    const size_t need = ((bytes ? bytes : 1) + ((size_t)1 << 20) - 1) & ~(((size_t)1 << 20) - 1);
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mu);
+        auto it = g_pin_free.lower_bound(need);
+        if (it != g_pin_free.end() && it->first <= 2 * need + ((size_t)4 << 20)) {
+            *p = it->second;
+            g_pin_cached -= it->first;
+            g_pin_cap[*p] = it->first;
+            g_pin_free.erase(it);
+            return cudaSuccess;
+        }
+    }
+    cudaError_t e = cudaMallocHost(p, need);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return e;
+    }
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    g_pin_cap[*p] = need;
+    return cudaSuccess;
+}
+
+// false: p is not a block of this cache
+static bool pin_free(void *p) {
+    if (!p) return true;
+    size_t cap = 0;
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mu);
+        auto it = g_pin_cap.find(p);
+        if (it == g_pin_cap.end()) return false;
+        cap = it->second;
+        g_pin_cap.erase(it);
+        if (g_pin_cached + cap <= PIN_CACHE_MAX) {
+            g_pin_free.emplace(cap, p);
+            g_pin_cached += cap;
+            return true;
+        }
+    }
+    cudaFreeHost(p);
+    return true;
+}
+
 static void free_batch(fnec_batch *b) {
     for (void *p : b->allocs) {
         if (b->pooled) cudaFreeAsync(p, b->st);
@@ -798,8 +855,8 @@ static void free_batch(fnec_batch *b) {
     }
     b->allocs.clear();
     if (!b->pooled) {  // pooled batches borrow their lane's pinned arenas
-        if (b->h_in) cudaFreeHost(b->h_in);
-        if (b->h_out) cudaFreeHost(b->h_out);
+        pin_free(b->h_in);
+        pin_free(b->h_out);
     }
     b->h_in = b->h_out = nullptr;
     if (b->gexec) cudaGraphExecDestroy(b->gexec);
@@ -1258,7 +1315,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
         b->h_in = place.in->p;
         b->t_pinned += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta0).count();
     } else {
-        e = cudaMallocHost((void **)&b->h_in, b->in_bytes);
+        e = pin_alloc((void **)&b->h_in, b->in_bytes);
     }
     if (e == cudaSuccess) e = dalloc(b, &b->d_in, b->in_bytes);
     if (e == cudaSuccess) {
@@ -1345,7 +1402,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
             b->h_out = place.out->p;
             b->t_pinned += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tp).count();
         } else {
-            e = cudaMallocHost((void **)&b->h_out, b->out_bytes);
+            e = pin_alloc((void **)&b->h_out, b->out_bytes);
         }
     }
     if (e == cudaSuccess && precision == FNEC_PRECISION_MIXED) {
@@ -1640,6 +1697,7 @@ int fnec_batch_create(fnec_ctx *ctx, const fnec_antenna *antennas, uint32_t n_an
     if (precision == FNEC_PRECISION_MIXED && !mixed_available())
         return fail(ctx, FNEC_ERR_UNSUPPORTED, "mixed precision path not built");
     cudaSetDevice(ctx->device);
+    const auto tc0 = std::chrono::steady_clock::now();
     std::vector<HostAnt> hs(n_antennas);
     // each antenna's host planning (segments, topology, junctions, sources)
     // is independent: spread over host threads for large batches
@@ -1660,7 +1718,13 @@ int fnec_batch_create(fnec_ctx *ctx, const fnec_antenna *antennas, uint32_t n_an
     }
     for (uint32_t a = 0; a < n_antennas; ++a)
         if (st_of[a] != FNEC_OK) return fail(ctx, st_of[a], "antenna " + std::to_string(a) + ": " + why_of[a]);
-    return build_batch(ctx, hs, precision, out);
+    const double ant_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tc0).count();
+    const int rc = build_batch(ctx, hs, precision, out);
+    if (rc == FNEC_OK && *out) {
+        (*out)->antennas_ms = ant_ms;
+        (*out)->create_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tc0).count();
+    }
+    return rc;
 }
 
 int fnec_batch_destroy(fnec_batch *b) {
@@ -1683,6 +1747,12 @@ int fnec_batch_get_info(const fnec_batch *b, fnec_batch_info *out) {
     out->device_bytes = b->dev_bytes;
     out->h2d_bytes = b->h2d;
     out->kernel_launches = b->launches;
+    out->create_ms = b->create_ms;
+    out->antennas_ms = b->antennas_ms;
+    out->alloc_ms = b->alloc_ms;
+    out->alloc_device_ms = b->t_dev;
+    out->alloc_pinned_ms = b->t_pinned;
+    out->alloc_mixed_ms = b->t_mixed;
     return FNEC_OK;
 }
 
@@ -2452,7 +2522,7 @@ static bool is_pinned(const void *p) {
 extern "C" int fnec_host_alloc(uint64_t bytes, void **out) {
     if (!out) return FNEC_ERR_BAD_ARG;
     *out = nullptr;
-    if (cudaMallocHost(out, bytes ? bytes : 1) != cudaSuccess) {
+    if (pin_alloc(out, (size_t)bytes) != cudaSuccess) {
         (void)cudaGetLastError();
         return FNEC_ERR_OUT_OF_MEMORY;
     }
@@ -2460,7 +2530,20 @@ extern "C" int fnec_host_alloc(uint64_t bytes, void **out) {
 }
 
 extern "C" int fnec_host_free(void *p) {
-    if (p && cudaFreeHost(p) != cudaSuccess) return FNEC_ERR_CUDA;
+    if (!p) return FNEC_OK;
+    if (pin_free(p)) return FNEC_OK;
+    return cudaFreeHost(p) == cudaSuccess ? FNEC_OK : FNEC_ERR_CUDA;  // not one of the cache's blocks
+}
+
+extern "C" int fnec_host_cache_release(uint64_t *released) {
+    std::multimap<size_t, void *> blocks;
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mu);
+        blocks.swap(g_pin_free);
+        if (released) *released = g_pin_cached;
+        g_pin_cached = 0;
+    }
+    for (auto &kv : blocks) cudaFreeHost(kv.second);
     return FNEC_OK;
 }
 

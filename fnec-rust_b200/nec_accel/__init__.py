@@ -118,7 +118,9 @@ class _UnitInfo(ctypes.Structure):
 class _BatchInfo(ctypes.Structure):
     _fields_ = [("n_units", _U32), ("max_s", _U32), ("total_currents", _U64), ("total_feeds", _U64),
                 ("total_points", _U64), ("device_bytes", _U64), ("h2d_bytes", _U64),
-                ("kernel_launches", _U64), ("n_systems", _U32)]
+                ("kernel_launches", _U64), ("n_systems", _U32),
+                ("create_ms", _D), ("antennas_ms", _D), ("alloc_ms", _D), ("alloc_device_ms", _D),
+                ("alloc_pinned_ms", _D), ("alloc_mixed_ms", _D)]
 
 
 class _ServerConfig(ctypes.Structure):
@@ -196,6 +198,7 @@ SIGNATURES = {
     "fnec_batch_resolve": (ctypes.c_int, [_P]),
     "fnec_test_fail_device_allocation": (ctypes.c_int, [_I32]),
     "fnec_test_fill_sincospi": (ctypes.c_int, [_P, _U64, _P, _P]),
+    "fnec_host_cache_release": (ctypes.c_int, [_P]),
     "fnec_batch_create": (ctypes.c_int, [_P, _P, _U32, _I32, _P]),
     "fnec_batch_destroy": (ctypes.c_int, [_P]),
     "fnec_batch_get_info": (ctypes.c_int, [_P, _P]),
@@ -604,6 +607,14 @@ def test_fail_device_allocation(after: int):
         raise AccelError(rc, "test_fail_device_allocation")
 
 
+def host_cache_release() -> int:
+    """Free the page-locked host blocks the library keeps for reuse; returns
+    their bytes."""
+    n = ctypes.c_uint64()
+    lib().fnec_host_cache_release(ctypes.byref(n))
+    return int(n.value)
+
+
 def test_fill_sincospi(x):
     """Test hook: the mixed fill's own sin(pi x), cos(pi x), run on the host
     (0 <= x < 2^50)."""
@@ -813,11 +824,7 @@ class HallenBatch:
         info = _BatchInfo()
         lib().fnec_batch_get_info(self._h, ctypes.byref(info))
         self.info = info
-        self.units = []
-        for u in range(info.n_units):
-            ui = _UnitInfo()
-            lib().fnec_batch_get_unit_info(self._h, u, ctypes.byref(ui))
-            self.units.append({k: getattr(ui, k) for k, _ in _UnitInfo._fields_})
+        self._units = None  # per-unit descriptions, read on first use
         # host result buffers, allocated once in page-locked memory: the
         # library copies straight into them
         self._host = []
@@ -994,6 +1001,19 @@ class HallenBatch:
             return None
         self.sync()
         return self.read()
+
+    @property
+    def units(self) -> list:
+        """One dict of _UnitInfo fields per solve unit, read from the library
+        on first use (one call per unit)."""
+        if self._units is None:
+            us = []
+            for u in range(self.info.n_units):
+                ui = _UnitInfo()
+                lib().fnec_batch_get_unit_info(self._h, u, ctypes.byref(ui))
+                us.append({k: getattr(ui, k) for k, _ in _UnitInfo._fields_})
+            self._units = us
+        return self._units
 
     def _pinned(self, shape, dtype):
         nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize

@@ -252,6 +252,11 @@ typedef struct {
     uint64_t h2d_bytes;      /* input bytes copied by fnec_batch_upload */
     uint64_t kernel_launches;/* launches issued by one fnec_batch_run  */
     uint32_t n_systems;      /* factorisations (antenna, frequency)     */
+    /* host milliseconds of fnec_batch_create: in all; the per-antenna
+     * planning (segments, topology, junctions, sources; on host threads);
+     * allocation in all, and its device, pinned-host and mixed-work parts
+     * (the rest: tables, packing, the first upload) */
+    double create_ms, antennas_ms, alloc_ms, alloc_device_ms, alloc_pinned_ms, alloc_mixed_ms;
 } fnec_batch_info;
 
 typedef struct fnec_ctx fnec_ctx;
@@ -502,9 +507,13 @@ int fnec_server_stats(fnec_server *s, fnec_server_stats_t *out, int32_t reset);
 
 /* Page-locked host memory (no counterpart in the reference).  Result arrays
  * passed to fnec_batch_read in such memory are written by direct device
- * copies, without the staging copy pageable memory needs. */
+ * copies, without the staging copy pageable memory needs.  Freed blocks
+ * (these and the batches' input / result arenas) are kept for reuse, up to
+ * 1 GiB in all: pinning pages is the slowest part of planning a batch.
+ * fnec_host_cache_release frees the kept blocks (*released: their bytes). */
 int fnec_host_alloc(uint64_t bytes, void **out);
 int fnec_host_free(void *p);
+int fnec_host_cache_release(uint64_t *released);
 
 /* Self-test of the 3xTF32 tensor-core GEMM that forms the mixed form's
  * Gram matrix (no counterpart in the reference): C = A B^T with A (m x k),
