@@ -718,11 +718,13 @@ struct fnec_batch {
     cudaEvent_t ev_copy = nullptr;
     MixedWork mixed;
     GridPlan grid;
-    // execution: the stream every operation of the batch is enqueued on;
-    // pooled batches take device memory from the stream-ordered pool and
-    // borrow their pinned host arenas (the server's lanes)
+    // execution: the stream every operation of the batch is enqueued on.
+    // Device memory comes from the device's stream-ordered pool (dev_pool),
+    // which keeps what a destroyed batch freed for the next one; pooled
+    // batches also borrow their pinned host arenas (the server's lanes)
     cudaStream_t st = nullptr;
     bool pooled = false;
+    bool dev_pool = true;
     bool allow_grid = true;
     unsigned char *stage = nullptr;  // page-locked staging of uploads (pooled batches)
     size_t stage_cap = 0, stage_used = 0;
@@ -771,8 +773,8 @@ static cudaError_t dalloc(fnec_batch *b, T **p, size_t count) {
     if (count == 0) count = 1;
     if (take_injected_alloc_failure()) return cudaErrorMemoryAllocation;
     const auto t0 = std::chrono::steady_clock::now();
-    cudaError_t e = b->pooled ? cudaMallocAsync((void **)p, sizeof(T) * count, b->st)
-                              : cudaMalloc((void **)p, sizeof(T) * count);
+    cudaError_t e = b->dev_pool ? cudaMallocAsync((void **)p, sizeof(T) * count, b->st)
+                                : cudaMalloc((void **)p, sizeof(T) * count);
     b->t_dev += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     if (e == cudaSuccess) {
         b->allocs.push_back(*p);
@@ -786,7 +788,7 @@ static cudaError_t up(fnec_batch *b, T *d, const std::vector<T> &h) {
     if (h.empty()) return cudaSuccess;
     b->h2d += sizeof(T) * h.size();
     const auto t0 = std::chrono::steady_clock::now();
-    DevAlloc dev{b->st, b->pooled, b->stage, b->stage_cap, &b->stage_used};
+    DevAlloc dev{b->st, b->dev_pool, b->stage, b->stage_cap, &b->stage_used};
     cudaError_t e = dev.upload(d, h.data(), sizeof(T) * h.size());
     b->t_copy += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
     return e;
@@ -850,7 +852,7 @@ static bool pin_free(void *p) {
 
 static void free_batch(fnec_batch *b) {
     for (void *p : b->allocs) {
-        if (b->pooled) cudaFreeAsync(p, b->st);
+        if (b->dev_pool) cudaFreeAsync(p, b->st);
         else cudaFree(p);
     }
     b->allocs.clear();
@@ -875,7 +877,7 @@ static void free_batch(fnec_batch *b) {
     if (b->side) cudaStreamDestroy(b->side);
     b->ev_fork = b->ev_join = nullptr;
     b->side = nullptr;
-    free_mixed(b->mixed, DevAlloc{b->st, b->pooled});
+    free_mixed(b->mixed, DevAlloc{b->st, b->dev_pool});
 }
 
 // Carve the packed input arena: every host table gets a 256-byte aligned
@@ -1408,7 +1410,7 @@ static int build_batch(fnec_ctx *ctx, std::vector<HostAnt> &hs, int precision, f
     if (e == cudaSuccess && precision == FNEC_PRECISION_MIXED) {
         const auto tm = std::chrono::steady_clock::now();
         e = alloc_mixed(b->mixed, b->units, b->solves, b->ants, b->max_s,
-                        DevAlloc{b->st, b->pooled, b->stage, b->stage_cap, &b->stage_used}, b->allow_grid);
+                        DevAlloc{b->st, b->dev_pool, b->stage, b->stage_cap, &b->stage_used}, b->allow_grid);
         b->t_mixed += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tm).count();
     }
     b->alloc_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - ta0).count();
@@ -1671,7 +1673,31 @@ int fnec_ctx_create(int device, fnec_ctx **out) {
         delete c;
         return FNEC_ERR_CUDA;
     }
+    // batches allocate from the device's stream-ordered pool: keep what a
+    // destroyed batch frees there for the next batch (unmapping and mapping
+    // device memory again costs tens of milliseconds for a large batch);
+    // fnec_device_cache_release gives it back
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
     *out = c;
+    return FNEC_OK;
+}
+
+int fnec_device_cache_release(fnec_ctx *ctx, uint64_t *released) {
+    if (!ctx) return FNEC_ERR_BAD_ARG;
+    if (released) *released = 0;
+    cudaSetDevice(ctx->device);
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) != cudaSuccess) return FNEC_ERR_CUDA;
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) return FNEC_ERR_CUDA;
+    uint64_t before = 0, after = 0;
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &before);
+    if (cudaMemPoolTrimTo(pool, 0) != cudaSuccess) return FNEC_ERR_CUDA;
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &after);
+    if (released) *released = before > after ? before - after : 0;
     return FNEC_OK;
 }
 
@@ -3393,11 +3419,34 @@ int fnec_server_create(fnec_ctx *ctx, const fnec_server_config *cfg, fnec_server
             return fail(ctx, FNEC_ERR_CUDA, "lane stream creation failed");
         }
     }
-    // keep pool memory freed by finished batches cached for the next ones
+    // keep pool memory freed by finished batches cached for the next ones,
+    // and map the HBM budget into the pool now (less what it holds already;
+    // at most the device's free memory less 2 GiB): a lane admitting a large
+    // batch under load then suballocates instead of waiting for the driver
+    // to map gigabytes (about a second for 8 GiB)
     cudaMemPool_t pool;
     if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
         uint64_t keep = UINT64_MAX;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        uint64_t held = 0;
+        size_t fr = 0, tot = 0;
+        cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &held);
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+            const uint64_t margin = (uint64_t)2 << 30;
+            uint64_t want = S->cfg.hbm_budget_bytes > held ? S->cfg.hbm_budget_bytes - held : 0;
+            want = std::min<uint64_t>(want, fr > margin ? fr - margin : 0);
+            void *p = nullptr;
+            if (want >= ((uint64_t)64 << 20)) {
+                if (cudaMallocAsync(&p, want, S->lanes[0].st) == cudaSuccess) {
+                    cudaFreeAsync(p, S->lanes[0].st);
+                    cudaStreamSynchronize(S->lanes[0].st);
+                } else {
+                    (void)cudaGetLastError();  // the pool grows on demand instead
+                }
+            }
+        } else {
+            (void)cudaGetLastError();
+        }
     }
     // page-locked arenas sized for typical batches up front: growing one later
     // frees the old arena, which waits for the whole device

@@ -199,6 +199,7 @@ SIGNATURES = {
     "fnec_test_fail_device_allocation": (ctypes.c_int, [_I32]),
     "fnec_test_fill_sincospi": (ctypes.c_int, [_P, _U64, _P, _P]),
     "fnec_host_cache_release": (ctypes.c_int, [_P]),
+    "fnec_device_cache_release": (ctypes.c_int, [_P, _P]),
     "fnec_batch_create": (ctypes.c_int, [_P, _P, _U32, _I32, _P]),
     "fnec_batch_destroy": (ctypes.c_int, [_P]),
     "fnec_batch_get_info": (ctypes.c_int, [_P, _P]),
@@ -612,6 +613,15 @@ def host_cache_release() -> int:
     their bytes."""
     n = ctypes.c_uint64()
     lib().fnec_host_cache_release(ctypes.byref(n))
+    return int(n.value)
+
+
+def device_cache_release(ctx: Optional["Context"] = None) -> int:
+    """Return the device memory that destroyed batches left in the device's
+    stream-ordered pool to the driver; returns its bytes."""
+    c = ctx or default_context()
+    n = ctypes.c_uint64()
+    c.check(lib().fnec_device_cache_release(c.handle, ctypes.byref(n)), "device_cache_release")
     return int(n.value)
 
 

@@ -412,7 +412,10 @@ int fnec_measure_fp32_peak(int device, double *ffma_tflops);
  * (fnec_server_result) until fnec_server_release.  Requests arriving while
  * batches run are admitted as lanes and memory free up; the lanes' planning,
  * kernels and copies overlap.  With more than one lane the grid-wide
- * (cooperative) kernels are not used. */
+ * (cooperative) kernels are not used.  At creation the server maps its HBM
+ * budget (at most the device's free memory less 2 GiB) into the device's
+ * stream-ordered pool, so that admission under load suballocates instead of
+ * waiting for the driver to map memory. */
 typedef struct fnec_server fnec_server;
 
 typedef struct {
@@ -514,6 +517,14 @@ int fnec_server_stats(fnec_server *s, fnec_server_stats_t *out, int32_t reset);
 int fnec_host_alloc(uint64_t bytes, void **out);
 int fnec_host_free(void *p);
 int fnec_host_cache_release(uint64_t *released);
+
+/* Device memory of batches comes from the device's stream-ordered pool, which
+ * keeps what a destroyed batch frees for the next batch (mapping and
+ * unmapping a large batch's memory costs tens of milliseconds).
+ * fnec_device_cache_release waits for the context's stream and returns the
+ * pool's unused memory to the driver (*released: its bytes), e.g. before
+ * another library on the device allocates. */
+int fnec_device_cache_release(fnec_ctx *ctx, uint64_t *released);
 
 /* Self-test of the 3xTF32 tensor-core GEMM that forms the mixed form's
  * Gram matrix (no counterpart in the reference): C = A B^T with A (m x k),

@@ -98,6 +98,35 @@ def test_device_allocation_failure_is_reported_and_leaks_nothing(acc, after):
     _dipole_ok(acc)
 
 
+def test_freed_batch_memory_is_reused_then_released(acc):
+    """A destroyed batch's device memory stays in the stream-ordered pool: a
+    second batch of the same shape takes it without growing the pool, and
+    device_cache_release hands it back to the driver; page-locked blocks are
+    kept the same way until host_cache_release."""
+    import torch
+
+    ant = acc.Antenna(acc.wires_array(DIPOLE), acc.sources_array([(1, 26, 1.0)]),
+                      [14.0e6 + 0.1e6 * k for k in range(64)], acc.GROUND_FREE, (19, 37, 0.0, 5.0, 0.0, 10.0))
+    for prec in (acc.PRECISION_FP64, acc.PRECISION_MIXED):
+        b = acc.HallenBatch([ant] * 8, precision=prec)
+        ref = np.concatenate(b.solve().currents)
+        b.close()
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info()
+        b = acc.HallenBatch([ant] * 8, precision=prec)
+        cur = np.concatenate(b.solve().currents)
+        assert np.array_equal(cur.view(np.uint64), ref.view(np.uint64))
+        b.close()
+        torch.cuda.synchronize()
+        free1, _ = torch.cuda.mem_get_info()
+        assert free1 == free0
+        released = acc.device_cache_release()
+        free2, _ = torch.cuda.mem_get_info()
+        assert released > 0 and free2 > free1
+    assert acc.host_cache_release() > 0
+    _dipole_ok(acc)
+
+
 def test_non_finite_geometry_is_refused_for_that_antenna_only(acc):
     """A NaN coordinate, an infinite radius or a NaN frequency never reaches
     a kernel: a batch naming such an antenna is refused with the antenna's

@@ -120,3 +120,30 @@ def test_request_footprint_bounds_the_batch(acc, precision):
             b = acc.HallenBatch([a], precision=precision)
             assert b.info.device_bytes <= est, (b.info.device_bytes, est)
             b.close()
+
+
+def test_server_maps_its_budget_up_front(acc):
+    """Creating a server maps its HBM budget into the device's pool, so the
+    batches it admits suballocate: serving leaves free device memory
+    unchanged."""
+    import torch
+
+    ants = _antennas(acc, 12, seed=27)
+    acc.device_cache_release()
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    budget = 2 << 30
+    with acc.Server(acc.PRECISION_MIXED, lanes=2, max_batch=4, hbm_budget_bytes=budget) as srv:
+        free1, _ = torch.cuda.mem_get_info()
+        assert free0 - free1 >= budget // 2, (free0, free1)
+        free = []
+        for _ in range(2):  # the first pass also loads any kernel not used before
+            reqs = [srv.submit(a) for a in ants]
+            for r in reqs:
+                srv.wait(r)
+                assert np.all(np.asarray(r.result()[3]) == 0)
+                r.release()
+            torch.cuda.synchronize()
+            free.append(torch.cuda.mem_get_info()[0])
+        assert free[1] == free[0], free
+        assert free1 - free[1] < budget // 8, (free1, free)
