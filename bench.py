@@ -294,15 +294,17 @@ def ff_directions(ground, rp):
     return n_int + nt * nph - int(on_t.sum()) * int(on_p.sum()) - int(below)
 
 
-def dram_traffic(phase, form, units):
+def dram_traffic(phase, form, units, workload=None):
     """DRAM bytes of one run of a phase, scaled by units from the per-unit
-    figure of an ncu capture committed under profiles/ (None if none)."""
+    figure of an ncu capture committed under profiles/ (None if none): the
+    capture of a smaller case of the same workload when there is one, else
+    of the sweep workload."""
     key = {("solve", "mixed"): "solve_mixed", ("farfield", "mixed"): "farfield", ("farfield", "fp64"): "farfield",
            ("fill", "fp64"): "fill_fp64"}.get((phase, form))
     try:
         with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "traffic.json")) as fh:
             t = json.load(fh)
-        e = t[key]
+        e = t.get(f"{key}_{workload}") or t[key]
         return float(e["bytes_per_unit"]) * units, "profiles/" + e["capture"]
     except Exception:
         return None, None
@@ -315,8 +317,10 @@ def phase_rooflines(form, o, n, s, g, d, shapes, fma, muladd, ffma, peaks, runs)
     3xTF32 tensor-core flops issued on the upper-triangle 128x128 tiles
     (mixed); factor (8/3) S^3 flops (GEPP) or (4/3) S^3 (the mixed form's
     Hermitian factor, lower triangle only); solve: plain back substitution 8 S^2
-    flops on a serial chain, mixed GMRES HBM bytes (iterations + 2) x
-    (32 N^2 + 8 S^2) (FP64 Z read twice, FP32 factor once per apply); far
+    flops on a serial chain, mixed GMRES HBM bytes (iterations + 1) x
+    (16 N^2 + 8 S^2 + 512 S) (FP64 Z streamed once per apply of M^H M, the
+    FP32 factor and its diagonal blocks' inverses once per preconditioner
+    apply); far
     field 8 N flops per direction (its sincos per wire run is not counted);
     antennas of z-parallel wires: 8 flops per (block row, segment) plus 8
     per (direction, run), the per-row path of the kernel."""
@@ -357,8 +361,11 @@ def phase_rooflines(form, o, n, s, g, d, shapes, fma, muladd, ffma, peaks, runs)
         s_s = np.array([u["s"] for u in shapes], np.float64)
         its = it if it is not None and len(it) == len(n_s) else np.full(len(n_s), 5.0)
         # per operator + preconditioner application: Z once (16 N^2), the
-        # FP32 factor (8 S^2), its diagonal block inverses (1 KB per row)
-        byt = float(np.sum((its + 2) * (16 * n_s * n_s + 8 * s_s * s_s + 1024 * s_s)))
+        # FP32 factor (8 S^2: L below and U above the diagonal blocks) and
+        # the diagonal blocks' FP32 inverses (two 32 x 32 complex64 blocks
+        # per 32 rows: 512 B per row); iterations + 1 of them (the first
+        # pass forms M^H y and applies the preconditioner to it)
+        byt = float(np.sum((its + 1) * (16 * n_s * n_s + 8 * s_s * s_s + 512 * s_s)))
         put("solve", byt / 1e9, peaks["hbm_gbs"], "GB/s", "hbm", peaks["source"])
     dd = np.asarray(d, np.float64)
     nr = np.asarray(runs, np.float64)
@@ -1013,7 +1020,7 @@ def run_batch_workload(args, acc, ctx, rank, local, dist, world, steps, warmup, 
     dom = max(("fill", "gram", "factor", "solve", "farfield"), key=lambda k: phase[k])
     roof = dict(rr[headline][dom])
     roof["kernel"] = dom
-    roof["traffic"], roof["traffic_source"] = dram_traffic(dom, headline, units_local)
+    roof["traffic"], roof["traffic_source"] = dram_traffic(dom, headline, units_local, args.workload)
     samples = flops["fill_samples"]
     per_step_units = job_units
     line = {

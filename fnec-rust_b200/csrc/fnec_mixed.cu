@@ -751,12 +751,48 @@ __global__ void __launch_bounds__(64) k_swap_u12_32(const UnitDesc *__restrict__
 // pair's deferred update of everything to the right and below.  lower:
 // only the tiles on and below the diagonal (the Hermitian factor; kparts
 // 1, col_end s), T (T + 1) / 2 of them, row-major.
+// Asynchronous 8-byte global -> shared copy (cp.async, no register
+// staging); valid false writes zeros and reads nothing (src points into the
+// matrix all the same).  cp_async_wait_all waits for this thread's copies.
+__device__ __forceinline__ void cp_async8(void *dst, const void *src, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ void lower_tile(int i, int &tr, int &tc) {
     int r = (int)((sqrtf(8.f * (float)i + 1.f) - 1.f) * 0.5f);
     while (r * (r + 1) / 2 > i) --r;
     while ((r + 1) * (r + 2) / 2 <= i) ++r;
     tr = r;
     tc = i - r * (r + 1) / 2;
+}
+
+// acc -= s_l s_u over the 32 panel columns for thread (ty, tx)'s 4 x 4
+// entries of a 64 x 64 trailing tile (rows ty + 16 a, columns tx + 16 b).
+// SKIP_UR: a diagonal tile of the Hermitian factor, whose upper-right 32 x
+// 32 block (a < 2, b >= 2) is left alone -- those entries belong to a later
+// step's U12, which that step's panel writes as its L21's mirror before
+// anything reads them (every other entry gets the same operations).
+template <bool SKIP_UR>
+__device__ __forceinline__ void tile_fma(float2 (&acc)[4][4], const float2 (*s_l)[MNB + 1], const float2 (*s_u)[64],
+                                         int ty, int tx) {
+#pragma unroll 4
+    for (int q = 0; q < MNB; ++q) {
+        float2 lv[4], uv[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) lv[a] = s_l[ty + 16 * a][q];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) uv[b] = s_u[q][tx + 16 * b];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                if (SKIP_UR && a < 2 && b >= 2) continue;
+                acc[a][b].x = fmaf(-lv[a].x, uv[b].x, fmaf(lv[a].y, uv[b].y, acc[a][b].x));
+                acc[a][b].y = fmaf(-lv[a].x, uv[b].y, fmaf(-lv[a].y, uv[b].x, acc[a][b].y));
+            }
+    }
 }
 
 __global__ void __launch_bounds__(256) k_trailing32(const UnitDesc *__restrict__ units, const MixedUnit *__restrict__ mus,
@@ -790,48 +826,37 @@ __global__ void __launch_bounds__(256) k_trailing32(const UnitDesc *__restrict__
     float2 *A = a32buf + mus[ui].a32_off;
     int tid = threadIdx.x;
     int ty = tid / 16, tx = tid % 16;
+    const bool skip_ur = lower && R0 == K0;  // a diagonal tile of the Hermitian factor (tile_fma)
     float2 acc[4][4];
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             int R = R0 + ty + 16 * a, K = K0 + tx + 16 * b;
-            acc[a][b] = (R < s && K < ce) ? A[(int64_t)R * s + K] : cf(0.f, 0.f);
+            acc[a][b] = (R < s && K < ce && !(skip_ur && a < 2 && b >= 2)) ? A[(int64_t)R * s + K] : cf(0.f, 0.f);
         }
     for (int part = 0; part < kparts; ++part) {
         const int cp = c0 + MNB * part;
         if (part) __syncthreads();  // the previous part's reads of s_l / s_u are done
         for (int e = tid; e < 64 * MNB; e += 256) {
-            int rr = e / MNB, q = e % MNB, R = R0 + rr;
-            s_l[rr][q] = (R < s) ? A[(int64_t)R * s + cp + q] : cf(0.f, 0.f);
+            const int rr = e / MNB, q = e % MNB, R = R0 + rr;
+            cp_async8(&s_l[rr][q], A + (int64_t)min(R, s - 1) * s + cp + q, R < s);
         }
         for (int e = tid; e < MNB * 64; e += 256) {
-            int q = e / 64, cc = e % 64, K = K0 + cc;
-            s_u[q][cc] = (K < ce) ? A[(int64_t)(cp + q) * s + K] : cf(0.f, 0.f);
+            const int q = e / 64, cc = e % 64, K = K0 + cc;
+            cp_async8(&s_u[q][cc], A + (int64_t)(cp + q) * s + min(K, ce - 1), K < ce);
         }
+        cp_async_wait_all();
         __syncthreads();
-#pragma unroll 4
-        for (int q = 0; q < MNB; ++q) {
-            float2 lv[4], uv[4];
-#pragma unroll
-            for (int a = 0; a < 4; ++a) lv[a] = s_l[ty + 16 * a][q];
-#pragma unroll
-            for (int b = 0; b < 4; ++b) uv[b] = s_u[q][tx + 16 * b];
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    acc[a][b].x = fmaf(-lv[a].x, uv[b].x, fmaf(lv[a].y, uv[b].y, acc[a][b].x));
-                    acc[a][b].y = fmaf(-lv[a].x, uv[b].y, fmaf(-lv[a].y, uv[b].x, acc[a][b].y));
-                }
-        }
+        if (skip_ur) tile_fma<true>(acc, s_l, s_u, ty, tx);
+        else tile_fma<false>(acc, s_l, s_u, ty, tx);
     }
 #pragma unroll
     for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             int R = R0 + ty + 16 * a, K = K0 + tx + 16 * b;
-            if (R < s && K < ce) A[(int64_t)R * s + K] = acc[a][b];
+            if (R < s && K < ce && !(skip_ur && a < 2 && b >= 2)) A[(int64_t)R * s + K] = acc[a][b];
         }
 }
 
@@ -1099,48 +1124,44 @@ __global__ void __launch_bounds__(FU_THREADS, 4) k_factor32_unit_herm(const Unit
         if (rows <= 0) continue;
         const int T = (rows + 63) / 64;
         const int ty = tid / 16, tx = tid % 16;
+        int staged_tr = -1;  // the tile row whose L21 block s_l holds
         for (int tile = 0; tile < T * (T + 1) / 2; ++tile) {
             int tr, tc;
             lower_tile(tile, tr, tc);
             const int R0 = r0 + tr * 64, K0 = r0 + tc * 64;
-            for (int e = tid; e < 64 * MNB; e += FU_THREADS) {
-                int rr = e / MNB, q = e % MNB, R = R0 + rr;
-                s_l[rr][q] = (R < s) ? A[(int64_t)R * s + c0 + q] : cf(0.f, 0.f);
+            // the panel blocks copied asynchronously (L21 only when the tile
+            // row changes: the tiles of a row share it) while this thread's
+            // A22 entries load
+            if (tr != staged_tr) {
+                for (int e = tid; e < 64 * MNB; e += FU_THREADS) {
+                    const int rr = e / MNB, q = e % MNB, R = R0 + rr;
+                    cp_async8(&s_l[rr][q], A + (int64_t)min(R, s - 1) * s + c0 + q, R < s);
+                }
+                staged_tr = tr;
             }
             for (int e = tid; e < MNB * 64; e += FU_THREADS) {
-                int q = e / 64, cc = e % 64, K = K0 + cc;
-                s_u[q][cc] = (K < s) ? A[(int64_t)(c0 + q) * s + K] : cf(0.f, 0.f);
+                const int q = e / 64, cc = e % 64, K = K0 + cc;
+                cp_async8(&s_u[q][cc], A + (int64_t)(c0 + q) * s + min(K, s - 1), K < s);
             }
-            __syncthreads();
+            const bool diag = tr == tc;
             float2 acc[4][4];
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
                 for (int b = 0; b < 4; ++b) {
                     int R = R0 + ty + 16 * a, K = K0 + tx + 16 * b;
-                    acc[a][b] = (R < s && K < s) ? A[(int64_t)R * s + K] : cf(0.f, 0.f);
+                    acc[a][b] = (R < s && K < s && !(diag && a < 2 && b >= 2)) ? A[(int64_t)R * s + K] : cf(0.f, 0.f);
                 }
-#pragma unroll 4
-            for (int q = 0; q < MNB; ++q) {
-                float2 lv[4], uv[4];
-#pragma unroll
-                for (int a = 0; a < 4; ++a) lv[a] = s_l[ty + 16 * a][q];
-#pragma unroll
-                for (int b = 0; b < 4; ++b) uv[b] = s_u[q][tx + 16 * b];
-#pragma unroll
-                for (int a = 0; a < 4; ++a)
-#pragma unroll
-                    for (int b = 0; b < 4; ++b) {
-                        acc[a][b].x = fmaf(-lv[a].x, uv[b].x, fmaf(lv[a].y, uv[b].y, acc[a][b].x));
-                        acc[a][b].y = fmaf(-lv[a].x, uv[b].y, fmaf(-lv[a].y, uv[b].x, acc[a][b].y));
-                    }
-            }
+            cp_async_wait_all();
+            __syncthreads();
+            if (diag) tile_fma<true>(acc, s_l, s_u, ty, tx);
+            else tile_fma<false>(acc, s_l, s_u, ty, tx);
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
                 for (int b = 0; b < 4; ++b) {
                     int R = R0 + ty + 16 * a, K = K0 + tx + 16 * b;
-                    if (R < s && K < s) A[(int64_t)R * s + K] = acc[a][b];
+                    if (R < s && K < s && !(diag && a < 2 && b >= 2)) A[(int64_t)R * s + K] = acc[a][b];
                 }
             __syncthreads();
         }
