@@ -317,10 +317,11 @@ def phase_rooflines(form, o, n, s, g, d, shapes, fma, muladd, ffma, peaks, runs)
     3xTF32 tensor-core flops issued on the upper-triangle 128x128 tiles
     (mixed); factor (8/3) S^3 flops (GEPP) or (4/3) S^3 (the mixed form's
     Hermitian factor, lower triangle only); solve: plain back substitution 8 S^2
-    flops on a serial chain, mixed GMRES HBM bytes (iterations + 1) x
-    (16 N^2 + 8 S^2 + 512 S) (FP64 Z streamed once per apply of M^H M, the
-    FP32 factor and its diagonal blocks' inverses once per preconditioner
-    apply); far
+    flops on a serial chain, mixed GMRES HBM bytes: 16 N^2 per iteration
+    (FP64 Z streamed once per apply of M^H M; one pass more for M^H y where
+    the Gram phase does not form it) and (iterations + 1) x (8 S^2 + 512 S)
+    (the FP32 factor and its diagonal blocks' inverses once per
+    preconditioner apply); far
     field 8 N flops per direction (its sincos per wire run is not counted);
     antennas of z-parallel wires: 8 flops per (block row, segment) plus 8
     per (direction, run), the per-row path of the kernel."""
@@ -360,12 +361,14 @@ def phase_rooflines(form, o, n, s, g, d, shapes, fma, muladd, ffma, peaks, runs)
         n_s = np.array([u["n"] for u in shapes], np.float64)
         s_s = np.array([u["s"] for u in shapes], np.float64)
         its = it if it is not None and len(it) == len(n_s) else np.full(len(n_s), 5.0)
-        # per operator + preconditioner application: Z once (16 N^2), the
-        # FP32 factor (8 S^2: L below and U above the diagonal blocks) and
-        # the diagonal blocks' FP32 inverses (two 32 x 32 complex64 blocks
-        # per 32 rows: 512 B per row); iterations + 1 of them (the first
-        # pass forms M^H y and applies the preconditioner to it)
-        byt = float(np.sum((its + 1) * (16 * n_s * n_s + 8 * s_s * s_s + 512 * s_s)))
+        # per iteration: Z once (16 N^2) for M^H M, the FP32 factor (8 S^2:
+        # L below and U above the diagonal blocks) and the diagonal blocks'
+        # FP32 inverses (two 32 x 32 complex64 blocks per 32 rows: 512 B per
+        # row); plus the first preconditioner application, and one more Z
+        # pass for M^H y unless the Gram phase formed it (systems of at most
+        # 8 homogeneous columns and 4 right-hand sides)
+        zpass = its + np.where(s_s - n_s <= 8, 0.0, 1.0)
+        byt = float(np.sum(zpass * 16 * n_s * n_s + (its + 1) * (8 * s_s * s_s + 512 * s_s)))
         put("solve", byt / 1e9, peaks["hbm_gbs"], "GB/s", "hbm", peaks["source"])
     dd = np.asarray(d, np.float64)
     nr = np.asarray(runs, np.float64)

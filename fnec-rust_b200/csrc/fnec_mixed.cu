@@ -56,6 +56,13 @@ __device__ __forceinline__ cx zcmul(cx a, cx b) { return {a.re * b.re + a.im * b
 __device__ __forceinline__ cx zadd(cx a, cx b) { return {a.re + b.re, a.im + b.im}; }
 __device__ __forceinline__ cx zsub(cx a, cx b) { return {a.re - b.re, a.im - b.im}; }
 __device__ __forceinline__ cx zscale(cx a, double s) { return {a.re * s, a.im * s}; }
+// One Z entry as a single 16-byte read-only load (Z is read-only after the
+// fill and its entries are 16-byte aligned); the struct's own copy would
+// issue two 8-byte loads.
+__device__ __forceinline__ cx ld_z(const cx *p) {
+    const double2 v = __ldg(reinterpret_cast<const double2 *>(p));
+    return {v.x, v.y};
+}
 __device__ __forceinline__ cx zdiv(cx a, cx b) {
     double inv = 1.0 / (b.re * b.re + b.im * b.im);
     return {(a.re * b.re + a.im * b.im) * inv, (a.im * b.re - a.re * b.im) * inv};
@@ -79,7 +86,8 @@ __constant__ double m_gl_w8[8] = {0.101228536290376, 0.222381034453374, 0.313706
 // length slen / radius srad); the far form takes the midpoint difference
 // d = om - sm and the half-length step hs = sd slen / 2 once per element,
 // then per Gauss-Legendre sample r = d - x_m hs, R^2 = |r|^2 + a^2, one
-// reciprocal square root for R and 1/R and sincospi_taylor(k R / pi).
+// reciprocal square root (rsqrt_newton) for R and 1/R and
+// sincospi_taylor(k R / pi).
 __device__ __forceinline__ cx elem_fast(const double *om, const double *od, const double *sm, const double *sd,
                                         double slen, double srad, double k, bool is_self) {
     double cos_alpha = od[0] * sd[0] + od[1] * sd[1] + od[2] * sd[2];
@@ -110,7 +118,7 @@ __device__ __forceinline__ cx elem_fast(const double *om, const double *od, cons
             const double xm = m_gl_n8[m];
             const double r0 = fma(-xm, h0, d0), r1 = fma(-xm, h1, d1), r2 = fma(-xm, h2, d2);
             const double r2s = fma(r0, r0, fma(r1, r1, fma(r2, r2, a2)));
-            const double inv = rsqrt(r2s);
+            const double inv = rsqrt_newton(r2s);
             double sn, cs;
             sincospi_taylor(kpi * (r2s * inv), sn, cs);
             const double wr = m_gl_w8[m] * inv;
@@ -263,7 +271,7 @@ __global__ void k_gram32_ccols(const UnitDesc *__restrict__ units, const AntDesc
     UnitDesc u = units[blockIdx.y];
     AntDesc a = ants[u.ant];
     int w = blockIdx.x;
-    if (w >= a.w) return;
+    if (w >= a.w || mus[blockIdx.y].first_solve >= 0) return;  // the latter: k_gram32_ccols_mhy
     int n = u.n, s = u.s;
     const cx *z = zbuf + u.z_off;
     const double *cv = cos_buf + u.cos_off;
@@ -286,6 +294,103 @@ __global__ void k_gram32_ccols(const UnitDesc *__restrict__ units, const AntDesc
         if (v == w)
             for (int q = b; q < e; ++q) d += cv[wrow[q]] * cv[wrow[q]];
         A[(int64_t)(n + w) * s + n + v] = cf((float)d, 0.f);
+    }
+}
+
+// The cos columns of k_gram32_ccols and every solve's M^H y together, for
+// a system of at most CM_MAX_W homogeneous columns and CM_MAX_RHS
+// right-hand sides whose solves are consecutive (MixedUnit::first_solve,
+// set at planning): one pass over Z instead of two, a thread per column c
+// (grid.x: blocks of 256 columns, grid.y: system).  The thread walks the
+// rows in order; the current wire's cos sum stays in registers and moves
+// through shared memory when the wire changes, so each wire's sum runs
+// over its rows in increasing order -- k_gram32_ccols's operations and
+// order.  (M^H y)[c] = sum_r conj(Z[r][c]) y[r] runs in row order and the
+// wire entries (M^H y)[n + q] over the wire's rows: the refinement
+// kernel's own sums, written into each solve's work vector b, which the
+// refinement then takes as it is.
+constexpr int CM_MAX_W = 8, CM_MAX_RHS = 4;
+__global__ void __launch_bounds__(256, 3) k_gram32_ccols_mhy(const UnitDesc *__restrict__ units,
+                                                         const UnitDesc *__restrict__ solves,
+                                                         const AntDesc *__restrict__ ants,
+                                                         const MixedUnit *__restrict__ smu,
+                                                         const MixedUnit *__restrict__ mus,
+                                                         const int32_t *__restrict__ ibuf,
+                                                         const cx *__restrict__ zbuf,
+                                                         const double *__restrict__ cos_buf,
+                                                         const cx *__restrict__ rhs, float2 *a32buf, cx *wbuf) {
+    __shared__ cx s_acc[CM_MAX_W][256];
+    const UnitDesc u = units[blockIdx.y];
+    const int first = smu[blockIdx.y].first_solve;
+    if (first < 0) return;
+    const AntDesc a = ants[u.ant];
+    const int n = u.n, s = u.s, W = a.w, nr = u.n_rhs;
+    const int c0 = (int)blockIdx.x * 256;
+    if (c0 >= n) return;
+    const int tid = threadIdx.x, c = c0 + tid;
+    const cx *z = zbuf + u.z_off;
+    const double *cv = cos_buf + u.cos_off;
+    const int32_t *rowwire = ibuf + a.rowwire_off;
+    const int32_t *wptr = ibuf + a.wptr_off, *wrow = ibuf + a.wrow_off;
+    float2 *A = a32buf + smu[blockIdx.y].a32_off;
+    const cx *y[CM_MAX_RHS];
+#pragma unroll
+    for (int k = 0; k < CM_MAX_RHS; ++k) y[k] = rhs + solves[first + min(k, nr - 1)].rhs_off;
+    for (int w = 0; w < W; ++w) s_acc[w][tid] = {0, 0};  // a thread's own column: no barrier
+    if (c < n) {
+        cx bacc[CM_MAX_RHS];
+#pragma unroll
+        for (int k = 0; k < CM_MAX_RHS; ++k) bacc[k] = {0, 0};
+        int cur = n > 0 ? rowwire[0] : 0;
+        double cr = 0, ci = 0;
+        constexpr int RB = 8;  // rows whose loads are in flight together
+        for (int r0 = 0; r0 < n; r0 += RB) {
+            cx zb[RB];
+#pragma unroll
+            for (int j = 0; j < RB; ++j) zb[j] = r0 + j < n ? ld_z(z + (int64_t)(r0 + j) * n + c) : cx{0, 0};
+#pragma unroll
+            for (int j = 0; j < RB; ++j) {
+                const int r = r0 + j;
+                if (r >= n) break;  // uniform over the block
+                const int w = rowwire[r];
+                if (w != cur) {  // uniform over the block
+                    s_acc[cur][tid] = {cr, ci};
+                    cur = w;
+                    cr = s_acc[w][tid].re;
+                    ci = s_acc[w][tid].im;
+                }
+                cr += -cv[r] * zb[j].re;
+                ci += -cv[r] * zb[j].im;
+#pragma unroll
+                for (int k = 0; k < CM_MAX_RHS; ++k)
+                    if (k < nr) bacc[k] = zadd(bacc[k], zcmul(zb[j], y[k][r]));
+            }
+        }
+        s_acc[cur][tid] = {cr, ci};
+        for (int w = 0; w < W; ++w) {
+            const cx v = s_acc[w][tid];
+            A[(int64_t)c * s + n + w] = cf((float)v.re, (float)-v.im);   // conj(Z) * (-cos)
+            A[(int64_t)(n + w) * s + c] = cf((float)v.re, (float)v.im);  // (-cos) * Z
+        }
+#pragma unroll
+        for (int k = 0; k < CM_MAX_RHS; ++k)
+            if (k < nr) wbuf[mus[first + k].w_off + c] = bacc[k];
+    }
+    if (blockIdx.x == 0) {
+        for (int e = tid; e < W * W; e += 256) {
+            const int w = e / W, v = e % W;
+            double d = 0;
+            if (v == w)
+                for (int q = wptr[w]; q < wptr[w + 1]; ++q) d += cv[wrow[q]] * cv[wrow[q]];
+            A[(int64_t)(n + w) * s + n + v] = cf((float)d, 0.f);
+        }
+        for (int e = tid; e < nr * W; e += 256) {
+            const int k = e / W, q = e % W;
+            const cx *yk = rhs + solves[first + k].rhs_off;
+            cx acc = {0, 0};
+            for (int kk = wptr[q]; kk < wptr[q + 1]; ++kk) acc = zadd(acc, zscale(yk[wrow[kk]], -cv[wrow[kk]]));
+            wbuf[mus[first + k].w_off + n + q] = acc;
+        }
     }
 }
 
@@ -1214,6 +1319,7 @@ __device__ double block_sum(double v, double *red) {
 // row costs no HBM traffic.
 constexpr int ARB = 16;  // rows per block (2 per warp)
 
+
 __device__ void apply_A(const GmresCtx &g, const cx *v, cx *out, cx *sv, cx *st, cx *so) {
     int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int n = g.n;
@@ -1239,7 +1345,7 @@ __device__ void apply_A(const GmresCtx &g, const cx *v, cx *out, cx *sv, cx *st,
             const cx x = sv[c];
 #pragma unroll
             for (int q = 0; q < RPW; ++q)
-                if (has[q]) acc[q] = zadd(acc[q], zmul(zr[q][c], x));
+                if (has[q]) acc[q] = zadd(acc[q], zmul(ld_z(zr[q] + c), x));
         }
 #pragma unroll
         for (int q = 0; q < RPW; ++q) {
@@ -1258,10 +1364,10 @@ __device__ void apply_A(const GmresCtx &g, const cx *v, cx *out, cx *sv, cx *st,
             int r = rb;
 #pragma unroll 4
             for (; r + 2 <= re; r += 2, zc += 2 * (int64_t)n) {
-                a0 = zadd(a0, zcmul(zc[0], st[r]));
-                a1 = zadd(a1, zcmul(zc[n], st[r + 1]));
+                a0 = zadd(a0, zcmul(ld_z(zc), st[r]));
+                a1 = zadd(a1, zcmul(ld_z(zc + n), st[r + 1]));
             }
-            if (r < re) a0 = zadd(a0, zcmul(zc[0], st[r]));
+            if (r < re) a0 = zadd(a0, zcmul(ld_z(zc), st[r]));
             so[c] = zadd(a0, a1);
         }
         // no barrier: st rows of the next block are disjoint, and so[c] is
@@ -1526,7 +1632,8 @@ __global__ void __launch_bounds__(256, MINB) k_gmres_ir(const UnitDesc *__restri
                                                   const float2 *__restrict__ a32buf, const int32_t *__restrict__ pivbuf,
                                                   cx *xbuf, cx *vbuf, cx *wbuf, const int32_t *__restrict__ status,
                                                   int staged, int skip_s, int only, int min_s,
-                                                  const int32_t *__restrict__ s_order, const float2 *__restrict__ binvbuf) {
+                                                  const int32_t *__restrict__ s_order, const float2 *__restrict__ binvbuf,
+                                                  int use_b) {
     extern __shared__ unsigned char s_dyn[];
     __shared__ cx sH[(GM + 1) * GM];
     __shared__ double scs[GM];
@@ -1586,18 +1693,22 @@ __global__ void __launch_bounds__(256, MINB) k_gmres_ir(const UnitDesc *__restri
         g.perm = perm;
     }
 
-    // b = M^H y (y is zero on the constraint rows)
-    for (int i = tid; i < g.rows; i += blockDim.x) g.t[i] = i < g.n ? g.y[i] : cx{0, 0};
-    __syncthreads();
-    for (int c = tid; c < g.n; c += blockDim.x) {
-        cx acc = {0, 0};
-        for (int rr = 0; rr < g.n; ++rr) acc = zadd(acc, zcmul(g.z[(int64_t)rr * g.n + c], g.t[rr]));
-        b[c] = acc;
-    }
-    for (int q = tid; q < g.w; q += blockDim.x) {
-        cx acc = {0, 0};
-        for (int k = g.wptr[q]; k < g.wptr[q + 1]; ++k) acc = zadd(acc, zscale(g.t[g.wrow[k]], -g.cv[g.wrow[k]]));
-        b[g.n + q] = acc;
+    // b = M^H y (y is zero on the constraint rows), unless the Gram phase
+    // of this run formed it with the same sums (k_gram32_ccols_mhy; use_b:
+    // the factor is fresh, not a resident re-solve with new sources)
+    if (!(use_b && mu.b_ready)) {
+        for (int i = tid; i < g.rows; i += blockDim.x) g.t[i] = i < g.n ? g.y[i] : cx{0, 0};
+        __syncthreads();
+        for (int c = tid; c < g.n; c += blockDim.x) {
+            cx acc = {0, 0};
+            for (int rr = 0; rr < g.n; ++rr) acc = zadd(acc, zcmul(ld_z(g.z + (int64_t)rr * g.n + c), g.t[rr]));
+            b[c] = acc;
+        }
+        for (int q = tid; q < g.w; q += blockDim.x) {
+            cx acc = {0, 0};
+            for (int k = g.wptr[q]; k < g.wptr[q + 1]; ++k) acc = zadd(acc, zscale(g.t[g.wrow[k]], -g.cv[g.wrow[k]]));
+            b[g.n + q] = acc;
+        }
     }
     // x0 = 0: the first cycle's residual is b itself (no operator pass), and
     // its first Krylov vector P^-1 b is the classical first guess
@@ -2344,6 +2455,8 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
         mu[i].iters = 0;
         mu[i].resid = 0.0;
         mu[i].cs_off = -1;
+        mu[i].b_ready = 0;
+        mu[i].first_solve = -1;
         v += (int64_t)(GM + 1) * u.s;
         wk += 6 * (int64_t)u.s + 2 * (int64_t)rows;  // 4 vectors + rows, then the unstaged copies
     }
@@ -2352,6 +2465,34 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
     for (size_t i = 0; i < systems.size(); ++i) {
         sysmu[i].a32_off = a32_of[i];
         sysmu[i].binv_off = binv_of[i];
+        sysmu[i].first_solve = -1;
+        sysmu[i].b_ready = 0;
+    }
+    // systems whose M^H y the Gram phase forms with its cos columns
+    // (k_gram32_ccols_mhy): few homogeneous columns and right-hand sides,
+    // solves numbered consecutively
+    w.mhy_systems = 0;
+    w.mhy_max_n = 0;
+    {
+        std::vector<int> first(systems.size(), -1), count(systems.size(), 0);
+        std::vector<char> consecutive(systems.size(), 1);
+        for (size_t i = 0; i < solves.size(); ++i) {
+            const int sy = solves[i].sys;
+            if (first[sy] < 0) first[sy] = (int)i;
+            else if (first[sy] + count[sy] != (int)i) consecutive[sy] = 0;
+            ++count[sy];
+        }
+        for (size_t i = 0; i < systems.size(); ++i) {
+            const UnitDesc &u = systems[i];
+            const AntDesc &a = ants[u.ant];
+            if (first[i] < 0 || !consecutive[i] || count[i] != u.n_rhs || u.n_rhs > CM_MAX_RHS || a.w > CM_MAX_W ||
+                a.hom2 != 0)
+                continue;
+            sysmu[i].first_solve = first[i];
+            for (int k = 0; k < count[i]; ++k) mu[first[i] + k].b_ready = 1;
+            ++w.mhy_systems;
+            w.mhy_max_n = std::max(w.mhy_max_n, u.n);
+        }
     }
     size_t b_mu = sizeof(MixedUnit) * (mu.size() + 1);
     size_t b_smu = sizeof(MixedUnit) * (sysmu.size() + 1);
@@ -2628,7 +2769,8 @@ uint64_t refine_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const Unit
     if (ns > 0) {
         auto gk = mw.gmres_minb == 4 ? k_gmres_ir<4> : k_gmres_ir<3>;
         gk<<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x, mw.v, mw.w, status,
-                                  staged, skip_s, -1, min_s, mw.s_order, mw.use_binv ? mw.binv : nullptr);
+                                  staged, skip_s, -1, min_s, mw.s_order, mw.use_binv ? mw.binv : nullptr,
+                                  fresh_factor ? 1 : 0);
         cudaError_t le = cudaPeekAtLastError();
         if (le != cudaSuccess && !marks.detail[0])
             std::snprintf(marks.detail, sizeof(marks.detail), "GMRES launch: %d solves, %zu B shared (%s), max_s %d, rows %d",
@@ -2662,7 +2804,7 @@ uint64_t refine_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const Unit
                 (void)cudaGetLastError();  // not co-resident: refine this solve in one CTA
                 k_gmres_ir<3><<<ns, 256, smem, st>>>(d_solves, d_ants, mw.mu, ibuf, crows, z, rhs, cosv, mw.a32, piv, x,
                                                   mw.v, mw.w, status, staged, INT_MAX, ui, 0, mw.s_order,
-                                                  mw.use_binv ? mw.binv : nullptr);
+                                                  mw.use_binv ? mw.binv : nullptr, fresh_factor ? 1 : 0);
             }
             L += 2;
         }
@@ -2706,6 +2848,12 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     {
         dim3 g(max_w > 0 ? max_w : 1, nu);
         k_gram32_ccols<<<g, 256, 0, st>>>(d_units, d_ants, mw.smu, ibuf, z, cosv, mw.a32);
+    }
+    if (mw.mhy_systems > 0) {
+        dim3 g((unsigned)((mw.mhy_max_n + 255) / 256), (unsigned)nu);
+        k_gram32_ccols_mhy<<<g, 256, 0, st>>>(d_units, d_solves, d_ants, mw.smu, mw.mu, ibuf, z, cosv, rhs, mw.a32,
+                                              mw.w);
+        ++L;
     }
     k_gram32_rest<<<nu, 256, 0, st>>>(d_units, d_ants, mw.smu, ibuf, crows, mw.a32);
     L += 3;
@@ -2928,6 +3076,36 @@ cudaError_t read_mixed_stats(MixedWork &mw, int32_t *iters, double *resid, cudaS
 }
 
 }  // namespace fnec
+
+namespace {
+__global__ void k_test_rsqrt(const double *x, int n, double *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = fnec::rsqrt_newton(x[i]);
+}
+}  // namespace
+
+// The fill's reciprocal square root on the device (n <= 2^20 values, each
+// normal, finite and > 0): staged through device memory of its own.
+extern "C" int fnec_test_fill_rsqrt(const double *x, uint64_t n, double *out) {
+    if (n && (!x || !out)) return FNEC_ERR_BAD_ARG;
+    if (n > ((uint64_t)1 << 20)) return FNEC_ERR_TOO_LARGE;
+    for (uint64_t i = 0; i < n; ++i)
+        if (!(x[i] >= 2.2250738585072014e-308 && x[i] < INFINITY)) return FNEC_ERR_BAD_ARG;
+    if (n == 0) return FNEC_OK;
+    double *d = nullptr;
+    if (cudaMalloc(&d, sizeof(double) * 2 * n) != cudaSuccess) {
+        (void)cudaGetLastError();
+        return FNEC_ERR_OUT_OF_MEMORY;
+    }
+    cudaError_t e = cudaMemcpy(d, x, sizeof(double) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_test_rsqrt<<<(unsigned)((n + 255) / 256), 256>>>(d, (int)n, d + n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out, d + n, sizeof(double) * n, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    return e == cudaSuccess ? FNEC_OK : FNEC_ERR_CUDA;
+}
 
 extern "C" int fnec_test_fill_sincospi(const double *x, uint64_t n, double *sin_out, double *cos_out) {
     if ((n && (!x || !sin_out || !cos_out))) return FNEC_ERR_BAD_ARG;

@@ -26,6 +26,8 @@ struct MixedUnit {
     double resid;     // final preconditioned relative residual
     int64_t cs_off;   // complex128 scratch of the cluster GMRES (-1: none)
     int64_t binv_off; // complex64 inverses of the factor's 32x32 diagonal blocks (per system)
+    int32_t b_ready;     // per solve: the Gram phase writes M^H y into the work vector b
+    int32_t first_solve; // per system: its first solve when the Gram phase forms M^H y, else -1
 };
 
 struct MixedWork {
@@ -40,6 +42,8 @@ struct MixedWork {
     cx *w = nullptr;
     int n_units = 0;
     int max_s = 0;
+    int mhy_systems = 0;  // systems whose M^H y the Gram phase forms (k_gram32_ccols_mhy)
+    int mhy_max_n = 0;    // and their largest N
     std::vector<MixedUnit> host;
     // large solves refined by the grid-wide GMRES, one cooperative launch each
     std::vector<int> grid_solves;

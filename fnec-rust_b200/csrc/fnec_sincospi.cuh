@@ -1,6 +1,7 @@
 // fnec_sincospi.cuh -- sin(pi x), cos(pi x) from a quadrant reduction and
-// Taylor series (host and device), for the FMA-contracted kernels whose
-// phases need about 1e-16 absolute accuracy but not a particular libm's bits.
+// Taylor series, and 1/sqrt(x) by Newton's iteration (host and device), for
+// the FMA-contracted kernels whose phases and distances need about 1e-16
+// relative accuracy but not a particular libm's bits.
 #pragma once
 #include <cmath>
 #include <cstring>
@@ -49,6 +50,25 @@ __host__ __device__ __forceinline__ void sincospi_taylor(double x, double &sn, d
     const double a = (q & 1) ? c0 : s0, b = (q & 1) ? s0 : c0;
     sn = (q & 2) ? -a : a;
     cs = ((q + 1) & 2) ? -b : b;
+}
+
+// 1/sqrt(x) for normal, finite x > 0: a single-precision first guess
+// (about 23 correct bits; the device's approximate reciprocal square root),
+// then two Newton steps for f(y) = y^-2 - x in FP64,
+// y <- y + (y / 2)(1 - x y^2), each doubling the correct bits: within about
+// 3e-16 relative of the true value over the fill's range (R^2 from 1e-8 to
+// 1e4 m^2).  Nine FP64 / conversion operations and no branch.
+__host__ __device__ __forceinline__ double rsqrt_newton(double x) {
+#ifdef __CUDA_ARCH__
+    double y = (double)rsqrtf((float)x);
+#else
+    double y = (double)(1.0f / std::sqrt((float)x));
+#endif
+    double e = fma(-x * y, y, 1.0);
+    y = fma(0.5 * y, e, y);
+    e = fma(-x * y, y, 1.0);
+    y = fma(0.5 * y, e, y);
+    return y;
 }
 
 // Either sign: sin(pi x) is odd, cos(pi x) even.

@@ -198,6 +198,7 @@ SIGNATURES = {
     "fnec_batch_resolve": (ctypes.c_int, [_P]),
     "fnec_test_fail_device_allocation": (ctypes.c_int, [_I32]),
     "fnec_test_fill_sincospi": (ctypes.c_int, [_P, _U64, _P, _P]),
+    "fnec_test_fill_rsqrt": (ctypes.c_int, [_P, _U64, _P]),
     "fnec_host_cache_release": (ctypes.c_int, [_P]),
     "fnec_device_cache_release": (ctypes.c_int, [_P, _P]),
     "fnec_batch_create": (ctypes.c_int, [_P, _P, _U32, _I32, _P]),
@@ -634,6 +635,17 @@ def test_fill_sincospi(x):
     if rc != OK:
         raise AccelError(rc, "test_fill_sincospi")
     return s, c
+
+
+def test_fill_rsqrt(x):
+    """Test hook: the mixed fill's reciprocal square root, run on the
+    current device (normal, finite, positive x; at most 2^20 values)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    out = np.empty_like(x)
+    rc = lib().fnec_test_fill_rsqrt(_ptr(x), len(x), _ptr(out))
+    if rc != OK:
+        raise AccelError(rc, "test_fill_rsqrt")
+    return out
 
 
 def measure_fp32_peak(device: int = 0) -> float:

@@ -554,6 +554,10 @@ int fnec_test_fail_device_allocation(int32_t after);
  * is compiled for the host): fnec_test_fill_sincospi runs it on the host
  * for n arguments 0 <= x < 2^50 (test use). */
 int fnec_test_fill_sincospi(const double *x, uint64_t n, double *sin_out, double *cos_out);
+/* The fill's reciprocal square root (a single-precision guess and two
+ * Newton steps), run on the current device for n <= 2^20 normal, finite,
+ * positive arguments (test use; allocates its own device memory). */
+int fnec_test_fill_rsqrt(const double *x, uint64_t n, double *out);
 
 /* Radiation pattern that allocates no device memory.  No counterpart in
  * the reference: it serves callers that cannot call cudaMalloc -- a host
