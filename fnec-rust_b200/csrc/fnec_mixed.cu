@@ -309,7 +309,11 @@ __global__ void k_gram32_ccols(const UnitDesc *__restrict__ units, const AntDesc
 // wire entries (M^H y)[n + q] over the wire's rows: the refinement
 // kernel's own sums, written into each solve's work vector b, which the
 // refinement then takes as it is.
+// NRMAX: one instance for the systems of one right-hand side (the common
+// case: fewer registers, so the next rows' loads fit beside the sums), one
+// for 2 .. CM_MAX_RHS; each skips the other's systems.
 constexpr int CM_MAX_W = 8, CM_MAX_RHS = 4;
+template <int NRMAX>
 __global__ void __launch_bounds__(256, 3) k_gram32_ccols_mhy(const UnitDesc *__restrict__ units,
                                                          const UnitDesc *__restrict__ solves,
                                                          const AntDesc *__restrict__ ants,
@@ -325,6 +329,7 @@ __global__ void __launch_bounds__(256, 3) k_gram32_ccols_mhy(const UnitDesc *__r
     if (first < 0) return;
     const AntDesc a = ants[u.ant];
     const int n = u.n, s = u.s, W = a.w, nr = u.n_rhs;
+    if ((NRMAX == 1) != (nr == 1)) return;  // the other instance's systems
     const int c0 = (int)blockIdx.x * 256;
     if (c0 >= n) return;
     const int tid = threadIdx.x, c = c0 + tid;
@@ -333,21 +338,26 @@ __global__ void __launch_bounds__(256, 3) k_gram32_ccols_mhy(const UnitDesc *__r
     const int32_t *rowwire = ibuf + a.rowwire_off;
     const int32_t *wptr = ibuf + a.wptr_off, *wrow = ibuf + a.wrow_off;
     float2 *A = a32buf + smu[blockIdx.y].a32_off;
-    const cx *y[CM_MAX_RHS];
+    const cx *y[NRMAX];
 #pragma unroll
-    for (int k = 0; k < CM_MAX_RHS; ++k) y[k] = rhs + solves[first + min(k, nr - 1)].rhs_off;
+    for (int k = 0; k < NRMAX; ++k) y[k] = rhs + solves[first + min(k, nr - 1)].rhs_off;
     for (int w = 0; w < W; ++w) s_acc[w][tid] = {0, 0};  // a thread's own column: no barrier
     if (c < n) {
-        cx bacc[CM_MAX_RHS];
+        cx bacc[NRMAX];
 #pragma unroll
-        for (int k = 0; k < CM_MAX_RHS; ++k) bacc[k] = {0, 0};
+        for (int k = 0; k < NRMAX; ++k) bacc[k] = {0, 0};
         int cur = n > 0 ? rowwire[0] : 0;
         double cr = 0, ci = 0;
-        constexpr int RB = 8;  // rows whose loads are in flight together
-        for (int r0 = 0; r0 < n; r0 += RB) {
-            cx zb[RB];
+        constexpr int RB = 4;  // rows per batch; the next batch's loads are in flight meanwhile
+        cx zb[RB], zn[RB];
 #pragma unroll
-            for (int j = 0; j < RB; ++j) zb[j] = r0 + j < n ? ld_z(z + (int64_t)(r0 + j) * n + c) : cx{0, 0};
+        for (int j = 0; j < RB; ++j) zb[j] = j < n ? ld_z(z + (int64_t)j * n + c) : cx{0, 0};
+        for (int r0 = 0; r0 < n; r0 += RB) {
+#pragma unroll
+            for (int j = 0; j < RB; ++j) {
+                const int r = r0 + RB + j;
+                zn[j] = r < n ? ld_z(z + (int64_t)r * n + c) : cx{0, 0};
+            }
 #pragma unroll
             for (int j = 0; j < RB; ++j) {
                 const int r = r0 + j;
@@ -362,9 +372,11 @@ __global__ void __launch_bounds__(256, 3) k_gram32_ccols_mhy(const UnitDesc *__r
                 cr += -cv[r] * zb[j].re;
                 ci += -cv[r] * zb[j].im;
 #pragma unroll
-                for (int k = 0; k < CM_MAX_RHS; ++k)
+                for (int k = 0; k < NRMAX; ++k)
                     if (k < nr) bacc[k] = zadd(bacc[k], zcmul(zb[j], y[k][r]));
             }
+#pragma unroll
+            for (int j = 0; j < RB; ++j) zb[j] = zn[j];
         }
         s_acc[cur][tid] = {cr, ci};
         for (int w = 0; w < W; ++w) {
@@ -373,7 +385,7 @@ __global__ void __launch_bounds__(256, 3) k_gram32_ccols_mhy(const UnitDesc *__r
             A[(int64_t)(n + w) * s + c] = cf((float)v.re, (float)v.im);  // (-cos) * Z
         }
 #pragma unroll
-        for (int k = 0; k < CM_MAX_RHS; ++k)
+        for (int k = 0; k < NRMAX; ++k)
             if (k < nr) wbuf[mus[first + k].w_off + c] = bacc[k];
     }
     if (blockIdx.x == 0) {
@@ -2851,9 +2863,11 @@ uint64_t run_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const UnitDes
     }
     if (mw.mhy_systems > 0) {
         dim3 g((unsigned)((mw.mhy_max_n + 255) / 256), (unsigned)nu);
-        k_gram32_ccols_mhy<<<g, 256, 0, st>>>(d_units, d_solves, d_ants, mw.smu, mw.mu, ibuf, z, cosv, rhs, mw.a32,
-                                              mw.w);
-        ++L;
+        k_gram32_ccols_mhy<1><<<g, 256, 0, st>>>(d_units, d_solves, d_ants, mw.smu, mw.mu, ibuf, z, cosv, rhs, mw.a32,
+                                                 mw.w);
+        k_gram32_ccols_mhy<CM_MAX_RHS><<<g, 256, 0, st>>>(d_units, d_solves, d_ants, mw.smu, mw.mu, ibuf, z, cosv, rhs,
+                                                          mw.a32, mw.w);
+        L += 2;
     }
     k_gram32_rest<<<nu, 256, 0, st>>>(d_units, d_ants, mw.smu, ibuf, crows, mw.a32);
     L += 3;
