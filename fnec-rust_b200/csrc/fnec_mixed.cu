@@ -1444,61 +1444,113 @@ __device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, cx *sy) {
     if (g.binv) {
         // block products with the diagonal blocks' inverses: every warp
         // takes rows of the 32x32 product (no serial substitution chain),
-        // then all threads update the rows outside the block
+        // then all threads update the rows outside the block (the refinement
+        // kernels run 256 threads: 8 warps x 4 rows of each block)
         __shared__ cx s_blk[32];
+        // each warp's 4 rows of the next block's inverse are loaded one block
+        // step ahead (blockDim 256: 8 warps x 4 rows = 32); entries outside
+        // an nb < 32 block are stored as zeros
+        float2 li[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) li[q] = g.binv[(wid + 8 * q) * 32 + lane];
         for (int c0 = 0; c0 < s; c0 += 32) {
             const int nb = min(32, s - c0);
-            const float2 *Li = g.binv + (int64_t)(c0 / 32) * 2048;
             const cx xk = lane < nb ? sy[c0 + lane] : cx{0, 0};
-            for (int i = wid; i < nb; i += (int)(blockDim.x >> 5)) {
-                cx p = warp_sum(lane < nb ? zmul(f2z(Li[i * 32 + lane]), xk) : cx{0, 0});
-                if (lane == 0) s_blk[i] = p;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int i = wid + 8 * q;
+                cx p = warp_sum(lane < nb ? zmul(f2z(li[q]), xk) : cx{0, 0});
+                if (lane == 0 && i < nb) s_blk[i] = p;
+            }
+            if (c0 + 32 < s) {
+                const float2 *Ln = g.binv + (int64_t)(c0 / 32 + 1) * 2048;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) li[q] = Ln[(wid + 8 * q) * 32 + lane];
             }
             __syncthreads();
             for (int i = tid; i < nb; i += blockDim.x) sy[c0 + i] = s_blk[i];
             if (nb == 32) {
-                for (int r = c0 + 32 + tid; r < s; r += blockDim.x) {
-                    const float2 *lrow = g.lu + (int64_t)r * s + c0;
-                    cx acc = sy[r];
+                // threads per row: adjacent lanes split a short trailing
+                // block's 32 columns (their partial sums meet by shuffles),
+                // so a step takes fewer rounds of dependent loads
+                const int rows = s - (c0 + 32);
+                const int tpr = rows <= 64 ? 4 : (rows <= 128 ? 2 : 1);
+                const int per = 256 / tpr, cols = 32 / tpr, part = tid % tpr;
+                for (int base = 0; base < rows; base += per) {
+                    const int r = c0 + 32 + base + tid / tpr;
+                    cx acc = {0, 0};
+                    if (r < s) {
+                        const float2 *lrow = g.lu + (int64_t)r * s + c0 + part * cols;
+                        const cx *sb = s_blk + part * cols;
+                        for (int c8 = 0; c8 < cols; c8 += 8) {
+                            float2 lr[8];
 #pragma unroll
-                    for (int c8 = 0; c8 < 32; c8 += 8) {
-                        float2 lr[8];
+                            for (int c = 0; c < 8; ++c) lr[c] = lrow[c8 + c];
 #pragma unroll
-                        for (int c = 0; c < 8; ++c) lr[c] = lrow[c8 + c];
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) acc = zsub(acc, zmul(f2z(lr[c]), s_blk[c8 + c]));
+                            for (int c = 0; c < 8; ++c) acc = zadd(acc, zmul(f2z(lr[c]), sb[c8 + c]));
+                        }
                     }
-                    sy[r] = acc;
+                    for (int o = tpr >> 1; o > 0; o >>= 1) {
+                        acc.re += __shfl_xor_sync(0xffffffffu, acc.re, o);
+                        acc.im += __shfl_xor_sync(0xffffffffu, acc.im, o);
+                    }
+                    if (r < s && part == 0) sy[r] = zsub(sy[r], acc);
                 }
             }
             __syncthreads();
         }
+        {
+            const float2 *Ul = g.binv + (int64_t)((s - 1) / 32) * 2048 + 1024;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) li[q] = Ul[(wid + 8 * q) * 32 + lane];
+        }
         for (int c0 = ((s - 1) / 32) * 32; c0 >= 0; c0 -= 32) {
             const int nb = min(32, s - c0);
-            const float2 *Ui = g.binv + (int64_t)(c0 / 32) * 2048 + 1024;
             const cx xk = lane < nb ? sy[c0 + lane] : cx{0, 0};
-            for (int i = wid; i < nb; i += (int)(blockDim.x >> 5)) {
-                cx p = warp_sum(lane < nb ? zmul(f2z(Ui[i * 32 + lane]), xk) : cx{0, 0});
-                if (lane == 0) s_blk[i] = p;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int i = wid + 8 * q;
+                cx p = warp_sum(lane < nb ? zmul(f2z(li[q]), xk) : cx{0, 0});
+                if (lane == 0 && i < nb) s_blk[i] = p;
+            }
+            if (c0 > 0) {
+                const float2 *Un = g.binv + (int64_t)(c0 / 32 - 1) * 2048 + 1024;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) li[q] = Un[(wid + 8 * q) * 32 + lane];
             }
             __syncthreads();
             for (int i = tid; i < nb; i += blockDim.x) sy[c0 + i] = s_blk[i];
-            for (int r = tid; r < c0; r += blockDim.x) {
-                const float2 *urow = g.lu + (int64_t)r * s + c0;
-                cx acc = sy[r];
-                if (nb == 32) {
+            if (nb == 32) {
+                const int rows = c0;
+                const int tpr = rows <= 64 ? 4 : (rows <= 128 ? 2 : 1);
+                const int per = 256 / tpr, cols = 32 / tpr, part = tid % tpr;
+                for (int base = 0; base < rows; base += per) {
+                    const int r = base + tid / tpr;
+                    cx acc = {0, 0};
+                    if (r < c0) {
+                        const float2 *urow = g.lu + (int64_t)r * s + c0 + part * cols;
+                        const cx *sb = s_blk + part * cols;
+                        for (int c8 = 0; c8 < cols; c8 += 8) {
+                            float2 ur[8];
 #pragma unroll
-                    for (int c8 = 0; c8 < 32; c8 += 8) {
-                        float2 ur[8];
+                            for (int c = 0; c < 8; ++c) ur[c] = urow[c8 + c];
 #pragma unroll
-                        for (int c = 0; c < 8; ++c) ur[c] = urow[c8 + c];
-#pragma unroll
-                        for (int c = 0; c < 8; ++c) acc = zsub(acc, zmul(f2z(ur[c]), s_blk[c8 + c]));
+                            for (int c = 0; c < 8; ++c) acc = zadd(acc, zmul(f2z(ur[c]), sb[c8 + c]));
+                        }
                     }
-                } else {
-                    for (int c = 0; c < nb; ++c) acc = zsub(acc, zmul(f2z(urow[c]), s_blk[c]));
+                    for (int o = tpr >> 1; o > 0; o >>= 1) {
+                        acc.re += __shfl_xor_sync(0xffffffffu, acc.re, o);
+                        acc.im += __shfl_xor_sync(0xffffffffu, acc.im, o);
+                    }
+                    if (r < c0 && part == 0) sy[r] = zsub(sy[r], acc);
                 }
-                sy[r] = acc;
+            } else {
+                for (int r = tid; r < c0; r += blockDim.x) {
+                    const float2 *urow = g.lu + (int64_t)r * s + c0;
+                    cx acc = sy[r];
+                    for (int c = 0; c < nb; ++c) acc = zsub(acc, zmul(f2z(urow[c]), s_blk[c]));
+                    sy[r] = acc;
+                }
             }
             __syncthreads();
         }
