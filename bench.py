@@ -300,7 +300,7 @@ def dram_traffic(phase, form, units, workload=None):
     capture of a smaller case of the same workload when there is one, else
     of the sweep workload."""
     key = {("solve", "mixed"): "solve_mixed", ("farfield", "mixed"): "farfield", ("farfield", "fp64"): "farfield",
-           ("fill", "fp64"): "fill_fp64"}.get((phase, form))
+           ("fill", "fp64"): "fill_fp64", ("fill", "mixed"): "fill_mixed"}.get((phase, form))
     try:
         with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), "profiles", "traffic.json")) as fh:
             t = json.load(fh)
