@@ -1651,16 +1651,21 @@ __device__ void apply_prec(const GmresCtx &g, const cx *in, cx *out, cx *sy) {
 // The inverses of every system's 32x32 diagonal blocks of the factor (any
 // factor: unit-lower L11, U11 on and above the diagonal), one CTA of 256
 // threads per block (herm_block_inverse).
+// One CTA per 32-row diagonal block of every system: tab[blockIdx.x] =
+// (system, block), built at planning, so no CTA is launched for a block a
+// system does not have.
 __global__ void __launch_bounds__(256) k_block_inv32(const UnitDesc *__restrict__ units,
                                                      const MixedUnit *__restrict__ smu,
                                                      const float2 *__restrict__ a32buf, float2 *binvbuf,
-                                                     const int32_t *__restrict__ status) {
+                                                     const int32_t *__restrict__ status,
+                                                     const int2 *__restrict__ tab) {
     __shared__ float2 sB[MNB][MNB + 1];
     __shared__ float2 sDinv[MNB];
     __shared__ float2 sX[2 * MNB * BI_PITCH];
-    const int ui = blockIdx.y;
+    const int2 t = tab[blockIdx.x];
+    const int ui = t.x;
     const UnitDesc u = units[ui];
-    const int c0 = blockIdx.x * 32, s = u.s;
+    const int c0 = t.y * 32, s = u.s;
     if (c0 >= s || status[ui] != 0) return;
     const int nb = min(32, s - c0);
     const float2 *A = a32buf + smu[ui].a32_off;
@@ -1676,7 +1681,7 @@ __global__ void __launch_bounds__(256) k_block_inv32(const UnitDesc *__restrict_
         sDinv[tid] = tid < nb ? cf(d.x / dn, -d.y / dn) : cf(0.f, 0.f);
     }
     __syncthreads();
-    herm_block_inverse(sB, sDinv, nb, sX, binvbuf + smu[ui].binv_off + (int64_t)blockIdx.x * 2048);
+    herm_block_inverse(sB, sDinv, nb, sX, binvbuf + smu[ui].binv_off + (int64_t)t.y * 2048);
 }
 
 __device__ double vnorm(const cx *v, int s, double *red) {
@@ -2566,7 +2571,11 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
     auto al = [](size_t x) { return (x + 255) / 256 * 256; };
     size_t b_ord = sizeof(int32_t) * (solves.size() + 1);
     size_t b_binv = sizeof(float2) * (size_t)(binv + 1);
-    size_t total = al(b_mu) + al(b_smu) + al(b_a32) + al(b_v) + al(b_w) + al(b_ord) + al(b_binv);
+    std::vector<int2> btab;  // (system, 32-row block) of every diagonal block
+    for (size_t i = 0; i < systems.size(); ++i)
+        for (int k = 0; k < (systems[i].s + 31) / 32; ++k) btab.push_back(make_int2((int)i, k));
+    size_t b_btab = sizeof(int2) * (btab.size() + 1);
+    size_t total = al(b_mu) + al(b_smu) + al(b_a32) + al(b_v) + al(b_w) + al(b_ord) + al(b_binv) + al(b_btab);
     cudaError_t e = dev.alloc(&w.base, total);
     if (e != cudaSuccess) return e;
     unsigned char *p = (unsigned char *)w.base;
@@ -2590,6 +2599,9 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
     w.s_order = (int32_t *)p;
     p += al(b_ord);
     w.binv = (float2 *)p;
+    p += al(b_binv);
+    w.binv_tab = (int2 *)p;
+    w.n_binv = (int)btab.size();
     w.bytes = total;
     w.n_units = (int)solves.size();
     w.max_s = max_s;
@@ -2750,6 +2762,7 @@ cudaError_t alloc_mixed(MixedWork &w, const std::vector<UnitDesc> &systems, cons
         if (!ok) (void)cudaGetLastError();  // one stream: the groups run in sequence
     }
     e = dev.upload(w.s_order, lpt.data(), sizeof(int32_t) * lpt.size());
+    if (e == cudaSuccess && !btab.empty()) e = dev.upload(w.binv_tab, btab.data(), sizeof(int2) * btab.size());
     if (e == cudaSuccess) e = dev.upload(w.mu, mu.data(), sizeof(MixedUnit) * mu.size());
     if (e == cudaSuccess)
         e = dev.upload(w.smu, sysmu.data(), sizeof(MixedUnit) * sysmu.size());
@@ -2802,9 +2815,10 @@ uint64_t refine_mixed(MixedWork &mw, const UnitDesc *d_units, int nu, const Unit
     const bool grid_refine = mw.grid_on && !mw.grid_solves.empty();
     const int skip_s = grid_refine ? GG_MIN_S : INT_MAX;
     if (fresh_factor && mw.use_binv && nu > 0) {  // the preconditioner's diagonal block inverses
-        k_block_inv32<<<dim3((unsigned)((max_s + 31) / 32), (unsigned)nu), 256, 0, st>>>(d_units, mw.smu, mw.a32, mw.binv,
-                                                                                      status);
-        ++L;
+        if (mw.n_binv > 0) {
+            k_block_inv32<<<(unsigned)mw.n_binv, 256, 0, st>>>(d_units, mw.smu, mw.a32, mw.binv, status, mw.binv_tab);
+            ++L;
+        }
     }
     int min_s = 0;  // solves below this are refined by the cluster kernel
     if (ns > 0 && mw.cluster_c > 1) {

@@ -37,6 +37,8 @@ struct MixedWork {
     MixedUnit *smu = nullptr;  // per system (a32_off only)
     float2 *a32 = nullptr;
     float2 *binv = nullptr;      // per system: ceil(S/32) x (L11^-1, U11^-1), 32x32 each
+    int2 *binv_tab = nullptr;    // (system, block) of every diagonal block: k_block_inv32's grid
+    int n_binv = 0;
     int32_t *s_order = nullptr;  // solves by decreasing N^2 (refinement launch order)
     cx *v = nullptr;
     cx *w = nullptr;
